@@ -1,0 +1,171 @@
+"""cheese_b200: B200-native rebuild of cheese's level-synchronous branch-and-bound search.
+
+The product is the sm_100a library behind include/cheese_b200.h (cheese_b200/lib/libcheese_b200.so) and the
+drop-in binary cheese_b200/bin/cheese. This module is a thin ctypes host over that C ABI, with the same
+interface as the reference's process boundary (src/cheese.cu:1851-1895): a spec text in, the per-level JSON
+statistics, the found circuit and the exit code out. There is no CPU fallback: without the compiled library
+every call raises.
+"""
+import ctypes as C
+import os
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libcheese_b200.so"
+BIN_DIR = PKG / "bin"
+MAX_DEPTH = 48
+
+CIRCUIT, PROOF, ERR_SPEC, ERR_USAGE, ERR_OVERFLOW, ERR_CUDA = 0, 1, 2, 3, 4, 5
+
+
+class LevelStats(C.Structure):
+    _fields_ = [("t", C.c_int), ("parents", C.c_int64), ("prefixes", C.c_int64), ("cut_w3", C.c_int64),
+                ("cut_lb", C.c_int64), ("survivors", C.c_int64), ("distinct", C.c_int64),
+                ("proved_unsat", C.c_int), ("seconds", C.c_double)]
+
+
+class Options(C.Structure):
+    _fields_ = [("depth", C.c_int), ("dedupe", C.c_int), ("sym", C.c_int), ("store64", C.c_int),
+                ("profile", C.c_int)]
+
+
+class Result(C.Structure):
+    _fields_ = [("rc", C.c_int), ("depth0", C.c_int), ("found_len", C.c_int), ("found", C.c_int * MAX_DEPTH),
+                ("n_found", C.c_int64), ("nsym", C.c_int), ("store64", C.c_int), ("levels", C.c_int),
+                ("prefixes", C.c_int64), ("kernel_launches", C.c_int64), ("t_evals", C.c_int64),
+                ("children", C.c_int64), ("expand_ms", C.c_double), ("dedupe_ms", C.c_double),
+                ("total_ms", C.c_double), ("error", C.c_char * 256)]
+
+
+LEVEL_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(LevelStats))
+
+# every C entry point of include/cheese_b200.h with its ctypes signature
+SIGNATURES = {
+    "cz_spec_parse": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
+    "cz_spec_free": (None, [C.c_void_p]),
+    "cz_spec_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "cz_spec_gate_name": (C.c_char_p, [C.c_void_p, C.c_int]),
+    "cz_spec_is_states": (C.c_int, [C.c_void_p]),
+    "cz_engine_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
+    "cz_engine_destroy": (None, [C.c_void_p]),
+    "cz_options_default": (None, [C.POINTER(Options)]),
+    "cz_search": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Options), LEVEL_FN, C.c_void_p, C.POINTER(Result)]),
+    "cz_search_text": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(Options), LEVEL_FN, C.c_void_p,
+                                 C.POINTER(Result)]),
+    "cz_version": (C.c_char_p, []),
+}
+
+_lib = None
+
+
+def lib():
+    """the compiled library (raises when it has not been built: there is no fallback path)"""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m cheese_b200.build`")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype, f.argtypes = res, args
+        _lib = L
+    return _lib
+
+
+class Spec:
+    """a parsed spec (the reference's text grammar)"""
+
+    def __init__(self, text):
+        if isinstance(text, str):
+            text = text.encode()
+        self._h = C.c_void_p()
+        err = C.create_string_buffer(256)
+        rc = lib().cz_spec_parse(text, len(text), C.byref(self._h), err, 256)
+        if rc:
+            raise SpecError(rc, err.value.decode())
+        n, g, d = C.c_int(), C.c_int(), C.c_int()
+        lib().cz_spec_info(self._h, C.byref(n), C.byref(g), C.byref(d))
+        self.n, self.gates, self.depth = n.value, g.value, d.value
+        self.names = [lib().cz_spec_gate_name(self._h, i).decode() for i in range(self.gates)]
+        self.states = bool(lib().cz_spec_is_states(self._h))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.cz_spec_free(self._h)
+            self._h = None
+
+
+class SpecError(Exception):
+    def __init__(self, rc, msg):
+        super().__init__(msg)
+        self.rc = rc
+
+
+class Engine:
+    """one CUDA device and stream; searches run one at a time on it"""
+
+    def __init__(self, device=0):
+        self._h = C.c_void_p()
+        err = C.create_string_buffer(256)
+        rc = lib().cz_engine_create(device, C.byref(self._h), err, 256)
+        if rc:
+            raise RuntimeError(f"engine on device {device}: {err.value.decode()}")
+
+    def close(self):
+        if self._h:
+            lib().cz_engine_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self.close()
+
+    def search(self, spec, depth=-1, dedupe=True, sym=True, store64=False, profile=False, on_level=None):
+        """run `cheese SPEC [--depth D] [--no-dedupe] [--no-sym]`; returns a SearchOutcome"""
+        if not isinstance(spec, Spec):
+            spec = Spec(spec)
+        opt = Options(depth, int(dedupe), int(sym), int(store64), int(profile))
+        levels = []
+
+        def cb(_user, p):
+            s = p.contents
+            d = {k: getattr(s, k) for k, _ in LevelStats._fields_}
+            d["proved_unsat"] = bool(d["proved_unsat"])
+            levels.append(d)
+            if on_level:
+                on_level(d)
+
+        res = Result()
+        rc = lib().cz_search(self._h, spec._h, C.byref(opt), LEVEL_FN(cb), None, C.byref(res))
+        return SearchOutcome(spec, rc, levels, res)
+
+
+class SearchOutcome:
+    def __init__(self, spec, rc, levels, res):
+        self.rc, self.levels, self.raw = rc, levels, res
+        self.depth0 = bool(res.depth0)
+        self.circuit = [spec.names[res.found[i]] for i in range(res.found_len)]
+        self.n_found = res.n_found
+        self.error = res.error.decode()
+
+    def lines(self, seconds=False):
+        """stdout of the reference binary for this search (seconds as 0.00 unless asked for)"""
+        out = []
+        for s in self.levels:
+            sec = f"{s['seconds']:.2f}" if seconds else "0.00"
+            out.append(f'{{"t": {s["t"]}, "parents": {s["parents"]}, "prefixes": {s["prefixes"]}, '
+                       f'"cut_w3": {s["cut_w3"]}, "cut_lb": {s["cut_lb"]}, "survivors": {s["survivors"]}, '
+                       f'"distinct": {s["distinct"]}, "proved_unsat": {"true" if s["distinct"] == 0 else "false"}, '
+                       f'"seconds": {sec}}}')
+        if self.rc == CIRCUIT:
+            if self.depth0:
+                out.append('{"found": 0, "circuit": []}')
+            else:
+                names = ", ".join(f'"{c}"' for c in self.circuit)
+                out.append(f'{{"t": {len(self.circuit)}, "found": {self.n_found or 1}, "circuit": [{names}], '
+                           f'"seconds": 0.00}}')
+        return out
+
+    @property
+    def exit_code(self):
+        return self.rc

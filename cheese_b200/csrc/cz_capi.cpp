@@ -1,0 +1,164 @@
+// C ABI over the C++ engine: no exception crosses it, every call returns 0 or a reference exit code.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/cheese_b200.h"
+#include "cz_engine.h"
+#include "cz_spec.h"
+
+struct cz_spec { cz::HostSpec hs; };
+struct cz_engine { cz::Engine *e; };
+
+namespace {
+void put_err(char *err, size_t n, const std::string &m) {
+  if (err && n) { std::snprintf(err, n, "%s", m.c_str()); }
+}
+}  // namespace
+
+extern "C" {
+
+int cz_spec_parse(const char *text, size_t len, cz_spec **out, char *err, size_t errlen) {
+  if (!out) return CZ_ERR_USAGE;
+  *out = nullptr;
+  try {
+    cz_spec *s = new cz_spec;
+    std::string e;
+    const int rc = cz::parse_spec(text ? text : "", text ? len : 0, s->hs, e);
+    if (rc) { put_err(err, errlen, e); delete s; return rc; }
+    *out = s;
+    return 0;
+  } catch (const std::exception &ex) {
+    put_err(err, errlen, ex.what());
+    return CZ_ERR_SPEC;
+  }
+}
+
+void cz_spec_free(cz_spec *spec) { delete spec; }
+
+int cz_spec_info(const cz_spec *spec, int *n, int *gates, int *depth) {
+  if (!spec) return CZ_ERR_USAGE;
+  if (n) *n = spec->hs.n;
+  if (gates) *gates = spec->hs.G;
+  if (depth) *depth = spec->hs.depth;
+  return 0;
+}
+
+const char *cz_spec_gate_name(const cz_spec *spec, int g) {
+  if (!spec || g < 0 || g >= spec->hs.G) return nullptr;
+  return spec->hs.names[g].c_str();
+}
+
+int cz_spec_is_states(const cz_spec *spec) { return spec && spec->hs.states; }
+
+int cz_engine_create(int device, cz_engine **out, char *err, size_t errlen) {
+  if (!out) return CZ_ERR_USAGE;
+  *out = nullptr;
+  int ndev = 0;
+  const cudaError_t ce = cudaGetDeviceCount(&ndev);
+  if (ce != cudaSuccess || device < 0 || device >= ndev) {
+    put_err(err, errlen, std::string("no CUDA device ") + std::to_string(device) + ": " +
+                             (ce != cudaSuccess ? cudaGetErrorString(ce) : "out of range"));
+    return CZ_ERR_CUDA;
+  }
+  try {
+    cz_engine *e = new cz_engine{new cz::Engine(device)};
+    *out = e;
+    return 0;
+  } catch (const std::exception &ex) {
+    put_err(err, errlen, ex.what());
+    return CZ_ERR_CUDA;
+  }
+}
+
+void cz_engine_destroy(cz_engine *engine) {
+  if (!engine) return;
+  delete engine->e;
+  delete engine;
+}
+
+void cz_options_default(cz_options *opt) {
+  if (!opt) return;
+  opt->depth = -1; opt->dedupe = 1; opt->sym = 1; opt->store64 = 0; opt->profile = 0;
+}
+
+int cz_search(cz_engine *engine, const cz_spec *spec, const cz_options *opt, cz_level_fn on_level, void *user,
+              cz_result *out) {
+  if (!engine || !spec || !out) return CZ_ERR_USAGE;
+  std::memset(out, 0, sizeof *out);
+  cz_options o;
+  cz_options_default(&o);
+  if (opt) o = *opt;
+  const cz::HostSpec &hs = spec->hs;
+  if (hs.states) {
+    put_err(out->error, sizeof out->error, "state targets: GPU path not ready yet, use build/cheese-cpu");
+    out->rc = CZ_ERR_USAGE;
+    return CZ_ERR_USAGE;
+  }
+  const int depth = o.depth >= 0 ? o.depth : hs.depth;
+  if (depth > CZ_MAX_DEPTH) {
+    put_err(out->error, sizeof out->error, "depth > " + std::to_string(CZ_MAX_DEPTH));
+    out->rc = CZ_ERR_USAGE;
+    return CZ_ERR_USAGE;
+  }
+  cz::Options eo;
+  eo.depth = depth; eo.dedupe = o.dedupe != 0; eo.sym = o.sym != 0; eo.store64 = o.store64; eo.profile = o.profile != 0;
+  cz::SearchResult r;
+  int rc;
+  try {
+    rc = engine->e->search(hs, eo, [&](const cz::LevelStats &L) {
+      if (!on_level) return;
+      cz_level_stats s;
+      s.t = L.t; s.parents = L.parents; s.prefixes = L.prefixes; s.cut_w3 = L.cut_w3; s.cut_lb = L.cut_lb;
+      s.survivors = L.survivors; s.distinct = L.distinct; s.proved_unsat = L.proved_unsat; s.seconds = L.seconds;
+      on_level(user, &s);
+    }, r);
+  } catch (const std::bad_alloc &) {
+    r.error = "host out of memory";
+    rc = CZ_ERR_CUDA;
+  } catch (const std::exception &ex) {
+    r.error = ex.what();
+    rc = CZ_ERR_CUDA;
+  }
+  out->rc = rc;
+  out->depth0 = r.depth0;
+  out->found_len = (int)r.circuit.size();
+  for (size_t i = 0; i < r.circuit.size() && i < CZ_MAX_DEPTH; i++) out->found[i] = r.circuit[i];
+  out->n_found = r.n_found;
+  out->nsym = r.nsym;
+  out->store64 = r.store64;
+  out->levels = r.levels;
+  out->prefixes = r.prefixes;
+  out->kernel_launches = r.launches;
+  out->t_evals = r.t_evals;
+  out->children = r.children;
+  out->expand_ms = r.expand_ms;
+  out->dedupe_ms = r.dedupe_ms;
+  out->total_ms = r.total_ms;
+  put_err(out->error, sizeof out->error, r.error);
+  return rc;
+}
+
+int cz_search_text(cz_engine *engine, const char *spec_text, size_t len, const cz_options *opt, cz_level_fn on_level,
+                   void *user, cz_result *out) {
+  if (!out) return CZ_ERR_USAGE;
+  cz_spec *s = nullptr;
+  char err[256] = {0};
+  const int prc = cz_spec_parse(spec_text, len, &s, err, sizeof err);
+  if (prc) {
+    std::memset(out, 0, sizeof *out);
+    out->rc = prc;
+    std::snprintf(out->error, sizeof out->error, "%s", err);
+    return prc;
+  }
+  const int rc = cz_search(engine, s, opt, on_level, user, out);
+  cz_spec_free(s);
+  return rc;
+}
+
+const char *cz_version(void) { return "cheese_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,61 @@
+// The B200 search engine (host C++): owns a device, a stream and grow-only device buffers; runs the
+// level-synchronous gate-count search of the reference (src/cheese.cu:1249-1377, 1762-1849) on sm_100a kernels.
+#pragma once
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "cz_spec.h"
+
+namespace cz {
+
+struct Options {
+  int depth = -1;            // -1: the spec's budget
+  bool dedupe = true;        // --no-dedupe
+  bool sym = true;           // --no-sym
+  int store64 = 0;           // 0: int32 residual limbs, promoted to int64 when a value leaves int32; 1: int64 from the start
+  bool profile = false;      // per-phase device times (CUDA events on the engine's stream)
+  bool nogoal = false;       // never report the goal (distance-table build)
+};
+
+struct LevelStats {
+  int t = 0;
+  long long parents = 0, prefixes = 0, cut_w3 = 0, cut_lb = 0, survivors = 0, distinct = 0;
+  bool proved_unsat = false;
+  double seconds = 0;
+};
+
+struct SearchResult {
+  int rc = 1;                          // 0 circuit, 1 proof (or stopped), 4 overflow, 5 CUDA error
+  bool depth0 = false;                 // the target equals the goal
+  std::vector<int> circuit;            // candidate indices of the found circuit
+  long long n_found = 0;
+  int nsym = 0;
+  bool store64 = false;                // the run used int64 limbs
+  int levels = 0;
+  long long prefixes = 0;              // sum of the per-level "prefixes" fields
+  long long launches = 0;              // kernels launched by the engine
+  long long t_evals = 0, children = 0; // T-bound evaluations, children evaluated past the window rules
+  double expand_ms = 0, dedupe_ms = 0, total_ms = 0;   // device times (profile) / host wall time
+  std::string error;
+};
+
+class Engine {
+ public:
+  explicit Engine(int device);
+  ~Engine();
+  Engine(const Engine &) = delete;
+  Engine &operator=(const Engine &) = delete;
+  // the plain search (no --mitm / --table); on_level is called after each completed level, in order
+  int search(const HostSpec &hs, const Options &opt, const std::function<void(const LevelStats &)> &on_level,
+             SearchResult &res);
+  void *stream() const;
+  int device() const { return dev_; }
+
+ private:
+  struct Impl;
+  Impl *impl_;
+  int dev_;
+};
+
+}  // namespace cz

@@ -1,0 +1,985 @@
+// sm_100a kernels and the level loop of the gate-count search.
+//
+// Reference semantics (src/cheese.cu): per level, every parent of the frontier is expanded by every candidate
+// gate in parent-major, gate-minor order (levels 1249-1377); a child is cut by the W2/W3 window rules (613-632),
+// its residual S g^-1 is normalised (145-174), compared with the goal (184-203), pruned by the lower bounds
+// (combine of H / structure / support / CX / T, 257-607) and, when alive, keyed by its symmetry class
+// (224-241). Survivors are deduplicated by exact class equality keeping the smallest index (1335-1343).
+//
+// B200 design:
+// * one warp per parent (dynamic work counter), parent residual staged in shared memory, all G children walked by
+//   the warp; each lane owns entries lane, lane + 32 of the residual;
+// * frontier residuals are kept in HBM (1 KB per 3-qubit node with int32 limbs) instead of being replayed from
+//   the prefix, so there is no per-level replay pass;
+// * each frontier node carries its T bound and CX bound. The T bound (the sde of the Pauli transfer matrix) is
+//   unchanged by right multiplication with a Clifford gate (the PTM of a Clifford is a signed permutation), and
+//   the F_p operator-Schmidt ranks behind the CX bound are unchanged by one-qubit gates (an invertible local map
+//   of the reshaped matrix). So only non-Clifford children (t, tdg) run the 64-point Walsh-Hadamard T bound and
+//   only multi-qubit children (cx) run the rank eliminations; the values are identical, not estimates;
+// * the T bound accumulates the 2-adic valuations of all transform outputs with two OR words: v = 2 m + d with
+//   m = ctz(OR of all coefficients) and d read from bit m of OR((a^c)|(b^d)), the same minimum valuation the
+//   reference reads off entry by entry (cheese.cu:419-449);
+// * dedupe = stable LSD radix sort of survivor keys, run detection, exact class comparison inside runs (warp per
+//   run), then a radix sort of the kept indices restores lexicographic order and a gather builds the next level.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+
+#include "cz_engine.h"
+#include "cz_sort.cuh"
+
+namespace cz {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int EXP_WARPS = 8;       // warps per expand block
+constexpr int INHERIT_KMAX = 60;   // the T bound is computed exactly (mod 2^32 / 2^64) only while 2(n + k) <= 128
+
+// ---------------- device-side spec ----------------
+struct DevSpec {
+  int n, G, depth, standard, lite, tdiv, ncuts, have_table, nsym, nogoal, gk, ncx;
+  int cutmask[CUTMAX], cutsize[CUTMAX], rad[CUTMAX];
+  uint64_t w1, w2, w3;                 // w, w^2, w^3 mod p with w = 3^((p-1)/8)
+  uint8_t symperm[SYMMAX][8];
+  uint8_t symconj[SYMMAX];
+  uint8_t gflags[GMAX];
+  int8_t gnq[GMAX], gik[GMAX];
+  int8_t gq[GMAX][3];
+  const uint8_t *bad2;
+  const uint32_t *bad3;
+  const int *cxtable;
+  const int4 *ginv;                    // GMAX x 64 local inverse matrices (a, b, c, d as int32)
+  const longlong2 *goal;               // N*N entries as (a, b), (c, d) pairs
+};
+
+struct NodeMeta { int16_t k; uint8_t T, c2, g1, g2, pad0, pad1; };   // g = 0xff: no gate
+
+struct DevStats {
+  unsigned long long w2, w3, dead, alive, found, first_found, n_surv, t_evals, children, work;
+  unsigned int ovf, surv_overflow;
+  unsigned long long n_work, n_kept;
+};
+
+template <typename ST> struct ExpandArgs {
+  long long m;
+  int t, rem, keep;
+  const Z4<ST> *R;
+  const NodeMeta *meta;
+  DevStats *st;
+  unsigned long long cap;
+  uint64_t *sh1, *sh2, *sidx;
+  Z4<ST> *sR;
+  NodeMeta *smeta;
+};
+
+// ---------------- arithmetic helpers ----------------
+template <typename ST> __device__ __forceinline__ bool zz(const Z4<ST> &x) { return !(x.a | x.b | x.c | x.d); }
+template <typename ST> __device__ __forceinline__ bool zq(const Z4<ST> &x, const Z4<ST> &y) {
+  return x.a == y.a && x.b == y.b && x.c == y.c && x.d == y.d;
+}
+template <typename ST> __device__ __forceinline__ Z4<ST> zcj(const Z4<ST> &x) { return {x.a, (ST)-x.d, (ST)-x.c, (ST)-x.b}; }
+template <typename U, typename ST> __device__ __forceinline__ Z4<U> toU(const Z4<ST> &x) {
+  return {(U)(int64_t)x.a, (U)(int64_t)x.b, (U)(int64_t)x.c, (U)(int64_t)x.d};
+}
+template <typename U> __device__ __forceinline__ Z4<U> umul(const Z4<U> &x, const Z4<U> &y) {
+  return {(U)(x.a * y.a - x.b * y.d - x.c * y.c - x.d * y.b), (U)(x.a * y.b + x.b * y.a - x.c * y.d - x.d * y.c),
+          (U)(x.a * y.c + x.b * y.b + x.c * y.a - x.d * y.d), (U)(x.a * y.d + x.b * y.c + x.c * y.b + x.d * y.a)};
+}
+template <typename U> __device__ __forceinline__ Z4<U> uadd(const Z4<U> &x, const Z4<U> &y) {
+  return {(U)(x.a + y.a), (U)(x.b + y.b), (U)(x.c + y.c), (U)(x.d + y.d)};
+}
+template <typename U> __device__ __forceinline__ Z4<U> usub(const Z4<U> &x, const Z4<U> &y) {
+  return {(U)(x.a - y.a), (U)(x.b - y.b), (U)(x.c - y.c), (U)(x.d - y.d)};
+}
+template <typename U> __device__ __forceinline__ Z4<U> ushfl(const Z4<U> &x, int m) {
+  return {__shfl_xor_sync(FULL, x.a, m), __shfl_xor_sync(FULL, x.b, m), __shfl_xor_sync(FULL, x.c, m),
+          __shfl_xor_sync(FULL, x.d, m)};
+}
+__device__ __forceinline__ uint64_t fmix64(uint64_t h) {
+  h ^= h >> 33; h *= 0xff51afd7ed558ccdULL; h ^= h >> 33; h *= 0xc4ceb9fe1a85ec53ULL; h ^= h >> 33;
+  return h;
+}
+__device__ __forceinline__ uint64_t tomodp(int64_t v) {
+  int64_t m = v % (int64_t)PRIME;
+  return (uint64_t)(m < 0 ? m + (int64_t)PRIME : m);
+}
+template <typename ST> __device__ __forceinline__ uint32_t zmodp(const Z4<ST> &x, const DevSpec &sp) {
+  const uint64_t r = tomodp(x.a) + tomodp(x.b) * sp.w1 % PRIME + tomodp(x.c) * sp.w2 % PRIME + tomodp(x.d) * sp.w3 % PRIME;
+  return (uint32_t)(r % PRIME);
+}
+
+// ---------------- per-warp bound evaluations (child residual S in shared memory) ----------------
+
+// T bound: max(0, max over nonzero PTM entries of their sde), Walsh-Hadamard form of cheese.cu:397-449
+template <int NQ, typename U, typename ST> __device__ int warp_ptm(const Z4<ST> *S, int k, int lane) {
+  constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
+  Z4<U> y[EPL];
+#pragma unroll
+  for (int j = 0; j < EPL; j++) {
+    const int e = lane + 32 * j;
+    y[j] = e < E ? toU<U>(zcj(S[e])) : Z4<U>{0, 0, 0, 0};
+  }
+  U o1 = 0, o2 = 0;
+#pragma unroll 1
+  for (int f = 0; f < E; f++) {         // f = (fa, fb): Q[x][c] = S[x ^ fa][c ^ fb] conj(S[x][c])
+    Z4<U> q[EPL];
+#pragma unroll
+    for (int j = 0; j < EPL; j++) {
+      const int e = lane + 32 * j;
+      q[j] = e < E ? umul(toU<U>(S[e ^ f]), y[j]) : Z4<U>{0, 0, 0, 0};
+    }
+#pragma unroll
+    for (int h = 1; h < E; h <<= 1) {
+      if (h < 32) {
+#pragma unroll
+        for (int j = 0; j < EPL; j++) {
+          const Z4<U> o = ushfl(q[j], h);
+          q[j] = (lane & h) ? usub(o, q[j]) : uadd(q[j], o);
+        }
+      } else {
+        const int hj = h >> 5;
+#pragma unroll
+        for (int j = 0; j < EPL; j++)
+          if (!(j & hj)) { const Z4<U> u = q[j], v = q[j | hj]; q[j] = uadd(u, v); q[j | hj] = usub(u, v); }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < EPL; j++) { o1 |= q[j].a | q[j].b | q[j].c | q[j].d; o2 |= (q[j].a ^ q[j].c) | (q[j].b ^ q[j].d); }
+  }
+#pragma unroll
+  for (int m = 16; m; m >>= 1) { o1 |= __shfl_xor_sync(FULL, o1, m); o2 |= __shfl_xor_sync(FULL, o2, m); }
+  if (!o1) return 0;
+  const int mv = sizeof(U) == 8 ? __ffsll((long long)o1) - 1 : __ffs((int)o1) - 1;
+  const int v = 2 * mv + (((o2 >> mv) & 1) ? 0 : 1);
+  const int top = 2 * (NQ + k);
+  return top - v > 0 ? top - v : 0;
+}
+template <int NQ, typename ST> __device__ __forceinline__ int ptm_bound(const Z4<ST> *S, int k, int lane) {
+  return 2 * (NQ + k) <= 64 ? warp_ptm<NQ, uint32_t, ST>(S, k, lane) : warp_ptm<NQ, uint64_t, ST>(S, k, lane);
+}
+
+// rank over F_p of the operator-Schmidt matrix across cut A (cheese.cu:271-303): lane j owns column j, fraction-free
+// elimination row by row (the rank does not depend on the order of elimination)
+template <int NQ, typename ST> __device__ int warp_cut_rank(const Z4<ST> *S, int A, int sa, const DevSpec &sp, int lane) {
+  constexpr int N = 1 << NQ, E = N * N;
+  const int na = sa, nb = NQ - sa, R = 1 << (2 * sa), Cc = E / R;
+  const bool act = lane < Cc;
+  const int ob = lane >> nb, ib = lane & ((1 << nb) - 1);
+  uint32_t v[4];
+#pragma unroll
+  for (int rr = 0; rr < 4; rr++) {
+    v[rr] = 0;
+    if (rr < R && act) {
+      const int oa = rr >> na, ia = rr & ((1 << na) - 1);
+      int o = 0, i = 0, xa = 0, xb = 0;
+#pragma unroll
+      for (int q = 0; q < NQ; q++) {
+        if ((A >> q) & 1) { o |= ((oa >> xa) & 1) << q; i |= ((ia >> xa) & 1) << q; xa++; }
+        else { o |= ((ob >> xb) & 1) << q; i |= ((ib >> xb) & 1) << q; xb++; }
+      }
+      v[rr] = zmodp(S[o * N + i], sp);
+    }
+  }
+  int rank = 0;
+#pragma unroll
+  for (int rr = 0; rr < 4; rr++) {
+    if (rr >= R) break;
+    const unsigned bal = __ballot_sync(FULL, act && v[rr] != 0);
+    if (!bal) continue;
+    const int piv = __ffs((int)bal) - 1;
+    const uint64_t a = __shfl_sync(FULL, v[rr], piv);
+#pragma unroll
+    for (int r2 = rr + 1; r2 < 4; r2++) {
+      if (r2 >= R) break;
+      const uint64_t b = __shfl_sync(FULL, v[r2], piv);
+      v[r2] = (uint32_t)((a * v[r2] + (PRIME - b) * (uint64_t)v[rr]) % PRIME);
+    }
+    rank++;
+  }
+  return rank;
+}
+
+template <int NQ, typename ST> __device__ int warp_cx_bound(const Z4<ST> *S, const DevSpec &sp, int lane) {
+  int idx = 0, mult = 1, mx = 0;
+  for (int i = 0; i < sp.ncuts; i++) {
+    const int rk = warp_cut_rank<NQ, ST>(S, sp.cutmask[i], sp.cutsize[i], sp, lane);
+    int need = 0;
+    while ((1 << need) < rk) need++;
+    if (need > sp.rad[i] - 1) need = sp.rad[i] - 1;
+    idx += need * mult;
+    mult *= sp.rad[i];
+    if (need > mx) mx = need;
+  }
+  return sp.have_table && idx < sp.ncx ? __ldg(&sp.cxtable[idx]) : mx;
+}
+
+// 2 when S is monomial with a non-affine permutation, else 0 (cheese.cu:322-338); lane c scans column c
+template <int NQ, typename ST> __device__ int warp_h_struct(const Z4<ST> *S, int lane) {
+  constexpr int N = 1 << NQ;
+  int nz = 0, row = 0;
+  if (lane < N)
+    for (int r = 0; r < N; r++) if (!zz(S[r * N + lane])) { nz++; row = r; }
+  if (__any_sync(FULL, lane < N && nz != 1)) return 0;
+  const int c0 = __shfl_sync(FULL, row, 0);
+  int x = c0;
+#pragma unroll
+  for (int i = 0; i < NQ; i++) {
+    const int pb = __shfl_sync(FULL, row, 1 << i);
+    if ((lane >> i) & 1) x ^= pb ^ c0;
+  }
+  return __any_sync(FULL, lane < N && row != x) ? 2 : 0;
+}
+
+// number of qubits S acts on non-trivially (cheese.cu:305-319)
+template <int NQ, typename ST> __device__ int warp_support(const Z4<ST> *S, int lane) {
+  constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
+  int cnt = 0;
+#pragma unroll
+  for (int q = 0; q < NQ; q++) {
+    const int bit = 1 << q;
+    bool nt = false;
+#pragma unroll
+    for (int j = 0; j < EPL; j++) {
+      const int e = lane + 32 * j;
+      if (e >= E) continue;
+      const int r = e >> NQ, c = e & (N - 1);
+      if ((r ^ c) & bit) { if (!zz(S[e])) nt = true; }
+      else if (!((r | c) & bit) && !zq(S[e], S[(r | bit) * N + (c | bit)])) nt = true;
+    }
+    cnt += __any_sync(FULL, nt);
+  }
+  return cnt;
+}
+
+__device__ __forceinline__ int combine(int h, int t, int c2, int supp) {   // cheese.cu:599-607
+  int best = 1 << 30;
+  const int hi = c2 > supp ? c2 : supp;
+  for (int c = c2; c <= hi; c++) {
+    const int one = (h + t > supp - 2 * c) ? h + t : supp - 2 * c;
+    if (c + one < best) best = c + one;
+  }
+  return best;
+}
+
+// child residual C = P g^-1, normalised; returns its exponent, sets ovf when a limb leaves the storage type
+template <int NQ, typename ST>
+__device__ int warp_child(const Z4<ST> *P, Z4<ST> *C, int g, int kp, const DevSpec &sp, int lane, bool &ovf) {
+  constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
+  const int nq = sp.gnq[g], L = 1 << nq;
+  const int q0 = sp.gq[g][0], q1 = nq > 1 ? sp.gq[g][1] : 0, q2 = nq > 2 ? sp.gq[g][2] : 0;
+  const int mask = (1 << q0) | (nq > 1 ? 1 << q1 : 0) | (nq > 2 ? 1 << q2 : 0);
+  const int4 *gi = sp.ginv + g * 64;
+  Zw acc[EPL];
+#pragma unroll
+  for (int j = 0; j < EPL; j++) {
+    const int e = lane + 32 * j;
+    acc[j] = Zw{0, 0, 0, 0};
+    if (e >= E) continue;
+    const int r = e >> NQ, col = e & (N - 1), base = col & ~mask;
+    int lc = (col >> q0) & 1;
+    if (nq > 1) lc |= ((col >> q1) & 1) << 1;
+    if (nq > 2) lc |= ((col >> q2) & 1) << 2;
+    for (int m = 0; m < L; m++) {
+      const int4 gm = __ldg(&gi[m * L + lc]);
+      if (!(gm.x | gm.y | gm.z | gm.w)) continue;
+      int x = base | ((m & 1) << q0);
+      if (nq > 1) x |= ((m >> 1) & 1) << q1;
+      if (nq > 2) x |= ((m >> 2) & 1) << q2;
+      const Z4<ST> s = P[r * N + x];
+      acc[j] = zadd(acc[j], zmul(Zw{(int64_t)s.a, (int64_t)s.b, (int64_t)s.c, (int64_t)s.d},
+                                 Zw{(int64_t)gm.x, (int64_t)gm.y, (int64_t)gm.z, (int64_t)gm.w}));
+    }
+  }
+  int k = kp + sp.gik[g];
+  while (k > 0) {                              // normalise: lower k while every entry is divisible by sqrt2
+    bool ok = true;
+#pragma unroll
+    for (int j = 0; j < EPL; j++) if (lane + 32 * j < E && !zdiv2ok(acc[j])) ok = false;
+    if (!__all_sync(FULL, ok)) break;
+#pragma unroll
+    for (int j = 0; j < EPL; j++) acc[j] = zdown(acc[j]);
+    k--;
+  }
+  bool of = false;
+#pragma unroll
+  for (int j = 0; j < EPL; j++) {
+    const int e = lane + 32 * j;
+    if (e >= E) continue;
+    if (sizeof(ST) == 4 && !(fits32(acc[j].a) && fits32(acc[j].b) && fits32(acc[j].c) && fits32(acc[j].d))) of = true;
+    C[e] = Z4<ST>{(ST)acc[j].a, (ST)acc[j].b, (ST)acc[j].c, (ST)acc[j].d};
+  }
+  ovf = __any_sync(FULL, of);
+  __syncwarp();
+  return k;
+}
+
+template <int NQ, typename ST> __device__ bool warp_goal(const Z4<ST> *S, int k, const DevSpec &sp, int lane) {
+  constexpr int E = (1 << NQ) * (1 << NQ), EPL = E >= 32 ? E / 32 : 1;
+  if (k != sp.gk) return false;
+  bool ok = true;
+#pragma unroll
+  for (int j = 0; j < EPL; j++) {
+    const int e = lane + 32 * j;
+    if (e >= E) continue;
+    const longlong2 g0 = __ldg(&sp.goal[2 * e]), g1 = __ldg(&sp.goal[2 * e + 1]);
+    const Z4<ST> x = S[e];
+    if ((int64_t)x.a != g0.x || (int64_t)x.b != g0.y || (int64_t)x.c != g1.x || (int64_t)x.d != g1.y) ok = false;
+  }
+  return __all_sync(FULL, ok);
+}
+
+// class key: the smallest (h1, h2) over the symmetry orbit of S; per orbit element a position-weighted sum of
+// per-entry hashes (the key only has to be class-invariant: classes are always compared exactly)
+template <int NQ, typename ST>
+__device__ void warp_class_key(const Z4<ST> *S, int k, const DevSpec &sp, const uint8_t (*perm)[8],
+                               const uint64_t *W1, const uint64_t *W2, int lane, uint64_t &k1, uint64_t &k2) {
+  constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
+  uint64_t f1[EPL], f2[EPL], c1[EPL], c2[EPL];
+#pragma unroll
+  for (int j = 0; j < EPL; j++) {
+    const int e = lane + 32 * j;
+    f1[j] = f2[j] = c1[j] = c2[j] = 0;
+    if (e >= E) continue;
+    const Z4<ST> x = S[e];
+    uint64_t h = fmix64((uint64_t)(int64_t)x.a * 0x9e3779b97f4a7c15ULL + (uint64_t)(int64_t)x.b);
+    h = fmix64(h ^ ((uint64_t)(int64_t)x.c * 0xc2b2ae3d27d4eb4fULL + (uint64_t)(int64_t)x.d));
+    f1[j] = h; f2[j] = fmix64(h + 0x632be59bd9b4e019ULL);
+    const Z4<ST> y = zcj(x);
+    h = fmix64((uint64_t)(int64_t)y.a * 0x9e3779b97f4a7c15ULL + (uint64_t)(int64_t)y.b);
+    h = fmix64(h ^ ((uint64_t)(int64_t)y.c * 0xc2b2ae3d27d4eb4fULL + (uint64_t)(int64_t)y.d));
+    c1[j] = h; c2[j] = fmix64(h + 0x632be59bd9b4e019ULL);
+  }
+  uint64_t b1 = ~0ULL, b2 = ~0ULL;
+  for (int s = 0; s < sp.nsym; s++) {
+    const bool cj = sp.symconj[s];
+    uint64_t a = 0, b = 0;
+#pragma unroll
+    for (int j = 0; j < EPL; j++) {
+      const int e = lane + 32 * j;
+      if (e >= E) continue;
+      const int pos = perm[s][e >> NQ] * N + perm[s][e & (N - 1)];
+      a += (cj ? c1[j] : f1[j]) * W1[pos];
+      b += (cj ? c2[j] : f2[j]) * W2[pos];
+    }
+#pragma unroll
+    for (int m = 16; m; m >>= 1) { a += __shfl_xor_sync(FULL, a, m); b += __shfl_xor_sync(FULL, b, m); }
+    const uint64_t x1 = fmix64(a + (uint64_t)k * 0xa0761d6478bd642fULL);
+    const uint64_t x2 = fmix64(b ^ ((uint64_t)k * 0xe7037ed1a0b428dbULL + 0x8ebc6af09c88c6e3ULL));
+    if (x1 < b1 || (x1 == b1 && x2 < b2)) { b1 = x1; b2 = x2; }
+  }
+  k1 = b1; k2 = b2;
+}
+
+template <int NQ, typename ST> struct ExpandSmem {
+  static constexpr int E = (1 << NQ) * (1 << NQ);
+  Z4<ST> P[EXP_WARPS][E];
+  Z4<ST> C[EXP_WARPS][E];
+  uint64_t W1[E], W2[E];
+  uint8_t perm[SYMMAX][8];
+};
+
+__device__ __forceinline__ void init_weights(uint64_t *W1, uint64_t *W2, int E) {
+  for (int i = threadIdx.x; i < E; i += blockDim.x) {
+    W1[i] = fmix64(0x243f6a8885a308d3ULL + (uint64_t)i * 0x13198a2e03707345ULL) | 1;
+    W2[i] = fmix64(0xa4093822299f31d0ULL + (uint64_t)i * 0x082efa98ec4e6c89ULL) | 1;
+  }
+}
+
+// ---------------- the level kernel ----------------
+template <int NQ, typename ST>
+__global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, const ExpandArgs<ST> a) {
+  constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
+  __shared__ ExpandSmem<NQ, ST> sm;
+  init_weights(sm.W1, sm.W2, E);
+  for (int i = threadIdx.x; i < SYMMAX * 8; i += blockDim.x) sm.perm[i / 8][i % 8] = sp.symperm[i / 8][i % 8];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  Z4<ST> *P = sm.P[w], *C = sm.C[w];
+  const int G = sp.G;
+  unsigned long long n_w2 = 0, n_w3 = 0, n_dead = 0, n_alive = 0, n_found = 0, n_teval = 0, n_child = 0;
+  unsigned long long first = ~0ULL;
+  bool ovf_any = false;
+  for (;;) {
+    unsigned long long p = 0;
+    if (lane == 0) p = atomicAdd(&a.st->work, 1ULL);
+    p = __shfl_sync(FULL, p, 0);
+    if ((long long)p >= a.m) break;
+#pragma unroll
+    for (int j = 0; j < EPL; j++) {
+      const int e = lane + 32 * j;
+      if (e < E) P[e] = a.R[p * E + e];
+    }
+    const NodeMeta pm = a.meta[p];
+    __syncwarp();
+    const int g1 = pm.g1 == 0xff ? -1 : pm.g1, g2 = pm.g2 == 0xff ? -1 : pm.g2;
+    for (int g = 0; g < G; g++) {
+      if (g1 >= 0 && __ldg(&sp.bad2[g1 * G + g])) { n_w2++; continue; }
+      if (g2 >= 0) {
+        const uint32_t tri = ((uint32_t)g2 * G + (uint32_t)g1) * G + (uint32_t)g;
+        if ((__ldg(&sp.bad3[tri >> 5]) >> (tri & 31)) & 1) { n_w3++; continue; }
+      }
+      n_child++;
+      bool ovf;
+      const int k = warp_child<NQ, ST>(P, C, g, pm.k, sp, lane, ovf);
+      if (ovf) { ovf_any = true; continue; }
+      if (warp_goal<NQ, ST>(C, k, sp, lane)) {
+        if (sp.nogoal) n_dead++;
+        else { n_found++; const unsigned long long o = p * (unsigned long long)G + g; if (o < first) first = o; }
+        continue;
+      }
+      const int rem = a.rem;
+      const uint8_t fl = sp.gflags[g];
+      const bool inheritT = (fl & GF_CLIFFORD) && k <= INHERIT_KMAX && pm.k <= INHERIT_KMAX;
+      bool alive = true;
+      int T = 0, c2 = 0;
+      if (sp.lite) {
+        if (k > rem) alive = false;
+        else {
+          if (inheritT) T = pm.T; else { T = ptm_bound<NQ, ST>(C, k, lane); n_teval++; }
+          alive = k + (T + sp.tdiv - 1) / sp.tdiv <= rem;
+        }
+      } else if (sp.standard) {
+        const int hs = warp_h_struct<NQ, ST>(C, lane), h = k > hs ? k : hs;
+        const int supp = warp_support<NQ, ST>(C, lane);
+        c2 = (fl & GF_ONEQ) ? pm.c2 : warp_cx_bound<NQ, ST>(C, sp, lane);
+        if (combine(h, 0, c2, supp) > rem) alive = false;
+        else {
+          if (inheritT) T = pm.T; else { T = ptm_bound<NQ, ST>(C, k, lane); n_teval++; }
+          alive = combine(h, T, c2, supp) <= rem;
+        }
+      }
+      if (!alive) { n_dead++; continue; }
+      n_alive++;
+      if (!a.keep) continue;
+      uint64_t k1, k2;
+      warp_class_key<NQ, ST>(C, k, sp, sm.perm, sm.W1, sm.W2, lane, k1, k2);
+      unsigned long long slot = 0;
+      if (lane == 0) slot = atomicAdd(&a.st->n_surv, 1ULL);
+      slot = __shfl_sync(FULL, slot, 0);
+      if (slot < a.cap) {
+#pragma unroll
+        for (int j = 0; j < EPL; j++) {
+          const int e = lane + 32 * j;
+          if (e < E) a.sR[slot * E + e] = C[e];
+        }
+        if (lane == 0) {
+          a.sh1[slot] = k1; a.sh2[slot] = k2; a.sidx[slot] = p * (unsigned long long)G + g;
+          NodeMeta nm;
+          nm.k = (int16_t)k; nm.T = (uint8_t)(T > 255 ? 255 : T); nm.c2 = (uint8_t)c2; nm.g1 = (uint8_t)g; nm.g2 = pm.g1;
+          nm.pad0 = nm.pad1 = 0;
+          a.smeta[slot] = nm;
+        }
+      } else if (lane == 0) {
+        a.st->surv_overflow = 1;
+      }
+      __syncwarp();
+    }
+    __syncwarp();
+  }
+  if (lane == 0) {
+    if (n_w2) atomicAdd(&a.st->w2, n_w2);
+    if (n_w3) atomicAdd(&a.st->w3, n_w3);
+    if (n_dead) atomicAdd(&a.st->dead, n_dead);
+    if (n_alive) atomicAdd(&a.st->alive, n_alive);
+    if (n_found) { atomicAdd(&a.st->found, n_found); atomicMin(&a.st->first_found, first); }
+    if (n_teval) atomicAdd(&a.st->t_evals, n_teval);
+    if (n_child) atomicAdd(&a.st->children, n_child);
+    if (ovf_any) a.st->ovf = 1;
+  }
+}
+
+// the root node's bounds (the target itself): T and CX bound for inheritance by its children
+template <int NQ, typename ST> __global__ void k_root(const DevSpec sp, const Z4<ST> *R, NodeMeta *meta, int tk) {
+  constexpr int E = (1 << NQ) * (1 << NQ);
+  __shared__ Z4<ST> S[E];
+  const int lane = threadIdx.x;
+  for (int e = lane; e < E; e += 32) S[e] = R[e];
+  __syncwarp();
+  int T = 0, c2 = 0;
+  if (sp.standard || sp.lite) T = ptm_bound<NQ, ST>(S, tk, lane);
+  if (sp.standard) c2 = warp_cx_bound<NQ, ST>(S, sp, lane);
+  if (lane == 0) {
+    NodeMeta m;
+    m.k = (int16_t)tk; m.T = (uint8_t)(T > 255 ? 255 : T); m.c2 = (uint8_t)c2; m.g1 = m.g2 = 0xff; m.pad0 = m.pad1 = 0;
+    *meta = m;
+  }
+}
+
+// ---------------- dedupe ----------------
+__global__ void k_sort_init(const uint64_t *h1, size_t n, uint64_t *keys, uint32_t *vals) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    keys[i] = h1[i];
+    vals[i] = (uint32_t)i;
+  }
+}
+
+// runs of equal top-32 key bits: singletons are kept at once, longer runs go to the exact resolver
+__global__ void k_runs(const uint64_t *keys, const uint32_t *slots, size_t n, const uint64_t *sidx, uint64_t *kidx,
+                       uint32_t *kslot, uint2 *work, DevStats *st) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t hk = (uint32_t)(keys[i] >> 32);
+    if (i > 0 && (uint32_t)(keys[i - 1] >> 32) == hk) continue;
+    size_t j = i + 1;
+    while (j < n && (uint32_t)(keys[j] >> 32) == hk) j++;
+    if (j == i + 1) {
+      const unsigned long long pos = atomicAdd(&st->n_kept, 1ULL);
+      kidx[pos] = sidx[slots[i]];
+      kslot[pos] = slots[i];
+    } else {
+      const unsigned long long w = atomicAdd(&st->n_work, 1ULL);
+      work[w] = make_uint2((unsigned)i, (unsigned)(j - i));
+    }
+  }
+}
+
+template <int NQ, typename ST>
+__device__ bool warp_same_class(const Z4<ST> *A, const Z4<ST> *B, const DevSpec &sp, const uint8_t (*perm)[8], int lane) {
+  constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
+  Z4<ST> av[EPL];
+#pragma unroll
+  for (int j = 0; j < EPL; j++) { const int e = lane + 32 * j; if (e < E) av[j] = A[e]; }
+  for (int s = 0; s < sp.nsym; s++) {
+    bool eq = true;
+#pragma unroll
+    for (int j = 0; j < EPL; j++) {
+      const int e = lane + 32 * j;
+      if (e >= E) continue;
+      const Z4<ST> v = sp.symconj[s] ? zcj(av[j]) : av[j];
+      if (!zq(v, B[perm[s][e >> NQ] * N + perm[s][e & (N - 1)]])) eq = false;
+    }
+    if (__all_sync(FULL, eq)) return true;
+  }
+  return false;
+}
+
+// one warp per run: order members by (h1, h2, index), then keep the first member of every exact class
+template <int NQ, typename ST>
+__global__ void k_resolve(const DevSpec sp, const uint2 *work, const uint32_t *slots, const uint64_t *sh1,
+                          const uint64_t *sh2, const uint64_t *sidx, const Z4<ST> *sR, const NodeMeta *smeta,
+                          uint32_t *tmp, uint64_t *kidx, uint32_t *kslot, DevStats *st) {
+  constexpr int E = (1 << NQ) * (1 << NQ);
+  __shared__ uint8_t perm[SYMMAX][8];
+  for (int i = threadIdx.x; i < SYMMAX * 8; i += blockDim.x) perm[i / 8][i % 8] = sp.symperm[i / 8][i % 8];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const unsigned long long nwork = st->n_work;
+  const unsigned long long nw = (unsigned long long)gridDim.x * (blockDim.x / 32);
+  for (unsigned long long wi = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); wi < nwork; wi += nw) {
+    const uint2 wk = work[wi];
+    const unsigned start = wk.x, len = wk.y;
+    for (unsigned a0 = 0; a0 < len; a0 += 32) {          // rank of member a among the run
+      const unsigned ai = a0 + lane;
+      uint64_t ah1 = 0, ah2 = 0, aix = 0;
+      uint32_t as = 0;
+      if (ai < len) { as = slots[start + ai]; ah1 = sh1[as]; ah2 = sh2[as]; aix = sidx[as]; }
+      unsigned rank = 0;
+      for (unsigned b = 0; b < len; b++) {
+        const uint32_t bs = slots[start + b];
+        const uint64_t bh1 = sh1[bs], bh2 = sh2[bs], bix = sidx[bs];
+        rank += (bh1 < ah1) || (bh1 == ah1 && (bh2 < ah2 || (bh2 == ah2 && bix < aix)));
+      }
+      if (ai < len) tmp[start + rank] = as;
+    }
+    __syncwarp();
+    unsigned gstart = 0;
+    for (unsigned i = 0; i < len; i++) {
+      const uint32_t si = tmp[start + i] & 0x7fffffffu;
+      if (i > 0) {
+        const uint32_t sp0 = tmp[start + i - 1] & 0x7fffffffu;
+        if (sh1[sp0] != sh1[si] || sh2[sp0] != sh2[si]) gstart = i;
+      }
+      bool dup = false;
+      for (unsigned i2 = gstart; i2 < i && !dup; i2++) {
+        const uint32_t t2 = tmp[start + i2];
+        if (!(t2 & 0x80000000u)) continue;
+        const uint32_t s2 = t2 & 0x7fffffffu;
+        if (smeta[s2].k != smeta[si].k) continue;
+        dup = warp_same_class<NQ, ST>(sR + (size_t)si * E, sR + (size_t)s2 * E, sp, perm, lane);
+      }
+      if (!dup && lane == 0) {
+        tmp[start + i] = si | 0x80000000u;
+        const unsigned long long pos = atomicAdd(&st->n_kept, 1ULL);
+        kidx[pos] = sidx[si];
+        kslot[pos] = si;
+      }
+      __syncwarp();
+    }
+  }
+}
+
+__global__ void k_keep_all(const uint64_t *sidx, size_t n, uint64_t *kidx, uint32_t *kslot) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    kidx[i] = sidx[i];
+    kslot[i] = (uint32_t)i;
+  }
+}
+
+// kept survivors (in index order) -> the next frontier: residual, bounds, tree links
+template <typename ST>
+__global__ void k_gather(const uint64_t *kidx, const uint32_t *kslot, size_t nk, int G, int E, const Z4<ST> *sR,
+                         const NodeMeta *smeta, Z4<ST> *R, NodeMeta *meta, uint32_t *par, uint8_t *gat) {
+  const size_t tot = nk * (size_t)E;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t j = i / E, e = i % E;
+    const uint32_t s = kslot[j];
+    R[i] = sR[(size_t)s * E + e];
+    if (e == 0) {
+      meta[j] = smeta[s];
+      par[j] = (uint32_t)(kidx[j] / (uint64_t)G);
+      gat[j] = (uint8_t)(kidx[j] % (uint64_t)G);
+    }
+  }
+}
+
+__global__ void k_widen(const Z4<int32_t> *in, Z4<int64_t> *out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const Z4<int32_t> x = in[i];
+    out[i] = Z4<int64_t>{x.a, x.b, x.c, x.d};
+  }
+}
+
+// ---------------- host helpers ----------------
+double now_s() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
+
+struct CudaError : std::runtime_error { using std::runtime_error::runtime_error; };
+void ck(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) throw CudaError(std::string("CUDA error after ") + what + ": " + cudaGetErrorString(e));
+}
+
+struct DBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  void ensure(size_t bytes) {
+    if (bytes <= cap) return;
+    if (p) ck(cudaFree(p), "free");
+    size_t c = std::max(bytes, cap + cap / 2);
+    c = (c + 255) & ~(size_t)255;
+    ck(cudaMalloc(&p, c), "cudaMalloc");
+    cap = c;
+  }
+  template <typename T> T *as() const { return (T *)p; }
+  void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+};
+
+uint64_t powmod_h(uint64_t a, uint64_t e) {
+  uint64_t r = 1;
+  while (e) { if (e & 1) r = r * a % PRIME; a = a * a % PRIME; e >>= 1; }
+  return r;
+}
+
+}  // namespace
+
+struct Engine::Impl {
+  int dev;
+  int nsm = 148;
+  cudaStream_t s = nullptr;
+  cudaEvent_t ev[4];
+  DBuf fR, fMeta;                          // frontier
+  DBuf sH1, sH2, sIdx, sR, sMeta;          // survivors of the current level
+  DBuf k0, k1, v0, v1, hist, part;         // sort
+  DBuf work, tmp, kidx, kslot;             // dedupe
+  DBuf ginv, bad2, bad3, cxt, goal, stats;
+  std::vector<DBuf> par, gat;              // tree, one level each
+  DevStats *hstats = nullptr;              // pinned
+  long long launches = 0;
+  long long front_m = 1;                   // nodes in the current frontier
+
+  explicit Impl(int d) : dev(d) {
+    ck(cudaSetDevice(dev), "cudaSetDevice");
+    ck(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+    for (auto &e : ev) ck(cudaEventCreate(&e), "event");
+    ck(cudaMallocHost(&hstats, sizeof(DevStats)), "pinned");
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    stats.ensure(sizeof(DevStats));
+  }
+  ~Impl() {
+    cudaSetDevice(dev);
+    for (DBuf *b : {&fR, &fMeta, &sH1, &sH2, &sIdx, &sR, &sMeta, &k0, &k1, &v0, &v1, &hist, &part, &work, &tmp, &kidx,
+                    &kslot, &ginv, &bad2, &bad3, &cxt, &goal, &stats})
+      b->release();
+    for (auto &b : par) b.release();
+    for (auto &b : gat) b.release();
+    if (hstats) cudaFreeHost(hstats);
+    for (auto &e : ev) cudaEventDestroy(e);
+    if (s) cudaStreamDestroy(s);
+  }
+
+  template <int NQ> int run(const HostSpec &hs, const Options &opt, const std::function<void(const LevelStats &)> &cb,
+                            SearchResult &res);
+  template <int NQ, typename ST>
+  int levels(const HostSpec &hs, const DevSpec &sp, const Options &opt, int depth, int &t_start,
+             const std::function<void(const LevelStats &)> &cb, SearchResult &res);
+};
+
+template <int NQ, typename ST>
+int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &opt, int depth, int &t_start,
+                         const std::function<void(const LevelStats &)> &cb, SearchResult &res) {
+  constexpr int E = (1 << NQ) * (1 << NQ);
+  const int G = hs.G;
+  long long m = front_m;
+  for (int t = t_start; t <= depth; t++) {
+    const double t0 = now_s();
+    const bool keep = t < depth;
+    // survivors capacity: every child that passes the window rules, bounded by what the previous level kept
+    unsigned long long cap = keep ? (unsigned long long)m * G : 0;
+    const unsigned long long cap_limit = (unsigned long long)8 << 30;   // 8 Gi residuals would be 8 TB: never hit
+    if (cap > cap_limit) cap = cap_limit;
+    DevStats *dst = stats.as<DevStats>();
+    for (int attempt = 0; attempt < 2; attempt++) {
+      if (keep) {
+        sH1.ensure(cap * 8); sH2.ensure(cap * 8); sIdx.ensure(cap * 8);
+        sR.ensure(cap * E * sizeof(Z4<ST>)); sMeta.ensure(cap * sizeof(NodeMeta));
+      }
+      ck(cudaMemsetAsync(dst, 0, sizeof(DevStats), s), "memset");
+      const unsigned long long ffinit = ~0ULL;
+      ck(cudaMemcpyAsync(&dst->first_found, &ffinit, 8, cudaMemcpyHostToDevice, s), "h2d");
+      ExpandArgs<ST> a;
+      a.m = m; a.t = t; a.rem = depth - t; a.keep = keep;
+      a.R = fR.as<Z4<ST>>(); a.meta = fMeta.as<NodeMeta>(); a.st = dst; a.cap = cap;
+      a.sh1 = sH1.as<uint64_t>(); a.sh2 = sH2.as<uint64_t>(); a.sidx = sIdx.as<uint64_t>();
+      a.sR = sR.as<Z4<ST>>(); a.smeta = sMeta.as<NodeMeta>();
+      const long long want = (m + EXP_WARPS - 1) / EXP_WARPS;
+      const long long grid = std::max<long long>(1, std::min<long long>(want, (long long)nsm * 2 * 8));
+      if (opt.profile) ck(cudaEventRecord(ev[0], s), "event");
+      k_expand<NQ, ST><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(sp, a);
+      launches++;
+      ck(cudaGetLastError(), "expand kernel");
+      if (opt.profile) ck(cudaEventRecord(ev[1], s), "event");
+      ck(cudaMemcpyAsync(hstats, dst, sizeof(DevStats), cudaMemcpyDeviceToHost, s), "d2h");
+      ck(cudaStreamSynchronize(s), "expand");
+      if (opt.profile) { float ms = 0; cudaEventElapsedTime(&ms, ev[0], ev[1]); res.expand_ms += ms; }
+      if (hstats->ovf) return -2;                       // promote to int64 limbs and redo this level
+      if (!hstats->surv_overflow) break;
+      cap = hstats->n_surv;                             // exact survivor count: grow and redo once
+    }
+    if (hstats->surv_overflow) { res.error = "survivor buffer overflow"; return RC_CUDA; }
+    const DevStats h = *hstats;
+    res.t_evals += (long long)h.t_evals;
+    res.children += (long long)h.children;
+    LevelStats L;
+    L.t = t; L.parents = m; L.prefixes = m * G - (long long)h.w2; L.cut_w3 = (long long)h.w3;
+    L.cut_lb = (long long)h.dead; L.survivors = (long long)h.alive;
+    res.prefixes += L.prefixes;
+    if (h.found) {                                     // the lexicographically first circuit of this level
+      const unsigned long long o = h.first_found;
+      std::vector<int> c(t);
+      c[t - 1] = (int)(o % G);
+      uint32_t i = (uint32_t)(o / G);
+      for (int l = t - 1; l >= 1; l--) {
+        uint8_t gg; uint32_t pp;
+        ck(cudaMemcpy(&gg, gat[l].as<uint8_t>() + i, 1, cudaMemcpyDeviceToHost), "d2h");
+        ck(cudaMemcpy(&pp, par[l].as<uint32_t>() + i, 4, cudaMemcpyDeviceToHost), "d2h");
+        c[l - 1] = gg; i = pp;
+      }
+      res.circuit = c;
+      res.n_found = (long long)h.found;
+      res.levels = t;
+      return RC_CIRCUIT;
+    }
+    long long distinct = 0;
+    const size_t ns = keep ? (size_t)h.n_surv : 0;
+    if (ns) {
+      if (opt.profile) ck(cudaEventRecord(ev[2], s), "event");
+      k0.ensure(ns * 8); k1.ensure(ns * 8); v0.ensure(ns * 4); v1.ensure(ns * 4);
+      kidx.ensure(ns * 8); kslot.ensure(ns * 4);
+      hist.ensure(sort_hist_words(ns) * 4);
+      part.ensure(scan_partials_words(sort_hist_words(ns)) * 4);
+      SortScratch sc{hist.as<uint32_t>(), part.as<uint32_t>(), hist.cap / 4, part.cap / 4};
+      const unsigned gb = (unsigned)std::min<size_t>((ns + 255) / 256, (size_t)nsm * 16);
+      if (opt.dedupe && ns > 1) {
+        work.ensure(ns * sizeof(uint2)); tmp.ensure(ns * 4);
+        k_sort_init<<<gb, 256, 0, s>>>(sH1.as<uint64_t>(), ns, k0.as<uint64_t>(), v0.as<uint32_t>());
+        launches++;
+        const bool f = radix_sort(k0.as<uint64_t>(), v0.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(), ns, 32,
+                                  64, sc, s, nullptr);
+        launches += 4 * 5;
+        const uint64_t *sk = f ? k1.as<uint64_t>() : k0.as<uint64_t>();
+        const uint32_t *sv = f ? v1.as<uint32_t>() : v0.as<uint32_t>();
+        k_runs<<<gb, 256, 0, s>>>(sk, sv, ns, sIdx.as<uint64_t>(), kidx.as<uint64_t>(), kslot.as<uint32_t>(),
+                                  work.as<uint2>(), dst);
+        k_resolve<NQ, ST><<<(unsigned)nsm * 4, 256, 0, s>>>(sp, work.as<uint2>(), sv, sH1.as<uint64_t>(),
+                                                            sH2.as<uint64_t>(), sIdx.as<uint64_t>(), sR.as<Z4<ST>>(),
+                                                            sMeta.as<NodeMeta>(), tmp.as<uint32_t>(),
+                                                            kidx.as<uint64_t>(), kslot.as<uint32_t>(), dst);
+        launches += 2;
+        ck(cudaGetLastError(), "dedupe");
+        ck(cudaMemcpyAsync(hstats, dst, sizeof(DevStats), cudaMemcpyDeviceToHost, s), "d2h");
+        ck(cudaStreamSynchronize(s), "dedupe");
+        distinct = (long long)hstats->n_kept;
+      } else {
+        k_keep_all<<<gb, 256, 0, s>>>(sIdx.as<uint64_t>(), ns, kidx.as<uint64_t>(), kslot.as<uint32_t>());
+        launches++;
+        distinct = (long long)ns;
+      }
+      // restore lexicographic order: sort kept (index, slot) pairs by index
+      int bits = 1;
+      while (bits < 64 && ((unsigned long long)m * G) >> bits) bits++;
+      const int hi = ((bits + 7) / 8) * 8;
+      const bool f2 = radix_sort(kidx.as<uint64_t>(), kslot.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(),
+                                 (size_t)distinct, 0, hi, sc, s, nullptr);
+      if (distinct > 1) launches += (hi / 8) * 5;
+      const uint64_t *ki = f2 ? k1.as<uint64_t>() : kidx.as<uint64_t>();
+      const uint32_t *vi = f2 ? v1.as<uint32_t>() : kslot.as<uint32_t>();
+      if ((int)par.size() <= t) { par.resize(t + 1); gat.resize(t + 1); }
+      par[t].ensure((size_t)distinct * 4);
+      gat[t].ensure((size_t)distinct);
+      fR.ensure((size_t)distinct * E * sizeof(Z4<ST>));
+      fMeta.ensure((size_t)distinct * sizeof(NodeMeta));
+      const size_t tot = (size_t)distinct * E;
+      const unsigned gg = (unsigned)std::min<size_t>((tot + 255) / 256, (size_t)nsm * 32);
+      k_gather<ST><<<gg, 256, 0, s>>>(ki, vi, (size_t)distinct, G, E, sR.as<Z4<ST>>(), sMeta.as<NodeMeta>(),
+                                      fR.as<Z4<ST>>(), fMeta.as<NodeMeta>(), par[t].as<uint32_t>(),
+                                      gat[t].as<uint8_t>());
+      launches++;
+      ck(cudaGetLastError(), "gather");
+      if (opt.profile) ck(cudaEventRecord(ev[3], s), "event");
+      ck(cudaStreamSynchronize(s), "gather");
+      if (opt.profile) { float ms = 0; cudaEventElapsedTime(&ms, ev[2], ev[3]); res.dedupe_ms += ms; }
+    }
+    L.distinct = distinct;
+    L.proved_unsat = distinct == 0;
+    L.seconds = now_s() - t0;
+    res.levels = t;
+    cb(L);
+    if (!distinct) return RC_PROOF;
+    m = distinct;
+    front_m = m;
+    t_start = t + 1;
+  }
+  return RC_PROOF;   // stopped at the last level (not reachable: the last level keeps nothing)
+}
+
+template <int NQ>
+int Engine::Impl::run(const HostSpec &hs, const Options &opt, const std::function<void(const LevelStats &)> &cb,
+                      SearchResult &res) {
+  constexpr int N = 1 << NQ, E = N * N;
+  const int depth = opt.depth >= 0 ? opt.depth : hs.depth;
+  const SymGroup grp = sym_group(hs, opt.sym);
+  res.nsym = grp.nsym;
+  // depth 0: the target is the identity (cheese.cu:1794-1801)
+  {
+    bool done = hs.tk == 0;
+    for (int r = 0; r < N && done; r++)
+      for (int c = 0; c < N && done; c++) {
+        const Zw x = hs.target[r * N + c];
+        done = r == c ? (x.a == 1 && !x.b && !x.c && !x.d) : zzero(x);
+      }
+    if (done && !opt.nogoal) { res.depth0 = true; return RC_CIRCUIT; }
+  }
+  // device spec
+  DevSpec sp;
+  std::memset(&sp, 0, sizeof sp);
+  sp.n = hs.n; sp.G = hs.G; sp.depth = depth; sp.standard = hs.standard; sp.lite = hs.lite;
+  sp.tdiv = hs.tdiv < 1 ? 1 : hs.tdiv; sp.ncuts = (int)hs.cutmask.size(); sp.have_table = !hs.cxtable.empty();
+  sp.ncx = (int)hs.cxtable.size();
+  sp.nsym = grp.nsym; sp.nogoal = opt.nogoal; sp.gk = 0;
+  for (int i = 0; i < sp.ncuts; i++) { sp.cutmask[i] = hs.cutmask[i]; sp.cutsize[i] = hs.cutsize[i]; sp.rad[i] = hs.rad[i]; }
+  sp.w1 = powmod_h(3, (PRIME - 1) / 8); sp.w2 = sp.w1 * sp.w1 % PRIME; sp.w3 = sp.w2 * sp.w1 % PRIME;
+  for (int s2 = 0; s2 < grp.nsym; s2++) {
+    for (int x = 0; x < N; x++) sp.symperm[s2][x] = grp.bperm[s2 * N + x];
+    sp.symconj[s2] = grp.conj[s2];
+  }
+  for (int g = 0; g < hs.G; g++) {
+    sp.gflags[g] = hs.gflags[g]; sp.gnq[g] = (int8_t)hs.gnq[g]; sp.gik[g] = (int8_t)hs.gik[g];
+    for (int j = 0; j < 3; j++) sp.gq[g][j] = (int8_t)hs.gq[g][j];
+  }
+  std::vector<int4> gi((size_t)GMAX * 64, int4{0, 0, 0, 0});
+  for (int g = 0; g < hs.G; g++)
+    for (int i = 0; i < LMAX * LMAX; i++) {
+      const Zw z = hs.ginv[g][i];
+      gi[(size_t)g * 64 + i] = int4{(int)z.a, (int)z.b, (int)z.c, (int)z.d};
+    }
+  std::vector<longlong2> gl(2 * E);
+  for (int r = 0; r < N; r++)
+    for (int c = 0; c < N; c++) {
+      gl[2 * (r * N + c)] = make_longlong2(r == c ? 1 : 0, 0);
+      gl[2 * (r * N + c) + 1] = make_longlong2(0, 0);
+    }
+  ginv.ensure(gi.size() * sizeof(int4)); bad2.ensure(hs.bad2.size() + 1); bad3.ensure(hs.bad3.size() * 4 + 4);
+  cxt.ensure(std::max<size_t>(1, hs.cxtable.size()) * 4); goal.ensure(gl.size() * sizeof(longlong2));
+  ck(cudaMemcpyAsync(ginv.p, gi.data(), gi.size() * sizeof(int4), cudaMemcpyHostToDevice, s), "h2d");
+  ck(cudaMemcpyAsync(bad2.p, hs.bad2.data(), hs.bad2.size(), cudaMemcpyHostToDevice, s), "h2d");
+  ck(cudaMemcpyAsync(bad3.p, hs.bad3.data(), hs.bad3.size() * 4, cudaMemcpyHostToDevice, s), "h2d");
+  if (!hs.cxtable.empty())
+    ck(cudaMemcpyAsync(cxt.p, hs.cxtable.data(), hs.cxtable.size() * 4, cudaMemcpyHostToDevice, s), "h2d");
+  ck(cudaMemcpyAsync(goal.p, gl.data(), gl.size() * sizeof(longlong2), cudaMemcpyHostToDevice, s), "h2d");
+  sp.ginv = ginv.as<int4>(); sp.bad2 = bad2.as<uint8_t>(); sp.bad3 = bad3.as<uint32_t>(); sp.cxtable = cxt.as<int>();
+  sp.goal = goal.as<longlong2>();
+
+  // storage: int32 limbs unless the target itself needs more (then int64 from the start)
+  bool wide = opt.store64 == 1;
+  for (const Zw &z : hs.target) if (!fits32(z.a) || !fits32(z.b) || !fits32(z.c) || !fits32(z.d)) wide = true;
+  // root node
+  fMeta.ensure(sizeof(NodeMeta));
+  if (!wide) {
+    std::vector<Z4<int32_t>> t32(E);
+    for (int i = 0; i < E; i++) t32[i] = {(int32_t)hs.target[i].a, (int32_t)hs.target[i].b, (int32_t)hs.target[i].c, (int32_t)hs.target[i].d};
+    fR.ensure(E * sizeof(Z4<int32_t>));
+    ck(cudaMemcpyAsync(fR.p, t32.data(), E * sizeof(Z4<int32_t>), cudaMemcpyHostToDevice, s), "h2d");
+    k_root<NQ, int32_t><<<1, 32, 0, s>>>(sp, fR.as<Z4<int32_t>>(), fMeta.as<NodeMeta>(), hs.tk);
+  } else {
+    fR.ensure(E * sizeof(Z4<int64_t>));
+    ck(cudaMemcpyAsync(fR.p, hs.target.data(), E * sizeof(Zw), cudaMemcpyHostToDevice, s), "h2d");
+    k_root<NQ, int64_t><<<1, 32, 0, s>>>(sp, fR.as<Z4<int64_t>>(), fMeta.as<NodeMeta>(), hs.tk);
+  }
+  launches++;
+  ck(cudaGetLastError(), "root kernel");
+  int t = 1;
+  int rc;
+  front_m = 1;
+  if (!wide) {
+    rc = levels<NQ, int32_t>(hs, sp, opt, depth, t, cb, res);
+    if (rc == -2) {   // a limb left int32: widen the current frontier and redo level t with int64 limbs
+      DBuf w;
+      w.ensure((size_t)front_m * E * sizeof(Z4<int64_t>));
+      const size_t ne = (size_t)front_m * E;
+      k_widen<<<(unsigned)std::min<size_t>((ne + 255) / 256, (size_t)nsm * 32), 256, 0, s>>>(fR.as<Z4<int32_t>>(),
+                                                                                          w.as<Z4<int64_t>>(), ne);
+      launches++;
+      ck(cudaStreamSynchronize(s), "widen");
+      std::swap(fR.p, w.p); std::swap(fR.cap, w.cap);
+      w.release();
+      wide = true;
+      rc = levels<NQ, int64_t>(hs, sp, opt, depth, t, cb, res);
+    }
+  } else {
+    rc = levels<NQ, int64_t>(hs, sp, opt, depth, t, cb, res);
+  }
+  res.store64 = wide;
+  return rc;
+}
+
+Engine::Engine(int device) : impl_(new Impl(device)), dev_(device) {}
+Engine::~Engine() { delete impl_; }
+void *Engine::stream() const { return impl_->s; }
+
+int Engine::search(const HostSpec &hs, const Options &opt, const std::function<void(const LevelStats &)> &cb,
+                   SearchResult &res) {
+  res = SearchResult{};
+  const double t0 = now_s();
+  const long long l0 = impl_->launches;
+  int rc;
+  try {
+    ck(cudaSetDevice(dev_), "cudaSetDevice");
+    switch (hs.n) {
+      case 1: rc = impl_->run<1>(hs, opt, cb, res); break;
+      case 2: rc = impl_->run<2>(hs, opt, cb, res); break;
+      case 3: rc = impl_->run<3>(hs, opt, cb, res); break;
+      default: res.error = "n = " + std::to_string(hs.n) + " not built"; rc = RC_USAGE;
+    }
+  } catch (const CudaError &e) {
+    res.error = e.what();
+    rc = RC_CUDA;
+  }
+  res.launches = impl_->launches - l0;
+  res.total_ms = (now_s() - t0) * 1e3;
+  res.rc = rc;
+  return rc;
+}
+
+}  // namespace cz

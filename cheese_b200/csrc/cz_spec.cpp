@@ -1,0 +1,277 @@
+// Spec parsing, symmetry group and gate properties (host side of the boundary).
+#include "cz_spec.h"
+
+#include <algorithm>
+#include <cctype>
+#include <cstdlib>
+#include <cstring>
+
+namespace cz {
+
+namespace {
+
+// whitespace tokenizer with std::istream-like failure: a failed numeric read poisons the stream
+struct Reader {
+  const char *p, *end;
+  bool fail = false;
+  bool tok(std::string &s) {
+    while (p < end && std::isspace((unsigned char)*p)) p++;
+    if (p >= end) return false;
+    const char *b = p;
+    while (p < end && !std::isspace((unsigned char)*p)) p++;
+    s.assign(b, p);
+    return true;
+  }
+  int64_t num() {
+    std::string s;
+    if (fail || !tok(s)) { fail = true; return 0; }
+    char *e;
+    const long long v = std::strtoll(s.c_str(), &e, 10);
+    if (e == s.c_str()) { fail = true; return 0; }
+    return v;
+  }
+  Zw zw() { Zw z; z.a = num(); z.b = num(); z.c = num(); z.d = num(); return z; }
+};
+
+// local Pauli P_b (digits per qubit: 0 I, 1 X, 2 Y, 3 Z): column x has w^phase at row x ^ flip
+void pauli_local(int b, int nq, std::vector<Zw> &M) {
+  const int L = 1 << nq;
+  M.assign(L * L, Zw{0, 0, 0, 0});
+  int flip = 0, ym = 0, zm = 0;
+  for (int q = 0; q < nq; q++) {
+    const int d = (b >> (2 * q)) & 3;
+    if (d == 1 || d == 2) flip |= 1 << q;
+    if (d == 2) ym |= 1 << q;
+    if (d == 3) zm |= 1 << q;
+  }
+  for (int x = 0; x < L; x++)
+    M[(x ^ flip) * L + x] = zwpow(2 * __builtin_popcount(ym) + 4 * __builtin_popcount(x & (ym | zm)));
+}
+
+// A is Clifford iff A P A^dag is a scalar times a Pauli for every local Pauli P (exact over Z[w])
+bool is_clifford(const std::array<Zw, LMAX * LMAX> &A, int nq) {
+  const int L = 1 << nq, P = 1 << (2 * nq);
+  std::vector<Zw> Pb, Q, B(L * L), AP(L * L);
+  for (int b = 1; b < P; b++) {
+    pauli_local(b, nq, Pb);
+    for (int r = 0; r < L; r++)
+      for (int c = 0; c < L; c++) {
+        Zw acc{0, 0, 0, 0};
+        for (int m = 0; m < L; m++) acc = zadd(acc, zmul(A[r * L + m], Pb[m * L + c]));
+        AP[r * L + c] = acc;
+      }
+    for (int r = 0; r < L; r++)
+      for (int c = 0; c < L; c++) {
+        Zw acc{0, 0, 0, 0};
+        for (int m = 0; m < L; m++) acc = zadd(acc, zmul(AP[r * L + m], zconj(A[c * L + m])));
+        B[r * L + c] = acc;
+      }
+    bool found = false;
+    for (int q = 1; q < P && !found; q++) {      // B Q^dag = s I with s != 0
+      pauli_local(q, nq, Q);
+      Zw s{0, 0, 0, 0};
+      bool ok = true;
+      for (int r = 0; r < L && ok; r++)
+        for (int c = 0; c < L && ok; c++) {
+          Zw acc{0, 0, 0, 0};
+          for (int m = 0; m < L; m++) acc = zadd(acc, zmul(B[r * L + m], zconj(Q[c * L + m])));
+          if (r == c) { if (r == 0) s = acc; else ok = zeq(acc, s); }
+          else ok = zzero(acc);
+        }
+      found = ok && !zzero(s);
+    }
+    if (!found) return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+int parse_spec(const char *text, size_t len, HostSpec &s, std::string &err) {
+  s = HostSpec{};
+  Reader in{text, text + len};
+  std::string tok;
+  bool have_start = false, have_goal_rows = false, have_ginfo = false;
+  if (!in.tok(tok) || tok != "cheese-spec") { err = "not a spec"; return RC_SPEC; }
+  (void)in.num();
+  while (!in.fail && in.tok(tok)) {
+    if (tok == "n") s.n = (int)in.num();
+    else if (tok == "mode" || tok == "phase") {
+      std::string v;
+      if (!in.tok(v)) break;
+      if (v == "states") s.states = 1;
+      else if (v != "unitary" && v != "exact") { err = "unsupported " + tok + " " + v; return RC_SPEC; }
+    } else if (tok == "pairs") s.m = (int)in.num();
+    else if (tok == "start") {                 // state targets: parsed for the grammar, refused at run time
+      (void)in.num();
+      if (s.n < 1 || s.n > NQMAX) { in.fail = true; break; }
+      const int N = 1 << s.n;
+      for (int i = 0; i < N * N; i++) (void)in.zw();
+      have_start = true;
+    } else if (tok == "goal") {
+      const int m = (int)in.num();
+      const int w = 2 + (int)s.cutmask.size();
+      for (int i = 0; i < m * w; i++) (void)in.num();
+      have_ginfo = m * w > 0;
+    } else if (tok == "depth") s.depth = (int)in.num();
+    else if (tok == "standard") s.standard = (int)in.num();
+    else if (tok == "lite") s.lite = (int)in.num();
+    else if (tok == "tdiv") s.tdiv = (int)in.num();
+    else if (tok == "gates") {
+      s.G = (int)in.num();
+      if (s.G > GMAX) { err = "too many gates"; return RC_SPEC; }
+      if (s.G < 0) { in.fail = true; break; }
+      for (int g = 0; g < s.G && !in.fail; g++) {
+        std::string name;
+        if (!in.tok(name)) { in.fail = true; break; }
+        const int nq = (int)in.num();
+        if (nq < 1 || nq > 3) { in.fail = true; break; }
+        std::array<int, 3> q{0, 0, 0};
+        for (int j = 0; j < nq; j++) q[j] = (int)in.num();
+        const int L = 1 << nq;
+        (void)in.num();                                  // forward exponent (state targets only)
+        for (int i = 0; i < L * L; i++) (void)in.zw();   // forward matrix
+        const int ik = (int)in.num();
+        std::array<Zw, LMAX * LMAX> inv{};
+        for (int i = 0; i < L * L; i++) inv[i] = in.zw();
+        s.names.push_back(name); s.gnq.push_back(nq); s.gq.push_back(q); s.gik.push_back(ik); s.ginv.push_back(inv);
+      }
+    } else if (tok == "bad2") {
+      const int m = (int)in.num();
+      s.bad2.assign((size_t)s.G * s.G, 0);
+      for (int i = 0; i < m && !in.fail; i++) {
+        const int a = (int)in.num(), b = (int)in.num();
+        if (a >= 0 && b >= 0 && a < s.G && b < s.G) s.bad2[a * s.G + b] = 1;
+      }
+    } else if (tok == "bad3") {
+      const int m = (int)in.num();
+      s.bad3.assign(((size_t)s.G * s.G * s.G + 31) / 32, 0);
+      for (int i = 0; i < m && !in.fail; i++) {
+        const int a = (int)in.num(), b = (int)in.num(), c = (int)in.num();
+        if (a < 0 || b < 0 || c < 0 || a >= s.G || b >= s.G || c >= s.G) continue;
+        const uint32_t t = (uint32_t)((a * s.G + b) * s.G + c);
+        s.bad3[t >> 5] |= 1u << (t & 31);
+      }
+    } else if (tok == "target") {
+      const int k = (int)in.num();
+      if (s.n < 1 || s.n > NQMAX) { err = "n = " + std::to_string(s.n) + " not built"; return RC_USAGE; }
+      const int N = 1 << s.n;
+      std::vector<Zw> M(N * N);
+      for (auto &x : M) x = in.zw();
+      if (!s.states) { s.target = M; s.tk = k; s.gk = 0; }
+      else have_goal_rows = true;
+    } else if (tok == "cuts") {
+      const int m = (int)in.num();
+      for (int i = 0; i < m && !in.fail; i++) {
+        const int sz = (int)in.num();
+        int mask = 0;
+        for (int j = 0; j < sz; j++) mask |= 1 << (int)in.num();
+        if ((int)s.cutmask.size() < CUTMAX) { s.cutmask.push_back(mask); s.cutsize.push_back(sz); s.rad.push_back(2 * sz + 1); }
+      }
+    } else if (tok == "cxtable") {
+      const int m = (int)in.num();
+      if (m < 0 || m > (1 << 22)) { err = "cxtable too large"; return RC_SPEC; }
+      s.cxtable.resize(m);
+      for (auto &v : s.cxtable) v = (int)in.num();
+    } else if (tok == "end") break;
+    else { err = "unknown spec field " + tok; return RC_SPEC; }
+  }
+  if (s.states) {                              // parsed for the grammar; the search refuses it (exit 3)
+    if (!have_start || !have_goal_rows || !have_ginfo || s.m < 1 || s.m > (1 << std::max(0, std::min(s.n, 6)))) {
+      err = "states spec incomplete";
+      return RC_SPEC;
+    }
+    return 0;
+  }
+  if (s.n < 1 || s.n > NQMAX) { err = "n = " + std::to_string(s.n) + " not built"; return RC_USAGE; }
+  const int N = 1 << s.n;
+  if ((int)s.target.size() != N * N) { s.target.assign(N * N, Zw{0, 0, 0, 0}); }
+  if (s.bad2.empty()) s.bad2.assign((size_t)s.G * s.G, 0);
+  if (s.bad3.empty()) s.bad3.assign(((size_t)s.G * s.G * s.G + 31) / 32, 0);
+  if (s.tdiv < 1) s.tdiv = 1;
+  for (int g = 0; g < s.G; g++) {
+    for (int j = 0; j < s.gnq[g]; j++)
+      if (s.gq[g][j] < 0 || s.gq[g][j] >= s.n) { err = "gate " + s.names[g] + " acts outside the register"; return RC_SPEC; }
+    uint8_t f = 0;
+    if (is_clifford(s.ginv[g], s.gnq[g])) f |= GF_CLIFFORD;
+    if (s.gnq[g] == 1) f |= GF_ONEQ;
+    s.gflags.push_back(f);
+  }
+  for (size_t i = 0; i < s.cutmask.size(); i++)
+    if (s.cutsize[i] > s.n / 2 || s.cutsize[i] < 1) { err = "cut larger than half the register"; return RC_SPEC; }
+  return 0;
+}
+
+namespace {
+std::vector<std::string> split_name(const std::string &nm) {
+  std::vector<std::string> parts;
+  size_t a = 0, b;
+  while ((b = nm.find('_', a)) != std::string::npos) { parts.push_back(nm.substr(a, b - a)); a = b + 1; }
+  parts.push_back(nm.substr(a));
+  return parts;
+}
+// image of candidate g under a relabelling (and conjugation): names are L_<gate>_<q>[_<q>...]
+int sym_gate(const HostSpec &hs, const std::vector<int> &perm, bool conj, int g) {
+  const std::vector<std::string> parts = split_name(hs.names[g]);
+  if (parts.size() < 2) return -1;
+  std::string gate = parts[1];
+  if (conj) {
+    if (gate == "t") gate = "tdg"; else if (gate == "tdg") gate = "t";
+    else if (gate == "s") gate = "sdg"; else if (gate == "sdg") gate = "s";
+    else if (gate != "x" && gate != "z" && gate != "h" && gate != "cx" && gate != "cz" && gate != "ccx") return -1;
+  }
+  std::vector<int> qs;
+  for (size_t i = 2; i < parts.size(); i++) {
+    const int q = std::atoi(parts[i].c_str());
+    if (q < 0 || q >= (int)perm.size()) return -1;
+    qs.push_back(perm[q]);
+  }
+  if (gate == "ccx" && qs.size() == 3 && qs[0] > qs[1]) std::swap(qs[0], qs[1]);
+  std::string want = "L_" + gate;
+  for (int q : qs) want += "_" + std::to_string(q);
+  for (int h = 0; h < hs.G; h++) if (hs.names[h] == want) return h;
+  return -1;
+}
+}  // namespace
+
+SymGroup sym_group(const HostSpec &hs, bool on) {
+  const int n = hs.n, N = 1 << n;
+  SymGroup g;
+  std::vector<int> p(n);
+  for (int i = 0; i < n; i++) p[i] = i;
+  std::vector<std::vector<int>> perms;
+  do perms.push_back(p); while (on && std::next_permutation(p.begin(), p.end()));
+  for (int cj = 0; cj < (on ? 2 : 1); cj++)
+    for (auto &pm : perms) {
+      std::vector<int> gm(hs.G);
+      bool ok = true;
+      for (int c = 0; c < hs.G && ok; c++) ok = (gm[c] = sym_gate(hs, pm, cj, c)) >= 0;
+      if (!ok) continue;
+      g.perm.push_back(pm); g.conj.push_back((uint8_t)cj); g.gmap.push_back(gm);
+      for (int x = 0; x < N; x++) {
+        int y = 0;
+        for (int i = 0; i < n; i++) if ((x >> i) & 1) y |= 1 << pm[i];
+        g.bperm.push_back((uint8_t)y);
+      }
+    }
+  g.nsym = (int)g.conj.size();
+  return g;
+}
+
+std::vector<int> inverse_gates(const HostSpec &hs) {
+  std::vector<int> inv(hs.G, -1);
+  for (int g = 0; g < hs.G; g++) {
+    const std::string &nm = hs.names[g];
+    const size_t a = nm.find('_');
+    if (a == std::string::npos) continue;
+    const size_t b = nm.find('_', a + 1);
+    std::string gate = nm.substr(a + 1, b == std::string::npos ? std::string::npos : b - a - 1);
+    if (gate == "t") gate = "tdg"; else if (gate == "tdg") gate = "t";
+    else if (gate == "s") gate = "sdg"; else if (gate == "sdg") gate = "s";
+    const std::string want = nm.substr(0, a + 1) + gate + (b == std::string::npos ? "" : nm.substr(b));
+    for (int h = 0; h < hs.G; h++) if (hs.names[h] == want) inv[g] = h;
+  }
+  return inv;
+}
+
+}  // namespace cz

@@ -1,0 +1,100 @@
+/* cheese_b200: C ABI of the B200-native rebuild of cheese's gate-count search.
+ *
+ * The reference (jkhav/cheese) has no in-process API: its boundary is the process interface of build/cheese
+ * (spec file in, one JSON line per level on stdout, exit code). This ABI exposes exactly that interface as calls
+ * on plain pointers and sizes, so the drop-in binary (cheese_b200/bin/cheese) and any FFI caller (ctypes, cgo,
+ * JNI ...) run the same code. Every entry point returns 0 or one of the reference's exit codes:
+ *   CZ_CIRCUIT 0, CZ_PROOF 1, CZ_ERR_SPEC 2, CZ_ERR_USAGE 3, CZ_ERR_OVERFLOW 4, CZ_ERR_CUDA 5
+ * (src/cheese.cu:1023-1026, 1153-1220, 1284-1285, 1848-1891). No C++ exception crosses the boundary.
+ * Threading: one engine per host thread; an engine owns one device and one stream.
+ */
+#ifndef CHEESE_B200_H
+#define CHEESE_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CZ_CIRCUIT 0
+#define CZ_PROOF 1
+#define CZ_ERR_SPEC 2
+#define CZ_ERR_USAGE 3
+#define CZ_ERR_OVERFLOW 4
+#define CZ_ERR_CUDA 5
+#define CZ_MAX_DEPTH 48
+
+typedef struct cz_spec cz_spec;
+typedef struct cz_engine cz_engine;
+
+/* Parses a spec in the reference's text grammar (replaces read_spec, src/cheese.cu:1149-1226; the writer is
+ * python/cheese/spec.py:356-415). Returns 0, CZ_ERR_SPEC (malformed: "not a spec", "unknown spec field X", ...)
+ * or CZ_ERR_USAGE (qubit count not built: n outside 1..3). err receives a one-line message. */
+int cz_spec_parse(const char *text, size_t len, cz_spec **out, char *err, size_t errlen);
+void cz_spec_free(cz_spec *spec);
+/* qubits, candidates and the spec's own budget ("depth" field) */
+int cz_spec_info(const cz_spec *spec, int *n, int *gates, int *depth);
+/* candidate name, e.g. "L_cx_0_1" (NULL when out of range) */
+const char *cz_spec_gate_name(const cz_spec *spec, int g);
+/* 1 when the spec is a state-target spec ("mode states"), which the GPU search refuses like the reference's
+ * GPU binary (src/cheese.cu:1871-1876) */
+int cz_spec_is_states(const cz_spec *spec);
+
+/* Search engine on CUDA device `device` (replaces the device setup of run<NQ>, src/cheese.cu:1762-1792). */
+int cz_engine_create(int device, cz_engine **out, char *err, size_t errlen);
+void cz_engine_destroy(cz_engine *engine);
+
+/* flags of the reference CLI (src/cheese.cu:1859-1868) */
+typedef struct {
+  int depth;        /* --depth D; -1: the spec's budget */
+  int dedupe;       /* 1; 0: --no-dedupe */
+  int sym;          /* 1; 0: --no-sym */
+  int store64;      /* 0: int32 limbs promoted to int64 on demand; 1: int64 limbs throughout */
+  int profile;      /* 1: record device times per phase (cz_result.expand_ms / dedupe_ms) */
+} cz_options;
+void cz_options_default(cz_options *opt);
+
+/* one JSON stats line of the reference (src/cheese.cu:1354-1356) */
+typedef struct {
+  int t;
+  int64_t parents, prefixes, cut_w3, cut_lb, survivors, distinct;
+  int proved_unsat;
+  double seconds;
+} cz_level_stats;
+typedef void (*cz_level_fn)(void *user, const cz_level_stats *level);
+
+typedef struct {
+  int rc;                      /* the exit code the reference binary would return */
+  int depth0;                  /* 1: the target is already the goal ({"found": 0, "circuit": []}) */
+  int found_len;               /* rc 0: gates in the lexicographically first shortest circuit */
+  int found[CZ_MAX_DEPTH];     /* candidate indices (names: cz_spec_gate_name) */
+  int64_t n_found;             /* circuits of that length found at that level ("found" field) */
+  int nsym;                    /* symmetry group size */
+  int store64;                 /* 1: the run used int64 limbs */
+  int levels;                  /* levels completed */
+  int64_t prefixes;            /* sum of the per-level "prefixes" fields */
+  int64_t kernel_launches;     /* device kernels launched by this call */
+  int64_t t_evals;             /* Walsh-Hadamard T-bound evaluations */
+  int64_t children;            /* children evaluated past the window rules */
+  double expand_ms, dedupe_ms; /* device time per phase (profile = 1) */
+  double total_ms;             /* host wall time of the call */
+  char error[256];
+} cz_result;
+
+/* The plain search of `cheese SPEC [flags]` without --mitm / --table (replaces run<NQ> + levels<NQ>,
+ * src/cheese.cu:1249-1377, 1762-1849). Calls on_level after every completed level (may be NULL). */
+int cz_search(cz_engine *engine, const cz_spec *spec, const cz_options *opt, cz_level_fn on_level, void *user,
+              cz_result *out);
+
+/* Convenience for FFI callers that hold the spec as text: parse + search in one call. */
+int cz_search_text(cz_engine *engine, const char *spec_text, size_t len, const cz_options *opt, cz_level_fn on_level,
+                   void *user, cz_result *out);
+
+/* The library version string and the CUDA architecture it was compiled for ("sm_100a"). */
+const char *cz_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

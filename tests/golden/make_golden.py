@@ -1,0 +1,118 @@
+"""Generate the golden fixtures of the gate-count search from the reference itself.
+
+Run in a container that has the reference source tree (read-only is fine) and the reference CPU build
+(`make -C oracle`, which compiles it from the reference's own sources into oracle/_ref/):
+
+    python tests/golden/make_golden.py [--ref /path/to/reference] [--quick]
+
+Writes
+  tests/golden/specs/<name>.spec        spec files written by the reference's spec generator (python/cheese/spec.py)
+  cheese_b200/data/base-n{2,3}.spec     the default Clifford+T spec per qubit count (its target is replaced per job)
+  tests/golden/cases.json               per case: spec, flags, exit code and the reference's stdout with every
+                                        "seconds" value replaced by 0.00 (machine dependent, never compared)
+The reference is used only here, to produce data; nothing at test time reads the reference tree.
+"""
+import argparse
+import io
+import json
+import random
+import re
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[2]
+GOLD = ROOT / "tests" / "golden"
+SECONDS = re.compile(r'"seconds": [0-9.]+')
+
+# (case name, target qasm stem, budget, extra flags): the reference's own regression verdicts (tests/check.sh),
+# its bench list (tests/bench.sh) and the deep proofs of the benchmark configuration
+CASES = [
+    ("cs-4", "cs", 4, []), ("cs-5", "cs", 5, []),
+    ("ccz-7", "ccz", 7, []), ("ccz-8", "ccz", 8, []), ("ccz-8-nosym", "ccz", 8, ["--no-sym"]),
+    ("qft_2-6", "qft_2", 6, []), ("qft_2-7", "qft_2", 7, []),
+    ("relative-phase-toffoli-9", "relative-phase-toffoli", 9, []),
+    ("toffoli-7-nodedupe", "toffoli", 7, ["--no-dedupe"]),
+    ("toffoli-9-nosym", "toffoli", 9, ["--no-sym"]),
+    ("fredkin-9", "fredkin", 9, []), ("peres-9", "peres", 9, []), ("half_adder_3-9", "half_adder_3", 9, []),
+] + [(f"toffoli-{d}", "toffoli", d, []) for d in range(1, 11)]
+SLOW = [("grover_3-10", "grover_3", 10, []), ("toffoli-11", "toffoli", 11, []), ("toffoli-12", "toffoli", 12, []),
+        ("toffoli-11-nosym", "toffoli", 11, ["--no-sym"])]
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--quick", action="store_true", help="skip the cases that take more than a few seconds")
+    o = ap.parse_args()
+    sys.dont_write_bytecode = True
+    sys.path.insert(0, str(Path(o.ref) / "python"))
+    from cheese import spec as refspec            # the reference's spec writer
+    sys.path.insert(0, str(ROOT))
+    from cheese_b200 import workloads
+
+    binp = ROOT / "oracle" / "_ref" / "cheese-cpu"
+    b64 = ROOT / "oracle" / "_ref" / "cheese-cpu-store64"
+    assert binp.exists(), "build the reference CPU binary first: make -C oracle"
+    (GOLD / "specs").mkdir(parents=True, exist_ok=True)
+
+    def write_spec(name, n, circ, depth):
+        buf = io.StringIO()
+        refspec.write_spec(buf, n, circ, depth)
+        (GOLD / "specs" / f"{name}.spec").write_text(buf.getvalue())
+        return buf.getvalue()
+
+    def run(case, spec, flags, exe=binp):
+        t0 = time.time()
+        p = subprocess.run([str(exe), str(GOLD / "specs" / f"{spec}.spec")] + flags, capture_output=True, text=True)
+        out = [SECONDS.sub('"seconds": 0.00', l) for l in p.stdout.splitlines()]
+        print(f"{case}: rc {p.returncode}, {len(out)} lines, {time.time() - t0:.1f} s", file=sys.stderr)
+        return {"name": case, "spec": spec, "flags": flags, "rc": p.returncode, "stdout": out}
+
+    # target specs written by the reference generator (budget line = the first budget used)
+    qdir = Path(o.ref) / "tests" / "qasm"
+    cases = []
+    written = set()
+    for name, stem, d, flags in CASES + ([] if o.quick else SLOW):
+        if stem not in written:
+            n, circ = refspec.parse_qasm(qdir / f"{stem}.qasm")
+            write_spec(stem, n, circ, d)
+            written.add(stem)
+        cases.append(run(name, stem, ["--depth", str(d)] + flags))
+
+    # base specs: identity target, default Clifford+T candidates, per qubit count
+    for n in (2, 3):
+        text = write_spec(f"base-n{n}", n, [], 1)
+        (ROOT / "cheese_b200" / "data" / f"base-n{n}.spec").write_text(text)
+
+    # seeded random circuits (the batched workload's generator): reference spec, checked against ours
+    rng = random.Random(20261203)
+    for i in range(24):
+        n, circ = workloads.random_circuit(rng, L=rng.randint(6, 9))
+        name = f"rand-{i:02d}"
+        text = write_spec(name, n, circ, len(circ))
+        assert text == workloads.make_spec(n, circ, len(circ)), f"{name}: spec assembly differs from the reference"
+        cases.append(run(name, name, []))
+        cases[-1]["circuit"] = [[g, list(qs)] for g, qs in circ]
+
+    # a state-target spec (RUS without measurement, ancilla qubit 1 of CS): the GPU binaries refuse it (exit 3)
+    n, circ = refspec.parse_qasm(qdir / "cs.qasm")
+    buf = io.StringIO()
+    refspec.write_spec(buf, n, circ, 5, inputs=[0, 1])
+    (GOLD / "specs" / "cs-states.spec").write_text(buf.getvalue())
+
+    # int32 overflow: a 2-qubit target (HT)^140 with sqrt2 exponent 72 (coefficients ~2^36); default build exits 4,
+    # the -DSTORE64 build runs the search
+    circ = [("h", (0,)), ("t", (0,))] * 140
+    write_spec("overflow", 2, circ, 4)
+    cases.append(run("overflow-4", "overflow", []))
+    c64 = run("overflow-4-store64", "overflow", [], exe=b64)
+    cases.append(c64)
+
+    (GOLD / "cases.json").write_text(json.dumps(cases, indent=1) + "\n")
+    print(f"{len(cases)} cases written", file=sys.stderr)
+
+
+if __name__ == "__main__":
+    main()
