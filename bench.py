@@ -1,0 +1,285 @@
+"""Benchmark of the gate-count search: the deep-proof workload, 3 qubits, default Clifford+T candidates (27).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = the three proofs of the deep-proof configuration: Toffoli at budgets 11 and 12 and CCZ at budget 8
+(every one exits 1: no circuit of at most that many gates exists). Metric: prefixes/s, the sum of the per-level
+"prefixes" fields of the reference's JSON statistics over the step, divided by the step time; the Toffoli budget-12
+proof time is reported beside it. Inputs are the reference's own targets (tests/golden/specs, written by its spec
+generator); nothing is random.
+
+value: device-timed (CUDA events on the engine's stream), specs parsed and their tables resident on the device,
+L2 flushed (256 MiB write) between steps. e2e: the same metric through the C ABI's text entry point
+(cz_search_text: parse, upload, search, read-back) timed on the host. Multi-GPU: replicas (every rank runs the
+whole workload on its own GPU; the search has no collective), value = all ranks' prefixes / max over ranks.
+
+--impl reference times the reference's own CPU build (oracle/_ref/cheese-cpu, compiled from the reference sources
+with its OpenMP recipe) on the host cores, on a bounded sample of the same workload per step.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+SPECS = ROOT / "tests" / "golden" / "specs"
+REF_CPU = ROOT / "oracle" / "_ref" / "cheese-cpu"
+WORKLOAD = [("toffoli", 11), ("toffoli", 12), ("ccz", 8)]
+METRIC = "prefixes/s"
+# algorithmic int32 operations (a multiply or an add counts 1) per unit of work of the level kernel, 3 qubits:
+#  T-bound evaluation: 64 (fa, fb) x 64 points x (16 mul + 12 add Z[w] product + 6 stages x 4 add/sub butterflies
+#  + 5 valuation ops)
+#  child evaluation: residual update S g^-1 over 64 entries (<= 2 Z[w] multiply-adds) + normalisation, goal,
+#  H-structure and support tests (~16 ops per entry)
+OPS_T_EVAL = 64 * 64 * (28 + 24 + 5)
+OPS_CHILD = 64 * (2 * 32 + 16)
+CLOCK_Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+           "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+           "clocks_event_reasons.sw_power_cap")
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def allreduce(vals, op):
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(vals, dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return t.tolist()
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs"""
+
+    def __init__(self, device):
+        self.device, self.rows, self.p = device, [], None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={CLOCK_Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "100", "-i", str(self.device)], stdout=subprocess.PIPE, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.p = None
+        return self
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            self.p.wait()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows),
+                "power_w_max": max((float(r[3]) for r in self.rows if r[3].replace(".", "").isdigit()), default=None)}
+
+
+def run_ref_cpu(cases, threads):
+    """the reference CPU build on (spec, budget) cases: (prefixes, seconds)"""
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    pre, t0 = 0, time.perf_counter()
+    for stem, d in cases:
+        p = subprocess.run([str(REF_CPU), str(SPECS / f"{stem}.spec"), "--depth", str(d)], capture_output=True,
+                           text=True, env=env, timeout=3600)
+        if p.returncode not in (0, 1):
+            raise RuntimeError(f"reference CPU build failed on {stem} {d}: {p.stderr[-300:]}")
+        pre += sum(json.loads(l).get("prefixes", 0) for l in p.stdout.splitlines() if '"prefixes"' in l)
+    return pre, time.perf_counter() - t0
+
+
+def reference_sample(steps, warmup, threads):
+    """bounded per-step sample of the workload for the reference CPU arm, sized so K + W steps take ~2.5 min"""
+    _, t10 = run_ref_cpu([("toffoli", 10)], threads)          # calibration (~2.4 s on 8 cores)
+    f = t10 / 2.4
+    budget = 150.0 / max(1, steps + warmup)
+    for cases, est in ([WORKLOAD, (17 + 72 + 0.1) * f], [[("ccz", 8), ("toffoli", 11)], (17 + 0.1) * f],
+                       [[("ccz", 8), ("toffoli", 10)], 2.5 * f]):
+        if est <= budget:
+            return cases
+    return [("ccz", 8), ("toffoli", 9)]
+
+
+def reference_arm(args, ws, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    if not REF_CPU.exists():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/cheese-cpu not built (make -C oracle)"}))
+        return
+    cases = reference_sample(args.steps, args.warmup, threads)
+    for _ in range(args.warmup):
+        run_ref_cpu(cases, threads)
+    pre = secs = 0.0
+    for _ in range(args.steps):
+        p, s = run_ref_cpu(cases, threads)
+        pre += p
+        secs += s
+    v = pre / secs
+    sample = " + ".join(f"{a}-{b}" for a, b in cases)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "prefixes/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "reference targets",
+        "config": {"workload": "deep proofs, 3 qubits, 27 Clifford+T candidates", "sample": sample,
+                   "threads": threads},
+        "cpu_baseline": {"value": v, "unit": "prefixes/s", "cores": threads, "kind": "reference",
+                         "sample": f"{sample} per step, reference CPU build (OpenMP, Thrust OMP backend)"},
+        "e2e": {"value": v, "unit": "prefixes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    ws, rank, local = dist_init() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
+                                                                 int(os.environ.get("RANK", "0")), 0)
+    if args.impl == "reference":
+        return reference_arm(args, ws, rank)
+
+    import torch
+    import cheese_b200 as cz
+    torch.cuda.set_device(local)
+    eng = cz.Engine(local)
+    stream = torch.cuda.ExternalStream(eng.stream, device=f"cuda:{local}")
+    texts = {stem: (SPECS / f"{stem}.spec").read_text() for stem, _ in WORKLOAD}
+    specs = {stem: cz.Spec(t) for stem, t in texts.items()}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def step(timed):
+        """the three proofs; returns (prefixes, device ms, toffoli-12 ms, per-search results)"""
+        outs, t12 = [], 0.0
+        tot = 0.0
+        for stem, d in WORKLOAD:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            o = eng.search(specs[stem], depth=d, profile=True)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            if o.rc != 1:
+                raise RuntimeError(f"{stem} {d}: exit {o.rc} ({o.error}), expected a proof")
+            tot += ms
+            if (stem, d) == ("toffoli", 12):
+                t12 = ms
+            outs.append(o)
+        return sum(o.raw.prefixes for o in outs), tot, t12, outs
+
+    for _ in range(args.warmup):
+        step(False)
+    peak_int = eng.int32_peak()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    prefixes = 0
+    dev_ms = t12_ms = 0.0
+    exp_ms = ops = 0.0
+    launches = exp_launches = 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1)                     # L2 (126 MB) flushed between steps
+            torch.cuda.synchronize()
+            p, ms, t12, outs = step(True)
+            prefixes += p
+            dev_ms += ms
+            t12_ms += t12
+            for o in outs:
+                r = o.raw
+                exp_ms += r.expand_ms
+                exp_launches += r.expand_launches
+                launches += r.kernel_launches
+                ops += r.t_evals * OPS_T_EVAL + r.children * OPS_CHILD
+    torch.cuda.synchronize()
+    # end to end through the C ABI's text entry point: parse + upload + search + read-back, host-timed
+    h2d = d2h = 0
+    e2e_pre = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for stem, d in WORKLOAD:
+            o = eng.search(texts[stem], depth=d)
+            e2e_pre += o.raw.prefixes
+            h2d += o.raw.h2d_bytes + len(texts[stem])
+            d2h += o.raw.d2h_bytes
+    e2e_s = time.perf_counter() - t0
+    step_ms = dev_ms / args.steps
+    if ws > 1:
+        step_ms, e2e_s = allreduce([step_ms, e2e_s], "max")
+        prefixes, e2e_pre = allreduce([float(prefixes), float(e2e_pre)], "sum")
+    value = prefixes / args.steps / (step_ms / 1e3)
+    launch_ms = exp_ms / max(1, exp_launches)
+    achieved = (ops / max(1, exp_launches)) / (launch_ms * 1e-3) if launch_ms > 0 else 0.0
+    traffic = None
+    tf = ROOT / "profiles" / "k_expand-traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get("bytes_per_launch")
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and REF_CPU.exists():
+        threads = os.cpu_count() or 1
+        cases = [("ccz", 8), ("toffoli", 11)]
+        cp, cs = run_ref_cpu(cases, threads)
+        cpu = {"value": cp / cs, "unit": "prefixes/s", "cores": threads, "kind": "reference",
+               "sample": "ccz-8 + toffoli-11 once, reference CPU build (OpenMP), %.1f s" % cs}
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "prefixes/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "reference targets (Toffoli, CCZ specs from its generator)",
+            "config": {"workload": "deep proofs, 3 qubits, 27 Clifford+T candidates: toffoli budget 11 + toffoli "
+                                   "budget 12 + ccz budget 8 per step", "parallelism": f"replicas x{ws}",
+                       "l2": "flushed between steps (256 MiB write)", "toffoli12_proof_ms": t12_ms / args.steps,
+                       "prefixes_per_step": prefixes / args.steps / ws},
+            "e2e": {"value": e2e_pre / e2e_s, "unit": "prefixes/s", "h2d_bytes_per_step": h2d // args.steps,
+                    "d2h_bytes_per_step": d2h // args.steps},
+            "gpu_launches": launches,
+            "roofline": {"bound": "int32", "kernel": "k_expand", "achieved": achieved / 1e12, "peak": peak_int / 1e12,
+                         "unit": "Tops/s", "frac": achieved / peak_int if peak_int else None, "traffic": traffic,
+                         "peak_source": "measured in this run: IMAD loop (multiply-add = 2 ops)",
+                         "launch_ms": launch_ms, "ops_per_launch": ops / max(1, exp_launches)},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(out))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    eng.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -34,7 +34,8 @@ class Result(C.Structure):
                 ("n_found", C.c_int64), ("nsym", C.c_int), ("store64", C.c_int), ("levels", C.c_int),
                 ("prefixes", C.c_int64), ("kernel_launches", C.c_int64), ("t_evals", C.c_int64),
                 ("children", C.c_int64), ("expand_ms", C.c_double), ("dedupe_ms", C.c_double),
-                ("total_ms", C.c_double), ("error", C.c_char * 256)]
+                ("total_ms", C.c_double), ("expand_launches", C.c_int64), ("h2d_bytes", C.c_int64),
+                ("d2h_bytes", C.c_int64), ("error", C.c_char * 256)]
 
 
 LEVEL_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(LevelStats))
@@ -52,6 +53,8 @@ SIGNATURES = {
     "cz_search": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Options), LEVEL_FN, C.c_void_p, C.POINTER(Result)]),
     "cz_search_text": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(Options), LEVEL_FN, C.c_void_p,
                                  C.POINTER(Result)]),
+    "cz_engine_stream": (C.c_void_p, [C.c_void_p]),
+    "cz_int32_peak": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "cz_version": (C.c_char_p, []),
 }
 
@@ -119,6 +122,17 @@ class Engine:
     def __del__(self):
         if getattr(self, "_h", None):
             self.close()
+
+    @property
+    def stream(self):
+        """the cudaStream_t the engine launches on (an integer handle)"""
+        return lib().cz_engine_stream(self._h)
+
+    def int32_peak(self):
+        v = C.c_double()
+        if lib().cz_int32_peak(self._h, C.byref(v)):
+            raise RuntimeError("int32 probe failed")
+        return v.value
 
     def search(self, spec, depth=-1, dedupe=True, sym=True, store64=False, profile=False, on_level=None):
         """run `cheese SPEC [--depth D] [--no-dedupe] [--no-sym]`; returns a SearchOutcome"""

@@ -138,6 +138,9 @@ int cz_search(cz_engine *engine, const cz_spec *spec, const cz_options *opt, cz_
   out->expand_ms = r.expand_ms;
   out->dedupe_ms = r.dedupe_ms;
   out->total_ms = r.total_ms;
+  out->expand_launches = r.expand_launches;
+  out->h2d_bytes = r.h2d_bytes;
+  out->d2h_bytes = r.d2h_bytes;
   put_err(out->error, sizeof out->error, r.error);
   return rc;
 }
@@ -157,6 +160,18 @@ int cz_search_text(cz_engine *engine, const char *spec_text, size_t len, const c
   const int rc = cz_search(engine, s, opt, on_level, user, out);
   cz_spec_free(s);
   return rc;
+}
+
+void *cz_engine_stream(cz_engine *engine) { return engine ? engine->e->stream() : nullptr; }
+
+int cz_int32_peak(cz_engine *engine, double *ops_per_s) {
+  if (!engine || !ops_per_s) return CZ_ERR_USAGE;
+  try {
+    *ops_per_s = engine->e->int32_peak();
+    return 0;
+  } catch (const std::exception &) {
+    return CZ_ERR_CUDA;
+  }
 }
 
 const char *cz_version(void) { return "cheese_b200 0.1 (sm_100a)"; }

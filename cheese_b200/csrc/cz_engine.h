@@ -37,6 +37,8 @@ struct SearchResult {
   long long launches = 0;              // kernels launched by the engine
   long long t_evals = 0, children = 0; // T-bound evaluations, children evaluated past the window rules
   double expand_ms = 0, dedupe_ms = 0, total_ms = 0;   // device times (profile) / host wall time
+  long long expand_launches = 0;       // level-kernel launches (the denominator of per-launch figures)
+  long long h2d_bytes = 0, d2h_bytes = 0;   // host<->device traffic of the call
   std::string error;
 };
 
@@ -50,6 +52,9 @@ class Engine {
   int search(const HostSpec &hs, const Options &opt, const std::function<void(const LevelStats &)> &on_level,
              SearchResult &res);
   void *stream() const;
+  // sustained int32 multiply-add throughput of this device (ops/s, a multiply-add counted as 2), measured by a
+  // register-resident IMAD loop timed with CUDA events
+  double int32_peak();
   int device() const { return dev_; }
 
  private:

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cctype>
 #include <cstdlib>
+#include <atomic>
 #include <cstring>
 
 namespace cz {
@@ -88,7 +89,9 @@ bool is_clifford(const std::array<Zw, LMAX * LMAX> &A, int nq) {
 }  // namespace
 
 int parse_spec(const char *text, size_t len, HostSpec &s, std::string &err) {
+  static std::atomic<uint64_t> next_uid{1};
   s = HostSpec{};
+  s.uid = next_uid++;
   Reader in{text, text + len};
   std::string tok;
   bool have_start = false, have_goal_rows = false, have_ginfo = false;

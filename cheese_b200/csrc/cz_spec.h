@@ -11,6 +11,7 @@
 namespace cz {
 
 struct HostSpec {
+  uint64_t uid = 0;                                 // unique per parse: device copies are cached by it
   int n = 0, depth = 0, standard = 0, lite = 0, tdiv = 1, G = 0, tk = 0;
   int states = 0, m = 0, gk = 0;
   std::vector<std::string> names;

@@ -79,6 +79,8 @@ typedef struct {
   int64_t children;            /* children evaluated past the window rules */
   double expand_ms, dedupe_ms; /* device time per phase (profile = 1) */
   double total_ms;             /* host wall time of the call */
+  int64_t expand_launches;     /* launches of the level kernel */
+  int64_t h2d_bytes, d2h_bytes;/* host<->device bytes moved by the call */
   char error[256];
 } cz_result;
 
@@ -90,6 +92,14 @@ int cz_search(cz_engine *engine, const cz_spec *spec, const cz_options *opt, cz_
 /* Convenience for FFI callers that hold the spec as text: parse + search in one call. */
 int cz_search_text(cz_engine *engine, const char *spec_text, size_t len, const cz_options *opt, cz_level_fn on_level,
                    void *user, cz_result *out);
+
+/* The CUDA stream (cudaStream_t) the engine launches on, for callers that order their own work or timing
+ * events after the engine's kernels. */
+void *cz_engine_stream(cz_engine *engine);
+
+/* Sustained int32 multiply-add throughput of the engine's device in ops/s (a multiply-add counts as 2): a
+ * register-resident IMAD loop timed with CUDA events. The denominator of the level kernel's roofline. */
+int cz_int32_peak(cz_engine *engine, double *ops_per_s);
 
 /* The library version string and the CUDA architecture it was compiled for ("sm_100a"). */
 const char *cz_version(void);
