@@ -53,6 +53,8 @@ SIGNATURES = {
     "cz_search": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Options), LEVEL_FN, C.c_void_p, C.POINTER(Result)]),
     "cz_search_text": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(Options), LEVEL_FN, C.c_void_p,
                                  C.POINTER(Result)]),
+    "cz_eval_bounds": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int),
+                                 C.POINTER(C.c_int)]),
     "cz_engine_stream": (C.c_void_p, [C.c_void_p]),
     "cz_int32_peak": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "cz_version": (C.c_char_p, []),
@@ -133,6 +135,20 @@ class Engine:
         if lib().cz_int32_peak(self._h, C.byref(v)):
             raise RuntimeError("int32 probe failed")
         return v.value
+
+    def eval_bounds(self, spec, residuals):
+        """[(k, rows)] -> [(T bound, CX bound, H structure, support)] computed on the device"""
+        if not isinstance(spec, Spec):
+            spec = Spec(spec)
+        n = len(residuals)
+        flat = [v for _, M in residuals for row in M for x in row for v in x]
+        ent = (C.c_int64 * len(flat))(*flat)
+        ks = (C.c_int * n)(*[k for k, _ in residuals])
+        out = (C.c_int * (4 * n))()
+        rc = lib().cz_eval_bounds(self._h, spec._h, n, ent, ks, out)
+        if rc:
+            raise RuntimeError(f"cz_eval_bounds failed: {rc}")
+        return [tuple(out[4 * i:4 * i + 4]) for i in range(n)]
 
     def search(self, spec, depth=-1, dedupe=True, sym=True, store64=False, profile=False, on_level=None):
         """run `cheese SPEC [--depth D] [--no-dedupe] [--no-sym]`; returns a SearchOutcome"""

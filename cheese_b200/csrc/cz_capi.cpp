@@ -162,6 +162,18 @@ int cz_search_text(cz_engine *engine, const char *spec_text, size_t len, const c
   return rc;
 }
 
+int cz_eval_bounds(cz_engine *engine, const cz_spec *spec, int count, const int64_t *entries, const int *k,
+                   int *bounds) {
+  if (!engine || !spec || count < 0 || (count && (!entries || !k || !bounds))) return CZ_ERR_USAGE;
+  if (!count) return 0;
+  std::string err;
+  try {
+    return engine->e->eval_bounds(spec->hs, count, entries, k, bounds, err);
+  } catch (const std::exception &) {
+    return CZ_ERR_CUDA;
+  }
+}
+
 void *cz_engine_stream(cz_engine *engine) { return engine ? engine->e->stream() : nullptr; }
 
 int cz_int32_peak(cz_engine *engine, double *ops_per_s) {

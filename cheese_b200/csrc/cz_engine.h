@@ -52,6 +52,9 @@ class Engine {
   int search(const HostSpec &hs, const Options &opt, const std::function<void(const LevelStats &)> &on_level,
              SearchResult &res);
   void *stream() const;
+  // bounds of `count` caller-given residuals (entries count x N^2 x (a, b, c, d), exponents k): per residual
+  // (T bound, CX bound, H structure, support) into out4
+  int eval_bounds(const HostSpec &hs, int count, const int64_t *entries, const int *k, int *out4, std::string &err);
   // sustained int32 multiply-add throughput of this device (ops/s, a multiply-add counted as 2), measured by a
   // register-resident IMAD loop timed with CUDA events
   double int32_peak();

@@ -109,6 +109,12 @@ __device__ __forceinline__ uint64_t tomodp(int64_t v) {
   return (uint64_t)(m < 0 ? m + (int64_t)PRIME : m);
 }
 template <typename ST> __device__ __forceinline__ uint32_t zmodp(const Z4<ST> &x, const DevSpec &sp) {
+  if (sizeof(ST) == 4) {   // |limb| <= 2^31, w^i < 2^30: the whole sum fits in int64, one reduction
+    const int64_t t = (int64_t)x.a + (int64_t)x.b * (int64_t)sp.w1 + (int64_t)x.c * (int64_t)sp.w2 +
+                      (int64_t)x.d * (int64_t)sp.w3;
+    int64_t m = t % (int64_t)PRIME;
+    return (uint32_t)(m < 0 ? m + (int64_t)PRIME : m);
+  }
   const uint64_t r = tomodp(x.a) + tomodp(x.b) * sp.w1 % PRIME + tomodp(x.c) * sp.w2 % PRIME + tomodp(x.d) * sp.w3 % PRIME;
   return (uint32_t)(r % PRIME);
 }
@@ -159,8 +165,111 @@ template <int NQ, typename U, typename ST> __device__ int warp_ptm(const Z4<ST> 
   const int top = 2 * (NQ + k);
   return top - v > 0 ? top - v : 0;
 }
+// The same bound for 3 qubits with the conjugate pairing of the products: for f = (fa, fb) != 0,
+// Q[e ^ f] = conj(Q[e]), so with j the lowest set bit of f and H = {e : e_j = 0} (32 points),
+//   X(z) = sum_{e in H} (-1)^{e.z} (Q[e] + (-1)^{f.z} conj(Q[e])),
+// i.e. half of the outputs are the 32-point transform of Q + conj Q = (2a, b - d, 0, d - b) and the other half that
+// of Q - conj Q = (0, b + d, 2c, b + d): four real 32-point transforms of (a, c, b - d, b + d) instead of a 64-point
+// transform over Z[w]. For f = 0, Q = |S[e]|^2 = (alpha, beta, 0, -beta). Valuations need only two OR words per
+// class: with m = ctz(OR of all coefficients), the sqrt2-parity bit is bit m of OR(a ^ c | b ^ d), which is bit m
+// of 2A | 2C | A0 (b - d and its negative agree at bit m).
+// Layout: 8 pairs per warp iteration, 4 lanes per pair, 8 products per lane (3 butterfly stages in registers, 2
+// across the 4 lanes as shuffle + multiply-add); pairs are ordered by j so the f-independent operand S[e] is a
+// 4-address broadcast in 7 of the 8 iterations.
+__device__ __forceinline__ int pair_of(int idx) {   // the 63 nonzero f ordered by lowest set bit; 64th: none
+  if (idx < 32) return 2 * idx + 1;
+  if (idx < 48) return 4 * (idx - 32) + 2;
+  if (idx < 56) return 8 * (idx - 48) + 4;
+  if (idx < 60) return 16 * (idx - 56) + 8;
+  if (idx < 62) return 32 * (idx - 60) + 16;
+  return idx == 62 ? 32 : 0;
+}
+template <typename ST> __device__ int warp_ptm3(const Z4<ST> *S, int k, int lane) {
+  using U = uint32_t;
+  U R1 = 0, R2 = 0, P = 0, Q = 0;
+  {   // f = 0: entries lane, lane + 32; bit 5 in registers, bits 0..4 across lanes
+    U al[2], be[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const Z4<U> y = toU<U>(S[lane + 32 * h]);
+      al[h] = y.a * y.a + y.b * y.b + y.c * y.c + y.d * y.d;
+      be[h] = y.a * y.b + y.b * y.c + y.c * y.d - y.d * y.a;
+    }
+    U a0 = al[0] + al[1], a1 = al[0] - al[1], b0 = be[0] + be[1], b1 = be[0] - be[1];
+#pragma unroll
+    for (int h = 1; h < 32; h <<= 1) {
+      const U sg = (lane & h) ? 0xffffffffu : 1u;
+      a0 = __shfl_xor_sync(FULL, a0, h) + sg * a0;
+      a1 = __shfl_xor_sync(FULL, a1, h) + sg * a1;
+      b0 = __shfl_xor_sync(FULL, b0, h) + sg * b0;
+      b1 = __shfl_xor_sync(FULL, b1, h) + sg * b1;
+    }
+    R1 = a0 | a1 | b0 | b1;
+    R2 = a0 | a1;
+  }
+  const int pg = lane >> 2, sub = lane & 3;
+#pragma unroll 1
+  for (int it = 0; it < 8; it++) {
+    const int f = pair_of(it * 8 + pg);
+    const int j = f ? __ffs(f) - 1 : 0;
+    const int lo = (1 << j) - 1;
+    U A[8], C[8], X[8], Y[8];     // transforms of a, c, b - d, b + d
+#pragma unroll
+    for (int kk = 0; kk < 8; kk++) {
+      const int i = sub * 8 + kk;
+      const int e = ((i & ~lo) << 1) | (i & lo);
+      if (f) {
+        const Z4<U> x = toU<U>(S[e ^ f]), y = toU<U>(S[e]);
+        const U m1 = y.b - y.d, m2 = y.a + y.c, m3 = y.b + y.d, m4 = y.a - y.c;
+        A[kk] = y.a * x.a + y.b * x.b + y.c * x.c + y.d * x.d;
+        C[kk] = y.a * x.c + y.b * x.d - y.c * x.a - y.d * x.b;
+        X[kk] = m1 * x.a + m2 * x.b + m3 * x.c - m4 * x.d;
+        Y[kk] = m4 * x.b + m1 * x.c + m2 * x.d - m3 * x.a;
+      } else {
+        A[kk] = C[kk] = X[kk] = Y[kk] = 0;
+      }
+    }
+#pragma unroll
+    for (int h = 1; h < 8; h <<= 1)
+#pragma unroll
+      for (int kk = 0; kk < 8; kk++)
+        if (!(kk & h)) {
+          U u, v;
+          u = A[kk]; v = A[kk | h]; A[kk] = u + v; A[kk | h] = u - v;
+          u = C[kk]; v = C[kk | h]; C[kk] = u + v; C[kk | h] = u - v;
+          u = X[kk]; v = X[kk | h]; X[kk] = u + v; X[kk | h] = u - v;
+          u = Y[kk]; v = Y[kk | h]; Y[kk] = u + v; Y[kk | h] = u - v;
+        }
+#pragma unroll
+    for (int h = 1; h < 4; h <<= 1) {
+      const U sg = (sub & h) ? 0xffffffffu : 1u;
+#pragma unroll
+      for (int kk = 0; kk < 8; kk++) {
+        A[kk] = __shfl_xor_sync(FULL, A[kk], h) + sg * A[kk];
+        C[kk] = __shfl_xor_sync(FULL, C[kk], h) + sg * C[kk];
+        X[kk] = __shfl_xor_sync(FULL, X[kk], h) + sg * X[kk];
+        Y[kk] = __shfl_xor_sync(FULL, Y[kk], h) + sg * Y[kk];
+      }
+    }
+#pragma unroll
+    for (int kk = 0; kk < 8; kk++) { P |= A[kk] | C[kk]; Q |= X[kk] | Y[kk]; }
+  }
+#pragma unroll
+  for (int m = 16; m; m >>= 1) {
+    P |= __shfl_xor_sync(FULL, P, m); Q |= __shfl_xor_sync(FULL, Q, m);
+    R1 |= __shfl_xor_sync(FULL, R1, m); R2 |= __shfl_xor_sync(FULL, R2, m);
+  }
+  const U O1 = (P << 1) | Q | R1, O2 = (P << 1) | R2;
+  if (!O1) return 0;
+  const int mv = __ffs((int)O1) - 1;
+  const int v = 2 * mv + (((O2 >> mv) & 1) ? 0 : 1);
+  const int top = 2 * (3 + k);
+  return top - v > 0 ? top - v : 0;
+}
 template <int NQ, typename ST> __device__ __forceinline__ int ptm_bound(const Z4<ST> *S, int k, int lane) {
-  return 2 * (NQ + k) <= 64 ? warp_ptm<NQ, uint32_t, ST>(S, k, lane) : warp_ptm<NQ, uint64_t, ST>(S, k, lane);
+  if (2 * (NQ + k) > 64) return warp_ptm<NQ, uint64_t, ST>(S, k, lane);
+  if (NQ == 3) return warp_ptm3<ST>(S, k, lane);
+  return warp_ptm<NQ, uint32_t, ST>(S, k, lane);
 }
 
 // rank over F_p of the operator-Schmidt matrix across cut A (cheese.cu:271-303): lane j owns column j, fraction-free
@@ -510,6 +619,25 @@ template <int NQ, typename ST> __global__ void k_root(const DevSpec sp, const Z4
   }
 }
 
+// bounds of caller-given residuals (one warp each): T bound, CX bound, H structure, support
+template <int NQ, typename ST>
+__global__ void __launch_bounds__(EXP_WARPS * 32) k_eval_bounds(const DevSpec sp, const Z4<ST> *R, const int *ks,
+                                                               int count, int4 *out) {
+  constexpr int E = (1 << NQ) * (1 << NQ);
+  __shared__ Z4<ST> S[EXP_WARPS][E];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int i = blockIdx.x * EXP_WARPS + w; i < count; i += gridDim.x * EXP_WARPS) {
+    for (int e = lane; e < E; e += 32) S[w][e] = R[(size_t)i * E + e];
+    __syncwarp();
+    const int T = ptm_bound<NQ, ST>(S[w], ks[i], lane);
+    const int c2 = sp.ncuts ? warp_cx_bound<NQ, ST>(S[w], sp, lane) : 0;
+    const int hs = warp_h_struct<NQ, ST>(S[w], lane);
+    const int su = warp_support<NQ, ST>(S[w], lane);
+    if (lane == 0) out[i] = make_int4(T, c2, hs, su);
+    __syncwarp();
+  }
+}
+
 // ---------------- dedupe ----------------
 __global__ void k_sort_init(const uint64_t *h1, size_t n, uint64_t *keys, uint32_t *vals) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -735,6 +863,9 @@ struct Engine::Impl {
 
   template <int NQ> int run(const HostSpec &hs, const Options &opt, const std::function<void(const LevelStats &)> &cb,
                             SearchResult &res);
+  template <int NQ> DevSpec prepare(const HostSpec &hs, const SymGroup &grp, int depth, bool nogoal);
+  template <int NQ, typename ST>
+  void eval_bounds(const HostSpec &hs, int count, const int64_t *ent, const int *ks, int *out4);
   template <int NQ, typename ST>
   int levels(const HostSpec &hs, const DevSpec &sp, const Options &opt, int depth, int &t_start,
              const std::function<void(const LevelStats &)> &cb, SearchResult &res);
@@ -884,29 +1015,14 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
 }
 
 template <int NQ>
-int Engine::Impl::run(const HostSpec &hs, const Options &opt, const std::function<void(const LevelStats &)> &cb,
-                      SearchResult &res) {
+DevSpec Engine::Impl::prepare(const HostSpec &hs, const SymGroup &grp, int depth, bool nogoal) {
   constexpr int N = 1 << NQ, E = N * N;
-  const int depth = opt.depth >= 0 ? opt.depth : hs.depth;
-  const SymGroup grp = sym_group(hs, opt.sym);
-  res.nsym = grp.nsym;
-  // depth 0: the target is the identity (cheese.cu:1794-1801)
-  {
-    bool done = hs.tk == 0;
-    for (int r = 0; r < N && done; r++)
-      for (int c = 0; c < N && done; c++) {
-        const Zw x = hs.target[r * N + c];
-        done = r == c ? (x.a == 1 && !x.b && !x.c && !x.d) : zzero(x);
-      }
-    if (done && !opt.nogoal) { res.depth0 = true; return RC_CIRCUIT; }
-  }
-  // device spec
   DevSpec sp;
   std::memset(&sp, 0, sizeof sp);
   sp.n = hs.n; sp.G = hs.G; sp.depth = depth; sp.standard = hs.standard; sp.lite = hs.lite;
   sp.tdiv = hs.tdiv < 1 ? 1 : hs.tdiv; sp.ncuts = (int)hs.cutmask.size(); sp.have_table = !hs.cxtable.empty();
   sp.ncx = (int)hs.cxtable.size();
-  sp.nsym = grp.nsym; sp.nogoal = opt.nogoal; sp.gk = 0;
+  sp.nsym = grp.nsym; sp.nogoal = nogoal; sp.gk = 0;
   for (int i = 0; i < sp.ncuts; i++) { sp.cutmask[i] = hs.cutmask[i]; sp.cutsize[i] = hs.cutsize[i]; sp.rad[i] = hs.rad[i]; }
   sp.w1 = powmod_h(3, (PRIME - 1) / 8); sp.w2 = sp.w1 * sp.w1 % PRIME; sp.w3 = sp.w2 * sp.w1 % PRIME;
   for (int s2 = 0; s2 < grp.nsym; s2++) {
@@ -952,6 +1068,28 @@ int Engine::Impl::run(const HostSpec &hs, const Options &opt, const std::functio
   sp.ginv = sd->ginv.as<int4>(); sp.bad2 = sd->bad2.as<uint8_t>(); sp.bad3 = sd->bad3.as<uint32_t>();
   sp.cxtable = sd->cxt.as<int>(); sp.goal = sd->goal.as<longlong2>();
 
+  return sp;
+}
+
+template <int NQ>
+int Engine::Impl::run(const HostSpec &hs, const Options &opt, const std::function<void(const LevelStats &)> &cb,
+                      SearchResult &res) {
+  constexpr int N = 1 << NQ, E = N * N;
+  const int depth = opt.depth >= 0 ? opt.depth : hs.depth;
+  const SymGroup grp = sym_group(hs, opt.sym);
+  res.nsym = grp.nsym;
+  // depth 0: the target is the identity (cheese.cu:1794-1801)
+  {
+    bool done = hs.tk == 0;
+    for (int r = 0; r < N && done; r++)
+      for (int c = 0; c < N && done; c++) {
+        const Zw x = hs.target[r * N + c];
+        done = r == c ? (x.a == 1 && !x.b && !x.c && !x.d) : zzero(x);
+      }
+    if (done && !opt.nogoal) { res.depth0 = true; return RC_CIRCUIT; }
+  }
+  DevSpec sp = prepare<NQ>(hs, grp, depth, opt.nogoal);
+
   // storage: int32 limbs unless the target itself needs more (then int64 from the start)
   bool wide = opt.store64 == 1;
   for (const Zw &z : hs.target) if (!fits32(z.a) || !fits32(z.b) || !fits32(z.c) || !fits32(z.d)) wide = true;
@@ -996,6 +1134,49 @@ int Engine::Impl::run(const HostSpec &hs, const Options &opt, const std::functio
   }
   res.store64 = wide;
   return rc;
+}
+
+template <int NQ, typename ST>
+void Engine::Impl::eval_bounds(const HostSpec &hs, int count, const int64_t *ent, const int *ks, int *out4) {
+  constexpr int E = (1 << NQ) * (1 << NQ);
+  const SymGroup grp = sym_group(hs, false);
+  const DevSpec sp = prepare<NQ>(hs, grp, hs.depth, false);
+  std::vector<Z4<ST>> r((size_t)count * E);
+  for (size_t i = 0; i < r.size(); i++)
+    r[i] = Z4<ST>{(ST)ent[4 * i], (ST)ent[4 * i + 1], (ST)ent[4 * i + 2], (ST)ent[4 * i + 3]};
+  DBuf dR, dK, dO;
+  dR.ensure(r.size() * sizeof(Z4<ST>)); dK.ensure((size_t)count * 4 + 4); dO.ensure((size_t)count * 16 + 16);
+  ck(cudaMemcpyAsync(dR.p, r.data(), r.size() * sizeof(Z4<ST>), cudaMemcpyHostToDevice, s), "h2d");
+  ck(cudaMemcpyAsync(dK.p, ks, (size_t)count * 4, cudaMemcpyHostToDevice, s), "h2d");
+  const int grid = std::max(1, std::min((count + EXP_WARPS - 1) / EXP_WARPS, nsm * 8));
+  k_eval_bounds<NQ, ST><<<grid, EXP_WARPS * 32, 0, s>>>(sp, dR.as<Z4<ST>>(), dK.as<int>(), count, dO.as<int4>());
+  launches++;
+  ck(cudaGetLastError(), "bounds kernel");
+  ck(cudaMemcpyAsync(out4, dO.p, (size_t)count * 16, cudaMemcpyDeviceToHost, s), "d2h");
+  ck(cudaStreamSynchronize(s), "bounds");
+  dR.release(); dK.release(); dO.release();
+}
+
+int Engine::eval_bounds(const HostSpec &hs, int count, const int64_t *ent, const int *ks, int *out4, std::string &err) {
+  try {
+    ck(cudaSetDevice(dev_), "cudaSetDevice");
+    const size_t E = (size_t)1 << (2 * hs.n);
+    bool wide = false;
+    for (size_t i = 0; i < (size_t)count * E * 4; i++) if (!fits32(ent[i])) wide = true;
+    switch (hs.n * 2 + wide) {
+      case 2: impl_->eval_bounds<1, int32_t>(hs, count, ent, ks, out4); break;
+      case 3: impl_->eval_bounds<1, int64_t>(hs, count, ent, ks, out4); break;
+      case 4: impl_->eval_bounds<2, int32_t>(hs, count, ent, ks, out4); break;
+      case 5: impl_->eval_bounds<2, int64_t>(hs, count, ent, ks, out4); break;
+      case 6: impl_->eval_bounds<3, int32_t>(hs, count, ent, ks, out4); break;
+      case 7: impl_->eval_bounds<3, int64_t>(hs, count, ent, ks, out4); break;
+      default: err = "n not built"; return RC_USAGE;
+    }
+  } catch (const CudaError &e) {
+    err = e.what();
+    return RC_CUDA;
+  }
+  return 0;
 }
 
 Engine::Engine(int device) : impl_(new Impl(device)), dev_(device) {}
