@@ -54,6 +54,12 @@ CZ_HD Zw zwpow(int p) {
 CZ_HD bool fits32(int64_t v) { return v >= INT32_MIN && v <= INT32_MAX; }
 
 // per-gate property bits (derived exactly from the local matrices on the host)
-enum GateFlag : uint8_t { GF_CLIFFORD = 1, GF_ONEQ = 2 };
+//  GF_CLIFFORD: maps Paulis to Paulis (the T bound of S g^-1 equals that of S)
+//  GF_ONEQ:     acts on one qubit (the CX bound of S g^-1 equals that of S)
+//  GF_MONAFF:   monomial with an affine permutation (the H-structure bound of S g^-1 equals that of S)
+//  GF_TDIAG:    one-qubit diagonal with an odd w-power ratio (all such gates on a qubit give the same T bound:
+//               they differ by a power of S, a Clifford)
+//  GF_RANK2:    two-qubit gate of operator-Schmidt rank <= 2 over F_p (cx, cz: the CX bound moves by at most 1)
+enum GateFlag : uint8_t { GF_CLIFFORD = 1, GF_ONEQ = 2, GF_MONAFF = 4, GF_TDIAG = 8, GF_RANK2 = 16 };
 
 }  // namespace cz

@@ -38,7 +38,8 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int EXP_WARPS = 8;       // warps per expand block
-constexpr int INHERIT_KMAX = 60;   // the T bound is computed exactly (mod 2^32 / 2^64) only while 2(n + k) <= 128
+constexpr int INHERIT_KMAX = 60;
+enum GateKind : uint8_t { GK_GENERAL = 0, GK_ONEQ = 1, GK_PERM = 2 };   // the T bound is computed exactly (mod 2^32 / 2^64) only while 2(n + k) <= 128
 
 // ---------------- device-side spec ----------------
 struct DevSpec {
@@ -48,6 +49,11 @@ struct DevSpec {
   uint8_t symperm[SYMMAX][8];
   uint8_t symconj[SYMMAX];
   uint8_t gflags[GMAX];
+  uint8_t gmask[GMAX];                 // qubits a gate acts on
+  uint8_t gkind[GMAX];                 // GK_*: how the child update multiplies by the gate
+  uint8_t gph[GMAX][4];                // one-qubit unit gates: w-power of ginv[m][lc] at [2 m + lc] (8: zero)
+  uint8_t gperm[GMAX][8];              // permutation gates: local column lc takes local row gperm[lc]
+  int goal_id;                         // the goal is the identity with exponent 0 (unitary targets)
   int8_t gnq[GMAX], gik[GMAX];
   int8_t gq[GMAX][3];
   const uint8_t *bad2;
@@ -57,7 +63,9 @@ struct DevSpec {
   const longlong2 *goal;               // N*N entries as (a, b), (c, d) pairs
 };
 
-struct NodeMeta { int16_t k; uint8_t T, c2, g1, g2, pad0, pad1; };   // g = 0xff: no gate
+// per frontier node: exponent, bounds carried to the children, last two gates (0xff: none), H structure (bit 0:
+// hs = 2) with the mask of qubits acted on non-trivially (bits 1..3), per-cut CX needs (2 bits per cut)
+struct NodeMeta { int16_t k; uint8_t T, c2, g1, g2, hsn, needs; };
 
 struct DevStats {
   unsigned long long w2, w3, dead, alive, found, first_found, n_surv, t_evals, children, work;
@@ -313,56 +321,31 @@ template <int NQ, typename ST> __device__ int warp_cut_rank(const Z4<ST> *S, int
   return rank;
 }
 
-template <int NQ, typename ST> __device__ int warp_cx_bound(const Z4<ST> *S, const DevSpec &sp, int lane) {
-  int idx = 0, mult = 1, mx = 0;
+// CX bound from the per-cut needs ceil(log2 rank) (cheese.cu:585-597). Cuts a gate does not cross keep their
+// parent's need (a gate inside one side is a local map); needs_in = the parent's packed needs, gmask = the gate's
+// qubits (0: recompute every cut). Returns the bound, packs the child's needs into needs_out.
+template <int NQ, typename ST>
+__device__ int warp_cx_bound(const Z4<ST> *S, const DevSpec &sp, int lane, int gmask, int needs_in, int &needs_out) {
+  constexpr int ALLQ = (1 << NQ) - 1;
+  int idx = 0, mult = 1, mx = 0, packed = 0;
+  const bool inherit = sp.ncuts <= 4 && gmask;
   for (int i = 0; i < sp.ncuts; i++) {
-    const int rk = warp_cut_rank<NQ, ST>(S, sp.cutmask[i], sp.cutsize[i], sp, lane);
-    int need = 0;
-    while ((1 << need) < rk) need++;
-    if (need > sp.rad[i] - 1) need = sp.rad[i] - 1;
+    const int A = sp.cutmask[i];
+    int need;
+    if (inherit && (!(gmask & A) || !(gmask & ~A & ALLQ))) need = (needs_in >> (2 * i)) & 3;
+    else {
+      const int rk = warp_cut_rank<NQ, ST>(S, A, sp.cutsize[i], sp, lane);
+      need = 0;
+      while ((1 << need) < rk) need++;
+      if (need > sp.rad[i] - 1) need = sp.rad[i] - 1;
+    }
+    if (i < 4) packed |= (need & 3) << (2 * i);
     idx += need * mult;
     mult *= sp.rad[i];
     if (need > mx) mx = need;
   }
+  needs_out = packed;
   return sp.have_table && idx < sp.ncx ? __ldg(&sp.cxtable[idx]) : mx;
-}
-
-// 2 when S is monomial with a non-affine permutation, else 0 (cheese.cu:322-338); lane c scans column c
-template <int NQ, typename ST> __device__ int warp_h_struct(const Z4<ST> *S, int lane) {
-  constexpr int N = 1 << NQ;
-  int nz = 0, row = 0;
-  if (lane < N)
-    for (int r = 0; r < N; r++) if (!zz(S[r * N + lane])) { nz++; row = r; }
-  if (__any_sync(FULL, lane < N && nz != 1)) return 0;
-  const int c0 = __shfl_sync(FULL, row, 0);
-  int x = c0;
-#pragma unroll
-  for (int i = 0; i < NQ; i++) {
-    const int pb = __shfl_sync(FULL, row, 1 << i);
-    if ((lane >> i) & 1) x ^= pb ^ c0;
-  }
-  return __any_sync(FULL, lane < N && row != x) ? 2 : 0;
-}
-
-// number of qubits S acts on non-trivially (cheese.cu:305-319)
-template <int NQ, typename ST> __device__ int warp_support(const Z4<ST> *S, int lane) {
-  constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
-  int cnt = 0;
-#pragma unroll
-  for (int q = 0; q < NQ; q++) {
-    const int bit = 1 << q;
-    bool nt = false;
-#pragma unroll
-    for (int j = 0; j < EPL; j++) {
-      const int e = lane + 32 * j;
-      if (e >= E) continue;
-      const int r = e >> NQ, c = e & (N - 1);
-      if ((r ^ c) & bit) { if (!zz(S[e])) nt = true; }
-      else if (!((r | c) & bit) && !zq(S[e], S[(r | bit) * N + (c | bit)])) nt = true;
-    }
-    cnt += __any_sync(FULL, nt);
-  }
-  return cnt;
 }
 
 __device__ __forceinline__ int combine(int h, int t, int c2, int supp) {   // cheese.cu:599-607
@@ -375,56 +358,173 @@ __device__ __forceinline__ int combine(int h, int t, int c2, int supp) {   // ch
   return best;
 }
 
-// child residual C = P g^-1, normalised; returns its exponent, sets ovf when a limb leaves the storage type
+// x times w^p (p < 8): a signed rotation of the coefficients
+template <typename ST> __device__ __forceinline__ Zw mul_unit(const Z4<ST> &x, int p) {
+  Zw r;
+  switch (p & 3) {
+    case 0: r = Zw{x.a, x.b, x.c, x.d}; break;
+    case 1: r = Zw{-(int64_t)x.d, x.a, x.b, x.c}; break;
+    case 2: r = Zw{-(int64_t)x.c, -(int64_t)x.d, x.a, x.b}; break;
+    default: r = Zw{-(int64_t)x.b, -(int64_t)x.c, -(int64_t)x.d, x.a};
+  }
+  if (p & 4) r = Zw{-r.a, -r.b, -r.c, -r.d};
+  return r;
+}
+
+// child residual C = P g^-1, normalised; returns its exponent, sets ovf when a limb leaves the storage type.
+// One-qubit gates whose inverse has only zero / w-power entries (x z h s sdg t tdg) pair entries that differ in
+// the gate's column bit, so each lane owns both inputs of its two outputs and the product is a rotation;
+// permutation gates (cx, ccx) copy; anything else multiplies out over Z[w].
 template <int NQ, typename ST>
 __device__ int warp_child(const Z4<ST> *P, Z4<ST> *C, int g, int kp, const DevSpec &sp, int lane, bool &ovf) {
-  constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
-  const int nq = sp.gnq[g], L = 1 << nq;
-  const int q0 = sp.gq[g][0], q1 = nq > 1 ? sp.gq[g][1] : 0, q2 = nq > 2 ? sp.gq[g][2] : 0;
-  const int mask = (1 << q0) | (nq > 1 ? 1 << q1 : 0) | (nq > 2 ? 1 << q2 : 0);
-  const int4 *gi = sp.ginv + g * 64;
-  Zw acc[EPL];
+  constexpr int N = 1 << NQ, E = N * N;
+  Zw v[2] = {Zw{0, 0, 0, 0}, Zw{0, 0, 0, 0}};
+  int ei[2] = {-1, -1};
+  const int kind = sp.gkind[g];
+  if (kind == GK_ONEQ) {
+    const int q = sp.gq[g][0], lo = (1 << q) - 1;
+    if (lane < E / 2) {
+      ei[0] = ((lane & ~lo) << 1) | (lane & lo);
+      ei[1] = ei[0] | (1 << q);
+      const Z4<ST> x0 = P[ei[0]], x1 = P[ei[1]];
+      const int p00 = sp.gph[g][0], p01 = sp.gph[g][1], p10 = sp.gph[g][2], p11 = sp.gph[g][3];
+      if (p00 < 8) v[0] = zadd(v[0], mul_unit(x0, p00));
+      if (p10 < 8) v[0] = zadd(v[0], mul_unit(x1, p10));
+      if (p01 < 8) v[1] = zadd(v[1], mul_unit(x0, p01));
+      if (p11 < 8) v[1] = zadd(v[1], mul_unit(x1, p11));
+    }
+  } else {
+    const int nq = sp.gnq[g], L = 1 << nq;
+    const int q0 = sp.gq[g][0], q1 = nq > 1 ? sp.gq[g][1] : 0, q2 = nq > 2 ? sp.gq[g][2] : 0;
+    const int mask = (1 << q0) | (nq > 1 ? 1 << q1 : 0) | (nq > 2 ? 1 << q2 : 0);
 #pragma unroll
-  for (int j = 0; j < EPL; j++) {
-    const int e = lane + 32 * j;
-    acc[j] = Zw{0, 0, 0, 0};
-    if (e >= E) continue;
-    const int r = e >> NQ, col = e & (N - 1), base = col & ~mask;
-    int lc = (col >> q0) & 1;
-    if (nq > 1) lc |= ((col >> q1) & 1) << 1;
-    if (nq > 2) lc |= ((col >> q2) & 1) << 2;
-    for (int m = 0; m < L; m++) {
-      const int4 gm = __ldg(&gi[m * L + lc]);
-      if (!(gm.x | gm.y | gm.z | gm.w)) continue;
-      int x = base | ((m & 1) << q0);
-      if (nq > 1) x |= ((m >> 1) & 1) << q1;
-      if (nq > 2) x |= ((m >> 2) & 1) << q2;
-      const Z4<ST> s = P[r * N + x];
-      acc[j] = zadd(acc[j], zmul(Zw{(int64_t)s.a, (int64_t)s.b, (int64_t)s.c, (int64_t)s.d},
-                                 Zw{(int64_t)gm.x, (int64_t)gm.y, (int64_t)gm.z, (int64_t)gm.w}));
+    for (int j = 0; j < 2; j++) {
+      const int e = lane + 32 * j;
+      if (e >= E) continue;
+      ei[j] = e;
+      const int r = e >> NQ, col = e & (N - 1), base = col & ~mask;
+      int lc = (col >> q0) & 1;
+      if (nq > 1) lc |= ((col >> q1) & 1) << 1;
+      if (nq > 2) lc |= ((col >> q2) & 1) << 2;
+      if (kind == GK_PERM) {
+        const int m = sp.gperm[g][lc];
+        int x = base | ((m & 1) << q0);
+        if (nq > 1) x |= ((m >> 1) & 1) << q1;
+        if (nq > 2) x |= ((m >> 2) & 1) << q2;
+        const Z4<ST> sv = P[r * N + x];
+        v[j] = Zw{sv.a, sv.b, sv.c, sv.d};
+        continue;
+      }
+      const int4 *gi = sp.ginv + g * 64;
+      for (int m = 0; m < L; m++) {
+        const int4 gm = __ldg(&gi[m * L + lc]);
+        if (!(gm.x | gm.y | gm.z | gm.w)) continue;
+        int x = base | ((m & 1) << q0);
+        if (nq > 1) x |= ((m >> 1) & 1) << q1;
+        if (nq > 2) x |= ((m >> 2) & 1) << q2;
+        const Z4<ST> sv = P[r * N + x];
+        v[j] = zadd(v[j], zmul(Zw{(int64_t)sv.a, (int64_t)sv.b, (int64_t)sv.c, (int64_t)sv.d},
+                               Zw{(int64_t)gm.x, (int64_t)gm.y, (int64_t)gm.z, (int64_t)gm.w}));
+      }
     }
   }
   int k = kp + sp.gik[g];
   while (k > 0) {                              // normalise: lower k while every entry is divisible by sqrt2
-    bool ok = true;
-#pragma unroll
-    for (int j = 0; j < EPL; j++) if (lane + 32 * j < E && !zdiv2ok(acc[j])) ok = false;
+    const bool ok = (ei[0] < 0 || zdiv2ok(v[0])) && (ei[1] < 0 || zdiv2ok(v[1]));
     if (!__all_sync(FULL, ok)) break;
-#pragma unroll
-    for (int j = 0; j < EPL; j++) acc[j] = zdown(acc[j]);
+    v[0] = zdown(v[0]);
+    v[1] = zdown(v[1]);
     k--;
   }
   bool of = false;
 #pragma unroll
-  for (int j = 0; j < EPL; j++) {
-    const int e = lane + 32 * j;
-    if (e >= E) continue;
-    if (sizeof(ST) == 4 && !(fits32(acc[j].a) && fits32(acc[j].b) && fits32(acc[j].c) && fits32(acc[j].d))) of = true;
-    C[e] = Z4<ST>{(ST)acc[j].a, (ST)acc[j].b, (ST)acc[j].c, (ST)acc[j].d};
+  for (int j = 0; j < 2; j++) {
+    if (ei[j] < 0) continue;
+    if (sizeof(ST) == 4 && !(fits32(v[j].a) && fits32(v[j].b) && fits32(v[j].c) && fits32(v[j].d))) of = true;
+    C[ei[j]] = Z4<ST>{(ST)v[j].a, (ST)v[j].b, (ST)v[j].c, (ST)v[j].d};
   }
   ovf = __any_sync(FULL, of);
   __syncwarp();
   return k;
+}
+
+template <int NQ, typename ST> __device__ bool warp_goal(const Z4<ST> *S, int k, const DevSpec &sp, int lane);
+
+// goal test, H structure (2 when S is monomial with a non-affine permutation, cheese.cu:322-338) and the mask of
+// qubits S acts on non-trivially (support = its popcount, cheese.cu:305-319) in one pass: each lane reads entries
+// lane and lane + 32; the nonzero pattern becomes a 64-bit mask by ballot for the monomial / affine test. Only the
+// qubits in test_q are examined for triviality; the others keep the bits of ntriv_in.
+struct Cheap { bool goal; int hs, ntriv; };
+template <int NQ, typename ST>
+__device__ Cheap warp_cheap(const Z4<ST> *S, int k, const DevSpec &sp, int lane, bool maybe_goal, bool need_hs,
+                            int test_q, int ntriv_in) {
+  constexpr int N = 1 << NQ, E = N * N;
+  Z4<ST> x[2];
+  bool val[2];
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    const int e = lane + 32 * j;
+    val[j] = e < E;
+    x[j] = val[j] ? S[e] : Z4<ST>{0, 0, 0, 0};
+  }
+  Cheap out{false, 0, ntriv_in & ~test_q};
+  if (maybe_goal) {
+    if (sp.goal_id) {
+      bool ok = k == 0;
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        if (!val[j]) continue;
+        const int e = lane + 32 * j, r = e >> NQ, c = e & (N - 1);
+        if (r == c ? !(x[j].a == 1 && !x[j].b && !x[j].c && !x[j].d) : !zz(x[j])) ok = false;
+      }
+      out.goal = __all_sync(FULL, ok);
+    } else {
+      out.goal = warp_goal<NQ, ST>(S, k, sp, lane);
+    }
+    if (out.goal) return out;
+  }
+  if (need_hs) {
+    const unsigned b0 = __ballot_sync(FULL, val[0] && !zz(x[0])), b1 = __ballot_sync(FULL, val[1] && !zz(x[1]));
+    const uint64_t M = (uint64_t)b0 | ((uint64_t)b1 << 32);
+    if (__popcll(M) == N) {                      // monomial iff every column has exactly one nonzero
+      int pi[N];
+      bool mono = true;
+#pragma unroll
+      for (int c = 0; c < N; c++) {
+        uint64_t colm = 0;
+#pragma unroll
+        for (int r = 0; r < N; r++) colm |= ((M >> (r * N + c)) & 1ULL) << r;
+        mono = mono && __popcll(colm) == 1;
+        pi[c] = __ffsll((long long)colm) - 1;
+      }
+      if (mono) {
+        bool aff = true;
+#pragma unroll
+        for (int j = 0; j < N; j++) {
+          int xx = pi[0];
+#pragma unroll
+          for (int i = 0; i < NQ; i++) if ((j >> i) & 1) xx ^= pi[1 << i] ^ pi[0];
+          if (pi[j] != xx) aff = false;
+        }
+        out.hs = aff ? 0 : 2;
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < NQ; q++) {
+    if (!((test_q >> q) & 1)) continue;
+    const int bit = 1 << q;
+    bool nt = false;
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      if (!val[j]) continue;
+      const int e = lane + 32 * j, r = e >> NQ, c = e & (N - 1);
+      if ((r ^ c) & bit) { if (!zz(x[j])) nt = true; }
+      else if (!((r | c) & bit) && !zq(x[j], S[(r | bit) * N + (c | bit)])) nt = true;
+    }
+    if (__any_sync(FULL, nt)) out.ntriv |= bit;
+  }
+  return out;
 }
 
 template <int NQ, typename ST> __device__ bool warp_goal(const Z4<ST> *S, int k, const DevSpec &sp, int lane) {
@@ -526,6 +626,10 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, 
     const NodeMeta pm = a.meta[p];
     __syncwarp();
     const int g1 = pm.g1 == 0xff ? -1 : pm.g1, g2 = pm.g2 == 0xff ? -1 : pm.g2;
+    const int kP = pm.k, TP = pm.T, c2P = pm.c2, hsP = (pm.hsn & 1) ? 2 : 0, ntP = (pm.hsn >> 1) & 7;
+    const int suppP = __popc(ntP);
+    const bool pre_ok = sp.standard && kP < INHERIT_KMAX;
+    unsigned tcache = 0;                       // per qubit: 1 + T bound of its odd-diagonal child (0: unknown)
     for (int g = 0; g < G; g++) {
       if (g1 >= 0 && __ldg(&sp.bad2[g1 * G + g])) { n_w2++; continue; }
       if (g2 >= 0) {
@@ -533,32 +637,68 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, 
         if ((__ldg(&sp.bad3[tri >> 5]) >> (tri & 31)) & 1) { n_w3++; continue; }
       }
       n_child++;
+      const int rem = a.rem;
+      const uint8_t fl = sp.gflags[g];
+      const int gm = sp.gmask[g], nq = sp.gnq[g], q0 = sp.gq[g][0];
+      const int tc = (int)((tcache >> (8 * q0)) & 0xff) - 1;
+      if (pre_ok) {
+        // lower bounds on the child's bounds from the parent's: k drops by at most the gate's sqrt2 exponent;
+        // H structure, T and CX bounds are unchanged by monomial-affine / Clifford / one-qubit gates; an odd
+        // diagonal changes T by at most 1; a gate of Schmidt rank 2 changes the CX bound by at most 1; support
+        // changes only on the gate's qubits. combine is monotone in every argument, so exceeding the budget with
+        // these proves the child dead (the goal has all bounds 0 and is never removed here).
+        const int ik = sp.gik[g] > 0 ? sp.gik[g] : 0;
+        int hlo = kP - ik;
+        if ((fl & GF_MONAFF) && hsP > hlo) hlo = hsP;
+        const int tlo = (fl & GF_CLIFFORD) ? TP : ((fl & GF_TDIAG) ? (tc >= 0 ? tc : TP - 1) : 0);
+        const int clo = (fl & GF_ONEQ) ? c2P : ((fl & GF_RANK2) ? c2P - 1 : 0);
+        const int slo = suppP - nq;
+        if (combine(hlo > 0 ? hlo : 0, tlo > 0 ? tlo : 0, clo > 0 ? clo : 0, slo > 0 ? slo : 0) > rem) {
+          n_dead++;
+          continue;
+        }
+      }
       bool ovf;
-      const int k = warp_child<NQ, ST>(P, C, g, pm.k, sp, lane, ovf);
+      const int k = warp_child<NQ, ST>(P, C, g, kP, sp, lane, ovf);
       if (ovf) { ovf_any = true; continue; }
-      if (warp_goal<NQ, ST>(C, k, sp, lane)) {
+      const bool need_b = sp.standard != 0;
+      const bool need_hs = need_b && !(fl & GF_MONAFF);
+      // the child is the goal only if the parent equals the gate, i.e. acts on no other qubit
+      const Cheap ch = warp_cheap<NQ, ST>(C, k, sp, lane, (ntP & ~gm) == 0 || !need_b, need_hs, need_b ? gm : 0, ntP);
+      if (ch.goal) {
         if (sp.nogoal) n_dead++;
         else { n_found++; const unsigned long long o = p * (unsigned long long)G + g; if (o < first) first = o; }
         continue;
       }
-      const int rem = a.rem;
-      const uint8_t fl = sp.gflags[g];
-      const bool inheritT = (fl & GF_CLIFFORD) && k <= INHERIT_KMAX && pm.k <= INHERIT_KMAX;
+      const bool inheritT = (fl & GF_CLIFFORD) && k <= INHERIT_KMAX && kP <= INHERIT_KMAX;
+      const bool cacheT = (fl & GF_TDIAG) && k <= INHERIT_KMAX;
       bool alive = true;
-      int T = 0, c2 = 0;
+      int T = 0, c2 = 0, hs = 0, needs = 0;
       if (sp.lite) {
         if (k > rem) alive = false;
         else {
-          if (inheritT) T = pm.T; else { T = ptm_bound<NQ, ST>(C, k, lane); n_teval++; }
+          if (inheritT) T = TP;
+          else if (cacheT && tc >= 0) T = tc;
+          else {
+            T = ptm_bound<NQ, ST>(C, k, lane); n_teval++;
+            if (cacheT) tcache |= (unsigned)(T + 1) << (8 * q0);
+          }
           alive = k + (T + sp.tdiv - 1) / sp.tdiv <= rem;
         }
-      } else if (sp.standard) {
-        const int hs = warp_h_struct<NQ, ST>(C, lane), h = k > hs ? k : hs;
-        const int supp = warp_support<NQ, ST>(C, lane);
-        c2 = (fl & GF_ONEQ) ? pm.c2 : warp_cx_bound<NQ, ST>(C, sp, lane);
+      } else if (need_b) {
+        hs = need_hs ? ch.hs : hsP;
+        const int h = k > hs ? k : hs;
+        const int supp = __popc(ch.ntriv);
+        if (fl & GF_ONEQ) { c2 = c2P; needs = pm.needs; }
+        else c2 = warp_cx_bound<NQ, ST>(C, sp, lane, gm, pm.needs, needs);
         if (combine(h, 0, c2, supp) > rem) alive = false;
         else {
-          if (inheritT) T = pm.T; else { T = ptm_bound<NQ, ST>(C, k, lane); n_teval++; }
+          if (inheritT) T = TP;
+          else if (cacheT && tc >= 0) T = tc;
+          else {
+            T = ptm_bound<NQ, ST>(C, k, lane); n_teval++;
+            if (cacheT) tcache |= (unsigned)(T + 1) << (8 * q0);
+          }
           alive = combine(h, T, c2, supp) <= rem;
         }
       }
@@ -580,7 +720,8 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, 
           a.sh1[slot] = k1; a.sh2[slot] = k2; a.sidx[slot] = p * (unsigned long long)G + g;
           NodeMeta nm;
           nm.k = (int16_t)k; nm.T = (uint8_t)(T > 255 ? 255 : T); nm.c2 = (uint8_t)c2; nm.g1 = (uint8_t)g; nm.g2 = pm.g1;
-          nm.pad0 = nm.pad1 = 0;
+          nm.hsn = (uint8_t)((hs == 2 ? 1 : 0) | ((need_b ? ch.ntriv : 0) << 1));
+          nm.needs = (uint8_t)needs;
           a.smeta[slot] = nm;
         }
       } else if (lane == 0) {
@@ -602,19 +743,25 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, 
   }
 }
 
-// the root node's bounds (the target itself): T and CX bound for inheritance by its children
+// the root node's bounds (the target itself), inherited or bracketed by its children
 template <int NQ, typename ST> __global__ void k_root(const DevSpec sp, const Z4<ST> *R, NodeMeta *meta, int tk) {
   constexpr int E = (1 << NQ) * (1 << NQ);
   __shared__ Z4<ST> S[E];
   const int lane = threadIdx.x;
   for (int e = lane; e < E; e += 32) S[e] = R[e];
   __syncwarp();
-  int T = 0, c2 = 0;
+  int T = 0, c2 = 0, needs = 0;
+  Cheap ch{false, 0, 0};
   if (sp.standard || sp.lite) T = ptm_bound<NQ, ST>(S, tk, lane);
-  if (sp.standard) c2 = warp_cx_bound<NQ, ST>(S, sp, lane);
+  if (sp.standard) {
+    c2 = warp_cx_bound<NQ, ST>(S, sp, lane, 0, 0, needs);
+    ch = warp_cheap<NQ, ST>(S, tk, sp, lane, false, true, (1 << NQ) - 1, 0);
+  }
   if (lane == 0) {
     NodeMeta m;
-    m.k = (int16_t)tk; m.T = (uint8_t)(T > 255 ? 255 : T); m.c2 = (uint8_t)c2; m.g1 = m.g2 = 0xff; m.pad0 = m.pad1 = 0;
+    m.k = (int16_t)tk; m.T = (uint8_t)(T > 255 ? 255 : T); m.c2 = (uint8_t)c2; m.g1 = m.g2 = 0xff;
+    m.hsn = (uint8_t)((ch.hs == 2 ? 1 : 0) | (ch.ntriv << 1));
+    m.needs = (uint8_t)needs;
     *meta = m;
   }
 }
@@ -630,10 +777,10 @@ __global__ void __launch_bounds__(EXP_WARPS * 32) k_eval_bounds(const DevSpec sp
     for (int e = lane; e < E; e += 32) S[w][e] = R[(size_t)i * E + e];
     __syncwarp();
     const int T = ptm_bound<NQ, ST>(S[w], ks[i], lane);
-    const int c2 = sp.ncuts ? warp_cx_bound<NQ, ST>(S[w], sp, lane) : 0;
-    const int hs = warp_h_struct<NQ, ST>(S[w], lane);
-    const int su = warp_support<NQ, ST>(S[w], lane);
-    if (lane == 0) out[i] = make_int4(T, c2, hs, su);
+    int needs = 0;
+    const int c2 = sp.ncuts ? warp_cx_bound<NQ, ST>(S[w], sp, lane, 0, 0, needs) : 0;
+    const Cheap ch = warp_cheap<NQ, ST>(S[w], ks[i], sp, lane, true, true, (1 << NQ) - 1, 0);
+    if (lane == 0) out[i] = make_int4(T, c2, ch.goal ? -1 : ch.hs, ch.goal ? -1 : __popc(ch.ntriv));
     __syncwarp();
   }
 }
@@ -1029,9 +1176,45 @@ DevSpec Engine::Impl::prepare(const HostSpec &hs, const SymGroup &grp, int depth
     for (int x = 0; x < N; x++) sp.symperm[s2][x] = grp.bperm[s2 * N + x];
     sp.symconj[s2] = grp.conj[s2];
   }
+  sp.goal_id = 1;
   for (int g = 0; g < hs.G; g++) {
     sp.gflags[g] = hs.gflags[g]; sp.gnq[g] = (int8_t)hs.gnq[g]; sp.gik[g] = (int8_t)hs.gik[g];
+    sp.gmask[g] = 0;
+    for (int j = 0; j < hs.gnq[g]; j++) sp.gmask[g] |= (uint8_t)(1 << hs.gq[g][j]);
     for (int j = 0; j < 3; j++) sp.gq[g][j] = (int8_t)hs.gq[g][j];
+    // how the child update multiplies by this gate: w-power entries (one qubit), a permutation, or general
+    const int L = 1 << hs.gnq[g];
+    auto unit_power = [](const Zw &z) -> int {   // p with z = w^p, 8 for zero, -1 otherwise
+      if (zzero(z)) return 8;
+      const int64_t c[4] = {z.a, z.b, z.c, z.d};
+      int nz = -1;
+      for (int i = 0; i < 4; i++) if (c[i]) { if (nz >= 0) return -1; nz = i; }
+      if (c[nz] == 1) return nz;
+      if (c[nz] == -1) return nz + 4;
+      return -1;
+    };
+    sp.gkind[g] = GK_GENERAL;
+    if (L == 2) {
+      bool ok = true;
+      for (int i = 0; i < 4; i++) { const int pw = unit_power(hs.ginv[g][i]); ok = ok && pw >= 0; sp.gph[g][i] = (uint8_t)(pw < 0 ? 8 : pw); }
+      if (ok) sp.gkind[g] = GK_ONEQ;
+    }
+    if (sp.gkind[g] == GK_GENERAL) {
+      bool perm = true;
+      int rowuse = 0;
+      for (int lc = 0; lc < L && perm; lc++) {
+        int one = -1;
+        for (int m = 0; m < L && perm; m++) {
+          const Zw z = hs.ginv[g][m * L + lc];
+          if (zzero(z)) continue;
+          if (one >= 0 || !(z.a == 1 && !z.b && !z.c && !z.d)) perm = false;
+          one = m;
+        }
+        if (one < 0 || (rowuse >> one) & 1) perm = false;
+        else { rowuse |= 1 << one; sp.gperm[g][lc] = (uint8_t)one; }
+      }
+      if (perm) sp.gkind[g] = GK_PERM;
+    }
   }
   std::vector<int4> gi((size_t)GMAX * 64, int4{0, 0, 0, 0});
   for (int g = 0; g < hs.G; g++)

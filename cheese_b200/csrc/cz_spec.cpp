@@ -86,6 +86,63 @@ bool is_clifford(const std::array<Zw, LMAX * LMAX> &A, int nq) {
   return true;
 }
 
+// monomial (one nonzero per row and column) with a permutation that is affine over GF(2)
+bool is_monomial_affine(const std::array<Zw, LMAX * LMAX> &A, int nq) {
+  const int L = 1 << nq;
+  int pi[LMAX];
+  for (int c = 0; c < L; c++) {
+    int nz = 0;
+    for (int r = 0; r < L; r++) if (!zzero(A[r * L + c])) { nz++; pi[c] = r; }
+    if (nz != 1) return false;
+  }
+  for (int j = 0; j < L; j++) {
+    int x = pi[0];
+    for (int i = 0; i < nq; i++) if ((j >> i) & 1) x ^= pi[1 << i] ^ pi[0];
+    if (pi[j] != x) return false;
+  }
+  return true;
+}
+
+// w-power p of a unit z = w^p, -1 otherwise
+int unit_power(const Zw &z) {
+  const int64_t c[4] = {z.a, z.b, z.c, z.d};
+  int nz = -1;
+  for (int i = 0; i < 4; i++) if (c[i]) { if (nz >= 0) return -1; nz = i; }
+  if (nz < 0) return -1;
+  if (c[nz] == 1) return nz;
+  if (c[nz] == -1) return nz + 4;
+  return -1;
+}
+
+// rank over F_p (p = 998244353, w -> 3^((p-1)/8)) of a two-qubit gate reshaped across its two qubits
+int schmidt_rank_p(const std::array<Zw, LMAX * LMAX> &A) {
+  const uint64_t P = PRIME;
+  auto pw = [&](uint64_t b, uint64_t e) { uint64_t r = 1; b %= P; while (e) { if (e & 1) r = r * b % P; b = b * b % P; e >>= 1; } return r; };
+  const uint64_t w = pw(3, (P - 1) / 8), w2 = w * w % P, w3 = w2 * w % P;
+  auto md = [&](int64_t v) { int64_t m = v % (int64_t)P; return (uint64_t)(m < 0 ? m + (int64_t)P : m); };
+  uint64_t M[4][4];
+  for (int o = 0; o < 4; o++)
+    for (int i = 0; i < 4; i++) {
+      const Zw z = A[o * 4 + i];
+      M[((o & 1) << 1) | (i & 1)][(((o >> 1) & 1) << 1) | ((i >> 1) & 1)] =
+          (md(z.a) + md(z.b) * w % P + md(z.c) * w2 % P + md(z.d) * w3 % P) % P;
+    }
+  int rank = 0;
+  for (int c = 0; c < 4 && rank < 4; c++) {
+    int piv = -1;
+    for (int r = rank; r < 4; r++) if (M[r][c]) { piv = r; break; }
+    if (piv < 0) continue;
+    for (int j = 0; j < 4; j++) std::swap(M[piv][j], M[rank][j]);
+    const uint64_t inv = pw(M[rank][c], P - 2);
+    for (int r = rank + 1; r < 4; r++) {
+      const uint64_t f = M[r][c] * inv % P;
+      for (int j = 0; j < 4; j++) M[r][j] = (M[r][j] + P - f * M[rank][j] % P) % P;
+    }
+    rank++;
+  }
+  return rank;
+}
+
 }  // namespace
 
 int parse_spec(const char *text, size_t len, HostSpec &s, std::string &err) {
@@ -198,6 +255,12 @@ int parse_spec(const char *text, size_t len, HostSpec &s, std::string &err) {
     uint8_t f = 0;
     if (is_clifford(s.ginv[g], s.gnq[g])) f |= GF_CLIFFORD;
     if (s.gnq[g] == 1) f |= GF_ONEQ;
+    if (is_monomial_affine(s.ginv[g], s.gnq[g])) f |= GF_MONAFF;
+    if (s.gnq[g] == 1 && zzero(s.ginv[g][1]) && zzero(s.ginv[g][2])) {
+      const int p0 = unit_power(s.ginv[g][0]), p1 = unit_power(s.ginv[g][3]);
+      if (p0 >= 0 && p1 >= 0 && ((p1 - p0) & 1)) f |= GF_TDIAG;
+    }
+    if (s.gnq[g] == 2 && schmidt_rank_p(s.ginv[g]) <= 2) f |= GF_RANK2;
     s.gflags.push_back(f);
   }
   for (size_t i = 0; i < s.cutmask.size(); i++)

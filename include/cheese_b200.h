@@ -95,7 +95,8 @@ int cz_search_text(cz_engine *engine, const char *spec_text, size_t len, const c
 
 /* Lower bounds of `count` residual matrices under the spec's cuts and CX table, computed by the same device code
  * as the search: entries = count x N^2 x (a, b, c, d) limbs (value (a + b w + c w^2 + d w^3) / sqrt2^k), k = their
- * exponents; bounds = count x 4 ints (T bound = PTM sde, CX bound, H structure 0/2, support). These are the
+ * exponents; bounds = count x 4 ints (T bound = PTM sde, CX bound, H structure 0/2, support; the last two are -1
+ * when the residual is the identity, where the search stops before the bounds). These are the
  * reference's ptm_wht, cx_bound, h_struct and support (src/cheese.cu:305-338, 585-597, 429-449). */
 int cz_eval_bounds(cz_engine *engine, const cz_spec *spec, int count, const int64_t *entries, const int *k,
                    int *bounds);
