@@ -55,6 +55,8 @@ SIGNATURES = {
                                  C.POINTER(Result)]),
     "cz_eval_bounds": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int),
                                  C.POINTER(C.c_int)]),
+    "cz_eval_bounds_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_char_p, C.c_size_t]),
     "cz_engine_stream": (C.c_void_p, [C.c_void_p]),
     "cz_int32_peak": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "cz_version": (C.c_char_p, []),

@@ -174,6 +174,23 @@ int cz_eval_bounds(cz_engine *engine, const cz_spec *spec, int count, const int6
   }
 }
 
+int cz_eval_bounds_noalloc(const cz_spec *spec, int count, const int64_t *d_entries, const int *d_k, int *d_bounds,
+                           void *stream, char *err, size_t errlen) {
+  static_assert(CZ_NOALLOC_SCRATCH_BYTES == cz::NOALLOC_SCRATCH_BYTES, "header and library disagree");
+  static_assert(CZ_NOALLOC_MAX_CXTABLE == cz::NOALLOC_MAX_CXTABLE, "header and library disagree");
+  if (!spec) { put_err(err, errlen, "null spec"); return CZ_ERR_USAGE; }
+  std::string e;
+  int rc;
+  try {
+    rc = cz::eval_bounds_noalloc(spec->hs, count, d_entries, d_k, d_bounds, stream, e);
+  } catch (const std::exception &ex) {
+    e = ex.what();
+    rc = CZ_ERR_CUDA;
+  }
+  put_err(err, errlen, e);
+  return rc;
+}
+
 void *cz_engine_stream(cz_engine *engine) { return engine ? engine->e->stream() : nullptr; }
 
 int cz_int32_peak(cz_engine *engine, double *ops_per_s) {

@@ -42,6 +42,18 @@ struct SearchResult {
   std::string error;
 };
 
+// Largest CX table and size of the device array used by eval_bounds_noalloc (see there).
+constexpr int NOALLOC_MAX_CXTABLE = 4096;
+constexpr size_t NOALLOC_SCRATCH_BYTES = 86016;
+
+// Bounds of `count` residuals held in the caller's device memory (entries: count x N^2 x 4 int64 limbs, 16-byte
+// aligned; exponents: count ints; bounds: count x 4 ints, 16-byte aligned), on the caller's stream, without any
+// device allocation: the spec's tables are staged in a static device array shared by all calls (calls that overlap
+// on the GPU race on it). The first call on a device looks the array up (cudaGetSymbolAddress); make that first
+// call before any stream capture.
+int eval_bounds_noalloc(const HostSpec &hs, int count, const int64_t *d_entries, const int *d_k, int *d_bounds,
+                        void *stream, std::string &err);
+
 class Engine {
  public:
   explicit Engine(int device);

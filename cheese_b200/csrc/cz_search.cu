@@ -27,6 +27,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <stdexcept>
 
 #include "cz_engine.h"
@@ -1161,8 +1162,10 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
   return RC_PROOF;   // stopped at the last level (not reachable: the last level keeps nothing)
 }
 
+// host part of the device spec: every field, plus the gate-matrix (gi) and goal (gl) tables to place on the device
 template <int NQ>
-DevSpec Engine::Impl::prepare(const HostSpec &hs, const SymGroup &grp, int depth, bool nogoal) {
+DevSpec devspec_host(const HostSpec &hs, const SymGroup &grp, int depth, bool nogoal, std::vector<int4> &gi,
+                     std::vector<longlong2> &gl) {
   constexpr int N = 1 << NQ, E = N * N;
   DevSpec sp;
   std::memset(&sp, 0, sizeof sp);
@@ -1216,18 +1219,26 @@ DevSpec Engine::Impl::prepare(const HostSpec &hs, const SymGroup &grp, int depth
       if (perm) sp.gkind[g] = GK_PERM;
     }
   }
-  std::vector<int4> gi((size_t)GMAX * 64, int4{0, 0, 0, 0});
+  gi.assign((size_t)GMAX * 64, int4{0, 0, 0, 0});
   for (int g = 0; g < hs.G; g++)
     for (int i = 0; i < LMAX * LMAX; i++) {
       const Zw z = hs.ginv[g][i];
       gi[(size_t)g * 64 + i] = int4{(int)z.a, (int)z.b, (int)z.c, (int)z.d};
     }
-  std::vector<longlong2> gl(2 * E);
+  gl.assign(2 * E, longlong2{});
   for (int r = 0; r < N; r++)
     for (int c = 0; c < N; c++) {
       gl[2 * (r * N + c)] = make_longlong2(r == c ? 1 : 0, 0);
       gl[2 * (r * N + c) + 1] = make_longlong2(0, 0);
     }
+  return sp;
+}
+
+template <int NQ>
+DevSpec Engine::Impl::prepare(const HostSpec &hs, const SymGroup &grp, int depth, bool nogoal) {
+  std::vector<int4> gi;
+  std::vector<longlong2> gl;
+  DevSpec sp = devspec_host<NQ>(hs, grp, depth, nogoal, gi, gl);
   SpecDev *sd = nullptr;                   // spec tables: uploaded once per parsed spec (small LRU)
   for (auto &x : specs) if (x.uid == hs.uid) sd = &x;
   if (!sd) {
@@ -1354,6 +1365,94 @@ int Engine::eval_bounds(const HostSpec &hs, int count, const int64_t *ent, const
       case 6: impl_->eval_bounds<3, int32_t>(hs, count, ent, ks, out4); break;
       case 7: impl_->eval_bounds<3, int64_t>(hs, count, ent, ks, out4); break;
       default: err = "n not built"; return RC_USAGE;
+    }
+  } catch (const CudaError &e) {
+    err = e.what();
+    return RC_CUDA;
+  }
+  return 0;
+}
+
+// ---------------- bound evaluation without device allocation ----------------
+// For callers that cannot allocate device memory: the spec's gate-matrix, CX and goal tables are staged in a
+// file-scope device array instead of engine buffers; the residuals, exponents and bounds stay in the caller's
+// device buffers. The array lives on every device that loads this library until the process exits.
+namespace {
+constexpr size_t NA_GINV = (size_t)GMAX * 64 * sizeof(int4);           // 64 gates x 8 x 8 local matrix
+constexpr size_t NA_CXT = (size_t)NOALLOC_MAX_CXTABLE * sizeof(int);
+constexpr size_t NA_GOAL = (size_t)64 * 2 * sizeof(longlong2);
+static_assert(NA_GINV + NA_CXT + NA_GOAL <= NOALLOC_SCRATCH_BYTES, "no-alloc scratch too small");
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[256];                // per device: the array's device address (set up on first use)
+
+template <int NQ>
+void eval_bounds_noalloc_nq(const HostSpec &hs, unsigned char *base, int count, const int64_t *d_entries,
+                            const int *d_k, int *d_bounds, cudaStream_t st) {
+  const SymGroup grp = sym_group(hs, false);
+  std::vector<int4> gi;
+  std::vector<longlong2> gl;
+  DevSpec sp = devspec_host<NQ>(hs, grp, hs.depth, false, gi, gl);
+  // every table is rewritten in full by each call (nothing carries over from the previous call's contents)
+  ck(cudaMemcpyAsync(base, gi.data(), NA_GINV, cudaMemcpyHostToDevice, st), "h2d");
+  std::vector<int> cx(NOALLOC_MAX_CXTABLE, 0);
+  std::copy(hs.cxtable.begin(), hs.cxtable.end(), cx.begin());
+  ck(cudaMemcpyAsync(base + NA_GINV, cx.data(), NA_CXT, cudaMemcpyHostToDevice, st), "h2d");
+  std::vector<longlong2> g64(64 * 2, longlong2{});
+  std::copy(gl.begin(), gl.end(), g64.begin());
+  ck(cudaMemcpyAsync(base + NA_GINV + NA_CXT, g64.data(), NA_GOAL, cudaMemcpyHostToDevice, st), "h2d");
+  ck(cudaStreamSynchronize(st), "table staging");   // the host tables above go out of scope
+  sp.ginv = (const int4 *)base;
+  sp.cxtable = (const int *)(base + NA_GINV);
+  sp.goal = (const longlong2 *)(base + NA_GINV + NA_CXT);
+  sp.bad2 = nullptr;
+  sp.bad3 = nullptr;
+  int nsm = 148;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = std::max(1, std::min((count + EXP_WARPS - 1) / EXP_WARPS, nsm * 8));
+  k_eval_bounds<NQ, int64_t><<<grid, EXP_WARPS * 32, 0, st>>>(sp, (const Z4<int64_t> *)d_entries, d_k, count,
+                                                              (int4 *)d_bounds);
+  ck(cudaGetLastError(), "bounds kernel");
+}
+}  // namespace
+
+int eval_bounds_noalloc(const HostSpec &hs, int count, const int64_t *d_entries, const int *d_k, int *d_bounds,
+                        void *stream, std::string &err) {
+  if (count < 0) { err = "count < 0"; return RC_USAGE; }
+  if (count == 0) return 0;
+  if (!d_entries || !d_k || !d_bounds) { err = "null device buffer"; return RC_USAGE; }
+  if (((uintptr_t)d_entries & 15) || ((uintptr_t)d_bounds & 15) || ((uintptr_t)d_k & 3)) {
+    err = "device buffers must be 16-byte aligned (entries, bounds) and 4-byte aligned (exponents)";
+    return RC_USAGE;
+  }
+  if (hs.n < 1 || hs.n > NQMAX) { err = "n = " + std::to_string(hs.n) + " not built"; return RC_USAGE; }
+  if (hs.cxtable.size() > (size_t)NOALLOC_MAX_CXTABLE) {
+    err = "CX table of " + std::to_string(hs.cxtable.size()) + " entries exceeds the " +
+          std::to_string(NOALLOC_MAX_CXTABLE) + " this entry point stages without allocating";
+    return RC_USAGE;
+  }
+  try {
+    int dev = 0;
+    ck(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= 256) { err = "device index out of range"; return RC_USAGE; }
+    unsigned char *base;
+    {
+      std::lock_guard<std::mutex> lk(g_noalloc_mu);
+      if (!g_noalloc_addr[dev]) {          // once per device, with that device current
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) { err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e); return RC_CUDA; }
+        g_noalloc_addr[dev] = p;
+      }
+      base = (unsigned char *)g_noalloc_addr[dev];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (hs.n) {
+      case 1: eval_bounds_noalloc_nq<1>(hs, base, count, d_entries, d_k, d_bounds, st); break;
+      case 2: eval_bounds_noalloc_nq<2>(hs, base, count, d_entries, d_k, d_bounds, st); break;
+      default: eval_bounds_noalloc_nq<3>(hs, base, count, d_entries, d_k, d_bounds, st); break;
     }
   } catch (const CudaError &e) {
     err = e.what();

@@ -101,6 +101,22 @@ int cz_search_text(cz_engine *engine, const char *spec_text, size_t len, const c
 int cz_eval_bounds(cz_engine *engine, const cz_spec *spec, int count, const int64_t *entries, const int *k,
                    int *bounds);
 
+/* No counterpart in the reference. The same bounds as cz_eval_bounds for callers that cannot allocate device
+ * memory (code running under a custom or fixed-size allocator, inside a memory-capped service, or in a process
+ * whose allocator is owned by another runtime): it calls no cudaMalloc / cudaFree and creates no engine. The
+ * caller passes device buffers: d_entries (count x N^2 x 4 int64 limbs, 16-byte aligned), d_k (count ints) and
+ * d_bounds (count x 4 ints, 16-byte aligned), and the stream to run on (NULL: the legacy default stream); the call
+ * returns once the kernel is queued after the staged tables. The spec's tables (gate matrices, CX table, goal)
+ * are staged in a static device array of CZ_NOALLOC_SCRATCH_BYTES that every GPU loading this library keeps
+ * until the process exits; a spec whose CX table has more than CZ_NOALLOC_MAX_CXTABLE entries is refused with
+ * CZ_ERR_USAGE. All calls share that array and each rewrites it in full, so calls that overlap on the GPU race.
+ * The first call on a device looks the array up (cudaGetSymbolAddress) with that device current: make it before
+ * any stream capture. */
+#define CZ_NOALLOC_SCRATCH_BYTES 86016
+#define CZ_NOALLOC_MAX_CXTABLE 4096
+int cz_eval_bounds_noalloc(const cz_spec *spec, int count, const int64_t *d_entries, const int *d_k, int *d_bounds,
+                           void *stream, char *err, size_t errlen);
+
 /* The CUDA stream (cudaStream_t) the engine launches on, for callers that order their own work or timing
  * events after the engine's kernels. */
 void *cz_engine_stream(cz_engine *engine);
