@@ -32,13 +32,15 @@ SPECS = ROOT / "tests" / "golden" / "specs"
 REF_CPU = ROOT / "oracle" / "_ref" / "cheese-cpu"
 WORKLOAD = [("toffoli", 11), ("toffoli", 12), ("ccz", 8)]
 METRIC = "prefixes/s"
-# algorithmic int32 operations (a multiply or an add counts 1) per unit of work of the level kernel, 3 qubits:
-#  T-bound evaluation: 64 (fa, fb) x 64 points x (16 mul + 12 add Z[w] product + 6 stages x 4 add/sub butterflies
-#  + 5 valuation ops)
-#  child evaluation: residual update S g^-1 over 64 entries (<= 2 Z[w] multiply-adds) + normalisation, goal,
-#  H-structure and support tests (~16 ops per entry)
-OPS_T_EVAL = 64 * 64 * (28 + 24 + 5)
-OPS_CHILD = 64 * (2 * 32 + 16)
+# algorithmic int32 operations (a multiply or an add counts 1) per unit of work of the level kernel, 3 qubits, as
+# the kernel computes them:
+#  T-bound evaluation (conjugate-pair form): 63 pairs (fa, fb) != 0 x [32 products x (4 four-term dot products:
+#  16 mul + 12 add, + 4 adds of operand combinations) + 4 real 32-point transforms (4 x 80 butterflies x 2) + 32 x 2
+#  OR words] + the (0, 0) pair [64 x (8 mul + 6 add) + 2 real 64-point transforms (2 x 192 x 2) + 64 x 2 OR]
+#  child whose residual is computed: update (<= 2 unit-multiple terms: 4 adds per entry), sqrt2-divisibility test
+#  (2 per entry), goal / support tests (4 per entry) over 64 entries
+OPS_T_EVAL = 63 * (32 * 32 + 640 + 64) + (64 * 14 + 768 + 128)
+OPS_CHILD = 64 * (4 + 2 + 4)
 CLOCK_Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
            "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
            "clocks_event_reasons.sw_power_cap")
@@ -223,7 +225,7 @@ def main():
                 exp_ms += r.expand_ms
                 exp_launches += r.expand_launches
                 launches += r.kernel_launches
-                ops += r.t_evals * OPS_T_EVAL + r.children * OPS_CHILD
+                ops += r.t_evals * OPS_T_EVAL + r.children_full * OPS_CHILD
     torch.cuda.synchronize()
     # end to end through the C ABI's text entry point: parse + upload + search + read-back, host-timed
     h2d = d2h = 0

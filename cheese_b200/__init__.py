@@ -35,7 +35,7 @@ class Result(C.Structure):
                 ("prefixes", C.c_int64), ("kernel_launches", C.c_int64), ("t_evals", C.c_int64),
                 ("children", C.c_int64), ("expand_ms", C.c_double), ("dedupe_ms", C.c_double),
                 ("total_ms", C.c_double), ("expand_launches", C.c_int64), ("h2d_bytes", C.c_int64),
-                ("d2h_bytes", C.c_int64), ("error", C.c_char * 256)]
+                ("d2h_bytes", C.c_int64), ("children_full", C.c_int64), ("error", C.c_char * 256)]
 
 
 LEVEL_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(LevelStats))

@@ -141,6 +141,7 @@ int cz_search(cz_engine *engine, const cz_spec *spec, const cz_options *opt, cz_
   out->expand_launches = r.expand_launches;
   out->h2d_bytes = r.h2d_bytes;
   out->d2h_bytes = r.d2h_bytes;
+  out->children_full = r.children_full;
   put_err(out->error, sizeof out->error, r.error);
   return rc;
 }

@@ -36,6 +36,7 @@ struct SearchResult {
   long long prefixes = 0;              // sum of the per-level "prefixes" fields
   long long launches = 0;              // kernels launched by the engine
   long long t_evals = 0, children = 0; // T-bound evaluations, children evaluated past the window rules
+  long long children_full = 0;         // children whose residual was computed (not decided from the parent)
   double expand_ms = 0, dedupe_ms = 0, total_ms = 0;   // device times (profile) / host wall time
   long long expand_launches = 0;       // level-kernel launches (the denominator of per-launch figures)
   long long h2d_bytes = 0, d2h_bytes = 0;   // host<->device traffic of the call

@@ -69,7 +69,7 @@ struct DevSpec {
 struct NodeMeta { int16_t k; uint8_t T, c2, g1, g2, hsn, needs; };
 
 struct DevStats {
-  unsigned long long w2, w3, dead, alive, found, first_found, n_surv, t_evals, children, work;
+  unsigned long long w2, w3, dead, alive, found, first_found, n_surv, t_evals, children, work, full;
   unsigned int ovf, surv_overflow;
   unsigned long long n_work, n_kept;
 };
@@ -131,7 +131,7 @@ template <typename ST> __device__ __forceinline__ uint32_t zmodp(const Z4<ST> &x
 // ---------------- per-warp bound evaluations (child residual S in shared memory) ----------------
 
 // T bound: max(0, max over nonzero PTM entries of their sde), Walsh-Hadamard form of cheese.cu:397-449
-template <int NQ, typename U, typename ST> __device__ int warp_ptm(const Z4<ST> *S, int k, int lane) {
+template <int NQ, typename U, typename ST> __device__ __noinline__ int warp_ptm(const Z4<ST> *S, int k, int lane) {
   constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
   Z4<U> y[EPL];
 #pragma unroll
@@ -193,7 +193,7 @@ __device__ __forceinline__ int pair_of(int idx) {   // the 63 nonzero f ordered 
   if (idx < 62) return 32 * (idx - 60) + 16;
   return idx == 62 ? 32 : 0;
 }
-template <typename ST> __device__ int warp_ptm3(const Z4<ST> *S, int k, int lane) {
+template <typename ST> __device__ __noinline__ int warp_ptm3(const Z4<ST> *S, int k, int lane) {
   using U = uint32_t;
   U R1 = 0, R2 = 0, P = 0, Q = 0;
   {   // f = 0: entries lane, lane + 32; bit 5 in registers, bits 0..4 across lanes
@@ -277,8 +277,8 @@ template <typename ST> __device__ int warp_ptm3(const Z4<ST> *S, int k, int lane
 }
 template <int NQ, typename ST> __device__ __forceinline__ int ptm_bound(const Z4<ST> *S, int k, int lane) {
   if (2 * (NQ + k) > 64) return warp_ptm<NQ, uint64_t, ST>(S, k, lane);
-  if (NQ == 3) return warp_ptm3<ST>(S, k, lane);
-  return warp_ptm<NQ, uint32_t, ST>(S, k, lane);
+  if constexpr (NQ == 3) return warp_ptm3<ST>(S, k, lane);
+  else return warp_ptm<NQ, uint32_t, ST>(S, k, lane);
 }
 
 // rank over F_p of the operator-Schmidt matrix across cut A (cheese.cu:271-303): lane j owns column j, fraction-free
@@ -326,7 +326,8 @@ template <int NQ, typename ST> __device__ int warp_cut_rank(const Z4<ST> *S, int
 // parent's need (a gate inside one side is a local map); needs_in = the parent's packed needs, gmask = the gate's
 // qubits (0: recompute every cut). Returns the bound, packs the child's needs into needs_out.
 template <int NQ, typename ST>
-__device__ int warp_cx_bound(const Z4<ST> *S, const DevSpec &sp, int lane, int gmask, int needs_in, int &needs_out) {
+__device__ __noinline__ int warp_cx_bound(const Z4<ST> *S, const DevSpec &sp, int lane, int gmask, int needs_in,
+                                          int &needs_out) {
   constexpr int ALLQ = (1 << NQ) - 1;
   int idx = 0, mult = 1, mx = 0, packed = 0;
   const bool inherit = sp.ncuts <= 4 && gmask;
@@ -371,66 +372,17 @@ template <typename ST> __device__ __forceinline__ Zw mul_unit(const Z4<ST> &x, i
   if (p & 4) r = Zw{-r.a, -r.b, -r.c, -r.d};
   return r;
 }
+// the same in int32, branch free: rotate by 2 if p & 2, by 1 if p & 1, negate if p & 4
+__device__ __forceinline__ int4 mul_unit32(int4 x, int p) {
+  int4 y = (p & 2) ? make_int4(-x.z, -x.w, x.x, x.y) : x;
+  y = (p & 1) ? make_int4(-y.w, y.x, y.y, y.z) : y;
+  return (p & 4) ? make_int4(-y.x, -y.y, -y.z, -y.w) : y;
+}
 
-// child residual C = P g^-1, normalised; returns its exponent, sets ovf when a limb leaves the storage type.
-// One-qubit gates whose inverse has only zero / w-power entries (x z h s sdg t tdg) pair entries that differ in
-// the gate's column bit, so each lane owns both inputs of its two outputs and the product is a rotation;
-// permutation gates (cx, ccx) copy; anything else multiplies out over Z[w].
-template <int NQ, typename ST>
-__device__ int warp_child(const Z4<ST> *P, Z4<ST> *C, int g, int kp, const DevSpec &sp, int lane, bool &ovf) {
-  constexpr int N = 1 << NQ, E = N * N;
-  Zw v[2] = {Zw{0, 0, 0, 0}, Zw{0, 0, 0, 0}};
-  int ei[2] = {-1, -1};
-  const int kind = sp.gkind[g];
-  if (kind == GK_ONEQ) {
-    const int q = sp.gq[g][0], lo = (1 << q) - 1;
-    if (lane < E / 2) {
-      ei[0] = ((lane & ~lo) << 1) | (lane & lo);
-      ei[1] = ei[0] | (1 << q);
-      const Z4<ST> x0 = P[ei[0]], x1 = P[ei[1]];
-      const int p00 = sp.gph[g][0], p01 = sp.gph[g][1], p10 = sp.gph[g][2], p11 = sp.gph[g][3];
-      if (p00 < 8) v[0] = zadd(v[0], mul_unit(x0, p00));
-      if (p10 < 8) v[0] = zadd(v[0], mul_unit(x1, p10));
-      if (p01 < 8) v[1] = zadd(v[1], mul_unit(x0, p01));
-      if (p11 < 8) v[1] = zadd(v[1], mul_unit(x1, p11));
-    }
-  } else {
-    const int nq = sp.gnq[g], L = 1 << nq;
-    const int q0 = sp.gq[g][0], q1 = nq > 1 ? sp.gq[g][1] : 0, q2 = nq > 2 ? sp.gq[g][2] : 0;
-    const int mask = (1 << q0) | (nq > 1 ? 1 << q1 : 0) | (nq > 2 ? 1 << q2 : 0);
-#pragma unroll
-    for (int j = 0; j < 2; j++) {
-      const int e = lane + 32 * j;
-      if (e >= E) continue;
-      ei[j] = e;
-      const int r = e >> NQ, col = e & (N - 1), base = col & ~mask;
-      int lc = (col >> q0) & 1;
-      if (nq > 1) lc |= ((col >> q1) & 1) << 1;
-      if (nq > 2) lc |= ((col >> q2) & 1) << 2;
-      if (kind == GK_PERM) {
-        const int m = sp.gperm[g][lc];
-        int x = base | ((m & 1) << q0);
-        if (nq > 1) x |= ((m >> 1) & 1) << q1;
-        if (nq > 2) x |= ((m >> 2) & 1) << q2;
-        const Z4<ST> sv = P[r * N + x];
-        v[j] = Zw{sv.a, sv.b, sv.c, sv.d};
-        continue;
-      }
-      const int4 *gi = sp.ginv + g * 64;
-      for (int m = 0; m < L; m++) {
-        const int4 gm = __ldg(&gi[m * L + lc]);
-        if (!(gm.x | gm.y | gm.z | gm.w)) continue;
-        int x = base | ((m & 1) << q0);
-        if (nq > 1) x |= ((m >> 1) & 1) << q1;
-        if (nq > 2) x |= ((m >> 2) & 1) << q2;
-        const Z4<ST> sv = P[r * N + x];
-        v[j] = zadd(v[j], zmul(Zw{(int64_t)sv.a, (int64_t)sv.b, (int64_t)sv.c, (int64_t)sv.d},
-                               Zw{(int64_t)gm.x, (int64_t)gm.y, (int64_t)gm.z, (int64_t)gm.w}));
-      }
-    }
-  }
-  int k = kp + sp.gik[g];
-  while (k > 0) {                              // normalise: lower k while every entry is divisible by sqrt2
+// normalise the lane's two entries (sqrt2 division while every entry allows it) and store them; returns k
+template <int NQ, typename ST, typename V>
+__device__ __forceinline__ int finish_child(V (&v)[2], const int (&ei)[2], int k, Z4<ST> *C, int lane, bool &ovf) {
+  while (k > 0) {
     const bool ok = (ei[0] < 0 || zdiv2ok(v[0])) && (ei[1] < 0 || zdiv2ok(v[1]));
     if (!__all_sync(FULL, ok)) break;
     v[0] = zdown(v[0]);
@@ -447,6 +399,110 @@ __device__ int warp_child(const Z4<ST> *P, Z4<ST> *C, int g, int kp, const DevSp
   ovf = __any_sync(FULL, of);
   __syncwarp();
   return k;
+}
+// int32 helpers for the fast path (exact: callers guarantee |coefficient| <= 2^28)
+struct I4 { int a, b, c, d; };
+__device__ __forceinline__ bool zdiv2ok(const I4 &x) { return !((x.a - x.c) & 1) && !((x.b - x.d) & 1); }
+__device__ __forceinline__ I4 zdown(const I4 &x) { return {(x.b - x.d) >> 1, (x.a + x.c) >> 1, (x.b + x.d) >> 1, (x.c - x.a) >> 1}; }
+__device__ __forceinline__ bool fits32(int) { return true; }
+
+// child residual C = P g^-1, general gate: multiplies the local matrix out over Z[w] in int64
+template <int NQ, typename ST>
+__device__ __noinline__ int child_general(const Z4<ST> *P, Z4<ST> *C, int g, int kp, const DevSpec *sp, int lane,
+                                          bool &ovf) {
+  constexpr int N = 1 << NQ, E = N * N;
+  Zw v[2] = {Zw{0, 0, 0, 0}, Zw{0, 0, 0, 0}};
+  int ei[2] = {-1, -1};
+  const int kind = sp->gkind[g];
+  const int nq = sp->gnq[g], L = 1 << nq;
+  const int q0 = sp->gq[g][0], q1 = nq > 1 ? sp->gq[g][1] : 0, q2 = nq > 2 ? sp->gq[g][2] : 0;
+  const int mask = (1 << q0) | (nq > 1 ? 1 << q1 : 0) | (nq > 2 ? 1 << q2 : 0);
+  if (kind == GK_ONEQ) {
+    const int lo = (1 << q0) - 1;
+    if (lane < E / 2) {
+      ei[0] = ((lane & ~lo) << 1) | (lane & lo);
+      ei[1] = ei[0] | (1 << q0);
+      const Z4<ST> x0 = P[ei[0]], x1 = P[ei[1]];
+      const int p00 = sp->gph[g][0], p01 = sp->gph[g][1], p10 = sp->gph[g][2], p11 = sp->gph[g][3];
+      if (p00 < 8) v[0] = zadd(v[0], mul_unit(x0, p00));
+      if (p10 < 8) v[0] = zadd(v[0], mul_unit(x1, p10));
+      if (p01 < 8) v[1] = zadd(v[1], mul_unit(x0, p01));
+      if (p11 < 8) v[1] = zadd(v[1], mul_unit(x1, p11));
+    }
+  } else {
+    for (int j = 0; j < 2; j++) {
+      const int e = lane + 32 * j;
+      if (e >= E) continue;
+      ei[j] = e;
+      const int r = e >> NQ, col = e & (N - 1), base = col & ~mask;
+      int lc = (col >> q0) & 1;
+      if (nq > 1) lc |= ((col >> q1) & 1) << 1;
+      if (nq > 2) lc |= ((col >> q2) & 1) << 2;
+      const int4 *gi = sp->ginv + g * 64;
+      for (int m = 0; m < L; m++) {
+        const int4 gm = __ldg(&gi[m * L + lc]);
+        if (!(gm.x | gm.y | gm.z | gm.w)) continue;
+        int x = base | ((m & 1) << q0);
+        if (nq > 1) x |= ((m >> 1) & 1) << q1;
+        if (nq > 2) x |= ((m >> 2) & 1) << q2;
+        const Z4<ST> sv = P[r * N + x];
+        v[j] = zadd(v[j], zmul(Zw{(int64_t)sv.a, (int64_t)sv.b, (int64_t)sv.c, (int64_t)sv.d},
+                               Zw{(int64_t)gm.x, (int64_t)gm.y, (int64_t)gm.z, (int64_t)gm.w}));
+      }
+    }
+  }
+  return finish_child<NQ, ST>(v, ei, kp + sp->gik[g], C, lane, ovf);
+}
+
+// child residual C = P g^-1, normalised; returns its exponent, sets ovf when a limb leaves the storage type.
+// Fast path (int32 limbs, |coefficient| <= 2^28, i.e. parent k <= 56): one-qubit gates whose inverse has only zero
+// / w-power entries (x z h s sdg t tdg) pair the entries that differ in the gate's column bit, so each lane owns
+// both inputs of its two outputs and every product is a signed rotation; permutation gates (cx, ccx) copy.
+// Anything else goes through child_general.
+template <int NQ, typename ST>
+__device__ __forceinline__ int warp_child(const Z4<ST> *P, Z4<ST> *C, int g, int kp, const DevSpec &sp,
+                                          const DevSpec *sps, int lane, bool &ovf) {
+  constexpr int N = 1 << NQ, E = N * N;
+  const int kind = sp.gkind[g];
+  if (sizeof(ST) != 4 || kp > 56 || kind == GK_GENERAL) return child_general<NQ, ST>(P, C, g, kp, sps, lane, ovf);
+  I4 v[2] = {I4{0, 0, 0, 0}, I4{0, 0, 0, 0}};
+  int ei[2] = {-1, -1};
+  const int4 *P4 = (const int4 *)P;
+  if (kind == GK_ONEQ) {
+    const int q = sp.gq[g][0], lo = (1 << q) - 1;
+    if (lane < E / 2) {
+      ei[0] = ((lane & ~lo) << 1) | (lane & lo);
+      ei[1] = ei[0] | (1 << q);
+      const int4 x0 = P4[ei[0]], x1 = P4[ei[1]];
+      const int p00 = sp.gph[g][0], p01 = sp.gph[g][1], p10 = sp.gph[g][2], p11 = sp.gph[g][3];
+      const int4 z = make_int4(0, 0, 0, 0);
+      const int4 a0 = p00 < 8 ? mul_unit32(x0, p00) : z, a1 = p10 < 8 ? mul_unit32(x1, p10) : z;
+      const int4 b0 = p01 < 8 ? mul_unit32(x0, p01) : z, b1 = p11 < 8 ? mul_unit32(x1, p11) : z;
+      v[0] = I4{a0.x + a1.x, a0.y + a1.y, a0.z + a1.z, a0.w + a1.w};
+      v[1] = I4{b0.x + b1.x, b0.y + b1.y, b0.z + b1.z, b0.w + b1.w};
+    }
+  } else {   // GK_PERM
+    const int nq = sp.gnq[g];
+    const int q0 = sp.gq[g][0], q1 = nq > 1 ? sp.gq[g][1] : 0, q2 = nq > 2 ? sp.gq[g][2] : 0;
+    const int mask = (1 << q0) | (nq > 1 ? 1 << q1 : 0) | (nq > 2 ? 1 << q2 : 0);
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      const int e = lane + 32 * j;
+      if (e >= E) continue;
+      ei[j] = e;
+      const int r = e >> NQ, col = e & (N - 1), base = col & ~mask;
+      int lc = (col >> q0) & 1;
+      if (nq > 1) lc |= ((col >> q1) & 1) << 1;
+      if (nq > 2) lc |= ((col >> q2) & 1) << 2;
+      const int m = sp.gperm[g][lc];
+      int x = base | ((m & 1) << q0);
+      if (nq > 1) x |= ((m >> 1) & 1) << q1;
+      if (nq > 2) x |= ((m >> 2) & 1) << q2;
+      const int4 sv = P4[r * N + x];
+      v[j] = I4{sv.x, sv.y, sv.z, sv.w};
+    }
+  }
+  return finish_child<NQ, ST>(v, ei, kp + sp.gik[g], C, lane, ovf);
 }
 
 template <int NQ, typename ST> __device__ bool warp_goal(const Z4<ST> *S, int k, const DevSpec &sp, int lane);
@@ -490,20 +546,20 @@ __device__ Cheap warp_cheap(const Z4<ST> *S, int k, const DevSpec &sp, int lane,
     if (__popcll(M) == N) {                      // monomial iff every column has exactly one nonzero
       int pi[N];
       bool mono = true;
-#pragma unroll
+#pragma unroll 1
       for (int c = 0; c < N; c++) {
         uint64_t colm = 0;
-#pragma unroll
+#pragma unroll 1
         for (int r = 0; r < N; r++) colm |= ((M >> (r * N + c)) & 1ULL) << r;
         mono = mono && __popcll(colm) == 1;
         pi[c] = __ffsll((long long)colm) - 1;
       }
       if (mono) {
         bool aff = true;
-#pragma unroll
+#pragma unroll 1
         for (int j = 0; j < N; j++) {
           int xx = pi[0];
-#pragma unroll
+#pragma unroll 1
           for (int i = 0; i < NQ; i++) if ((j >> i) & 1) xx ^= pi[1 << i] ^ pi[0];
           if (pi[j] != xx) aff = false;
         }
@@ -546,7 +602,7 @@ template <int NQ, typename ST> __device__ bool warp_goal(const Z4<ST> *S, int k,
 // class key: the smallest (h1, h2) over the symmetry orbit of S; per orbit element a position-weighted sum of
 // per-entry hashes (the key only has to be class-invariant: classes are always compared exactly)
 template <int NQ, typename ST>
-__device__ void warp_class_key(const Z4<ST> *S, int k, const DevSpec &sp, const uint8_t (*perm)[8],
+__device__ __noinline__ void warp_class_key(const Z4<ST> *S, int k, int nsym, unsigned conjmask, const uint8_t (*perm)[8],
                                const uint64_t *W1, const uint64_t *W2, int lane, uint64_t &k1, uint64_t &k2) {
   constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
   uint64_t f1[EPL], f2[EPL], c1[EPL], c2[EPL];
@@ -565,8 +621,8 @@ __device__ void warp_class_key(const Z4<ST> *S, int k, const DevSpec &sp, const 
     c1[j] = h; c2[j] = fmix64(h + 0x632be59bd9b4e019ULL);
   }
   uint64_t b1 = ~0ULL, b2 = ~0ULL;
-  for (int s = 0; s < sp.nsym; s++) {
-    const bool cj = sp.symconj[s];
+  for (int s = 0; s < nsym; s++) {
+    const bool cj = (conjmask >> s) & 1;
     uint64_t a = 0, b = 0;
 #pragma unroll
     for (int j = 0; j < EPL; j++) {
@@ -605,13 +661,17 @@ template <int NQ, typename ST>
 __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, const ExpandArgs<ST> a) {
   constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
   __shared__ ExpandSmem<NQ, ST> sm;
+  __shared__ DevSpec s_sp;                     // the spec for out-of-line helpers (a shared address, no local copy)
+  for (int i = threadIdx.x; i < (int)(sizeof(DevSpec) / 4); i += blockDim.x) ((int *)&s_sp)[i] = ((const int *)&sp)[i];
   init_weights(sm.W1, sm.W2, E);
   for (int i = threadIdx.x; i < SYMMAX * 8; i += blockDim.x) sm.perm[i / 8][i % 8] = sp.symperm[i / 8][i % 8];
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   Z4<ST> *P = sm.P[w], *C = sm.C[w];
   const int G = sp.G;
-  unsigned long long n_w2 = 0, n_w3 = 0, n_dead = 0, n_alive = 0, n_found = 0, n_teval = 0, n_child = 0;
+  unsigned conjmask = 0;
+  for (int i = 0; i < sp.nsym; i++) conjmask |= (unsigned)(sp.symconj[i] != 0) << i;
+  unsigned long long n_w2 = 0, n_w3 = 0, n_dead = 0, n_alive = 0, n_found = 0, n_teval = 0, n_child = 0, n_full = 0;
   unsigned long long first = ~0ULL;
   bool ovf_any = false;
   for (;;) {
@@ -660,7 +720,8 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, 
         }
       }
       bool ovf;
-      const int k = warp_child<NQ, ST>(P, C, g, kP, sp, lane, ovf);
+      n_full++;
+      const int k = warp_child<NQ, ST>(P, C, g, kP, sp, &s_sp, lane, ovf);
       if (ovf) { ovf_any = true; continue; }
       const bool need_b = sp.standard != 0;
       const bool need_hs = need_b && !(fl & GF_MONAFF);
@@ -691,7 +752,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, 
         const int h = k > hs ? k : hs;
         const int supp = __popc(ch.ntriv);
         if (fl & GF_ONEQ) { c2 = c2P; needs = pm.needs; }
-        else c2 = warp_cx_bound<NQ, ST>(C, sp, lane, gm, pm.needs, needs);
+        else c2 = warp_cx_bound<NQ, ST>(C, s_sp, lane, gm, pm.needs, needs);
         if (combine(h, 0, c2, supp) > rem) alive = false;
         else {
           if (inheritT) T = TP;
@@ -707,7 +768,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, 
       n_alive++;
       if (!a.keep) continue;
       uint64_t k1, k2;
-      warp_class_key<NQ, ST>(C, k, sp, sm.perm, sm.W1, sm.W2, lane, k1, k2);
+      warp_class_key<NQ, ST>(C, k, sp.nsym, conjmask, sm.perm, sm.W1, sm.W2, lane, k1, k2);
       unsigned long long slot = 0;
       if (lane == 0) slot = atomicAdd(&a.st->n_surv, 1ULL);
       slot = __shfl_sync(FULL, slot, 0);
@@ -740,6 +801,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, 
     if (n_found) { atomicAdd(&a.st->found, n_found); atomicMin(&a.st->first_found, first); }
     if (n_teval) atomicAdd(&a.st->t_evals, n_teval);
     if (n_child) atomicAdd(&a.st->children, n_child);
+    if (n_full) atomicAdd(&a.st->full, n_full);
     if (ovf_any) a.st->ovf = 1;
   }
 }
@@ -1067,6 +1129,7 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
     const DevStats h = *hstats;
     res.t_evals += (long long)h.t_evals;
     res.children += (long long)h.children;
+    res.children_full += (long long)h.full;
     LevelStats L;
     L.t = t; L.parents = m; L.prefixes = m * G - (long long)h.w2; L.cut_w3 = (long long)h.w3;
     L.cut_lb = (long long)h.dead; L.survivors = (long long)h.alive;

@@ -81,6 +81,7 @@ typedef struct {
   double total_ms;             /* host wall time of the call */
   int64_t expand_launches;     /* launches of the level kernel */
   int64_t h2d_bytes, d2h_bytes;/* host<->device bytes moved by the call */
+  int64_t children_full;       /* children whose residual was computed (the rest were decided from the parent) */
   char error[256];
 } cz_result;
 
