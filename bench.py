@@ -211,7 +211,7 @@ def main():
     prefixes = 0
     dev_ms = t12_ms = 0.0
     exp_ms = ops = 0.0
-    launches = exp_launches = 0
+    launches = exp_launches = parents = 0
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             flush.fill_(1)                     # L2 (126 MB) flushed between steps
@@ -221,6 +221,7 @@ def main():
             dev_ms += ms
             t12_ms += t12
             for o in outs:
+                parents += sum(l["parents"] for l in o.levels)
                 r = o.raw
                 exp_ms += r.expand_ms
                 exp_launches += r.expand_launches
@@ -246,9 +247,12 @@ def main():
     launch_ms = exp_ms / max(1, exp_launches)
     achieved = (ops / max(1, exp_launches)) / (launch_ms * 1e-3) if launch_ms > 0 else 0.0
     traffic = None
-    tf = ROOT / "profiles" / "k_expand-traffic.json"
-    if tf.exists():
-        traffic = json.loads(tf.read_text()).get("bytes_per_launch")
+    tf = ROOT / "profiles" / "k_expand-toffoli11-level6.md"
+    if tf.exists():   # ncu DRAM bytes per parent of a captured launch, scaled to this run's average launch
+        import re
+        m = re.search(r"bytes per parent \(for bench.py scaling\): (\d+)", tf.read_text())
+        if m and exp_launches:
+            traffic = int(m.group(1)) * parents / exp_launches
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and REF_CPU.exists():
         threads = os.cpu_count() or 1
