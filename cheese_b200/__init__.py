@@ -40,6 +40,26 @@ class Result(C.Structure):
 
 LEVEL_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(LevelStats))
 
+
+class TcOptions(C.Structure):
+    _fields_ = [("table_k", C.c_int), ("maxt", C.c_int), ("cache_dir", C.c_char_p)]
+
+
+class TcLevel(C.Structure):
+    _fields_ = [("table", C.c_int), ("t", C.c_int), ("parents", C.c_int64), ("children", C.c_int64),
+                ("cosets", C.c_int64), ("fresh", C.c_int64), ("seconds", C.c_double)]
+
+
+class TcResult(C.Structure):
+    _fields_ = [("rc", C.c_int), ("tcount", C.c_int), ("split_j", C.c_int), ("split_c", C.c_int), ("maxt", C.c_int),
+                ("nrot", C.c_int), ("rot_p", C.c_int * 64), ("rot_inv", C.c_int * 64), ("table_cosets", C.c_int64),
+                ("table_levels", C.c_int), ("table_loaded", C.c_int), ("table_built", C.c_int),
+                ("table_resident", C.c_int), ("table_seconds", C.c_double), ("total_seconds", C.c_double),
+                ("kernel_launches", C.c_int64), ("table_path", C.c_char * 256), ("error", C.c_char * 256)]
+
+
+TC_LEVEL_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(TcLevel))
+
 # every C entry point of include/cheese_b200.h with its ctypes signature
 SIGNATURES = {
     "cz_spec_parse": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
@@ -59,6 +79,10 @@ SIGNATURES = {
                                          C.c_char_p, C.c_size_t]),
     "cz_engine_stream": (C.c_void_p, [C.c_void_p]),
     "cz_int32_peak": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "cz_tcount_options_default": (None, [C.POINTER(TcOptions)]),
+    "cz_tspec_check": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(C.c_int), C.c_char_p, C.c_size_t]),
+    "cz_tcount": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(TcOptions), TC_LEVEL_FN, C.c_void_p,
+                            C.POINTER(TcResult)]),
     "cz_version": (C.c_char_p, []),
 }
 
@@ -108,6 +132,18 @@ class SpecError(Exception):
         self.rc = rc
 
 
+def tspec_check(text):
+    """qubit count of a tcount-spec, parsed on the host; raises SpecError (rc 2 or 3) like the reference's reader"""
+    if isinstance(text, str):
+        text = text.encode()
+    n = C.c_int()
+    err = C.create_string_buffer(256)
+    rc = lib().cz_tspec_check(text, len(text), C.byref(n), err, 256)
+    if rc:
+        raise SpecError(rc, err.value.decode())
+    return n.value
+
+
 class Engine:
     """one CUDA device and stream; searches run one at a time on it"""
 
@@ -151,6 +187,28 @@ class Engine:
         if rc:
             raise RuntimeError(f"cz_eval_bounds failed: {rc}")
         return [tuple(out[4 * i:4 * i + 4]) for i in range(n)]
+
+    def tcount(self, tspec, table_k=4, maxt=16, cache_dir="build", on_level=None):
+        """`tcount TSPEC --table K --max T`: (rc, level dicts, result dict)"""
+        if isinstance(tspec, str):
+            tspec = tspec.encode()
+        opt = TcOptions(table_k, maxt, cache_dir.encode() if cache_dir else None)
+        levels = []
+
+        def cb(_u, p):
+            l = p.contents
+            d = {k: getattr(l, k) for k, _ in TcLevel._fields_}
+            levels.append(d)
+            if on_level:
+                on_level(d)
+
+        res = TcResult()
+        rc = lib().cz_tcount(self._h, tspec, len(tspec), C.byref(opt), TC_LEVEL_FN(cb), None, C.byref(res))
+        out = {k: getattr(res, k) for k, _ in TcResult._fields_ if k not in ("rot_p", "rot_inv")}
+        out["rotations"] = [[res.rot_p[i], res.rot_inv[i]] for i in range(res.nrot)]
+        out["error"] = res.error.decode()
+        out["table_path"] = res.table_path.decode()
+        return rc, levels, out
 
     def search(self, spec, depth=-1, dedupe=True, sym=True, store64=False, profile=False, on_level=None):
         """run `cheese SPEC [--depth D] [--no-dedupe] [--no-sym]`; returns a SearchOutcome"""

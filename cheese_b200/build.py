@@ -21,9 +21,9 @@ HOSTCXX = os.environ.get("CZ_HOSTCXX", "/usr/bin/g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-ccbin", HOSTCXX, "-Xcompiler", "-fPIC"]
 
-LIB_SOURCES = ["cz_search.cu", "cz_spec.cpp", "cz_capi.cpp"]
-HEADERS = ["cz_common.h", "cz_spec.h", "cz_engine.h", "cz_sort.cuh"]
-BINARIES = {"cheese": "cli_cheese.cpp"}
+LIB_SOURCES = ["cz_search.cu", "cz_tcount.cu", "cz_spec.cpp", "cz_capi.cpp"]
+HEADERS = ["cz_common.h", "cz_spec.h", "cz_engine.h", "cz_sort.cuh", "cz_tcount.h"]
+BINARIES = {"cheese": "cli_cheese.cpp", "tcount": "cli_tcount.cpp"}
 
 
 def _stale(out, deps):

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <string>
@@ -9,9 +10,10 @@
 #include "../../include/cheese_b200.h"
 #include "cz_engine.h"
 #include "cz_spec.h"
+#include "cz_tcount.h"
 
 struct cz_spec { cz::HostSpec hs; };
-struct cz_engine { cz::Engine *e; };
+struct cz_engine { cz::Engine *e; cz::TcountContext *tc; };
 
 namespace {
 void put_err(char *err, size_t n, const std::string &m) {
@@ -65,7 +67,7 @@ int cz_engine_create(int device, cz_engine **out, char *err, size_t errlen) {
     return CZ_ERR_CUDA;
   }
   try {
-    cz_engine *e = new cz_engine{new cz::Engine(device)};
+    cz_engine *e = new cz_engine{new cz::Engine(device), nullptr};
     *out = e;
     return 0;
   } catch (const std::exception &ex) {
@@ -76,6 +78,7 @@ int cz_engine_create(int device, cz_engine **out, char *err, size_t errlen) {
 
 void cz_engine_destroy(cz_engine *engine) {
   if (!engine) return;
+  if (engine->tc) cz::tcount_context_destroy(engine->tc);
   delete engine->e;
   delete engine;
 }
@@ -202,6 +205,66 @@ int cz_int32_peak(cz_engine *engine, double *ops_per_s) {
   } catch (const std::exception &) {
     return CZ_ERR_CUDA;
   }
+}
+
+void cz_tcount_options_default(cz_tcount_options *opt) {
+  if (!opt) return;
+  opt->table_k = 4; opt->maxt = 16; opt->cache_dir = "build";
+}
+
+int cz_tspec_check(const char *tspec, size_t len, int *n, char *err, size_t errlen) {
+  cz::TSpec sp;
+  std::string msg;
+  const int rc = cz::parse_tspec(tspec ? tspec : "", tspec ? len : 0, sp, msg);
+  if (n) *n = rc ? 0 : sp.n;
+  if (err && errlen) put_err(err, errlen, msg);
+  return rc;
+}
+
+int cz_tcount(cz_engine *engine, const char *tspec, size_t len, const cz_tcount_options *opt,
+              cz_tcount_level_fn on_level, void *user, cz_tcount_result *out) {
+  if (!engine || !out) return CZ_ERR_USAGE;
+  std::memset(out, 0, sizeof *out);
+  cz_tcount_options o;
+  cz_tcount_options_default(&o);
+  if (opt) o = *opt;
+  cz::TSpec sp;
+  std::string err;
+  int rc = cz::parse_tspec(tspec ? tspec : "", tspec ? len : 0, sp, err);
+  if (rc) { out->rc = rc; put_err(out->error, sizeof out->error, err); return rc; }
+  if (o.table_k < 0 || o.table_k > 32 || o.maxt < 0 || o.maxt > 63) {
+    out->rc = CZ_ERR_USAGE;
+    put_err(out->error, sizeof out->error, "table depth or max T-count out of range");
+    return CZ_ERR_USAGE;
+  }
+  cz::TcOptions to;
+  to.table_k = o.table_k; to.maxt = o.maxt;
+  to.use_cache = o.cache_dir != nullptr;
+  if (o.cache_dir) to.cache_dir = o.cache_dir;
+  cz::TcResult r;
+  try {
+    if (!engine->tc) engine->tc = cz::tcount_context_create(engine->e->device(), engine->e->stream());
+    rc = cz::tcount_run(engine->tc, sp, to, [&](const cz::TcLevel &L) {
+      if (!on_level) return;
+      cz_tcount_level l;
+      l.table = L.table; l.t = L.t; l.parents = L.parents; l.children = L.children; l.cosets = L.cosets;
+      l.fresh = L.fresh; l.seconds = L.seconds;
+      on_level(user, &l);
+    }, r);
+  } catch (const std::exception &ex) {
+    r.error = ex.what();
+    rc = CZ_ERR_CUDA;
+  }
+  out->rc = rc;
+  out->tcount = r.tcount; out->split_j = r.split_j; out->split_c = r.split_c; out->maxt = r.maxt;
+  out->nrot = (int)std::min<size_t>(r.rotations.size(), CZ_TCOUNT_MAXROT);
+  for (int i = 0; i < out->nrot; i++) { out->rot_p[i] = r.rotations[i].first; out->rot_inv[i] = r.rotations[i].second; }
+  out->table_cosets = r.table_cosets; out->table_levels = r.table_levels;
+  out->table_loaded = r.table_loaded; out->table_built = r.table_built; out->table_resident = r.table_resident;
+  out->table_seconds = r.table_seconds; out->total_seconds = r.total_seconds; out->kernel_launches = r.launches;
+  put_err(out->table_path, sizeof out->table_path, r.table_path);
+  put_err(out->error, sizeof out->error, r.error);
+  return rc;
 }
 
 const char *cz_version(void) { return "cheese_b200 0.1 (sm_100a)"; }

@@ -8,6 +8,7 @@
 #include <cstdint>
 
 namespace cz {
+namespace {   // each translation unit that sorts gets its own copy of these kernels
 
 constexpr int SORT_THREADS = 256;
 constexpr int SORT_ITEMS = 16;
@@ -180,4 +181,5 @@ inline bool radix_sort(uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1, s
   return flip;
 }
 
+}  // namespace
 }  // namespace cz

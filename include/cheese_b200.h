@@ -126,6 +126,53 @@ void *cz_engine_stream(cz_engine *engine);
  * register-resident IMAD loop timed with CUDA events. The denominator of the level kernel's roofline. */
 int cz_int32_peak(cz_engine *engine, double *ops_per_s);
 
+/* ---------------- T-count (the reference's build/tcount, src/tcount.cu) ---------------- */
+/* flags of `tcount TSPEC [--table K] [--max T]` (tcount.cu:452-465) and the table cache directory: the table of
+ * (n, K) is cached in <cache_dir>/tcount-table-n<n>-k<K>.cz.bin; a reference-written
+ * <cache_dir>/tcount-table-n<n>-k<K>.bin is read too (its tree is used, its keys recomputed). */
+typedef struct {
+  int table_k;            /* --table K (default 4) */
+  int maxt;               /* --max T (default 16) */
+  const char *cache_dir;  /* default "build"; NULL: no cache */
+} cz_tcount_options;
+void cz_tcount_options_default(cz_tcount_options *opt);
+
+/* one JSON line of grow() (tcount.cu:391-392) */
+typedef struct {
+  int table;              /* 1: "dir": "table" (table build); 0: "dir": "search" */
+  int t;
+  int64_t parents, children, cosets, fresh;   /* fresh = the "new" field */
+  double seconds;
+} cz_tcount_level;
+typedef void (*cz_tcount_level_fn)(void *user, const cz_tcount_level *level);
+
+#define CZ_TCOUNT_MAXROT 64
+typedef struct {
+  int rc;                 /* 0 found, 1 none with T-count <= maxt, 2 spec, 3 usage, 4 overflow, 5 CUDA */
+  int tcount;             /* rc 0: the optimal T-count (up to global phase) */
+  int split_j, split_c;   /* levels from the search and from the table */
+  int maxt;
+  int nrot;               /* U = X_1 ... X_t C: rotation p = rot_p[i], X = R(P_p) (rot_inv 0) or R(P_p)^-1 (1) */
+  int rot_p[CZ_TCOUNT_MAXROT], rot_inv[CZ_TCOUNT_MAXROT];
+  int64_t table_cosets;   /* cosets in the table (all levels) */
+  int table_levels;
+  int table_loaded, table_built, table_resident;   /* where the table came from this call */
+  double table_seconds, total_seconds;
+  int64_t kernel_launches;
+  char table_path[256];
+  char error[256];
+} cz_tcount_result;
+
+/* Parse a tcount-spec without touching the device: 0 and the qubit count in *n, or 2 (not a tcount spec, unknown
+ * field, short matrix: the exits of tcount.cu's read_spec, :434-450) / 3 (n outside 1..3) with the message. */
+int cz_tspec_check(const char *tspec, size_t len, int *n, char *err, size_t errlen);
+
+/* Optimal T-count of the unitary whose tcount-spec (the grammar of tcount.cu:434-450, written by
+ * python/cheese/tcount.py:157-168) is given (replaces tcount.cu's main, :452-532). The engine keeps each (n, K)
+ * table resident in device memory after its first use. */
+int cz_tcount(cz_engine *engine, const char *tspec, size_t len, const cz_tcount_options *opt,
+              cz_tcount_level_fn on_level, void *user, cz_tcount_result *out);
+
 /* The library version string and the CUDA architecture it was compiled for ("sm_100a"). */
 const char *cz_version(void);
 
