@@ -60,6 +60,25 @@ class TcResult(C.Structure):
 
 TC_LEVEL_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(TcLevel))
 
+
+class CliffTableInfo(C.Structure):
+    _fields_ = [("n", C.c_int), ("order", C.c_int64), ("elements", C.c_int64), ("max_distance", C.c_int),
+                ("per_distance", C.c_int64 * 32), ("built", C.c_int), ("seconds", C.c_double)]
+
+
+class CliffResult(C.Structure):
+    _fields_ = [("rc", C.c_int), ("clifford_gates", C.c_int), ("clifford_gates_before", C.c_int),
+                ("t_gates", C.c_int), ("seconds", C.c_double), ("table", CliffTableInfo),
+                ("kernel_launches", C.c_int64), ("text_len", C.c_size_t), ("error", C.c_char * 256)]
+
+
+CLIFF_STEP_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.c_int64, C.c_int)
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("nq", C.c_int), ("jobs", C.c_int), ("running", C.c_int), ("frontier", C.c_int64),
+                ("steps", C.c_int64), ("kernel_launches", C.c_int64), ("device_bytes", C.c_int64)]
+
 # every C entry point of include/cheese_b200.h with its ctypes signature
 SIGNATURES = {
     "cz_spec_parse": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
@@ -83,6 +102,21 @@ SIGNATURES = {
     "cz_tspec_check": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(C.c_int), C.c_char_p, C.c_size_t]),
     "cz_tcount": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(TcOptions), TC_LEVEL_FN, C.c_void_p,
                             C.POINTER(TcResult)]),
+    "cz_clifford_table": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(CliffTableInfo), C.c_char_p, C.c_size_t]),
+    "cz_clifford_dist": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.c_size_t, C.POINTER(C.c_int)]),
+    "cz_clifford_element": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.c_size_t,
+                                      C.POINTER(C.c_uint64)]),
+    "cz_cliffjob_check": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_char_p,
+                                    C.c_size_t]),
+    "cz_cliffopt": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.c_int, CLIFF_STEP_FN, C.c_void_p, C.c_char_p,
+                              C.c_size_t, C.POINTER(CliffResult)]),
+    "cz_batch_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "cz_batch_destroy": (None, [C.c_void_p]),
+    "cz_batch_submit": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Options)]),
+    "cz_batch_step": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "cz_batch_info_get": (C.c_int, [C.c_void_p, C.POINTER(BatchInfo)]),
+    "cz_batch_done": (C.c_int, [C.c_void_p, C.c_int]),
+    "cz_batch_result": (C.c_int, [C.c_void_p, C.c_int, LEVEL_FN, C.c_void_p, C.POINTER(Result)]),
     "cz_version": (C.c_char_p, []),
 }
 
@@ -210,6 +244,60 @@ class Engine:
         out["table_path"] = res.table_path.decode()
         return rc, levels, out
 
+    def clifford_table(self, n):
+        """the resident BFS table of the n-qubit Clifford group: info dict (per_distance as a list)"""
+        info = CliffTableInfo()
+        err = C.create_string_buffer(256)
+        rc = lib().cz_clifford_table(self._h, n, C.byref(info), err, 256)
+        if rc:
+            raise RuntimeError(f"cz_clifford_table failed ({rc}): {err.value.decode()}")
+        d = {k: getattr(info, k) for k, _ in CliffTableInfo._fields_ if k != "per_distance"}
+        d["per_distance"] = [info.per_distance[i] for i in range(info.max_distance + 1)]
+        return d
+
+    def clifford_dist(self, n, tableaux):
+        m = len(tableaux)
+        arr = (C.c_uint64 * max(m, 1))(*tableaux)
+        out = (C.c_int * max(m, 1))()
+        rc = lib().cz_clifford_dist(self._h, n, arr, m, out)
+        if rc:
+            raise RuntimeError(f"cz_clifford_dist failed: {rc}")
+        return list(out[:m])
+
+    def clifford_element(self, n, indices):
+        m = len(indices)
+        arr = (C.c_uint64 * max(m, 1))(*indices)
+        out = (C.c_uint64 * max(m, 1))()
+        rc = lib().cz_clifford_element(self._h, n, arr, m, out)
+        if rc:
+            raise RuntimeError(f"cz_clifford_element failed: {rc}")
+        return list(out[:m])
+
+    def cliffopt(self, job, beam=16, on_step=None):
+        """`cliffopt JOB --beam B`: (rc, result dict, output lines after the JSON line, step tuples)"""
+        if isinstance(job, str):
+            job = job.encode()
+        steps = []
+
+        def cb(_u, j, placements, best):
+            steps.append((j, placements, best))
+            if on_step:
+                on_step(j, placements, best)
+
+        cap = 1 << 16
+        while True:
+            buf = C.create_string_buffer(cap)
+            res = CliffResult()
+            steps.clear()
+            rc = lib().cz_cliffopt(self._h, job, len(job), beam, CLIFF_STEP_FN(cb), None, buf, cap, C.byref(res))
+            if rc or res.text_len < cap:
+                break
+            cap = res.text_len + 1
+        out = {k: getattr(res, k) for k, _ in CliffResult._fields_ if k not in ("table", "error")}
+        out["error"] = res.error.decode()
+        out["table_built"] = res.table.built
+        return rc, out, buf.value.decode().splitlines(), list(steps)
+
     def search(self, spec, depth=-1, dedupe=True, sym=True, store64=False, profile=False, on_level=None):
         """run `cheese SPEC [--depth D] [--no-dedupe] [--no-sym]`; returns a SearchOutcome"""
         if not isinstance(spec, Spec):
@@ -228,6 +316,67 @@ class Engine:
         res = Result()
         rc = lib().cz_search(self._h, spec._h, C.byref(opt), LEVEL_FN(cb), None, C.byref(res))
         return SearchOutcome(spec, rc, levels, res)
+
+
+class Batch:
+    """a batch session of one qubit count on an engine: submit specs, step, collect SearchOutcomes"""
+
+    def __init__(self, engine, nq):
+        self.engine = engine
+        self._h = C.c_void_p()
+        rc = lib().cz_batch_create(engine._h, nq, C.byref(self._h))
+        if rc:
+            raise RuntimeError(f"cz_batch_create failed: {rc}")
+        self.specs = {}
+
+    def submit(self, spec, depth=-1, dedupe=True, sym=True, store64=False):
+        if not isinstance(spec, Spec):
+            spec = Spec(spec)
+        opt = Options(depth, int(dedupe), int(sym), int(store64), 0)
+        jid = lib().cz_batch_submit(self._h, spec._h, C.byref(opt))
+        if jid < 0:
+            raise RuntimeError(f"cz_batch_submit failed: {-jid}")
+        self.specs[jid] = spec
+        return jid
+
+    def step(self):
+        r = C.c_int()
+        rc = lib().cz_batch_step(self._h, C.byref(r))
+        if rc:
+            raise RuntimeError(f"cz_batch_step failed: {rc}")
+        return r.value
+
+    def run(self):
+        while self.step():
+            pass
+
+    def info(self):
+        i = BatchInfo()
+        lib().cz_batch_info_get(self._h, C.byref(i))
+        return {k: getattr(i, k) for k, _ in BatchInfo._fields_}
+
+    def done(self, jid):
+        return bool(lib().cz_batch_done(self._h, jid))
+
+    def result(self, jid):
+        levels = []
+
+        def cb(_user, p):
+            s = p.contents
+            d = {k: getattr(s, k) for k, _ in LevelStats._fields_}
+            d["proved_unsat"] = bool(d["proved_unsat"])
+            levels.append(d)
+
+        res = Result()
+        rc = lib().cz_batch_result(self._h, jid, LEVEL_FN(cb), None, C.byref(res))
+        if rc:
+            raise RuntimeError(f"cz_batch_result failed: {rc}")
+        return SearchOutcome(self.specs[jid], res.rc, levels, res)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.cz_batch_destroy(self._h)
+            self._h = None
 
 
 class SearchOutcome:

@@ -5,6 +5,8 @@
 Outputs (git-ignored, carried to the GPU host with the working tree):
     cheese_b200/lib/libcheese_b200.so     the C ABI of include/cheese_b200.h
     cheese_b200/bin/cheese                drop-in for the reference's build/cheese
+    cheese_b200/bin/tcount                drop-in for the reference's build/tcount
+    cheese_b200/bin/cliffopt              drop-in for the reference's build/cliffopt
 """
 import os
 import subprocess
@@ -21,9 +23,9 @@ HOSTCXX = os.environ.get("CZ_HOSTCXX", "/usr/bin/g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-ccbin", HOSTCXX, "-Xcompiler", "-fPIC"]
 
-LIB_SOURCES = ["cz_search.cu", "cz_tcount.cu", "cz_spec.cpp", "cz_capi.cpp"]
-HEADERS = ["cz_common.h", "cz_spec.h", "cz_engine.h", "cz_sort.cuh", "cz_tcount.h"]
-BINARIES = {"cheese": "cli_cheese.cpp", "tcount": "cli_tcount.cpp"}
+LIB_SOURCES = ["cz_search.cu", "cz_tcount.cu", "cz_clifford.cu", "cz_spec.cpp", "cz_capi.cpp"]
+HEADERS = ["cz_common.h", "cz_spec.h", "cz_engine.h", "cz_sort.cuh", "cz_tcount.h", "cz_clifford.h", "cz_tableau.h"]
+BINARIES = {"cheese": "cli_cheese.cpp", "tcount": "cli_tcount.cpp", "cliffopt": "cli_cliffopt.cpp"}
 
 
 def _stale(out, deps):

@@ -10,10 +10,12 @@
 #include "../../include/cheese_b200.h"
 #include "cz_engine.h"
 #include "cz_spec.h"
+#include "cz_clifford.h"
 #include "cz_tcount.h"
 
 struct cz_spec { cz::HostSpec hs; };
-struct cz_engine { cz::Engine *e; cz::TcountContext *tc; };
+struct cz_batch { cz::BatchSession *b; };
+struct cz_engine { cz::Engine *e; cz::TcountContext *tc; cz::CliffordContext *cl; };
 
 namespace {
 void put_err(char *err, size_t n, const std::string &m) {
@@ -67,7 +69,7 @@ int cz_engine_create(int device, cz_engine **out, char *err, size_t errlen) {
     return CZ_ERR_CUDA;
   }
   try {
-    cz_engine *e = new cz_engine{new cz::Engine(device), nullptr};
+    cz_engine *e = new cz_engine{new cz::Engine(device), nullptr, nullptr};
     *out = e;
     return 0;
   } catch (const std::exception &ex) {
@@ -79,6 +81,7 @@ int cz_engine_create(int device, cz_engine **out, char *err, size_t errlen) {
 void cz_engine_destroy(cz_engine *engine) {
   if (!engine) return;
   if (engine->tc) cz::tcount_context_destroy(engine->tc);
+  if (engine->cl) cz::clifford_context_destroy(engine->cl);
   delete engine->e;
   delete engine;
 }
@@ -147,6 +150,110 @@ int cz_search(cz_engine *engine, const cz_spec *spec, const cz_options *opt, cz_
   out->children_full = r.children_full;
   put_err(out->error, sizeof out->error, r.error);
   return rc;
+}
+
+namespace {
+void fill_result(const cz::SearchResult &r, cz_result *out) {
+  out->rc = r.rc;
+  out->depth0 = r.depth0;
+  out->found_len = (int)r.circuit.size();
+  for (size_t i = 0; i < r.circuit.size() && i < CZ_MAX_DEPTH; i++) out->found[i] = r.circuit[i];
+  out->n_found = r.n_found;
+  out->nsym = r.nsym;
+  out->store64 = r.store64;
+  out->levels = r.levels;
+  out->prefixes = r.prefixes;
+  out->kernel_launches = r.launches;
+  out->t_evals = r.t_evals;
+  out->children = r.children;
+  out->expand_ms = r.expand_ms;
+  out->dedupe_ms = r.dedupe_ms;
+  out->total_ms = r.total_ms;
+  out->expand_launches = r.expand_launches;
+  out->h2d_bytes = r.h2d_bytes;
+  out->d2h_bytes = r.d2h_bytes;
+  out->children_full = r.children_full;
+  put_err(out->error, sizeof out->error, r.error);
+}
+}  // namespace
+
+int cz_batch_create(cz_engine *engine, int nq, cz_batch **out) {
+  if (!engine || !out || nq < 1 || nq > 3) return CZ_ERR_USAGE;
+  *out = nullptr;
+  try {
+    *out = new cz_batch{new cz::BatchSession(*engine->e, nq)};
+    return 0;
+  } catch (const std::exception &) {
+    return CZ_ERR_CUDA;
+  }
+}
+
+void cz_batch_destroy(cz_batch *batch) {
+  if (!batch) return;
+  delete batch->b;
+  delete batch;
+}
+
+int cz_batch_submit(cz_batch *batch, const cz_spec *spec, const cz_options *opt) {
+  if (!batch || !spec) return -CZ_ERR_USAGE;
+  const cz::HostSpec &hs = spec->hs;
+  if (hs.states || hs.n != batch->b->nq()) return -CZ_ERR_USAGE;
+  cz_options o;
+  cz_options_default(&o);
+  if (opt) o = *opt;
+  const int depth = o.depth >= 0 ? o.depth : hs.depth;
+  if (depth > CZ_MAX_DEPTH) return -CZ_ERR_USAGE;
+  cz::Options eo;
+  eo.depth = depth; eo.dedupe = o.dedupe != 0; eo.sym = o.sym != 0; eo.store64 = o.store64; eo.profile = false;
+  try {
+    return batch->b->submit(hs, eo);
+  } catch (const std::exception &) {
+    return -CZ_ERR_CUDA;
+  }
+}
+
+int cz_batch_step(cz_batch *batch, int *running) {
+  if (!batch) return CZ_ERR_USAGE;
+  try {
+    const int r = batch->b->step();
+    if (running) *running = r;
+    return 0;
+  } catch (const std::exception &) {
+    return CZ_ERR_CUDA;
+  }
+}
+
+int cz_batch_info_get(const cz_batch *batch, cz_batch_info *out) {
+  if (!batch || !out) return CZ_ERR_USAGE;
+  out->nq = batch->b->nq();
+  out->jobs = batch->b->jobs();
+  out->running = batch->b->running();
+  out->frontier = batch->b->frontier();
+  out->steps = batch->b->steps();
+  out->kernel_launches = batch->b->launches();
+  out->device_bytes = (int64_t)batch->b->device_bytes();
+  return 0;
+}
+
+int cz_batch_done(const cz_batch *batch, int job) {
+  if (!batch || job < 0 || job >= batch->b->jobs()) return 0;
+  return batch->b->job(job).done ? 1 : 0;
+}
+
+int cz_batch_result(const cz_batch *batch, int job, cz_level_fn on_level, void *user, cz_result *out) {
+  if (!batch || !out || job < 0 || job >= batch->b->jobs()) return CZ_ERR_USAGE;
+  std::memset(out, 0, sizeof *out);
+  const cz::BatchJob &j = batch->b->job(job);
+  if (!j.done) return CZ_ERR_USAGE;
+  for (const cz::LevelStats &L : j.levels) {
+    if (!on_level) break;
+    cz_level_stats s;
+    s.t = L.t; s.parents = L.parents; s.prefixes = L.prefixes; s.cut_w3 = L.cut_w3; s.cut_lb = L.cut_lb;
+    s.survivors = L.survivors; s.distinct = L.distinct; s.proved_unsat = L.proved_unsat; s.seconds = L.seconds;
+    on_level(user, &s);
+  }
+  fill_result(j.res, out);
+  return 0;
 }
 
 int cz_search_text(cz_engine *engine, const char *spec_text, size_t len, const cz_options *opt, cz_level_fn on_level,
@@ -265,6 +372,96 @@ int cz_tcount(cz_engine *engine, const char *tspec, size_t len, const cz_tcount_
   put_err(out->table_path, sizeof out->table_path, r.table_path);
   put_err(out->error, sizeof out->error, r.error);
   return rc;
+}
+
+int cz_cliffjob_check(const char *job, size_t len, int *n, int *t_gates, char *err, size_t errlen) {
+  cz::CliffJob J;
+  std::string msg;
+  const int rc = cz::parse_cliff_job(job ? job : "", job ? len : 0, J, msg);
+  if (n) *n = rc ? 0 : J.n;
+  if (t_gates) *t_gates = rc ? 0 : (int)J.tq.size();
+  if (err && errlen) put_err(err, errlen, msg);
+  return rc;
+}
+
+namespace {
+void fill_table_info(const cz::CliffTableInfo &i, cz_clifford_table_info *o) {
+  std::memset(o, 0, sizeof *o);
+  o->n = i.n; o->order = i.order; o->elements = i.elements; o->max_distance = i.max_distance;
+  for (int d = 0; d < 32; d++) o->per_distance[d] = i.per_distance[d];
+  o->built = i.built; o->seconds = i.seconds;
+}
+cz::CliffordContext *cliff_ctx(cz_engine *engine) {
+  if (!engine->cl) engine->cl = cz::clifford_context_create(engine->e->device(), engine->e->stream());
+  return engine->cl;
+}
+}  // namespace
+
+int cz_clifford_table(cz_engine *engine, int n, cz_clifford_table_info *out, char *err, size_t errlen) {
+  if (!engine) return CZ_ERR_USAGE;
+  try {
+    cz::CliffTableInfo info;
+    std::string e;
+    const int rc = cz::clifford_table(cliff_ctx(engine), n, info, e);
+    if (rc) { put_err(err, errlen, e); return rc; }
+    if (out) fill_table_info(info, out);
+    return 0;
+  } catch (const std::exception &ex) {
+    put_err(err, errlen, ex.what());
+    return CZ_ERR_CUDA;
+  }
+}
+
+int cz_cliffopt(cz_engine *engine, const char *job, size_t len, int beam, cz_cliffopt_step_fn on_step, void *user,
+                char *text, size_t text_cap, cz_cliffopt_result *out) {
+  if (!engine || !out) return CZ_ERR_USAGE;
+  std::memset(out, 0, sizeof *out);
+  cz::CliffJob J;
+  std::string err;
+  int rc = cz::parse_cliff_job(job ? job : "", job ? len : 0, J, err);
+  if (rc) { out->rc = rc; put_err(out->error, sizeof out->error, err); return rc; }
+  cz::CliffOptResult r;
+  try {
+    rc = cz::cliffopt_run(cliff_ctx(engine), J, beam, [&](int j, const cz::CliffStep &st) {
+      if (on_step) on_step(user, j, st.placements, st.best_partial);
+    }, r);
+  } catch (const std::exception &ex) {
+    r.error = ex.what();
+    rc = CZ_ERR_CUDA;
+  }
+  out->rc = rc;
+  out->clifford_gates = r.clifford_gates; out->clifford_gates_before = r.before; out->t_gates = r.t_gates;
+  out->seconds = r.seconds;
+  fill_table_info(r.table, &out->table);
+  out->kernel_launches = r.launches;
+  out->text_len = r.text.size();
+  if (text && text_cap) {
+    const size_t m = std::min(text_cap - 1, r.text.size());
+    std::memcpy(text, r.text.data(), m);
+    text[m] = 0;
+  }
+  put_err(out->error, sizeof out->error, r.error);
+  return rc;
+}
+
+int cz_clifford_dist(cz_engine *engine, int n, const uint64_t *tableaux, size_t count, int *out) {
+  if (!engine || (count && (!tableaux || !out))) return CZ_ERR_USAGE;
+  try {
+    std::string e;
+    return cz::clifford_dist(cliff_ctx(engine), n, tableaux, count, out, e);
+  } catch (const std::exception &) {
+    return CZ_ERR_CUDA;
+  }
+}
+
+int cz_clifford_element(cz_engine *engine, int n, const uint64_t *index, size_t count, uint64_t *tableaux) {
+  if (!engine || (count && (!index || !tableaux))) return CZ_ERR_USAGE;
+  try {
+    std::string e;
+    return cz::clifford_element(cliff_ctx(engine), n, index, count, tableaux, e);
+  } catch (const std::exception &) {
+    return CZ_ERR_CUDA;
+  }
 }
 
 const char *cz_version(void) { return "cheese_b200 0.1 (sm_100a)"; }

@@ -79,4 +79,39 @@ class Engine {
   int dev_;
 };
 
+// Many searches of one qubit count advanced together, one level per step, in shared launches (continuous batching):
+// jobs join at the next step after submit and leave when they finish; each job's per-level statistics, exit code
+// and circuit are those of Engine::search on the same spec and options. Jobs the batched kernels do not cover (int64
+// limbs, --no-dedupe, distance-table builds) run through Engine::search inside step().
+struct BatchJob {
+  bool done = false;
+  SearchResult res;
+  std::vector<LevelStats> levels;
+  int joined_step = -1, finished_step = -1;
+  bool plain = false;                  // ran through Engine::search
+};
+
+class BatchSession {
+ public:
+  BatchSession(Engine &engine, int nq);
+  ~BatchSession();
+  BatchSession(const BatchSession &) = delete;
+  BatchSession &operator=(const BatchSession &) = delete;
+  int nq() const;
+  // the job's id; it joins at the next step
+  int submit(const HostSpec &hs, const Options &opt);
+  // one level of every running job (admitting the submitted ones first); returns the jobs still running
+  int step();
+  int running() const;
+  const BatchJob &job(int id) const;
+  int jobs() const;
+  long long frontier() const;          // nodes in the batch frontier
+  long long launches() const;          // kernels launched by the session
+  long long steps() const;
+  size_t device_bytes() const;         // device memory held by the session's buffers
+  struct Impl;
+ private:
+  Impl *impl_;
+};
+
 }  // namespace cz

@@ -27,6 +27,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <stdexcept>
 
@@ -657,6 +658,151 @@ __device__ __forceinline__ void init_weights(uint64_t *W1, uint64_t *W2, int E) 
 }
 
 // ---------------- the level kernel ----------------
+// per-warp tallies of one job's children, flushed to that job's DevStats
+struct WarpTally {
+  unsigned long long w2 = 0, w3 = 0, dead = 0, alive = 0, found = 0, teval = 0, child = 0, full = 0;
+  unsigned long long first = ~0ULL;
+  bool ovf = false;
+  __device__ __forceinline__ void flush(DevStats *st, int lane) {
+    if (lane == 0) {
+      if (w2) atomicAdd(&st->w2, w2);
+      if (w3) atomicAdd(&st->w3, w3);
+      if (dead) atomicAdd(&st->dead, dead);
+      if (alive) atomicAdd(&st->alive, alive);
+      if (found) { atomicAdd(&st->found, found); atomicMin(&st->first_found, first); }
+      if (teval) atomicAdd(&st->t_evals, teval);
+      if (child) atomicAdd(&st->children, child);
+      if (full) atomicAdd(&st->full, full);
+      if (ovf) st->ovf = 1;
+    }
+    *this = WarpTally{};
+  }
+};
+template <typename ST> struct ExpandOut {
+  DevStats *st;                    // survivor slot counter and overflow flag
+  unsigned long long cap;
+  uint64_t *sh1, *sh2, *sidx;
+  Z4<ST> *sR;
+  NodeMeta *smeta;
+};
+
+// every child of parent p (residual already in P): window rules, exact prechecks, child residual, bounds, class key,
+// survivor append. sp is the parent's spec (kernel parameter or a shared copy), sps its shared-memory address for
+// the out-of-line helpers; child index = p * GS + g.
+template <int NQ, typename ST>
+__device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *sps, const uint8_t (*perm)[8],
+                                              unsigned conjmask, const uint64_t *W1, const uint64_t *W2,
+                                              const Z4<ST> *P, Z4<ST> *C, unsigned long long p, const NodeMeta pm,
+                                              int rem, bool keep, int GS, const ExpandOut<ST> &o, WarpTally &c,
+                                              int lane) {
+  constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
+  const int G = sp.G;
+  const int g1 = pm.g1 == 0xff ? -1 : pm.g1, g2 = pm.g2 == 0xff ? -1 : pm.g2;
+  const int kP = pm.k, TP = pm.T, c2P = pm.c2, hsP = (pm.hsn & 1) ? 2 : 0, ntP = (pm.hsn >> 1) & 7;
+  const int suppP = __popc(ntP);
+  const bool pre_ok = sp.standard && kP < INHERIT_KMAX;
+  unsigned tcache = 0;                       // per qubit: 1 + T bound of its odd-diagonal child (0: unknown)
+  for (int g = 0; g < G; g++) {
+    if (g1 >= 0 && __ldg(&sp.bad2[g1 * G + g])) { c.w2++; continue; }
+    if (g2 >= 0) {
+      const uint32_t tri = ((uint32_t)g2 * G + (uint32_t)g1) * G + (uint32_t)g;
+      if ((__ldg(&sp.bad3[tri >> 5]) >> (tri & 31)) & 1) { c.w3++; continue; }
+    }
+    c.child++;
+    const uint8_t fl = sp.gflags[g];
+    const int gm = sp.gmask[g], nq = sp.gnq[g], q0 = sp.gq[g][0];
+    const int tc = (int)((tcache >> (8 * q0)) & 0xff) - 1;
+    if (pre_ok) {
+      // lower bounds on the child's bounds from the parent's: k drops by at most the gate's sqrt2 exponent;
+      // H structure, T and CX bounds are unchanged by monomial-affine / Clifford / one-qubit gates; an odd
+      // diagonal changes T by at most 1; a gate of Schmidt rank 2 changes the CX bound by at most 1; support
+      // changes only on the gate's qubits. combine is monotone in every argument, so exceeding the budget with
+      // these proves the child dead (the goal has all bounds 0 and is never removed here).
+      const int ik = sp.gik[g] > 0 ? sp.gik[g] : 0;
+      int hlo = kP - ik;
+      if ((fl & GF_MONAFF) && hsP > hlo) hlo = hsP;
+      const int tlo = (fl & GF_CLIFFORD) ? TP : ((fl & GF_TDIAG) ? (tc >= 0 ? tc : TP - 1) : 0);
+      const int clo = (fl & GF_ONEQ) ? c2P : ((fl & GF_RANK2) ? c2P - 1 : 0);
+      const int slo = suppP - nq;
+      if (combine(hlo > 0 ? hlo : 0, tlo > 0 ? tlo : 0, clo > 0 ? clo : 0, slo > 0 ? slo : 0) > rem) {
+        c.dead++;
+        continue;
+      }
+    }
+    bool ovf;
+    c.full++;
+    const int k = warp_child<NQ, ST>(P, C, g, kP, sp, sps, lane, ovf);
+    if (ovf) { c.ovf = true; continue; }
+    const bool need_b = sp.standard != 0;
+    const bool need_hs = need_b && !(fl & GF_MONAFF);
+    // the child is the goal only if the parent equals the gate, i.e. acts on no other qubit
+    const Cheap ch = warp_cheap<NQ, ST>(C, k, sp, lane, (ntP & ~gm) == 0 || !need_b, need_hs, need_b ? gm : 0, ntP);
+    if (ch.goal) {
+      if (sp.nogoal) c.dead++;
+      else { c.found++; const unsigned long long oi = p * (unsigned long long)GS + g; if (oi < c.first) c.first = oi; }
+      continue;
+    }
+    const bool inheritT = (fl & GF_CLIFFORD) && k <= INHERIT_KMAX && kP <= INHERIT_KMAX;
+    const bool cacheT = (fl & GF_TDIAG) && k <= INHERIT_KMAX;
+    bool alive = true;
+    int T = 0, c2 = 0, hs = 0, needs = 0;
+    if (sp.lite) {
+      if (k > rem) alive = false;
+      else {
+        if (inheritT) T = TP;
+        else if (cacheT && tc >= 0) T = tc;
+        else {
+          T = ptm_bound<NQ, ST>(C, k, lane); c.teval++;
+          if (cacheT) tcache |= (unsigned)(T + 1) << (8 * q0);
+        }
+        alive = k + (T + sp.tdiv - 1) / sp.tdiv <= rem;
+      }
+    } else if (need_b) {
+      hs = need_hs ? ch.hs : hsP;
+      const int h = k > hs ? k : hs;
+      const int supp = __popc(ch.ntriv);
+      if (fl & GF_ONEQ) { c2 = c2P; needs = pm.needs; }
+      else c2 = warp_cx_bound<NQ, ST>(C, *sps, lane, gm, pm.needs, needs);
+      if (combine(h, 0, c2, supp) > rem) alive = false;
+      else {
+        if (inheritT) T = TP;
+        else if (cacheT && tc >= 0) T = tc;
+        else {
+          T = ptm_bound<NQ, ST>(C, k, lane); c.teval++;
+          if (cacheT) tcache |= (unsigned)(T + 1) << (8 * q0);
+        }
+        alive = combine(h, T, c2, supp) <= rem;
+      }
+    }
+    if (!alive) { c.dead++; continue; }
+    c.alive++;
+    if (!keep) continue;
+    uint64_t k1, k2;
+    warp_class_key<NQ, ST>(C, k, sp.nsym, conjmask, perm, W1, W2, lane, k1, k2);
+    unsigned long long slot = 0;
+    if (lane == 0) slot = atomicAdd(&o.st->n_surv, 1ULL);
+    slot = __shfl_sync(FULL, slot, 0);
+    if (slot < o.cap) {
+#pragma unroll
+      for (int j = 0; j < EPL; j++) {
+        const int e = lane + 32 * j;
+        if (e < E) o.sR[slot * E + e] = C[e];
+      }
+      if (lane == 0) {
+        o.sh1[slot] = k1; o.sh2[slot] = k2; o.sidx[slot] = p * (unsigned long long)GS + g;
+        NodeMeta nm;
+        nm.k = (int16_t)k; nm.T = (uint8_t)(T > 255 ? 255 : T); nm.c2 = (uint8_t)c2; nm.g1 = (uint8_t)g; nm.g2 = pm.g1;
+        nm.hsn = (uint8_t)((hs == 2 ? 1 : 0) | ((need_b ? ch.ntriv : 0) << 1));
+        nm.needs = (uint8_t)needs;
+        o.smeta[slot] = nm;
+      }
+    } else if (lane == 0) {
+      o.st->surv_overflow = 1;
+    }
+    __syncwarp();
+  }
+}
+
 template <int NQ, typename ST>
 __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, const ExpandArgs<ST> a) {
   constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
@@ -668,12 +814,10 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, 
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   Z4<ST> *P = sm.P[w], *C = sm.C[w];
-  const int G = sp.G;
   unsigned conjmask = 0;
   for (int i = 0; i < sp.nsym; i++) conjmask |= (unsigned)(sp.symconj[i] != 0) << i;
-  unsigned long long n_w2 = 0, n_w3 = 0, n_dead = 0, n_alive = 0, n_found = 0, n_teval = 0, n_child = 0, n_full = 0;
-  unsigned long long first = ~0ULL;
-  bool ovf_any = false;
+  const ExpandOut<ST> o{a.st, a.cap, a.sh1, a.sh2, a.sidx, a.sR, a.smeta};
+  WarpTally c;
   for (;;) {
     unsigned long long p = 0;
     if (lane == 0) p = atomicAdd(&a.st->work, 1ULL);
@@ -686,124 +830,79 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, 
     }
     const NodeMeta pm = a.meta[p];
     __syncwarp();
-    const int g1 = pm.g1 == 0xff ? -1 : pm.g1, g2 = pm.g2 == 0xff ? -1 : pm.g2;
-    const int kP = pm.k, TP = pm.T, c2P = pm.c2, hsP = (pm.hsn & 1) ? 2 : 0, ntP = (pm.hsn >> 1) & 7;
-    const int suppP = __popc(ntP);
-    const bool pre_ok = sp.standard && kP < INHERIT_KMAX;
-    unsigned tcache = 0;                       // per qubit: 1 + T bound of its odd-diagonal child (0: unknown)
-    for (int g = 0; g < G; g++) {
-      if (g1 >= 0 && __ldg(&sp.bad2[g1 * G + g])) { n_w2++; continue; }
-      if (g2 >= 0) {
-        const uint32_t tri = ((uint32_t)g2 * G + (uint32_t)g1) * G + (uint32_t)g;
-        if ((__ldg(&sp.bad3[tri >> 5]) >> (tri & 31)) & 1) { n_w3++; continue; }
-      }
-      n_child++;
-      const int rem = a.rem;
-      const uint8_t fl = sp.gflags[g];
-      const int gm = sp.gmask[g], nq = sp.gnq[g], q0 = sp.gq[g][0];
-      const int tc = (int)((tcache >> (8 * q0)) & 0xff) - 1;
-      if (pre_ok) {
-        // lower bounds on the child's bounds from the parent's: k drops by at most the gate's sqrt2 exponent;
-        // H structure, T and CX bounds are unchanged by monomial-affine / Clifford / one-qubit gates; an odd
-        // diagonal changes T by at most 1; a gate of Schmidt rank 2 changes the CX bound by at most 1; support
-        // changes only on the gate's qubits. combine is monotone in every argument, so exceeding the budget with
-        // these proves the child dead (the goal has all bounds 0 and is never removed here).
-        const int ik = sp.gik[g] > 0 ? sp.gik[g] : 0;
-        int hlo = kP - ik;
-        if ((fl & GF_MONAFF) && hsP > hlo) hlo = hsP;
-        const int tlo = (fl & GF_CLIFFORD) ? TP : ((fl & GF_TDIAG) ? (tc >= 0 ? tc : TP - 1) : 0);
-        const int clo = (fl & GF_ONEQ) ? c2P : ((fl & GF_RANK2) ? c2P - 1 : 0);
-        const int slo = suppP - nq;
-        if (combine(hlo > 0 ? hlo : 0, tlo > 0 ? tlo : 0, clo > 0 ? clo : 0, slo > 0 ? slo : 0) > rem) {
-          n_dead++;
-          continue;
-        }
-      }
-      bool ovf;
-      n_full++;
-      const int k = warp_child<NQ, ST>(P, C, g, kP, sp, &s_sp, lane, ovf);
-      if (ovf) { ovf_any = true; continue; }
-      const bool need_b = sp.standard != 0;
-      const bool need_hs = need_b && !(fl & GF_MONAFF);
-      // the child is the goal only if the parent equals the gate, i.e. acts on no other qubit
-      const Cheap ch = warp_cheap<NQ, ST>(C, k, sp, lane, (ntP & ~gm) == 0 || !need_b, need_hs, need_b ? gm : 0, ntP);
-      if (ch.goal) {
-        if (sp.nogoal) n_dead++;
-        else { n_found++; const unsigned long long o = p * (unsigned long long)G + g; if (o < first) first = o; }
-        continue;
-      }
-      const bool inheritT = (fl & GF_CLIFFORD) && k <= INHERIT_KMAX && kP <= INHERIT_KMAX;
-      const bool cacheT = (fl & GF_TDIAG) && k <= INHERIT_KMAX;
-      bool alive = true;
-      int T = 0, c2 = 0, hs = 0, needs = 0;
-      if (sp.lite) {
-        if (k > rem) alive = false;
-        else {
-          if (inheritT) T = TP;
-          else if (cacheT && tc >= 0) T = tc;
-          else {
-            T = ptm_bound<NQ, ST>(C, k, lane); n_teval++;
-            if (cacheT) tcache |= (unsigned)(T + 1) << (8 * q0);
-          }
-          alive = k + (T + sp.tdiv - 1) / sp.tdiv <= rem;
-        }
-      } else if (need_b) {
-        hs = need_hs ? ch.hs : hsP;
-        const int h = k > hs ? k : hs;
-        const int supp = __popc(ch.ntriv);
-        if (fl & GF_ONEQ) { c2 = c2P; needs = pm.needs; }
-        else c2 = warp_cx_bound<NQ, ST>(C, s_sp, lane, gm, pm.needs, needs);
-        if (combine(h, 0, c2, supp) > rem) alive = false;
-        else {
-          if (inheritT) T = TP;
-          else if (cacheT && tc >= 0) T = tc;
-          else {
-            T = ptm_bound<NQ, ST>(C, k, lane); n_teval++;
-            if (cacheT) tcache |= (unsigned)(T + 1) << (8 * q0);
-          }
-          alive = combine(h, T, c2, supp) <= rem;
-        }
-      }
-      if (!alive) { n_dead++; continue; }
-      n_alive++;
-      if (!a.keep) continue;
-      uint64_t k1, k2;
-      warp_class_key<NQ, ST>(C, k, sp.nsym, conjmask, sm.perm, sm.W1, sm.W2, lane, k1, k2);
-      unsigned long long slot = 0;
-      if (lane == 0) slot = atomicAdd(&a.st->n_surv, 1ULL);
-      slot = __shfl_sync(FULL, slot, 0);
-      if (slot < a.cap) {
-#pragma unroll
-        for (int j = 0; j < EPL; j++) {
-          const int e = lane + 32 * j;
-          if (e < E) a.sR[slot * E + e] = C[e];
-        }
-        if (lane == 0) {
-          a.sh1[slot] = k1; a.sh2[slot] = k2; a.sidx[slot] = p * (unsigned long long)G + g;
-          NodeMeta nm;
-          nm.k = (int16_t)k; nm.T = (uint8_t)(T > 255 ? 255 : T); nm.c2 = (uint8_t)c2; nm.g1 = (uint8_t)g; nm.g2 = pm.g1;
-          nm.hsn = (uint8_t)((hs == 2 ? 1 : 0) | ((need_b ? ch.ntriv : 0) << 1));
-          nm.needs = (uint8_t)needs;
-          a.smeta[slot] = nm;
-        }
-      } else if (lane == 0) {
-        a.st->surv_overflow = 1;
-      }
-      __syncwarp();
-    }
+    expand_parent<NQ, ST>(sp, &s_sp, sm.perm, conjmask, sm.W1, sm.W2, P, C, p, pm, a.rem, a.keep != 0, sp.G, o, c,
+                          lane);
     __syncwarp();
   }
-  if (lane == 0) {
-    if (n_w2) atomicAdd(&a.st->w2, n_w2);
-    if (n_w3) atomicAdd(&a.st->w3, n_w3);
-    if (n_dead) atomicAdd(&a.st->dead, n_dead);
-    if (n_alive) atomicAdd(&a.st->alive, n_alive);
-    if (n_found) { atomicAdd(&a.st->found, n_found); atomicMin(&a.st->first_found, first); }
-    if (n_teval) atomicAdd(&a.st->t_evals, n_teval);
-    if (n_child) atomicAdd(&a.st->children, n_child);
-    if (n_full) atomicAdd(&a.st->full, n_full);
-    if (ovf_any) a.st->ovf = 1;
+  c.flush(a.st, lane);
+}
+
+// ---------------- the batched level kernel ----------------
+// Many searches of one qubit count in one launch: the frontier is the concatenation of every job's nodes (each
+// job's nodes contiguous, in its own order), fjob gives each node's job, specs[job] its device spec, jt[job] its
+// current level. Child indices are p * 64 + g over the batch frontier, so each job's children keep its own order.
+constexpr int BATCH_GS = 64;
+constexpr int MAXDEPTH_WALK = 48;   // deepest circuit of a batched job
+template <typename ST> struct BatchArgs {
+  long long m;
+  const Z4<ST> *R;
+  const NodeMeta *meta;
+  const uint32_t *fjob;             // job of every frontier node
+  const DevSpec *specs;
+  const int *jt;
+  DevStats *jst;                   // per job
+  DevStats *st;                    // batch-wide: work counter, survivor slots
+  unsigned long long cap;
+  uint64_t *sh1, *sh2, *sidx;
+  Z4<ST> *sR;
+  NodeMeta *smeta;
+};
+
+template <int NQ, typename ST>
+__global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand_batch(const BatchArgs<ST> a) {
+  constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
+  __shared__ Z4<ST> sP[EXP_WARPS][E], sC[EXP_WARPS][E];
+  __shared__ uint64_t W1[E], W2[E];
+  __shared__ DevSpec sps[EXP_WARPS];           // each warp's current job spec
+  init_weights(W1, W2, E);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  Z4<ST> *P = sP[w], *C = sC[w];
+  DevSpec &sp = sps[w];
+  const ExpandOut<ST> o{a.st, a.cap, a.sh1, a.sh2, a.sidx, a.sR, a.smeta};
+  WarpTally c;
+  int job = -1, rem = 0;
+  bool keep = false;
+  unsigned conjmask = 0;
+  for (;;) {
+    unsigned long long p = 0;
+    if (lane == 0) p = atomicAdd(&a.st->work, 1ULL);
+    p = __shfl_sync(FULL, p, 0);
+    if ((long long)p >= a.m) break;
+    const int pj = (int)a.fjob[p];
+    if (pj != job) {                             // another job: flush the tallies, load its spec
+      if (job >= 0) c.flush(a.jst + job, lane);
+      job = pj;
+      __syncwarp();
+      for (int i = lane; i < (int)(sizeof(DevSpec) / 4); i += 32) ((int *)&sp)[i] = ((const int *)(a.specs + job))[i];
+      __syncwarp();
+      const int t = a.jt[job];
+      rem = sp.depth - t;
+      keep = t < sp.depth;
+      conjmask = 0;
+      for (int i = 0; i < sp.nsym; i++) conjmask |= (unsigned)(sp.symconj[i] != 0) << i;
+    }
+#pragma unroll
+    for (int j = 0; j < EPL; j++) {
+      const int e = lane + 32 * j;
+      if (e < E) P[e] = a.R[p * E + e];
+    }
+    const NodeMeta pm = a.meta[p];
+    __syncwarp();
+    expand_parent<NQ, ST>(sp, &sp, sp.symperm, conjmask, W1, W2, P, C, p, pm, rem, keep, BATCH_GS, o, c, lane);
+    __syncwarp();
   }
+  if (job >= 0) c.flush(a.jst + job, lane);
 }
 
 // the root node's bounds (the target itself), inherited or bracketed by its children
@@ -1574,5 +1673,609 @@ int Engine::search(const HostSpec &hs, const Options &opt, const std::function<v
   res.rc = rc;
   return rc;
 }
+
+// ---------------- batched search (continuous batching over many jobs of one qubit count) ----------------
+namespace {
+
+__global__ void k_jst_init(DevStats *jst, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    DevStats z;
+    memset(&z, 0, sizeof z);
+    z.first_found = ~0ULL;
+    jst[i] = z;
+  }
+}
+
+// the roots of newly admitted jobs: one warp each (the bounds of k_root with the job's spec)
+template <int NQ>
+__global__ void k_root_batch(const DevSpec *specs, const uint32_t *rjob, const int *rtk, int nroots,
+                             const Z4<int32_t> *R, NodeMeta *meta) {
+  constexpr int E = (1 << NQ) * (1 << NQ);
+  __shared__ Z4<int32_t> S[E];
+  const int i = blockIdx.x, lane = threadIdx.x;
+  if (i >= nroots) return;
+  const DevSpec &sp = specs[rjob[i]];
+  const int tk = rtk[i];
+  for (int e = lane; e < E; e += 32) S[e] = R[(size_t)i * E + e];
+  __syncwarp();
+  int T = 0, c2 = 0, needs = 0;
+  Cheap ch{false, 0, 0};
+  if (sp.standard || sp.lite) T = ptm_bound<NQ, int32_t>(S, tk, lane);
+  if (sp.standard) {
+    c2 = warp_cx_bound<NQ, int32_t>(S, sp, lane, 0, 0, needs);
+    ch = warp_cheap<NQ, int32_t>(S, tk, sp, lane, false, true, (1 << NQ) - 1, 0);
+  }
+  if (lane == 0) {
+    NodeMeta m;
+    m.k = (int16_t)tk; m.T = (uint8_t)(T > 255 ? 255 : T); m.c2 = (uint8_t)c2; m.g1 = m.g2 = 0xff;
+    m.hsn = (uint8_t)((ch.hs == 2 ? 1 : 0) | (ch.ntriv << 1));
+    m.needs = (uint8_t)needs;
+    meta[i] = m;
+  }
+}
+
+// survivors of jobs still running -> (key, slot) pairs; the job is mixed into the key so runs stay within a job
+__global__ void k_bsort_init(const uint64_t *h1, const uint64_t *sidx, size_t n, const uint32_t *fjob,
+                             const uint8_t *jact, uint64_t *keys, uint32_t *vals, unsigned long long *cnt) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t nit = (n + stride - 1) / stride;
+  const int lane = threadIdx.x & 31;
+  for (size_t it = 0; it < nit; it++) {
+    const size_t i = it * stride + blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    uint32_t job = 0;
+    bool act = false;
+    if (i < n) { job = fjob[sidx[i] / BATCH_GS]; act = jact[job] != 0; }
+    const unsigned bal = __ballot_sync(FULL, act);
+    if (!bal) continue;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(cnt, (unsigned long long)__popc(bal));
+    base = __shfl_sync(FULL, base, 0);
+    if (act) {
+      const unsigned long long pos = base + __popc(bal & ((1u << lane) - 1));
+      keys[pos] = h1[i] + (uint64_t)(job + 1) * 0x9e3779b97f4a7c15ULL;
+      vals[pos] = (uint32_t)i;
+    }
+  }
+}
+
+// k_resolve for a batch: members of different jobs are never the same class; each job's own symmetry group
+template <int NQ, typename ST>
+__global__ void k_resolve_batch(const DevSpec *specs, const uint32_t *fjob, const uint2 *work, const uint32_t *slots,
+                                const uint64_t *sh1, const uint64_t *sh2, const uint64_t *sidx, const Z4<ST> *sR,
+                                const NodeMeta *smeta, uint32_t *tmp, uint64_t *kidx, uint32_t *kslot, DevStats *st) {
+  constexpr int E = (1 << NQ) * (1 << NQ);
+  const int lane = threadIdx.x & 31;
+  const unsigned long long nwork = st->n_work;
+  const unsigned long long nw = (unsigned long long)gridDim.x * (blockDim.x / 32);
+  for (unsigned long long wi = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); wi < nwork; wi += nw) {
+    const uint2 wk = work[wi];
+    const unsigned start = wk.x, len = wk.y;
+    for (unsigned a0 = 0; a0 < len; a0 += 32) {
+      const unsigned ai = a0 + lane;
+      uint64_t ah1 = 0, ah2 = 0, aix = 0;
+      uint32_t as = 0;
+      if (ai < len) { as = slots[start + ai]; ah1 = sh1[as]; ah2 = sh2[as]; aix = sidx[as]; }
+      unsigned rank = 0;
+      for (unsigned b = 0; b < len; b++) {
+        const uint32_t bs = slots[start + b];
+        const uint64_t bh1 = sh1[bs], bh2 = sh2[bs], bix = sidx[bs];
+        rank += (bh1 < ah1) || (bh1 == ah1 && (bh2 < ah2 || (bh2 == ah2 && bix < aix)));
+      }
+      if (ai < len) tmp[start + rank] = as;
+    }
+    __syncwarp();
+    unsigned gstart = 0;
+    for (unsigned i = 0; i < len; i++) {
+      const uint32_t si = tmp[start + i] & 0x7fffffffu;
+      if (i > 0) {
+        const uint32_t sp0 = tmp[start + i - 1] & 0x7fffffffu;
+        if (sh1[sp0] != sh1[si] || sh2[sp0] != sh2[si]) gstart = i;
+      }
+      const uint32_t ji = fjob[sidx[si] / BATCH_GS];
+      bool dup = false;
+      for (unsigned i2 = gstart; i2 < i && !dup; i2++) {
+        const uint32_t t2 = tmp[start + i2];
+        if (!(t2 & 0x80000000u)) continue;
+        const uint32_t s2 = t2 & 0x7fffffffu;
+        if (smeta[s2].k != smeta[si].k || fjob[sidx[s2] / BATCH_GS] != ji) continue;
+        dup = warp_same_class<NQ, ST>(sR + (size_t)si * E, sR + (size_t)s2 * E, specs[ji], specs[ji].symperm, lane);
+      }
+      if (!dup && lane == 0) {
+        tmp[start + i] = si | 0x80000000u;
+        const unsigned long long pos = atomicAdd(&st->n_kept, 1ULL);
+        kidx[pos] = sidx[si];
+        kslot[pos] = si;
+      }
+      __syncwarp();
+    }
+  }
+}
+
+__global__ void k_bcount(const uint64_t *kidx, size_t nk, const uint32_t *fjob, unsigned long long *jdist) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nk; i += (size_t)gridDim.x * blockDim.x)
+    atomicAdd(&jdist[fjob[kidx[i] / BATCH_GS]], 1ULL);
+}
+__global__ void k_fjob_next(const uint64_t *kidx, size_t nk, const uint32_t *fjob, uint32_t *fjob2) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nk; i += (size_t)gridDim.x * blockDim.x)
+    fjob2[i] = fjob[kidx[i] / BATCH_GS];
+}
+// circuits of jobs that found the goal: child index o at step s and job level t, walked back through the tree
+// arrays of steps s - 1 .. s - t + 1
+__global__ void k_walk(const unsigned long long *fo, const int *ft, const int *fs, int nf, const uint32_t *const *tpar,
+                       const uint8_t *const *tgat, int *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  const unsigned long long o = fo[i];
+  const int t = ft[i], s = fs[i];
+  int *c = out + (size_t)i * MAXDEPTH_WALK;
+  c[t - 1] = (int)(o % BATCH_GS);
+  unsigned long long p = o / BATCH_GS;
+  for (int l = t - 1; l >= 1; l--) {
+    const int step = s - (t - l);
+    c[l - 1] = tgat[step][p];
+    p = tpar[step][p];
+  }
+}
+
+struct SpecTables { DBuf ginv, bad2, bad3, cxt, goal; };   // one spec's device tables, shared by equal specs
+
+uint64_t bytes_hash(uint64_t h, const void *p, size_t n) {
+  const unsigned char *b = (const unsigned char *)p;
+  for (size_t i = 0; i < n; i++) { h ^= b[i]; h *= 1099511628211ULL; }
+  return h;
+}
+
+}  // namespace
+
+struct BatchSession::Impl {
+  virtual ~Impl() {}
+  virtual int nq() const = 0;
+  virtual int submit(const HostSpec &hs, const Options &opt) = 0;
+  virtual int step() = 0;
+  virtual int running() const = 0;
+  virtual const BatchJob &job(int id) const = 0;
+  virtual int jobs() const = 0;
+  virtual long long frontier() const = 0;
+  virtual long long launches() const = 0;
+  virtual long long steps() const = 0;
+  virtual size_t device_bytes() const = 0;
+};
+
+namespace {
+
+template <int NQ>
+struct BatchImpl : BatchSession::Impl {
+  static constexpr int N = 1 << NQ, E = N * N;
+  using ST = int32_t;
+  struct Job {
+    HostSpec hs;
+    Options opt;
+    int depth = 0;
+    DevSpec sp;
+    int t = 1;                       // the level this job runs at its next step
+    long long seg = 0;               // its nodes in the frontier
+    bool queued = true, running = false;
+    BatchJob out;
+  };
+  Engine &eng;
+  cudaStream_t s;
+  int nsm = 148;
+  std::vector<Job> J;
+  std::vector<int> queue;            // submitted, not yet admitted
+  std::map<uint64_t, SpecTables *> tables;
+  DBuf dspecs, jt, jst, jact, jdist;
+  DBuf fR, fMeta, fJob, fR2, fMeta2, fJob2;
+  DBuf sH1, sH2, sIdx, sR, sMeta, stats;
+  DBuf k0, k1, v0, v1, hist, part, work, tmp, kidx, kslot, cnt;
+  DBuf rJob, rTk, tptr, wbuf;
+  std::vector<DBuf> tpar, tgat;      // tree of every step
+  long long m = 0;                   // frontier nodes
+  long long nlaunch = 0, nstep = 0;
+  int nrun = 0;
+  size_t spec_cap = 0;
+
+  BatchImpl(Engine &e) : eng(e), s((cudaStream_t)e.stream()) {
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e.device());
+    stats.ensure(sizeof(DevStats));
+    cnt.ensure(64);
+  }
+  ~BatchImpl() override {
+    cudaSetDevice(eng.device());
+    for (DBuf *b : {&dspecs, &jt, &jst, &jact, &jdist, &fR, &fMeta, &fJob, &fR2, &fMeta2, &fJob2, &sH1, &sH2, &sIdx,
+                    &sR, &sMeta, &stats, &k0, &k1, &v0, &v1, &hist, &part, &work, &tmp, &kidx, &kslot, &cnt, &rJob,
+                    &rTk, &tptr, &wbuf})
+      b->release();
+    for (auto &b : tpar) b.release();
+    for (auto &b : tgat) b.release();
+    for (auto &kv : tables) {
+      kv.second->ginv.release(); kv.second->bad2.release(); kv.second->bad3.release(); kv.second->cxt.release();
+      kv.second->goal.release();
+      delete kv.second;
+    }
+  }
+  int nq() const override { return NQ; }
+  int running() const override { return nrun + (int)queue.size(); }
+  const BatchJob &job(int id) const override { return J.at(id).out; }
+  int jobs() const override { return (int)J.size(); }
+  long long frontier() const override { return m; }
+  long long launches() const override { return nlaunch; }
+  long long steps() const override { return nstep; }
+  size_t device_bytes() const override {
+    size_t b = 0;
+    for (const DBuf *x : {&dspecs, &jt, &jst, &jact, &jdist, &fR, &fMeta, &fJob, &fR2, &fMeta2, &fJob2, &sH1, &sH2,
+                          &sIdx, &sR, &sMeta, &k0, &k1, &v0, &v1, &hist, &part, &work, &tmp, &kidx, &kslot})
+      b += x->cap;
+    for (auto &x : tpar) b += x.cap;
+    for (auto &x : tgat) b += x.cap;
+    return b;
+  }
+
+  int submit(const HostSpec &hs, const Options &opt) override {
+    Job j;
+    j.hs = hs;
+    j.opt = opt;
+    j.depth = opt.depth >= 0 ? opt.depth : hs.depth;
+    J.push_back(std::move(j));
+    queue.push_back((int)J.size() - 1);
+    return (int)J.size() - 1;
+  }
+
+  void finish(Job &j, int rc) {
+    j.out.done = true;
+    j.out.res.rc = rc;
+    j.out.finished_step = (int)nstep;
+    if (j.running) nrun--;
+    j.running = false;
+  }
+  void run_plain(Job &j) {
+    j.out.levels.clear();
+    SearchResult r;
+    eng.search(j.hs, j.opt, [&](const LevelStats &L) { j.out.levels.push_back(L); }, r);
+    j.out.res = r;
+    j.out.plain = true;
+    j.out.done = true;
+    j.out.finished_step = (int)nstep;
+  }
+
+  // device tables of a spec, shared by every job whose tables have the same content
+  void upload_spec(Job &j) {
+    const SymGroup grp = sym_group(j.hs, j.opt.sym);
+    j.out.res.nsym = grp.nsym;
+    std::vector<int4> gi;
+    std::vector<longlong2> gl;
+    j.sp = devspec_host<NQ>(j.hs, grp, j.depth, false, gi, gl);
+    uint64_t h = 1469598103934665603ULL;
+    h = bytes_hash(h, gi.data(), gi.size() * sizeof(int4));
+    h = bytes_hash(h, j.hs.bad2.data(), j.hs.bad2.size());
+    h = bytes_hash(h, j.hs.bad3.data(), j.hs.bad3.size() * 4);
+    h = bytes_hash(h, j.hs.cxtable.data(), j.hs.cxtable.size() * 4);
+    h = bytes_hash(h, gl.data(), gl.size() * sizeof(longlong2));
+    SpecTables *tb;
+    auto it = tables.find(h);
+    if (it != tables.end()) tb = it->second;
+    else {
+      tb = new SpecTables;
+      tb->ginv.ensure(gi.size() * sizeof(int4)); tb->bad2.ensure(j.hs.bad2.size() + 1);
+      tb->bad3.ensure(j.hs.bad3.size() * 4 + 4); tb->cxt.ensure(std::max<size_t>(1, j.hs.cxtable.size()) * 4);
+      tb->goal.ensure(gl.size() * sizeof(longlong2));
+      ck(cudaMemcpyAsync(tb->ginv.p, gi.data(), gi.size() * sizeof(int4), cudaMemcpyHostToDevice, s), "h2d");
+      ck(cudaMemcpyAsync(tb->bad2.p, j.hs.bad2.data(), j.hs.bad2.size(), cudaMemcpyHostToDevice, s), "h2d");
+      ck(cudaMemcpyAsync(tb->bad3.p, j.hs.bad3.data(), j.hs.bad3.size() * 4, cudaMemcpyHostToDevice, s), "h2d");
+      if (!j.hs.cxtable.empty())
+        ck(cudaMemcpyAsync(tb->cxt.p, j.hs.cxtable.data(), j.hs.cxtable.size() * 4, cudaMemcpyHostToDevice, s), "h2d");
+      ck(cudaMemcpyAsync(tb->goal.p, gl.data(), gl.size() * sizeof(longlong2), cudaMemcpyHostToDevice, s), "h2d");
+      ck(cudaStreamSynchronize(s), "spec upload");
+      tables[h] = tb;
+    }
+    j.sp.ginv = tb->ginv.as<int4>(); j.sp.bad2 = tb->bad2.as<uint8_t>(); j.sp.bad3 = tb->bad3.as<uint32_t>();
+    j.sp.cxtable = tb->cxt.as<int>(); j.sp.goal = tb->goal.as<longlong2>();
+  }
+
+  // admit the queued jobs: depth-0 and unsupported ones finish here, the others append their root to the frontier
+  void admit() {
+    std::vector<int> roots;
+    for (int id : queue) {
+      Job &j = J[id];
+      j.queued = false;
+      j.out.joined_step = (int)nstep;
+      bool ident = j.hs.tk == 0;
+      for (int r = 0; r < N && ident; r++)
+        for (int c = 0; c < N && ident; c++) {
+          const Zw x = j.hs.target[r * N + c];
+          ident = r == c ? (x.a == 1 && !x.b && !x.c && !x.d) : zzero(x);
+        }
+      if (ident && !j.opt.nogoal) { j.out.res.depth0 = true; j.out.res.nsym = sym_group(j.hs, j.opt.sym).nsym; finish(j, RC_CIRCUIT); continue; }
+      bool wide = j.opt.store64 == 1;
+      auto f32 = [](int64_t v) { return v >= INT32_MIN && v <= INT32_MAX; };
+      for (const Zw &z : j.hs.target) if (!f32(z.a) || !f32(z.b) || !f32(z.c) || !f32(z.d)) wide = true;
+      if (wide || !j.opt.dedupe || j.opt.nogoal || j.depth < 1 || j.depth > MAXDEPTH_WALK) { run_plain(j); continue; }
+      upload_spec(j);
+      roots.push_back(id);
+    }
+    queue.clear();
+    // device specs: one per job id
+    if (J.size() > spec_cap) {
+      spec_cap = std::max<size_t>(J.size(), spec_cap * 2);
+      DBuf nd;
+      nd.ensure(spec_cap * sizeof(DevSpec));
+      if (dspecs.p) ck(cudaMemcpyAsync(nd.p, dspecs.p, dspecs.cap < spec_cap * sizeof(DevSpec) ? dspecs.cap : spec_cap * sizeof(DevSpec), cudaMemcpyDeviceToDevice, s), "d2d");
+      ck(cudaStreamSynchronize(s), "specs");
+      dspecs.release();
+      dspecs = nd;
+      nd.p = nullptr;
+    }
+    if (roots.empty()) return;
+    std::vector<Z4<int32_t>> rr(roots.size() * E);
+    std::vector<uint32_t> rj(roots.size());
+    std::vector<int> rk(roots.size());
+    for (size_t i = 0; i < roots.size(); i++) {
+      Job &j = J[roots[i]];
+      for (int e = 0; e < E; e++)
+        rr[i * E + e] = {(int32_t)j.hs.target[e].a, (int32_t)j.hs.target[e].b, (int32_t)j.hs.target[e].c,
+                         (int32_t)j.hs.target[e].d};
+      rj[i] = (uint32_t)roots[i];
+      rk[i] = j.hs.tk;
+      ck(cudaMemcpyAsync(dspecs.as<DevSpec>() + roots[i], &j.sp, sizeof(DevSpec), cudaMemcpyHostToDevice, s), "h2d");
+      j.t = 1;
+      j.seg = 1;
+      j.running = true;
+      nrun++;
+    }
+    const long long nr = (long long)roots.size();
+    // grow the frontier (contents kept) and append the roots
+    auto grow_keep = [&](DBuf &b, size_t bytes, size_t keep) {
+      if (bytes <= b.cap) return;
+      DBuf nb;
+      nb.ensure(bytes);
+      if (keep) ck(cudaMemcpyAsync(nb.p, b.p, keep, cudaMemcpyDeviceToDevice, s), "d2d");
+      ck(cudaStreamSynchronize(s), "grow");
+      b.release();
+      b = nb;
+      nb.p = nullptr;
+    };
+    grow_keep(fR, (size_t)(m + nr) * E * sizeof(Z4<ST>), (size_t)m * E * sizeof(Z4<ST>));
+    grow_keep(fMeta, (size_t)(m + nr) * sizeof(NodeMeta), (size_t)m * sizeof(NodeMeta));
+    grow_keep(fJob, (size_t)(m + nr) * 4, (size_t)m * 4);
+    rJob.ensure(nr * 4); rTk.ensure(nr * 4);
+    ck(cudaMemcpyAsync(fR.as<Z4<ST>>() + m * E, rr.data(), rr.size() * sizeof(Z4<ST>), cudaMemcpyHostToDevice, s), "h2d");
+    ck(cudaMemcpyAsync(fJob.as<uint32_t>() + m, rj.data(), nr * 4, cudaMemcpyHostToDevice, s), "h2d");
+    ck(cudaMemcpyAsync(rJob.p, rj.data(), nr * 4, cudaMemcpyHostToDevice, s), "h2d");
+    ck(cudaMemcpyAsync(rTk.p, rk.data(), nr * 4, cudaMemcpyHostToDevice, s), "h2d");
+    k_root_batch<NQ><<<(unsigned)nr, 32, 0, s>>>(dspecs.as<DevSpec>(), rJob.as<uint32_t>(), rTk.as<int>(), (int)nr,
+                                                 fR.as<Z4<ST>>() + m * E, fMeta.as<NodeMeta>() + m);
+    nlaunch++;
+    ck(cudaGetLastError(), "root kernel");
+    ck(cudaStreamSynchronize(s), "admit");
+    m += nr;
+  }
+
+  int step() override {
+    ck(cudaSetDevice(eng.device()), "cudaSetDevice");
+    if (!queue.empty()) admit();
+    if (m == 0) { nstep++; return running(); }
+    const double t0 = now_s();
+    const int nj = (int)J.size();
+    // per-job level and stats
+    std::vector<int> ht(nj, 0);
+    for (int i = 0; i < nj; i++) ht[i] = J[i].t;
+    jt.ensure(nj * 4); jst.ensure(nj * sizeof(DevStats)); jact.ensure(nj + 4); jdist.ensure(nj * 8);
+    ck(cudaMemcpyAsync(jt.p, ht.data(), nj * 4, cudaMemcpyHostToDevice, s), "h2d");
+    k_jst_init<<<(nj + 255) / 256, 256, 0, s>>>(jst.as<DevStats>(), nj);
+    nlaunch++;
+    // survivors: at most every child; retried with the exact count if that does not fit
+    unsigned long long cap = 0;
+    for (auto &j : J) if (j.running && j.t < j.depth) cap += (unsigned long long)j.seg * j.hs.G;
+    const unsigned long long cap_limit = (unsigned long long)24 << 20;   // survivors per attempt (24 Mi x 1 KB)
+    if (cap > cap_limit) cap = cap_limit;
+    DevStats *dst = stats.as<DevStats>();
+    DevStats h{};
+    for (int attempt = 0; attempt < 2; attempt++) {
+      if (cap) {
+        sH1.ensure(cap * 8); sH2.ensure(cap * 8); sIdx.ensure(cap * 8);
+        sR.ensure(cap * E * sizeof(Z4<ST>)); sMeta.ensure(cap * sizeof(NodeMeta));
+      }
+      ck(cudaMemsetAsync(dst, 0, sizeof(DevStats), s), "memset");
+      if (attempt) { k_jst_init<<<(nj + 255) / 256, 256, 0, s>>>(jst.as<DevStats>(), nj); nlaunch++; }
+      BatchArgs<ST> a;
+      a.m = m; a.R = fR.as<Z4<ST>>(); a.meta = fMeta.as<NodeMeta>(); a.fjob = fJob.as<uint32_t>();
+      a.specs = dspecs.as<DevSpec>(); a.jt = jt.as<int>(); a.jst = jst.as<DevStats>(); a.st = dst; a.cap = cap;
+      a.sh1 = sH1.as<uint64_t>(); a.sh2 = sH2.as<uint64_t>(); a.sidx = sIdx.as<uint64_t>();
+      a.sR = sR.as<Z4<ST>>(); a.smeta = sMeta.as<NodeMeta>();
+      const long long want = (m + EXP_WARPS - 1) / EXP_WARPS;
+      const long long grid = std::max<long long>(1, std::min<long long>(want, (long long)nsm * 2 * 8));
+      k_expand_batch<NQ, ST><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(a);
+      nlaunch++;
+      ck(cudaGetLastError(), "batched expand");
+      ck(cudaMemcpyAsync(&h, dst, sizeof(DevStats), cudaMemcpyDeviceToHost, s), "d2h");
+      ck(cudaStreamSynchronize(s), "batched expand");
+      if (!h.surv_overflow) break;
+      cap = h.n_surv;
+    }
+    if (h.surv_overflow) throw CudaError("survivor buffer overflow");
+    std::vector<DevStats> hj(nj);
+    ck(cudaMemcpyAsync(hj.data(), jst.p, nj * sizeof(DevStats), cudaMemcpyDeviceToHost, s), "d2h");
+    ck(cudaStreamSynchronize(s), "job stats");
+    // found / overflowed jobs leave; the others go on to dedupe
+    std::vector<uint8_t> act(nj, 0);
+    std::vector<int> found_ids, overflow_ids;
+    size_t nsort = 0;
+    for (int i = 0; i < nj; i++) {
+      Job &j = J[i];
+      if (!j.running) continue;
+      if (hj[i].ovf) { overflow_ids.push_back(i); continue; }
+      if (hj[i].found) { found_ids.push_back(i); continue; }
+      act[i] = 1;
+      if (j.t < j.depth) nsort += hj[i].alive;
+    }
+    if (!found_ids.empty()) {
+      // circuits: walk each found child back through the tree (one thread per job)
+      const int nf = (int)found_ids.size();
+      std::vector<unsigned long long> fo(nf);
+      std::vector<int> ft(nf), fs(nf);
+      for (int i = 0; i < nf; i++) { fo[i] = hj[found_ids[i]].first_found; ft[i] = J[found_ids[i]].t; fs[i] = (int)nstep; }
+      std::vector<const uint32_t *> pp(nstep + 1, nullptr);
+      std::vector<const uint8_t *> gp(nstep + 1, nullptr);
+      for (long long st2 = 0; st2 < nstep && st2 < (long long)tpar.size(); st2++) { pp[st2] = tpar[st2].as<uint32_t>(); gp[st2] = tgat[st2].as<uint8_t>(); }
+      const size_t pb = pp.size() * sizeof(void *);
+      tptr.ensure(2 * pb + (size_t)nf * (8 + 4 + 4) + (size_t)nf * MAXDEPTH_WALK * 4 + 64);
+      char *base = (char *)tptr.p;
+      ck(cudaMemcpyAsync(base, pp.data(), pb, cudaMemcpyHostToDevice, s), "h2d");
+      ck(cudaMemcpyAsync(base + pb, gp.data(), pb, cudaMemcpyHostToDevice, s), "h2d");
+      char *q = base + 2 * pb;
+      unsigned long long *dfo = (unsigned long long *)q; q += (size_t)nf * 8;
+      int *dft = (int *)q; q += (size_t)nf * 4;
+      int *dfs = (int *)q; q += (size_t)nf * 4;
+      int *dout = (int *)q;
+      ck(cudaMemcpyAsync(dfo, fo.data(), nf * 8, cudaMemcpyHostToDevice, s), "h2d");
+      ck(cudaMemcpyAsync(dft, ft.data(), nf * 4, cudaMemcpyHostToDevice, s), "h2d");
+      ck(cudaMemcpyAsync(dfs, fs.data(), nf * 4, cudaMemcpyHostToDevice, s), "h2d");
+      k_walk<<<(nf + 63) / 64, 64, 0, s>>>(dfo, dft, dfs, nf, (const uint32_t *const *)base,
+                                           (const uint8_t *const *)(base + pb), dout);
+      nlaunch++;
+      std::vector<int> circ((size_t)nf * MAXDEPTH_WALK);
+      ck(cudaMemcpyAsync(circ.data(), dout, circ.size() * 4, cudaMemcpyDeviceToHost, s), "d2h");
+      ck(cudaStreamSynchronize(s), "walk");
+      for (int i = 0; i < nf; i++) {
+        Job &j = J[found_ids[i]];
+        j.out.res.circuit.assign(circ.begin() + (size_t)i * MAXDEPTH_WALK, circ.begin() + (size_t)i * MAXDEPTH_WALK + j.t);
+        j.out.res.n_found = (long long)hj[found_ids[i]].found;
+        j.out.res.levels = j.t;
+        account(j, hj[found_ids[i]]);
+        finish(j, RC_CIRCUIT);
+      }
+    }
+    // dedupe of the running jobs' survivors (one sort over all of them)
+    std::vector<unsigned long long> dist(nj, 0);
+    size_t distinct = 0;
+    const uint64_t *ki = nullptr;
+    const uint32_t *vi = nullptr;
+    if (nsort) {
+      ck(cudaMemcpyAsync(jact.p, act.data(), nj, cudaMemcpyHostToDevice, s), "h2d");
+      const size_t ns = (size_t)h.n_surv;
+      k0.ensure(nsort * 8); k1.ensure(nsort * 8); v0.ensure(nsort * 4); v1.ensure(nsort * 4);
+      kidx.ensure(nsort * 8); kslot.ensure(nsort * 4); work.ensure(nsort * sizeof(uint2)); tmp.ensure(nsort * 4);
+      hist.ensure(sort_hist_words(nsort) * 4);
+      part.ensure(scan_partials_words(sort_hist_words(nsort)) * 4);
+      SortScratch sc{hist.as<uint32_t>(), part.as<uint32_t>(), hist.cap / 4, part.cap / 4};
+      ck(cudaMemsetAsync(cnt.p, 0, 8, s), "memset");
+      const unsigned gb = (unsigned)std::max<size_t>(1, std::min<size_t>((ns + 255) / 256, (size_t)nsm * 16));
+      k_bsort_init<<<gb, 256, 0, s>>>(sH1.as<uint64_t>(), sIdx.as<uint64_t>(), ns, fJob.as<uint32_t>(),
+                                      jact.as<uint8_t>(), k0.as<uint64_t>(), v0.as<uint32_t>(),
+                                      cnt.as<unsigned long long>());
+      nlaunch++;
+      int ln = 0;
+      const bool f = radix_sort(k0.as<uint64_t>(), v0.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(), nsort, 32,
+                                64, sc, s, &ln);
+      nlaunch += ln;
+      const uint64_t *sk = f ? k1.as<uint64_t>() : k0.as<uint64_t>();
+      const uint32_t *sv = f ? v1.as<uint32_t>() : v0.as<uint32_t>();
+      ck(cudaMemsetAsync(dst, 0, sizeof(DevStats), s), "memset");
+      const unsigned gs = (unsigned)std::max<size_t>(1, std::min<size_t>((nsort + 255) / 256, (size_t)nsm * 16));
+      k_runs<<<gs, 256, 0, s>>>(sk, sv, nsort, sIdx.as<uint64_t>(), kidx.as<uint64_t>(), kslot.as<uint32_t>(),
+                                work.as<uint2>(), dst);
+      k_resolve_batch<NQ, ST><<<(unsigned)nsm * 4, 256, 0, s>>>(dspecs.as<DevSpec>(), fJob.as<uint32_t>(),
+                                                                work.as<uint2>(), sv, sH1.as<uint64_t>(),
+                                                                sH2.as<uint64_t>(), sIdx.as<uint64_t>(),
+                                                                sR.as<Z4<ST>>(), sMeta.as<NodeMeta>(),
+                                                                tmp.as<uint32_t>(), kidx.as<uint64_t>(),
+                                                                kslot.as<uint32_t>(), dst);
+      nlaunch += 2;
+      ck(cudaGetLastError(), "batched dedupe");
+      ck(cudaMemcpyAsync(&h, dst, sizeof(DevStats), cudaMemcpyDeviceToHost, s), "d2h");
+      ck(cudaStreamSynchronize(s), "batched dedupe");
+      distinct = (size_t)h.n_kept;
+      ck(cudaMemsetAsync(jdist.p, 0, nj * 8, s), "memset");
+      k_bcount<<<(unsigned)std::max<size_t>(1, std::min<size_t>((distinct + 255) / 256, (size_t)nsm * 16)), 256, 0, s>>>(
+          kidx.as<uint64_t>(), distinct, fJob.as<uint32_t>(), jdist.as<unsigned long long>());
+      nlaunch++;
+      ck(cudaMemcpyAsync(dist.data(), jdist.p, nj * 8, cudaMemcpyDeviceToHost, s), "d2h");
+      // the next frontier in child-index order (every job's children contiguous, in its own order)
+      int bits = 1;
+      while (bits < 64 && ((unsigned long long)m * BATCH_GS) >> bits) bits++;
+      const int hi = ((bits + 7) / 8) * 8;
+      ln = 0;
+      const bool f2 = radix_sort(kidx.as<uint64_t>(), kslot.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(),
+                                 distinct, 0, hi, sc, s, &ln);
+      nlaunch += ln;
+      ki = f2 ? k1.as<uint64_t>() : kidx.as<uint64_t>();
+      vi = f2 ? v1.as<uint32_t>() : kslot.as<uint32_t>();
+      if ((long long)tpar.size() <= nstep) { tpar.resize(nstep + 1); tgat.resize(nstep + 1); }
+      tpar[nstep].ensure(distinct * 4 + 4);
+      tgat[nstep].ensure(distinct + 4);
+      fR2.ensure(distinct * E * sizeof(Z4<ST>) + 16); fMeta2.ensure(distinct * sizeof(NodeMeta) + 16);
+      fJob2.ensure(distinct * 4 + 4);
+      const size_t tot = distinct * E;
+      const unsigned gg = (unsigned)std::max<size_t>(1, std::min<size_t>((tot + 255) / 256, (size_t)nsm * 32));
+      k_gather<ST><<<gg, 256, 0, s>>>(ki, vi, distinct, BATCH_GS, E, sR.as<Z4<ST>>(), sMeta.as<NodeMeta>(),
+                                      fR2.as<Z4<ST>>(), fMeta2.as<NodeMeta>(), tpar[nstep].as<uint32_t>(),
+                                      tgat[nstep].as<uint8_t>());
+      k_fjob_next<<<(unsigned)std::max<size_t>(1, std::min<size_t>((distinct + 255) / 256, (size_t)nsm * 16)), 256, 0, s>>>(
+          ki, distinct, fJob.as<uint32_t>(), fJob2.as<uint32_t>());
+      nlaunch += 2;
+      ck(cudaGetLastError(), "batched gather");
+      ck(cudaStreamSynchronize(s), "batched gather");
+      std::swap(fR, fR2); std::swap(fMeta, fMeta2); std::swap(fJob, fJob2);
+    } else if ((long long)tpar.size() <= nstep) {
+      tpar.resize(nstep + 1); tgat.resize(nstep + 1);
+    }
+    // level lines of the running jobs
+    const double secs = now_s() - t0;
+    for (int i = 0; i < nj; i++) {
+      Job &j = J[i];
+      if (!j.running || !act[i]) continue;
+      const DevStats &d = hj[i];
+      LevelStats L;
+      L.t = j.t; L.parents = j.seg; L.prefixes = j.seg * j.hs.G - (long long)d.w2; L.cut_w3 = (long long)d.w3;
+      L.cut_lb = (long long)d.dead; L.survivors = (long long)d.alive;
+      L.distinct = j.t < j.depth ? (long long)dist[i] : 0;
+      L.proved_unsat = L.distinct == 0;
+      L.seconds = secs;
+      j.out.levels.push_back(L);
+      j.out.res.prefixes += L.prefixes;
+      account(j, d);
+      j.out.res.levels = j.t;
+      if (L.distinct == 0) { finish(j, RC_PROOF); continue; }
+      j.seg = L.distinct;
+      j.t++;
+    }
+    m = (long long)distinct;
+    nstep++;
+    // jobs whose int32 limbs overflowed: rerun alone (the plain path promotes them to int64)
+    for (int id : overflow_ids) {
+      Job &j = J[id];
+      if (j.running) nrun--;
+      j.running = false;
+      run_plain(j);
+    }
+    return running();
+  }
+  void account(Job &j, const DevStats &d) {
+    j.out.res.t_evals += (long long)d.t_evals;
+    j.out.res.children += (long long)d.children;
+    j.out.res.children_full += (long long)d.full;
+  }
+};
+
+}  // namespace
+
+BatchSession::BatchSession(Engine &engine, int nq) {
+  switch (nq) {
+    case 1: impl_ = new BatchImpl<1>(engine); break;
+    case 2: impl_ = new BatchImpl<2>(engine); break;
+    case 3: impl_ = new BatchImpl<3>(engine); break;
+    default: throw std::invalid_argument("qubit count must be 1, 2 or 3");
+  }
+}
+BatchSession::~BatchSession() { delete impl_; }
+int BatchSession::nq() const { return impl_->nq(); }
+int BatchSession::submit(const HostSpec &hs, const Options &opt) { return impl_->submit(hs, opt); }
+int BatchSession::step() { return impl_->step(); }
+int BatchSession::running() const { return impl_->running(); }
+const BatchJob &BatchSession::job(int id) const { return impl_->job(id); }
+int BatchSession::jobs() const { return impl_->jobs(); }
+long long BatchSession::frontier() const { return impl_->frontier(); }
+long long BatchSession::launches() const { return impl_->launches(); }
+long long BatchSession::steps() const { return impl_->steps(); }
+size_t BatchSession::device_bytes() const { return impl_->device_bytes(); }
 
 }  // namespace cz

@@ -90,6 +90,29 @@ typedef struct {
 int cz_search(cz_engine *engine, const cz_spec *spec, const cz_options *opt, cz_level_fn on_level, void *user,
               cz_result *out);
 
+/* ---------------- batched searches (no counterpart in the reference: it runs one search per process) ----------------
+ * A batch session advances many searches of one qubit count together, one level per step, in shared launches
+ * (continuous batching): a submitted job joins at the next step, a finished job leaves. Every job's level lines,
+ * exit code and circuit equal cz_search's on the same spec and options. */
+typedef struct cz_batch cz_batch;
+typedef struct {
+  int nq, jobs, running;
+  int64_t frontier;                 /* nodes in the shared frontier */
+  int64_t steps, kernel_launches;
+  int64_t device_bytes;             /* device memory held by the session */
+} cz_batch_info;
+int cz_batch_create(cz_engine *engine, int nq, cz_batch **out);
+void cz_batch_destroy(cz_batch *batch);
+/* Queue a search (the spec's qubit count must be the session's): the job id (>= 0), or -(exit code). */
+int cz_batch_submit(cz_batch *batch, const cz_spec *spec, const cz_options *opt);
+/* One level of every running job (admitting the queued ones first); *running = jobs not finished yet. */
+int cz_batch_step(cz_batch *batch, int *running);
+int cz_batch_info_get(const cz_batch *batch, cz_batch_info *out);
+/* 1 when the job has finished. */
+int cz_batch_done(const cz_batch *batch, int job);
+/* A finished job: its level lines through on_level (in order) and its result, as cz_search gives them. */
+int cz_batch_result(const cz_batch *batch, int job, cz_level_fn on_level, void *user, cz_result *out);
+
 /* Convenience for FFI callers that hold the spec as text: parse + search in one call. */
 int cz_search_text(cz_engine *engine, const char *spec_text, size_t len, const cz_options *opt, cz_level_fn on_level,
                    void *user, cz_result *out);
@@ -172,6 +195,46 @@ int cz_tspec_check(const char *tspec, size_t len, int *n, char *err, size_t errl
  * table resident in device memory after its first use. */
 int cz_tcount(cz_engine *engine, const char *tspec, size_t len, const cz_tcount_options *opt,
               cz_tcount_level_fn on_level, void *user, cz_tcount_result *out);
+
+/* ---------------- Clifford table (the reference's build/cliffopt, src/clifford.cu) ---------------- */
+/* Tableau of an n <= 3 qubit Clifford up to phase, as the reference packs it (clifford.cu:16-19, 46-58): row
+ * i < n is the image of X_i, row n + i the image of Z_i, each row (x bits | z bits << n | sign << 2n) of 2n + 1
+ * bits, row i at bit i * (2n + 1). */
+typedef struct {
+  int n;
+  int64_t order, elements;          /* group order up to phase; elements reached by the BFS (equal when correct) */
+  int max_distance;
+  int64_t per_distance[32];         /* elements at each minimal gate count (the "clifford gates d" lines) */
+  int built;                        /* 1: built by this call; 0: resident from an earlier call */
+  double seconds;
+} cz_clifford_table_info;
+
+/* The BFS distance table of the n-qubit Clifford group over H, S, Sdg, X, Z and CX (clifford.cu:247-276), built
+ * once per engine and kept resident: 0, 3 (n not 1..3), 4 (group order mismatch), 5 (CUDA). */
+int cz_clifford_table(cz_engine *engine, int n, cz_clifford_table_info *out, char *err, size_t errlen);
+/* Minimal gate counts of tableaux (-1 for a word that is not a valid tableau). */
+int cz_clifford_dist(cz_engine *engine, int n, const uint64_t *tableaux, size_t count, int *out);
+/* The group element of each index in [0, order): index -> element is a fixed bijection (uniform draws). */
+int cz_clifford_element(cz_engine *engine, int n, const uint64_t *index, size_t count, uint64_t *tableaux);
+
+/* Parse a cliffopt job (clifford.cu:213-238) on the host: 0, or 2 ("bad job file", "unknown Clifford gate X"). */
+int cz_cliffjob_check(const char *job, size_t len, int *n, int *t_gates, char *err, size_t errlen);
+
+/* one "T gate j: P placements x beam, best partial C" line (clifford.cu:330) */
+typedef void (*cz_cliffopt_step_fn)(void *user, int tgate, int64_t placements, int best_partial);
+typedef struct {
+  int rc;                           /* 0, 2 job, 3 usage, 4 table / reconstruction, 5 CUDA */
+  int clifford_gates, clifford_gates_before, t_gates;
+  double seconds;
+  cz_clifford_table_info table;
+  int64_t kernel_launches;
+  size_t text_len;                  /* length of the gate lines (text is truncated to text_cap - 1) */
+  char error[256];
+} cz_cliffopt_result;
+/* `cliffopt JOB --beam B` (replaces clifford.cu's main, :240-384): fewer Clifford gates around the job's T gates.
+ * text receives the output lines after the JSON line: one gate per line, T gates as "t q" / "tdg q". */
+int cz_cliffopt(cz_engine *engine, const char *job, size_t len, int beam, cz_cliffopt_step_fn on_step, void *user,
+                char *text, size_t text_cap, cz_cliffopt_result *out);
 
 /* The library version string and the CUDA architecture it was compiled for ("sm_100a"). */
 const char *cz_version(void);

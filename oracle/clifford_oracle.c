@@ -1,6 +1,6 @@
 /* clifford-oracle: CPU restatement of the reference's cliffopt (src/clifford.cu). TEST INFRASTRUCTURE ONLY: the
  * checker of cheese_b200's Clifford-table path, never linked into it.
- *   clifford-oracle JOB [--beam B] [--dist-only]
+ *   clifford-oracle JOB... [--beam B] [--dist-only]
  * Same job grammar, stdout and stderr lines as the reference (clifford.cu:213-384), times printed as 0.0 / 0.00.
  * The reference leaves one thing open: the order of the placement candidates of a T gate (k_cands appends them with
  * an atomic counter, clifford.cu:170-183), which decides ties in the beam. Here, as in cheese_b200, candidates are
@@ -141,28 +141,13 @@ static int parse_gate(FILE *f, gate *g) {
 }
 static const char *gname(int k) { static const char *nm[] = {"h", "s", "sdg", "x", "z", "cx", "y"}; return nm[k]; }
 
-int main(int argc, char **argv) {
-  if (argc < 2) { fprintf(stderr, "usage: cliffopt JOB [--beam B]\n"); return 3; }
-  FILE *f = fopen(argv[1], "r");
-  int t = 0, bad = !f;
-  if (!bad && fscanf(f, "%d %d", &n, &t) != 2) bad = 1;
-  if (t < 0 || t > 4096) bad = 1;
-  int *tq = calloc(t + 1, sizeof(int)), *td = calloc(t + 1, sizeof(int));
-  for (int i = 0; !bad && i < t; i++) if (fscanf(f, "%d %d", &tq[i], &td[i]) != 2) bad = 1;
-  gate **seg = calloc(t + 1, sizeof(gate *));
-  int *segn = calloc(t + 1, sizeof(int));
-  for (int j = 0; !bad && j <= t; j++) {
-    if (fscanf(f, "%d", &segn[j]) != 1 || segn[j] < 0) { bad = 1; break; }
-    seg[j] = calloc(segn[j] + 1, sizeof(gate));
-    for (int i = 0; i < segn[j]; i++) if (parse_gate(f, &seg[j][i])) { bad = 1; break; }
-  }
-  if (bad || n < 1 || n > 3) { fprintf(stderr, "bad job file\n"); return 2; }
-  fclose(f);
-  int beam = 16, dist_only = 0;
-  for (int i = 2; i < argc; i++) {
-    if (!strcmp(argv[i], "--beam") && i + 1 < argc) { beam = atoi(argv[++i]); beam = beam < 1 ? 1 : beam > 255 ? 255 : beam; }
-    else if (!strcmp(argv[i], "--dist-only")) dist_only = 1;
-  }
+/* the table of n qubits: BFS from the identity (clifford.cu:247-276), then the placement candidates per qubit
+ * ordered by (K, q') */
+static int table_n;
+static long cap;
+static cand *cands[3];
+static long ncand[3];
+static int build_table(void) {
   rb = 2 * n + 1;
   ng = 0;
   for (int q = 0; q < n; q++) for (int k = GH; k <= GZ; k++) { gate g = {k, q, 0}; G[ng++] = g; }
@@ -172,8 +157,9 @@ int main(int argc, char **argv) {
   const long order = n == 1 ? 24 : n == 2 ? 11520 : 92897280;
   int lg = 4;
   while ((1L << lg) < order * 4 / 3) lg++;
-  const long cap = 1L << lg;
+  cap = 1L << lg;
   mask = (uint64_t)cap - 1;
+  free(keys); free(dist);
   keys = calloc(cap, 8); dist = calloc(cap, 1);
   uint64_t *fa = malloc(8 * (order / 2 + 1024)), *fb = malloc(8 * (order / 2 + 1024));
   long nf = 1, total = 1;
@@ -193,20 +179,11 @@ int main(int argc, char **argv) {
   }
   free(fa); free(fb);
   fprintf(stderr, "clifford table: %ld elements (group order %ld), 0.0 s\n", total, order);
-  if (total != order) { fprintf(stderr, "group order mismatch\n"); return 4; }
+  if (total != order) { fprintf(stderr, "group order mismatch\n"); return 1; }
 
-  uint64_t *D = malloc(8 * (t + 1));
-  for (int j = 0; j <= t; j++) { uint64_t X = identity(); for (int i = 0; i < segn[j]; i++) X = apply(X, seg[j][i]); D[j] = X; }
-  if (dist_only) {   /* one line per segment: its minimal gate count */
-    for (int j = 0; j <= t; j++) printf("%d\n", find(D[j]));
-    return 0;
-  }
-
-  /* 2. beam search over the placements (clifford.cu:281-330) */
-  cand *cands[3] = {0};
-  long ncand[3] = {0};
   for (int q = 0; q < n; q++) {
     long m = 0, mcap = 1024;
+    free(cands[q]);
     cands[q] = malloc(sizeof(cand) * mcap);
     for (long s = 0; s < cap; s++) {
       const uint64_t K = keys[s];
@@ -223,8 +200,37 @@ int main(int argc, char **argv) {
     qsort(cands[q], m, sizeof(cand), candcmp);
     ncand[q] = m;
   }
-  int **parent = calloc(t + 1, sizeof(int *)), **flips = calloc(t + 1, sizeof(int *));
-  cand **chosen = calloc(t + 1, sizeof(cand *));
+  table_n = n;
+  return 0;
+}
+
+static int run_job(const char *path, int beam, int dist_only) {
+  FILE *f = fopen(path, "r");
+  int t = 0, bad = !f;
+  if (!bad && fscanf(f, "%d %d", &n, &t) != 2) bad = 1;
+  if (bad || t < 0 || t > 4096) { if (f) fclose(f); fprintf(stderr, "bad job file\n"); return 2; }
+  int *tq = calloc(t + 1, sizeof(int)), *td = calloc(t + 1, sizeof(int));
+  for (int i = 0; !bad && i < t; i++) if (fscanf(f, "%d %d", &tq[i], &td[i]) != 2) bad = 1;
+  gate **seg = calloc(t + 1, sizeof(gate *));
+  int *segn = calloc(t + 1, sizeof(int));
+  for (int j = 0; !bad && j <= t; j++) {
+    if (fscanf(f, "%d", &segn[j]) != 1 || segn[j] < 0) { bad = 1; break; }
+    seg[j] = calloc(segn[j] + 1, sizeof(gate));
+    for (int i = 0; i < segn[j]; i++) if (parse_gate(f, &seg[j][i])) { bad = 1; break; }
+  }
+  if (f) fclose(f);
+  if (bad || n < 1 || n > 3) { fprintf(stderr, "bad job file\n"); return 2; }
+  if (n != table_n && build_table()) return 4;
+  uint64_t *D = malloc(8 * (t + 1));
+  for (int j = 0; j <= t; j++) { uint64_t X = identity(); for (int i = 0; i < segn[j]; i++) X = apply(X, seg[j][i]); D[j] = X; }
+  if (dist_only) {   /* one line per segment: its minimal gate count */
+    for (int j = 0; j <= t; j++) printf("%d\n", find(D[j]));
+    return 0;
+  }
+
+  /* 2. beam search over the placements (clifford.cu:281-330) */
+  int **parent = calloc((size_t)t + 1, sizeof(int *)), **flips = calloc((size_t)t + 1, sizeof(int *));
+  cand **chosen = calloc((size_t)t + 1, sizeof(cand *));
   uint64_t Kprev[256];
   int bcost[256], nb = 1;
   bcost[0] = 0; Kprev[0] = 0;
@@ -303,4 +309,25 @@ int main(int argc, char **argv) {
     if (j < t) printf("%s %d\n", dag[j] ? "tdg" : "t", K[j].qp);
   }
   return 0;
+  return 0;
+}
+
+int main(int argc, char **argv) {
+  if (argc < 2) { fprintf(stderr, "usage: cliffopt JOB [--beam B]\n"); return 3; }
+  int beam = 16, dist_only = 0, njobs = 0;
+  const char *jobs[256];
+  for (int i = 1; i < argc; i++) {
+    if (!strcmp(argv[i], "--beam") && i + 1 < argc) { beam = atoi(argv[++i]); beam = beam < 1 ? 1 : beam > 255 ? 255 : beam; }
+    else if (!strcmp(argv[i], "--dist-only")) dist_only = 1;
+    else if (njobs < 256) jobs[njobs++] = argv[i];
+  }
+  /* several jobs share one table per qubit count: each output starts with a "### JOB" line */
+  int rc = 0;
+  for (int i = 0; i < njobs; i++) {
+    if (njobs > 1) { printf("### %s\n", jobs[i]); fflush(stdout); fprintf(stderr, "### %s\n", jobs[i]); }
+    rc = run_job(jobs[i], beam, dist_only);
+    fflush(stdout);
+    if (njobs > 1) printf("### rc %d\n", rc);
+  }
+  return rc;
 }

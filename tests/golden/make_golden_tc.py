@@ -11,6 +11,11 @@ by `make -C oracle refgpu`):
   runs the reference programs on every input (fresh table caches) and writes OUTDIR/tcount_cases.json and
   OUTDIR/cliffopt_cases.json: arguments, exit code, stdout ("seconds" values replaced by 0.00) and the stderr lines
   that carry results (table sizes, BFS counts per distance). The JSON files are committed under tests/golden/.
+
+Step 3 (any machine, after `make -C oracle oracle`):
+    python tests/golden/make_golden_tc.py oracle
+  writes tests/golden/cliffopt_oracle.json: the C restatement's cliffopt outputs for the jobs with T gates, whose
+  beam ties the reference leaves to an atomic counter (see oracle/clifford_oracle.c).
 """
 import json
 import os
@@ -44,6 +49,13 @@ def inputs(ref):
         reftc.write_spec(buf, n, refspec.unitary(n, circ))
         assert buf.getvalue() == tcwork.tspec(n, workloads.unitary(n, circ)), t
         (GOLD / "tcount" / f"{t}.tspec").write_text(buf.getvalue())
+    # the reference's published optimal decompositions (benchmarks/optimal/<t>-tcount.json: search levels with the
+    # K = 4 table loaded, then the result line), seconds stripped
+    opt = []
+    for t in TARGETS:
+        lines = (Path(ref) / "benchmarks" / "optimal" / f"{t}-tcount.json").read_text().splitlines()
+        opt.append({"name": t, "stdout": [SECONDS.sub('"seconds": 0.00', l) for l in lines if l.strip()]})
+    (GOLD / "tcount" / "optimal.json").write_text(json.dumps(opt, indent=1) + "\n")
     rng = random.Random(4096)
     for i in range(8):
         circ, k = tcwork.tcount_query(rng, 3)
@@ -60,14 +72,15 @@ def inputs(ref):
         (GOLD / "cliffopt" / f"t3-{i}.job").write_text(tcwork.random_clifford_job(rng, 3, 12, 2 + i))
 
 
-def run(exe, args, cwd):
-    p = subprocess.run([str(exe)] + args, capture_output=True, text=True, cwd=cwd, timeout=1800)
+def run(exe, args, cwd, timeout=600):
+    p = subprocess.run([str(exe)] + args, capture_output=True, text=True, cwd=cwd, timeout=timeout)
     out = [SECONDS.sub('"seconds": 0.00', l) for l in p.stdout.splitlines()]
     err = [re.sub(r"\(([0-9.]+) s\)|, [0-9.]+ s$|\(loaded, [0-9.]+ s\)", "", l) for l in p.stderr.splitlines()]
     return {"args": args, "rc": p.returncode, "stdout": out, "stderr": err}
 
 
 def outputs(outdir):
+    """every case is bounded (a few minutes at most on a B200); the JSON files are rewritten after each case"""
     outdir = Path(outdir)
     outdir.mkdir(parents=True, exist_ok=True)
     tc = ROOT / "oracle" / "_ref" / "tcount-ref"
@@ -78,9 +91,14 @@ def outputs(outdir):
     spec = lambda name: str(GOLD / "tcount" / f"{name}.tspec")
 
     def case(name, args):
-        r = run(tc, args, work)
+        try:
+            r = run(tc, args, work)
+        except subprocess.TimeoutExpired:
+            print(name, "timed out", file=sys.stderr, flush=True)
+            return
         r["name"] = name
         cases.append(r)
+        (outdir / "tcount_cases.json").write_text(json.dumps(cases, indent=1) + "\n")
         print(name, r["rc"], r["stdout"][-1] if r["stdout"] else "", file=sys.stderr, flush=True)
 
     # 3 qubits: the default table (K = 4) is built by the first run, loaded by the others
@@ -90,9 +108,11 @@ def outputs(outdir):
     for i in range(8):
         case(f"q3-{i}-k4", [spec(f"q3-{i}"), "--table", "4"])
     case("toffoli-k4-max5", [spec("toffoli"), "--table", "4", "--max", "5"])
-    for K in (1, 2, 3):
-        case(f"toffoli-k{K}", [spec("toffoli"), "--table", str(K)])
-    # 2 qubits: K = 6 (the driver's default for n <= 2) and smaller tables
+    # smaller tables: K = 3 needs four search levels for the Toffoli (K = 1, 2 need far more: not run)
+    case("toffoli-k3", [spec("toffoli"), "--table", "3"])
+    case("toffoli-k2-max4", [spec("toffoli"), "--table", "2", "--max", "4"])
+    case("toffoli-k1-max3", [spec("toffoli"), "--table", "1", "--max", "3"])
+    # 2 qubits: K = 6 and smaller tables
     case("cs-k6", [spec("cs"), "--table", "6"])
     case("qft_2-k6", [spec("qft_2"), "--table", "6"])
     for i in range(4):
@@ -100,20 +120,43 @@ def outputs(outdir):
     for K in (2, 4):
         case(f"cs-k{K}", [spec("cs"), "--table", str(K)])
         case(f"qft_2-k{K}", [spec("qft_2"), "--table", str(K)])
-    (outdir / "tcount_cases.json").write_text(json.dumps(cases, indent=1) + "\n")
 
     jobs = []
     for j in sorted((GOLD / "cliffopt").glob("*.job")):
-        r = run(co, [str(j)], work)
+        try:
+            r = run(co, [str(j)], work)
+        except subprocess.TimeoutExpired:
+            print(j.stem, "timed out", file=sys.stderr, flush=True)
+            continue
         r["name"] = j.stem
         jobs.append(r)
+        (outdir / "cliffopt_cases.json").write_text(json.dumps(jobs, indent=1) + "\n")
         print(j.stem, r["rc"], r["stdout"][:1], file=sys.stderr, flush=True)
-    (outdir / "cliffopt_cases.json").write_text(json.dumps(jobs, indent=1) + "\n")
     shutil.rmtree(work, ignore_errors=True)
 
 
+def oracle_outputs():
+    """the C restatement's outputs for the cliffopt jobs with T gates (3 qubits: about a minute of table build plus
+    minutes of beam per job on a few CPU cores), at beams 16 and 4 -> tests/golden/cliffopt_oracle.json. Its
+    candidate order is the product's, so these are exact expectations for the GPU path."""
+    exe = ROOT / "oracle" / "_ref" / "clifford-oracle"
+    jobs = sorted((GOLD / "cliffopt").glob("t3-*.job"))
+    out = []
+    for beam in (16, 4):
+        p = subprocess.run([str(exe)] + [str(j) for j in jobs] + ["--beam", str(beam)], capture_output=True, text=True,
+                           timeout=7200)
+        blocks = p.stdout.split("### ")[1:]
+        for j, blk in zip(jobs, [b for b in blocks if not b.startswith("rc ")]):
+            lines = blk.splitlines()[1:]
+            out.append({"name": j.stem, "beam": beam, "stdout": lines})
+        print("beam", beam, "done", file=sys.stderr, flush=True)
+    (GOLD / "cliffopt_oracle.json").write_text(json.dumps(out, indent=1) + "\n")
+
+
 if __name__ == "__main__":
-    if sys.argv[1] == "inputs":
+    if sys.argv[1] == "oracle":
+        oracle_outputs()
+    elif sys.argv[1] == "inputs":
         ref = sys.argv[sys.argv.index("--ref") + 1] if "--ref" in sys.argv else "/root/reference"
         inputs(ref)
     else:
