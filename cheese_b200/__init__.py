@@ -75,6 +75,22 @@ class CliffResult(C.Structure):
 CLIFF_STEP_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.c_int64, C.c_int)
 
 
+class ServerOptions(C.Structure):
+    _fields_ = [("device", C.c_int), ("memory_gb", C.c_double), ("max_jobs", C.c_int), ("tcount_table_k", C.c_int),
+                ("beam", C.c_int), ("cache_dir", C.c_char_p)]
+
+
+class ServerResult(C.Structure):
+    _fields_ = [("rc", C.c_int), ("kind", C.c_int), ("latency_s", C.c_double), ("queued_s", C.c_double),
+                ("gpu_work", C.c_int64), ("text_len", C.c_size_t), ("error", C.c_char * 256)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("batch_steps", C.c_int64),
+                ("batch_admitted", C.c_int64), ("batch_deferred", C.c_int64), ("batch_peak_running", C.c_int64),
+                ("batch_peak_bytes", C.c_int64), ("queued", C.c_int64 * 3)]
+
+
 class BatchInfo(C.Structure):
     _fields_ = [("nq", C.c_int), ("jobs", C.c_int), ("running", C.c_int), ("frontier", C.c_int64),
                 ("steps", C.c_int64), ("kernel_launches", C.c_int64), ("device_bytes", C.c_int64)]
@@ -115,8 +131,19 @@ SIGNATURES = {
     "cz_batch_submit": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Options)]),
     "cz_batch_step": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "cz_batch_info_get": (C.c_int, [C.c_void_p, C.POINTER(BatchInfo)]),
+    "cz_batch_error": (C.c_char_p, [C.c_void_p]),
     "cz_batch_done": (C.c_int, [C.c_void_p, C.c_int]),
     "cz_batch_result": (C.c_int, [C.c_void_p, C.c_int, LEVEL_FN, C.c_void_p, C.POINTER(Result)]),
+    "cz_server_options_default": (None, [C.POINTER(ServerOptions)]),
+    "cz_server_create": (C.c_int, [C.POINTER(ServerOptions), C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
+    "cz_server_destroy": (None, [C.c_void_p]),
+    "cz_server_submit": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_size_t, C.c_int]),
+    "cz_server_poll": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(ServerResult), C.c_char_p, C.c_size_t]),
+    "cz_server_wait": (C.c_int, [C.c_void_p, C.c_longlong, C.c_double]),
+    "cz_server_stats_get": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
+    "cz_server_replay": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_char_p),
+                                   C.POINTER(C.c_size_t), C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_double,
+                                   C.POINTER(C.c_int)]),
     "cz_version": (C.c_char_p, []),
 }
 
@@ -343,7 +370,7 @@ class Batch:
         r = C.c_int()
         rc = lib().cz_batch_step(self._h, C.byref(r))
         if rc:
-            raise RuntimeError(f"cz_batch_step failed: {rc}")
+            raise RuntimeError(f"cz_batch_step failed ({rc}): {lib().cz_batch_error(self._h).decode()}")
         return r.value
 
     def run(self):
@@ -377,6 +404,80 @@ class Batch:
         if getattr(self, "_h", None) and _lib is not None:
             _lib.cz_batch_destroy(self._h)
             self._h = None
+
+
+REQ_GATES, REQ_TCOUNT, REQ_CLIFFORD = 0, 1, 2
+
+
+class Server:
+    """the persistent request server (gate-count searches batched continuously, T-count and Clifford requests on
+    their own streams); results are the reference programs' stdout for each request"""
+
+    def __init__(self, device=0, memory_gb=150.0, max_jobs=4096, tcount_table_k=4, beam=16, cache_dir=None):
+        o = ServerOptions()
+        lib().cz_server_options_default(C.byref(o))
+        o.device, o.memory_gb, o.max_jobs, o.tcount_table_k, o.beam = device, memory_gb, max_jobs, tcount_table_k, beam
+        o.cache_dir = cache_dir.encode() if cache_dir else None
+        self._opt = o
+        self._h = C.c_void_p()
+        err = C.create_string_buffer(256)
+        rc = lib().cz_server_create(C.byref(o), C.byref(self._h), err, 256)
+        if rc:
+            raise RuntimeError(f"cz_server_create failed ({rc}): {err.value.decode()}")
+
+    def submit(self, kind, text, depth=-1):
+        b = text.encode() if isinstance(text, str) else text
+        rid = lib().cz_server_submit(self._h, kind, b, len(b), depth)
+        if rid < 0:
+            raise RuntimeError(f"cz_server_submit failed: {-rid}")
+        return rid
+
+    def poll(self, rid, cap=1 << 20):
+        res = ServerResult()
+        buf = C.create_string_buffer(cap)
+        st = lib().cz_server_poll(self._h, rid, C.byref(res), buf, cap)
+        if st < 0:
+            raise KeyError(rid)
+        if st == 0:
+            return None
+        if res.text_len >= cap:
+            return self.poll(rid, res.text_len + 1)
+        return {"rc": res.rc, "kind": res.kind, "latency_s": res.latency_s, "queued_s": res.queued_s,
+                "gpu_work": res.gpu_work, "text": buf.value.decode(), "error": res.error.decode()}
+
+    def wait(self, count, timeout=600.0):
+        return lib().cz_server_wait(self._h, count, timeout) == 0
+
+    def stats(self):
+        s = ServerStats()
+        lib().cz_server_stats_get(self._h, C.byref(s))
+        d = {k: getattr(s, k) for k, _ in ServerStats._fields_ if k != "queued"}
+        d["queued"] = list(s.queued)
+        return d
+
+    def replay(self, requests, arrivals, timeout=1800.0):
+        """requests [(kind, text, depth)], arrival offsets in seconds: submitted on time by the library; ids"""
+        n = len(requests)
+        kinds = (C.c_int * n)(*[k for k, _, _ in requests])
+        blobs = [t.encode() if isinstance(t, str) else t for _, t, _ in requests]
+        texts = (C.c_char_p * n)(*blobs)
+        lens = (C.c_size_t * n)(*[len(b) for b in blobs])
+        depths = (C.c_int * n)(*[d for _, _, d in requests])
+        arr = (C.c_double * n)(*arrivals)
+        ids = (C.c_int * n)()
+        rc = lib().cz_server_replay(self._h, n, kinds, texts, lens, depths, arr, timeout, ids)
+        if rc:
+            raise TimeoutError("replay did not finish")
+        return list(ids)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().cz_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        if _lib is not None:
+            self.close()
 
 
 class SearchOutcome:

@@ -23,8 +23,9 @@ HOSTCXX = os.environ.get("CZ_HOSTCXX", "/usr/bin/g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-ccbin", HOSTCXX, "-Xcompiler", "-fPIC"]
 
-LIB_SOURCES = ["cz_search.cu", "cz_tcount.cu", "cz_clifford.cu", "cz_spec.cpp", "cz_capi.cpp"]
-HEADERS = ["cz_common.h", "cz_spec.h", "cz_engine.h", "cz_sort.cuh", "cz_tcount.h", "cz_clifford.h", "cz_tableau.h"]
+LIB_SOURCES = ["cz_search.cu", "cz_tcount.cu", "cz_clifford.cu", "cz_spec.cpp", "cz_capi.cpp", "cz_serve.cpp"]
+HEADERS = ["cz_common.h", "cz_spec.h", "cz_engine.h", "cz_sort.cuh", "cz_tcount.h", "cz_clifford.h", "cz_tableau.h",
+           "cz_capi_internal.h"]
 BINARIES = {"cheese": "cli_cheese.cpp", "tcount": "cli_tcount.cpp", "cliffopt": "cli_cliffopt.cpp"}
 
 
@@ -59,7 +60,7 @@ def build(force=False, verbose=False, ptxas_info=False):
             extra = ["-Xptxas", "-v"] if (ptxas_info and s.endswith(".cu")) else []
             _run([NVCC, *COMMON, *ARCH, *extra, "-c", CSRC / s, "-o", o], verbose or ptxas_info)
             objs.append(o)
-        _run([NVCC, *COMMON, *ARCH, "-shared", *objs, "-o", LIB, "-lcudart"], verbose)
+        _run([NVCC, *COMMON, *ARCH, "-shared", *objs, "-o", LIB, "-lcudart", "-lpthread"], verbose)
     for name, src in BINARIES.items():
         out = BIN / name
         if force or _stale(out, [CSRC / src, LIB, ROOT / "include" / "cheese_b200.h"]):

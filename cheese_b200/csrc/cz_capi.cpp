@@ -7,15 +7,7 @@
 #include <new>
 #include <string>
 
-#include "../../include/cheese_b200.h"
-#include "cz_engine.h"
-#include "cz_spec.h"
-#include "cz_clifford.h"
-#include "cz_tcount.h"
-
-struct cz_spec { cz::HostSpec hs; };
-struct cz_batch { cz::BatchSession *b; };
-struct cz_engine { cz::Engine *e; cz::TcountContext *tc; cz::CliffordContext *cl; };
+#include "cz_capi_internal.h"
 
 namespace {
 void put_err(char *err, size_t n, const std::string &m) {
@@ -181,7 +173,7 @@ int cz_batch_create(cz_engine *engine, int nq, cz_batch **out) {
   if (!engine || !out || nq < 1 || nq > 3) return CZ_ERR_USAGE;
   *out = nullptr;
   try {
-    *out = new cz_batch{new cz::BatchSession(*engine->e, nq)};
+    *out = new cz_batch{new cz::BatchSession(*engine->e, nq), std::string()};
     return 0;
   } catch (const std::exception &) {
     return CZ_ERR_CUDA;
@@ -218,9 +210,13 @@ int cz_batch_step(cz_batch *batch, int *running) {
     const int r = batch->b->step();
     if (running) *running = r;
     return 0;
-  } catch (const std::exception &) {
+  } catch (const std::exception &ex) {
+    batch->err = ex.what();
     return CZ_ERR_CUDA;
   }
+}
+
+const char *cz_batch_error(const cz_batch *batch) { return batch ? batch->err.c_str() : "";
 }
 
 int cz_batch_info_get(const cz_batch *batch, cz_batch_info *out) {

@@ -109,6 +109,8 @@ class BatchSession {
   long long launches() const;          // kernels launched by the session
   long long steps() const;
   size_t device_bytes() const;         // device memory held by the session's buffers
+  // the frontier-memory estimate of the next step: the frontier plus room for every running job's children
+  size_t projected_bytes() const;
   struct Impl;
  private:
   Impl *impl_;

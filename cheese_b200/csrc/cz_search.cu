@@ -844,7 +844,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, 
 constexpr int BATCH_GS = 64;
 constexpr int MAXDEPTH_WALK = 48;   // deepest circuit of a batched job
 template <typename ST> struct BatchArgs {
-  long long m;
+  long long m, p0;                 // the chunk of the frontier this launch expands: nodes [p0, m)
   const Z4<ST> *R;
   const NodeMeta *meta;
   const uint32_t *fjob;             // job of every frontier node
@@ -876,7 +876,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand_batch(const BatchA
   unsigned conjmask = 0;
   for (;;) {
     unsigned long long p = 0;
-    if (lane == 0) p = atomicAdd(&a.st->work, 1ULL);
+    if (lane == 0) p = a.p0 + atomicAdd(&a.st->work, 1ULL);
     p = __shfl_sync(FULL, p, 0);
     if ((long long)p >= a.m) break;
     const int pj = (int)a.fjob[p];
@@ -1108,9 +1108,14 @@ struct DBuf {
   size_t cap = 0;
   void ensure(size_t bytes) {
     if (bytes <= cap) return;
+    const size_t old = cap;
     if (p) ck(cudaFree(p), "free");
-    size_t c = std::max(bytes, cap + cap / 2);
-    c = (c + 255) & ~(size_t)255;
+    p = nullptr;
+    cap = 0;
+    // grow by half again for small buffers; exactly (2 MiB granules) once a buffer passes 1 GiB
+    size_t c = bytes >= ((size_t)1 << 30) ? bytes : std::max(bytes, old + old / 2);
+    c = (c + ((size_t)2 << 20) - 1) & ~(((size_t)2 << 20) - 1);
+    if (bytes < ((size_t)2 << 20)) c = (bytes + 255) & ~(size_t)255;
     ck(cudaMalloc(&p, c), "cudaMalloc");
     cap = c;
   }
@@ -1189,9 +1194,10 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
   for (int t = t_start; t <= depth; t++) {
     const double t0 = now_s();
     const bool keep = t < depth;
-    // survivors capacity: every child that passes the window rules, bounded by what the previous level kept
+    // survivors capacity: every child, up to 32 GiB of survivor records; when more survive, the level is redone
+    // once with the exact count (the kernel counts every survivor, stored or not)
     unsigned long long cap = keep ? (unsigned long long)m * G : 0;
-    const unsigned long long cap_limit = (unsigned long long)8 << 30;   // 8 Gi residuals would be 8 TB: never hit
+    const unsigned long long cap_limit = ((unsigned long long)32 << 30) / (E * sizeof(Z4<ST>) + 40);
     if (cap > cap_limit) cap = cap_limit;
     DevStats *dst = stats.as<DevStats>();
     for (int attempt = 0; attempt < 2; attempt++) {
@@ -1839,6 +1845,7 @@ struct BatchSession::Impl {
   virtual long long launches() const = 0;
   virtual long long steps() const = 0;
   virtual size_t device_bytes() const = 0;
+  virtual size_t projected_bytes() const = 0;
 };
 
 namespace {
@@ -1907,6 +1914,14 @@ struct BatchImpl : BatchSession::Impl {
       b += x->cap;
     for (auto &x : tpar) b += x.cap;
     for (auto &x : tgat) b += x.cap;
+    return b;
+  }
+
+  size_t projected_bytes() const override {
+    const size_t node = E * sizeof(Z4<ST>) + sizeof(NodeMeta) + 4, surv = E * sizeof(Z4<ST>) + 40 + 36;
+    size_t b = (size_t)m * node;
+    for (const Job &j : J)
+      if (j.running && j.t < j.depth) b += (size_t)j.seg * (size_t)j.hs.G * surv;
     return b;
   }
 
@@ -2023,16 +2038,6 @@ struct BatchImpl : BatchSession::Impl {
     }
     const long long nr = (long long)roots.size();
     // grow the frontier (contents kept) and append the roots
-    auto grow_keep = [&](DBuf &b, size_t bytes, size_t keep) {
-      if (bytes <= b.cap) return;
-      DBuf nb;
-      nb.ensure(bytes);
-      if (keep) ck(cudaMemcpyAsync(nb.p, b.p, keep, cudaMemcpyDeviceToDevice, s), "d2d");
-      ck(cudaStreamSynchronize(s), "grow");
-      b.release();
-      b = nb;
-      nb.p = nullptr;
-    };
     grow_keep(fR, (size_t)(m + nr) * E * sizeof(Z4<ST>), (size_t)m * E * sizeof(Z4<ST>));
     grow_keep(fMeta, (size_t)(m + nr) * sizeof(NodeMeta), (size_t)m * sizeof(NodeMeta));
     grow_keep(fJob, (size_t)(m + nr) * 4, (size_t)m * 4);
@@ -2049,108 +2054,110 @@ struct BatchImpl : BatchSession::Impl {
     m += nr;
   }
 
+  // grow b to `bytes`, keeping its first `keep` bytes
+  void grow_keep(DBuf &b, size_t bytes, size_t keep) {
+    if (bytes <= b.cap) return;
+    DBuf nb;
+    nb.ensure(bytes + bytes / 2);
+    if (keep) ck(cudaMemcpyAsync(nb.p, b.p, keep, cudaMemcpyDeviceToDevice, s), "d2d");
+    ck(cudaStreamSynchronize(s), "grow");
+    b.release();
+    b = nb;
+    nb.p = nullptr;
+  }
+
+  // One level of every running job. The frontier holds the jobs in id order, each contiguous; it is processed in
+  // chunks of whole jobs whose children fit the survivor budget: expand, then (found / overflowed jobs leave)
+  // dedupe over the chunk's survivors and append its distinct children to the next frontier and the tree.
   int step() override {
     ck(cudaSetDevice(eng.device()), "cudaSetDevice");
     if (!queue.empty()) admit();
     if (m == 0) { nstep++; return running(); }
     const double t0 = now_s();
     const int nj = (int)J.size();
-    // per-job level and stats
     std::vector<int> ht(nj, 0);
     for (int i = 0; i < nj; i++) ht[i] = J[i].t;
     jt.ensure(nj * 4); jst.ensure(nj * sizeof(DevStats)); jact.ensure(nj + 4); jdist.ensure(nj * 8);
     ck(cudaMemcpyAsync(jt.p, ht.data(), nj * 4, cudaMemcpyHostToDevice, s), "h2d");
     k_jst_init<<<(nj + 255) / 256, 256, 0, s>>>(jst.as<DevStats>(), nj);
     nlaunch++;
-    // survivors: at most every child; retried with the exact count if that does not fit
-    unsigned long long cap = 0;
-    for (auto &j : J) if (j.running && j.t < j.depth) cap += (unsigned long long)j.seg * j.hs.G;
-    const unsigned long long cap_limit = (unsigned long long)24 << 20;   // survivors per attempt (24 Mi x 1 KB)
-    if (cap > cap_limit) cap = cap_limit;
-    DevStats *dst = stats.as<DevStats>();
-    DevStats h{};
-    for (int attempt = 0; attempt < 2; attempt++) {
-      if (cap) {
-        sH1.ensure(cap * 8); sH2.ensure(cap * 8); sIdx.ensure(cap * 8);
-        sR.ensure(cap * E * sizeof(Z4<ST>)); sMeta.ensure(cap * sizeof(NodeMeta));
+    const unsigned long long cap_limit = ((unsigned long long)32 << 30) / (E * sizeof(Z4<ST>) + 40);
+    // chunks of whole jobs (frontier order = id order)
+    struct Chunk { long long p0, p1; unsigned long long cap; std::vector<int> jobs; };
+    std::vector<Chunk> chunks;
+    {
+      Chunk c{0, 0, 0, {}};
+      long long off = 0;
+      for (int i = 0; i < nj; i++) {
+        Job &j = J[i];
+        if (!j.running || j.seg == 0) continue;
+        const unsigned long long need = j.t < j.depth ? (unsigned long long)j.seg * j.hs.G : 0;
+        if (!c.jobs.empty() && c.cap + need > cap_limit) { chunks.push_back(c); c = Chunk{off, off, 0, {}}; }
+        c.jobs.push_back(i);
+        c.cap += need;
+        off += j.seg;
+        c.p1 = off;
       }
-      ck(cudaMemsetAsync(dst, 0, sizeof(DevStats), s), "memset");
-      if (attempt) { k_jst_init<<<(nj + 255) / 256, 256, 0, s>>>(jst.as<DevStats>(), nj); nlaunch++; }
-      BatchArgs<ST> a;
-      a.m = m; a.R = fR.as<Z4<ST>>(); a.meta = fMeta.as<NodeMeta>(); a.fjob = fJob.as<uint32_t>();
-      a.specs = dspecs.as<DevSpec>(); a.jt = jt.as<int>(); a.jst = jst.as<DevStats>(); a.st = dst; a.cap = cap;
-      a.sh1 = sH1.as<uint64_t>(); a.sh2 = sH2.as<uint64_t>(); a.sidx = sIdx.as<uint64_t>();
-      a.sR = sR.as<Z4<ST>>(); a.smeta = sMeta.as<NodeMeta>();
-      const long long want = (m + EXP_WARPS - 1) / EXP_WARPS;
-      const long long grid = std::max<long long>(1, std::min<long long>(want, (long long)nsm * 2 * 8));
-      k_expand_batch<NQ, ST><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(a);
-      nlaunch++;
-      ck(cudaGetLastError(), "batched expand");
-      ck(cudaMemcpyAsync(&h, dst, sizeof(DevStats), cudaMemcpyDeviceToHost, s), "d2h");
-      ck(cudaStreamSynchronize(s), "batched expand");
-      if (!h.surv_overflow) break;
-      cap = h.n_surv;
+      if (!c.jobs.empty()) chunks.push_back(c);
+      if (off != m) throw std::logic_error("batch frontier out of step with its jobs");
     }
-    if (h.surv_overflow) throw CudaError("survivor buffer overflow");
+    if ((long long)tpar.size() <= nstep) { tpar.resize(nstep + 1); tgat.resize(nstep + 1); }
     std::vector<DevStats> hj(nj);
-    ck(cudaMemcpyAsync(hj.data(), jst.p, nj * sizeof(DevStats), cudaMemcpyDeviceToHost, s), "d2h");
-    ck(cudaStreamSynchronize(s), "job stats");
-    // found / overflowed jobs leave; the others go on to dedupe
     std::vector<uint8_t> act(nj, 0);
-    std::vector<int> found_ids, overflow_ids;
-    size_t nsort = 0;
-    for (int i = 0; i < nj; i++) {
-      Job &j = J[i];
-      if (!j.running) continue;
-      if (hj[i].ovf) { overflow_ids.push_back(i); continue; }
-      if (hj[i].found) { found_ids.push_back(i); continue; }
-      act[i] = 1;
-      if (j.t < j.depth) nsort += hj[i].alive;
-    }
-    if (!found_ids.empty()) {
-      // circuits: walk each found child back through the tree (one thread per job)
-      const int nf = (int)found_ids.size();
-      std::vector<unsigned long long> fo(nf);
-      std::vector<int> ft(nf), fs(nf);
-      for (int i = 0; i < nf; i++) { fo[i] = hj[found_ids[i]].first_found; ft[i] = J[found_ids[i]].t; fs[i] = (int)nstep; }
-      std::vector<const uint32_t *> pp(nstep + 1, nullptr);
-      std::vector<const uint8_t *> gp(nstep + 1, nullptr);
-      for (long long st2 = 0; st2 < nstep && st2 < (long long)tpar.size(); st2++) { pp[st2] = tpar[st2].as<uint32_t>(); gp[st2] = tgat[st2].as<uint8_t>(); }
-      const size_t pb = pp.size() * sizeof(void *);
-      tptr.ensure(2 * pb + (size_t)nf * (8 + 4 + 4) + (size_t)nf * MAXDEPTH_WALK * 4 + 64);
-      char *base = (char *)tptr.p;
-      ck(cudaMemcpyAsync(base, pp.data(), pb, cudaMemcpyHostToDevice, s), "h2d");
-      ck(cudaMemcpyAsync(base + pb, gp.data(), pb, cudaMemcpyHostToDevice, s), "h2d");
-      char *q = base + 2 * pb;
-      unsigned long long *dfo = (unsigned long long *)q; q += (size_t)nf * 8;
-      int *dft = (int *)q; q += (size_t)nf * 4;
-      int *dfs = (int *)q; q += (size_t)nf * 4;
-      int *dout = (int *)q;
-      ck(cudaMemcpyAsync(dfo, fo.data(), nf * 8, cudaMemcpyHostToDevice, s), "h2d");
-      ck(cudaMemcpyAsync(dft, ft.data(), nf * 4, cudaMemcpyHostToDevice, s), "h2d");
-      ck(cudaMemcpyAsync(dfs, fs.data(), nf * 4, cudaMemcpyHostToDevice, s), "h2d");
-      k_walk<<<(nf + 63) / 64, 64, 0, s>>>(dfo, dft, dfs, nf, (const uint32_t *const *)base,
-                                           (const uint8_t *const *)(base + pb), dout);
-      nlaunch++;
-      std::vector<int> circ((size_t)nf * MAXDEPTH_WALK);
-      ck(cudaMemcpyAsync(circ.data(), dout, circ.size() * 4, cudaMemcpyDeviceToHost, s), "d2h");
-      ck(cudaStreamSynchronize(s), "walk");
-      for (int i = 0; i < nf; i++) {
-        Job &j = J[found_ids[i]];
-        j.out.res.circuit.assign(circ.begin() + (size_t)i * MAXDEPTH_WALK, circ.begin() + (size_t)i * MAXDEPTH_WALK + j.t);
-        j.out.res.n_found = (long long)hj[found_ids[i]].found;
-        j.out.res.levels = j.t;
-        account(j, hj[found_ids[i]]);
-        finish(j, RC_CIRCUIT);
-      }
-    }
-    // dedupe of the running jobs' survivors (one sort over all of them)
     std::vector<unsigned long long> dist(nj, 0);
-    size_t distinct = 0;
-    const uint64_t *ki = nullptr;
-    const uint32_t *vi = nullptr;
-    if (nsort) {
-      ck(cudaMemcpyAsync(jact.p, act.data(), nj, cudaMemcpyHostToDevice, s), "h2d");
+    std::vector<int> overflow_ids;
+    size_t total_distinct = 0;
+    DevStats *dst = stats.as<DevStats>();
+    for (const Chunk &ch : chunks) {
+      const long long cm = ch.p1 - ch.p0;
+      const int jlo = ch.jobs.front(), jn = ch.jobs.back() - jlo + 1;
+      unsigned long long cap = std::min<unsigned long long>(ch.cap, cap_limit);
+      DevStats h{};
+      for (int attempt = 0; attempt < 2; attempt++) {
+        if (cap) {
+          sH1.ensure(cap * 8); sH2.ensure(cap * 8); sIdx.ensure(cap * 8);
+          sR.ensure(cap * E * sizeof(Z4<ST>)); sMeta.ensure(cap * sizeof(NodeMeta));
+        }
+        ck(cudaMemsetAsync(dst, 0, sizeof(DevStats), s), "memset");
+        if (attempt) {                                   // the chunk's jobs start over (ids jlo..jhi)
+          k_jst_init<<<(jn + 255) / 256, 256, 0, s>>>(jst.as<DevStats>() + jlo, jn);
+          nlaunch++;
+        }
+        BatchArgs<ST> a;
+        a.m = ch.p1; a.p0 = ch.p0;
+        a.R = fR.as<Z4<ST>>(); a.meta = fMeta.as<NodeMeta>(); a.fjob = fJob.as<uint32_t>();
+        a.specs = dspecs.as<DevSpec>(); a.jt = jt.as<int>(); a.jst = jst.as<DevStats>(); a.st = dst; a.cap = cap;
+        a.sh1 = sH1.as<uint64_t>(); a.sh2 = sH2.as<uint64_t>(); a.sidx = sIdx.as<uint64_t>();
+        a.sR = sR.as<Z4<ST>>(); a.smeta = sMeta.as<NodeMeta>();
+        const long long want = (cm + EXP_WARPS - 1) / EXP_WARPS;
+        const long long grid = std::max<long long>(1, std::min<long long>(want, (long long)nsm * 2 * 8));
+        k_expand_batch<NQ, ST><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(a);
+        nlaunch++;
+        ck(cudaGetLastError(), "batched expand");
+        ck(cudaMemcpyAsync(&h, dst, sizeof(DevStats), cudaMemcpyDeviceToHost, s), "d2h");
+        ck(cudaStreamSynchronize(s), "batched expand");
+        if (!h.surv_overflow) break;
+        cap = h.n_surv;                                   // every survivor was counted: redo with the exact room
+      }
+      if (h.surv_overflow) throw std::runtime_error("survivor buffer overflow");
+      ck(cudaMemcpyAsync(hj.data() + jlo, jst.as<DevStats>() + jlo, jn * sizeof(DevStats), cudaMemcpyDeviceToHost, s),
+         "d2h");
+      ck(cudaStreamSynchronize(s), "job stats");
+      std::vector<int> found_ids;
+      size_t nsort = 0;
+      for (int i : ch.jobs) {
+        Job &j = J[i];
+        if (hj[i].ovf) { overflow_ids.push_back(i); continue; }
+        if (hj[i].found) { found_ids.push_back(i); continue; }
+        act[i] = 1;
+        if (j.t < j.depth) nsort += hj[i].alive;
+      }
+      if (!found_ids.empty()) walk(found_ids, hj);
+      if (!nsort) continue;
+      // dedupe of the chunk's running jobs' survivors
+      std::vector<uint8_t> cact(nj, 0);
+      for (int i : ch.jobs) cact[i] = act[i];
+      ck(cudaMemcpyAsync(jact.p, cact.data(), nj, cudaMemcpyHostToDevice, s), "h2d");
       const size_t ns = (size_t)h.n_surv;
       k0.ensure(nsort * 8); k1.ensure(nsort * 8); v0.ensure(nsort * 4); v1.ensure(nsort * 4);
       kidx.ensure(nsort * 8); kslot.ensure(nsort * 4); work.ensure(nsort * sizeof(uint2)); tmp.ensure(nsort * 4);
@@ -2183,41 +2190,43 @@ struct BatchImpl : BatchSession::Impl {
       ck(cudaGetLastError(), "batched dedupe");
       ck(cudaMemcpyAsync(&h, dst, sizeof(DevStats), cudaMemcpyDeviceToHost, s), "d2h");
       ck(cudaStreamSynchronize(s), "batched dedupe");
-      distinct = (size_t)h.n_kept;
+      const size_t distinct = (size_t)h.n_kept;
       ck(cudaMemsetAsync(jdist.p, 0, nj * 8, s), "memset");
       k_bcount<<<(unsigned)std::max<size_t>(1, std::min<size_t>((distinct + 255) / 256, (size_t)nsm * 16)), 256, 0, s>>>(
           kidx.as<uint64_t>(), distinct, fJob.as<uint32_t>(), jdist.as<unsigned long long>());
       nlaunch++;
-      ck(cudaMemcpyAsync(dist.data(), jdist.p, nj * 8, cudaMemcpyDeviceToHost, s), "d2h");
-      // the next frontier in child-index order (every job's children contiguous, in its own order)
+      std::vector<unsigned long long> cd(nj, 0);
+      ck(cudaMemcpyAsync(cd.data(), jdist.p, nj * 8, cudaMemcpyDeviceToHost, s), "d2h");
+      // the chunk's distinct children in child-index order, appended to the next frontier and this step's tree
       int bits = 1;
-      while (bits < 64 && ((unsigned long long)m * BATCH_GS) >> bits) bits++;
+      while (bits < 64 && ((unsigned long long)ch.p1 * BATCH_GS) >> bits) bits++;
       const int hi = ((bits + 7) / 8) * 8;
       ln = 0;
       const bool f2 = radix_sort(kidx.as<uint64_t>(), kslot.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(),
                                  distinct, 0, hi, sc, s, &ln);
       nlaunch += ln;
-      ki = f2 ? k1.as<uint64_t>() : kidx.as<uint64_t>();
-      vi = f2 ? v1.as<uint32_t>() : kslot.as<uint32_t>();
-      if ((long long)tpar.size() <= nstep) { tpar.resize(nstep + 1); tgat.resize(nstep + 1); }
-      tpar[nstep].ensure(distinct * 4 + 4);
-      tgat[nstep].ensure(distinct + 4);
-      fR2.ensure(distinct * E * sizeof(Z4<ST>) + 16); fMeta2.ensure(distinct * sizeof(NodeMeta) + 16);
-      fJob2.ensure(distinct * 4 + 4);
+      const uint64_t *ki = f2 ? k1.as<uint64_t>() : kidx.as<uint64_t>();
+      const uint32_t *vi = f2 ? v1.as<uint32_t>() : kslot.as<uint32_t>();
+      const size_t o0 = total_distinct, o1 = total_distinct + distinct;
+      grow_keep(tpar[nstep], o1 * 4 + 4, o0 * 4);
+      grow_keep(tgat[nstep], o1 + 4, o0);
+      grow_keep(fR2, o1 * E * sizeof(Z4<ST>) + 16, o0 * E * sizeof(Z4<ST>));
+      grow_keep(fMeta2, o1 * sizeof(NodeMeta) + 16, o0 * sizeof(NodeMeta));
+      grow_keep(fJob2, o1 * 4 + 4, o0 * 4);
       const size_t tot = distinct * E;
       const unsigned gg = (unsigned)std::max<size_t>(1, std::min<size_t>((tot + 255) / 256, (size_t)nsm * 32));
       k_gather<ST><<<gg, 256, 0, s>>>(ki, vi, distinct, BATCH_GS, E, sR.as<Z4<ST>>(), sMeta.as<NodeMeta>(),
-                                      fR2.as<Z4<ST>>(), fMeta2.as<NodeMeta>(), tpar[nstep].as<uint32_t>(),
-                                      tgat[nstep].as<uint8_t>());
+                                      fR2.as<Z4<ST>>() + o0 * E, fMeta2.as<NodeMeta>() + o0,
+                                      tpar[nstep].as<uint32_t>() + o0, tgat[nstep].as<uint8_t>() + o0);
       k_fjob_next<<<(unsigned)std::max<size_t>(1, std::min<size_t>((distinct + 255) / 256, (size_t)nsm * 16)), 256, 0, s>>>(
-          ki, distinct, fJob.as<uint32_t>(), fJob2.as<uint32_t>());
+          ki, distinct, fJob.as<uint32_t>(), fJob2.as<uint32_t>() + o0);
       nlaunch += 2;
       ck(cudaGetLastError(), "batched gather");
       ck(cudaStreamSynchronize(s), "batched gather");
-      std::swap(fR, fR2); std::swap(fMeta, fMeta2); std::swap(fJob, fJob2);
-    } else if ((long long)tpar.size() <= nstep) {
-      tpar.resize(nstep + 1); tgat.resize(nstep + 1);
+      for (int i : ch.jobs) dist[i] = cd[i];
+      total_distinct = o1;
     }
+    std::swap(fR, fR2); std::swap(fMeta, fMeta2); std::swap(fJob, fJob2);
     // level lines of the running jobs
     const double secs = now_s() - t0;
     for (int i = 0; i < nj; i++) {
@@ -2234,20 +2243,60 @@ struct BatchImpl : BatchSession::Impl {
       j.out.res.prefixes += L.prefixes;
       account(j, d);
       j.out.res.levels = j.t;
-      if (L.distinct == 0) { finish(j, RC_PROOF); continue; }
+      if (L.distinct == 0) { j.seg = 0; finish(j, RC_PROOF); continue; }
       j.seg = L.distinct;
       j.t++;
     }
-    m = (long long)distinct;
+    m = (long long)total_distinct;
     nstep++;
     // jobs whose int32 limbs overflowed: rerun alone (the plain path promotes them to int64)
     for (int id : overflow_ids) {
       Job &j = J[id];
       if (j.running) nrun--;
       j.running = false;
+      j.seg = 0;
       run_plain(j);
     }
     return running();
+  }
+
+  // circuits of the jobs that found the goal at this step: one thread per job walks the tree back
+  void walk(const std::vector<int> &found_ids, const std::vector<DevStats> &hj) {
+    const int nf = (int)found_ids.size();
+    std::vector<unsigned long long> fo(nf);
+    std::vector<int> ft(nf), fs(nf);
+    for (int i = 0; i < nf; i++) { fo[i] = hj[found_ids[i]].first_found; ft[i] = J[found_ids[i]].t; fs[i] = (int)nstep; }
+    std::vector<const uint32_t *> pp(nstep + 1, nullptr);
+    std::vector<const uint8_t *> gp(nstep + 1, nullptr);
+    for (long long st2 = 0; st2 < nstep && st2 < (long long)tpar.size(); st2++) { pp[st2] = tpar[st2].as<uint32_t>(); gp[st2] = tgat[st2].as<uint8_t>(); }
+    const size_t pb = pp.size() * sizeof(void *);
+    tptr.ensure(2 * pb + (size_t)nf * (8 + 4 + 4) + (size_t)nf * MAXDEPTH_WALK * 4 + 64);
+    char *base = (char *)tptr.p;
+    ck(cudaMemcpyAsync(base, pp.data(), pb, cudaMemcpyHostToDevice, s), "h2d");
+    ck(cudaMemcpyAsync(base + pb, gp.data(), pb, cudaMemcpyHostToDevice, s), "h2d");
+    char *q = base + 2 * pb;
+    unsigned long long *dfo = (unsigned long long *)q; q += (size_t)nf * 8;
+    int *dft = (int *)q; q += (size_t)nf * 4;
+    int *dfs = (int *)q; q += (size_t)nf * 4;
+    int *dout = (int *)q;
+    ck(cudaMemcpyAsync(dfo, fo.data(), nf * 8, cudaMemcpyHostToDevice, s), "h2d");
+    ck(cudaMemcpyAsync(dft, ft.data(), nf * 4, cudaMemcpyHostToDevice, s), "h2d");
+    ck(cudaMemcpyAsync(dfs, fs.data(), nf * 4, cudaMemcpyHostToDevice, s), "h2d");
+    k_walk<<<(nf + 63) / 64, 64, 0, s>>>(dfo, dft, dfs, nf, (const uint32_t *const *)base,
+                                         (const uint8_t *const *)(base + pb), dout);
+    nlaunch++;
+    std::vector<int> circ((size_t)nf * MAXDEPTH_WALK);
+    ck(cudaMemcpyAsync(circ.data(), dout, circ.size() * 4, cudaMemcpyDeviceToHost, s), "d2h");
+    ck(cudaStreamSynchronize(s), "walk");
+    for (int i = 0; i < nf; i++) {
+      Job &j = J[found_ids[i]];
+      j.out.res.circuit.assign(circ.begin() + (size_t)i * MAXDEPTH_WALK, circ.begin() + (size_t)i * MAXDEPTH_WALK + j.t);
+      j.out.res.n_found = (long long)hj[found_ids[i]].found;
+      j.out.res.levels = j.t;
+      account(j, hj[found_ids[i]]);
+      j.seg = 0;
+      finish(j, RC_CIRCUIT);
+    }
   }
   void account(Job &j, const DevStats &d) {
     j.out.res.t_evals += (long long)d.t_evals;
@@ -2277,5 +2326,6 @@ long long BatchSession::frontier() const { return impl_->frontier(); }
 long long BatchSession::launches() const { return impl_->launches(); }
 long long BatchSession::steps() const { return impl_->steps(); }
 size_t BatchSession::device_bytes() const { return impl_->device_bytes(); }
+size_t BatchSession::projected_bytes() const { return impl_->projected_bytes(); }
 
 }  // namespace cz

@@ -413,11 +413,12 @@ struct Buf {
 
 // a tree of peel sequences: level l holds (parent, rotation) per node; keys of the top level
 struct Tree {
-  std::vector<Buf> par, gat;       // index 0 unused (the root)
+  std::vector<Buf> par = std::vector<Buf>(1), gat = std::vector<Buf>(1);   // level l at [l]; [0] unused (the root)
   std::vector<long long> n{1};
   Buf F1, F2;                      // keys of the top level
   int top() const { return (int)n.size() - 1; }
   THist hist() const {
+    if (par.size() != n.size() || gat.size() != n.size()) throw std::logic_error("tree levels out of step");
     THist H{};
     for (int l = 1; l <= top() && l <= MAXT; l++) { H.par[l] = par[l].as<uint32_t>(); H.gat[l] = gat[l].as<uint8_t>(); }
     return H;

@@ -107,11 +107,57 @@ void cz_batch_destroy(cz_batch *batch);
 int cz_batch_submit(cz_batch *batch, const cz_spec *spec, const cz_options *opt);
 /* One level of every running job (admitting the queued ones first); *running = jobs not finished yet. */
 int cz_batch_step(cz_batch *batch, int *running);
+/* the message of the last failed cz_batch_step ("" if none) */
+const char *cz_batch_error(const cz_batch *batch);
 int cz_batch_info_get(const cz_batch *batch, cz_batch_info *out);
 /* 1 when the job has finished. */
 int cz_batch_done(const cz_batch *batch, int job);
 /* A finished job: its level lines through on_level (in order) and its result, as cz_search gives them. */
 int cz_batch_result(const cz_batch *batch, int job, cz_level_fn on_level, void *user, cz_result *out);
+
+/* ---------------- serving (no counterpart in the reference) ----------------
+ * A persistent request server on one GPU. Requests of three kinds arrive at any time; each kind has a worker thread
+ * with its own engine and stream, so their device work overlaps: gate-count searches are continuously batched
+ * (admitted at the next level step while the batch's frontier-memory estimate leaves room under memory_gb),
+ * T-count queries and Clifford-segment jobs use their resident tables. A request's output text is the stdout the
+ * reference program prints for it ("seconds" fields 0.00). */
+typedef struct cz_server cz_server;
+#define CZ_REQ_GATES 0            /* text: a cheese spec; depth: budget (-1: the spec's) */
+#define CZ_REQ_TCOUNT 1           /* text: a tcount-spec */
+#define CZ_REQ_CLIFFORD 2         /* text: a cliffopt job */
+typedef struct {
+  int device;
+  double memory_gb;               /* device memory the gate-count batch may plan for */
+  int max_jobs;                   /* gate-count jobs running at once */
+  int tcount_table_k;             /* --table K of T-count queries */
+  int beam;                       /* --beam of Clifford jobs */
+  const char *cache_dir;          /* T-count table cache directory (NULL: none) */
+} cz_server_options;
+typedef struct {
+  int rc, kind;
+  double latency_s, queued_s;     /* submit -> done, submit -> started */
+  int64_t gpu_work;               /* prefixes (gate count), children (T count), placements (Clifford) */
+  size_t text_len;
+  char error[256];
+} cz_server_result;
+typedef struct {
+  int64_t submitted, completed, batch_steps, batch_admitted, batch_deferred, batch_peak_running, batch_peak_bytes;
+  int64_t queued[3];
+} cz_server_stats;
+void cz_server_options_default(cz_server_options *opt);
+int cz_server_create(const cz_server_options *opt, cz_server **out, char *err, size_t errlen);
+void cz_server_destroy(cz_server *server);
+/* the request id (>= 0), or -(exit code) */
+int cz_server_submit(cz_server *server, int kind, const char *text, size_t len, int depth);
+/* 1 done (out and text filled), 0 still running, < 0 unknown id */
+int cz_server_poll(cz_server *server, int id, cz_server_result *out, char *text, size_t text_cap);
+/* wait until `count` requests have completed since the server started: 0, or 1 on timeout */
+int cz_server_wait(cz_server *server, long long count, double timeout_s);
+int cz_server_stats_get(cz_server *server, cz_server_stats *out);
+/* Submit request i at arrival_s[i] seconds after the call (host clock), then wait for all of them: ids[i] gets
+ * each request id. 0, or 1 on timeout. */
+int cz_server_replay(cz_server *server, int n, const int *kinds, const char *const *texts, const size_t *lens,
+                     const int *depths, const double *arrival_s, double timeout_s, int *ids);
 
 /* Convenience for FFI callers that hold the spec as text: parse + search in one call. */
 int cz_search_text(cz_engine *engine, const char *spec_text, size_t len, const cz_options *opt, cz_level_fn on_level,

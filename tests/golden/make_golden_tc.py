@@ -97,6 +97,7 @@ def outputs(outdir):
             print(name, "timed out", file=sys.stderr, flush=True)
             return
         r["name"] = name
+        r["args"] = [str(Path(args[0]).relative_to(ROOT))] + args[1:]
         cases.append(r)
         (outdir / "tcount_cases.json").write_text(json.dumps(cases, indent=1) + "\n")
         print(name, r["rc"], r["stdout"][-1] if r["stdout"] else "", file=sys.stderr, flush=True)
@@ -129,6 +130,7 @@ def outputs(outdir):
             print(j.stem, "timed out", file=sys.stderr, flush=True)
             continue
         r["name"] = j.stem
+        r["args"] = [str(j.relative_to(ROOT))]
         jobs.append(r)
         (outdir / "cliffopt_cases.json").write_text(json.dumps(jobs, indent=1) + "\n")
         print(j.stem, r["rc"], r["stdout"][:1], file=sys.stderr, flush=True)
