@@ -122,6 +122,8 @@ SIGNATURES = {
     "cz_clifford_dist": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.c_size_t, C.POINTER(C.c_int)]),
     "cz_clifford_element": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.c_size_t,
                                       C.POINTER(C.c_uint64)]),
+    "cz_clifford_words": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.c_size_t, C.POINTER(C.c_int),
+                                    C.POINTER(C.c_int)]),
     "cz_cliffjob_check": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_char_p,
                                     C.c_size_t]),
     "cz_cliffopt": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.c_int, CLIFF_STEP_FN, C.c_void_p, C.c_char_p,
@@ -299,6 +301,25 @@ class Engine:
         if rc:
             raise RuntimeError(f"cz_clifford_element failed: {rc}")
         return list(out[:m])
+
+    def clifford_words(self, n, tableaux):
+        """optimal words [(gate name, qubits)] of tableaux (from the resident Clifford table)"""
+        m = len(tableaux)
+        arr = (C.c_uint64 * max(m, 1))(*tableaux)
+        words = (C.c_int * (max(m, 1) * 32 * 3))()
+        lens = (C.c_int * max(m, 1))()
+        rc = lib().cz_clifford_words(self._h, n, arr, m, words, lens)
+        if rc:
+            raise RuntimeError(f"cz_clifford_words failed: {rc}")
+        names = ["h", "s", "sdg", "x", "z", "cx", "y"]
+        out = []
+        for i in range(m):
+            w = []
+            for j in range(lens[i]):
+                k, a, b = words[(i * 32 + j) * 3:(i * 32 + j) * 3 + 3]
+                w.append((names[k], (a, b) if k == 5 else (a,)))
+            out.append(w)
+        return out
 
     def cliffopt(self, job, beam=16, on_step=None):
         """`cliffopt JOB --beam B`: (rc, result dict, output lines after the JSON line, step tuples)"""

@@ -450,6 +450,23 @@ int cz_clifford_dist(cz_engine *engine, int n, const uint64_t *tableaux, size_t 
   }
 }
 
+int cz_clifford_words(cz_engine *engine, int n, const uint64_t *tableaux, size_t count, int *words, int *lens) {
+  if (!engine || (count && (!tableaux || !words || !lens))) return CZ_ERR_USAGE;
+  try {
+    std::string e;
+    std::vector<std::vector<int>> w;
+    const int rc = cz::clifford_words(cliff_ctx(engine), n, tableaux, count, w, e);
+    if (rc) return rc;
+    for (size_t i = 0; i < count; i++) {
+      lens[i] = (int)(w[i].size() / 3);
+      for (size_t j = 0; j < w[i].size() && j < (size_t)CZ_CLIFFORD_WORDMAX * 3; j++) words[i * CZ_CLIFFORD_WORDMAX * 3 + j] = w[i][j];
+    }
+    return 0;
+  } catch (const std::exception &) {
+    return CZ_ERR_CUDA;
+  }
+}
+
 int cz_clifford_element(cz_engine *engine, int n, const uint64_t *index, size_t count, uint64_t *tableaux) {
   if (!engine || (count && (!index || !tableaux))) return CZ_ERR_USAGE;
   try {

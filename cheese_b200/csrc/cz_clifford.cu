@@ -824,6 +824,28 @@ int clifford_dist(CliffordContext *c, int n, const uint64_t *tabp, size_t count,
   }
 }
 
+int clifford_words(CliffordContext *c, int n, const uint64_t *tabp, size_t count,
+                   std::vector<std::vector<int>> &words, std::string &err) {
+  CliffTableInfo info;
+  const int rc = clifford_table(c, n, info, err);
+  if (rc) return rc;
+  try {
+    std::vector<std::vector<int>> w;
+    c->words(*c->tables[n], std::vector<uint64_t>(tabp, tabp + count), w);
+    const GateSet gs = gate_set(n);
+    words.assign(count, {});
+    for (size_t i = 0; i < count; i++)
+      for (int g : w[i]) { words[i].push_back(gs.k[g]); words[i].push_back(gs.a[g]); words[i].push_back(gs.b[g]); }
+    return 0;
+  } catch (const std::logic_error &e) {
+    err = e.what();
+    return 4;
+  } catch (const std::exception &e) {
+    err = e.what();
+    return 5;
+  }
+}
+
 int clifford_element(CliffordContext *c, int n, const uint64_t *index, size_t count, uint64_t *tabp, std::string &err) {
   CliffTableInfo info;
   const int rc = clifford_table(c, n, info, err);

@@ -46,6 +46,9 @@ int cliffopt_run(CliffordContext *c, const CliffJob &job, int beam,
                  const std::function<void(int, const CliffStep &)> &on_step, CliffOptResult &res);
 // minimal gate counts of tableaux (-1: not a valid tableau)
 int clifford_dist(CliffordContext *c, int n, const uint64_t *tab, size_t count, int *out, std::string &err);
+// an optimal word of each tableau: (kind, a, b) triples, kinds as in the job grammar (h s sdg x z cx y = 0..6)
+int clifford_words(CliffordContext *c, int n, const uint64_t *tab, size_t count,
+                   std::vector<std::vector<int>> &words, std::string &err);
 // the group element of each rank (index in [0, order))
 int clifford_element(CliffordContext *c, int n, const uint64_t *index, size_t count, uint64_t *tab, std::string &err);
 

@@ -1131,6 +1131,16 @@ uint64_t powmod_h(uint64_t a, uint64_t e) {
 
 }  // namespace
 
+// survivor records to provision for `children` children at an expected survivor rate: 1.5x the expectation
+// plus 4096, at least 1 Mi (never more than every child), at most 32 GiB of records
+inline unsigned long long survivor_room(unsigned long long children, double rate, size_t rec = 1064) {
+  const unsigned long long lim = ((unsigned long long)32 << 30) / rec;
+  double want = 1.5 * rate * (double)children + 4096.0;
+  if (want < (double)(1 << 20)) want = (double)(1 << 20);
+  unsigned long long cap = want >= (double)children ? children : (unsigned long long)want;
+  return cap > lim ? lim : cap;
+}
+
 struct Engine::Impl {
   int dev;
   int nsm = 148;
@@ -1191,14 +1201,14 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
   constexpr int E = (1 << NQ) * (1 << NQ);
   const int G = hs.G;
   long long m = front_m;
+  double surv_rate = 1.0;                              // survivors per child of the previous level
   for (int t = t_start; t <= depth; t++) {
     const double t0 = now_s();
     const bool keep = t < depth;
-    // survivors capacity: every child, up to 32 GiB of survivor records; when more survive, the level is redone
-    // once with the exact count (the kernel counts every survivor, stored or not)
-    unsigned long long cap = keep ? (unsigned long long)m * G : 0;
-    const unsigned long long cap_limit = ((unsigned long long)32 << 30) / (E * sizeof(Z4<ST>) + 40);
-    if (cap > cap_limit) cap = cap_limit;
+    // survivors capacity: the previous level's survivor rate with room to spare (at least 1 Mi records, at most
+    // every child); when more survive, the level is redone once with the exact count (the kernel counts every
+    // survivor, stored or not)
+    unsigned long long cap = keep ? survivor_room((unsigned long long)m * G, surv_rate, E * sizeof(Z4<ST>) + 40) : 0;
     DevStats *dst = stats.as<DevStats>();
     for (int attempt = 0; attempt < 2; attempt++) {
       if (keep) {
@@ -1232,6 +1242,7 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
     }
     if (hstats->surv_overflow) { res.error = "survivor buffer overflow"; return RC_CUDA; }
     const DevStats h = *hstats;
+    if (m * G > 0) surv_rate = (double)h.alive / ((double)m * G);
     res.t_evals += (long long)h.t_evals;
     res.children += (long long)h.children;
     res.children_full += (long long)h.full;
@@ -1861,6 +1872,7 @@ struct BatchImpl : BatchSession::Impl {
     DevSpec sp;
     int t = 1;                       // the level this job runs at its next step
     long long seg = 0;               // its nodes in the frontier
+    double rate = 1.0;               // survivors per child at its previous level
     bool queued = true, running = false;
     BatchJob out;
   };
@@ -2081,25 +2093,30 @@ struct BatchImpl : BatchSession::Impl {
     ck(cudaMemcpyAsync(jt.p, ht.data(), nj * 4, cudaMemcpyHostToDevice, s), "h2d");
     k_jst_init<<<(nj + 255) / 256, 256, 0, s>>>(jst.as<DevStats>(), nj);
     nlaunch++;
-    const unsigned long long cap_limit = ((unsigned long long)32 << 30) / (E * sizeof(Z4<ST>) + 40);
-    // chunks of whole jobs (frontier order = id order)
-    struct Chunk { long long p0, p1; unsigned long long cap; std::vector<int> jobs; };
+    const size_t rec = E * sizeof(Z4<ST>) + 40;
+    const unsigned long long cap_limit = ((unsigned long long)32 << 30) / rec;
+    // chunks of whole jobs (frontier order = id order) whose expected survivors fit the budget; each chunk's room
+    // is its jobs' expected survivors (previous survivor rate x 1.5) and never more than all their children
+    struct Chunk { long long p0, p1; unsigned long long cap, all; std::vector<int> jobs; };
     std::vector<Chunk> chunks;
     {
-      Chunk c{0, 0, 0, {}};
+      Chunk c{0, 0, 0, 0, {}};
       long long off = 0;
       for (int i = 0; i < nj; i++) {
         Job &j = J[i];
         if (!j.running || j.seg == 0) continue;
-        const unsigned long long need = j.t < j.depth ? (unsigned long long)j.seg * j.hs.G : 0;
-        if (!c.jobs.empty() && c.cap + need > cap_limit) { chunks.push_back(c); c = Chunk{off, off, 0, {}}; }
+        const unsigned long long all = j.t < j.depth ? (unsigned long long)j.seg * j.hs.G : 0;
+        const unsigned long long want = all ? std::min<unsigned long long>(all, (unsigned long long)(1.5 * j.rate * (double)all) + 4096) : 0;
+        if (!c.jobs.empty() && c.cap + want > cap_limit) { chunks.push_back(c); c = Chunk{off, off, 0, 0, {}}; }
         c.jobs.push_back(i);
-        c.cap += need;
+        c.cap += want;
+        c.all += all;
         off += j.seg;
         c.p1 = off;
       }
       if (!c.jobs.empty()) chunks.push_back(c);
       if (off != m) throw std::logic_error("batch frontier out of step with its jobs");
+      for (Chunk &ch : chunks) ch.cap = std::min(ch.all, std::max<unsigned long long>(ch.cap, 1 << 20));
     }
     if ((long long)tpar.size() <= nstep) { tpar.resize(nstep + 1); tgat.resize(nstep + 1); }
     std::vector<DevStats> hj(nj);
@@ -2239,6 +2256,7 @@ struct BatchImpl : BatchSession::Impl {
       L.distinct = j.t < j.depth ? (long long)dist[i] : 0;
       L.proved_unsat = L.distinct == 0;
       L.seconds = secs;
+      if (j.seg * j.hs.G > 0) j.rate = (double)d.alive / ((double)j.seg * j.hs.G);
       j.out.levels.push_back(L);
       j.out.res.prefixes += L.prefixes;
       account(j, d);

@@ -53,22 +53,74 @@ def pauli(n, p):
     return tuple(out)
 
 
+_MONO = {}
+
+
+def _monomial(n):
+    """per Pauli p: flip[p] (P_p maps column x to row x ^ flip) and ph[p, x] (entry w^ph)"""
+    if n not in _MONO:
+        P, N = 4 ** n, 1 << n
+        flip = np.zeros(P, dtype=np.int64)
+        ph = np.zeros((P, N), dtype=np.int64)
+        for p in range(P):
+            for x in range(N):
+                f = k = 0
+                for q in range(n):
+                    d, bit = (p >> (2 * q)) & 3, (x >> q) & 1
+                    if d == 1:
+                        f |= 1 << q
+                    elif d == 2:
+                        f |= 1 << q
+                        k += 2 + 4 * bit
+                    elif d == 3:
+                        k += 4 * bit
+                flip[p] = f
+                ph[p, x] = k & 7
+        _MONO[n] = (flip, ph)
+    return _MONO[n]
+
+
+def _wrot(v, k):
+    """w^k v elementwise: v holds Z[w] values as (4, ...) components, k integers shaped like v[0] (w^4 = -1)"""
+    if np.ndim(k) == 0:                                       # one power for every element: a signed rotation
+        k = int(k) % 8
+        out = np.empty_like(v)
+        for i in range(4):
+            j = (i - k) % 4
+            out[i] = -v[j] if ((j + k) // 4) % 2 else v[j]
+        return out
+    k = np.asarray(k) % 8
+    out = np.empty_like(v)
+    for i in range(4):
+        j = (i - k) % 4                                       # the component that lands on w^i
+        neg = ((j + k) // 4) % 2 == 1
+        val = np.take_along_axis(v, j[None], axis=0)[0]
+        out[i] = np.where(neg, -val, val)
+    return out
+
+
 def channel(n, U):
-    """(e, x, y) int arrays: Uc[a][b] = (x + y sqrt2) / sqrt2^e, normalised (e minimal)"""
+    """(e, x, y) int arrays: Uc[a][b] = (x + y sqrt2) / sqrt2^e, normalised (e minimal).
+    P_b is monomial, so U P_b U^dag is two column gathers and one Z[w] matrix product per b, and Tr(P_a A) is a
+    gather of A's entries at (x ^ flip_a, x) times w-powers, for all a at once."""
     k, M = U
     N, P = 1 << n, 4 ** n
-    Mz = tuple(np.array([[M[r][c][i] for c in range(N)] for r in range(N)], dtype=np.int64) for i in range(4))
-    Md = zmat_dag(Mz)
-    paulis = [pauli(n, p) for p in range(P)]
+    Mz = np.array([[M[r][c] for c in range(N)] for r in range(N)], dtype=np.int64).transpose(2, 0, 1)   # (4, N, N)
+    Md = np.stack(zmat_dag(tuple(Mz)))
+    flip, ph = _monomial(n)
+    xs = np.arange(N)
     X = np.zeros((P, P), dtype=np.int64)
     Y = np.zeros((P, P), dtype=np.int64)
+    rows = xs[None, :] ^ flip[:, None]                      # (P, N): row index x ^ flip_a
+    phs = ph[np.arange(P)[:, None], rows]                    # Tr(P_a A) = sum_x w^ph_a(x ^ f_a) A[x ^ f_a, x]
     for b in range(P):
-        A = zmat_mul(zmat_mul(Mz, paulis[b]), Md)          # sqrt2^2k U P_b U^dag
-        for a in range(P):
-            T = zmat_mul(paulis[a], A)
-            tr = [int(np.trace(t)) for t in T]
-            assert tr[2] == 0 and tr[3] == -tr[1], "trace not real"
-            X[a, b], Y[a, b] = tr[0], tr[1]                # value (x + y sqrt2) / sqrt2^(2k + 2n)
+        cols = xs ^ flip[b]                                  # (Mz P_b)[r, y] = Mz[r, y ^ flip_b] w^ph_b(y)
+        MP = _wrot(Mz[:, :, cols], np.broadcast_to(ph[b][None, :], (N, N)))
+        A = np.stack(zmat_mul(tuple(MP), tuple(Md)))        # (4, N, N): sqrt2^2k U P_b U^dag
+        G = A[:, rows, xs[None, :]]                          # (4, P, N): A[x ^ flip_a, x]
+        T = _wrot(G, phs).sum(axis=2)                        # (4, P): Tr(P_a A)
+        assert (T[2] == 0).all() and (T[3] == -T[1]).all(), "trace not real"
+        X[:, b], Y[:, b] = T[0], T[1]
     e = 2 * k + 2 * n
     while e > 0 and not (X & 1).any():                     # (x + y s) / s = y + (x / 2) s
         X, Y = Y, X // 2
@@ -170,8 +222,31 @@ def random_clifford_job(rng, n=3, length=40, tcount=0):
     return cliffopt_job(n, ts, segs)
 
 
+def unitary_np(n, circ):
+    """the exact unitary of a gate list as workloads.unitary gives it (same gates, same normal form), computed with
+    numpy row operations: (k, M) with M an N x N nested list of Z[w] 4-tuples"""
+    from .workloads import _GATES
+    N = 1 << n
+    U = np.zeros((4, N, N), dtype=np.int64)
+    U[0] = np.eye(N, dtype=np.int64)
+    k = 0
+    for g, qs in circ:
+        gk, loc = _GATES[g]
+        mask = sum(1 << q for q in qs)
+        bases = np.array([b for b in range(N) if not b & mask], dtype=np.int64)
+        rows = {l: bases | sum(((l >> j) & 1) << q for j, q in enumerate(qs)) for l in range(1 << len(qs))}
+        new = np.zeros_like(U)
+        for (l, m), pw in loc.items():
+            new[:, rows[l], :] += _wrot(U[:, rows[m], :], pw)
+        U = new
+        if gk:                                                # keep the normal form (entries stay small)
+            k, U = _zden(k + gk, tuple(U))
+            U = np.stack(U)
+    return k, [[tuple(int(v) for v in U[:, r, c]) for c in range(N)] for r in range(N)]
+
+
 def tspec_of_circuit(n, circ):
-    return tspec(n, unitary(n, circ))
+    return tspec(n, unitary_np(n, circ))
 
 
 # ---------- exact check of a T-count decomposition (the role of tcount.py verify, :171-185) ----------
@@ -231,3 +306,64 @@ def verify_decomposition(n, U, rotations):
         Xi = X if inv else zmat_dag(X)                        # X_i^-1: R(P)^dag = R(P)^-1
         W = _zden(W[0] + kr, zmat_mul(Xi, W[1]))
     return is_clifford(n, W[0], W[1])
+
+
+# ---------------- table-driven workloads (uniform group elements from the resident Clifford table) ----------------
+CLIFFORD_ORDER = {1: 24, 2: 11520, 3: 92897280}
+
+
+def uniform_clifford_words(engine, n, rng, count):
+    """`count` uniform random n-qubit Cliffords (up to phase) as optimal words: a uniform index into the group's
+    rank table, that element's optimal word from the distance table"""
+    idx = [rng.randrange(CLIFFORD_ORDER[n]) for _ in range(count)]
+    return engine.clifford_words(n, engine.clifford_element(n, idx))
+
+
+def table_queries(engine, seed, count=1024, n=3):
+    """the table-driven T-count workload: U = C0 T(q1) C1 ... T(qk) Ck with k uniform in [1, 7], Ci uniform group
+    elements, qi uniform qubits: [(circuit, k)]"""
+    rng = random.Random(seed)
+    ks = [rng.randint(1, 7) for _ in range(count)]
+    words = uniform_clifford_words(engine, n, rng, sum(k + 1 for k in ks))
+    out, w = [], 0
+    for k in ks:
+        circ = list(words[w])
+        w += 1
+        for _ in range(k):
+            circ.append(("t", (rng.randrange(n),)))
+            circ += words[w]
+            w += 1
+        out.append((circ, k))
+    return out
+
+
+def serve_requests(engine, seed, count):
+    """the serving mix: 60% gate-count searches (random 2-3 qubit circuits as in the batched workload, budgets
+    4..11), 30% T-count queries (as table_queries), 10% Clifford-segment minimisations (random 3-qubit Clifford
+    words as zero-T cliffopt jobs): [(kind, text, depth, info)] with kind 0 / 1 / 2"""
+    from .workloads import make_spec, random_circuit
+    rng = random.Random(seed)
+    kinds = [0 if u < 0.6 else (1 if u < 0.9 else 2) for u in (rng.random() for _ in range(count))]
+    nq = sum(1 for k in kinds if k == 1)
+    queries = table_queries(engine, seed + 1, nq) if nq else []
+    out, qi = [], 0
+    for kind in kinds:
+        if kind == 0:
+            n, circ = random_circuit(rng, L=rng.randint(4, 11))
+            out.append((0, make_spec(n, circ, len(circ)), -1, {"n": n, "circuit": circ}))
+        elif kind == 1:
+            circ, k = queries[qi]
+            qi += 1
+            out.append((1, tspec_of_circuit(3, circ), -1, {"n": 3, "circuit": circ, "k": k}))
+        else:
+            out.append((2, random_clifford_job(rng, 3, 40, 0), -1, {"n": 3}))
+    return out
+
+
+def poisson_arrivals(seed, count, rate):
+    rng = random.Random(seed)
+    t, out = 0.0, []
+    for _ in range(count):
+        t += rng.expovariate(rate)
+        out.append(t)
+    return out

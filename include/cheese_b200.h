@@ -260,6 +260,10 @@ typedef struct {
 int cz_clifford_table(cz_engine *engine, int n, cz_clifford_table_info *out, char *err, size_t errlen);
 /* Minimal gate counts of tableaux (-1 for a word that is not a valid tableau). */
 int cz_clifford_dist(cz_engine *engine, int n, const uint64_t *tableaux, size_t count, int *out);
+/* An optimal word of each tableau (the read-back of clifford.cu:352-371): words = count x CZ_CLIFFORD_WORDMAX x
+ * (kind, a, b), kinds 0..6 = h s sdg x z cx y, lens = gates per word. */
+#define CZ_CLIFFORD_WORDMAX 32
+int cz_clifford_words(cz_engine *engine, int n, const uint64_t *tableaux, size_t count, int *words, int *lens);
 /* The group element of each index in [0, order): index -> element is a fixed bijection (uniform draws). */
 int cz_clifford_element(cz_engine *engine, int n, const uint64_t *index, size_t count, uint64_t *tableaux);
 

@@ -1,0 +1,69 @@
+"""The serving loop on the GPU: a seeded Poisson stream of gate-count, T-count and Clifford-segment requests is
+answered while requests overlap on the device, and every answer equals the plain entry point's answer for the same
+request on its own (same stdout lines and exit code)."""
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def eng():
+    from cheese_b200 import Engine
+    return Engine()
+
+
+def _plain_text(eng, kind, text, depth):
+    if kind == 0:
+        r = eng.search(text, depth=depth)
+        return r.rc, "".join(l + "\n" for l in r.lines())
+    if kind == 1:
+        from test_gpu_tcount import lines
+        rc, levels, res = eng.tcount(text, table_k=4, cache_dir=None)
+        return rc, "".join(l + "\n" for l in lines(levels, rc, res))
+    rc, res, out, _ = eng.cliffopt(text)
+    head = (f'{{"clifford_gates": {res["clifford_gates"]}, "clifford_gates_before": {res["clifford_gates_before"]}, '
+            f'"t_gates": {res["t_gates"]}, "seconds": 0.00}}\n')
+    return rc, head + "".join(l + "\n" for l in out)
+
+
+def test_served_equals_alone(eng):
+    from cheese_b200 import Server, tcwork
+    reqs = tcwork.serve_requests(eng, 21, 48)
+    assert {k for k, *_ in reqs} == {0, 1, 2}
+    srv = Server(memory_gb=100)
+    try:
+        ids = srv.replay([(k, t, d) for k, t, d, _ in reqs], tcwork.poisson_arrivals(3, len(reqs), 200.0))
+        st = srv.stats()
+        assert st["completed"] == len(reqs)
+        for (kind, text, depth, info), rid in zip(reqs, ids):
+            got = srv.poll(rid)
+            assert got is not None and got["kind"] == kind
+            rc, want = _plain_text(eng, kind, text, depth)
+            assert got["rc"] == rc, (kind, got["error"])
+            assert got["text"] == want
+            assert got["latency_s"] >= got["queued_s"] >= 0
+            if kind == 1 and rc == 0:
+                import json
+                res = json.loads(want.splitlines()[-1])
+                assert res["tcount"] <= info["k"]
+                from cheese_b200 import tcwork as tw
+                assert tw.verify_decomposition(3, tw.unitary_np(3, info["circuit"]), res["rotations"])
+    finally:
+        srv.close()
+
+
+def test_admission_under_a_small_budget(eng):
+    """a memory budget that holds only a few jobs at once defers the rest; answers are unchanged"""
+    from cheese_b200 import Server, workloads
+    jobs = [(n, workloads.make_spec(n, c, d)) for n, c, d in workloads.batch(31, 24)]
+    srv = Server(memory_gb=0.05, max_jobs=4)
+    try:
+        ids = srv.replay([(0, s, -1) for _, s in jobs], [0.0] * len(jobs))
+        st = srv.stats()
+        assert st["batch_peak_running"] <= 4
+        for (n, s), rid in zip(jobs, ids):
+            rc, want = _plain_text(eng, 0, s, -1)
+            got = srv.poll(rid)
+            assert got["rc"] == rc and got["text"] == want
+    finally:
+        srv.close()
