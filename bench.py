@@ -159,6 +159,88 @@ def reference_arm(args, ws, rank):
         "e2e": {"value": v, "unit": "prefixes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
+def systems(eng, args):
+    """the batched, served and table-driven workloads beside the headline metric (one GPU)"""
+    import statistics
+    import cheese_b200 as cz
+    from cheese_b200 import tcwork, workloads
+    out = {}
+    # batched search: 512 seeded targets, plain job by job vs one batch session per qubit count
+    jobs = workloads.batch(1, 512)
+    specs = [cz.Spec(workloads.make_spec(n, c, d)) for n, c, d in jobs]
+    eng.search(specs[0])
+    t0 = time.perf_counter()
+    plain = [eng.search(s) for s in specs]
+    tp = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    sess = {n: cz.Batch(eng, n) for n in (2, 3)}
+    ids = [sess[s.n].submit(s) for s in specs]
+    for b in sess.values():
+        b.run()
+    tb = time.perf_counter() - t0
+    bad = sum(1 for s, i, p in zip(specs, ids, plain)
+              if (lambda r: r.rc != p.rc or r.lines() != p.lines() or r.circuit != p.circuit)(sess[s.n].result(i)))
+    out["batched"] = {"workload": "512 seeded targets: random circuits of L in [6,12] gates over 2-3 qubits "
+                                  "(T/Tdg with prob 0.3), budget L", "plain_jobs_s": 512 / tp, "batched_jobs_s": 512 / tb,
+                      "speedup": tp / tb, "mismatches": bad,
+                      "launches": sum(b.info()["kernel_launches"] for b in sess.values()),
+                      "steps": sum(b.info()["steps"] for b in sess.values())}
+    del sess, plain
+    # table-driven T count: Clifford BFS table + K = 4 coset table (3 qubits), then seeded queries, each verified
+    t0 = time.perf_counter()
+    ct = eng.clifford_table(3)
+    t_cl = time.perf_counter() - t0
+    qs = tcwork.table_queries(eng, 4, 1024)
+    nq = min(len(qs), 256)
+    specs_t = [tcwork.tspec_of_circuit(3, c) for c, _ in qs[:nq]]
+    t0 = time.perf_counter()
+    rc, lv, r0 = eng.tcount(specs_t[0], table_k=4, cache_dir=None)
+    t_tab = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    res = [eng.tcount(t, table_k=4, cache_dir=None) for t in specs_t]
+    t_q = time.perf_counter() - t0
+    ver = sum(1 for (c, k), (rc, _, r) in zip(qs[:nq], res)
+              if rc == 0 and r["tcount"] <= k and tcwork.verify_decomposition(3, tcwork.unitary_np(3, c), r["rotations"]))
+    out["table_tcount"] = {"workload": f"{nq} of 1024 seeded queries C0 T C1 .. T Ck, k in [1,7], Ci uniform 3-qubit "
+                                       "Cliffords (uniform index into the BFS table, its optimal word)",
+                           "clifford_table_s": ct["seconds"] if ct["built"] else t_cl,
+                           "clifford_elements": ct["elements"], "coset_table_s": r0["table_seconds"],
+                           "coset_table_cosets": r0["table_cosets"], "queries": nq, "queries_s": nq / t_q,
+                           "ms_per_query": 1e3 * t_q / nq, "verified": ver}
+    # serving: seeded Poisson streams of the mixed workload, against the same requests run one by one
+    N = args.serve_requests
+    reqs = tcwork.serve_requests(eng, 5, N)
+    t0 = time.perf_counter()
+    for kind, text, depth, _ in reqs:
+        if kind == 0:
+            eng.search(text, depth=depth)
+        elif kind == 1:
+            eng.tcount(text, table_k=4, cache_dir=None)
+        else:
+            eng.cliffopt(text)
+    t_seq = time.perf_counter() - t0
+    srv = cz.Server(memory_gb=100.0)
+    warm = [srv.submit(k, t) for k, t, _, _ in [next(r for r in reqs if r[0] == 1), next(r for r in reqs if r[0] == 2)]]
+    srv.wait(2, 900)
+    rates = {}
+    for rate in (10, 30, 100, 300, 1000):
+        arr = tcwork.poisson_arrivals(rate, N, rate)
+        t0 = time.perf_counter()
+        rid = srv.replay([(k, t, d) for k, t, d, _ in reqs], arr)
+        wall = time.perf_counter() - t0
+        lat = sorted(srv.poll(i)["latency_s"] for i in rid)
+        rates[str(rate)] = {"jobs_s": N / wall, "p50_ms": 1e3 * lat[len(lat) // 2],
+                            "p99_ms": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))]}
+    st = srv.stats()
+    srv.close()
+    out["served"] = {"workload": f"{N} requests per rate: 60% gate-count searches (2-3 qubits, budgets 4..11), 30% "
+                                 "T-count queries, 10% Clifford-segment minimisations; seeded Poisson arrivals",
+                     "sequential_jobs_s": N / t_seq, "rates": rates,
+                     "peak_jobs_s_vs_sequential": max(v["jobs_s"] for v in rates.values()) / (N / t_seq),
+                     "batch_peak_running": st["batch_peak_running"], "batch_steps": st["batch_steps"]}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -166,6 +248,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-systems", action="store_true", help="skip the batched / served / table-driven lines")
+    ap.add_argument("--serve-requests", type=int, default=120)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     ws, rank, local = dist_init() if args.impl == "ours" else (int(os.environ.get("WORLD_SIZE", "1")),
@@ -260,6 +344,7 @@ def main():
         cp, cs = run_ref_cpu(cases, threads)
         cpu = {"value": cp / cs, "unit": "prefixes/s", "cores": threads, "kind": "reference",
                "sample": "ccz-8 + toffoli-11 once, reference CPU build (OpenMP), %.1f s" % cs}
+    extra = systems(eng, args) if (rank == 0 and ws == 1 and not args.no_systems) else {}
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": "prefixes/s", "n_gpus": ws, "steps": args.steps,
@@ -279,6 +364,7 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }
+        out.update(extra)
         print(json.dumps(out))
     if ws > 1:
         import torch.distributed as dist

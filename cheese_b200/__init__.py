@@ -93,7 +93,8 @@ class ServerStats(C.Structure):
 
 class BatchInfo(C.Structure):
     _fields_ = [("nq", C.c_int), ("jobs", C.c_int), ("running", C.c_int), ("frontier", C.c_int64),
-                ("steps", C.c_int64), ("kernel_launches", C.c_int64), ("device_bytes", C.c_int64)]
+                ("steps", C.c_int64), ("kernel_launches", C.c_int64), ("device_bytes", C.c_int64),
+                ("waits", C.c_int64)]
 
 # every C entry point of include/cheese_b200.h with its ctypes signature
 SIGNATURES = {
@@ -131,6 +132,7 @@ SIGNATURES = {
     "cz_batch_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "cz_batch_destroy": (None, [C.c_void_p]),
     "cz_batch_submit": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Options)]),
+    "cz_batch_set_memory": (C.c_int, [C.c_void_p, C.c_double]),
     "cz_batch_step": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "cz_batch_info_get": (C.c_int, [C.c_void_p, C.POINTER(BatchInfo)]),
     "cz_batch_error": (C.c_char_p, [C.c_void_p]),
@@ -369,12 +371,14 @@ class Engine:
 class Batch:
     """a batch session of one qubit count on an engine: submit specs, step, collect SearchOutcomes"""
 
-    def __init__(self, engine, nq):
+    def __init__(self, engine, nq, memory_gb=None):
         self.engine = engine
         self._h = C.c_void_p()
         rc = lib().cz_batch_create(engine._h, nq, C.byref(self._h))
         if rc:
             raise RuntimeError(f"cz_batch_create failed: {rc}")
+        if memory_gb is not None:
+            lib().cz_batch_set_memory(self._h, memory_gb)
         self.specs = {}
 
     def submit(self, spec, depth=-1, dedupe=True, sym=True, store64=False):

@@ -186,6 +186,12 @@ void cz_batch_destroy(cz_batch *batch) {
   delete batch;
 }
 
+int cz_batch_set_memory(cz_batch *batch, double gb) {
+  if (!batch || !(gb > 0)) return CZ_ERR_USAGE;
+  batch->b->set_memory_budget((size_t)(gb * 1e9));
+  return 0;
+}
+
 int cz_batch_submit(cz_batch *batch, const cz_spec *spec, const cz_options *opt) {
   if (!batch || !spec) return -CZ_ERR_USAGE;
   const cz::HostSpec &hs = spec->hs;
@@ -228,6 +234,7 @@ int cz_batch_info_get(const cz_batch *batch, cz_batch_info *out) {
   out->steps = batch->b->steps();
   out->kernel_launches = batch->b->launches();
   out->device_bytes = (int64_t)batch->b->device_bytes();
+  out->waits = batch->b->waits();
   return 0;
 }
 

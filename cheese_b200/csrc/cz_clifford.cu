@@ -74,7 +74,10 @@ struct Gen {
 
 struct ClCudaError : std::runtime_error { using std::runtime_error::runtime_error; };
 void clk(cudaError_t e, const char *what) {
-  if (e != cudaSuccess) throw ClCudaError(std::string("CUDA error after ") + what + ": " + cudaGetErrorString(e));
+  if (e != cudaSuccess) {
+    cudaGetLastError();            // a failed allocation must not be reported again by the next launch check
+    throw ClCudaError(std::string("CUDA error after ") + what + ": " + cudaGetErrorString(e));
+  }
 }
 double cl_now() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
 

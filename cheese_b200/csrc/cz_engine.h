@@ -111,6 +111,10 @@ class BatchSession {
   size_t device_bytes() const;         // device memory held by the session's buffers
   // the frontier-memory estimate of the next step: the frontier plus room for every running job's children
   size_t projected_bytes() const;
+  // device bytes a step may plan for (default: 80% of the free memory when the session was made); jobs beyond it
+  // wait a step, their nodes carried over
+  void set_memory_budget(size_t bytes);
+  long long waits() const;             // job-steps spent waiting for memory
   struct Impl;
  private:
   Impl *impl_;

@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -73,7 +74,19 @@ struct DevStats {
   unsigned long long w2, w3, dead, alive, found, first_found, n_surv, t_evals, children, work, full;
   unsigned int ovf, surv_overflow;
   unsigned long long n_work, n_kept;
+  unsigned long long n_tq, tq_work;   // deferred T evaluations: queued, taken
 };
+
+// A T-bound evaluation deferred from the level kernel to k_tbound: the parent, up to two children that share one
+// T bound (odd diagonals on one qubit: P T_q = (P Tdg_q) S_q with S_q Clifford), and the bounds already known
+// (k, the CX bound, its per-cut needs and the H structure are the parent's for these one-qubit diagonal gates).
+struct TQEntry {
+  unsigned long long p;
+  int16_t k;
+  uint8_t n, g[2], c2, needs, hs, ntriv[2];
+  uint8_t pad[4];
+};
+static_assert(sizeof(TQEntry) == 24, "T queue entry layout");
 
 template <typename ST> struct ExpandArgs {
   long long m;
@@ -83,8 +96,9 @@ template <typename ST> struct ExpandArgs {
   DevStats *st;
   unsigned long long cap;
   uint64_t *sh1, *sh2, *sidx;
-  Z4<ST> *sR;
   NodeMeta *smeta;
+  TQEntry *tq;                     // deferred T evaluations (nullptr: in place)
+  unsigned long long tqcap;
 };
 
 // ---------------- arithmetic helpers ----------------
@@ -678,12 +692,15 @@ struct WarpTally {
     *this = WarpTally{};
   }
 };
+// a survivor is a 32-byte record (class key, child index, bounds); its residual is recomputed from the parent
+// where it is needed (exact class comparison, the next frontier)
 template <typename ST> struct ExpandOut {
   DevStats *st;                    // survivor slot counter and overflow flag
   unsigned long long cap;
   uint64_t *sh1, *sh2, *sidx;
-  Z4<ST> *sR;
   NodeMeta *smeta;
+  TQEntry *tq;                     // deferred T evaluations (nullptr: evaluate in place)
+  unsigned long long tqcap;
 };
 
 // every child of parent p (residual already in P): window rules, exact prechecks, child residual, bounds, class key,
@@ -702,6 +719,28 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
   const int suppP = __popc(ntP);
   const bool pre_ok = sp.standard && kP < INHERIT_KMAX;
   unsigned tcache = 0;                       // per qubit: 1 + T bound of its odd-diagonal child (0: unknown)
+  unsigned long long pend[3] = {0, 0, 0};    // per qubit: 1 + queue entry of its deferred odd-diagonal child
+  // queue a deferred T evaluation: a second odd diagonal on the same qubit joins its sibling's entry
+  auto defer = [&](int g, int k, int c2, int needs, int hs, int ntriv, int q0, bool tdiag) {
+    if (tdiag && pend[q0]) {
+      const unsigned long long e = pend[q0] - 1;
+      if (lane == 0) { o.tq[e].g[1] = (uint8_t)g; o.tq[e].ntriv[1] = (uint8_t)ntriv; o.tq[e].n = 2; }
+      pend[q0] = 0;                          // an entry holds two children
+      return;
+    }
+    unsigned long long e = 0;
+    if (lane == 0) e = atomicAdd(&o.st->n_tq, 1ULL);
+    e = __shfl_sync(FULL, e, 0);
+    if (e >= o.tqcap) return;                // counted: the host redoes the level with room for every entry
+    if (lane == 0) {
+      TQEntry q;
+      q.p = p; q.k = (int16_t)k; q.n = 1; q.g[0] = (uint8_t)g; q.g[1] = 0xff; q.c2 = (uint8_t)c2;
+      q.needs = (uint8_t)needs; q.hs = (uint8_t)hs; q.ntriv[0] = (uint8_t)ntriv; q.ntriv[1] = 0;
+      q.pad[0] = q.pad[1] = q.pad[2] = q.pad[3] = 0;
+      o.tq[e] = q;
+    }
+    if (tdiag) pend[q0] = e + 1;
+  };
   for (int g = 0; g < G; g++) {
     if (g1 >= 0 && __ldg(&sp.bad2[g1 * G + g])) { c.w2++; continue; }
     if (g2 >= 0) {
@@ -751,6 +790,7 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
       else {
         if (inheritT) T = TP;
         else if (cacheT && tc >= 0) T = tc;
+        else if (o.tq) { defer(g, k, 0, 0, 0, 0, q0, cacheT && (fl & GF_ONEQ) && k == kP); continue; }
         else {
           T = ptm_bound<NQ, ST>(C, k, lane); c.teval++;
           if (cacheT) tcache |= (unsigned)(T + 1) << (8 * q0);
@@ -767,6 +807,12 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
       else {
         if (inheritT) T = TP;
         else if (cacheT && tc >= 0) T = tc;
+        else if (o.tq) {
+          // siblings share an entry only when every bound but support is the parent's (one-qubit monomial gates)
+          const bool share = cacheT && (fl & GF_ONEQ) && (fl & GF_MONAFF) && k == kP;
+          defer(g, k, c2, needs, hs, ch.ntriv, q0, share);
+          continue;
+        }
         else {
           T = ptm_bound<NQ, ST>(C, k, lane); c.teval++;
           if (cacheT) tcache |= (unsigned)(T + 1) << (8 * q0);
@@ -783,11 +829,6 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
     if (lane == 0) slot = atomicAdd(&o.st->n_surv, 1ULL);
     slot = __shfl_sync(FULL, slot, 0);
     if (slot < o.cap) {
-#pragma unroll
-      for (int j = 0; j < EPL; j++) {
-        const int e = lane + 32 * j;
-        if (e < E) o.sR[slot * E + e] = C[e];
-      }
       if (lane == 0) {
         o.sh1[slot] = k1; o.sh2[slot] = k2; o.sidx[slot] = p * (unsigned long long)GS + g;
         NodeMeta nm;
@@ -816,7 +857,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, 
   Z4<ST> *P = sm.P[w], *C = sm.C[w];
   unsigned conjmask = 0;
   for (int i = 0; i < sp.nsym; i++) conjmask |= (unsigned)(sp.symconj[i] != 0) << i;
-  const ExpandOut<ST> o{a.st, a.cap, a.sh1, a.sh2, a.sidx, a.sR, a.smeta};
+  const ExpandOut<ST> o{a.st, a.cap, a.sh1, a.sh2, a.sidx, a.smeta, a.tq, a.tqcap};
   WarpTally c;
   for (;;) {
     unsigned long long p = 0;
@@ -854,8 +895,9 @@ template <typename ST> struct BatchArgs {
   DevStats *st;                    // batch-wide: work counter, survivor slots
   unsigned long long cap;
   uint64_t *sh1, *sh2, *sidx;
-  Z4<ST> *sR;
   NodeMeta *smeta;
+  TQEntry *tq;
+  unsigned long long tqcap;
 };
 
 template <int NQ, typename ST>
@@ -869,7 +911,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand_batch(const BatchA
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   Z4<ST> *P = sP[w], *C = sC[w];
   DevSpec &sp = sps[w];
-  const ExpandOut<ST> o{a.st, a.cap, a.sh1, a.sh2, a.sidx, a.sR, a.smeta};
+  const ExpandOut<ST> o{a.st, a.cap, a.sh1, a.sh2, a.sidx, a.smeta, a.tq, a.tqcap};
   WarpTally c;
   int job = -1, rem = 0;
   bool keep = false;
@@ -903,6 +945,115 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand_batch(const BatchA
     __syncwarp();
   }
   if (job >= 0) c.flush(a.jst + job, lane);
+}
+
+// a survivor's residual: its parent (index sidx / GS in frontier R) times its gate g = sidx % GS, into C; P is the
+// warp's staging buffer. The same warp_child as the level kernel, so the result is the residual it evaluated.
+template <int NQ, typename ST>
+__device__ __forceinline__ void warp_materialize(const Z4<ST> *R, const NodeMeta *meta, unsigned long long sidx, int GS,
+                                                 const DevSpec &sp, const DevSpec *sps, Z4<ST> *P, Z4<ST> *C, int lane) {
+  constexpr int E = (1 << NQ) * (1 << NQ), EPL = E >= 32 ? E / 32 : 1;
+  const unsigned long long p = sidx / (unsigned long long)GS;
+  const int g = (int)(sidx % (unsigned long long)GS);
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < EPL; j++) {
+    const int e = lane + 32 * j;
+    if (e < E) P[e] = R[p * E + e];
+  }
+  __syncwarp();
+  bool ovf;
+  (void)warp_child<NQ, ST>(P, C, g, meta[p].k, sp, sps, lane, ovf);
+  __syncwarp();
+}
+
+// ---------------- deferred T bounds ----------------
+// One warp per queued entry: recompute the child from its parent, evaluate the T bound once for the entry's
+// children, finish their alive test, and write the survivors' records, as the level kernel would have. With jobs
+// (fjob != nullptr) the parent's job gives the spec, level and counters.
+constexpr int TB_WARPS = 8;
+template <typename ST> struct TBoundArgs {
+  const Z4<ST> *R;
+  const NodeMeta *meta;
+  const TQEntry *tq;
+  unsigned long long tqcap;
+  int GS, rem, keep;                // rem, keep: without jobs
+  const uint32_t *fjob;
+  const DevSpec *specs;
+  const int *jt;
+  DevStats *jst;
+  DevStats *st;                     // queue counters, survivor slots (and the counters without jobs)
+  unsigned long long cap;
+  uint64_t *sh1, *sh2, *sidx;
+  NodeMeta *smeta;
+};
+template <int NQ, typename ST>
+__global__ void __launch_bounds__(TB_WARPS * 32) k_tbound(const __grid_constant__ DevSpec sp0, const TBoundArgs<ST> a) {
+  constexpr int N = 1 << NQ, E = N * N;
+  __shared__ Z4<ST> sP[TB_WARPS][E], sC[TB_WARPS][E];
+  __shared__ uint64_t W1[E], W2[E];
+  __shared__ DevSpec sps[TB_WARPS];
+  init_weights(W1, W2, E);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  Z4<ST> *P = sP[w], *C = sC[w];
+  DevSpec &sp = sps[w];
+  const unsigned long long n = a.st->n_tq < a.tqcap ? a.st->n_tq : a.tqcap;
+  WarpTally c;
+  int job = -2, rem = a.rem;
+  bool keep = a.keep != 0;
+  unsigned conjmask = 0;
+  for (;;) {
+    unsigned long long e = 0;
+    if (lane == 0) e = atomicAdd(&a.st->tq_work, 1ULL);
+    e = __shfl_sync(FULL, e, 0);
+    if (e >= n) break;
+    const TQEntry q = a.tq[e];
+    const int pj = a.fjob ? (int)a.fjob[q.p] : -1;
+    if (pj != job) {                                 // the spec of this entry's job (or the search's)
+      if (job >= 0) c.flush(a.jst + job, lane);
+      job = pj;
+      __syncwarp();
+      const int *src = (const int *)(a.fjob ? a.specs + job : &sp0);
+      for (int i = lane; i < (int)(sizeof(DevSpec) / 4); i += 32) ((int *)&sp)[i] = src[i];
+      __syncwarp();
+      if (a.fjob) { const int t = a.jt[job]; rem = sp.depth - t; keep = t < sp.depth; }
+      conjmask = 0;
+      for (int i = 0; i < sp.nsym; i++) conjmask |= (unsigned)(sp.symconj[i] != 0) << i;
+    }
+    const NodeMeta pm = a.meta[q.p];
+    int T = 0;
+    for (int s2 = 0; s2 < q.n; s2++) {
+      warp_materialize<NQ, ST>(a.R, a.meta, q.p * (unsigned long long)a.GS + q.g[s2], a.GS, sp, &sp, P, C, lane);
+      if (s2 == 0) { T = ptm_bound<NQ, ST>(C, q.k, lane); c.teval++; }
+      bool alive;
+      if (sp.lite) alive = q.k + (T + sp.tdiv - 1) / sp.tdiv <= rem;
+      else alive = combine(q.k > q.hs ? q.k : q.hs, T, q.c2, __popc(q.ntriv[s2])) <= rem;
+      if (!alive) { c.dead++; continue; }
+      c.alive++;
+      if (!keep) continue;
+      uint64_t k1, k2;
+      warp_class_key<NQ, ST>(C, q.k, sp.nsym, conjmask, sp.symperm, W1, W2, lane, k1, k2);
+      unsigned long long slot = 0;
+      if (lane == 0) slot = atomicAdd(&a.st->n_surv, 1ULL);
+      slot = __shfl_sync(FULL, slot, 0);
+      if (slot < a.cap) {
+        if (lane == 0) {
+          a.sh1[slot] = k1; a.sh2[slot] = k2; a.sidx[slot] = q.p * (unsigned long long)a.GS + q.g[s2];
+          NodeMeta nm;
+          nm.k = q.k; nm.T = (uint8_t)(T > 255 ? 255 : T); nm.c2 = q.c2; nm.g1 = q.g[s2]; nm.g2 = pm.g1;
+          nm.hsn = (uint8_t)((q.hs == 2 ? 1 : 0) | (q.ntriv[s2] << 1));
+          nm.needs = q.needs;
+          a.smeta[slot] = nm;
+        }
+      } else if (lane == 0) {
+        a.st->surv_overflow = 1;
+      }
+      __syncwarp();
+    }
+  }
+  if (a.fjob) { if (job >= 0) c.flush(a.jst + job, lane); }
+  else c.flush(a.st, lane);
 }
 
 // the root node's bounds (the target itself), inherited or bracketed by its children
@@ -994,19 +1145,31 @@ __device__ bool warp_same_class(const Z4<ST> *A, const Z4<ST> *B, const DevSpec 
   return false;
 }
 
-// one warp per run: order members by (h1, h2, index), then keep the first member of every exact class
+constexpr int RES_WARPS = 4;       // warps per resolve / materialize block
+template <int NQ, typename ST> struct ResolveSmem {
+  static constexpr int E = (1 << NQ) * (1 << NQ);
+  Z4<ST> A[RES_WARPS][E], B[RES_WARPS][E], P[RES_WARPS][E];
+};
+
+// one warp per run: order members by (h1, h2, index), then keep the first member of every exact class. With jobs
+// (fjob != nullptr) members of different jobs are never one class and each job's spec and symmetry group apply.
 template <int NQ, typename ST>
-__global__ void k_resolve(const DevSpec sp, const uint2 *work, const uint32_t *slots, const uint64_t *sh1,
-                          const uint64_t *sh2, const uint64_t *sidx, const Z4<ST> *sR, const NodeMeta *smeta,
-                          uint32_t *tmp, uint64_t *kidx, uint32_t *kslot, DevStats *st) {
-  constexpr int E = (1 << NQ) * (1 << NQ);
-  __shared__ uint8_t perm[SYMMAX][8];
-  for (int i = threadIdx.x; i < SYMMAX * 8; i += blockDim.x) perm[i / 8][i % 8] = sp.symperm[i / 8][i % 8];
+__global__ void __launch_bounds__(RES_WARPS * 32) k_resolve(const DevSpec sp, const DevSpec *specs, const uint32_t *fjob,
+                                                          int GS, const Z4<ST> *R, const NodeMeta *meta,
+                                                          const uint2 *work, const uint32_t *slots, const uint64_t *sh1,
+                                                          const uint64_t *sh2, const uint64_t *sidx,
+                                                          const NodeMeta *smeta, uint32_t *tmp, uint64_t *kidx,
+                                                          uint32_t *kslot, DevStats *st) {
+  __shared__ ResolveSmem<NQ, ST> sm;
+  __shared__ DevSpec s_sp;
+  if (!specs)
+    for (int i = threadIdx.x; i < (int)(sizeof(DevSpec) / 4); i += blockDim.x) ((int *)&s_sp)[i] = ((const int *)&sp)[i];
   __syncthreads();
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  Z4<ST> *A = sm.A[w], *B = sm.B[w], *P = sm.P[w];
   const unsigned long long nwork = st->n_work;
-  const unsigned long long nw = (unsigned long long)gridDim.x * (blockDim.x / 32);
-  for (unsigned long long wi = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); wi < nwork; wi += nw) {
+  const unsigned long long nw = (unsigned long long)gridDim.x * RES_WARPS;
+  for (unsigned long long wi = blockIdx.x * RES_WARPS + w; wi < nwork; wi += nw) {
     const uint2 wk = work[wi];
     const unsigned start = wk.x, len = wk.y;
     for (unsigned a0 = 0; a0 < len; a0 += 32) {          // rank of member a among the run
@@ -1030,13 +1193,18 @@ __global__ void k_resolve(const DevSpec sp, const uint2 *work, const uint32_t *s
         const uint32_t sp0 = tmp[start + i - 1] & 0x7fffffffu;
         if (sh1[sp0] != sh1[si] || sh2[sp0] != sh2[si]) gstart = i;
       }
-      bool dup = false;
+      const uint32_t ji = fjob ? fjob[sidx[si] / (unsigned long long)GS] : 0;
+      const DevSpec &jsp = specs ? specs[ji] : s_sp;
+      bool dup = false, haveA = false;
       for (unsigned i2 = gstart; i2 < i && !dup; i2++) {
         const uint32_t t2 = tmp[start + i2];
         if (!(t2 & 0x80000000u)) continue;
         const uint32_t s2 = t2 & 0x7fffffffu;
         if (smeta[s2].k != smeta[si].k) continue;
-        dup = warp_same_class<NQ, ST>(sR + (size_t)si * E, sR + (size_t)s2 * E, sp, perm, lane);
+        if (fjob && fjob[sidx[s2] / (unsigned long long)GS] != ji) continue;
+        if (!haveA) { warp_materialize<NQ, ST>(R, meta, sidx[si], GS, jsp, &jsp, P, A, lane); haveA = true; }
+        warp_materialize<NQ, ST>(R, meta, sidx[s2], GS, jsp, &jsp, P, B, lane);
+        dup = warp_same_class<NQ, ST>(A, B, jsp, jsp.symperm, lane);
       }
       if (!dup && lane == 0) {
         tmp[start + i] = si | 0x80000000u;
@@ -1056,19 +1224,38 @@ __global__ void k_keep_all(const uint64_t *sidx, size_t n, uint64_t *kidx, uint3
   }
 }
 
-// kept survivors (in index order) -> the next frontier: residual, bounds, tree links
-template <typename ST>
-__global__ void k_gather(const uint64_t *kidx, const uint32_t *kslot, size_t nk, int G, int E, const Z4<ST> *sR,
-                         const NodeMeta *smeta, Z4<ST> *R, NodeMeta *meta, uint32_t *par, uint8_t *gat) {
-  const size_t tot = nk * (size_t)E;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot; i += (size_t)gridDim.x * blockDim.x) {
-    const size_t j = i / E, e = i % E;
-    const uint32_t s = kslot[j];
-    R[i] = sR[(size_t)s * E + e];
-    if (e == 0) {
-      meta[j] = smeta[s];
-      par[j] = (uint32_t)(kidx[j] / (uint64_t)G);
-      gat[j] = (uint8_t)(kidx[j] % (uint64_t)G);
+// kept survivors (in index order) -> the next frontier: residual recomputed from the parent, bounds, tree links
+// (and job ids, with jobs). One warp per kept child; consecutive warps mostly share a parent.
+template <int NQ, typename ST>
+__global__ void __launch_bounds__(RES_WARPS * 32) k_materialize(const DevSpec sp, const DevSpec *specs,
+                                                              const uint32_t *fjob, int GS, const Z4<ST> *R,
+                                                              const NodeMeta *meta, const uint64_t *kidx,
+                                                              const uint32_t *kslot, size_t nk, const NodeMeta *smeta,
+                                                              Z4<ST> *R2, NodeMeta *meta2, uint32_t *par,
+                                                              uint8_t *gat, uint32_t *fjob2) {
+  constexpr int E = (1 << NQ) * (1 << NQ), EPL = E >= 32 ? E / 32 : 1;
+  __shared__ Z4<ST> sP[RES_WARPS][E], sC[RES_WARPS][E];
+  __shared__ DevSpec s_sp;
+  if (!specs)
+    for (int i = threadIdx.x; i < (int)(sizeof(DevSpec) / 4); i += blockDim.x) ((int *)&s_sp)[i] = ((const int *)&sp)[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (size_t j = blockIdx.x * (size_t)RES_WARPS + w; j < nk; j += (size_t)gridDim.x * RES_WARPS) {
+    const unsigned long long o = kidx[j];
+    const unsigned long long p = o / (unsigned long long)GS;
+    const uint32_t job = fjob ? fjob[p] : 0;
+    const DevSpec &jsp = specs ? specs[job] : s_sp;
+    warp_materialize<NQ, ST>(R, meta, o, GS, jsp, &jsp, sP[w], sC[w], lane);
+#pragma unroll
+    for (int q = 0; q < EPL; q++) {
+      const int e = lane + 32 * q;
+      if (e < E) R2[j * E + e] = sC[w][e];
+    }
+    if (lane == 0) {
+      meta2[j] = smeta[kslot[j]];
+      par[j] = (uint32_t)p;
+      gat[j] = (uint8_t)(o % (unsigned long long)GS);
+      if (fjob2) fjob2[j] = job;
     }
   }
 }
@@ -1100,7 +1287,10 @@ double now_s() { return std::chrono::duration<double>(std::chrono::steady_clock:
 
 struct CudaError : std::runtime_error { using std::runtime_error::runtime_error; };
 void ck(cudaError_t e, const char *what) {
-  if (e != cudaSuccess) throw CudaError(std::string("CUDA error after ") + what + ": " + cudaGetErrorString(e));
+  if (e != cudaSuccess) {
+    cudaGetLastError();            // a failed allocation must not be reported again by the next launch check
+    throw CudaError(std::string("CUDA error after ") + what + ": " + cudaGetErrorString(e));
+  }
 }
 
 struct DBuf {
@@ -1116,6 +1306,11 @@ struct DBuf {
     size_t c = bytes >= ((size_t)1 << 30) ? bytes : std::max(bytes, old + old / 2);
     c = (c + ((size_t)2 << 20) - 1) & ~(((size_t)2 << 20) - 1);
     if (bytes < ((size_t)2 << 20)) c = (bytes + 255) & ~(size_t)255;
+    if (c >= ((size_t)64 << 20) && std::getenv("CZ_TRACE_ALLOC")) {   // large device allocations, for diagnosis
+      size_t fr = 0, tot = 0;
+      cudaMemGetInfo(&fr, &tot);
+      std::fprintf(stderr, "cz alloc %.3f GB (free %.3f GB)\n", c / 1e9, fr / 1e9);
+    }
     ck(cudaMalloc(&p, c), "cudaMalloc");
     cap = c;
   }
@@ -1132,9 +1327,9 @@ uint64_t powmod_h(uint64_t a, uint64_t e) {
 }  // namespace
 
 // survivor records to provision for `children` children at an expected survivor rate: 1.5x the expectation
-// plus 4096, at least 1 Mi (never more than every child), at most 32 GiB of records
-inline unsigned long long survivor_room(unsigned long long children, double rate, size_t rec = 1064) {
-  const unsigned long long lim = ((unsigned long long)32 << 30) / rec;
+// plus 4096, at least 1 Mi (never more than every child), at most 8 GiB of records
+inline unsigned long long survivor_room(unsigned long long children, double rate, size_t rec) {
+  const unsigned long long lim = ((unsigned long long)8 << 30) / rec;
   double want = 1.5 * rate * (double)children + 4096.0;
   if (want < (double)(1 << 20)) want = (double)(1 << 20);
   unsigned long long cap = want >= (double)children ? children : (unsigned long long)want;
@@ -1146,8 +1341,9 @@ struct Engine::Impl {
   int nsm = 148;
   cudaStream_t s = nullptr;
   cudaEvent_t ev[4];
-  DBuf fR, fMeta;                          // frontier
-  DBuf sH1, sH2, sIdx, sR, sMeta;          // survivors of the current level
+  DBuf fR, fMeta, fR2, fMeta2;             // frontier, next frontier
+  DBuf sH1, sH2, sIdx, sMeta;              // survivors of the current level (32-byte records)
+  DBuf tq;                                 // deferred T evaluations of the current level
   DBuf k0, k1, v0, v1, hist, part;         // sort
   DBuf work, tmp, kidx, kslot;             // dedupe
   DBuf stats;
@@ -1174,8 +1370,8 @@ struct Engine::Impl {
   }
   ~Impl() {
     cudaSetDevice(dev);
-    for (DBuf *b : {&fR, &fMeta, &sH1, &sH2, &sIdx, &sR, &sMeta, &k0, &k1, &v0, &v1, &hist, &part, &work, &tmp, &kidx,
-                    &kslot, &stats})
+    for (DBuf *b : {&fR, &fMeta, &fR2, &fMeta2, &sH1, &sH2, &sIdx, &sMeta, &tq, &k0, &k1, &v0, &v1, &hist, &part,
+                    &work, &tmp, &kidx, &kslot, &stats})
       b->release();
     for (auto &sd : specs) sd.release();
     for (auto &b : par) b.release();
@@ -1208,13 +1404,18 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
     // survivors capacity: the previous level's survivor rate with room to spare (at least 1 Mi records, at most
     // every child); when more survive, the level is redone once with the exact count (the kernel counts every
     // survivor, stored or not)
-    unsigned long long cap = keep ? survivor_room((unsigned long long)m * G, surv_rate, E * sizeof(Z4<ST>) + 40) : 0;
+    unsigned long long cap = keep ? survivor_room((unsigned long long)m * G, surv_rate, 40) : 0;
     DevStats *dst = stats.as<DevStats>();
+    // deferred T evaluations: at most one entry per child of a gate whose T bound is not inherited
+    int ncl = 0;
+    for (int g = 0; g < G; g++) ncl += !(hs.gflags[g] & GF_CLIFFORD);
+    unsigned long long tqcap = (unsigned long long)m * (unsigned long long)std::max(1, ncl) + 1024;
     for (int attempt = 0; attempt < 2; attempt++) {
       if (keep) {
         sH1.ensure(cap * 8); sH2.ensure(cap * 8); sIdx.ensure(cap * 8);
-        sR.ensure(cap * E * sizeof(Z4<ST>)); sMeta.ensure(cap * sizeof(NodeMeta));
+        sMeta.ensure(cap * sizeof(NodeMeta));
       }
+      tq.ensure(tqcap * sizeof(TQEntry));
       ck(cudaMemsetAsync(dst, 0, sizeof(DevStats), s), "memset");
       const unsigned long long ffinit = ~0ULL;
       ck(cudaMemcpyAsync(&dst->first_found, &ffinit, 8, cudaMemcpyHostToDevice, s), "h2d");
@@ -1222,12 +1423,19 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
       a.m = m; a.t = t; a.rem = depth - t; a.keep = keep;
       a.R = fR.as<Z4<ST>>(); a.meta = fMeta.as<NodeMeta>(); a.st = dst; a.cap = cap;
       a.sh1 = sH1.as<uint64_t>(); a.sh2 = sH2.as<uint64_t>(); a.sidx = sIdx.as<uint64_t>();
-      a.sR = sR.as<Z4<ST>>(); a.smeta = sMeta.as<NodeMeta>();
+      a.smeta = sMeta.as<NodeMeta>();
+      a.tq = tq.as<TQEntry>(); a.tqcap = tqcap;
       const long long want = (m + EXP_WARPS - 1) / EXP_WARPS;
       const long long grid = std::max<long long>(1, std::min<long long>(want, (long long)nsm * 2 * 8));
       if (opt.profile) ck(cudaEventRecord(ev[0], s), "event");
       k_expand<NQ, ST><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(sp, a);
-      launches++;
+      TBoundArgs<ST> tb;
+      tb.R = fR.as<Z4<ST>>(); tb.meta = fMeta.as<NodeMeta>(); tb.tq = tq.as<TQEntry>(); tb.tqcap = tqcap;
+      tb.GS = G; tb.rem = depth - t; tb.keep = keep; tb.fjob = nullptr; tb.specs = nullptr; tb.jt = nullptr;
+      tb.jst = nullptr; tb.st = dst; tb.cap = cap; tb.sh1 = sH1.as<uint64_t>(); tb.sh2 = sH2.as<uint64_t>();
+      tb.sidx = sIdx.as<uint64_t>(); tb.smeta = sMeta.as<NodeMeta>();
+      k_tbound<NQ, ST><<<(unsigned)nsm * 4, TB_WARPS * 32, 0, s>>>(sp, tb);
+      launches += 2;
       expand_launches++;
       ck(cudaGetLastError(), "expand kernel");
       if (opt.profile) ck(cudaEventRecord(ev[1], s), "event");
@@ -1237,9 +1445,11 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
       ck(cudaStreamSynchronize(s), "expand");
       if (opt.profile) { float ms = 0; cudaEventElapsedTime(&ms, ev[0], ev[1]); res.expand_ms += ms; }
       if (hstats->ovf) return -2;                       // promote to int64 limbs and redo this level
-      if (!hstats->surv_overflow) break;
-      cap = hstats->n_surv;                             // exact survivor count: grow and redo once
+      if (!hstats->surv_overflow && hstats->n_tq <= tqcap) break;
+      cap = std::max<unsigned long long>(cap, hstats->n_surv);   // exact counts: grow and redo once
+      tqcap = std::max<unsigned long long>(tqcap, hstats->n_tq);
     }
+    if (hstats->n_tq > tqcap) { res.error = "T queue overflow"; return RC_CUDA; }
     if (hstats->surv_overflow) { res.error = "survivor buffer overflow"; return RC_CUDA; }
     const DevStats h = *hstats;
     if (m * G > 0) surv_rate = (double)h.alive / ((double)m * G);
@@ -1288,10 +1498,10 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
         const uint32_t *sv = f ? v1.as<uint32_t>() : v0.as<uint32_t>();
         k_runs<<<gb, 256, 0, s>>>(sk, sv, ns, sIdx.as<uint64_t>(), kidx.as<uint64_t>(), kslot.as<uint32_t>(),
                                   work.as<uint2>(), dst);
-        k_resolve<NQ, ST><<<(unsigned)nsm * 4, 256, 0, s>>>(sp, work.as<uint2>(), sv, sH1.as<uint64_t>(),
-                                                            sH2.as<uint64_t>(), sIdx.as<uint64_t>(), sR.as<Z4<ST>>(),
-                                                            sMeta.as<NodeMeta>(), tmp.as<uint32_t>(),
-                                                            kidx.as<uint64_t>(), kslot.as<uint32_t>(), dst);
+        k_resolve<NQ, ST><<<(unsigned)nsm * 8, RES_WARPS * 32, 0, s>>>(
+            sp, nullptr, nullptr, G, fR.as<Z4<ST>>(), fMeta.as<NodeMeta>(), work.as<uint2>(), sv, sH1.as<uint64_t>(),
+            sH2.as<uint64_t>(), sIdx.as<uint64_t>(), sMeta.as<NodeMeta>(), tmp.as<uint32_t>(), kidx.as<uint64_t>(),
+            kslot.as<uint32_t>(), dst);
         launches += 2;
         ck(cudaGetLastError(), "dedupe");
         ck(cudaMemcpyAsync(hstats, dst, sizeof(DevStats), cudaMemcpyDeviceToHost, s), "d2h");
@@ -1315,15 +1525,19 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
       if ((int)par.size() <= t) { par.resize(t + 1); gat.resize(t + 1); }
       par[t].ensure((size_t)distinct * 4);
       gat[t].ensure((size_t)distinct);
-      fR.ensure((size_t)distinct * E * sizeof(Z4<ST>));
-      fMeta.ensure((size_t)distinct * sizeof(NodeMeta));
-      const size_t tot = (size_t)distinct * E;
-      const unsigned gg = (unsigned)std::min<size_t>((tot + 255) / 256, (size_t)nsm * 32);
-      k_gather<ST><<<gg, 256, 0, s>>>(ki, vi, (size_t)distinct, G, E, sR.as<Z4<ST>>(), sMeta.as<NodeMeta>(),
-                                      fR.as<Z4<ST>>(), fMeta.as<NodeMeta>(), par[t].as<uint32_t>(),
-                                      gat[t].as<uint8_t>());
+      fR2.ensure((size_t)distinct * E * sizeof(Z4<ST>));
+      fMeta2.ensure((size_t)distinct * sizeof(NodeMeta));
+      const unsigned gg = (unsigned)std::max<size_t>(1, std::min<size_t>(((size_t)distinct + RES_WARPS - 1) / RES_WARPS,
+                                                                         (size_t)nsm * 16));
+      k_materialize<NQ, ST><<<gg, RES_WARPS * 32, 0, s>>>(sp, nullptr, nullptr, G, fR.as<Z4<ST>>(),
+                                                          fMeta.as<NodeMeta>(), ki, vi, (size_t)distinct,
+                                                          sMeta.as<NodeMeta>(), fR2.as<Z4<ST>>(),
+                                                          fMeta2.as<NodeMeta>(), par[t].as<uint32_t>(),
+                                                          gat[t].as<uint8_t>(), nullptr);
       launches++;
       ck(cudaGetLastError(), "gather");
+      std::swap(fR, fR2);
+      std::swap(fMeta, fMeta2);
       if (opt.profile) ck(cudaEventRecord(ev[3], s), "event");
       ck(cudaStreamSynchronize(s), "gather");
       if (opt.profile) { float ms = 0; cudaEventElapsedTime(&ms, ev[2], ev[3]); res.dedupe_ms += ms; }
@@ -1755,82 +1969,39 @@ __global__ void k_bsort_init(const uint64_t *h1, const uint64_t *sidx, size_t n,
   }
 }
 
-// k_resolve for a batch: members of different jobs are never the same class; each job's own symmetry group
-template <int NQ, typename ST>
-__global__ void k_resolve_batch(const DevSpec *specs, const uint32_t *fjob, const uint2 *work, const uint32_t *slots,
-                                const uint64_t *sh1, const uint64_t *sh2, const uint64_t *sidx, const Z4<ST> *sR,
-                                const NodeMeta *smeta, uint32_t *tmp, uint64_t *kidx, uint32_t *kslot, DevStats *st) {
-  constexpr int E = (1 << NQ) * (1 << NQ);
-  const int lane = threadIdx.x & 31;
-  const unsigned long long nwork = st->n_work;
-  const unsigned long long nw = (unsigned long long)gridDim.x * (blockDim.x / 32);
-  for (unsigned long long wi = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); wi < nwork; wi += nw) {
-    const uint2 wk = work[wi];
-    const unsigned start = wk.x, len = wk.y;
-    for (unsigned a0 = 0; a0 < len; a0 += 32) {
-      const unsigned ai = a0 + lane;
-      uint64_t ah1 = 0, ah2 = 0, aix = 0;
-      uint32_t as = 0;
-      if (ai < len) { as = slots[start + ai]; ah1 = sh1[as]; ah2 = sh2[as]; aix = sidx[as]; }
-      unsigned rank = 0;
-      for (unsigned b = 0; b < len; b++) {
-        const uint32_t bs = slots[start + b];
-        const uint64_t bh1 = sh1[bs], bh2 = sh2[bs], bix = sidx[bs];
-        rank += (bh1 < ah1) || (bh1 == ah1 && (bh2 < ah2 || (bh2 == ah2 && bix < aix)));
-      }
-      if (ai < len) tmp[start + rank] = as;
-    }
-    __syncwarp();
-    unsigned gstart = 0;
-    for (unsigned i = 0; i < len; i++) {
-      const uint32_t si = tmp[start + i] & 0x7fffffffu;
-      if (i > 0) {
-        const uint32_t sp0 = tmp[start + i - 1] & 0x7fffffffu;
-        if (sh1[sp0] != sh1[si] || sh2[sp0] != sh2[si]) gstart = i;
-      }
-      const uint32_t ji = fjob[sidx[si] / BATCH_GS];
-      bool dup = false;
-      for (unsigned i2 = gstart; i2 < i && !dup; i2++) {
-        const uint32_t t2 = tmp[start + i2];
-        if (!(t2 & 0x80000000u)) continue;
-        const uint32_t s2 = t2 & 0x7fffffffu;
-        if (smeta[s2].k != smeta[si].k || fjob[sidx[s2] / BATCH_GS] != ji) continue;
-        dup = warp_same_class<NQ, ST>(sR + (size_t)si * E, sR + (size_t)s2 * E, specs[ji], specs[ji].symperm, lane);
-      }
-      if (!dup && lane == 0) {
-        tmp[start + i] = si | 0x80000000u;
-        const unsigned long long pos = atomicAdd(&st->n_kept, 1ULL);
-        kidx[pos] = sidx[si];
-        kslot[pos] = si;
-      }
-      __syncwarp();
-    }
-  }
-}
-
 __global__ void k_bcount(const uint64_t *kidx, size_t nk, const uint32_t *fjob, unsigned long long *jdist) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nk; i += (size_t)gridDim.x * blockDim.x)
     atomicAdd(&jdist[fjob[kidx[i] / BATCH_GS]], 1ULL);
 }
-__global__ void k_fjob_next(const uint64_t *kidx, size_t nk, const uint32_t *fjob, uint32_t *fjob2) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nk; i += (size_t)gridDim.x * blockDim.x)
-    fjob2[i] = fjob[kidx[i] / BATCH_GS];
-}
-// circuits of jobs that found the goal: child index o at step s and job level t, walked back through the tree
-// arrays of steps s - 1 .. s - t + 1
-__global__ void k_walk(const unsigned long long *fo, const int *ft, const int *fs, int nf, const uint32_t *const *tpar,
-                       const uint8_t *const *tgat, int *out) {
+// circuits of jobs that found the goal: child o at step s, at job level t; walked back through the tree of steps
+// s - 1 .. s0 (the job's first step). A node carried over a step its job waited has gate 0xff there.
+__global__ void k_walk(const unsigned long long *fo, const int *ft, const int *fs, const int *fs0, int nf,
+                       const uint32_t *const *tpar, const uint8_t *const *tgat, int *out, int *bad) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nf) return;
   const unsigned long long o = fo[i];
-  const int t = ft[i], s = fs[i];
+  const int t = ft[i], s = fs[i], s0 = fs0[i];
   int *c = out + (size_t)i * MAXDEPTH_WALK;
-  c[t - 1] = (int)(o % BATCH_GS);
+  int pos = t - 1;
+  c[pos] = (int)(o % BATCH_GS);
   unsigned long long p = o / BATCH_GS;
-  for (int l = t - 1; l >= 1; l--) {
-    const int step = s - (t - l);
-    c[l - 1] = tgat[step][p];
-    p = tpar[step][p];
+  for (int st = s - 1; st >= s0 && pos > 0; st--) {
+    const uint8_t g = tgat[st][p];
+    p = tpar[st][p];
+    if (g != 0xff) c[--pos] = g;
+  }
+  if (pos != 0) atomicOr(bad, 1);
+}
+
+// nodes of jobs that wait this step: carried to the next frontier unchanged (tree: same node, no gate)
+template <typename ST>
+__global__ void k_carry(long long p0, long long n, int E, const Z4<ST> *R, const NodeMeta *meta, const uint32_t *fjob,
+                        Z4<ST> *R2, NodeMeta *meta2, uint32_t *fjob2, uint32_t *par, uint8_t *gat) {
+  const size_t tot = (size_t)n * E;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t j = i / E;
+    R2[i] = R[(size_t)p0 * E + i];
+    if (i % E == 0) { meta2[j] = meta[p0 + j]; fjob2[j] = fjob[p0 + j]; par[j] = (uint32_t)(p0 + j); gat[j] = 0xff; }
   }
 }
 
@@ -1857,6 +2028,8 @@ struct BatchSession::Impl {
   virtual long long steps() const = 0;
   virtual size_t device_bytes() const = 0;
   virtual size_t projected_bytes() const = 0;
+  virtual void set_budget(size_t bytes) = 0;
+  virtual long long waits() const = 0;
 };
 
 namespace {
@@ -1873,6 +2046,7 @@ struct BatchImpl : BatchSession::Impl {
     int t = 1;                       // the level this job runs at its next step
     long long seg = 0;               // its nodes in the frontier
     double rate = 1.0;               // survivors per child at its previous level
+    double drate = 1.0;              // distinct per survivor at its previous level
     bool queued = true, running = false;
     BatchJob out;
   };
@@ -1884,7 +2058,8 @@ struct BatchImpl : BatchSession::Impl {
   std::map<uint64_t, SpecTables *> tables;
   DBuf dspecs, jt, jst, jact, jdist;
   DBuf fR, fMeta, fJob, fR2, fMeta2, fJob2;
-  DBuf sH1, sH2, sIdx, sR, sMeta, stats;
+  DBuf sH1, sH2, sIdx, sMeta, stats;       // survivors: 32-byte records
+  DBuf tq;                                 // deferred T evaluations
   DBuf k0, k1, v0, v1, hist, part, work, tmp, kidx, kslot, cnt;
   DBuf rJob, rTk, tptr, wbuf;
   std::vector<DBuf> tpar, tgat;      // tree of every step
@@ -1897,11 +2072,17 @@ struct BatchImpl : BatchSession::Impl {
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e.device());
     stats.ensure(sizeof(DevStats));
     cnt.ensure(64);
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) budget = (size_t)(0.8 * (double)fr);
   }
+  size_t budget = (size_t)64 << 30;  // device bytes a step may plan for (frontiers + survivors)
+  void set_budget(size_t b) override { budget = b; }
+  long long nwait = 0;               // job-steps spent waiting for memory
+  long long waits() const override { return nwait; }
   ~BatchImpl() override {
     cudaSetDevice(eng.device());
     for (DBuf *b : {&dspecs, &jt, &jst, &jact, &jdist, &fR, &fMeta, &fJob, &fR2, &fMeta2, &fJob2, &sH1, &sH2, &sIdx,
-                    &sR, &sMeta, &stats, &k0, &k1, &v0, &v1, &hist, &part, &work, &tmp, &kidx, &kslot, &cnt, &rJob,
+                    &sMeta, &tq, &stats, &k0, &k1, &v0, &v1, &hist, &part, &work, &tmp, &kidx, &kslot, &cnt, &rJob,
                     &rTk, &tptr, &wbuf})
       b->release();
     for (auto &b : tpar) b.release();
@@ -1922,18 +2103,21 @@ struct BatchImpl : BatchSession::Impl {
   size_t device_bytes() const override {
     size_t b = 0;
     for (const DBuf *x : {&dspecs, &jt, &jst, &jact, &jdist, &fR, &fMeta, &fJob, &fR2, &fMeta2, &fJob2, &sH1, &sH2,
-                          &sIdx, &sR, &sMeta, &k0, &k1, &v0, &v1, &hist, &part, &work, &tmp, &kidx, &kslot})
+                          &sIdx, &sMeta, &k0, &k1, &v0, &v1, &hist, &part, &work, &tmp, &kidx, &kslot})
       b += x->cap;
     for (auto &x : tpar) b += x.cap;
     for (auto &x : tgat) b += x.cap;
     return b;
   }
 
-  size_t projected_bytes() const override {
-    const size_t node = E * sizeof(Z4<ST>) + sizeof(NodeMeta) + 4, surv = E * sizeof(Z4<ST>) + 40 + 36;
+  size_t projected_bytes() const override {   // this frontier + every running job's expected survivors and nodes
+    const size_t node = E * sizeof(Z4<ST>) + sizeof(NodeMeta) + 4 + 5, surv = 40 + 36;
     size_t b = (size_t)m * node;
     for (const Job &j : J)
-      if (j.running && j.t < j.depth) b += (size_t)j.seg * (size_t)j.hs.G * surv;
+      if (j.running && j.t < j.depth) {
+        const double all = (double)j.seg * j.hs.G;
+        b += (size_t)(std::min(all, 1.5 * j.rate * all + 4096.0) * (double)(surv + node));
+      }
     return b;
   }
 
@@ -2066,11 +2250,11 @@ struct BatchImpl : BatchSession::Impl {
     m += nr;
   }
 
-  // grow b to `bytes`, keeping its first `keep` bytes
+  // grow b to `bytes`, keeping its first `keep` bytes (half again as much room below 1 GB, a tenth above)
   void grow_keep(DBuf &b, size_t bytes, size_t keep) {
     if (bytes <= b.cap) return;
     DBuf nb;
-    nb.ensure(bytes + bytes / 2);
+    nb.ensure(bytes + (bytes < ((size_t)1 << 30) ? bytes / 2 : bytes / 10));
     if (keep) ck(cudaMemcpyAsync(nb.p, b.p, keep, cudaMemcpyDeviceToDevice, s), "d2d");
     ck(cudaStreamSynchronize(s), "grow");
     b.release();
@@ -2093,47 +2277,103 @@ struct BatchImpl : BatchSession::Impl {
     ck(cudaMemcpyAsync(jt.p, ht.data(), nj * 4, cudaMemcpyHostToDevice, s), "h2d");
     k_jst_init<<<(nj + 255) / 256, 256, 0, s>>>(jst.as<DevStats>(), nj);
     nlaunch++;
-    const size_t rec = E * sizeof(Z4<ST>) + 40;
-    const unsigned long long cap_limit = ((unsigned long long)32 << 30) / rec;
-    // chunks of whole jobs (frontier order = id order) whose expected survivors fit the budget; each chunk's room
-    // is its jobs' expected survivors (previous survivor rate x 1.5) and never more than all their children
-    struct Chunk { long long p0, p1; unsigned long long cap, all; std::vector<int> jobs; };
-    std::vector<Chunk> chunks;
+    const size_t rec = 40 + 36;                                          // survivor record + its sort entries
+    const size_t node = E * sizeof(Z4<ST>) + sizeof(NodeMeta) + 4 + 5;     // frontier node + its tree entry
+    const unsigned long long cap_limit = ((unsigned long long)8 << 30) / rec;
+    // the plan, in frontier (= id) order: chunks of advancing jobs whose expected survivors fit the survivor
+    // budget, and runs of waiting jobs carried over unchanged. A job advances while the step's planned memory (this
+    // frontier, the next one, survivor room) stays under the session budget; the first job always advances.
+    struct Op { bool carry; long long p0, p1; unsigned long long cap, all; std::vector<int> jobs; };
+    std::vector<Op> ops;
+    size_t step_budget = budget;
+    {                                                     // never plan past what the device has left
+      size_t fr = 0, tot = 0;
+      if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+        const size_t mine = fR2.cap + fMeta2.cap + fJob2.cap + sH1.cap + sH2.cap + sIdx.cap + sMeta.cap + k0.cap +
+                            k1.cap + v0.cap + v1.cap + kidx.cap + kslot.cap + work.cap + tmp.cap;
+        step_budget = std::min(step_budget, (size_t)(0.9 * (double)(fr + mine)));
+      }
+    }
     {
-      Chunk c{0, 0, 0, 0, {}};
+      size_t planned = (size_t)m * node;
+      bool any_adv = false;
+      Op c{false, 0, 0, 0, 0, {}};
       long long off = 0;
       for (int i = 0; i < nj; i++) {
         Job &j = J[i];
         if (!j.running || j.seg == 0) continue;
         const unsigned long long all = j.t < j.depth ? (unsigned long long)j.seg * j.hs.G : 0;
         const unsigned long long want = all ? std::min<unsigned long long>(all, (unsigned long long)(1.5 * j.rate * (double)all) + 4096) : 0;
-        if (!c.jobs.empty() && c.cap + want > cap_limit) { chunks.push_back(c); c = Chunk{off, off, 0, 0, {}}; }
+        const size_t cost = (size_t)want * (node + rec);
+        const bool adv = !any_adv || planned + cost <= step_budget;
+        planned += adv ? cost : (size_t)j.seg * node;
+        any_adv |= adv;
+        if (!c.jobs.empty() && (c.carry == adv || (adv && c.cap + want > cap_limit))) { ops.push_back(c); c = Op{!adv, off, off, 0, 0, {}}; }
+        c.carry = !adv;
         c.jobs.push_back(i);
-        c.cap += want;
-        c.all += all;
+        if (adv) { c.cap += want; c.all += all; }
         off += j.seg;
         c.p1 = off;
       }
-      if (!c.jobs.empty()) chunks.push_back(c);
+      if (!c.jobs.empty()) ops.push_back(c);
       if (off != m) throw std::logic_error("batch frontier out of step with its jobs");
-      for (Chunk &ch : chunks) ch.cap = std::min(ch.all, std::max<unsigned long long>(ch.cap, 1 << 20));
+      for (Op &o : ops) if (!o.carry) o.cap = std::min(o.all, std::max<unsigned long long>(o.cap, 1 << 20));
     }
     if ((long long)tpar.size() <= nstep) { tpar.resize(nstep + 1); tgat.resize(nstep + 1); }
+    {
+      size_t est = 0;                                     // next frontier: carried nodes + expected distinct children
+      for (const Op &o : ops) {
+        if (o.carry) { est += (size_t)(o.p1 - o.p0); continue; }
+        for (int i : o.jobs) {
+          const Job &j = J[i];
+          const double all = j.t < j.depth ? (double)j.seg * j.hs.G : 0.0;
+          est += (size_t)std::min(all, (1.25 * j.rate * all + 1024.0) * j.drate);
+        }
+      }
+      fR2.ensure(est * E * sizeof(Z4<ST>) + 16); fMeta2.ensure(est * sizeof(NodeMeta) + 16); fJob2.ensure(est * 4 + 4);
+      tpar[nstep].ensure(est * 4 + 4); tgat[nstep].ensure(est + 4);
+    }
     std::vector<DevStats> hj(nj);
     std::vector<uint8_t> act(nj, 0);
     std::vector<unsigned long long> dist(nj, 0);
     std::vector<int> overflow_ids;
     size_t total_distinct = 0;
     DevStats *dst = stats.as<DevStats>();
-    for (const Chunk &ch : chunks) {
+    for (const Op &ch : ops) {
+      if (ch.carry) {                                     // waiting jobs: nodes carried over unchanged
+        const long long n = ch.p1 - ch.p0;
+        const size_t o0 = total_distinct, o1 = total_distinct + (size_t)n;
+        grow_keep(tpar[nstep], o1 * 4 + 4, o0 * 4);
+        grow_keep(tgat[nstep], o1 + 4, o0);
+        grow_keep(fR2, o1 * E * sizeof(Z4<ST>) + 16, o0 * E * sizeof(Z4<ST>));
+        grow_keep(fMeta2, o1 * sizeof(NodeMeta) + 16, o0 * sizeof(NodeMeta));
+        grow_keep(fJob2, o1 * 4 + 4, o0 * 4);
+        const size_t tot = (size_t)n * E;
+        const unsigned gg = (unsigned)std::max<size_t>(1, std::min<size_t>((tot + 255) / 256, (size_t)nsm * 32));
+        k_carry<ST><<<gg, 256, 0, s>>>(ch.p0, n, E, fR.as<Z4<ST>>(), fMeta.as<NodeMeta>(), fJob.as<uint32_t>(),
+                                       fR2.as<Z4<ST>>() + o0 * E, fMeta2.as<NodeMeta>() + o0, fJob2.as<uint32_t>() + o0,
+                                       tpar[nstep].as<uint32_t>() + o0, tgat[nstep].as<uint8_t>() + o0);
+        nlaunch++;
+        nwait += (long long)ch.jobs.size();
+        ck(cudaGetLastError(), "carry");
+        total_distinct = o1;
+        continue;
+      }
       const long long cm = ch.p1 - ch.p0;
       const int jlo = ch.jobs.front(), jn = ch.jobs.back() - jlo + 1;
       unsigned long long cap = std::min<unsigned long long>(ch.cap, cap_limit);
+      unsigned long long tqcap = 1024;                  // deferred T evaluations: one per non-Clifford child at most
+      for (int i : ch.jobs) {
+        int ncl = 0;
+        for (int g = 0; g < J[i].hs.G; g++) ncl += !(J[i].hs.gflags[g] & GF_CLIFFORD);
+        tqcap += (unsigned long long)J[i].seg * (unsigned long long)std::max(1, ncl);
+      }
       DevStats h{};
       for (int attempt = 0; attempt < 2; attempt++) {
+        tq.ensure(tqcap * sizeof(TQEntry));
         if (cap) {
           sH1.ensure(cap * 8); sH2.ensure(cap * 8); sIdx.ensure(cap * 8);
-          sR.ensure(cap * E * sizeof(Z4<ST>)); sMeta.ensure(cap * sizeof(NodeMeta));
+          sMeta.ensure(cap * sizeof(NodeMeta));
         }
         ck(cudaMemsetAsync(dst, 0, sizeof(DevStats), s), "memset");
         if (attempt) {                                   // the chunk's jobs start over (ids jlo..jhi)
@@ -2145,18 +2385,26 @@ struct BatchImpl : BatchSession::Impl {
         a.R = fR.as<Z4<ST>>(); a.meta = fMeta.as<NodeMeta>(); a.fjob = fJob.as<uint32_t>();
         a.specs = dspecs.as<DevSpec>(); a.jt = jt.as<int>(); a.jst = jst.as<DevStats>(); a.st = dst; a.cap = cap;
         a.sh1 = sH1.as<uint64_t>(); a.sh2 = sH2.as<uint64_t>(); a.sidx = sIdx.as<uint64_t>();
-        a.sR = sR.as<Z4<ST>>(); a.smeta = sMeta.as<NodeMeta>();
+        a.smeta = sMeta.as<NodeMeta>();
+        a.tq = tq.as<TQEntry>(); a.tqcap = tqcap;
         const long long want = (cm + EXP_WARPS - 1) / EXP_WARPS;
         const long long grid = std::max<long long>(1, std::min<long long>(want, (long long)nsm * 2 * 8));
         k_expand_batch<NQ, ST><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(a);
-        nlaunch++;
+        TBoundArgs<ST> tb;
+        tb.R = fR.as<Z4<ST>>(); tb.meta = fMeta.as<NodeMeta>(); tb.tq = tq.as<TQEntry>(); tb.tqcap = tqcap;
+        tb.GS = BATCH_GS; tb.rem = 0; tb.keep = 0; tb.fjob = fJob.as<uint32_t>(); tb.specs = dspecs.as<DevSpec>();
+        tb.jt = jt.as<int>(); tb.jst = jst.as<DevStats>(); tb.st = dst; tb.cap = cap; tb.sh1 = sH1.as<uint64_t>();
+        tb.sh2 = sH2.as<uint64_t>(); tb.sidx = sIdx.as<uint64_t>(); tb.smeta = sMeta.as<NodeMeta>();
+        k_tbound<NQ, ST><<<(unsigned)nsm * 4, TB_WARPS * 32, 0, s>>>(DevSpec{}, tb);
+        nlaunch += 2;
         ck(cudaGetLastError(), "batched expand");
         ck(cudaMemcpyAsync(&h, dst, sizeof(DevStats), cudaMemcpyDeviceToHost, s), "d2h");
         ck(cudaStreamSynchronize(s), "batched expand");
-        if (!h.surv_overflow) break;
-        cap = h.n_surv;                                   // every survivor was counted: redo with the exact room
+        if (!h.surv_overflow && h.n_tq <= tqcap) break;
+        cap = std::max<unsigned long long>(cap, h.n_surv);  // every survivor and entry was counted: exact room
+        tqcap = std::max<unsigned long long>(tqcap, h.n_tq);
       }
-      if (h.surv_overflow) throw std::runtime_error("survivor buffer overflow");
+      if (h.surv_overflow || h.n_tq > tqcap) throw std::runtime_error("survivor or T queue overflow");
       ck(cudaMemcpyAsync(hj.data() + jlo, jst.as<DevStats>() + jlo, jn * sizeof(DevStats), cudaMemcpyDeviceToHost, s),
          "d2h");
       ck(cudaStreamSynchronize(s), "job stats");
@@ -2197,12 +2445,10 @@ struct BatchImpl : BatchSession::Impl {
       const unsigned gs = (unsigned)std::max<size_t>(1, std::min<size_t>((nsort + 255) / 256, (size_t)nsm * 16));
       k_runs<<<gs, 256, 0, s>>>(sk, sv, nsort, sIdx.as<uint64_t>(), kidx.as<uint64_t>(), kslot.as<uint32_t>(),
                                 work.as<uint2>(), dst);
-      k_resolve_batch<NQ, ST><<<(unsigned)nsm * 4, 256, 0, s>>>(dspecs.as<DevSpec>(), fJob.as<uint32_t>(),
-                                                                work.as<uint2>(), sv, sH1.as<uint64_t>(),
-                                                                sH2.as<uint64_t>(), sIdx.as<uint64_t>(),
-                                                                sR.as<Z4<ST>>(), sMeta.as<NodeMeta>(),
-                                                                tmp.as<uint32_t>(), kidx.as<uint64_t>(),
-                                                                kslot.as<uint32_t>(), dst);
+      k_resolve<NQ, ST><<<(unsigned)nsm * 8, RES_WARPS * 32, 0, s>>>(
+          DevSpec{}, dspecs.as<DevSpec>(), fJob.as<uint32_t>(), BATCH_GS, fR.as<Z4<ST>>(), fMeta.as<NodeMeta>(),
+          work.as<uint2>(), sv, sH1.as<uint64_t>(), sH2.as<uint64_t>(), sIdx.as<uint64_t>(), sMeta.as<NodeMeta>(),
+          tmp.as<uint32_t>(), kidx.as<uint64_t>(), kslot.as<uint32_t>(), dst);
       nlaunch += 2;
       ck(cudaGetLastError(), "batched dedupe");
       ck(cudaMemcpyAsync(&h, dst, sizeof(DevStats), cudaMemcpyDeviceToHost, s), "d2h");
@@ -2230,14 +2476,13 @@ struct BatchImpl : BatchSession::Impl {
       grow_keep(fR2, o1 * E * sizeof(Z4<ST>) + 16, o0 * E * sizeof(Z4<ST>));
       grow_keep(fMeta2, o1 * sizeof(NodeMeta) + 16, o0 * sizeof(NodeMeta));
       grow_keep(fJob2, o1 * 4 + 4, o0 * 4);
-      const size_t tot = distinct * E;
-      const unsigned gg = (unsigned)std::max<size_t>(1, std::min<size_t>((tot + 255) / 256, (size_t)nsm * 32));
-      k_gather<ST><<<gg, 256, 0, s>>>(ki, vi, distinct, BATCH_GS, E, sR.as<Z4<ST>>(), sMeta.as<NodeMeta>(),
-                                      fR2.as<Z4<ST>>() + o0 * E, fMeta2.as<NodeMeta>() + o0,
-                                      tpar[nstep].as<uint32_t>() + o0, tgat[nstep].as<uint8_t>() + o0);
-      k_fjob_next<<<(unsigned)std::max<size_t>(1, std::min<size_t>((distinct + 255) / 256, (size_t)nsm * 16)), 256, 0, s>>>(
-          ki, distinct, fJob.as<uint32_t>(), fJob2.as<uint32_t>() + o0);
-      nlaunch += 2;
+      const unsigned gg = (unsigned)std::max<size_t>(1, std::min<size_t>((distinct + RES_WARPS - 1) / RES_WARPS,
+                                                                         (size_t)nsm * 16));
+      k_materialize<NQ, ST><<<gg, RES_WARPS * 32, 0, s>>>(
+          DevSpec{}, dspecs.as<DevSpec>(), fJob.as<uint32_t>(), BATCH_GS, fR.as<Z4<ST>>(), fMeta.as<NodeMeta>(), ki, vi,
+          distinct, sMeta.as<NodeMeta>(), fR2.as<Z4<ST>>() + o0 * E, fMeta2.as<NodeMeta>() + o0,
+          tpar[nstep].as<uint32_t>() + o0, tgat[nstep].as<uint8_t>() + o0, fJob2.as<uint32_t>() + o0);
+      nlaunch++;
       ck(cudaGetLastError(), "batched gather");
       ck(cudaStreamSynchronize(s), "batched gather");
       for (int i : ch.jobs) dist[i] = cd[i];
@@ -2257,6 +2502,7 @@ struct BatchImpl : BatchSession::Impl {
       L.proved_unsat = L.distinct == 0;
       L.seconds = secs;
       if (j.seg * j.hs.G > 0) j.rate = (double)d.alive / ((double)j.seg * j.hs.G);
+      if (d.alive > 0 && j.t < j.depth) j.drate = std::min(1.0, (double)dist[i] / (double)d.alive);
       j.out.levels.push_back(L);
       j.out.res.prefixes += L.prefixes;
       account(j, d);
@@ -2282,13 +2528,16 @@ struct BatchImpl : BatchSession::Impl {
   void walk(const std::vector<int> &found_ids, const std::vector<DevStats> &hj) {
     const int nf = (int)found_ids.size();
     std::vector<unsigned long long> fo(nf);
-    std::vector<int> ft(nf), fs(nf);
-    for (int i = 0; i < nf; i++) { fo[i] = hj[found_ids[i]].first_found; ft[i] = J[found_ids[i]].t; fs[i] = (int)nstep; }
+    std::vector<int> ft(nf), fs(nf), fs0(nf);
+    for (int i = 0; i < nf; i++) {
+      fo[i] = hj[found_ids[i]].first_found; ft[i] = J[found_ids[i]].t; fs[i] = (int)nstep;
+      fs0[i] = J[found_ids[i]].out.joined_step;
+    }
     std::vector<const uint32_t *> pp(nstep + 1, nullptr);
     std::vector<const uint8_t *> gp(nstep + 1, nullptr);
     for (long long st2 = 0; st2 < nstep && st2 < (long long)tpar.size(); st2++) { pp[st2] = tpar[st2].as<uint32_t>(); gp[st2] = tgat[st2].as<uint8_t>(); }
     const size_t pb = pp.size() * sizeof(void *);
-    tptr.ensure(2 * pb + (size_t)nf * (8 + 4 + 4) + (size_t)nf * MAXDEPTH_WALK * 4 + 64);
+    tptr.ensure(2 * pb + (size_t)nf * (8 + 4 + 4 + 4) + (size_t)nf * MAXDEPTH_WALK * 4 + 64);
     char *base = (char *)tptr.p;
     ck(cudaMemcpyAsync(base, pp.data(), pb, cudaMemcpyHostToDevice, s), "h2d");
     ck(cudaMemcpyAsync(base + pb, gp.data(), pb, cudaMemcpyHostToDevice, s), "h2d");
@@ -2296,16 +2545,22 @@ struct BatchImpl : BatchSession::Impl {
     unsigned long long *dfo = (unsigned long long *)q; q += (size_t)nf * 8;
     int *dft = (int *)q; q += (size_t)nf * 4;
     int *dfs = (int *)q; q += (size_t)nf * 4;
+    int *dfs0 = (int *)q; q += (size_t)nf * 4;
     int *dout = (int *)q;
     ck(cudaMemcpyAsync(dfo, fo.data(), nf * 8, cudaMemcpyHostToDevice, s), "h2d");
     ck(cudaMemcpyAsync(dft, ft.data(), nf * 4, cudaMemcpyHostToDevice, s), "h2d");
     ck(cudaMemcpyAsync(dfs, fs.data(), nf * 4, cudaMemcpyHostToDevice, s), "h2d");
-    k_walk<<<(nf + 63) / 64, 64, 0, s>>>(dfo, dft, dfs, nf, (const uint32_t *const *)base,
-                                         (const uint8_t *const *)(base + pb), dout);
+    ck(cudaMemcpyAsync(dfs0, fs0.data(), nf * 4, cudaMemcpyHostToDevice, s), "h2d");
+    ck(cudaMemsetAsync(cnt.p, 0, 4, s), "memset");
+    k_walk<<<(nf + 63) / 64, 64, 0, s>>>(dfo, dft, dfs, dfs0, nf, (const uint32_t *const *)base,
+                                         (const uint8_t *const *)(base + pb), dout, cnt.as<int>());
     nlaunch++;
     std::vector<int> circ((size_t)nf * MAXDEPTH_WALK);
+    int bad = 0;
     ck(cudaMemcpyAsync(circ.data(), dout, circ.size() * 4, cudaMemcpyDeviceToHost, s), "d2h");
+    ck(cudaMemcpyAsync(&bad, cnt.p, 4, cudaMemcpyDeviceToHost, s), "d2h");
     ck(cudaStreamSynchronize(s), "walk");
+    if (bad) throw std::logic_error("batch tree walk ended early");
     for (int i = 0; i < nf; i++) {
       Job &j = J[found_ids[i]];
       j.out.res.circuit.assign(circ.begin() + (size_t)i * MAXDEPTH_WALK, circ.begin() + (size_t)i * MAXDEPTH_WALK + j.t);
@@ -2345,5 +2600,7 @@ long long BatchSession::launches() const { return impl_->launches(); }
 long long BatchSession::steps() const { return impl_->steps(); }
 size_t BatchSession::device_bytes() const { return impl_->device_bytes(); }
 size_t BatchSession::projected_bytes() const { return impl_->projected_bytes(); }
+void BatchSession::set_memory_budget(size_t bytes) { impl_->set_budget(bytes); }
+long long BatchSession::waits() const { return impl_->waits(); }
 
 }  // namespace cz

@@ -117,7 +117,10 @@ struct cz_server {
         const int nq = sp->hs.n;
         const double need = (double)sp->hs.G * ((double)(1 << (2 * nq)) * 16.0 + 40.0);
         if (running > 0 && projected + need > budget) { batch_deferred++; break; }
-        if (!sess[nq]) sess[nq] = new cz::BatchSession(*eng->e, nq);
+        if (!sess[nq]) {
+          sess[nq] = new cz::BatchSession(*eng->e, nq);
+          sess[nq]->set_memory_budget((size_t)budget);
+        }
         cz::Options o;
         o.depth = r->depth >= 0 ? r->depth : sp->hs.depth;
         const int jid = sess[nq]->submit(sp->hs, o);

@@ -394,7 +394,10 @@ __global__ void k_tc_seen_gather(const uint32_t *order, size_t n, const uint64_t
 double now_s() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
 struct TcCudaError : std::runtime_error { using std::runtime_error::runtime_error; };
 void tck(cudaError_t e, const char *what) {
-  if (e != cudaSuccess) throw TcCudaError(std::string("CUDA error after ") + what + ": " + cudaGetErrorString(e));
+  if (e != cudaSuccess) {
+    cudaGetLastError();            // a failed allocation must not be reported again by the next launch check
+    throw TcCudaError(std::string("CUDA error after ") + what + ": " + cudaGetErrorString(e));
+  }
 }
 struct Buf {
   void *p = nullptr;

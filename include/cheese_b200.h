@@ -100,9 +100,13 @@ typedef struct {
   int64_t frontier;                 /* nodes in the shared frontier */
   int64_t steps, kernel_launches;
   int64_t device_bytes;             /* device memory held by the session */
+  int64_t waits;                    /* job-steps a job waited for memory */
 } cz_batch_info;
 int cz_batch_create(cz_engine *engine, int nq, cz_batch **out);
 void cz_batch_destroy(cz_batch *batch);
+/* Device memory a step may plan for (default: 80% of the free memory when the session was made). When a step's
+ * jobs would need more, the later jobs wait that step (their nodes carried over); results do not change. */
+int cz_batch_set_memory(cz_batch *batch, double gb);
 /* Queue a search (the spec's qubit count must be the session's): the job id (>= 0), or -(exit code). */
 int cz_batch_submit(cz_batch *batch, const cz_spec *spec, const cz_options *opt);
 /* One level of every running job (admitting the queued ones first); *running = jobs not finished yet. */

@@ -46,6 +46,18 @@ def test_mixed_batch_matches_plain(eng):
             assert verify.equivalent(s, r.circuit)
 
 
+def test_memory_bound_session_matches_plain(eng):
+    """a budget too small for every job at once makes jobs wait steps (nodes carried over); results unchanged"""
+    from cheese_b200 import Batch
+    jobs = [(n, s) for n, s in _jobs(15, 48) if n == 3]
+    b = Batch(eng, 3, memory_gb=0.05)
+    ids = [b.submit(s) for _, s in jobs]
+    b.run()
+    assert b.info()["waits"] > 0
+    for (n, s), jid in zip(jobs, ids):
+        _same(b.result(jid), _plain(eng, s))
+
+
 def test_alone_equals_in_mix(eng):
     from cheese_b200 import Batch
     jobs = _jobs(12, 24)
