@@ -2286,7 +2286,7 @@ struct BatchImpl : BatchSession::Impl {
     struct Op { bool carry; long long p0, p1; unsigned long long cap, all; std::vector<int> jobs; };
     std::vector<Op> ops;
     size_t step_budget = budget;
-    {                                                     // never plan past what the device has left
+    if ((size_t)m * node * 8 > budget / 4) {              // a large step: never plan past what the device has left
       size_t fr = 0, tot = 0;
       if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
         const size_t mine = fR2.cap + fMeta2.cap + fJob2.cap + sH1.cap + sH2.cap + sIdx.cap + sMeta.cap + k0.cap +

@@ -181,9 +181,9 @@ struct cz_server {
           i++;
         }
       }
-      // a session with nothing running is dropped, so its buffers go back to the device
+      // a session stays (its buffers are reused by the next jobs) until it has held many jobs and none runs
       for (int q = 1; q <= 3; q++)
-        if (sess[q] && !sess[q]->running()) {
+        if (sess[q] && !sess[q]->running() && sess[q]->jobs() > 4096) {
           bool used = false;
           for (auto &l : live) used |= l.nq == q;
           if (!used) { delete sess[q]; sess[q] = nullptr; }
