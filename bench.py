@@ -377,7 +377,7 @@ def main():
             "e2e": {"value": e2e_pre / e2e_s, "unit": "prefixes/s", "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps},
             "gpu_launches": launches,
-            "roofline": {"bound": "int32", "kernel": "k_expand", "achieved": achieved / 1e12, "peak": peak_int / 1e12,
+            "roofline": {"bound": "int32", "kernel": "k_expand + k_tbound (one level)", "achieved": achieved / 1e12, "peak": peak_int / 1e12,
                          "unit": "Tops/s", "frac": achieved / peak_int if peak_int else None, "traffic": traffic,
                          "peak_source": "measured in this run: IMAD loop (multiply-add = 2 ops)",
                          "launch_ms": launch_ms, "ops_per_launch": ops / max(1, exp_launches)},
