@@ -21,12 +21,12 @@ CIRCUIT, PROOF, ERR_SPEC, ERR_USAGE, ERR_OVERFLOW, ERR_CUDA = 0, 1, 2, 3, 4, 5
 class LevelStats(C.Structure):
     _fields_ = [("t", C.c_int), ("parents", C.c_int64), ("prefixes", C.c_int64), ("cut_w3", C.c_int64),
                 ("cut_lb", C.c_int64), ("survivors", C.c_int64), ("distinct", C.c_int64),
-                ("proved_unsat", C.c_int), ("seconds", C.c_double)]
+                ("proved_unsat", C.c_int), ("seconds", C.c_double), ("table", C.c_int)]
 
 
 class Options(C.Structure):
     _fields_ = [("depth", C.c_int), ("dedupe", C.c_int), ("sym", C.c_int), ("store64", C.c_int),
-                ("profile", C.c_int)]
+                ("profile", C.c_int), ("table_k", C.c_int), ("cache_dir", C.c_char_p)]
 
 
 class Result(C.Structure):
@@ -35,7 +35,10 @@ class Result(C.Structure):
                 ("prefixes", C.c_int64), ("kernel_launches", C.c_int64), ("t_evals", C.c_int64),
                 ("children", C.c_int64), ("expand_ms", C.c_double), ("dedupe_ms", C.c_double),
                 ("total_ms", C.c_double), ("expand_launches", C.c_int64), ("h2d_bytes", C.c_int64),
-                ("d2h_bytes", C.c_int64), ("children_full", C.c_int64), ("error", C.c_char * 256)]
+                ("d2h_bytes", C.c_int64), ("children_full", C.c_int64), ("table_k", C.c_int),
+                ("table_split", C.c_int * 2), ("table_proof", C.c_int), ("table_classes", C.c_int64),
+                ("table_levels", C.c_int), ("table_loaded", C.c_int), ("table_built", C.c_int),
+                ("table_seconds", C.c_double), ("table_path", C.c_char * 256), ("error", C.c_char * 256)]
 
 
 LEVEL_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(LevelStats))
@@ -348,11 +351,14 @@ class Engine:
         out["table_built"] = res.table.built
         return rc, out, buf.value.decode().splitlines(), list(steps)
 
-    def search(self, spec, depth=-1, dedupe=True, sym=True, store64=False, profile=False, on_level=None):
-        """run `cheese SPEC [--depth D] [--no-dedupe] [--no-sym]`; returns a SearchOutcome"""
+    def search(self, spec, depth=-1, dedupe=True, sym=True, store64=False, profile=False, on_level=None,
+               table_k=0, cache_dir="build"):
+        """run `cheese SPEC [--depth D] [--no-dedupe] [--no-sym] [--table K]`; returns a SearchOutcome
+        (cache_dir: where the distance table of --table K is cached, None for no cache)"""
         if not isinstance(spec, Spec):
             spec = Spec(spec)
-        opt = Options(depth, int(dedupe), int(sym), int(store64), int(profile))
+        opt = Options(depth, int(dedupe), int(sym), int(store64), int(profile), int(table_k),
+                      cache_dir.encode() if cache_dir else None)
         levels = []
 
         def cb(_user, p):
@@ -384,7 +390,7 @@ class Batch:
     def submit(self, spec, depth=-1, dedupe=True, sym=True, store64=False):
         if not isinstance(spec, Spec):
             spec = Spec(spec)
-        opt = Options(depth, int(dedupe), int(sym), int(store64), 0)
+        opt = Options(depth, int(dedupe), int(sym), int(store64), 0, 0, None)
         jid = lib().cz_batch_submit(self._h, spec._h, C.byref(opt))
         if jid < 0:
             raise RuntimeError(f"cz_batch_submit failed: {-jid}")
@@ -512,13 +518,19 @@ class SearchOutcome:
         self.circuit = [spec.names[res.found[i]] for i in range(res.found_len)]
         self.n_found = res.n_found
         self.error = res.error.decode()
+        self.table_split = (res.table_split[0], res.table_split[1])
+        self.table = {k: getattr(res, k) for k in ("table_k", "table_proof", "table_classes", "table_levels",
+                                                   "table_loaded", "table_built", "table_seconds")}
+        self.table["table_path"] = res.table_path.decode()
 
-    def lines(self, seconds=False):
-        """stdout of the reference binary for this search (seconds as 0.00 unless asked for)"""
+    def lines(self, seconds=False, depth=None):
+        """stdout of the reference binary for this search (seconds as 0.00 unless asked for; depth: the --depth
+        of a --table run, for its proof line)"""
         out = []
         for s in self.levels:
             sec = f"{s['seconds']:.2f}" if seconds else "0.00"
-            out.append(f'{{"t": {s["t"]}, "parents": {s["parents"]}, "prefixes": {s["prefixes"]}, '
+            pre = '"dir": "table", ' if s.get("table") else ""
+            out.append(f'{{{pre}"t": {s["t"]}, "parents": {s["parents"]}, "prefixes": {s["prefixes"]}, '
                        f'"cut_w3": {s["cut_w3"]}, "cut_lb": {s["cut_lb"]}, "survivors": {s["survivors"]}, '
                        f'"distinct": {s["distinct"]}, "proved_unsat": {"true" if s["distinct"] == 0 else "false"}, '
                        f'"seconds": {sec}}}')
@@ -527,8 +539,12 @@ class SearchOutcome:
                 out.append('{"found": 0, "circuit": []}')
             else:
                 names = ", ".join(f'"{c}"' for c in self.circuit)
-                out.append(f'{{"t": {len(self.circuit)}, "found": {self.n_found or 1}, "circuit": [{names}], '
+                tab = (f', "table": [{self.table_split[0]}, {self.table_split[1]}]'
+                       if sum(self.table_split) > 0 else "")
+                out.append(f'{{"t": {len(self.circuit)}, "found": {self.n_found or 1}, "circuit": [{names}]{tab}, '
                            f'"seconds": 0.00}}')
+        elif self.rc == PROOF and self.table["table_proof"]:
+            out.append(f'{{"depth": {depth}, "proved_unsat": true, "table": {self.table["table_k"]}}}')
         return out
 
     @property

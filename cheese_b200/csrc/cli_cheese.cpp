@@ -14,9 +14,9 @@
 static double now() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
 
 static void print_level(void *, const cz_level_stats *s) {
-  std::printf("{\"t\": %d, \"parents\": %lld, \"prefixes\": %lld, \"cut_w3\": %lld, \"cut_lb\": %lld, \"survivors\": %lld, "
+  std::printf("{%s\"t\": %d, \"parents\": %lld, \"prefixes\": %lld, \"cut_w3\": %lld, \"cut_lb\": %lld, \"survivors\": %lld, "
               "\"distinct\": %lld, \"proved_unsat\": %s, \"seconds\": %.2f}\n",
-              s->t, (long long)s->parents, (long long)s->prefixes, (long long)s->cut_w3, (long long)s->cut_lb,
+              s->table ? "\"dir\": \"table\", " : "", s->t, (long long)s->parents, (long long)s->prefixes, (long long)s->cut_w3, (long long)s->cut_lb,
               (long long)s->survivors, (long long)s->distinct, s->distinct ? "false" : "true", s->seconds);
   std::fflush(stdout);
 }
@@ -56,11 +56,12 @@ int main(int argc, char **argv) {
     return 3;
   }
   if (prc == CZ_ERR_USAGE || !spec) { std::fprintf(stderr, "n = %d not built (NQ_MIN..NQ_MAX)\n", n); return 3; }
-  if (mitm || tablek > 0) {
-    std::fprintf(stderr, "--mitm / --table: not available in this build\n");
+  if (mitm) {
+    std::fprintf(stderr, "--mitm: not available in this build\n");
     return 3;
   }
   opt.depth = depth;
+  opt.table_k = tablek > 0 ? tablek : 0;
   opt.profile = profile;
   cz_engine *eng = nullptr;
   if (cz_engine_create(0, &eng, err, sizeof err)) { std::fprintf(stderr, "CUDA error after engine: %s\n", err); return 5; }
@@ -68,14 +69,25 @@ int main(int argc, char **argv) {
   const double t0 = now();
   const int rc = cz_search(eng, spec, &opt, print_level, nullptr, &res);
   std::fprintf(stderr, "symmetry classes: %d group elements\n", res.nsym);
+  if (res.table_loaded)
+    std::fprintf(stderr, "table %s: %lld classes (loaded, %.1f s)\n", res.table_path, (long long)res.table_classes,
+                 res.table_seconds);
+  else if (res.table_built)
+    std::fprintf(stderr, "table: %lld classes within %d gates (%.1f s), cached in %s\n", (long long)res.table_classes,
+                 res.table_levels, res.table_seconds, res.table_path);
   int code = rc;
   if (rc == CZ_CIRCUIT) {
     if (res.depth0) std::printf("{\"found\": 0, \"circuit\": []}\n");
     else {
       std::printf("{\"t\": %d, \"found\": %lld, \"circuit\": [", res.found_len, (long long)(res.n_found ? res.n_found : 1));
       for (int i = 0; i < res.found_len; i++) std::printf("%s\"%s\"", i ? ", " : "", cz_spec_gate_name(spec, res.found[i]));
-      std::printf("], \"seconds\": %.2f}\n", now() - t0);
+      if (res.table_split[0] + res.table_split[1] > 0)
+        std::printf("], \"table\": [%d, %d], \"seconds\": %.2f}\n", res.table_split[0], res.table_split[1], now() - t0);
+      else
+        std::printf("], \"seconds\": %.2f}\n", now() - t0);
     }
+  } else if (rc == CZ_PROOF && res.table_proof) {
+    std::printf("{\"depth\": %d, \"proved_unsat\": true, \"table\": %d}\n", depth, res.table_k);
   } else if (rc == CZ_ERR_CUDA) {
     std::fprintf(stderr, "%s\n", res.error);
   } else if (rc != CZ_PROOF) {

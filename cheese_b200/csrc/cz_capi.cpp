@@ -80,68 +80,8 @@ void cz_engine_destroy(cz_engine *engine) {
 
 void cz_options_default(cz_options *opt) {
   if (!opt) return;
-  opt->depth = -1; opt->dedupe = 1; opt->sym = 1; opt->store64 = 0; opt->profile = 0;
-}
-
-int cz_search(cz_engine *engine, const cz_spec *spec, const cz_options *opt, cz_level_fn on_level, void *user,
-              cz_result *out) {
-  if (!engine || !spec || !out) return CZ_ERR_USAGE;
-  std::memset(out, 0, sizeof *out);
-  cz_options o;
-  cz_options_default(&o);
-  if (opt) o = *opt;
-  const cz::HostSpec &hs = spec->hs;
-  if (hs.states) {
-    put_err(out->error, sizeof out->error, "state targets: GPU path not ready yet, use build/cheese-cpu");
-    out->rc = CZ_ERR_USAGE;
-    return CZ_ERR_USAGE;
-  }
-  const int depth = o.depth >= 0 ? o.depth : hs.depth;
-  if (depth > CZ_MAX_DEPTH) {
-    put_err(out->error, sizeof out->error, "depth > " + std::to_string(CZ_MAX_DEPTH));
-    out->rc = CZ_ERR_USAGE;
-    return CZ_ERR_USAGE;
-  }
-  cz::Options eo;
-  eo.depth = depth; eo.dedupe = o.dedupe != 0; eo.sym = o.sym != 0; eo.store64 = o.store64; eo.profile = o.profile != 0;
-  cz::SearchResult r;
-  int rc;
-  try {
-    rc = engine->e->search(hs, eo, [&](const cz::LevelStats &L) {
-      if (!on_level) return;
-      cz_level_stats s;
-      s.t = L.t; s.parents = L.parents; s.prefixes = L.prefixes; s.cut_w3 = L.cut_w3; s.cut_lb = L.cut_lb;
-      s.survivors = L.survivors; s.distinct = L.distinct; s.proved_unsat = L.proved_unsat; s.seconds = L.seconds;
-      on_level(user, &s);
-    }, r);
-  } catch (const std::bad_alloc &) {
-    r.error = "host out of memory";
-    rc = CZ_ERR_CUDA;
-  } catch (const std::exception &ex) {
-    r.error = ex.what();
-    rc = CZ_ERR_CUDA;
-  }
-  out->rc = rc;
-  out->depth0 = r.depth0;
-  out->found_len = (int)r.circuit.size();
-  for (size_t i = 0; i < r.circuit.size() && i < CZ_MAX_DEPTH; i++) out->found[i] = r.circuit[i];
-  out->n_found = r.n_found;
-  out->nsym = r.nsym;
-  out->store64 = r.store64;
-  out->levels = r.levels;
-  out->prefixes = r.prefixes;
-  out->kernel_launches = r.launches;
-  out->t_evals = r.t_evals;
-  out->children = r.children;
-  out->expand_ms = r.expand_ms;
-  out->dedupe_ms = r.dedupe_ms;
-  out->total_ms = r.total_ms;
-  out->expand_launches = r.expand_launches;
-  out->h2d_bytes = r.h2d_bytes;
-  out->d2h_bytes = r.d2h_bytes;
-  out->children_full = r.children_full;
-  put_err(out->error, sizeof out->error, r.error);
-  return rc;
+  opt->depth = -1; opt->dedupe = 1; opt->sym = 1; opt->store64 = 0; opt->profile = 0; opt->table_k = 0;
+  opt->cache_dir = "build";
 }
 
 namespace {
@@ -165,9 +105,76 @@ void fill_result(const cz::SearchResult &r, cz_result *out) {
   out->h2d_bytes = r.h2d_bytes;
   out->d2h_bytes = r.d2h_bytes;
   out->children_full = r.children_full;
+  out->table_k = r.table_k;
+  out->table_split[0] = r.table_split[0];
+  out->table_split[1] = r.table_split[1];
+  out->table_proof = r.table_proof;
+  out->table_classes = r.table_classes;
+  out->table_levels = r.table_levels;
+  out->table_loaded = r.table_loaded;
+  out->table_built = r.table_built;
+  out->table_seconds = r.table_seconds;
+  put_err(out->table_path, sizeof out->table_path, r.table_path);
   put_err(out->error, sizeof out->error, r.error);
 }
+
+cz_level_stats level_stats(const cz::LevelStats &L) {
+  cz_level_stats s;
+  s.t = L.t; s.parents = L.parents; s.prefixes = L.prefixes; s.cut_w3 = L.cut_w3; s.cut_lb = L.cut_lb;
+  s.survivors = L.survivors; s.distinct = L.distinct; s.proved_unsat = L.proved_unsat; s.seconds = L.seconds;
+  s.table = L.table;
+  return s;
+}
 }  // namespace
+
+int cz_search(cz_engine *engine, const cz_spec *spec, const cz_options *opt, cz_level_fn on_level, void *user,
+              cz_result *out) {
+  if (!engine || !spec || !out) return CZ_ERR_USAGE;
+  std::memset(out, 0, sizeof *out);
+  cz_options o;
+  cz_options_default(&o);
+  if (opt) o = *opt;
+  const cz::HostSpec &hs = spec->hs;
+  if (hs.states) {
+    put_err(out->error, sizeof out->error, "state targets: GPU path not ready yet, use build/cheese-cpu");
+    out->rc = CZ_ERR_USAGE;
+    return CZ_ERR_USAGE;
+  }
+  const int depth = o.depth >= 0 ? o.depth : hs.depth;
+  if (depth > CZ_MAX_DEPTH) {
+    put_err(out->error, sizeof out->error, "depth > " + std::to_string(CZ_MAX_DEPTH));
+    out->rc = CZ_ERR_USAGE;
+    return CZ_ERR_USAGE;
+  }
+  cz::Options eo;
+  eo.depth = depth; eo.dedupe = o.dedupe != 0; eo.sym = o.sym != 0; eo.store64 = o.store64; eo.profile = o.profile != 0;
+  if (o.table_k < 0 || o.table_k > CZ_MAX_DEPTH) {
+    put_err(out->error, sizeof out->error, "table depth out of range");
+    out->rc = CZ_ERR_USAGE;
+    return CZ_ERR_USAGE;
+  }
+  eo.table_k = o.table_k;
+  eo.cache_dir = o.cache_dir ? o.cache_dir : "";
+  cz::SearchResult r;
+  int rc;
+  try {
+    rc = engine->e->search(hs, eo, [&](const cz::LevelStats &L) {
+      if (!on_level) return;
+      const cz_level_stats s = level_stats(L);
+      on_level(user, &s);
+    }, r);
+  } catch (const std::bad_alloc &) {
+    r.error = "host out of memory";
+    rc = CZ_ERR_CUDA;
+  } catch (const std::exception &ex) {
+    r.error = ex.what();
+    rc = CZ_ERR_CUDA;
+  }
+  r.rc = rc;
+  fill_result(r, out);
+  return rc;
+}
+
 
 int cz_batch_create(cz_engine *engine, int nq, cz_batch **out) {
   if (!engine || !out || nq < 1 || nq > 3) return CZ_ERR_USAGE;
@@ -250,9 +257,7 @@ int cz_batch_result(const cz_batch *batch, int job, cz_level_fn on_level, void *
   if (!j.done) return CZ_ERR_USAGE;
   for (const cz::LevelStats &L : j.levels) {
     if (!on_level) break;
-    cz_level_stats s;
-    s.t = L.t; s.parents = L.parents; s.prefixes = L.prefixes; s.cut_w3 = L.cut_w3; s.cut_lb = L.cut_lb;
-    s.survivors = L.survivors; s.distinct = L.distinct; s.proved_unsat = L.proved_unsat; s.seconds = L.seconds;
+    const cz_level_stats s = level_stats(L);
     on_level(user, &s);
   }
   fill_result(j.res, out);

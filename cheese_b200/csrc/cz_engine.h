@@ -16,6 +16,8 @@ struct Options {
   int store64 = 0;           // 0: int32 residual limbs, promoted to int64 when a value leaves int32; 1: int64 from the start
   bool profile = false;      // per-phase device times (CUDA events on the engine's stream)
   bool nogoal = false;       // never report the goal (distance-table build)
+  int table_k = 0;           // --table K
+  std::string cache_dir = "build";   // distance-table cache directory ("" : no cache)
 };
 
 struct LevelStats {
@@ -23,6 +25,7 @@ struct LevelStats {
   long long parents = 0, prefixes = 0, cut_w3 = 0, cut_lb = 0, survivors = 0, distinct = 0;
   bool proved_unsat = false;
   double seconds = 0;
+  bool table = false;        // a level of the distance-table build
 };
 
 struct SearchResult {
@@ -40,6 +43,13 @@ struct SearchResult {
   double expand_ms = 0, dedupe_ms = 0, total_ms = 0;   // device times (profile) / host wall time
   long long expand_launches = 0;       // level-kernel launches (the denominator of per-launch figures)
   long long h2d_bytes = 0, d2h_bytes = 0;   // host<->device traffic of the call
+  // --table K
+  int table_k = 0, table_split[2] = {0, 0};
+  bool table_proof = false, table_loaded = false, table_built = false;
+  long long table_classes = 0;
+  int table_levels = 0;
+  double table_seconds = 0;
+  std::string table_path;
   std::string error;
 };
 

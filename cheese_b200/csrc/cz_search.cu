@@ -40,6 +40,7 @@ namespace cz {
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
+constexpr int RC_STOP = -3;        // levels(): stopped after the requested level
 constexpr int EXP_WARPS = 8;       // warps per expand block
 constexpr int INHERIT_KMAX = 60;
 enum GateKind : uint8_t { GK_GENERAL = 0, GK_ONEQ = 1, GK_PERM = 2 };   // the T bound is computed exactly (mod 2^32 / 2^64) only while 2(n + k) <= 128
@@ -1260,6 +1261,185 @@ __global__ void __launch_bounds__(RES_WARPS * 32) k_materialize(const DevSpec sp
   }
 }
 
+// ---------------- distance table (--table K) ----------------
+__global__ void k_keys_gather(const uint32_t *order, size_t n, const uint64_t *a1, const uint64_t *a2,
+                              const uint32_t *ai, const uint32_t *al, uint64_t *s1, uint64_t *s2, uint32_t *si,
+                              uint32_t *sl) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t o = order[i];
+    s1[i] = a1[o]; s2[i] = a2[o]; si[i] = ai[o]; sl[i] = al[o];
+  }
+}
+// the class key of every node of a frontier (one warp each)
+template <int NQ, typename ST>
+__global__ void __launch_bounds__(RES_WARPS * 32) k_node_keys(const __grid_constant__ DevSpec sp, const Z4<ST> *R,
+                                                            const NodeMeta *meta, long long n, uint64_t *F1,
+                                                            uint64_t *F2) {
+  constexpr int E = (1 << NQ) * (1 << NQ), EPL = E >= 32 ? E / 32 : 1;
+  __shared__ Z4<ST> sC[RES_WARPS][E];
+  __shared__ uint64_t W1[E], W2[E];
+  init_weights(W1, W2, E);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned conjmask = 0;
+  for (int i = 0; i < sp.nsym; i++) conjmask |= (unsigned)(sp.symconj[i] != 0) << i;
+  for (long long j = blockIdx.x * (long long)RES_WARPS + w; j < n; j += (long long)gridDim.x * RES_WARPS) {
+#pragma unroll
+    for (int q = 0; q < EPL; q++) {
+      const int e = lane + 32 * q;
+      if (e < E) sC[w][e] = R[j * E + e];
+    }
+    __syncwarp();
+    uint64_t k1, k2;
+    warp_class_key<NQ, ST>(sC[w], meta[j].k, sp.nsym, conjmask, sp.symperm, W1, W2, lane, k1, k2);
+    if (lane == 0) { F1[j] = k1; F2[j] = k2; }
+    __syncwarp();
+  }
+}
+
+// the residual of table node (lvl, idx): the identity times the inverses of its path's gates, into C (P, path:
+// scratch); returns its exponent
+template <int NQ, typename ST>
+__device__ int warp_replay(const DevSpec &sp, const uint32_t *const *tpar, const uint8_t *const *tgat, int lvl,
+                           uint32_t idx, Z4<ST> *P, Z4<ST> *C, uint8_t *path, int lane) {
+  constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
+  if (lane == 0)
+    for (int l = lvl; l >= 1; l--) { path[l - 1] = tgat[l][idx]; idx = tpar[l][idx]; }
+#pragma unroll
+  for (int q = 0; q < EPL; q++) {
+    const int e = lane + 32 * q;
+    if (e < E) C[e] = (e >> NQ) == (e & (N - 1)) ? Z4<ST>{1, 0, 0, 0} : Z4<ST>{0, 0, 0, 0};
+  }
+  __syncwarp();
+  int k = 0;
+  for (int i = 0; i < lvl; i++) {
+#pragma unroll
+    for (int q = 0; q < EPL; q++) {
+      const int e = lane + 32 * q;
+      if (e < E) P[e] = C[e];
+    }
+    __syncwarp();
+    bool ovf;
+    k = warp_child<NQ, ST>(P, C, path[i], k, sp, &sp, lane, ovf);
+    __syncwarp();
+  }
+  return k;
+}
+
+__device__ __forceinline__ long long keys_lower(const uint64_t *S1, long long n, uint64_t h1) {
+  long long lo = 0, hi = n;
+  while (lo < hi) { const long long mid = (lo + hi) >> 1; if (S1[mid] < h1) lo = mid + 1; else hi = mid; }
+  return lo;
+}
+
+// table build: is each kept child's class already in the table at a lower level? (hash match, then exact)
+template <int NQ, typename ST>
+__global__ void __launch_bounds__(RES_WARPS * 32) k_seen_filter(
+    const __grid_constant__ DevSpec sp, int GS, const Z4<ST> *R, const NodeMeta *meta, const uint64_t *kidx,
+    const uint32_t *kslot, size_t nk, const uint64_t *sh1, const uint64_t *sh2, const NodeMeta *smeta,
+    const uint64_t *S1, const uint64_t *S2, const uint32_t *Sidx, const uint32_t *Slvl, long long ns,
+    const uint32_t *const *tpar, const uint8_t *const *tgat, uint8_t *old) {
+  __shared__ ResolveSmem<NQ, ST> sm;
+  __shared__ uint8_t spath[RES_WARPS][64];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (size_t i = blockIdx.x * (size_t)RES_WARPS + w; i < nk; i += (size_t)gridDim.x * RES_WARPS) {
+    const uint32_t sl = kslot[i];
+    const uint64_t h1 = sh1[sl], h2 = sh2[sl];
+    const int ka = smeta[sl].k;
+    bool dup = false, haveA = false;
+    for (long long x = keys_lower(S1, ns, h1); x < ns && S1[x] == h1 && !dup; x++) {
+      if (S2[x] != h2) continue;
+      if (!haveA) { warp_materialize<NQ, ST>(R, meta, kidx[i], GS, sp, &sp, sm.P[w], sm.A[w], lane); haveA = true; }
+      const int kb = warp_replay<NQ, ST>(sp, tpar, tgat, (int)Slvl[x], Sidx[x], sm.P[w], sm.B[w], spath[w], lane);
+      if (kb == ka) dup = warp_same_class<NQ, ST>(sm.A[w], sm.B[w], sp, sp.symperm, lane);
+    }
+    if (lane == 0) old[i] = dup;
+    __syncwarp();
+  }
+}
+__global__ void k_drop_old(const uint64_t *kidx, const uint32_t *kslot, size_t nk, const uint8_t *old, uint64_t *kidx2,
+                           uint32_t *kslot2, unsigned long long *cnt) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nk; i += (size_t)gridDim.x * blockDim.x)
+    if (!old[i]) {
+      const unsigned long long p = atomicAdd(cnt, 1ULL);
+      kidx2[p] = kidx[i];
+      kslot2[p] = kslot[i];
+    }
+}
+// node j of a frontier against the table: the first entry of its class key with level <= maxc, or -1
+__global__ void k_table_lookup(const uint64_t *F1, const uint64_t *F2, long long n, const uint64_t *S1,
+                               const uint64_t *S2, const uint32_t *Slvl, long long ns, int maxc, long long *hit) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
+    long long r = -1;
+    for (long long x = keys_lower(S1, ns, F1[j]); x < ns && S1[x] == F1[j]; x++)
+      if (S2[x] == F2[j] && (int)Slvl[x] <= maxc) { r = x; break; }
+    hit[j] = r;
+  }
+}
+// one warp: every (entry x, symmetry s) from x0 on with s(E_x) == S exactly, in the reference's order
+// (cheese.cu:1570-1575); up to cap pairs into out
+template <int NQ, typename ST>
+__global__ void k_table_confirm(const __grid_constant__ DevSpec sp, const Z4<ST> *S, int ks, const uint64_t *S1,
+                                const uint64_t *S2, const uint32_t *Sidx, const uint32_t *Slvl, long long ns,
+                                long long x0, int maxc, const uint32_t *const *tpar, const uint8_t *const *tgat,
+                                int2 *out, int cap, int *nout) {
+  constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
+  __shared__ Z4<ST> A[E], B[E], P[E];
+  __shared__ uint8_t path[64];
+  const int lane = threadIdx.x;
+#pragma unroll
+  for (int q = 0; q < EPL; q++) {
+    const int e = lane + 32 * q;
+    if (e < E) A[e] = S[e];
+  }
+  __syncwarp();
+  int cnt = 0;
+  const uint64_t h1 = S1[x0], h2 = S2[x0];
+  for (long long x = x0; x < ns && S1[x] == h1; x++) {
+    if (S2[x] != h2 || (int)Slvl[x] > maxc) continue;
+    const int kb = warp_replay<NQ, ST>(sp, tpar, tgat, (int)Slvl[x], Sidx[x], P, B, path, lane);
+    if (kb != ks) continue;
+    for (int sy = 0; sy < sp.nsym; sy++) {
+      bool eq = true;
+#pragma unroll
+      for (int q = 0; q < EPL; q++) {
+        const int e = lane + 32 * q;
+        if (e >= E) continue;
+        const Z4<ST> v = sp.symconj[sy] ? zcj(B[e]) : B[e];
+        if (!zq(v, A[sp.symperm[sy][e >> NQ] * N + sp.symperm[sy][e & (N - 1)]])) eq = false;
+      }
+      if (__all_sync(FULL, eq)) {
+        if (lane == 0 && cnt < cap) out[cnt] = make_int2((int)x, sy);
+        cnt++;
+      }
+    }
+  }
+  if (lane == 0) *nout = cnt < cap ? cnt : cap;
+}
+
+// keys of table level lvl from its tree (a table file written by another program): replay + class key
+template <int NQ, typename ST>
+__global__ void __launch_bounds__(RES_WARPS * 32) k_replay_keys(const __grid_constant__ DevSpec sp, int lvl,
+                                                              long long n, const uint32_t *const *tpar,
+                                                              const uint8_t *const *tgat, uint64_t *F1, uint64_t *F2) {
+  constexpr int E = (1 << NQ) * (1 << NQ);
+  __shared__ Z4<ST> sP[RES_WARPS][E], sC[RES_WARPS][E];
+  __shared__ uint64_t W1[E], W2[E];
+  __shared__ uint8_t spath[RES_WARPS][64];
+  init_weights(W1, W2, E);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned conjmask = 0;
+  for (int i = 0; i < sp.nsym; i++) conjmask |= (unsigned)(sp.symconj[i] != 0) << i;
+  for (long long j = blockIdx.x * (long long)RES_WARPS + w; j < n; j += (long long)gridDim.x * RES_WARPS) {
+    const int k = warp_replay<NQ, ST>(sp, tpar, tgat, lvl, (uint32_t)j, sP[w], sC[w], spath[w], lane);
+    uint64_t k1, k2;
+    warp_class_key<NQ, ST>(sC[w], k, sp.nsym, conjmask, sp.symperm, W1, W2, lane, k1, k2);
+    if (lane == 0) { F1[j] = k1; F2[j] = k2; }
+    __syncwarp();
+  }
+}
+
 __global__ void k_widen(const Z4<int32_t> *in, Z4<int64_t> *out, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const Z4<int32_t> x = in[i];
@@ -1356,6 +1536,23 @@ struct Engine::Impl {
   SpecDev specs[8];
   long long use_clock = 0;
   std::vector<DBuf> par, gat;              // tree, one level each
+  std::vector<long long> level_n;          // nodes per level of the tree
+  struct DistTable {                       // --table K: every class within K gates, its tree and sorted keys
+    int K = 0, nl = 0;
+    std::vector<DBuf> par, gat;            // [l], l = 1..nl
+    std::vector<long long> n;              // [0..nl]
+    DBuf S1, S2, Sidx, Slvl;               // class keys sorted by S1 (stable: lower levels first)
+    long long ns = 0;
+    void release() {
+      for (auto &b : par) b.release();
+      for (auto &b : gat) b.release();
+      S1.release(); S2.release(); Sidx.release(); Slvl.release();
+    }
+  };
+  std::map<std::string, DistTable *> dtabs;   // resident tables by cache path
+  DistTable *building = nullptr;           // a table build: children are filtered against it, levels added to it
+  bool want_keys = false;                  // keep the frontier's class keys (fK1, fK2)
+  DBuf fK1, fK2, tptrs, keys2, old;
   DevStats *hstats = nullptr;              // pinned
   long long launches = 0, expand_launches = 0, h2d = 0, d2h = 0;
   long long front_m = 1;                   // nodes in the current frontier
@@ -1374,6 +1571,8 @@ struct Engine::Impl {
                     &work, &tmp, &kidx, &kslot, &stats})
       b->release();
     for (auto &sd : specs) sd.release();
+    for (auto &kv : dtabs) { kv.second->release(); delete kv.second; }
+    for (DBuf *b : {&fK1, &fK2, &tptrs, &keys2, &old}) b->release();
     for (auto &b : par) b.release();
     for (auto &b : gat) b.release();
     if (hstats) cudaFreeHost(hstats);
@@ -1388,17 +1587,28 @@ struct Engine::Impl {
   void eval_bounds(const HostSpec &hs, int count, const int64_t *ent, const int *ks, int *out4);
   template <int NQ, typename ST>
   int levels(const HostSpec &hs, const DevSpec &sp, const Options &opt, int depth, int &t_start,
-             const std::function<void(const LevelStats &)> &cb, SearchResult &res);
+             const std::function<void(const LevelStats &)> &cb, SearchResult &res, int stop = 1 << 30);
+  // --table K
+  template <int NQ> int run_table(const HostSpec &hs, const Options &opt, const std::function<void(const LevelStats &)> &cb,
+                                  SearchResult &res);
+  template <int NQ> DistTable *get_table(const HostSpec &hs, const SymGroup &grp, int K, const Options &opt,
+                                         const std::function<void(const LevelStats &)> &cb, SearchResult &res);
+  template <int NQ> int table_levels_keys(const DevSpec &sp, long long n);   // keys of the frontier into fK1/fK2
+  void seen_add(DistTable &D, long long n, int lvl);                         // append fK1/fK2 level to D's keys
+  const void *const *upload_tree(const std::vector<DBuf> &p, const std::vector<DBuf> &g, int upto);
+  bool table_load(const std::string &path, DistTable &D, int K);
+  void table_save(const std::string &path, const DistTable &D);
 };
 
 template <int NQ, typename ST>
 int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &opt, int depth, int &t_start,
-                         const std::function<void(const LevelStats &)> &cb, SearchResult &res) {
+                         const std::function<void(const LevelStats &)> &cb, SearchResult &res, int stop) {
   constexpr int E = (1 << NQ) * (1 << NQ);
   const int G = hs.G;
   long long m = front_m;
   double surv_rate = 1.0;                              // survivors per child of the previous level
-  for (int t = t_start; t <= depth; t++) {
+  if ((int)level_n.size() < t_start) level_n.resize(t_start, 0);
+  for (int t = t_start; t <= depth && t <= stop; t++) {
     const double t0 = now_s();
     const bool keep = t < depth;
     // survivors capacity: the previous level's survivor rate with room to spare (at least 1 Mi records, at most
@@ -1513,6 +1723,29 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
         launches++;
         distinct = (long long)ns;
       }
+      if (building && distinct) {   // a table level: drop classes the table holds at a lower level
+        const void *const *tp = upload_tree(par, gat, t - 1);
+        old.ensure((size_t)distinct + 8); keys2.ensure((size_t)distinct * 12 + 16);
+        const unsigned gq = (unsigned)std::max<long long>(1, std::min<long long>((distinct + RES_WARPS - 1) / RES_WARPS,
+                                                                                 (long long)nsm * 16));
+        k_seen_filter<NQ, ST><<<gq, RES_WARPS * 32, 0, s>>>(
+            sp, G, fR.as<Z4<ST>>(), fMeta.as<NodeMeta>(), kidx.as<uint64_t>(), kslot.as<uint32_t>(), (size_t)distinct,
+            sH1.as<uint64_t>(), sH2.as<uint64_t>(), sMeta.as<NodeMeta>(), building->S1.as<uint64_t>(),
+            building->S2.as<uint64_t>(), building->Sidx.as<uint32_t>(), building->Slvl.as<uint32_t>(), building->ns,
+            (const uint32_t *const *)tp, (const uint8_t *const *)(tp + t), old.as<uint8_t>());
+        ck(cudaMemsetAsync(&dst->n_work, 0, 8, s), "memset");
+        uint64_t *ki2 = (uint64_t *)keys2.p;
+        uint32_t *ks2 = (uint32_t *)(ki2 + distinct);
+        k_drop_old<<<gb, 256, 0, s>>>(kidx.as<uint64_t>(), kslot.as<uint32_t>(), (size_t)distinct, old.as<uint8_t>(),
+                                      ki2, ks2, &dst->n_work);
+        launches += 2;
+        unsigned long long kept_new = 0;
+        ck(cudaMemcpyAsync(&kept_new, &dst->n_work, 8, cudaMemcpyDeviceToHost, s), "d2h");
+        ck(cudaStreamSynchronize(s), "table filter");
+        ck(cudaMemcpyAsync(kidx.p, ki2, kept_new * 8, cudaMemcpyDeviceToDevice, s), "d2d");
+        ck(cudaMemcpyAsync(kslot.p, ks2, kept_new * 4, cudaMemcpyDeviceToDevice, s), "d2d");
+        distinct = (long long)kept_new;
+      }
       // restore lexicographic order: sort kept (index, slot) pairs by index
       int bits = 1;
       while (bits < 64 && ((unsigned long long)m * G) >> bits) bits++;
@@ -1538,6 +1771,8 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
       ck(cudaGetLastError(), "gather");
       std::swap(fR, fR2);
       std::swap(fMeta, fMeta2);
+      if ((building || want_keys) && distinct) table_levels_keys<NQ>(sp, distinct);
+      if (building && distinct) seen_add(*building, distinct, t);
       if (opt.profile) ck(cudaEventRecord(ev[3], s), "event");
       ck(cudaStreamSynchronize(s), "gather");
       if (opt.profile) { float ms = 0; cudaEventElapsedTime(&ms, ev[2], ev[3]); res.dedupe_ms += ms; }
@@ -1545,14 +1780,449 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
     L.distinct = distinct;
     L.proved_unsat = distinct == 0;
     L.seconds = now_s() - t0;
+    L.table = building != nullptr;
     res.levels = t;
     cb(L);
     if (!distinct) return RC_PROOF;
     m = distinct;
     front_m = m;
+    if ((int)level_n.size() <= t) level_n.resize(t + 1, 0);
+    level_n[t] = distinct;
     t_start = t + 1;
+    if (t == stop) return RC_STOP;
   }
   return RC_PROOF;   // stopped at the last level (not reachable: the last level keeps nothing)
+}
+
+// ---------------- distance table (--table K), host ----------------
+// device array of the tree's per-level pointers: par[0..upto] then gat[0..upto]
+const void *const *Engine::Impl::upload_tree(const std::vector<DBuf> &p, const std::vector<DBuf> &g, int upto) {
+  std::vector<const void *> v(2 * (upto + 1), nullptr);
+  for (int l = 1; l <= upto && l < (int)p.size(); l++) { v[l] = p[l].p; v[upto + 1 + l] = g[l].p; }
+  tptrs.ensure(v.size() * sizeof(void *) + 16);
+  ck(cudaMemcpyAsync(tptrs.p, v.data(), v.size() * sizeof(void *), cudaMemcpyHostToDevice, s), "h2d");
+  return (const void *const *)tptrs.p;
+}
+
+template <int NQ>
+int Engine::Impl::table_levels_keys(const DevSpec &sp, long long n) {
+  fK1.ensure(n * 8 + 8); fK2.ensure(n * 8 + 8);
+  const unsigned g = (unsigned)std::max<long long>(1, std::min<long long>((n + RES_WARPS - 1) / RES_WARPS, (long long)nsm * 16));
+  k_node_keys<NQ, int32_t><<<g, RES_WARPS * 32, 0, s>>>(sp, fR.as<Z4<int32_t>>(), fMeta.as<NodeMeta>(), n,
+                                                        fK1.as<uint64_t>(), fK2.as<uint64_t>());
+  launches++;
+  ck(cudaGetLastError(), "node keys");
+  return 0;
+}
+
+// append level `lvl` (its keys in fK1/fK2, n nodes) to the table's keys, kept sorted by h1 (stable)
+void Engine::Impl::seen_add(DistTable &D, long long n, int lvl) {
+  const size_t tot = (size_t)(D.ns + n);
+  DBuf a1, a2, ai, al;
+  a1.ensure(tot * 8); a2.ensure(tot * 8); ai.ensure(tot * 4); al.ensure(tot * 4);
+  if (D.ns) {
+    ck(cudaMemcpyAsync(a1.p, D.S1.p, D.ns * 8, cudaMemcpyDeviceToDevice, s), "d2d");
+    ck(cudaMemcpyAsync(a2.p, D.S2.p, D.ns * 8, cudaMemcpyDeviceToDevice, s), "d2d");
+    ck(cudaMemcpyAsync(ai.p, D.Sidx.p, D.ns * 4, cudaMemcpyDeviceToDevice, s), "d2d");
+    ck(cudaMemcpyAsync(al.p, D.Slvl.p, D.ns * 4, cudaMemcpyDeviceToDevice, s), "d2d");
+  }
+  ck(cudaMemcpyAsync(a1.as<uint64_t>() + D.ns, fK1.p, n * 8, cudaMemcpyDeviceToDevice, s), "d2d");
+  ck(cudaMemcpyAsync(a2.as<uint64_t>() + D.ns, fK2.p, n * 8, cudaMemcpyDeviceToDevice, s), "d2d");
+  {
+    std::vector<uint32_t> idx(n), lv(n, (uint32_t)lvl);
+    for (long long i = 0; i < n; i++) idx[i] = (uint32_t)i;
+    ck(cudaMemcpyAsync(ai.as<uint32_t>() + D.ns, idx.data(), n * 4, cudaMemcpyHostToDevice, s), "h2d");
+    ck(cudaMemcpyAsync(al.as<uint32_t>() + D.ns, lv.data(), n * 4, cudaMemcpyHostToDevice, s), "h2d");
+    ck(cudaStreamSynchronize(s), "h2d");
+  }
+  k0.ensure(tot * 8); k1.ensure(tot * 8); v0.ensure(tot * 4); v1.ensure(tot * 4);
+  hist.ensure(sort_hist_words(tot) * 4); part.ensure(scan_partials_words(sort_hist_words(tot)) * 4);
+  SortScratch sc{hist.as<uint32_t>(), part.as<uint32_t>(), hist.cap / 4, part.cap / 4};
+  const unsigned gb = (unsigned)std::max<size_t>(1, std::min<size_t>((tot + 255) / 256, (size_t)nsm * 16));
+  k_sort_init<<<gb, 256, 0, s>>>(a1.as<uint64_t>(), tot, k0.as<uint64_t>(), v0.as<uint32_t>());
+  const bool f = radix_sort(k0.as<uint64_t>(), v0.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(), tot, 0, 64, sc,
+                            s, nullptr);
+  launches += 1 + 8 * 5;
+  const uint32_t *order = f ? v1.as<uint32_t>() : v0.as<uint32_t>();
+  D.S1.ensure(tot * 8); D.S2.ensure(tot * 8); D.Sidx.ensure(tot * 4); D.Slvl.ensure(tot * 4);
+  k_keys_gather<<<gb, 256, 0, s>>>(order, tot, a1.as<uint64_t>(), a2.as<uint64_t>(), ai.as<uint32_t>(),
+                                   al.as<uint32_t>(), D.S1.as<uint64_t>(), D.S2.as<uint64_t>(), D.Sidx.as<uint32_t>(),
+                                   D.Slvl.as<uint32_t>());
+  launches++;
+  ck(cudaStreamSynchronize(s), "table keys");
+  a1.release(); a2.release(); ai.release(); al.release();
+  D.ns = (long long)tot;
+}
+
+namespace {
+uint64_t fnv_bytes(uint64_t h, const void *p, size_t n) {
+  const unsigned char *c = (const unsigned char *)p;
+  for (size_t i = 0; i < n; i++) { h ^= c[i]; h *= 0x100000001b3ULL; }
+  return h;
+}
+// the cache file name of the reference (cheese.cu:1442-1451): FNV-1a over the candidate names, n, K, the symmetry
+// group and the window tables, so either program finds a table the other wrote
+std::string dist_table_path(const HostSpec &hs, const SymGroup &grp, int K, const std::string &dir) {
+  uint64_t h = 0xcbf29ce484222325ULL;
+  for (const auto &nm : hs.names) h = fnv_bytes(h, nm.c_str(), nm.size() + 1);
+  h = fnv_bytes(h, &hs.n, sizeof hs.n);
+  h = fnv_bytes(h, &K, sizeof K);
+  h = fnv_bytes(h, grp.bperm.data(), grp.bperm.size());
+  h = fnv_bytes(h, grp.conj.data(), grp.conj.size());
+  h = fnv_bytes(h, hs.bad2.data(), hs.bad2.size());
+  h = fnv_bytes(h, hs.bad3.data(), hs.bad3.size() * 4);
+  char buf[96];
+  std::snprintf(buf, sizeof buf, "table-n%d-k%d-%016llx.bin", hs.n, K, (unsigned long long)h);
+  return dir.empty() ? std::string() : dir + "/" + buf;
+}
+constexpr uint32_t DT_MAGIC = 0x54445a43u;   // "CZDT": the file's keys use this build's class hash
+constexpr uint32_t DT_KEY_VERSION = 1;
+
+// exact check on the host: the circuit's gates, applied to the target (residual times each gate's inverse), give
+// the goal (the identity, exponent 0)
+bool host_circuit_ok(const HostSpec &hs, const std::vector<int> &c) {
+  const int n = hs.n, N = 1 << n;
+  std::vector<Zw> S(hs.target.begin(), hs.target.end()), T(N * N);
+  int k = hs.tk;
+  for (int g : c) {
+    const int nq = hs.gnq[g], L = 1 << nq;
+    int mask = 0;
+    for (int j = 0; j < nq; j++) mask |= 1 << hs.gq[g][j];
+    for (int r = 0; r < N; r++)
+      for (int col = 0; col < N; col++) {
+        const int base = col & ~mask;
+        int lc = 0;
+        for (int j = 0; j < nq; j++) lc |= ((col >> hs.gq[g][j]) & 1) << j;
+        Zw v{0, 0, 0, 0};
+        for (int m2 = 0; m2 < L; m2++) {
+          int x = base;
+          for (int j = 0; j < nq; j++) x |= ((m2 >> j) & 1) << hs.gq[g][j];
+          v = zadd(v, zmul(S[r * N + x], hs.ginv[g][m2 * L + lc]));
+        }
+        T[r * N + col] = v;
+      }
+    S.swap(T);
+    k += hs.gik[g];
+    while (k > 0) {
+      bool ok = true;
+      for (const Zw &z : S) ok = ok && zdiv2ok(z);
+      if (!ok) break;
+      for (Zw &z : S) z = zdown(z);
+      k--;
+    }
+  }
+  if (k != 0) return false;
+  for (int r = 0; r < N; r++)
+    for (int col = 0; col < N; col++) {
+      const Zw z = S[r * N + col];
+      if (r == col ? !(z.a == 1 && !z.b && !z.c && !z.d) : !zzero(z)) return false;
+    }
+  return true;
+}
+}  // namespace
+
+bool Engine::Impl::table_load(const std::string &path, DistTable &D, int K) {
+  FILE *f = path.empty() ? nullptr : std::fopen(path.c_str(), "rb");
+  if (!f) return false;
+  int nl = 0;
+  bool ok = std::fread(&nl, sizeof nl, 1, f) == 1 && nl >= 0 && nl <= K;
+  std::vector<std::vector<uint32_t>> P;
+  std::vector<std::vector<uint8_t>> G;
+  for (int l = 1; ok && l <= nl; l++) {
+    long n = 0;
+    ok = std::fread(&n, sizeof n, 1, f) == 1 && n > 0;
+    if (!ok) break;
+    P.emplace_back(n); G.emplace_back(n);
+    ok = std::fread(P.back().data(), 4, n, f) == (size_t)n && std::fread(G.back().data(), 1, n, f) == (size_t)n;
+  }
+  long ns = 0;
+  std::vector<uint64_t> k1, k2;
+  std::vector<uint32_t> ki, kl;
+  bool trusted = false;
+  if (ok && std::fread(&ns, sizeof ns, 1, f) == 1 && ns > 0) {
+    k1.resize(ns); k2.resize(ns); ki.resize(ns); kl.resize(ns);
+    bool kok = true;
+    for (long i = 0; kok && i < ns; i++)
+      kok = std::fread(&k1[i], 8, 1, f) == 1 && std::fread(&k2[i], 8, 1, f) == 1 && std::fread(&ki[i], 4, 1, f) == 1 &&
+            std::fread(&kl[i], 4, 1, f) == 1;
+    uint32_t trailer[2] = {0, 0};
+    trusted = kok && std::fread(trailer, 4, 2, f) == 2 && trailer[0] == DT_MAGIC && trailer[1] == DT_KEY_VERSION;
+  } else {
+    ok = false;
+  }
+  std::fclose(f);
+  if (!ok) return false;
+  D.K = K; D.nl = nl;
+  D.par.assign(nl + 1, DBuf{}); D.gat.assign(nl + 1, DBuf{}); D.n.assign(nl + 1, 0);
+  D.n[0] = 1;
+  for (int l = 1; l <= nl; l++) {
+    const long long n = (long long)P[l - 1].size();
+    D.n[l] = n;
+    D.par[l].ensure(n * 4 + 4); D.gat[l].ensure(n + 4);
+    ck(cudaMemcpyAsync(D.par[l].p, P[l - 1].data(), n * 4, cudaMemcpyHostToDevice, s), "h2d");
+    ck(cudaMemcpyAsync(D.gat[l].p, G[l - 1].data(), n, cudaMemcpyHostToDevice, s), "h2d");
+  }
+  if (trusted) {
+    D.S1.ensure(ns * 8); D.S2.ensure(ns * 8); D.Sidx.ensure(ns * 4); D.Slvl.ensure(ns * 4);
+    ck(cudaMemcpyAsync(D.S1.p, k1.data(), ns * 8, cudaMemcpyHostToDevice, s), "h2d");
+    ck(cudaMemcpyAsync(D.S2.p, k2.data(), ns * 8, cudaMemcpyHostToDevice, s), "h2d");
+    ck(cudaMemcpyAsync(D.Sidx.p, ki.data(), ns * 4, cudaMemcpyHostToDevice, s), "h2d");
+    ck(cudaMemcpyAsync(D.Slvl.p, kl.data(), ns * 4, cudaMemcpyHostToDevice, s), "h2d");
+    D.ns = ns;
+  }
+  ck(cudaStreamSynchronize(s), "table load");
+  return true;   // untrusted keys: the caller recomputes them (D.ns == 0)
+}
+
+void Engine::Impl::table_save(const std::string &path, const DistTable &D) {
+  if (path.empty()) return;
+  FILE *f = std::fopen(path.c_str(), "wb");
+  if (!f) { std::fprintf(stderr, "cannot write %s (table not cached)\n", path.c_str()); return; }
+  const int nl = D.nl;
+  std::fwrite(&nl, sizeof nl, 1, f);
+  for (int l = 1; l <= nl; l++) {
+    const long n = (long)D.n[l];
+    std::vector<uint32_t> P(n);
+    std::vector<uint8_t> G(n);
+    cudaMemcpy(P.data(), D.par[l].p, n * 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(G.data(), D.gat[l].p, n, cudaMemcpyDeviceToHost);
+    std::fwrite(&n, sizeof n, 1, f); std::fwrite(P.data(), 4, n, f); std::fwrite(G.data(), 1, n, f);
+  }
+  const long ns = (long)D.ns;
+  std::vector<uint64_t> a1(ns), a2(ns);
+  std::vector<uint32_t> ai(ns), al(ns);
+  cudaMemcpy(a1.data(), D.S1.p, ns * 8, cudaMemcpyDeviceToHost);
+  cudaMemcpy(a2.data(), D.S2.p, ns * 8, cudaMemcpyDeviceToHost);
+  cudaMemcpy(ai.data(), D.Sidx.p, ns * 4, cudaMemcpyDeviceToHost);
+  cudaMemcpy(al.data(), D.Slvl.p, ns * 4, cudaMemcpyDeviceToHost);
+  std::fwrite(&ns, sizeof ns, 1, f);
+  for (long i = 0; i < ns; i++) {   // the reference's key record layout {h1, h2, idx, lvl}; the keys are this build's
+    std::fwrite(&a1[i], 8, 1, f); std::fwrite(&a2[i], 8, 1, f); std::fwrite(&ai[i], 4, 1, f); std::fwrite(&al[i], 4, 1, f);
+  }
+  const uint32_t trailer[2] = {DT_MAGIC, DT_KEY_VERSION};   // past the reference's layout: its reader stops before
+  std::fwrite(trailer, 4, 2, f);
+  std::fclose(f);
+}
+
+// the table of (spec tables, symmetry group, K): resident, else the cache file, else built from the identity by the
+// level search without bounds, each level filtered against the classes of the lower ones (cheese.cu:1495-1517)
+template <int NQ>
+Engine::Impl::DistTable *Engine::Impl::get_table(const HostSpec &hs, const SymGroup &grp, int K, const Options &opt,
+                                                 const std::function<void(const LevelStats &)> &cb,
+                                                 SearchResult &res) {
+  constexpr int N = 1 << NQ, E = N * N;
+  const std::string path = dist_table_path(hs, grp, K, opt.cache_dir);
+  const std::string key = path.empty() ? dist_table_path(hs, grp, K, ".") : path;
+  res.table_path = path;
+  auto it = dtabs.find(key);
+  if (it != dtabs.end()) return it->second;
+  const double t0 = now_s();
+  HostSpec hI = hs;                                   // the identity as target, no bounds, never "found"
+  hI.target.assign(E, Zw{0, 0, 0, 0});
+  for (int i = 0; i < N; i++) hI.target[i * N + i] = Zw{1, 0, 0, 0};
+  hI.tk = 0; hI.standard = 0; hI.lite = 0; hI.uid = hs.uid ^ 0x7461626c65ULL;
+  const DevSpec sp = prepare<NQ>(hI, grp, K + 1, true);
+  DistTable *D = new DistTable;
+  if (table_load(path, *D, K)) {
+    res.table_loaded = true;
+    if (!D->ns) {                                     // another program's keys: recompute them with this build's hash
+      fK1.ensure(16); fK2.ensure(16);
+      fR.ensure(E * sizeof(Z4<int32_t>)); fMeta.ensure(sizeof(NodeMeta));
+      std::vector<Z4<int32_t>> id(E, Z4<int32_t>{0, 0, 0, 0});
+      for (int i = 0; i < N; i++) id[i * N + i] = Z4<int32_t>{1, 0, 0, 0};
+      ck(cudaMemcpyAsync(fR.p, id.data(), E * sizeof(Z4<int32_t>), cudaMemcpyHostToDevice, s), "h2d");
+      k_root<NQ, int32_t><<<1, 32, 0, s>>>(sp, fR.as<Z4<int32_t>>(), fMeta.as<NodeMeta>(), 0);
+      table_levels_keys<NQ>(sp, 1);
+      seen_add(*D, 1, 0);
+      for (int l = 1; l <= D->nl; l++) {
+        const void *const *tp = upload_tree(D->par, D->gat, l);
+        const long long n = D->n[l];
+        fK1.ensure(n * 8 + 8); fK2.ensure(n * 8 + 8);
+        const unsigned g = (unsigned)std::max<long long>(1, std::min<long long>((n + RES_WARPS - 1) / RES_WARPS, (long long)nsm * 16));
+        k_replay_keys<NQ, int32_t><<<g, RES_WARPS * 32, 0, s>>>(sp, l, n, (const uint32_t *const *)tp,
+                                                                (const uint8_t *const *)(tp + l + 1),
+                                                                fK1.as<uint64_t>(), fK2.as<uint64_t>());
+        launches++;
+        ck(cudaGetLastError(), "table keys");
+        seen_add(*D, n, l);
+      }
+    }
+  } else {
+    D->release();
+    *D = DistTable{};
+    D->K = K;
+    fR.ensure(E * sizeof(Z4<int32_t>)); fMeta.ensure(sizeof(NodeMeta));
+    std::vector<Z4<int32_t>> id(E, Z4<int32_t>{0, 0, 0, 0});
+    for (int i = 0; i < N; i++) id[i * N + i] = Z4<int32_t>{1, 0, 0, 0};
+    ck(cudaMemcpyAsync(fR.p, id.data(), E * sizeof(Z4<int32_t>), cudaMemcpyHostToDevice, s), "h2d");
+    k_root<NQ, int32_t><<<1, 32, 0, s>>>(sp, fR.as<Z4<int32_t>>(), fMeta.as<NodeMeta>(), 0);
+    launches++;
+    table_levels_keys<NQ>(sp, 1);
+    seen_add(*D, 1, 0);
+    front_m = 1;
+    level_n.assign(1, 1);
+    building = D;
+    Options o = opt;
+    o.dedupe = true;
+    o.nogoal = true;
+    int t = 1;
+    const int rc = levels<NQ, int32_t>(hI, sp, o, K + 1, t, cb, res, K);
+    building = nullptr;
+    if (rc == -2) { delete D; throw std::overflow_error("coefficient overflow (int32) in the distance table"); }
+    D->nl = t - 1;                                    // levels that added classes
+    D->par.assign(D->nl + 1, DBuf{}); D->gat.assign(D->nl + 1, DBuf{}); D->n.assign(D->nl + 1, 1);
+    for (int l = 1; l <= D->nl; l++) {                // the tree levels move into the table
+      std::swap(D->par[l], par[l]);
+      std::swap(D->gat[l], gat[l]);
+      D->n[l] = level_n[l];
+    }
+    res.table_built = true;
+    table_save(path, *D);
+  }
+  res.table_seconds = now_s() - t0;
+  dtabs[key] = D;
+  return D;
+}
+
+// the search with a distance table (cheese.cu:1804-1838): levels 1 .. D - K, and after each level (and for the
+// target itself) every node whose class is in the table within the remaining budget is a circuit candidate,
+// confirmed exactly; past level D - K every residual outside the table needs more than K gates
+template <int NQ>
+int Engine::Impl::run_table(const HostSpec &hs, const Options &opt, const std::function<void(const LevelStats &)> &cb,
+                            SearchResult &res) {
+  constexpr int N = 1 << NQ, E = N * N;
+  const int depth = opt.depth >= 0 ? opt.depth : hs.depth;
+  const int K = opt.table_k;
+  const SymGroup grp = sym_group(hs, opt.sym);
+  res.nsym = grp.nsym;
+  res.table_k = K;
+  {
+    bool done = hs.tk == 0;
+    for (int r = 0; r < N && done; r++)
+      for (int c = 0; c < N && done; c++) {
+        const Zw x = hs.target[r * N + c];
+        done = r == c ? (x.a == 1 && !x.b && !x.c && !x.d) : zzero(x);
+      }
+    if (done) { res.depth0 = true; return RC_CIRCUIT; }
+  }
+  for (const Zw &z : hs.target)
+    if (!fits32(z.a) || !fits32(z.b) || !fits32(z.c) || !fits32(z.d)) {
+      res.error = "target coefficients exceed int32";
+      return RC_OVERFLOW;
+    }
+  DistTable *D;
+  try {
+    D = get_table<NQ>(hs, grp, K, opt, cb, res);
+  } catch (const std::overflow_error &e) {
+    res.error = e.what();
+    return RC_OVERFLOW;
+  }
+  res.table_classes = D->ns;
+  res.table_levels = D->nl;
+  const DevSpec sp = prepare<NQ>(hs, grp, depth, false);
+  {
+    std::vector<Z4<int32_t>> t32(E);
+    for (int i = 0; i < E; i++) t32[i] = {(int32_t)hs.target[i].a, (int32_t)hs.target[i].b, (int32_t)hs.target[i].c, (int32_t)hs.target[i].d};
+    fR.ensure(E * sizeof(Z4<int32_t>)); fMeta.ensure(sizeof(NodeMeta));
+    ck(cudaMemcpyAsync(fR.p, t32.data(), E * sizeof(Z4<int32_t>), cudaMemcpyHostToDevice, s), "h2d");
+    k_root<NQ, int32_t><<<1, 32, 0, s>>>(sp, fR.as<Z4<int32_t>>(), fMeta.as<NodeMeta>(), hs.tk);
+    launches++;
+    table_levels_keys<NQ>(sp, 1);
+    ck(cudaStreamSynchronize(s), "root");
+  }
+  front_m = 1;
+  level_n.assign(1, 1);
+  const std::vector<int> inv = inverse_gates(hs);
+  want_keys = true;
+  int t_next = 1;
+  for (int t = 0; t <= depth - K || t == 0; t++) {
+    if (t > 0) {
+      const int rc = levels<NQ, int32_t>(hs, sp, opt, depth, t_next, cb, res, t);
+      if (rc == -2) { want_keys = false; res.error = "coefficient overflow (int32) in table mode"; return RC_OVERFLOW; }
+      if (rc != RC_STOP) { want_keys = false; return rc; }
+    }
+    // candidates: nodes of level t whose class is in the table within depth - t gates, cheapest first
+    const long long n = front_m;
+    const int maxc = depth - t;
+    tmp.ensure(n * 8 + 8);
+    k_table_lookup<<<(unsigned)std::max<long long>(1, std::min<long long>((n + 255) / 256, (long long)nsm * 16)), 256, 0, s>>>(
+        fK1.as<uint64_t>(), fK2.as<uint64_t>(), n, D->S1.as<uint64_t>(), D->S2.as<uint64_t>(), D->Slvl.as<uint32_t>(),
+        D->ns, maxc, tmp.as<long long>());
+    launches++;
+    std::vector<long long> hit(n);
+    ck(cudaMemcpyAsync(hit.data(), tmp.p, n * 8, cudaMemcpyDeviceToHost, s), "d2h");
+    ck(cudaStreamSynchronize(s), "table lookup");
+    std::vector<std::pair<int, long long>> cand;
+    for (long long j = 0; j < n; j++)
+      if (hit[j] >= 0) {
+        uint32_t lv = 0;
+        ck(cudaMemcpy(&lv, D->Slvl.as<uint32_t>() + hit[j], 4, cudaMemcpyDeviceToHost), "d2h");
+        cand.push_back({(int)lv, j});
+      }
+    std::sort(cand.begin(), cand.end());
+    const void *const *tp = upload_tree(D->par, D->gat, D->nl);
+    DBuf outb;
+    outb.ensure(64 * sizeof(int2) + 16);
+    for (const auto &cd : cand) {
+      const long long j = cd.second;
+      NodeMeta mj;
+      ck(cudaMemcpy(&mj, fMeta.as<NodeMeta>() + j, sizeof mj, cudaMemcpyDeviceToHost), "d2h");
+      k_table_confirm<NQ, int32_t><<<1, 32, 0, s>>>(sp, fR.as<Z4<int32_t>>() + j * E, mj.k, D->S1.as<uint64_t>(),
+                                                    D->S2.as<uint64_t>(), D->Sidx.as<uint32_t>(), D->Slvl.as<uint32_t>(),
+                                                    D->ns, hit[j], maxc, (const uint32_t *const *)tp,
+                                                    (const uint8_t *const *)(tp + D->nl + 1), outb.as<int2>(), 64,
+                                                    (int *)(outb.as<int2>() + 64));
+      launches++;
+      int nout = 0;
+      std::vector<int2> pairs(64);
+      ck(cudaMemcpyAsync(&nout, outb.as<int2>() + 64, 4, cudaMemcpyDeviceToHost, s), "d2h");
+      ck(cudaMemcpyAsync(pairs.data(), outb.p, 64 * sizeof(int2), cudaMemcpyDeviceToHost, s), "d2h");
+      ck(cudaStreamSynchronize(s), "table confirm");
+      if (!nout) continue;
+      std::vector<int> pre(t);                        // the node's prefix
+      {
+        uint32_t i = (uint32_t)j;
+        for (int l = t; l >= 1; l--) {
+          uint8_t gg; uint32_t pp;
+          ck(cudaMemcpy(&gg, gat[l].as<uint8_t>() + i, 1, cudaMemcpyDeviceToHost), "d2h");
+          ck(cudaMemcpy(&pp, par[l].as<uint32_t>() + i, 4, cudaMemcpyDeviceToHost), "d2h");
+          pre[l - 1] = gg; i = pp;
+        }
+      }
+      for (int q = 0; q < nout; q++) {
+        const int x = pairs[q].x, sy = pairs[q].y;
+        uint32_t lv = 0, ix = 0;
+        ck(cudaMemcpy(&lv, D->Slvl.as<uint32_t>() + x, 4, cudaMemcpyDeviceToHost), "d2h");
+        ck(cudaMemcpy(&ix, D->Sidx.as<uint32_t>() + x, 4, cudaMemcpyDeviceToHost), "d2h");
+        std::vector<int> w(lv);                       // the table sequence, from the identity
+        uint32_t i = ix;
+        for (int l = (int)lv; l >= 1; l--) {
+          uint8_t gg; uint32_t pp;
+          ck(cudaMemcpy(&gg, D->gat[l].as<uint8_t>() + i, 1, cudaMemcpyDeviceToHost), "d2h");
+          ck(cudaMemcpy(&pp, D->par[l].as<uint32_t>() + i, 4, cudaMemcpyDeviceToHost), "d2h");
+          w[l - 1] = gg; i = pp;
+        }
+        std::vector<int> full = pre;                  // the suffix: w reversed, inverted, relabelled by the symmetry
+        bool okmap = true;
+        for (int a = (int)w.size() - 1; a >= 0; a--) {
+          const int gi = inv[w[a]];
+          if (gi < 0) { okmap = false; break; }
+          full.push_back(grp.gmap[sy][gi]);
+        }
+        if (okmap && host_circuit_ok(hs, full)) {
+          want_keys = false;
+          res.circuit = full;
+          res.n_found = 1;
+          res.table_split[0] = t;
+          res.table_split[1] = (int)full.size() - t;
+          return RC_CIRCUIT;
+        }
+      }
+    }
+  }
+  want_keys = false;
+  res.table_proof = true;
+  return RC_PROOF;
 }
 
 // host part of the device spec: every field, plus the gate-matrix (gi) and goal (gl) tables to place on the device
@@ -1886,11 +2556,20 @@ int Engine::search(const HostSpec &hs, const Options &opt, const std::function<v
   int rc;
   try {
     ck(cudaSetDevice(dev_), "cudaSetDevice");
-    switch (hs.n) {
-      case 1: rc = impl_->run<1>(hs, opt, cb, res); break;
-      case 2: rc = impl_->run<2>(hs, opt, cb, res); break;
-      case 3: rc = impl_->run<3>(hs, opt, cb, res); break;
-      default: res.error = "n = " + std::to_string(hs.n) + " not built"; rc = RC_USAGE;
+    if (opt.table_k > 0 && !hs.states) {
+      switch (hs.n) {
+        case 1: rc = impl_->run_table<1>(hs, opt, cb, res); break;
+        case 2: rc = impl_->run_table<2>(hs, opt, cb, res); break;
+        case 3: rc = impl_->run_table<3>(hs, opt, cb, res); break;
+        default: res.error = "n = " + std::to_string(hs.n) + " not built"; rc = RC_USAGE;
+      }
+    } else {
+      switch (hs.n) {
+        case 1: rc = impl_->run<1>(hs, opt, cb, res); break;
+        case 2: rc = impl_->run<2>(hs, opt, cb, res); break;
+        case 3: rc = impl_->run<3>(hs, opt, cb, res); break;
+        default: res.error = "n = " + std::to_string(hs.n) + " not built"; rc = RC_USAGE;
+      }
     }
   } catch (const CudaError &e) {
     res.error = e.what();

@@ -34,6 +34,8 @@ constexpr int TC_T = 256;        // threads per CTA
 constexpr int MAXP = 64;         // 4^n, n <= 3
 constexpr int MAXT = 32;         // deepest peel sequence
 constexpr unsigned FULLM = 0xffffffffu;
+constexpr uint32_t TC_CACHE_MAGIC = 0x43545a43u;   // "CZTC": the table file's keys use this build's coset hash
+constexpr uint32_t TC_KEY_VERSION = 1;
 
 struct TDev {
   int n, P, lp, G;               // lp = log2 P
@@ -631,10 +633,41 @@ bool TcountContext::load(const std::string &path, const TDev &si, Table &tab, in
     P.emplace_back(n); G.emplace_back(n);
     ok = std::fread(P.back().data(), 4, n, f) == (size_t)n && std::fread(G.back().data(), 1, n, f) == (size_t)n;
   }
+  // keys: trusted only when the file ends with this build's trailer (same key hash); else recomputed below
+  long ns = 0;
+  std::vector<uint64_t> k1, k2;
+  std::vector<uint32_t> ki, kl;
+  bool trusted = false;
+  if (ok && std::fread(&ns, sizeof ns, 1, f) == 1 && ns > 0) {
+    k1.resize(ns); k2.resize(ns); ki.resize(ns); kl.resize(ns);
+    bool kok = true;
+    for (long i = 0; kok && i < ns; i++)
+      kok = std::fread(&k1[i], 8, 1, f) == 1 && std::fread(&k2[i], 8, 1, f) == 1 && std::fread(&ki[i], 4, 1, f) == 1 &&
+            std::fread(&kl[i], 4, 1, f) == 1;
+    uint32_t trailer[2] = {0, 0};
+    trusted = kok && std::fread(trailer, 4, 2, f) == 2 && trailer[0] == TC_CACHE_MAGIC && trailer[1] == TC_KEY_VERSION;
+  }
   std::fclose(f);
   if (!ok) return false;
-  // the file's keys were made by whichever program wrote it: recompute every node's key with this build's hash
   Tree &D = tab.D;
+  if (trusted) {
+    for (int l = 1; l <= nl; l++) {
+      const long long n = (long long)P[l - 1].size();
+      D.par.emplace_back(); D.gat.emplace_back(); D.n.push_back(n);
+      D.par.back().ensure(n * 4 + 4); D.gat.back().ensure(n + 4);
+      tck(cudaMemcpyAsync(D.par.back().p, P[l - 1].data(), n * 4, cudaMemcpyHostToDevice, s), "h2d");
+      tck(cudaMemcpyAsync(D.gat.back().p, G[l - 1].data(), n, cudaMemcpyHostToDevice, s), "h2d");
+    }
+    tab.S1.ensure(ns * 8); tab.S2.ensure(ns * 8); tab.Sidx.ensure(ns * 4); tab.Slvl.ensure(ns * 4);
+    tck(cudaMemcpyAsync(tab.S1.p, k1.data(), ns * 8, cudaMemcpyHostToDevice, s), "h2d");
+    tck(cudaMemcpyAsync(tab.S2.p, k2.data(), ns * 8, cudaMemcpyHostToDevice, s), "h2d");
+    tck(cudaMemcpyAsync(tab.Sidx.p, ki.data(), ns * 4, cudaMemcpyHostToDevice, s), "h2d");
+    tck(cudaMemcpyAsync(tab.Slvl.p, kl.data(), ns * 4, cudaMemcpyHostToDevice, s), "h2d");
+    tck(cudaStreamSynchronize(s), "h2d");
+    tab.ns = ns;
+    return true;
+  }
+  // keys made by another program (a reference-written file): recompute every node's key with this build's hash
   for (int l = 1; l <= nl; l++) {
     const long long n = (long long)P[l - 1].size();
     D.par.emplace_back(); D.gat.emplace_back(); D.n.push_back(n);
@@ -693,6 +726,8 @@ void TcountContext::save(const std::string &path, const Table &tab) {
   for (long i = 0; i < ns; i++) {
     std::fwrite(&a1[i], 8, 1, f); std::fwrite(&a2[i], 8, 1, f); std::fwrite(&ai[i], 4, 1, f); std::fwrite(&al[i], 4, 1, f);
   }
+  const uint32_t trailer[2] = {TC_CACHE_MAGIC, TC_KEY_VERSION};   // past the reference's layout: its reader stops before
+  std::fwrite(trailer, 4, 2, f);
   std::fclose(f);
 }
 

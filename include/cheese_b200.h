@@ -52,6 +52,8 @@ typedef struct {
   int sym;          /* 1; 0: --no-sym */
   int store64;      /* 0: int32 limbs promoted to int64 on demand; 1: int64 limbs throughout */
   int profile;      /* 1: record device times per phase (cz_result.expand_ms / dedupe_ms) */
+  int table_k;      /* --table K: 0 none; K > 0 the distance table of the last K gates (cheese.cu:1431-1593) */
+  const char *cache_dir;   /* distance-table cache directory ("build" by default; NULL: no cache) */
 } cz_options;
 void cz_options_default(cz_options *opt);
 
@@ -61,6 +63,7 @@ typedef struct {
   int64_t parents, prefixes, cut_w3, cut_lb, survivors, distinct;
   int proved_unsat;
   double seconds;
+  int table;        /* 1: a level of the distance-table build (the "dir": "table" lines) */
 } cz_level_stats;
 typedef void (*cz_level_fn)(void *user, const cz_level_stats *level);
 
@@ -82,11 +85,21 @@ typedef struct {
   int64_t expand_launches;     /* launches of the level kernel */
   int64_t h2d_bytes, d2h_bytes;/* host<->device bytes moved by the call */
   int64_t children_full;       /* children whose residual was computed (the rest were decided from the parent) */
+  /* --table K */
+  int table_k;                 /* 0: not a table run */
+  int table_split[2];          /* rc 0 through the table: [search levels, table gates] (the "table" field) */
+  int table_proof;             /* rc 1 through the table: {"depth": D, "proved_unsat": true, "table": K} */
+  int64_t table_classes;       /* classes in the table */
+  int table_levels;
+  int table_loaded, table_built;
+  double table_seconds;
+  char table_path[256];
   char error[256];
 } cz_result;
 
-/* The plain search of `cheese SPEC [flags]` without --mitm / --table (replaces run<NQ> + levels<NQ>,
- * src/cheese.cu:1249-1377, 1762-1849). Calls on_level after every completed level (may be NULL). */
+/* The search of `cheese SPEC [flags]` without --mitm (replaces run<NQ> + levels<NQ>, src/cheese.cu:1249-1377,
+ * 1762-1849, and with opt->table_k the distance-table mode, :1431-1593, 1804-1838). Calls on_level after every
+ * completed level, table-build levels included (may be NULL). */
 int cz_search(cz_engine *engine, const cz_spec *spec, const cz_options *opt, cz_level_fn on_level, void *user,
               cz_result *out);
 

@@ -10,6 +10,9 @@ Writes
   cheese_b200/data/base-n{2,3}.spec     the default Clifford+T spec per qubit count (its target is replaced per job)
   tests/golden/cases.json               per case: spec, flags, exit code and the reference's stdout with every
                                         "seconds" value replaced by 0.00 (machine dependent, never compared)
+  tests/golden/table_cases.json         the same for --table K runs, each in a fresh working directory (so the
+                                        reference builds its distance table and prints the "dir": "table" lines),
+                                        plus the reference's stderr table line
 The reference is used only here, to produce data; nothing at test time reads the reference tree.
 """
 import argparse
@@ -41,10 +44,57 @@ SLOW = [("grover_3-10", "grover_3", 10, []), ("toffoli-11", "toffoli", 11, []), 
         ("toffoli-11-nosym", "toffoli", 11, ["--no-sym"])]
 
 
+# --table K cases (reference cheese.cu:1804-1838): proofs through the table, proofs by a level, and circuits found
+# in the table; (case name, target stem, budget, K, extra flags)
+TABLE_CASES = [
+    ("toffoli-7-table3", "toffoli", 7, 3, []), ("toffoli-9-table4", "toffoli", 9, 4, []),
+    ("toffoli-10-table5", "toffoli", 10, 5, []), ("ccz-8-table4", "ccz", 8, 4, []),
+    ("ccz-7-table3", "ccz", 7, 3, []), ("toffoli-9-table4-nosym", "toffoli", 9, 4, ["--no-sym"]),
+    ("cs-5-table3", "cs", 5, 3, []), ("qft_2-7-table3", "qft_2", 7, 3, []),
+]
+
+
+def table_cases(binp, write_spec):
+    """--table K golden cases: named targets plus seeded random ones (found circuits), each run in its own empty
+    working directory so that the reference builds (and prints) its distance table"""
+    import tempfile
+    from cheese_b200 import workloads
+    out = []
+
+    def run(case, spec, flags):
+        with tempfile.TemporaryDirectory() as cwd:
+            t0 = time.time()
+            p = subprocess.run([str(binp), str(GOLD / "specs" / f"{spec}.spec")] + flags, capture_output=True,
+                               text=True, cwd=cwd)
+        lines = [SECONDS.sub('"seconds": 0.00', l) for l in p.stdout.splitlines()]
+        tab = [l for l in p.stderr.splitlines() if l.startswith("table")]
+        print(f"{case}: rc {p.returncode}, {len(lines)} lines, {time.time() - t0:.1f} s", file=sys.stderr)
+        return {"name": case, "spec": spec, "flags": flags, "rc": p.returncode, "stdout": lines,
+                "stderr_table": re.sub(r"\(([0-9.]+) s\)", "(0.0 s)", tab[0]) if tab else ""}
+
+    for name, stem, d, k, flags in TABLE_CASES:
+        out.append(run(name, stem, ["--depth", str(d), "--table", str(k)] + flags))
+    rng = random.Random(77)
+    for i in range(8):
+        n, circ = workloads.random_circuit(rng, n=3 if i < 6 else 2, L=rng.randint(6, 9))
+        name = f"table-rand-{i}"
+        write_spec(name, n, circ, len(circ))
+        k = 3 if i % 2 == 0 else 4
+        out.append(run(f"{name}-table{k}", name, ["--table", str(k)]))
+        out[-1]["circuit"] = [[g, list(qs)] for g, qs in circ]
+    # budgets below the table depth: only the target's own class is looked up
+    for name, stem, d, k in [("table-rand-4-depth2-table3", "table-rand-4", 2, 3),
+                             ("table-rand-4-depth3-table4", "table-rand-4", 3, 4)]:
+        out.append(run(name, stem, ["--depth", str(d), "--table", str(k)]))
+    (GOLD / "table_cases.json").write_text(json.dumps(out, indent=1) + "\n")
+    print(f"{len(out)} table cases written", file=sys.stderr)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--quick", action="store_true", help="skip the cases that take more than a few seconds")
+    ap.add_argument("--table-only", action="store_true", help="write only the --table K cases")
     o = ap.parse_args()
     sys.dont_write_bytecode = True
     sys.path.insert(0, str(Path(o.ref) / "python"))
@@ -70,6 +120,9 @@ def main():
         print(f"{case}: rc {p.returncode}, {len(out)} lines, {time.time() - t0:.1f} s", file=sys.stderr)
         return {"name": case, "spec": spec, "flags": flags, "rc": p.returncode, "stdout": out}
 
+    if o.table_only:
+        table_cases(binp, write_spec)
+        return
     # target specs written by the reference generator (budget line = the first budget used)
     qdir = Path(o.ref) / "tests" / "qasm"
     cases = []
@@ -112,6 +165,7 @@ def main():
 
     (GOLD / "cases.json").write_text(json.dumps(cases, indent=1) + "\n")
     print(f"{len(cases)} cases written", file=sys.stderr)
+    table_cases(binp, write_spec)
 
 
 if __name__ == "__main__":
