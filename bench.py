@@ -207,6 +207,56 @@ def systems(eng, args):
                            "clifford_elements": ct["elements"], "coset_table_s": r0["table_seconds"],
                            "coset_table_cosets": r0["table_cosets"], "queries": nq, "queries_s": nq / t_q,
                            "ms_per_query": 1e3 * t_q / nq, "verified": ver}
+    # distance table (--table 8, 17.9M classes): the optimum of Toffoli (15 gates, budgets 1..14 proved) and the
+    # Fredkin proofs of budgets 15 and 16, through the library (table built once, resident) and as the reference's
+    # run.sh does it (one drop-in process per budget, the table cached on disk by the first)
+    import tempfile
+    from cheese_b200 import verify
+    eng.trim()                                # the batched and headline buffers go back to the device
+    eng_t = cz.Engine()
+    tsp = {nm: (SPECS / f"{nm}.spec").read_text() for nm in ("toffoli", "fredkin")}
+    t0 = time.perf_counter()
+    r = eng_t.search(tsp["toffoli"], depth=1, table_k=8, cache_dir=None)
+    t_build = time.perf_counter() - t0
+    classes = r.table["table_classes"]
+    budgets = {}
+    t0 = time.perf_counter()
+    for d in range(1, 16):
+        a = time.perf_counter()
+        r = eng_t.search(tsp["toffoli"], depth=d, table_k=8, cache_dir=None)
+        budgets[d] = (r.rc, time.perf_counter() - a)
+        if r.rc == 0:
+            break
+    t_loop = time.perf_counter() - t0
+    opt_ok = r.rc == 0 and len(r.circuit) == 15 and verify.equivalent(tsp["toffoli"], r.circuit)
+    fred = {}
+    for d in (15, 16):
+        a = time.perf_counter()
+        rf = eng_t.search(tsp["fredkin"], depth=d, table_k=8, cache_dir=None)
+        fred[str(d)] = {"rc": rf.rc, "s": time.perf_counter() - a, "error": rf.error}
+    del eng_t
+    tmp = Path(tempfile.mkdtemp())
+    (tmp / "build").mkdir()
+    t0 = time.perf_counter()
+    cli = {}
+    for d in range(1, 16):
+        a = time.perf_counter()
+        p = subprocess.run([str(cz.BIN_DIR / "cheese"), str(SPECS / "toffoli.spec"), "--depth", str(d), "--table", "8"],
+                           cwd=tmp, capture_output=True, text=True, timeout=600)
+        cli[str(d)] = {"rc": p.returncode, "s": time.perf_counter() - a}
+        if p.returncode != 1:
+            break
+    t_cli = time.perf_counter() - t0
+    out["table_gatecount"] = {
+        "workload": "--table 8, 3 qubits, 27 Clifford+T candidates: Toffoli budgets 1..15 (optimum 15), Fredkin "
+                    "budgets 15 and 16 (proofs)",
+        "table_classes": classes, "table_build_s": t_build,
+        "toffoli_optimum_s": t_loop, "toffoli_budget14_s": budgets.get(14, (None, None))[1],
+        "toffoli_budget15_s": budgets.get(15, (None, None))[1], "toffoli_optimum_verified": bool(opt_ok),
+        "fredkin": fred,
+        "toffoli_optimum_cli_s": t_cli, "cli_budgets": cli,
+        "reference_published": "RTX 3060 Ti: K=8 table 17.9M classes in 30 s; Toffoli optimum 27 s (budget 14 1.5 s, "
+                               "15 11.1 s); Fredkin budget 15 11.3 s, 16 91 s (docs/PLAN.md:87-95)"}
     # serving: seeded Poisson streams of the mixed workload, against the same requests run one by one
     N = args.serve_requests
     reqs = tcwork.serve_requests(eng, 5, N)
@@ -221,8 +271,6 @@ def systems(eng, args):
     t_seq = time.perf_counter() - t0
     # the same requests through the drop-in binaries, one process per request (how the reference's scripts run
     # them), on a subset: the T-count table cache is written once beforehand and loaded by every process
-    import subprocess
-    import tempfile
     tmp = Path(tempfile.mkdtemp())
     (tmp / "build").mkdir()
     exes = [cz.BIN_DIR / "cheese", cz.BIN_DIR / "tcount", cz.BIN_DIR / "cliffopt"]

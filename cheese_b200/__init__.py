@@ -108,6 +108,7 @@ SIGNATURES = {
     "cz_spec_is_states": (C.c_int, [C.c_void_p]),
     "cz_engine_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
     "cz_engine_destroy": (None, [C.c_void_p]),
+    "cz_engine_trim": (C.c_int64, [C.c_void_p]),
     "cz_options_default": (None, [C.POINTER(Options)]),
     "cz_search": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Options), LEVEL_FN, C.c_void_p, C.POINTER(Result)]),
     "cz_search_text": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(Options), LEVEL_FN, C.c_void_p,
@@ -230,6 +231,11 @@ class Engine:
     def __del__(self):
         if getattr(self, "_h", None):
             self.close()
+
+    def trim(self):
+        """release the cached device work buffers (kept at peak size between calls otherwise); resident tables stay.
+        Returns the bytes released."""
+        return lib().cz_engine_trim(self._h)
 
     @property
     def stream(self):

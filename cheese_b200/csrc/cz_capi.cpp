@@ -70,6 +70,11 @@ int cz_engine_create(int device, cz_engine **out, char *err, size_t errlen) {
   }
 }
 
+int64_t cz_engine_trim(cz_engine *engine) {
+  if (!engine) return 0;
+  return (int64_t)engine->e->trim();
+}
+
 void cz_engine_destroy(cz_engine *engine) {
   if (!engine) return;
   if (engine->tc) cz::tcount_context_destroy(engine->tc);

@@ -82,6 +82,9 @@ class Engine {
   // register-resident IMAD loop timed with CUDA events
   double int32_peak();
   int device() const { return dev_; }
+  // release the cached work buffers (frontiers, survivor records, sort scratch, tree); resident distance tables and
+  // spec tables stay; returns the bytes released
+  size_t trim();
 
  private:
   struct Impl;

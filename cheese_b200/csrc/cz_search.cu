@@ -1270,6 +1270,27 @@ __global__ void k_keys_gather(const uint32_t *order, size_t n, const uint64_t *a
     s1[i] = a1[o]; s2[i] = a2[o]; si[i] = ai[o]; sl[i] = al[o];
   }
 }
+// one key record of a table file, as the reference lays it out: {h1, h2, idx, lvl}, 24 bytes
+struct KeyRec { uint64_t h1, h2; uint32_t idx, lvl; };
+static_assert(sizeof(KeyRec) == 24, "key record layout");
+__global__ void k_keys_pack(const uint64_t *s1, const uint64_t *s2, const uint32_t *si, const uint32_t *sl, long long n,
+                            KeyRec *r) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    r[i] = KeyRec{s1[i], s2[i], si[i], sl[i]};
+}
+__global__ void k_keys_unpack(const KeyRec *r, long long n, uint64_t *s1, uint64_t *s2, uint32_t *si, uint32_t *sl) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const KeyRec x = r[i];
+    s1[i] = x.h1; s2[i] = x.h2; si[i] = x.idx; sl[i] = x.lvl;
+  }
+}
+// the (index, level) columns of the keys of one new table level: 0..n-1 and lvl
+__global__ void k_level_ids(uint32_t *idx, uint32_t *lv, long long n, uint32_t lvl) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    idx[i] = (uint32_t)i;
+    lv[i] = lvl;
+  }
+}
 // the class key of every node of a frontier (one warp each)
 template <int NQ, typename ST>
 __global__ void __launch_bounds__(RES_WARPS * 32) k_node_keys(const __grid_constant__ DevSpec sp, const Z4<ST> *R,
@@ -1565,6 +1586,18 @@ struct Engine::Impl {
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     stats.ensure(sizeof(DevStats));
   }
+  size_t trim() {
+    size_t n = 0;
+    for (DBuf *b : {&fR, &fMeta, &fR2, &fMeta2, &sH1, &sH2, &sIdx, &sMeta, &tq, &k0, &k1, &v0, &v1, &hist, &part,
+                    &work, &tmp, &kidx, &kslot, &fK1, &fK2, &keys2, &old}) {
+      n += b->cap;
+      b->release();
+    }
+    for (auto &b : par) { n += b.cap; b.release(); }
+    for (auto &b : gat) { n += b.cap; b.release(); }
+    front_m = 0;
+    return n;
+  }
   ~Impl() {
     cudaSetDevice(dev);
     for (DBuf *b : {&fR, &fMeta, &fR2, &fMeta2, &sH1, &sH2, &sIdx, &sMeta, &tq, &k0, &k1, &v0, &v1, &hist, &part,
@@ -1829,11 +1862,9 @@ void Engine::Impl::seen_add(DistTable &D, long long n, int lvl) {
   ck(cudaMemcpyAsync(a1.as<uint64_t>() + D.ns, fK1.p, n * 8, cudaMemcpyDeviceToDevice, s), "d2d");
   ck(cudaMemcpyAsync(a2.as<uint64_t>() + D.ns, fK2.p, n * 8, cudaMemcpyDeviceToDevice, s), "d2d");
   {
-    std::vector<uint32_t> idx(n), lv(n, (uint32_t)lvl);
-    for (long long i = 0; i < n; i++) idx[i] = (uint32_t)i;
-    ck(cudaMemcpyAsync(ai.as<uint32_t>() + D.ns, idx.data(), n * 4, cudaMemcpyHostToDevice, s), "h2d");
-    ck(cudaMemcpyAsync(al.as<uint32_t>() + D.ns, lv.data(), n * 4, cudaMemcpyHostToDevice, s), "h2d");
-    ck(cudaStreamSynchronize(s), "h2d");
+    const unsigned gi = (unsigned)std::max<long long>(1, std::min<long long>((n + 255) / 256, (long long)nsm * 16));
+    k_level_ids<<<gi, 256, 0, s>>>(ai.as<uint32_t>() + D.ns, al.as<uint32_t>() + D.ns, n, (uint32_t)lvl);
+    launches++;
   }
   k0.ensure(tot * 8); k1.ensure(tot * 8); v0.ensure(tot * 4); v1.ensure(tot * 4);
   hist.ensure(sort_hist_words(tot) * 4); part.ensure(scan_partials_words(sort_hist_words(tot)) * 4);
@@ -1936,17 +1967,18 @@ bool Engine::Impl::table_load(const std::string &path, DistTable &D, int K) {
     ok = std::fread(P.back().data(), 4, n, f) == (size_t)n && std::fread(G.back().data(), 1, n, f) == (size_t)n;
   }
   long ns = 0;
-  std::vector<uint64_t> k1, k2;
-  std::vector<uint32_t> ki, kl;
+  std::vector<KeyRec> keys;
   bool trusted = false;
   if (ok && std::fread(&ns, sizeof ns, 1, f) == 1 && ns > 0) {
-    k1.resize(ns); k2.resize(ns); ki.resize(ns); kl.resize(ns);
-    bool kok = true;
-    for (long i = 0; kok && i < ns; i++)
-      kok = std::fread(&k1[i], 8, 1, f) == 1 && std::fread(&k2[i], 8, 1, f) == 1 && std::fread(&ki[i], 4, 1, f) == 1 &&
-            std::fread(&kl[i], 4, 1, f) == 1;
+    // the keys are read only when the file ends with this library's trailer (the same class hash)
     uint32_t trailer[2] = {0, 0};
-    trusted = kok && std::fread(trailer, 4, 2, f) == 2 && trailer[0] == DT_MAGIC && trailer[1] == DT_KEY_VERSION;
+    const long pos = std::ftell(f);
+    trusted = pos >= 0 && std::fseek(f, pos + ns * (long)sizeof(KeyRec), SEEK_SET) == 0 &&
+              std::fread(trailer, 4, 2, f) == 2 && trailer[0] == DT_MAGIC && trailer[1] == DT_KEY_VERSION;
+    if (trusted) {
+      keys.resize(ns);
+      trusted = std::fseek(f, pos, SEEK_SET) == 0 && std::fread(keys.data(), sizeof(KeyRec), ns, f) == (size_t)ns;
+    }
   } else {
     ok = false;
   }
@@ -1964,10 +1996,12 @@ bool Engine::Impl::table_load(const std::string &path, DistTable &D, int K) {
   }
   if (trusted) {
     D.S1.ensure(ns * 8); D.S2.ensure(ns * 8); D.Sidx.ensure(ns * 4); D.Slvl.ensure(ns * 4);
-    ck(cudaMemcpyAsync(D.S1.p, k1.data(), ns * 8, cudaMemcpyHostToDevice, s), "h2d");
-    ck(cudaMemcpyAsync(D.S2.p, k2.data(), ns * 8, cudaMemcpyHostToDevice, s), "h2d");
-    ck(cudaMemcpyAsync(D.Sidx.p, ki.data(), ns * 4, cudaMemcpyHostToDevice, s), "h2d");
-    ck(cudaMemcpyAsync(D.Slvl.p, kl.data(), ns * 4, cudaMemcpyHostToDevice, s), "h2d");
+    tmp.ensure(ns * sizeof(KeyRec));
+    ck(cudaMemcpyAsync(tmp.p, keys.data(), ns * sizeof(KeyRec), cudaMemcpyHostToDevice, s), "h2d");
+    const unsigned gb = (unsigned)std::max<long>(1, std::min<long>((ns + 255) / 256, (long)nsm * 16));
+    k_keys_unpack<<<gb, 256, 0, s>>>(tmp.as<KeyRec>(), ns, D.S1.as<uint64_t>(), D.S2.as<uint64_t>(),
+                                     D.Sidx.as<uint32_t>(), D.Slvl.as<uint32_t>());
+    launches++;
     D.ns = ns;
   }
   ck(cudaStreamSynchronize(s), "table load");
@@ -1989,16 +2023,19 @@ void Engine::Impl::table_save(const std::string &path, const DistTable &D) {
     std::fwrite(&n, sizeof n, 1, f); std::fwrite(P.data(), 4, n, f); std::fwrite(G.data(), 1, n, f);
   }
   const long ns = (long)D.ns;
-  std::vector<uint64_t> a1(ns), a2(ns);
-  std::vector<uint32_t> ai(ns), al(ns);
-  cudaMemcpy(a1.data(), D.S1.p, ns * 8, cudaMemcpyDeviceToHost);
-  cudaMemcpy(a2.data(), D.S2.p, ns * 8, cudaMemcpyDeviceToHost);
-  cudaMemcpy(ai.data(), D.Sidx.p, ns * 4, cudaMemcpyDeviceToHost);
-  cudaMemcpy(al.data(), D.Slvl.p, ns * 4, cudaMemcpyDeviceToHost);
-  std::fwrite(&ns, sizeof ns, 1, f);
-  for (long i = 0; i < ns; i++) {   // the reference's key record layout {h1, h2, idx, lvl}; the keys are this build's
-    std::fwrite(&a1[i], 8, 1, f); std::fwrite(&a2[i], 8, 1, f); std::fwrite(&ai[i], 4, 1, f); std::fwrite(&al[i], 4, 1, f);
+  std::vector<KeyRec> keys(ns);     // the reference's key record layout; the keys are this library's class hash
+  {
+    DBuf rec;
+    rec.ensure(ns * sizeof(KeyRec) + 16);
+    const unsigned gb = (unsigned)std::max<long>(1, std::min<long>((ns + 255) / 256, (long)nsm * 16));
+    k_keys_pack<<<gb, 256, 0, s>>>(D.S1.as<uint64_t>(), D.S2.as<uint64_t>(), D.Sidx.as<uint32_t>(),
+                                   D.Slvl.as<uint32_t>(), ns, rec.as<KeyRec>());
+    ck(cudaMemcpyAsync(keys.data(), rec.p, ns * sizeof(KeyRec), cudaMemcpyDeviceToHost, s), "d2h");
+    ck(cudaStreamSynchronize(s), "table keys");
+    rec.release();
   }
+  std::fwrite(&ns, sizeof ns, 1, f);
+  std::fwrite(keys.data(), sizeof(KeyRec), ns, f);
   const uint32_t trailer[2] = {DT_MAGIC, DT_KEY_VERSION};   // past the reference's layout: its reader stops before
   std::fwrite(trailer, 4, 2, f);
   std::fclose(f);
@@ -2526,6 +2563,11 @@ int eval_bounds_noalloc(const HostSpec &hs, int count, const int64_t *d_entries,
 
 Engine::Engine(int device) : impl_(new Impl(device)), dev_(device) {}
 Engine::~Engine() { delete impl_; }
+size_t Engine::trim() {
+  cudaSetDevice(dev_);
+  cudaStreamSynchronize(impl_->s);
+  return impl_->trim();
+}
 void *Engine::stream() const { return impl_->s; }
 
 double Engine::int32_peak() {

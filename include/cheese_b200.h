@@ -44,6 +44,10 @@ int cz_spec_is_states(const cz_spec *spec);
 /* Search engine on CUDA device `device` (replaces the device setup of run<NQ>, src/cheese.cu:1762-1792). */
 int cz_engine_create(int device, cz_engine **out, char *err, size_t errlen);
 void cz_engine_destroy(cz_engine *engine);
+/* Release the engine's cached device work buffers (frontiers, survivor records, sort scratch, search tree), which it
+ * otherwise keeps at their peak size for the next call; resident distance tables stay. Returns the bytes released.
+ * No reference counterpart: the reference's processes run one search each and free everything at exit. */
+int64_t cz_engine_trim(cz_engine *engine);
 
 /* flags of the reference CLI (src/cheese.cu:1859-1868) */
 typedef struct {

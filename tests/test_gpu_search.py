@@ -113,3 +113,13 @@ def test_drop_in_binary(tmp_path):
     assert p.returncode == 3 and "depth > 48" in p.stderr
     p = subprocess.run([str(exe), str(spec_path("cs-states"))], capture_output=True, text=True)
     assert p.returncode == 3 and "state targets" in p.stderr
+
+
+def test_trim_releases_and_search_repeats(engine):
+    """trim() frees the cached work buffers; the next search allocates again and answers the same"""
+    c = GOLD["toffoli-10"]
+    a = engine.search(spec_text(c["spec"]), depth=10)
+    assert engine.trim() > 0
+    assert engine.trim() == 0
+    b = engine.search(spec_text(c["spec"]), depth=10)
+    assert (a.rc, a.lines()) == (b.rc, b.lines()) == (c["rc"], c["stdout"])
