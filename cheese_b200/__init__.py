@@ -21,12 +21,12 @@ CIRCUIT, PROOF, ERR_SPEC, ERR_USAGE, ERR_OVERFLOW, ERR_CUDA = 0, 1, 2, 3, 4, 5
 class LevelStats(C.Structure):
     _fields_ = [("t", C.c_int), ("parents", C.c_int64), ("prefixes", C.c_int64), ("cut_w3", C.c_int64),
                 ("cut_lb", C.c_int64), ("survivors", C.c_int64), ("distinct", C.c_int64),
-                ("proved_unsat", C.c_int), ("seconds", C.c_double), ("table", C.c_int)]
+                ("proved_unsat", C.c_int), ("seconds", C.c_double), ("dir", C.c_int)]
 
 
 class Options(C.Structure):
     _fields_ = [("depth", C.c_int), ("dedupe", C.c_int), ("sym", C.c_int), ("store64", C.c_int),
-                ("profile", C.c_int), ("table_k", C.c_int), ("cache_dir", C.c_char_p)]
+                ("profile", C.c_int), ("table_k", C.c_int), ("cache_dir", C.c_char_p), ("mitm", C.c_int)]
 
 
 class Result(C.Structure):
@@ -38,7 +38,10 @@ class Result(C.Structure):
                 ("d2h_bytes", C.c_int64), ("children_full", C.c_int64), ("table_k", C.c_int),
                 ("table_split", C.c_int * 2), ("table_proof", C.c_int), ("table_classes", C.c_int64),
                 ("table_levels", C.c_int), ("table_loaded", C.c_int), ("table_built", C.c_int),
-                ("table_seconds", C.c_double), ("table_path", C.c_char * 256), ("error", C.c_char * 256)]
+                ("table_seconds", C.c_double), ("table_path", C.c_char * 256), ("mitm_join", C.c_int),
+                ("mitm_forward", C.c_int64), ("mitm_backward", C.c_int64), ("mitm_hash_matches", C.c_int64),
+                ("mitm_seconds", C.c_double), ("mitm_split", C.c_int * 2), ("mitm_found", C.c_int),
+                ("mitm_proof", C.c_int), ("error", C.c_char * 256)]
 
 
 LEVEL_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(LevelStats))
@@ -358,13 +361,13 @@ class Engine:
         return rc, out, buf.value.decode().splitlines(), list(steps)
 
     def search(self, spec, depth=-1, dedupe=True, sym=True, store64=False, profile=False, on_level=None,
-               table_k=0, cache_dir="build"):
-        """run `cheese SPEC [--depth D] [--no-dedupe] [--no-sym] [--table K]`; returns a SearchOutcome
+               table_k=0, cache_dir="build", mitm=False):
+        """run `cheese SPEC [--depth D] [--no-dedupe] [--no-sym] [--table K] [--mitm]`; returns a SearchOutcome
         (cache_dir: where the distance table of --table K is cached, None for no cache)"""
         if not isinstance(spec, Spec):
             spec = Spec(spec)
         opt = Options(depth, int(dedupe), int(sym), int(store64), int(profile), int(table_k),
-                      cache_dir.encode() if cache_dir else None)
+                      cache_dir.encode() if cache_dir else None, int(mitm))
         levels = []
 
         def cb(_user, p):
@@ -396,7 +399,7 @@ class Batch:
     def submit(self, spec, depth=-1, dedupe=True, sym=True, store64=False):
         if not isinstance(spec, Spec):
             spec = Spec(spec)
-        opt = Options(depth, int(dedupe), int(sym), int(store64), 0, 0, None)
+        opt = Options(depth, int(dedupe), int(sym), int(store64), 0, 0, None, 0)
         jid = lib().cz_batch_submit(self._h, spec._h, C.byref(opt))
         if jid < 0:
             raise RuntimeError(f"cz_batch_submit failed: {-jid}")
@@ -528,6 +531,9 @@ class SearchOutcome:
         self.table = {k: getattr(res, k) for k in ("table_k", "table_proof", "table_classes", "table_levels",
                                                    "table_loaded", "table_built", "table_seconds")}
         self.table["table_path"] = res.table_path.decode()
+        self.mitm = {k: getattr(res, k) for k in ("mitm_join", "mitm_forward", "mitm_backward", "mitm_hash_matches",
+                                                  "mitm_seconds", "mitm_found", "mitm_proof")}
+        self.mitm["mitm_split"] = (res.mitm_split[0], res.mitm_split[1])
 
     def lines(self, seconds=False, depth=None):
         """stdout of the reference binary for this search (seconds as 0.00 unless asked for; depth: the --depth
@@ -535,20 +541,27 @@ class SearchOutcome:
         out = []
         for s in self.levels:
             sec = f"{s['seconds']:.2f}" if seconds else "0.00"
-            pre = '"dir": "table", ' if s.get("table") else ""
+            pre = {1: '"dir": "table", ', 2: '"dir": "fwd", ', 3: '"dir": "bwd", '}.get(s.get("dir", 0), "")
             out.append(f'{{{pre}"t": {s["t"]}, "parents": {s["parents"]}, "prefixes": {s["prefixes"]}, '
                        f'"cut_w3": {s["cut_w3"]}, "cut_lb": {s["cut_lb"]}, "survivors": {s["survivors"]}, '
                        f'"distinct": {s["distinct"]}, "proved_unsat": {"true" if s["distinct"] == 0 else "false"}, '
                        f'"seconds": {sec}}}')
+        m = self.mitm
+        if m["mitm_join"]:
+            sec = f"{m['mitm_seconds']:.2f}" if seconds else "0.00"
+            out.append(f'{{"dir": "join", "forward": {m["mitm_forward"]}, "backward": {m["mitm_backward"]}, '
+                       f'"hash_matches": {m["mitm_hash_matches"]}, "seconds": {sec}}}')
         if self.rc == CIRCUIT:
             if self.depth0:
                 out.append('{"found": 0, "circuit": []}')
             else:
                 names = ", ".join(f'"{c}"' for c in self.circuit)
-                tab = (f', "table": [{self.table_split[0]}, {self.table_split[1]}]'
-                       if sum(self.table_split) > 0 else "")
+                tab = (f', "mitm": [{m["mitm_split"][0]}, {m["mitm_split"][1]}]' if m["mitm_found"] else
+                       f', "table": [{self.table_split[0]}, {self.table_split[1]}]' if sum(self.table_split) > 0 else "")
                 out.append(f'{{"t": {len(self.circuit)}, "found": {self.n_found or 1}, "circuit": [{names}]{tab}, '
                            f'"seconds": 0.00}}')
+        elif self.rc == PROOF and m["mitm_proof"]:
+            out.append(f'{{"depth": {depth}, "proved_unsat": true, "mitm": [{m["mitm_split"][0]}, {m["mitm_split"][1]}]}}')
         elif self.rc == PROOF and self.table["table_proof"]:
             out.append(f'{{"depth": {depth}, "proved_unsat": true, "table": {self.table["table_k"]}}}')
         return out

@@ -16,7 +16,8 @@ static double now() { return std::chrono::duration<double>(std::chrono::steady_c
 static void print_level(void *, const cz_level_stats *s) {
   std::printf("{%s\"t\": %d, \"parents\": %lld, \"prefixes\": %lld, \"cut_w3\": %lld, \"cut_lb\": %lld, \"survivors\": %lld, "
               "\"distinct\": %lld, \"proved_unsat\": %s, \"seconds\": %.2f}\n",
-              s->table ? "\"dir\": \"table\", " : "", s->t, (long long)s->parents, (long long)s->prefixes, (long long)s->cut_w3, (long long)s->cut_lb,
+              s->dir == 1 ? "\"dir\": \"table\", " : s->dir == 2 ? "\"dir\": \"fwd\", " : s->dir == 3 ? "\"dir\": \"bwd\", " : "",
+              s->t, (long long)s->parents, (long long)s->prefixes, (long long)s->cut_w3, (long long)s->cut_lb,
               (long long)s->survivors, (long long)s->distinct, s->distinct ? "false" : "true", s->seconds);
   std::fflush(stdout);
 }
@@ -56,11 +57,8 @@ int main(int argc, char **argv) {
     return 3;
   }
   if (prc == CZ_ERR_USAGE || !spec) { std::fprintf(stderr, "n = %d not built (NQ_MIN..NQ_MAX)\n", n); return 3; }
-  if (mitm) {
-    std::fprintf(stderr, "--mitm: not available in this build\n");
-    return 3;
-  }
   opt.depth = depth;
+  opt.mitm = mitm;
   opt.table_k = tablek > 0 ? tablek : 0;
   opt.profile = profile;
   cz_engine *eng = nullptr;
@@ -76,16 +74,25 @@ int main(int argc, char **argv) {
     std::fprintf(stderr, "table: %lld classes within %d gates (%.1f s), cached in %s\n", (long long)res.table_classes,
                  res.table_levels, res.table_seconds, res.table_path);
   int code = rc;
+  if (res.mitm_join)
+    std::printf("{\"dir\": \"join\", \"forward\": %lld, \"backward\": %lld, \"hash_matches\": %lld, \"seconds\": %.2f}\n",
+                (long long)res.mitm_forward, (long long)res.mitm_backward, (long long)res.mitm_hash_matches,
+                res.mitm_seconds);
   if (rc == CZ_CIRCUIT) {
     if (res.depth0) std::printf("{\"found\": 0, \"circuit\": []}\n");
     else {
       std::printf("{\"t\": %d, \"found\": %lld, \"circuit\": [", res.found_len, (long long)(res.n_found ? res.n_found : 1));
       for (int i = 0; i < res.found_len; i++) std::printf("%s\"%s\"", i ? ", " : "", cz_spec_gate_name(spec, res.found[i]));
-      if (res.table_split[0] + res.table_split[1] > 0)
+      if (res.mitm_found)
+        std::printf("], \"mitm\": [%d, %d], \"seconds\": %.2f}\n", res.mitm_split[0], res.mitm_split[1], now() - t0);
+      else if (res.table_split[0] + res.table_split[1] > 0)
         std::printf("], \"table\": [%d, %d], \"seconds\": %.2f}\n", res.table_split[0], res.table_split[1], now() - t0);
       else
         std::printf("], \"seconds\": %.2f}\n", now() - t0);
     }
+  } else if (rc == CZ_PROOF && res.mitm_proof) {
+    std::printf("{\"depth\": %d, \"proved_unsat\": true, \"mitm\": [%d, %d]}\n", depth, res.mitm_split[0],
+                res.mitm_split[1]);
   } else if (rc == CZ_PROOF && res.table_proof) {
     std::printf("{\"depth\": %d, \"proved_unsat\": true, \"table\": %d}\n", depth, res.table_k);
   } else if (rc == CZ_ERR_CUDA) {

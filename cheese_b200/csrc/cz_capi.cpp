@@ -86,7 +86,7 @@ void cz_engine_destroy(cz_engine *engine) {
 void cz_options_default(cz_options *opt) {
   if (!opt) return;
   opt->depth = -1; opt->dedupe = 1; opt->sym = 1; opt->store64 = 0; opt->profile = 0; opt->table_k = 0;
-  opt->cache_dir = "build";
+  opt->cache_dir = "build"; opt->mitm = 0;
 }
 
 namespace {
@@ -120,6 +120,15 @@ void fill_result(const cz::SearchResult &r, cz_result *out) {
   out->table_built = r.table_built;
   out->table_seconds = r.table_seconds;
   put_err(out->table_path, sizeof out->table_path, r.table_path);
+  out->mitm_join = r.mitm_join;
+  out->mitm_forward = r.mitm_forward;
+  out->mitm_backward = r.mitm_backward;
+  out->mitm_hash_matches = r.mitm_hash_matches;
+  out->mitm_seconds = r.mitm_seconds;
+  out->mitm_split[0] = r.mitm_split[0];
+  out->mitm_split[1] = r.mitm_split[1];
+  out->mitm_found = r.mitm_found;
+  out->mitm_proof = r.mitm_proof;
   put_err(out->error, sizeof out->error, r.error);
 }
 
@@ -127,7 +136,7 @@ cz_level_stats level_stats(const cz::LevelStats &L) {
   cz_level_stats s;
   s.t = L.t; s.parents = L.parents; s.prefixes = L.prefixes; s.cut_w3 = L.cut_w3; s.cut_lb = L.cut_lb;
   s.survivors = L.survivors; s.distinct = L.distinct; s.proved_unsat = L.proved_unsat; s.seconds = L.seconds;
-  s.table = L.table;
+  s.dir = L.dir;
   return s;
 }
 }  // namespace
@@ -160,6 +169,7 @@ int cz_search(cz_engine *engine, const cz_spec *spec, const cz_options *opt, cz_
   }
   eo.table_k = o.table_k;
   eo.cache_dir = o.cache_dir ? o.cache_dir : "";
+  eo.mitm = o.mitm != 0;
   cz::SearchResult r;
   int rc;
   try {

@@ -18,6 +18,7 @@ struct Options {
   bool nogoal = false;       // never report the goal (distance-table build)
   int table_k = 0;           // --table K
   std::string cache_dir = "build";   // distance-table cache directory ("" : no cache)
+  bool mitm = false;         // --mitm
 };
 
 struct LevelStats {
@@ -25,7 +26,8 @@ struct LevelStats {
   long long parents = 0, prefixes = 0, cut_w3 = 0, cut_lb = 0, survivors = 0, distinct = 0;
   bool proved_unsat = false;
   double seconds = 0;
-  bool table = false;        // a level of the distance-table build
+  int dir = 0;               // 0 a plain level; 1 a level of the distance-table build ("dir": "table"); 2 / 3 a
+                             // forward / backward level of the meet-in-the-middle search ("dir": "fwd" / "bwd")
 };
 
 struct SearchResult {
@@ -50,6 +52,12 @@ struct SearchResult {
   int table_levels = 0;
   double table_seconds = 0;
   std::string table_path;
+  // --mitm
+  bool mitm_join = false;              // the join ran (its "dir": "join" line)
+  long long mitm_forward = 0, mitm_backward = 0, mitm_hash_matches = 0;
+  double mitm_seconds = 0;
+  int mitm_split[2] = {0, 0};          // [forward levels, backward levels] of the found circuit or of the proof
+  bool mitm_found = false, mitm_proof = false;
   std::string error;
 };
 

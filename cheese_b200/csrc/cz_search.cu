@@ -1461,6 +1461,172 @@ __global__ void __launch_bounds__(RES_WARPS * 32) k_replay_keys(const __grid_con
   }
 }
 
+// ---------------- meet in the middle (--mitm) ----------------
+// the flat list of backward nodes over levels 1..top: node j sits at level l with off[l] <= j < off[l + 1]
+struct MitmLevels { long long off[DMAX + 2]; int top; };
+
+// residual of backward node (lvl, idx): S0 (exponent k0) times the inverses of its path's gates, into C; P, path:
+// scratch. Returns its exponent.
+template <int NQ>
+__device__ int warp_replay_from(const DevSpec &sp, const uint32_t *const *tpar, const uint8_t *const *tgat, int lvl,
+                                uint32_t idx, const Z4<int32_t> *S0, int k0, Z4<int32_t> *P, Z4<int32_t> *C,
+                                uint8_t *path, int lane, bool &ovf) {
+  constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
+  if (lane == 0)
+    for (int l = lvl; l >= 1; l--) { path[l - 1] = tgat[l][idx]; idx = tpar[l][idx]; }
+#pragma unroll
+  for (int q = 0; q < EPL; q++) {
+    const int e = lane + 32 * q;
+    if (e < E) C[e] = S0[e];
+  }
+  __syncwarp();
+  int k = k0;
+  ovf = false;
+  for (int i = 0; i < lvl; i++) {
+#pragma unroll
+    for (int q = 0; q < EPL; q++) {
+      const int e = lane + 32 * q;
+      if (e < E) P[e] = C[e];
+    }
+    __syncwarp();
+    bool o;
+    k = warp_child<NQ, int32_t>(P, C, path[i], k, sp, &sp, lane, o);
+    ovf = ovf || o;
+    __syncwarp();
+  }
+  (void)N;
+  return k;
+}
+
+// K = U R (exponents add), normalised; int64 accumulation, ovf when a limb of K leaves int32
+template <int NQ>
+__device__ int warp_mul_left(const Z4<int32_t> *U, int ku, const Z4<int32_t> *R, int kr, Z4<int32_t> *K, int lane,
+                             bool &ovf) {
+  constexpr int N = 1 << NQ, E = N * N;
+  Zw v[2] = {Zw{0, 0, 0, 0}, Zw{0, 0, 0, 0}};
+  int ei[2] = {-1, -1};
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    const int e = lane + 32 * j;
+    if (e >= E) continue;
+    ei[j] = e;
+    const int r = e >> NQ, c = e & (N - 1);
+    for (int m = 0; m < N; m++) {
+      const Z4<int32_t> u = U[r * N + m];
+      if (!(u.a | u.b | u.c | u.d)) continue;
+      const Z4<int32_t> x = R[m * N + c];
+      v[j] = zadd(v[j], zmul(Zw{u.a, u.b, u.c, u.d}, Zw{x.a, x.b, x.c, x.d}));
+    }
+  }
+  return finish_child<NQ, int32_t>(v, ei, ku + kr, K, lane, ovf);
+}
+
+// per-block copies of U and U^dag, and per-warp scratch for the backward keys and the confirmation
+template <int NQ> struct MitmSmem {
+  static constexpr int E = (1 << NQ) * (1 << NQ);
+  Z4<int32_t> U[E], Ud[E];
+  Z4<int32_t> P[RES_WARPS][E], C[RES_WARPS][E], K[RES_WARPS][E];
+  uint64_t W1[E], W2[E];
+  uint8_t path[RES_WARPS][64];
+};
+template <int NQ>
+__device__ void mitm_smem_init(MitmSmem<NQ> &sm, const Z4<int32_t> *U, const Z4<int32_t> *Ud) {
+  constexpr int E = MitmSmem<NQ>::E;
+  for (int e = threadIdx.x; e < E; e += blockDim.x) { sm.U[e] = U[e]; sm.Ud[e] = Ud[e]; }
+  init_weights(sm.W1, sm.W2, E);
+  __syncthreads();
+}
+// K of backward node j: U times its residual (rebuilt from U^dag), in sm.K[w]; returns K's exponent
+template <int NQ>
+__device__ int mitm_bwd_residual(const DevSpec &sp, MitmSmem<NQ> &sm, const MitmLevels &lv, const uint32_t *const *tpar,
+                                 const uint8_t *const *tgat, long long j, int ku, int w, int lane, bool &ovf) {
+  int l = 1;
+  while (l < lv.top && j >= lv.off[l + 1]) l++;
+  bool o1, o2;
+  const int kr = warp_replay_from<NQ>(sp, tpar, tgat, l, (uint32_t)(j - lv.off[l]), sm.Ud, ku, sm.P[w], sm.C[w],
+                                      sm.path[w], lane, o1);
+  const int k = warp_mul_left<NQ>(sm.U, ku, sm.C[w], kr, sm.K[w], lane, o2);
+  ovf = o1 || o2;
+  return k;
+}
+
+// keys (h1, h2) of every backward node, hashed like the frontier nodes (no symmetry: the join needs exact residuals)
+template <int NQ>
+__global__ void __launch_bounds__(RES_WARPS * 32) k_mitm_bwd_keys(const __grid_constant__ DevSpec sp,
+                                                                const Z4<int32_t> *U, const Z4<int32_t> *Ud, int ku,
+                                                                const __grid_constant__ MitmLevels lv,
+                                                                const uint32_t *const *tpar, const uint8_t *const *tgat,
+                                                                long long nb, uint64_t *B1, uint64_t *B2, int *ovf) {
+  __shared__ MitmSmem<NQ> sm;
+  mitm_smem_init<NQ>(sm, U, Ud);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (long long j = blockIdx.x * (long long)RES_WARPS + w; j < nb; j += (long long)gridDim.x * RES_WARPS) {
+    bool o;
+    const int k = mitm_bwd_residual<NQ>(sp, sm, lv, tpar, tgat, j, ku, w, lane, o);
+    uint64_t k1, k2;
+    warp_class_key<NQ, int32_t>(sm.K[w], k, 1, 0u, sp.symperm, sm.W1, sm.W2, lane, k1, k2);
+    if (lane == 0) {
+      B1[j] = k1; B2[j] = k2;
+      if (o) atomicExch(ovf, 1);
+    }
+    __syncwarp();
+  }
+}
+
+// forward keys sorted by h1 (stable): gather (h1, h2, forward index) in sorted order
+__global__ void k_mitm_sorted(const uint32_t *order, long long n, const uint64_t *F1, const uint64_t *F2, uint64_t *S1,
+                              uint64_t *S2, uint32_t *Si) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const uint32_t o = order[i];
+    S1[i] = F1[o]; S2[i] = F2[o]; Si[i] = o;
+  }
+}
+// per backward key: the first sorted forward key equal in (h1, h2), or -1; the matching j are listed (any order)
+__global__ void k_mitm_match(const uint64_t *B1, const uint64_t *B2, long long nb, const uint64_t *S1,
+                             const uint64_t *S2, long long nf, long long *pos, long long *hits,
+                             unsigned long long *nhits) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < nb; j += (long long)gridDim.x * blockDim.x) {
+    long long r = -1;
+    for (long long x = keys_lower(S1, nf, B1[j]); x < nf && S1[x] == B1[j]; x++)
+      if (S2[x] == B2[j]) { r = x; break; }
+    pos[j] = r;
+    if (r >= 0) hits[atomicAdd(nhits, 1ULL)] = j;
+  }
+}
+// exact confirmation of hash matches (one warp per candidate j): the first forward node of the equal-key run whose
+// residual equals K = U R'_j exactly (entries and exponent), else -1
+template <int NQ>
+__global__ void __launch_bounds__(RES_WARPS * 32) k_mitm_confirm(
+    const __grid_constant__ DevSpec sp, const Z4<int32_t> *U, const Z4<int32_t> *Ud, int ku,
+    const __grid_constant__ MitmLevels lv, const uint32_t *const *tpar, const uint8_t *const *tgat, const long long *cand,
+    long long nc, const long long *pos, const uint64_t *S1, const uint64_t *S2, const uint32_t *Si, long long nf,
+    const Z4<int32_t> *FR, const NodeMeta *FM, long long *match) {
+  constexpr int E = MitmSmem<NQ>::E, EPL = E >= 32 ? E / 32 : 1;
+  __shared__ MitmSmem<NQ> sm;
+  mitm_smem_init<NQ>(sm, U, Ud);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (long long c = blockIdx.x * (long long)RES_WARPS + w; c < nc; c += (long long)gridDim.x * RES_WARPS) {
+    const long long j = cand[c];
+    bool o;
+    const int k = mitm_bwd_residual<NQ>(sp, sm, lv, tpar, tgat, j, ku, w, lane, o);
+    long long r = -1;
+    const long long x0 = pos[j];
+    for (long long x = x0; x0 >= 0 && x < nf && S1[x] == S1[x0] && r < 0; x++) {
+      if (S2[x] != S2[x0]) continue;
+      const uint32_t f = Si[x];
+      bool eq = FM[f].k == k;
+#pragma unroll
+      for (int q = 0; q < EPL; q++) {
+        const int e = lane + 32 * q;
+        if (e < E && !zq(FR[(size_t)f * E + e], sm.K[w][e])) eq = false;
+      }
+      if (__all_sync(FULL, eq) && !o) r = f;
+    }
+    if (lane == 0) match[c] = r;
+    __syncwarp();
+  }
+}
+
 __global__ void k_widen(const Z4<int32_t> *in, Z4<int64_t> *out, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const Z4<int32_t> x = in[i];
@@ -1577,6 +1743,25 @@ struct Engine::Impl {
   DevStats *hstats = nullptr;              // pinned
   long long launches = 0, expand_launches = 0, h2d = 0, d2h = 0;
   long long front_m = 1;                   // nodes in the current frontier
+  int level_dir = 0;                       // the "dir" of the level lines: 2 forward, 3 backward (--mitm)
+  struct SideTree {                        // --mitm: the backward tree while the forward one is the engine's own
+    std::vector<DBuf> par, gat;
+    DBuf fR, fMeta;
+    long long front_m = 1;
+    std::vector<long long> level_n;
+    size_t release() {
+      size_t n = fR.cap + fMeta.cap;
+      for (auto &b : par) { n += b.cap; b.release(); }
+      for (auto &b : gat) { n += b.cap; b.release(); }
+      fR.release(); fMeta.release();
+      return n;
+    }
+  } side;
+  void swap_side() {                       // make the backward tree the current one, or back
+    std::swap(par, side.par); std::swap(gat, side.gat);
+    std::swap(fR, side.fR); std::swap(fMeta, side.fMeta);
+    std::swap(front_m, side.front_m); std::swap(level_n, side.level_n);
+  }
 
   explicit Impl(int d) : dev(d) {
     ck(cudaSetDevice(dev), "cudaSetDevice");
@@ -1595,6 +1780,7 @@ struct Engine::Impl {
     }
     for (auto &b : par) { n += b.cap; b.release(); }
     for (auto &b : gat) { n += b.cap; b.release(); }
+    n += side.release();
     front_m = 0;
     return n;
   }
@@ -1608,6 +1794,7 @@ struct Engine::Impl {
     for (DBuf *b : {&fK1, &fK2, &tptrs, &keys2, &old}) b->release();
     for (auto &b : par) b.release();
     for (auto &b : gat) b.release();
+    side.release();
     if (hstats) cudaFreeHost(hstats);
     for (auto &e : ev) cudaEventDestroy(e);
     if (s) cudaStreamDestroy(s);
@@ -1627,6 +1814,9 @@ struct Engine::Impl {
   template <int NQ> DistTable *get_table(const HostSpec &hs, const SymGroup &grp, int K, const Options &opt,
                                          const std::function<void(const LevelStats &)> &cb, SearchResult &res);
   template <int NQ> int table_levels_keys(const DevSpec &sp, long long n);   // keys of the frontier into fK1/fK2
+  // --mitm
+  template <int NQ> int run_mitm(const HostSpec &hs, const Options &opt, const std::function<void(const LevelStats &)> &cb,
+                                 SearchResult &res);
   void seen_add(DistTable &D, long long n, int lvl);                         // append fK1/fK2 level to D's keys
   const void *const *upload_tree(const std::vector<DBuf> &p, const std::vector<DBuf> &g, int upto);
   bool table_load(const std::string &path, DistTable &D, int K);
@@ -1813,7 +2003,7 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
     L.distinct = distinct;
     L.proved_unsat = distinct == 0;
     L.seconds = now_s() - t0;
-    L.table = building != nullptr;
+    L.dir = building ? 1 : level_dir;
     res.levels = t;
     cb(L);
     if (!distinct) return RC_PROOF;
@@ -2262,6 +2452,209 @@ int Engine::Impl::run_table(const HostSpec &hs, const Options &opt, const std::f
   return RC_PROOF;
 }
 
+// the meet-in-the-middle search (cheese.cu:1595-1760): the search on U (forward) and on U^dag (backward) grow one
+// level at a time, the side with the smaller frontier first, until their depths add up to D; a circuit found by a
+// side's own levels ends the search (a backward one is reversed and inverted). Then every backward node q
+// (levels 1..b) is joined with the forward frontier at level a: K = U R'_q equals a forward residual exactly iff the
+// forward prefix followed by q^-1 is a circuit. No match is a proof. Symmetry classes are off (exact residuals).
+template <int NQ>
+int Engine::Impl::run_mitm(const HostSpec &hs, const Options &opt, const std::function<void(const LevelStats &)> &cb,
+                           SearchResult &res) {
+  constexpr int N = 1 << NQ, E = N * N;
+  const int depth = opt.depth >= 0 ? opt.depth : hs.depth;
+  const SymGroup grp = sym_group(hs, false);
+  res.nsym = grp.nsym;
+  {
+    bool done = hs.tk == 0;
+    for (int r = 0; r < N && done; r++)
+      for (int c = 0; c < N && done; c++) {
+        const Zw x = hs.target[r * N + c];
+        done = r == c ? (x.a == 1 && !x.b && !x.c && !x.d) : zzero(x);
+      }
+    if (done) { res.depth0 = true; return RC_CIRCUIT; }
+  }
+  const std::vector<int> inv = inverse_gates(hs);
+  for (int g = 0; g < hs.G; g++)
+    if (inv[g] < 0) { res.error = "--mitm: no inverse candidate for " + hs.names[g]; return RC_USAGE; }
+  for (const Zw &z : hs.target)
+    if (!fits32(z.a) || !fits32(z.b) || !fits32(z.c) || !fits32(z.d)) {
+      res.error = "--mitm: target coefficients exceed int32";
+      return RC_OVERFLOW;
+    }
+  const DevSpec sp = prepare<NQ>(hs, grp, depth, false);
+  std::vector<Z4<int32_t>> hU(E), hUd(E);
+  for (int r = 0; r < N; r++)
+    for (int c = 0; c < N; c++) {
+      const Zw x = hs.target[r * N + c];
+      hU[r * N + c] = {(int32_t)x.a, (int32_t)x.b, (int32_t)x.c, (int32_t)x.d};
+      const Zw t = hs.target[c * N + r];                // U^dag (conjugate transpose), same sqrt2 exponent
+      const Zw y{t.a, -t.d, -t.c, -t.b};
+      hUd[r * N + c] = {(int32_t)y.a, (int32_t)y.b, (int32_t)y.c, (int32_t)y.d};
+    }
+  DBuf dU;
+  dU.ensure(2 * E * sizeof(Z4<int32_t>));
+  ck(cudaMemcpyAsync(dU.p, hU.data(), E * sizeof(Z4<int32_t>), cudaMemcpyHostToDevice, s), "h2d");
+  ck(cudaMemcpyAsync(dU.as<Z4<int32_t>>() + E, hUd.data(), E * sizeof(Z4<int32_t>), cudaMemcpyHostToDevice, s), "h2d");
+  h2d += 2 * E * sizeof(Z4<int32_t>);
+  const Z4<int32_t> *U = dU.as<Z4<int32_t>>(), *Ud = U + E;
+  auto root = [&](const Z4<int32_t> *M) {              // the current tree restarts at M
+    fR.ensure(E * sizeof(Z4<int32_t>)); fMeta.ensure(sizeof(NodeMeta));
+    ck(cudaMemcpyAsync(fR.p, M, E * sizeof(Z4<int32_t>), cudaMemcpyDeviceToDevice, s), "d2d");
+    k_root<NQ, int32_t><<<1, 32, 0, s>>>(sp, fR.as<Z4<int32_t>>(), fMeta.as<NodeMeta>(), hs.tk);
+    launches++;
+    ck(cudaGetLastError(), "root kernel");
+    front_m = 1;
+    level_n.assign(1, 1);
+  };
+  root(U);
+  swap_side();
+  root(Ud);
+  swap_side();
+  ck(cudaStreamSynchronize(s), "roots");
+  int a = 0, b = 0;
+  long long nF = 1, nB = 1;
+  bool bdead = false;
+  auto done = [&]() { level_dir = 0; dU.release(); };
+  while (a + b < depth) {
+    const bool fwd = bdead || nF <= nB;
+    if (!fwd) swap_side();
+    level_dir = fwd ? 2 : 3;
+    int t = (fwd ? a : b) + 1;
+    const int stop = t;
+    res.circuit.clear();
+    res.n_found = 0;
+    const int rc = levels<NQ, int32_t>(hs, sp, opt, depth, t, cb, res, stop);
+    if (fwd) { a = t - 1; nF = front_m; } else { b = t - 1; nB = front_m; }
+    if (!fwd) swap_side();
+    if (rc == RC_CIRCUIT) {
+      if (!fwd) {                                       // a circuit q for U^dag: U = q^-1
+        std::vector<int> c;
+        for (int i = (int)res.circuit.size() - 1; i >= 0; i--) c.push_back(inv[res.circuit[i]]);
+        res.circuit = c;
+      }
+      done();
+      return RC_CIRCUIT;
+    }
+    if (rc == -2) { done(); res.error = "--mitm: coefficients exceed int32"; return RC_OVERFLOW; }
+    if (rc == RC_PROOF) {
+      if (fwd) { done(); return RC_PROOF; }
+      bdead = true;                                     // no suffix is longer than b: the join below is complete
+      break;
+    }
+    if (rc != RC_STOP) { done(); return rc; }
+  }
+  level_dir = 0;
+  res.mitm_split[0] = a;
+  res.mitm_split[1] = b;
+  const long long nf = level_n.size() > (size_t)a ? level_n[a] : 0;
+  MitmLevels lv;
+  std::memset(&lv, 0, sizeof lv);
+  lv.top = b;
+  long long nb = 0;
+  for (int l = 1; l <= b; l++) { lv.off[l] = nb; nb += side.level_n[l]; }
+  lv.off[b + 1] = nb;
+  if (!nb || !nf) { res.mitm_proof = true; done(); return RC_PROOF; }
+  const double tj = now_s();
+  // forward keys, sorted by h1 (stable), with their frontier index
+  table_levels_keys<NQ>(sp, nf);
+  DBuf S1, S2, Si, B1, B2, pos, hits, flags;
+  k0.ensure(nf * 8); k1.ensure(nf * 8); v0.ensure(nf * 4); v1.ensure(nf * 4);
+  hist.ensure(sort_hist_words(nf) * 4); part.ensure(scan_partials_words(sort_hist_words(nf)) * 4);
+  SortScratch sc{hist.as<uint32_t>(), part.as<uint32_t>(), hist.cap / 4, part.cap / 4};
+  const unsigned gf = (unsigned)std::max<long long>(1, std::min<long long>((nf + 255) / 256, (long long)nsm * 16));
+  k_sort_init<<<gf, 256, 0, s>>>(fK1.as<uint64_t>(), nf, k0.as<uint64_t>(), v0.as<uint32_t>());
+  const bool fl = radix_sort(k0.as<uint64_t>(), v0.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(), nf, 0, 64, sc,
+                             s, nullptr);
+  launches += 1 + 8 * 5;
+  S1.ensure(nf * 8); S2.ensure(nf * 8); Si.ensure(nf * 4);
+  k_mitm_sorted<<<gf, 256, 0, s>>>(fl ? v1.as<uint32_t>() : v0.as<uint32_t>(), nf, fK1.as<uint64_t>(),
+                                   fK2.as<uint64_t>(), S1.as<uint64_t>(), S2.as<uint64_t>(), Si.as<uint32_t>());
+  launches++;
+  // backward keys: every backward node rebuilt from U^dag, multiplied by U, hashed
+  const void *const *tp = upload_tree(side.par, side.gat, b);
+  B1.ensure(nb * 8); B2.ensure(nb * 8); flags.ensure(16);
+  ck(cudaMemsetAsync(flags.p, 0, 16, s), "memset");
+  const unsigned gw = (unsigned)std::max<long long>(1, std::min<long long>((nb + RES_WARPS - 1) / RES_WARPS, (long long)nsm * 16));
+  k_mitm_bwd_keys<NQ><<<gw, RES_WARPS * 32, 0, s>>>(sp, U, Ud, hs.tk, lv, (const uint32_t *const *)tp,
+                                                    (const uint8_t *const *)(tp + b + 1), nb, B1.as<uint64_t>(),
+                                                    B2.as<uint64_t>(), flags.as<int>());
+  launches++;
+  ck(cudaGetLastError(), "mitm keys");
+  pos.ensure(nb * 8); hits.ensure(nb * 8);
+  unsigned long long *nh_d = (unsigned long long *)(flags.as<int>() + 2);
+  const unsigned gb = (unsigned)std::max<long long>(1, std::min<long long>((nb + 255) / 256, (long long)nsm * 16));
+  k_mitm_match<<<gb, 256, 0, s>>>(B1.as<uint64_t>(), B2.as<uint64_t>(), nb, S1.as<uint64_t>(), S2.as<uint64_t>(), nf,
+                                  pos.as<long long>(), hits.as<long long>(), nh_d);
+  launches++;
+  int hflags[4] = {0, 0, 0, 0};
+  ck(cudaMemcpyAsync(hflags, flags.p, 16, cudaMemcpyDeviceToHost, s), "d2h");
+  ck(cudaStreamSynchronize(s), "mitm join");
+  d2h += 16;
+  if (hflags[0]) {
+    S1.release(); S2.release(); Si.release(); B1.release(); B2.release(); pos.release(); hits.release(); flags.release();
+    done();
+    res.error = "--mitm: coefficients exceed int32";
+    return RC_OVERFLOW;
+  }
+  unsigned long long nh = 0;
+  std::memcpy(&nh, hflags + 2, 8);
+  res.mitm_join = true;
+  res.mitm_forward = nf;
+  res.mitm_backward = nb;
+  res.mitm_hash_matches = (long long)nh;
+  res.mitm_seconds = now_s() - tj;
+  int rc = RC_PROOF;
+  if (nh) {                                             // exact confirmation, candidates in backward order
+    std::vector<long long> cand(nh), match(nh);
+    ck(cudaMemcpyAsync(cand.data(), hits.p, nh * 8, cudaMemcpyDeviceToHost, s), "d2h");
+    ck(cudaStreamSynchronize(s), "d2h");
+    std::sort(cand.begin(), cand.end());
+    ck(cudaMemcpyAsync(hits.p, cand.data(), nh * 8, cudaMemcpyHostToDevice, s), "h2d");
+    DBuf mb;
+    mb.ensure(nh * 8);
+    const unsigned gc = (unsigned)std::max<unsigned long long>(1, std::min<unsigned long long>((nh + RES_WARPS - 1) / RES_WARPS, (unsigned long long)nsm * 16));
+    k_mitm_confirm<NQ><<<gc, RES_WARPS * 32, 0, s>>>(sp, U, Ud, hs.tk, lv, (const uint32_t *const *)tp,
+                                                     (const uint8_t *const *)(tp + b + 1), hits.as<long long>(),
+                                                     (long long)nh, pos.as<long long>(), S1.as<uint64_t>(),
+                                                     S2.as<uint64_t>(), Si.as<uint32_t>(), nf, fR.as<Z4<int32_t>>(),
+                                                     fMeta.as<NodeMeta>(), mb.as<long long>());
+    launches++;
+    ck(cudaGetLastError(), "mitm confirm");
+    ck(cudaMemcpyAsync(match.data(), mb.p, nh * 8, cudaMemcpyDeviceToHost, s), "d2h");
+    ck(cudaStreamSynchronize(s), "mitm confirm");
+    mb.release();
+    auto path = [&](const std::vector<DBuf> &P, const std::vector<DBuf> &G, int l, uint32_t i) {
+      std::vector<int> q(l);
+      for (; l >= 1; l--) {
+        uint8_t gg; uint32_t pp;
+        ck(cudaMemcpy(&gg, G[l].as<uint8_t>() + i, 1, cudaMemcpyDeviceToHost), "d2h");
+        ck(cudaMemcpy(&pp, P[l].as<uint32_t>() + i, 4, cudaMemcpyDeviceToHost), "d2h");
+        q[l - 1] = gg; i = pp;
+      }
+      return q;
+    };
+    for (unsigned long long c = 0; c < nh && rc == RC_PROOF; c++) {
+      if (match[c] < 0) continue;
+      const long long j = cand[c];
+      int l = 1;
+      while (l < b && j >= lv.off[l + 1]) l++;
+      const std::vector<int> q = path(side.par, side.gat, l, (uint32_t)(j - lv.off[l]));
+      std::vector<int> full = path(par, gat, a, (uint32_t)match[c]);
+      for (int i = (int)q.size() - 1; i >= 0; i--) full.push_back(inv[q[i]]);
+      if (!host_circuit_ok(hs, full)) continue;
+      res.circuit = full;
+      res.n_found = 1;
+      res.mitm_found = true;
+      res.mitm_split[1] = (int)q.size();
+      rc = RC_CIRCUIT;
+    }
+  }
+  if (rc == RC_PROOF) res.mitm_proof = true;
+  S1.release(); S2.release(); Si.release(); B1.release(); B2.release(); pos.release(); hits.release(); flags.release();
+  done();
+  return rc;
+}
+
 // host part of the device spec: every field, plus the gate-matrix (gi) and goal (gl) tables to place on the device
 template <int NQ>
 DevSpec devspec_host(const HostSpec &hs, const SymGroup &grp, int depth, bool nogoal, std::vector<int4> &gi,
@@ -2598,7 +2991,14 @@ int Engine::search(const HostSpec &hs, const Options &opt, const std::function<v
   int rc;
   try {
     ck(cudaSetDevice(dev_), "cudaSetDevice");
-    if (opt.table_k > 0 && !hs.states) {
+    if (opt.mitm && !hs.states) {
+      switch (hs.n) {
+        case 1: rc = impl_->run_mitm<1>(hs, opt, cb, res); break;
+        case 2: rc = impl_->run_mitm<2>(hs, opt, cb, res); break;
+        case 3: rc = impl_->run_mitm<3>(hs, opt, cb, res); break;
+        default: res.error = "n = " + std::to_string(hs.n) + " not built"; rc = RC_USAGE;
+      }
+    } else if (opt.table_k > 0 && !hs.states) {
       switch (hs.n) {
         case 1: rc = impl_->run_table<1>(hs, opt, cb, res); break;
         case 2: rc = impl_->run_table<2>(hs, opt, cb, res); break;

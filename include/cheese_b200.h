@@ -58,6 +58,7 @@ typedef struct {
   int profile;      /* 1: record device times per phase (cz_result.expand_ms / dedupe_ms) */
   int table_k;      /* --table K: 0 none; K > 0 the distance table of the last K gates (cheese.cu:1431-1593) */
   const char *cache_dir;   /* distance-table cache directory ("build" by default; NULL: no cache) */
+  int mitm;         /* --mitm: meet in the middle (cheese.cu:1595-1760); symmetry classes off, like the reference */
 } cz_options;
 void cz_options_default(cz_options *opt);
 
@@ -67,7 +68,7 @@ typedef struct {
   int64_t parents, prefixes, cut_w3, cut_lb, survivors, distinct;
   int proved_unsat;
   double seconds;
-  int table;        /* 1: a level of the distance-table build (the "dir": "table" lines) */
+  int dir;          /* the line's "dir" field: 0 none; 1 "table" (distance-table build); 2 "fwd" / 3 "bwd" (--mitm) */
 } cz_level_stats;
 typedef void (*cz_level_fn)(void *user, const cz_level_stats *level);
 
@@ -98,6 +99,12 @@ typedef struct {
   int table_loaded, table_built;
   double table_seconds;
   char table_path[256];
+  /* --mitm */
+  int mitm_join;               /* 1: the join ran: {"dir": "join", "forward", "backward", "hash_matches", "seconds"} */
+  int64_t mitm_forward, mitm_backward, mitm_hash_matches;
+  double mitm_seconds;
+  int mitm_split[2];           /* [forward levels, backward levels]: the "mitm" field of the circuit or proof line */
+  int mitm_found, mitm_proof;  /* rc 0 / rc 1 through the join */
   char error[256];
 } cz_result;
 

@@ -10,6 +10,7 @@ Writes
   cheese_b200/data/base-n{2,3}.spec     the default Clifford+T spec per qubit count (its target is replaced per job)
   tests/golden/cases.json               per case: spec, flags, exit code and the reference's stdout with every
                                         "seconds" value replaced by 0.00 (machine dependent, never compared)
+  tests/golden/mitm_cases.json          the same for --mitm runs
   tests/golden/table_cases.json         the same for --table K runs, each in a fresh working directory (so the
                                         reference builds its distance table and prints the "dir": "table" lines),
                                         plus the reference's stderr table line
@@ -54,6 +55,34 @@ TABLE_CASES = [
 ]
 
 
+# --mitm cases (reference cheese.cu:1595-1760): proofs through the join, proofs by a forward level, circuits found by
+# the join or by a tree level; (case name, spec stem, flags)
+MITM_CASES = [(f"toffoli-{d}-mitm", "toffoli", ["--depth", str(d), "--mitm"]) for d in range(4, 11)] + [
+    ("ccz-7-mitm", "ccz", ["--depth", "7", "--mitm"]), ("ccz-8-mitm", "ccz", ["--depth", "8", "--mitm"]),
+    ("cs-4-mitm", "cs", ["--depth", "4", "--mitm"]), ("cs-5-mitm", "cs", ["--depth", "5", "--mitm"]),
+    ("qft_2-6-mitm", "qft_2", ["--depth", "6", "--mitm"]), ("qft_2-7-mitm", "qft_2", ["--depth", "7", "--mitm"]),
+    ("relative-phase-toffoli-9-mitm", "relative-phase-toffoli", ["--depth", "9", "--mitm"]),
+    ("peres-9-mitm", "peres", ["--depth", "9", "--mitm"]), ("fredkin-9-mitm", "fredkin", ["--depth", "9", "--mitm"]),
+    ("half_adder_3-9-mitm", "half_adder_3", ["--depth", "9", "--mitm"]),
+    ("toffoli-7-mitm-nodedupe", "toffoli", ["--depth", "7", "--mitm", "--no-dedupe"]),
+    ("toffoli-9-mitm-table4", "toffoli", ["--depth", "9", "--mitm", "--table", "4"]),
+] + [(f"rand-{i:02d}-mitm", f"rand-{i:02d}", ["--mitm"]) for i in range(24)] + [
+    (f"table-rand-{i}-mitm", f"table-rand-{i}", ["--mitm"]) for i in range(8)]
+
+
+def mitm_cases(binp):
+    out = []
+    for name, stem, flags in MITM_CASES:
+        t0 = time.time()
+        p = subprocess.run([str(binp), str(GOLD / "specs" / f"{stem}.spec")] + flags, capture_output=True, text=True,
+                           timeout=3600)
+        lines = [SECONDS.sub('"seconds": 0.00', l) for l in p.stdout.splitlines()]
+        print(f"{name}: rc {p.returncode}, {len(lines)} lines, {time.time() - t0:.1f} s", file=sys.stderr)
+        out.append({"name": name, "spec": stem, "flags": flags, "rc": p.returncode, "stdout": lines})
+    (GOLD / "mitm_cases.json").write_text(json.dumps(out, indent=1) + "\n")
+    print(f"{len(out)} mitm cases written", file=sys.stderr)
+
+
 def table_cases(binp, write_spec):
     """--table K golden cases: named targets plus seeded random ones (found circuits), each run in its own empty
     working directory so that the reference builds (and prints) its distance table"""
@@ -95,6 +124,7 @@ def main():
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--quick", action="store_true", help="skip the cases that take more than a few seconds")
     ap.add_argument("--table-only", action="store_true", help="write only the --table K cases")
+    ap.add_argument("--mitm-only", action="store_true", help="write only the --mitm cases")
     o = ap.parse_args()
     sys.dont_write_bytecode = True
     sys.path.insert(0, str(Path(o.ref) / "python"))
@@ -122,6 +152,9 @@ def main():
 
     if o.table_only:
         table_cases(binp, write_spec)
+        return
+    if o.mitm_only:
+        mitm_cases(binp)
         return
     # target specs written by the reference generator (budget line = the first budget used)
     qdir = Path(o.ref) / "tests" / "qasm"
@@ -166,6 +199,7 @@ def main():
     (GOLD / "cases.json").write_text(json.dumps(cases, indent=1) + "\n")
     print(f"{len(cases)} cases written", file=sys.stderr)
     table_cases(binp, write_spec)
+    mitm_cases(binp)
 
 
 if __name__ == "__main__":
