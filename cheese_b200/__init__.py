@@ -47,6 +47,11 @@ class Result(C.Structure):
 LEVEL_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(LevelStats))
 
 
+class SpecGenInfo(C.Structure):
+    _fields_ = [("n", C.c_int), ("gates", C.c_int), ("candidates", C.c_int), ("w2_pairs", C.c_int),
+                ("w3_triples", C.c_int)]
+
+
 class TcOptions(C.Structure):
     _fields_ = [("table_k", C.c_int), ("maxt", C.c_int), ("cache_dir", C.c_char_p)]
 
@@ -124,6 +129,12 @@ SIGNATURES = {
     "cz_int32_peak": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "cz_tcount_options_default": (None, [C.POINTER(TcOptions)]),
     "cz_tspec_check": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(C.c_int), C.c_char_p, C.c_size_t]),
+    "cz_spec_generate": (C.c_int, [C.c_char_p, C.c_size_t, C.c_int, C.c_int, C.POINTER(C.c_char_p),
+                                   C.POINTER(C.c_int), C.c_int, C.c_int, C.c_char_p, C.c_size_t,
+                                   C.POINTER(C.c_size_t), C.POINTER(SpecGenInfo), C.c_char_p, C.c_size_t]),
+    "cz_tspec_generate": (C.c_int, [C.c_char_p, C.c_size_t, C.c_int, C.c_int, C.POINTER(C.c_char_p),
+                                    C.POINTER(C.c_int), C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t), C.c_char_p,
+                                    C.c_size_t]),
     "cz_tcount": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(TcOptions), TC_LEVEL_FN, C.c_void_p,
                             C.POINTER(TcResult)]),
     "cz_clifford_table": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(CliffTableInfo), C.c_char_p, C.c_size_t]),
@@ -202,6 +213,49 @@ class SpecError(Exception):
     def __init__(self, rc, msg):
         super().__init__(msg)
         self.rc = rc
+
+
+def _gen_args(circ, qasm):
+    if qasm is not None:
+        q = qasm.encode() if isinstance(qasm, str) else qasm
+        return q, len(q), 0, None, None
+    names = (C.c_char_p * max(1, len(circ)))(*[g.encode() for g, _ in circ])
+    qs = (C.c_int * max(3, 3 * len(circ)))(*[v for _, q in circ for v in (list(q) + [-1, -1, -1])[:3]])
+    return None, 0, len(circ), names, qs
+
+
+def _gen_call(fn, *args):
+    cap = 1 << 16
+    while True:
+        out = C.create_string_buffer(cap)
+        need = C.c_size_t()
+        err = C.create_string_buffer(256)
+        rc = fn(*args, out, cap, C.byref(need), err, 256)
+        if rc == 3 and need.value + 1 > cap:
+            cap = need.value + 1
+            continue
+        if rc:
+            raise SpecError(rc, err.value.decode())
+        return out.value.decode()
+
+
+def spec_generate(n=None, circ=None, depth=1, w3=True, qasm=None):
+    """the gate-count spec text of a target circuit (gate list [(name, qubits)] on n qubits, or QASM text), as the
+    reference's spec generator writes it; returns (text, info dict)"""
+    q, ql, ng, names, qs = _gen_args(circ, qasm)
+    info = SpecGenInfo()
+
+    def fn(*a):
+        *head, out, cap, need, err, errlen = a
+        return lib().cz_spec_generate(*head, out, cap, need, C.byref(info), err, errlen)
+    text = _gen_call(fn, q, ql, n or 0, ng, names, qs, depth, 0 if w3 else 1)
+    return text, {k: getattr(info, k) for k, _ in SpecGenInfo._fields_}
+
+
+def tspec_generate(n=None, circ=None, qasm=None):
+    """the T-count spec text of a target circuit, as the reference's tcount.py writes it"""
+    q, ql, ng, names, qs = _gen_args(circ, qasm)
+    return _gen_call(lib().cz_tspec_generate, q, ql, n or 0, ng, names, qs)
 
 
 def tspec_check(text):
@@ -446,7 +500,7 @@ class Batch:
             self._h = None
 
 
-REQ_GATES, REQ_TCOUNT, REQ_CLIFFORD = 0, 1, 2
+REQ_GATES, REQ_TCOUNT, REQ_CLIFFORD, REQ_GATES_QASM, REQ_TCOUNT_QASM = 0, 1, 2, 3, 4
 
 
 class Server:

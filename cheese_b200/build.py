@@ -23,10 +23,12 @@ HOSTCXX = os.environ.get("CZ_HOSTCXX", "/usr/bin/g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-ccbin", HOSTCXX, "-Xcompiler", "-fPIC"]
 
-LIB_SOURCES = ["cz_search.cu", "cz_tcount.cu", "cz_clifford.cu", "cz_spec.cpp", "cz_capi.cpp", "cz_serve.cpp"]
+LIB_SOURCES = ["cz_search.cu", "cz_tcount.cu", "cz_clifford.cu", "cz_spec.cpp", "cz_specgen.cpp", "cz_capi.cpp",
+               "cz_serve.cpp"]
 HEADERS = ["cz_common.h", "cz_spec.h", "cz_engine.h", "cz_sort.cuh", "cz_tcount.h", "cz_clifford.h", "cz_tableau.h",
-           "cz_capi_internal.h"]
-BINARIES = {"cheese": "cli_cheese.cpp", "tcount": "cli_tcount.cpp", "cliffopt": "cli_cliffopt.cpp"}
+           "cz_capi_internal.h", "cz_specgen.h"]
+BINARIES = {"cheese": "cli_cheese.cpp", "tcount": "cli_tcount.cpp", "cliffopt": "cli_cliffopt.cpp",
+            "cheese-spec": "cli_spec.cpp"}
 
 
 def _stale(out, deps):

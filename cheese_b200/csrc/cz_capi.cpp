@@ -8,6 +8,7 @@
 #include <string>
 
 #include "cz_capi_internal.h"
+#include "cz_specgen.h"
 
 namespace {
 void put_err(char *err, size_t n, const std::string &m) {
@@ -507,3 +508,60 @@ int cz_clifford_element(cz_engine *engine, int n, const uint64_t *index, size_t 
 const char *cz_version(void) { return "cheese_b200 0.1 (sm_100a)"; }
 
 }  // extern "C"
+
+namespace {
+int specgen_input(const char *qasm, size_t qasm_len, int n, int ngates, const char *const *names, const int *qubits,
+                  int &nq, std::vector<cz::CircGate> &circ, std::string &err) {
+  if (qasm) return cz::parse_qasm(qasm, qasm_len, nq, circ, err);
+  if (ngates < 0 || (ngates > 0 && (!names || !qubits))) { err = "bad gate list"; return CZ_ERR_SPEC; }
+  nq = n;
+  circ.clear();
+  for (int i = 0; i < ngates; i++) {
+    cz::CircGate g;
+    g.g = names[i] ? names[i] : "";
+    for (int j = 0; j < 3 && qubits[3 * i + j] >= 0; j++) g.q[g.nq++] = qubits[3 * i + j];
+    circ.push_back(g);
+  }
+  return 0;
+}
+int specgen_out(const std::string &text, char *out, size_t cap, size_t *out_len) {
+  if (out_len) *out_len = text.size();
+  if (!out || cap < text.size() + 1) return CZ_ERR_USAGE;
+  std::memcpy(out, text.c_str(), text.size() + 1);
+  return 0;
+}
+}  // namespace
+
+int cz_spec_generate(const char *qasm, size_t qasm_len, int n, int ngates, const char *const *names,
+                     const int *qubits, int depth, int no_w3, char *out, size_t cap, size_t *out_len,
+                     cz_specgen_info *info, char *err, size_t errlen) {
+  std::string e, text;
+  std::vector<cz::CircGate> circ;
+  int nq = 0;
+  int rc = specgen_input(qasm, qasm_len, n, ngates, names, qubits, nq, circ, e);
+  cz::SpecGenInfo gi;
+  if (!rc) rc = cz::spec_generate(nq, circ, depth, no_w3 == 0, text, gi, e);
+  if (rc) {
+    put_err(err, errlen, e);
+    return rc;
+  }
+  if (info) {
+    info->n = nq; info->gates = (int)circ.size(); info->candidates = gi.candidates;
+    info->w2_pairs = gi.bad2; info->w3_triples = gi.bad3;
+  }
+  return specgen_out(text, out, cap, out_len);
+}
+
+int cz_tspec_generate(const char *qasm, size_t qasm_len, int n, int ngates, const char *const *names,
+                      const int *qubits, char *out, size_t cap, size_t *out_len, char *err, size_t errlen) {
+  std::string e, text;
+  std::vector<cz::CircGate> circ;
+  int nq = 0;
+  int rc = specgen_input(qasm, qasm_len, n, ngates, names, qubits, nq, circ, e);
+  if (!rc) rc = cz::tspec_generate(nq, circ, text, e);
+  if (rc) {
+    put_err(err, errlen, e);
+    return rc;
+  }
+  return specgen_out(text, out, cap, out_len);
+}

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "cz_capi_internal.h"
+#include "cz_specgen.h"
 
 namespace {
 
@@ -28,6 +29,7 @@ double wall() { return std::chrono::duration<double>(std::chrono::steady_clock::
 
 struct Req {
   int id = 0, kind = 0, depth = -1;
+  bool qasm = false;               // text is an OpenQASM target: the spec is generated here
   std::string text;
   double t_submit = 0, t_start = 0, t_done = 0;
   bool done = false;
@@ -95,8 +97,23 @@ struct cz_server {
       for (Req *r; (r = pop(0, live.empty() && waiting.empty())) != nullptr;) {
         cz_spec *sp = nullptr;
         char e2[256] = {0};
-        const int prc = cz_spec_parse(r->text.data(), r->text.size(), &sp, e2, sizeof e2);
         r->t_start = wall();
+        if (r->qasm) {                       // an OpenQASM target: its spec, budget = its gate count by default
+          int nq = 0;
+          std::vector<cz::CircGate> circ;
+          std::string ge, text;
+          cz::SpecGenInfo gi;
+          int grc = cz::parse_qasm(r->text.data(), r->text.size(), nq, circ, ge);
+          if (!grc) grc = cz::spec_generate(nq, circ, r->depth >= 0 ? r->depth : (int)circ.size(), true, text, gi, ge);
+          if (grc) {
+            r->rc = grc;
+            r->error = ge;
+            finish(r);
+            continue;
+          }
+          r->text.swap(text);
+        }
+        const int prc = cz_spec_parse(r->text.data(), r->text.size(), &sp, e2, sizeof e2);
         if (prc || sp->hs.states || (r->depth >= 0 ? r->depth : sp->hs.depth) > CZ_MAX_DEPTH) {
           r->rc = prc ? prc : CZ_ERR_USAGE;
           r->error = prc ? e2 : "unsupported request";
@@ -209,6 +226,20 @@ struct cz_server {
       Req *r = pop(1, true);
       if (!r) continue;
       r->t_start = wall();
+      if (r->qasm) {                         // an OpenQASM target: its T-count spec
+        int nq = 0;
+        std::vector<cz::CircGate> circ;
+        std::string ge, text;
+        int grc = cz::parse_qasm(r->text.data(), r->text.size(), nq, circ, ge);
+        if (!grc) grc = cz::tspec_generate(nq, circ, text, ge);
+        if (grc) {
+          r->rc = grc;
+          r->error = ge;
+          finish(r);
+          continue;
+        }
+        r->text.swap(text);
+      }
       std::string out;
       long long children = 0;
       auto on_level = [](void *u, const cz_tcount_level *l) {
@@ -319,17 +350,19 @@ void cz_server_destroy(cz_server *s) {
 }
 
 int cz_server_submit(cz_server *s, int kind, const char *text, size_t len, int depth) {
-  if (!s || kind < 0 || kind > 2 || (!text && len)) return -CZ_ERR_USAGE;
+  if (!s || kind < 0 || kind > 4 || (!text && len)) return -CZ_ERR_USAGE;
   Req *r = new Req;
   r->kind = kind;
   r->depth = depth;
+  r->qasm = kind >= CZ_REQ_GATES_QASM;
+  const int q = kind == CZ_REQ_GATES_QASM ? 0 : kind == CZ_REQ_TCOUNT_QASM ? 1 : kind;
   r->text.assign(text ? text : "", len);
   std::lock_guard<std::mutex> lk(s->mu);
   r->id = s->next_id++;
   r->t_submit = wall();
   s->reqs[r->id] = r;
-  s->queue[kind].push_back(r);
-  s->cv_work[kind].notify_one();
+  s->queue[q].push_back(r);
+  s->cv_work[q].notify_one();
   return r->id;
 }
 

@@ -1,0 +1,724 @@
+// Spec generation on the host, in exact Z[w] arithmetic (w = e^{i pi/4}; an element is a + b w + c w^2 + d w^3, a
+// matrix is its entries over sqrt2^k with k as small as possible). Restates the reference's generators:
+// python/cheese/spec.py (gate table :16-27, matrices :75-110, candidates :127-136, window rules :139-186, CX table
+// :189-228, gate-set flags :317-319, text :322-350) and python/cheese/tcount.py (channel :79-101, rotation tables
+// :104-129, text :157-168). Integer overflow is detected, never wrapped.
+#include "cz_specgen.h"
+
+#include <algorithm>
+#include <array>
+#include <cctype>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <set>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+namespace cz {
+namespace {
+
+struct Z {
+  int64_t a = 0, b = 0, c = 0, d = 0;
+  bool zero() const { return !a && !b && !c && !d; }
+  bool operator==(const Z &o) const { return a == o.a && b == o.b && c == o.c && d == o.d; }
+  bool operator!=(const Z &o) const { return !(*this == o); }
+};
+
+int64_t chk(__int128 v) {
+  if (v > INT64_MAX || v < INT64_MIN) throw std::overflow_error("coefficient exceeds 64 bits");
+  return (int64_t)v;
+}
+Z zadd(const Z &x, const Z &y) {
+  return {chk((__int128)x.a + y.a), chk((__int128)x.b + y.b), chk((__int128)x.c + y.c), chk((__int128)x.d + y.d)};
+}
+Z zmul(const Z &x, const Z &y) {   // w^4 = -1
+  const int64_t X[4] = {x.a, x.b, x.c, x.d}, Y[4] = {y.a, y.b, y.c, y.d};
+  __int128 o[4] = {0, 0, 0, 0};
+  for (int i = 0; i < 4; i++) {
+    if (!X[i]) continue;
+    for (int j = 0; j < 4; j++) {
+      if (!Y[j]) continue;
+      const __int128 p = (__int128)X[i] * Y[j];
+      if (i + j < 4) o[i + j] += p; else o[i + j - 4] -= p;
+    }
+  }
+  return {chk(o[0]), chk(o[1]), chk(o[2]), chk(o[3])};
+}
+Z wpow(int p) {
+  p = ((p % 8) + 8) % 8;
+  Z z;
+  int64_t *v[4] = {&z.a, &z.b, &z.c, &z.d};
+  *v[p % 4] = p < 4 ? 1 : -1;
+  return z;
+}
+Z conj(const Z &x) { return {x.a, -x.d, -x.c, -x.b}; }
+bool down(const Z &x, Z &out) {    // x / sqrt2 when it stays in Z[w] (sqrt2 = w - w^3)
+  if (((x.a - x.c) & 1) || ((x.b - x.d) & 1)) return false;
+  out = {(x.b - x.d) / 2, (x.a + x.c) / 2, (x.b + x.d) / 2, (x.c - x.a) / 2};
+  return true;
+}
+int val(Z x) {                      // how often sqrt2 divides x (at most 400, as the reference caps it)
+  int v = 0;
+  Z y;
+  while (down(x, y)) {
+    x = y;
+    if (++v > 400) break;
+  }
+  return v;
+}
+
+struct Mat {
+  int k = 0, N = 0;
+  std::vector<Z> e;                 // row-major N x N
+  Z &at(int r, int c) { return e[(size_t)r * N + c]; }
+  const Z &at(int r, int c) const { return e[(size_t)r * N + c]; }
+};
+void normalise(Mat &M) {
+  std::vector<Z> D(M.e.size());
+  while (M.k > 0) {
+    bool ok = true;
+    for (size_t i = 0; i < M.e.size() && ok; i++) ok = down(M.e[i], D[i]);
+    if (!ok) break;
+    M.e.swap(D);
+    M.k--;
+  }
+}
+Mat identity(int N) {
+  Mat M;
+  M.N = N;
+  M.e.assign((size_t)N * N, Z{});
+  for (int i = 0; i < N; i++) M.at(i, i) = Z{1, 0, 0, 0};
+  return M;
+}
+Mat matmul(const Mat &A, const Mat &B) {
+  Mat C;
+  C.N = A.N;
+  C.k = A.k + B.k;
+  C.e.assign((size_t)A.N * A.N, Z{});
+  for (int i = 0; i < A.N; i++)
+    for (int l = 0; l < A.N; l++) {
+      const Z &x = A.at(i, l);
+      if (x.zero()) continue;
+      for (int j = 0; j < A.N; j++) {
+        const Z &y = B.at(l, j);
+        if (!y.zero()) C.at(i, j) = zadd(C.at(i, j), zmul(x, y));
+      }
+    }
+  normalise(C);
+  return C;
+}
+Mat dagger(const Mat &A) {
+  Mat D = A;
+  for (int r = 0; r < A.N; r++)
+    for (int c = 0; c < A.N; c++) D.at(r, c) = conj(A.at(c, r));
+  return D;
+}
+
+// local gate matrices: entry (l, m) = sum of w^p over the listed phases, over sqrt2^k; bit j of a local index is
+// the gate's j-th qubit (cx / ccx: the controls first, the target last)
+struct GateDef {
+  int k = 0, dim = 0;
+  std::vector<std::vector<int>> ph;   // dim x dim lists of phase exponents
+  Z entry(int l, int m) const {
+    Z x;
+    for (int p : ph[(size_t)l * dim + m]) x = zadd(x, wpow(p));
+    return x;
+  }
+  int arity() const { return dim == 2 ? 1 : dim == 4 ? 2 : 3; }
+};
+GateDef diag1(int p) { GateDef g; g.dim = 2; g.ph.assign(4, {}); g.ph[0] = {0}; g.ph[3] = {p}; return g; }
+const std::map<std::string, GateDef> &gates() {
+  static const std::map<std::string, GateDef> G = [] {
+    std::map<std::string, GateDef> m;
+    GateDef x; x.dim = 2; x.ph.assign(4, {}); x.ph[1] = {0}; x.ph[2] = {0}; m["x"] = x;
+    GateDef y; y.dim = 2; y.ph.assign(4, {}); y.ph[1] = {6}; y.ph[2] = {2}; m["y"] = y;
+    m["z"] = diag1(4); m["s"] = diag1(2); m["sdg"] = diag1(6); m["t"] = diag1(1); m["tdg"] = diag1(7);
+    GateDef h; h.k = 1; h.dim = 2; h.ph = {{0}, {0}, {0}, {4}}; m["h"] = h;
+    GateDef cx; cx.dim = 4; cx.ph.assign(16, {});
+    cx.ph[0 * 4 + 0] = {0}; cx.ph[1 * 4 + 3] = {0}; cx.ph[2 * 4 + 2] = {0}; cx.ph[3 * 4 + 1] = {0}; m["cx"] = cx;
+    GateDef cz; cz.dim = 4; cz.ph.assign(16, {});
+    cz.ph[0] = {0}; cz.ph[5] = {0}; cz.ph[10] = {0}; cz.ph[15] = {4}; m["cz"] = cz;
+    GateDef ccx; ccx.dim = 8; ccx.ph.assign(64, {});
+    for (int l = 0; l < 8; l++) ccx.ph[(size_t)l * 8 + (l == 3 ? 7 : l == 7 ? 3 : l)] = {0};
+    m["ccx"] = ccx;
+    return m;
+  }();
+  return G;
+}
+std::string dagger_name(const std::string &g) {
+  if (g == "s") return "sdg";
+  if (g == "sdg") return "s";
+  if (g == "t") return "tdg";
+  if (g == "tdg") return "t";
+  return g;                         // every other gate of the table is its own inverse
+}
+
+// 2^n x 2^n matrix of gate g on qubits qs (bit q of an index is qubit q)
+Mat gate_matrix(const GateDef &G, const int *qs, int n) {
+  const int N = 1 << n, L = G.dim, nq = G.arity();
+  int mask = 0;
+  for (int j = 0; j < nq; j++) mask |= 1 << qs[j];
+  Mat M;
+  M.N = N;
+  M.k = G.k;
+  M.e.assign((size_t)N * N, Z{});
+  std::vector<int> idx(L);
+  for (int base = 0; base < N; base++) {
+    if (base & mask) continue;
+    for (int l = 0; l < L; l++) {
+      int x = base;
+      for (int j = 0; j < nq; j++) x |= ((l >> j) & 1) << qs[j];
+      idx[l] = x;
+    }
+    for (int l = 0; l < L; l++)
+      for (int m = 0; m < L; m++)
+        for (int p : G.ph[(size_t)l * L + m]) M.at(idx[l], idx[m]) = zadd(M.at(idx[l], idx[m]), wpow(p));
+  }
+  normalise(M);
+  return M;
+}
+
+Mat unitary(int n, const std::vector<CircGate> &circ) {
+  Mat U = identity(1 << n);
+  for (const CircGate &g : circ) U = matmul(gate_matrix(gates().at(g.g), g.q, n), U);
+  return U;
+}
+
+struct Cand { std::string name, g; int nq; int q[3]; };
+std::vector<Cand> candidates(int n, const std::vector<std::string> &gs) {
+  std::vector<Cand> out;
+  for (const std::string &g : gs) {
+    const int ar = gates().at(g).arity();
+    std::vector<std::vector<int>> qss;
+    if (ar == 1) {
+      for (int q = 0; q < n; q++) qss.push_back({q});
+    } else if (ar == 2) {
+      for (int a = 0; a < n; a++)
+        for (int b = 0; b < n; b++)
+          if (a != b) qss.push_back({a, b});
+    } else {                        // permutations of 3 qubits in lexicographic order, controls unordered
+      for (int a = 0; a < n; a++)
+        for (int b = 0; b < n; b++)
+          for (int c = 0; c < n; c++)
+            if (a != b && a != c && b != c && a < b) qss.push_back({a, b, c});
+    }
+    for (const auto &qs : qss) {
+      Cand c;
+      c.g = g;
+      c.nq = ar;
+      c.name = "L_" + g + "_";
+      for (int j = 0; j < ar; j++) {
+        c.q[j] = qs[j];
+        c.name += (j ? "_" : "") + std::to_string(qs[j]);
+      }
+      for (int j = ar; j < 3; j++) c.q[j] = -1;
+      out.push_back(c);
+    }
+  }
+  return out;
+}
+
+// key of a product on its qubits after stripping the qubits it acts on trivially (spec.py canon): the qubit list,
+// the exponent and the matrix, serialised
+std::string canon_key(std::vector<int> qubits, Mat M) {
+  for (int i = (int)qubits.size() - 1; i >= 0; i--) {
+    const int N = M.N, bit = 1 << i;
+    bool trivial = true;
+    for (int r = 0; r < N && trivial; r++)
+      for (int c = 0; c < N && trivial; c++) {
+        if ((r ^ c) & bit) trivial = M.at(r, c).zero();
+        else if (!((r | c) & bit)) trivial = M.at(r, c) == M.at(r | bit, c | bit);
+      }
+    if (!trivial) continue;
+    std::vector<int> keep;
+    for (int r = 0; r < N; r++) if (!(r & bit)) keep.push_back(r);
+    Mat S;
+    S.N = (int)keep.size();
+    S.k = M.k;
+    S.e.resize((size_t)S.N * S.N);
+    for (int r = 0; r < S.N; r++)
+      for (int c = 0; c < S.N; c++) S.at(r, c) = M.at(keep[r], keep[c]);
+    normalise(S);
+    M = S;
+    qubits.erase(qubits.begin() + i);
+  }
+  std::string key;
+  auto put = [&](int64_t v) { key.append((const char *)&v, 8); };
+  put((int64_t)qubits.size());
+  for (int q : qubits) put(q);
+  put(M.k);
+  put(M.N);
+  for (const Z &z : M.e) { put(z.a); put(z.b); put(z.c); put(z.d); }
+  return key;
+}
+std::string product_key(const std::vector<Cand> &cs, const int *seq, int len) {
+  std::vector<int> U;
+  for (int i = 0; i < len; i++)
+    for (int j = 0; j < cs[seq[i]].nq; j++) U.push_back(cs[seq[i]].q[j]);
+  std::sort(U.begin(), U.end());
+  U.erase(std::unique(U.begin(), U.end()), U.end());
+  Mat P = identity(1 << U.size());
+  for (int i = 0; i < len; i++) {
+    const Cand &c = cs[seq[i]];
+    int lq[3] = {0, 0, 0};
+    for (int j = 0; j < c.nq; j++) lq[j] = (int)(std::find(U.begin(), U.end(), c.q[j]) - U.begin());
+    P = matmul(gate_matrix(gates().at(c.g), lq, (int)U.size()), P);
+  }
+  return canon_key(U, P);
+}
+
+// W2 / W3 window rules (spec.py sym_rules): a pair (triple) is cut when its product equals the identity, a single
+// candidate (a pair), or the product of an earlier pair (triple) in the enumeration order
+void sym_rules(const std::vector<Cand> &cs, bool use3, std::vector<std::array<int, 2>> &bad2,
+               std::vector<std::array<int, 3>> &bad3) {
+  const int G = (int)cs.size();
+  std::set<std::string> shortk;
+  shortk.insert(canon_key({}, identity(1)));
+  for (int g = 0; g < G; g++) shortk.insert(product_key(cs, &g, 1));
+  std::unordered_map<std::string, int> first;
+  std::vector<std::string> keys2;
+  std::vector<uint8_t> isbad((size_t)G * G, 0);
+  for (int f = 0; f < G; f++)
+    for (int g = 0; g < G; g++) {
+      const int pr[2] = {f, g};
+      std::string k = product_key(cs, pr, 2);
+      bool bad = shortk.count(k) > 0;
+      if (!bad) {
+        auto it = first.find(k);
+        if (it == first.end()) first.emplace(k, f * G + g);
+        else bad = it->second != f * G + g;
+      }
+      if (bad) { bad2.push_back({f, g}); isbad[(size_t)f * G + g] = 1; }
+      keys2.push_back(std::move(k));
+    }
+  // triples (f, g, h) with (f, g) and (g, h) both kept, (f, g) ascending; two triples of one (f, g) never share a
+  // product (their last gates would be equal operators, and then one of the (g, h) pairs is cut), so which triple
+  // of a key comes first does not depend on the order of h
+  size_t ntrip = 0;
+  for (int f = 0; f < G; f++)
+    for (int g = 0; g < G; g++) {
+      if (isbad[(size_t)f * G + g]) continue;
+      for (int h = 0; h < G; h++) ntrip += !isbad[(size_t)g * G + h];
+    }
+  if (!use3 || ntrip > 300000) return;
+  for (auto &k : keys2) shortk.insert(std::move(k));
+  std::unordered_map<std::string, long> first3;
+  for (int f = 0; f < G; f++)
+    for (int g = 0; g < G; g++) {
+      if (isbad[(size_t)f * G + g]) continue;
+      for (int h = 0; h < G; h++) {
+        if (isbad[(size_t)g * G + h]) continue;
+        const int tr[3] = {f, g, h};
+        const long id = ((long)f * G + g) * G + h;
+        std::string k = product_key(cs, tr, 3);
+        bool bad = shortk.count(k) > 0;
+        if (!bad) {
+          auto it = first3.find(k);
+          if (it == first3.end()) first3.emplace(std::move(k), id);
+          else bad = it->second != id;
+        }
+        if (bad) bad3.push_back({f, g, h});
+      }
+    }
+}
+
+// CX lower bound (spec.py cuts / cx_table): per qubit bipartition a demand in [0, 2|A|]; the table holds, for every
+// demand vector (mixed radix), the fewest two-qubit gates whose crossings meet every demand
+std::vector<std::vector<int>> cuts(int n) {
+  std::vector<std::vector<int>> out;
+  for (int r = 1; r <= n / 2; r++) {
+    std::vector<int> A(r);
+    for (int i = 0; i < r; i++) A[i] = i;
+    while (true) {
+      const bool has0 = std::find(A.begin(), A.end(), 0) != A.end();
+      if (!(r == n - r && !has0)) out.push_back(A);
+      int i = r - 1;
+      while (i >= 0 && A[i] == n - r + i) i--;
+      if (i < 0) break;
+      A[i]++;
+      for (int j = i + 1; j < r; j++) A[j] = A[j - 1] + 1;
+    }
+  }
+  return out;
+}
+bool cx_table(int n, const std::vector<std::vector<int>> &cs, std::vector<int> &rad, std::vector<int> &best) {
+  rad.clear();
+  long size = 1;
+  for (const auto &A : cs) { rad.push_back(2 * (int)A.size() + 1); size *= rad.back(); }
+  if (size > 2000000) return false;
+  std::vector<std::array<int, 2>> pairs;
+  for (int a = 0; a < n; a++)
+    for (int b = a + 1; b < n; b++) pairs.push_back({a, b});
+  int top = 0;
+  for (int r : rad) top = std::max(top, r - 1);
+  const int INF = 1 << 30;
+  best.assign(size, INF);
+  std::vector<int> x(pairs.size(), 0);
+  while (true) {
+    long idx = 0, mult = 1;
+    int sum = 0;
+    for (int v : x) sum += v;
+    for (size_t ci = 0; ci < cs.size(); ci++) {
+      int cross = 0;
+      for (size_t p = 0; p < pairs.size(); p++) {
+        const bool ina = std::find(cs[ci].begin(), cs[ci].end(), pairs[p][0]) != cs[ci].end();
+        const bool inb = std::find(cs[ci].begin(), cs[ci].end(), pairs[p][1]) != cs[ci].end();
+        if (ina != inb) cross += x[p];
+      }
+      idx += std::min(cross, rad[ci] - 1) * mult;
+      mult *= rad[ci];
+    }
+    best[idx] = std::min(best[idx], sum);
+    size_t p = pairs.size();             // next x in itertools.product order (last digit fastest)
+    while (p > 0 && x[p - 1] == top) x[--p] = 0;
+    if (p == 0) break;
+    x[p - 1]++;
+  }
+  long mult = 1;
+  for (int r : rad) {                    // superset minimum, one dimension at a time
+    for (long i = size - 1; i >= 0; i--)
+      if ((i / mult) % r < r - 1) best[i] = std::min(best[i], best[i + mult]);
+    mult *= r;
+  }
+  return true;
+}
+
+// P_b applied to a vector: digits per qubit 0 I, 1 X, 2 Y, 3 Z
+std::vector<Z> pauli_apply(int n, int b, const std::vector<Z> &row) {
+  std::vector<Z> out(row.size());
+  for (size_t x = 0; x < row.size(); x++) {
+    if (row[x].zero()) continue;
+    int flip = 0, ph = 0;
+    for (int q = 0; q < n; q++) {
+      const int dg = (b >> (2 * q)) & 3, bit = (int)(x >> q) & 1;
+      if (dg == 1) flip |= 1 << q;
+      else if (dg == 2) { flip |= 1 << q; ph += 2 + 4 * bit; }
+      else if (dg == 3) ph += 4 * bit;
+    }
+    out[x ^ flip] = zmul(row[x], wpow(ph));
+  }
+  return out;
+}
+Z inner(const std::vector<Z> &u, const std::vector<Z> &v) {
+  Z acc;
+  for (size_t i = 0; i < u.size(); i++)
+    if (!u[i].zero() && !v[i].zero()) acc = zadd(acc, zmul(conj(u[i]), v[i]));
+  return acc;
+}
+// the most one gate changes the T bound: the sde of its Pauli-transfer matrix (spec.py ptm_sde)
+int ptm_sde(const std::string &g) {
+  const GateDef &G = gates().at(g);
+  const int nq = G.arity(), N = 1 << nq;
+  int qs[3] = {0, 1, 2};
+  const Mat U = gate_matrix(G, qs, nq);
+  std::vector<std::vector<Z>> cols(N, std::vector<Z>(N));
+  for (int c = 0; c < N; c++)
+    for (int r = 0; r < N; r++) cols[c][r] = U.at(r, c);
+  int best = 0;
+  for (int b = 0; b < (1 << (2 * nq)); b++) {
+    std::vector<std::vector<Z>> PB(N);
+    for (int c = 0; c < N; c++) {
+      std::vector<Z> e(N);
+      e[c] = Z{1, 0, 0, 0};
+      PB[c] = pauli_apply(nq, b, e);
+    }
+    std::vector<std::vector<Z>> UPBc(N, std::vector<Z>(N));   // column c of U P_b
+    for (int r = 0; r < N; r++)
+      for (int c = 0; c < N; c++) {
+        Z acc;
+        for (int x = 0; x < N; x++) acc = zadd(acc, zmul(U.at(r, x), PB[c][x]));
+        UPBc[c][r] = acc;
+      }
+    for (int a = 0; a < (1 << (2 * nq)); a++) {
+      Z acc;
+      for (int c = 0; c < N; c++) acc = zadd(acc, inner(cols[c], pauli_apply(nq, a, UPBc[c])));
+      if (!acc.zero()) best = std::max(best, 2 * (nq + U.k) - val(acc));
+    }
+  }
+  return best;
+}
+
+// the parts of a spec that depend only on (n, gate set, W3 on/off), cached
+struct GateSetPart {
+  std::vector<Cand> cs;
+  std::string text;          // "standard" .. through the bad3 block
+  std::string tail;          // "cuts" .. "end"
+  int nbad2 = 0, nbad3 = 0;
+};
+std::mutex cache_mu;
+std::map<std::string, std::shared_ptr<const GateSetPart>> cache;
+
+std::string zs(const Z &x) {
+  return std::to_string(x.a) + " " + std::to_string(x.b) + " " + std::to_string(x.c) + " " + std::to_string(x.d);
+}
+
+std::shared_ptr<const GateSetPart> gate_set_part(int n, const std::vector<std::string> &gs, bool use3) {
+  std::string key = std::to_string(n) + (use3 ? "|w3" : "|w2");
+  for (const auto &g : gs) key += "|" + g;
+  {
+    std::lock_guard<std::mutex> lk(cache_mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+  }
+  auto P = std::make_shared<GateSetPart>();
+  P->cs = candidates(n, gs);
+  std::vector<std::array<int, 2>> bad2;
+  std::vector<std::array<int, 3>> bad3;
+  sym_rules(P->cs, use3, bad2, bad3);
+  P->nbad2 = (int)bad2.size();
+  P->nbad3 = (int)bad3.size();
+  static const std::set<std::string> STANDARD = {"x", "y", "z", "s", "sdg", "t", "tdg", "cx", "cz", "h"};
+  bool standard = true, lite = true;
+  for (const auto &g : gs) {
+    standard = standard && STANDARD.count(g);
+    lite = lite && (STANDARD.count(g) || g == "ccx");
+  }
+  lite = lite && !standard;
+  int tdiv = 1;
+  if (lite) {
+    tdiv = 0;
+    for (const auto &g : gs)
+      if (g == "t" || g == "tdg" || g == "ccx") tdiv = std::max(tdiv, ptm_sde(g));
+  }
+  std::string &w = P->text;
+  w += "standard " + std::to_string(standard ? 1 : 0) + "\n";
+  if (lite) w += "lite 1\ntdiv " + std::to_string(tdiv) + "\n";
+  w += "gates " + std::to_string(P->cs.size()) + "\n";
+  for (const Cand &c : P->cs) {
+    const GateDef &G = gates().at(c.g), &I = gates().at(dagger_name(c.g));
+    w += c.name + " " + std::to_string(c.nq);
+    for (int j = 0; j < c.nq; j++) w += " " + std::to_string(c.q[j]);
+    w += " " + std::to_string(G.k);
+    for (int l = 0; l < G.dim; l++)
+      for (int m = 0; m < G.dim; m++) w += " " + zs(G.entry(l, m));
+    w += " " + std::to_string(I.k);
+    for (int l = 0; l < I.dim; l++)
+      for (int m = 0; m < I.dim; m++) w += " " + zs(I.entry(l, m));
+    w += "\n";
+  }
+  w += "bad2 " + std::to_string(bad2.size()) + "\n";
+  for (const auto &p : bad2) w += std::to_string(p[0]) + " " + std::to_string(p[1]) + "\n";
+  w += "bad3 " + std::to_string(bad3.size()) + "\n";
+  for (const auto &t : bad3) w += std::to_string(t[0]) + " " + std::to_string(t[1]) + " " + std::to_string(t[2]) + "\n";
+  const auto cs = cuts(n);
+  std::string &tl = P->tail;
+  tl += "cuts " + std::to_string(cs.size()) + "\n";
+  for (const auto &A : cs) {
+    tl += std::to_string(A.size());
+    for (int q : A) tl += " " + std::to_string(q);
+    tl += "\n";
+  }
+  std::vector<int> rad, best;
+  if (!cx_table(n, cs, rad, best)) {
+    tl += "cxtable 0\n";
+  } else {
+    tl += "cxtable " + std::to_string(best.size()) + "\n";
+    for (size_t i = 0; i < best.size(); i++) tl += (i ? " " : "") + std::to_string(best[i]);
+    tl += "\n";
+  }
+  tl += "end\n";
+  std::lock_guard<std::mutex> lk(cache_mu);
+  auto it = cache.emplace(key, P).first;
+  return it->second;
+}
+
+int check_circuit(int n, const std::vector<CircGate> &circ, std::string &err) {
+  if (n < 1 || n > 6) { err = "n = " + std::to_string(n) + " out of range (1..6)"; return 2; }
+  for (const CircGate &g : circ) {
+    auto it = gates().find(g.g);
+    if (it == gates().end()) { err = "unknown gate " + g.g; return 2; }
+    if (g.nq != it->second.arity()) { err = "gate " + g.g + " needs " + std::to_string(it->second.arity()) + " qubits"; return 2; }
+    for (int j = 0; j < g.nq; j++) {
+      if (g.q[j] < 0 || g.q[j] >= n) { err = "qubit " + std::to_string(g.q[j]) + " out of range"; return 2; }
+      for (int i = 0; i < j; i++)
+        if (g.q[i] == g.q[j]) { err = "gate " + g.g + " repeats qubit " + std::to_string(g.q[j]); return 2; }
+    }
+  }
+  return 0;
+}
+
+}  // namespace
+
+int parse_qasm(const char *text, size_t len, int &n, std::vector<CircGate> &circ, std::string &err) {
+  n = 0;
+  circ.clear();
+  size_t pos = 0;
+  while (pos < len) {
+    size_t e = pos;
+    while (e < len && text[e] != '\n') e++;
+    std::string line(text + pos, e - pos);
+    pos = e + 1;
+    const size_t cm = line.find("//");
+    if (cm != std::string::npos) line = line.substr(0, cm);
+    size_t a = 0, b = line.size();
+    while (a < b && isspace((unsigned char)line[a])) a++;
+    while (b > a && isspace((unsigned char)line[b - 1])) b--;
+    line = line.substr(a, b - a);
+    auto digits_in_brackets = [](const std::string &s, size_t from, int &v, size_t &end) {
+      if (from >= s.size() || s[from] != '[') return false;
+      size_t i = from + 1;
+      if (i >= s.size() || !isdigit((unsigned char)s[i])) return false;
+      long x = 0;
+      while (i < s.size() && isdigit((unsigned char)s[i])) x = x * 10 + (s[i++] - '0');
+      if (i >= s.size() || s[i] != ']') return false;
+      v = (int)x;
+      end = i + 1;
+      return true;
+    };
+    int v;
+    size_t end;
+    if (line.compare(0, 4, "qreg") == 0 && line.size() > 4 && isspace((unsigned char)line[4])) {
+      size_t i = 4;
+      while (i < line.size() && isspace((unsigned char)line[i])) i++;
+      const size_t w0 = i;
+      while (i < line.size() && (isalnum((unsigned char)line[i]) || line[i] == '_')) i++;
+      if (i > w0 && digits_in_brackets(line, i, v, end)) { n = v; continue; }
+    }
+    if (line.compare(0, 5, "qubit") == 0 && digits_in_brackets(line, 5, v, end)) { n = v; continue; }
+    size_t i = 0;
+    while (i < line.size() && line[i] >= 'a' && line[i] <= 'z') i++;
+    if (i == 0 || i >= line.size() || !isspace((unsigned char)line[i])) continue;
+    const std::string g = line.substr(0, i);
+    const size_t semi = line.rfind(';');
+    if (semi == std::string::npos || semi < i) continue;
+    if (!gates().count(g)) continue;
+    CircGate cg;
+    cg.g = g;
+    const std::string args = line.substr(i, semi - i);
+    for (size_t k = 0; k < args.size(); k++) {
+      if (args[k] != '[') continue;
+      if (digits_in_brackets(args, k, v, end)) {
+        if (cg.nq < 3) cg.q[cg.nq] = v;
+        cg.nq++;
+        k = end - 1;
+      }
+    }
+    circ.push_back(cg);
+  }
+  if (n <= 0) { err = "no qubit register"; return 2; }
+  return check_circuit(n, circ, err);
+}
+
+int spec_generate(int n, const std::vector<CircGate> &circ, int depth, bool use_w3, std::string &out,
+                  SpecGenInfo &info, std::string &err) {
+  try {
+    if (int rc = check_circuit(n, circ, err)) return rc;
+    std::set<std::string> gs = {"x", "z", "h", "s", "sdg", "t", "tdg", "cx"};
+    for (const CircGate &g : circ) gs.insert(g.g);
+    const std::vector<std::string> gl(gs.begin(), gs.end());   // byte order, as Python's sorted()
+    const auto P = gate_set_part(n, gl, use_w3);
+    const Mat U = unitary(n, circ);
+    out = "cheese-spec 1\nn " + std::to_string(n) + "\nmode unitary\nphase exact\ndepth " + std::to_string(depth) + "\n";
+    out += P->text;
+    out += "target " + std::to_string(U.k) + "\n";
+    for (int r = 0; r < U.N; r++) {
+      for (int c = 0; c < U.N; c++) out += (c ? " " : "") + zs(U.at(r, c));
+      out += "\n";
+    }
+    out += P->tail;
+    info.candidates = (int)P->cs.size();
+    info.bad2 = P->nbad2;
+    info.bad3 = P->nbad3;
+    return 0;
+  } catch (const std::overflow_error &e) {
+    err = e.what();
+    return 2;
+  }
+}
+
+int tspec_generate(int n, const std::vector<CircGate> &circ, std::string &out, std::string &err) {
+  try {
+    if (int rc = check_circuit(n, circ, err)) return rc;
+    if (n > 4) { err = "T-count specs for n <= 4"; return 2; }
+    const Mat U = unitary(n, circ);
+    const int P = 1 << (2 * n), N = 1 << n;
+    std::vector<Mat> paulis(P);
+    for (int p = 0; p < P; p++) {
+      Mat M;
+      M.N = N;
+      M.e.assign((size_t)N * N, Z{});
+      for (int x = 0; x < N; x++) {
+        int flip = 0, ph = 0;
+        for (int q = 0; q < n; q++) {
+          const int dg = (p >> (2 * q)) & 3, bit = (x >> q) & 1;
+          if (dg == 1) flip |= 1 << q;
+          else if (dg == 2) { flip |= 1 << q; ph += 2 + 4 * bit; }
+          else if (dg == 3) ph += 4 * bit;
+        }
+        M.at(x ^ flip, x) = wpow(ph);
+      }
+      paulis[p] = M;
+    }
+    // channel: Uc[a][b] = Tr(P_a U P_b U^dag) / 2^n = (x + y sqrt2) / sqrt2^e, one exponent for the matrix
+    const Mat Ud = dagger(U);
+    std::vector<int> ks((size_t)P * P);
+    std::vector<std::array<int64_t, 2>> xy((size_t)P * P);
+    int kmax = 0;
+    for (int b = 0; b < P; b++) {
+      const Mat A = matmul(matmul(U, paulis[b]), Ud);
+      for (int a = 0; a < P; a++) {
+        const Mat T = matmul(paulis[a], A);
+        Z tr;
+        for (int i = 0; i < N; i++) tr = zadd(tr, T.at(i, i));
+        if (tr.c != 0 || tr.d != -tr.b) { err = "channel entry not real"; return 2; }
+        ks[(size_t)a * P + b] = T.k;
+        xy[(size_t)a * P + b] = {tr.a, tr.b};
+        kmax = std::max(kmax, T.k);
+      }
+    }
+    int E = kmax + 2 * n;
+    for (size_t i = 0; i < xy.size(); i++)
+      for (int s = 0; s < E - 2 * n - ks[i]; s++) xy[i] = {chk((__int128)2 * xy[i][1]), xy[i][0]};   // times sqrt2
+    while (E > 0) {
+      bool even = true;
+      for (const auto &v : xy) even = even && (v[0] % 2 == 0);
+      if (!even) break;
+      for (auto &v : xy) v = {v[1], v[0] / 2};                                                      // over sqrt2
+      E--;
+    }
+    out = "tcount-spec 1\nn " + std::to_string(n) + "\nchannel " + std::to_string(E) + "\n";
+    for (int a = 0; a < P; a++) {
+      for (int b = 0; b < P; b++)
+        out += (b ? " " : "") + std::to_string(xy[(size_t)a * P + b][0]) + " " + std::to_string(xy[(size_t)a * P + b][1]);
+      out += "\n";
+    }
+    // rotation tables: for each P_p (p >= 1) and Pauli c, (-1, 0) when they commute, else (r, sign) with
+    // i P_p P_c = sign P_r
+    out += "rotations " + std::to_string(P - 1) + "\n";
+    const Z iw{0, 0, 1, 0};
+    for (int p = 1; p < P; p++) {
+      for (int c = 0; c < P; c++) {
+        const Mat M1 = matmul(paulis[p], paulis[c]), M2 = matmul(paulis[c], paulis[p]);
+        int hr = -1, hs = 0;
+        if (M1.e != M2.e) {
+          std::vector<Z> M(M1.e.size());
+          for (size_t i = 0; i < M.size(); i++) M[i] = zmul(iw, M1.e[i]);
+          for (int r = 0; r < P && hr < 0; r++)
+            for (int sign : {1, -1}) {
+              bool eq = true;
+              for (size_t i = 0; i < M.size() && eq; i++) {
+                const Z &q = paulis[r].e[i];
+                eq = M[i] == Z{sign * q.a, sign * q.b, sign * q.c, sign * q.d};
+              }
+              if (eq) { hr = r; hs = sign; }
+            }
+          if (hr < 0) { err = "i P Q is not a signed Pauli"; return 2; }
+        }
+        out += (c ? " " : "") + std::to_string(hr) + " " + std::to_string(hs);
+      }
+      out += "\n";
+    }
+    out += "end\n";
+    return 0;
+  } catch (const std::overflow_error &e) {
+    err = e.what();
+    return 2;
+  }
+}
+
+}  // namespace cz

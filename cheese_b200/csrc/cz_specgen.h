@@ -1,0 +1,29 @@
+// Host-side spec generation: the target circuit -> the text spec of the gate-count search (what the reference's
+// python/cheese/spec.py writes, unitary targets) and the T-count spec (python/cheese/tcount.py:79-168), in exact
+// Z[w] arithmetic. The per-gate-set parts (candidates, window rules, CX table) are cached, so a served request pays
+// only for its target.
+#pragma once
+#include <string>
+#include <vector>
+
+namespace cz {
+
+struct CircGate {
+  std::string g;     // x y z s sdg t tdg h cx cz ccx
+  int nq = 0;
+  int q[3] = {-1, -1, -1};
+};
+
+// OpenQASM subset of the reference's parse_qasm (spec.py:113-123): "qreg name[n];" or "qubit[n];" sets the qubit
+// count, "g args;" with g a known gate adds it on the qubits [i] named in args; everything else is skipped
+int parse_qasm(const char *text, size_t len, int &n, std::vector<CircGate> &circ, std::string &err);
+
+struct SpecGenInfo { int candidates = 0, bad2 = 0, bad3 = 0; };
+// the gate-count spec of the circuit's unitary with budget `depth` (gate set: Clifford+T plus the circuit's own
+// gates); returns 0, or 2 with err (unknown gate, bad qubit, n out of range, coefficient overflow)
+int spec_generate(int n, const std::vector<CircGate> &circ, int depth, bool use_w3, std::string &out,
+                  SpecGenInfo &info, std::string &err);
+// the T-count spec (channel representation and Pauli rotation tables) of the circuit's unitary
+int tspec_generate(int n, const std::vector<CircGate> &circ, std::string &out, std::string &err);
+
+}  // namespace cz

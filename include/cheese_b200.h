@@ -153,6 +153,9 @@ typedef struct cz_server cz_server;
 #define CZ_REQ_GATES 0            /* text: a cheese spec; depth: budget (-1: the spec's) */
 #define CZ_REQ_TCOUNT 1           /* text: a tcount-spec */
 #define CZ_REQ_CLIFFORD 2         /* text: a cliffopt job */
+#define CZ_REQ_GATES_QASM 3       /* text: an OpenQASM target, its spec generated in the server (cz_spec_generate);
+                                     depth: budget (-1: the circuit's gate count) */
+#define CZ_REQ_TCOUNT_QASM 4      /* text: an OpenQASM target, its tcount-spec generated in the server */
 typedef struct {
   int device;
   double memory_gb;               /* device memory the gate-count batch may plan for */
@@ -313,6 +316,31 @@ typedef struct {
  * text receives the output lines after the JSON line: one gate per line, T gates as "t q" / "tdg q". */
 int cz_cliffopt(cz_engine *engine, const char *job, size_t len, int beam, cz_cliffopt_step_fn on_step, void *user,
                 char *text, size_t text_cap, cz_cliffopt_result *out);
+
+/* ---------------- spec generation (the reference's python/cheese/spec.py and tcount.py writers) ---------------- */
+typedef struct {
+  int n;                 /* qubits */
+  int gates;             /* gates of the target circuit */
+  int candidates;        /* candidate gates of the spec */
+  int w2_pairs, w3_triples;
+} cz_specgen_info;
+/* The gate-count spec of a target circuit with budget `depth`, as `python -m cheese.spec TARGET.qasm DEPTH
+ * [--no-w3]` writes it (spec.py:127-350, unitary targets): Clifford+T plus the circuit's own gates as candidates,
+ * the W2/W3 window rules, the target unitary, the cuts and the CX table. The W3 triples are listed by (first,
+ * second) gate and then by third gate (the reference lists the third gates of one (first, second) in Python set
+ * order); the set of triples is the same. The per-gate-set parts are cached across calls (thread safe).
+ * The circuit is either QASM text (the reference's parse_qasm subset, spec.py:113-123: qreg/qubit declaration,
+ * one known gate per statement) or, with qasm NULL, n qubits and ngates gates: names[i] with qubits
+ * qubits[3 i .. 3 i + arity). The text goes to out (cap bytes, NUL-terminated); out_len receives the length it
+ * needs without the NUL. Returns 0, 2 (bad circuit: err), or 3 (cap too small: nothing written).
+ * No compiled counterpart in the reference (its generator is Python). */
+int cz_spec_generate(const char *qasm, size_t qasm_len, int n, int ngates, const char *const *names,
+                     const int *qubits, int depth, int no_w3, char *out, size_t cap, size_t *out_len,
+                     cz_specgen_info *info, char *err, size_t errlen);
+/* The T-count spec of a target circuit, as `python -m cheese.tcount spec TARGET.qasm` writes it (tcount.py:79-168):
+ * the channel representation and the Pauli rotation tables. Arguments and returns as cz_spec_generate. */
+int cz_tspec_generate(const char *qasm, size_t qasm_len, int n, int ngates, const char *const *names,
+                      const int *qubits, char *out, size_t cap, size_t *out_len, char *err, size_t errlen);
 
 /* The library version string and the CUDA architecture it was compiled for ("sm_100a"). */
 const char *cz_version(void);

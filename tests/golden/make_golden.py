@@ -11,6 +11,8 @@ Writes
   tests/golden/cases.json               per case: spec, flags, exit code and the reference's stdout with every
                                         "seconds" value replaced by 0.00 (machine dependent, never compared)
   tests/golden/mitm_cases.json          the same for --mitm runs
+  tests/golden/spec_circuits.json       the reference's qasm targets (circuit, budget) and extra reference-written
+                                        specs (W3 off, ccx, cz / y gate sets) for the C++ spec generator
   tests/golden/table_cases.json         the same for --table K runs, each in a fresh working directory (so the
                                         reference builds its distance table and prints the "dir": "table" lines),
                                         plus the reference's stderr table line
@@ -70,6 +72,39 @@ MITM_CASES = [(f"toffoli-{d}-mitm", "toffoli", ["--depth", str(d), "--mitm"]) fo
     (f"table-rand-{i}-mitm", f"table-rand-{i}", ["--mitm"]) for i in range(8)]
 
 
+# targets whose reference-written spec files the C++ spec generator is checked against
+SPECGEN_TARGETS = ["cs", "ccz", "qft_2", "toffoli", "fredkin", "peres", "half_adder_3", "relative-phase-toffoli",
+                   "grover_3"]
+
+
+def specgen_cases(ref, write_spec):
+    """circuits of the reference's own qasm targets (parsed by its parse_qasm) with the budget of their committed
+    spec files, and a few specs the reference's generator writes for other gate sets (W3 off; with ccx, the "lite"
+    bounds; with cz and y)"""
+    from cheese import spec as refspec
+    out = {}
+    qdir = Path(ref) / "tests" / "qasm"
+    for stem in SPECGEN_TARGETS:
+        n, circ = refspec.parse_qasm(qdir / f"{stem}.qasm")
+        text = (GOLD / "specs" / f"{stem}.spec").read_text()
+        depth = int(text.split("\ndepth ")[1].split()[0])
+        out[stem] = {"n": n, "circuit": [[g, list(qs)] for g, qs in circ], "depth": depth,
+                     "qasm": (qdir / f"{stem}.qasm").read_text()}
+    extra = {
+        "toffoli-now3": (3, out["toffoli"]["circuit"], 9, False),
+        "ccx-lite": (3, [["ccx", [0, 1, 2]], ["h", [2]], ["t", [1]]], 5, True),
+        "cz-y": (2, [["cz", [0, 1]], ["y", [1]], ["h", [0]], ["t", [0]]], 5, True),
+        "ccx-lite-n4": (4, [["ccx", [0, 2, 3]], ["cx", [1, 0]]], 3, True),
+    }
+    for name, (n, circ, d, use3) in extra.items():
+        buf = io.StringIO()
+        refspec.write_spec(buf, n, [(g, tuple(q)) for g, q in circ], d, use3=use3)
+        (GOLD / "specs" / f"{name}.spec").write_text(buf.getvalue())
+        out[name] = {"n": n, "circuit": circ, "depth": d, "w3": use3}
+    (GOLD / "spec_circuits.json").write_text(json.dumps(out, indent=1) + "\n")
+    print(f"{len(out)} spec-generation cases written", file=sys.stderr)
+
+
 def mitm_cases(binp):
     out = []
     for name, stem, flags in MITM_CASES:
@@ -125,6 +160,7 @@ def main():
     ap.add_argument("--quick", action="store_true", help="skip the cases that take more than a few seconds")
     ap.add_argument("--table-only", action="store_true", help="write only the --table K cases")
     ap.add_argument("--mitm-only", action="store_true", help="write only the --mitm cases")
+    ap.add_argument("--specgen-only", action="store_true", help="write only the spec-generation cases")
     o = ap.parse_args()
     sys.dont_write_bytecode = True
     sys.path.insert(0, str(Path(o.ref) / "python"))
@@ -155,6 +191,9 @@ def main():
         return
     if o.mitm_only:
         mitm_cases(binp)
+        return
+    if o.specgen_only:
+        specgen_cases(o.ref, write_spec)
         return
     # target specs written by the reference generator (budget line = the first budget used)
     qdir = Path(o.ref) / "tests" / "qasm"
@@ -200,6 +239,7 @@ def main():
     print(f"{len(cases)} cases written", file=sys.stderr)
     table_cases(binp, write_spec)
     mitm_cases(binp)
+    specgen_cases(o.ref, write_spec)
 
 
 if __name__ == "__main__":

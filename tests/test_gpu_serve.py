@@ -67,3 +67,41 @@ def test_admission_under_a_small_budget(eng):
             assert got["rc"] == rc and got["text"] == want
     finally:
         srv.close()
+
+
+def test_qasm_requests(eng):
+    """OpenQASM targets: the server generates the spec / tcount-spec itself; answers equal the plain entry points on
+    the specs the reference's writer made"""
+    import json
+    from cheese_b200 import Server, tcwork, workloads
+    from conftest import GOLD, spec_text
+    circuits = json.loads((GOLD / "spec_circuits.json").read_text())
+    cases = [c for c in json.loads((GOLD / "cases.json").read_text()) if "circuit" in c][:10]
+    srv = Server(memory_gb=50)
+    try:
+        reqs = []
+        for c in cases:
+            text = spec_text(c["spec"])
+            n = int(text.split("\nn ")[1].split()[0])
+            reqs.append((0, workloads.qasm(n, [(g, tuple(q)) for g, q in c["circuit"]]), -1, text, None))
+        for name in ("cs", "ccz", "toffoli"):
+            c = circuits[name]
+            reqs.append((0, c["qasm"], c["depth"], spec_text(name), c["depth"]))
+            reqs.append((1, c["qasm"], -1, (GOLD / "tcount" / f"{name}.tspec").read_text(), None))
+        reqs.append((0, "OPENQASM 2.0;\nqreg q[2];\nfoo q[0];\nu9 q[1];\nh q[5];\n", 3, None, None))
+        ids = [srv.submit(3 if k == 0 else 4, q, d) for k, q, d, _, _ in reqs]
+        srv.wait(len(ids), 900)
+        for (k, q, d, want_text, dd), rid in zip(reqs, ids):
+            got = srv.poll(rid)
+            if want_text is None:
+                assert got["rc"] == 2 and "out of range" in got["error"]
+                continue
+            if k == 0:
+                r = eng.search(want_text, depth=dd if dd is not None else -1)
+                assert got["rc"] == r.rc and got["text"] == "".join(l + "\n" for l in r.lines())
+            else:
+                from test_gpu_tcount import lines
+                rc, levels, res = eng.tcount(want_text, table_k=4, cache_dir=None)
+                assert got["rc"] == rc and got["text"] == "".join(l + "\n" for l in lines(levels, rc, res))
+    finally:
+        srv.close()
