@@ -102,6 +102,8 @@ def test_qasm_requests(eng):
             else:
                 from test_gpu_tcount import lines
                 rc, levels, res = eng.tcount(want_text, table_k=4, cache_dir=None)
-                assert got["rc"] == rc and got["text"] == "".join(l + "\n" for l in lines(levels, rc, res))
+                # the table levels are printed by whichever engine builds the table first: compare the rest
+                nt = [l for l in got["text"].splitlines() if not l.startswith('{"dir": "table"')]
+                assert got["rc"] == rc and nt == [l for l in lines(levels, rc, res) if not l.startswith('{"dir": "table"')]
     finally:
         srv.close()
