@@ -162,6 +162,7 @@ def reference_arm(args, ws, rank):
 def systems(eng, args):
     """the batched, served and table-driven workloads beside the headline metric (one GPU)"""
     import statistics
+    import torch
     import cheese_b200 as cz
     from cheese_b200 import tcwork, workloads
     out = {}
@@ -231,9 +232,10 @@ def systems(eng, args):
     opt_ok = r.rc == 0 and len(r.circuit) == 15 and verify.equivalent(tsp["toffoli"], r.circuit)
     fred = {}
     for d in (15, 16):
+        free_gb = torch.cuda.mem_get_info()[0] / 1e9
         a = time.perf_counter()
         rf = eng_t.search(tsp["fredkin"], depth=d, table_k=8, cache_dir=None)
-        fred[str(d)] = {"rc": rf.rc, "s": time.perf_counter() - a, "error": rf.error}
+        fred[str(d)] = {"rc": rf.rc, "s": time.perf_counter() - a, "error": rf.error, "free_gb_before": free_gb}
     del eng_t
     tmp = Path(tempfile.mkdtemp())
     (tmp / "build").mkdir()

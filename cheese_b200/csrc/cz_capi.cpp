@@ -73,7 +73,10 @@ int cz_engine_create(int device, cz_engine **out, char *err, size_t errlen) {
 
 int64_t cz_engine_trim(cz_engine *engine) {
   if (!engine) return 0;
-  return (int64_t)engine->e->trim();
+  size_t n = engine->e->trim();
+  if (engine->tc) n += cz::tcount_context_trim(engine->tc);
+  if (engine->cl) n += cz::clifford_context_trim(engine->cl);
+  return (int64_t)n;
 }
 
 void cz_engine_destroy(cz_engine *engine) {

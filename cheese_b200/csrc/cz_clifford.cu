@@ -384,6 +384,15 @@ class CliffordContext {
                     &out, &len})
       b->release();
   }
+  size_t trim() {                              // work buffers back to the device; resident tables stay
+    size_t n = 0;
+    for (CBuf *b : {&cnt, &cost, &hist, &below, &nbelow, &blk, &blkoff, &part, &eql, &tabs, &bc, &pk, &pm, &tmp, &out,
+                    &len}) {
+      n += b->cap;
+      b->release();
+    }
+    return n;
+  }
   unsigned grid(unsigned long long n, int per = 8) const {
     return (unsigned)std::max<unsigned long long>(1, std::min<unsigned long long>((n + CL_T - 1) / CL_T,
                                                                                    (unsigned long long)nsm * per));
@@ -673,6 +682,11 @@ int parse_cliff_job(const char *text, size_t len, CliffJob &J, std::string &err)
 
 CliffordContext *clifford_context_create(int device, void *stream) { return new CliffordContext(device, stream); }
 void clifford_context_destroy(CliffordContext *c) { delete c; }
+size_t clifford_context_trim(CliffordContext *c) {
+  cudaSetDevice(c->dev);
+  cudaStreamSynchronize(c->s);
+  return c->trim();
+}
 
 int clifford_table(CliffordContext *c, int n, CliffTableInfo &info, std::string &err) {
   if (n < 1 || n > 3) { err = "n must be 1, 2 or 3"; return 3; }

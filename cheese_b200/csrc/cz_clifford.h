@@ -40,6 +40,8 @@ struct CliffOptResult {
 class CliffordContext;
 CliffordContext *clifford_context_create(int device, void *stream);
 void clifford_context_destroy(CliffordContext *c);
+// release the work buffers (kept at peak size between calls); resident tables stay; returns the bytes released
+size_t clifford_context_trim(CliffordContext *c);
 // the table of n qubits, resident after the first call: 0 or 5 (CUDA error) / 4 (group order mismatch)
 int clifford_table(CliffordContext *c, int n, CliffTableInfo &info, std::string &err);
 int cliffopt_run(CliffordContext *c, const CliffJob &job, int beam,

@@ -458,6 +458,14 @@ class TcountContext {
                    &kept, &hits})
       b->release();
   }
+  size_t trim() {                              // work buffers back to the device; resident tables stay
+    size_t n = 0;
+    for (Buf *b : {&bx, &by, &ix, &iy, &tr, &ts, &h1, &h2, &k0, &k1, &v0, &v1, &hist, &part, &work, &tmp, &kept, &hits}) {
+      n += b->cap;
+      b->release();
+    }
+    return n;
+  }
   size_t smem(int P) const { return tsm_bytes(P); }
   void check_ovf() {
     int v = 0;
@@ -817,6 +825,11 @@ int parse_tspec(const char *text, size_t len, TSpec &s, std::string &err) {
 
 TcountContext *tcount_context_create(int device, void *stream) { return new TcountContext(device, stream); }
 void tcount_context_destroy(TcountContext *c) { delete c; }
+size_t tcount_context_trim(TcountContext *c) {
+  cudaSetDevice(c->dev);
+  cudaStreamSynchronize(c->s);
+  return c->trim();
+}
 
 int tcount_run(TcountContext *ctx, const TSpec &sp, const TcOptions &opt,
                const std::function<void(const TcLevel &)> &on_level, TcResult &res) {

@@ -49,6 +49,8 @@ struct TcOptions {
 class TcountContext;                // device state of one engine: resident tables per (n, K)
 TcountContext *tcount_context_create(int device, void *stream);
 void tcount_context_destroy(TcountContext *);
+// release the work buffers (kept at peak size between calls); resident tables stay; returns the bytes released
+size_t tcount_context_trim(TcountContext *);
 int tcount_run(TcountContext *ctx, const TSpec &sp, const TcOptions &opt,
                const std::function<void(const TcLevel &)> &on_level, TcResult &res);
 
