@@ -231,11 +231,15 @@ def systems(eng, args):
     t_loop = time.perf_counter() - t0
     opt_ok = r.rc == 0 and len(r.circuit) == 15 and verify.equivalent(tsp["toffoli"], r.circuit)
     fred = {}
-    for d in (15, 16):
+    for d in (15, 16, 17):
         free_gb = torch.cuda.mem_get_info()[0] / 1e9
         a = time.perf_counter()
         rf = eng_t.search(tsp["fredkin"], depth=d, table_k=8, cache_dir=None)
         fred[str(d)] = {"rc": rf.rc, "s": time.perf_counter() - a, "error": rf.error, "free_gb_before": free_gb}
+        if rf.rc == 0:
+            fred[str(d)]["verified"] = bool(verify.equivalent(tsp["fredkin"], rf.circuit))
+            fred[str(d)]["gates"] = len(rf.circuit)
+        eng_t.trim()
     del eng_t
     tmp = Path(tempfile.mkdtemp())
     (tmp / "build").mkdir()
@@ -251,14 +255,15 @@ def systems(eng, args):
     t_cli = time.perf_counter() - t0
     out["table_gatecount"] = {
         "workload": "--table 8, 3 qubits, 27 Clifford+T candidates: Toffoli budgets 1..15 (optimum 15), Fredkin "
-                    "budgets 15 and 16 (proofs)",
+                    "budgets 15 and 16 (proofs) and 17 (optimum 17)",
         "table_classes": classes, "table_build_s": t_build,
         "toffoli_optimum_s": t_loop, "toffoli_budget14_s": budgets.get(14, (None, None))[1],
         "toffoli_budget15_s": budgets.get(15, (None, None))[1], "toffoli_optimum_verified": bool(opt_ok),
         "fredkin": fred,
         "toffoli_optimum_cli_s": t_cli, "cli_budgets": cli,
         "reference_published": "RTX 3060 Ti: K=8 table 17.9M classes in 30 s; Toffoli optimum 27 s (budget 14 1.5 s, "
-                               "15 11.1 s); Fredkin budget 15 11.3 s, 16 91 s (docs/PLAN.md:87-95)"}
+                               "15 11.1 s); Fredkin budget 15 11.3 s, 16 91 s, 17 out of memory at level 8 "
+                               "(docs/PLAN.md:87-95)"}
     # serving: seeded Poisson streams of the mixed workload, against the same requests run one by one
     N = args.serve_requests
     reqs = tcwork.serve_requests(eng, 5, N)

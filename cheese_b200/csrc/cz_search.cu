@@ -1284,6 +1284,16 @@ __global__ void k_keys_unpack(const KeyRec *r, long long n, uint64_t *s1, uint64
     s1[i] = x.h1; s2[i] = x.h2; si[i] = x.idx; sl[i] = x.lvl;
   }
 }
+// class keys of a materialized frontier from its survivor records: node j came from survivor slot vi[j], whose
+// keys the level kernels computed with the same class hash
+__global__ void k_keys_from_slots(const uint32_t *vi, long long n, const uint64_t *sh1, const uint64_t *sh2,
+                                  uint64_t *F1, uint64_t *F2) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
+    const uint32_t sl = vi[j];
+    F1[j] = sh1[sl];
+    F2[j] = sh2[sl];
+  }
+}
 // the (index, level) columns of the keys of one new table level: 0..n-1 and lvl
 __global__ void k_level_ids(uint32_t *idx, uint32_t *lv, long long n, uint32_t lvl) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -1387,15 +1397,52 @@ __global__ void k_drop_old(const uint64_t *kidx, const uint32_t *kslot, size_t n
       kslot2[p] = kslot[i];
     }
 }
-// node j of a frontier against the table: the first entry of its class key with level <= maxc, or -1
+// node j of a frontier against the table: the first entry of its class key with level <= maxc, or -1; the nodes
+// with a hit are listed (any order) with their entry
 __global__ void k_table_lookup(const uint64_t *F1, const uint64_t *F2, long long n, const uint64_t *S1,
-                               const uint64_t *S2, const uint32_t *Slvl, long long ns, int maxc, long long *hit) {
+                               const uint64_t *S2, const uint32_t *Slvl, long long ns, int maxc, longlong2 *hits,
+                               unsigned long long cap, unsigned long long *nhits) {
   for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
     long long r = -1;
     for (long long x = keys_lower(S1, ns, F1[j]); x < ns && S1[x] == F1[j]; x++)
       if (S2[x] == F2[j] && (int)Slvl[x] <= maxc) { r = x; break; }
-    hit[j] = r;
+    if (r >= 0) {
+      const unsigned long long i = atomicAdd(nhits, 1ULL);
+      if (i < cap) hits[i] = make_longlong2(j, r);
+    }
   }
+}
+// the tree arrays of a level whose residuals are not kept: node j is child kidx[j] = parent x GS + gate
+__global__ void k_tree_only(const uint64_t *kidx, long long n, int GS, uint32_t *par, uint8_t *gat) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long o = kidx[j];
+    par[j] = (uint32_t)(o / (unsigned long long)GS);
+    gat[j] = (uint8_t)(o % (unsigned long long)GS);
+  }
+}
+// one warp: the residual of child sidx = parent x GS + gate, from its parent's, and its exponent
+template <int NQ, typename ST>
+__global__ void k_child_residual(const __grid_constant__ DevSpec sp, const Z4<ST> *R, const NodeMeta *meta,
+                                 unsigned long long sidx, int GS, Z4<ST> *out, int *kout) {
+  constexpr int E = (1 << NQ) * (1 << NQ), EPL = E >= 32 ? E / 32 : 1;
+  __shared__ Z4<ST> P[E], C[E];
+  const int lane = threadIdx.x;
+  const unsigned long long p = sidx / (unsigned long long)GS;
+  const int g = (int)(sidx % (unsigned long long)GS);
+#pragma unroll
+  for (int q = 0; q < EPL; q++) {
+    const int e = lane + 32 * q;
+    if (e < E) P[e] = R[p * E + e];
+  }
+  __syncwarp();
+  bool ovf;
+  const int k = warp_child<NQ, ST>(P, C, g, meta[p].k, sp, &sp, lane, ovf);
+#pragma unroll
+  for (int q = 0; q < EPL; q++) {
+    const int e = lane + 32 * q;
+    if (e < E) out[e] = C[e];
+  }
+  if (lane == 0) *kout = k;
 }
 // one warp: every (entry x, symmetry s) from x0 on with s(E_x) == S exactly, in the reference's order
 // (cheese.cu:1570-1575); up to cap pairs into out
@@ -1738,7 +1785,9 @@ struct Engine::Impl {
   };
   std::map<std::string, DistTable *> dtabs;   // resident tables by cache path
   DistTable *building = nullptr;           // a table build: children are filtered against it, levels added to it
-  bool want_keys = false;                  // keep the frontier's class keys (fK1, fK2)
+  bool want_keys = false;
+  bool lean_level = false;                 // the last level of a levels() call keeps its tree and keys, not its
+                                           // residuals (the last searched level of --table K)                  // keep the frontier's class keys (fK1, fK2)
   DBuf fK1, fK2, tptrs, keys2, old;
   DevStats *hstats = nullptr;              // pinned
   long long launches = 0, expand_launches = 0, h2d = 0, d2h = 0;
@@ -1981,20 +2030,31 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
       if ((int)par.size() <= t) { par.resize(t + 1); gat.resize(t + 1); }
       par[t].ensure((size_t)distinct * 4);
       gat[t].ensure((size_t)distinct);
-      fR2.ensure((size_t)distinct * E * sizeof(Z4<ST>));
-      fMeta2.ensure((size_t)distinct * sizeof(NodeMeta));
-      const unsigned gg = (unsigned)std::max<size_t>(1, std::min<size_t>(((size_t)distinct + RES_WARPS - 1) / RES_WARPS,
-                                                                         (size_t)nsm * 16));
-      k_materialize<NQ, ST><<<gg, RES_WARPS * 32, 0, s>>>(sp, nullptr, nullptr, G, fR.as<Z4<ST>>(),
-                                                          fMeta.as<NodeMeta>(), ki, vi, (size_t)distinct,
-                                                          sMeta.as<NodeMeta>(), fR2.as<Z4<ST>>(),
-                                                          fMeta2.as<NodeMeta>(), par[t].as<uint32_t>(),
-                                                          gat[t].as<uint8_t>(), nullptr);
-      launches++;
-      ck(cudaGetLastError(), "gather");
-      std::swap(fR, fR2);
-      std::swap(fMeta, fMeta2);
-      if ((building || want_keys) && distinct) table_levels_keys<NQ>(sp, distinct);
+      if (lean_level && t == stop) {               // tree and keys only; the frontier stays the parents'
+        k_tree_only<<<gb, 256, 0, s>>>(ki, distinct, G, par[t].as<uint32_t>(), gat[t].as<uint8_t>());
+        launches++;
+        ck(cudaGetLastError(), "tree");
+      } else {
+        fR2.ensure((size_t)distinct * E * sizeof(Z4<ST>));
+        fMeta2.ensure((size_t)distinct * sizeof(NodeMeta));
+        const unsigned gg = (unsigned)std::max<size_t>(1, std::min<size_t>(((size_t)distinct + RES_WARPS - 1) / RES_WARPS,
+                                                                           (size_t)nsm * 16));
+        k_materialize<NQ, ST><<<gg, RES_WARPS * 32, 0, s>>>(sp, nullptr, nullptr, G, fR.as<Z4<ST>>(),
+                                                            fMeta.as<NodeMeta>(), ki, vi, (size_t)distinct,
+                                                            sMeta.as<NodeMeta>(), fR2.as<Z4<ST>>(),
+                                                            fMeta2.as<NodeMeta>(), par[t].as<uint32_t>(),
+                                                            gat[t].as<uint8_t>(), nullptr);
+        launches++;
+        ck(cudaGetLastError(), "gather");
+        std::swap(fR, fR2);
+        std::swap(fMeta, fMeta2);
+      }
+      if ((building || want_keys) && distinct) {   // the frontier's class keys, from its survivor records
+        fK1.ensure(distinct * 8 + 8); fK2.ensure(distinct * 8 + 8);
+        k_keys_from_slots<<<gb, 256, 0, s>>>(vi, distinct, sH1.as<uint64_t>(), sH2.as<uint64_t>(), fK1.as<uint64_t>(),
+                                             fK2.as<uint64_t>());
+        launches++;
+      }
       if (building && distinct) seen_add(*building, distinct, t);
       if (opt.profile) ck(cudaEventRecord(ev[3], s), "event");
       ck(cudaStreamSynchronize(s), "gather");
@@ -2363,40 +2423,67 @@ int Engine::Impl::run_table(const HostSpec &hs, const Options &opt, const std::f
   want_keys = true;
   int t_next = 1;
   for (int t = 0; t <= depth - K || t == 0; t++) {
+    bool lean = false;
     if (t > 0) {
+      lean_level = t == depth - K;      // the last level searched: its residuals are rebuilt only for candidates
       const int rc = levels<NQ, int32_t>(hs, sp, opt, depth, t_next, cb, res, t);
+      lean = lean_level;
+      lean_level = false;
       if (rc == -2) { want_keys = false; res.error = "coefficient overflow (int32) in table mode"; return RC_OVERFLOW; }
       if (rc != RC_STOP) { want_keys = false; return rc; }
     }
     // candidates: nodes of level t whose class is in the table within depth - t gates, cheapest first
     const long long n = front_m;
     const int maxc = depth - t;
-    tmp.ensure(n * 8 + 8);
+    const unsigned long long hcap = 1 << 16;
+    tmp.ensure(hcap * sizeof(longlong2) + 16);
+    unsigned long long *nh_d = (unsigned long long *)(tmp.as<longlong2>() + hcap);
+    ck(cudaMemsetAsync(nh_d, 0, 8, s), "memset");
     k_table_lookup<<<(unsigned)std::max<long long>(1, std::min<long long>((n + 255) / 256, (long long)nsm * 16)), 256, 0, s>>>(
         fK1.as<uint64_t>(), fK2.as<uint64_t>(), n, D->S1.as<uint64_t>(), D->S2.as<uint64_t>(), D->Slvl.as<uint32_t>(),
-        D->ns, maxc, tmp.as<long long>());
+        D->ns, maxc, tmp.as<longlong2>(), hcap, nh_d);
     launches++;
-    std::vector<long long> hit(n);
-    ck(cudaMemcpyAsync(hit.data(), tmp.p, n * 8, cudaMemcpyDeviceToHost, s), "d2h");
+    unsigned long long nh = 0;
+    ck(cudaMemcpyAsync(&nh, nh_d, 8, cudaMemcpyDeviceToHost, s), "d2h");
     ck(cudaStreamSynchronize(s), "table lookup");
-    std::vector<std::pair<int, long long>> cand;
-    for (long long j = 0; j < n; j++)
-      if (hit[j] >= 0) {
-        uint32_t lv = 0;
-        ck(cudaMemcpy(&lv, D->Slvl.as<uint32_t>() + hit[j], 4, cudaMemcpyDeviceToHost), "d2h");
-        cand.push_back({(int)lv, j});
-      }
+    if (nh > hcap) { want_keys = false; res.error = "table lookup: more than 65536 candidates"; return RC_CUDA; }
+    std::vector<longlong2> hl(nh);
+    if (nh) ck(cudaMemcpy(hl.data(), tmp.p, nh * sizeof(longlong2), cudaMemcpyDeviceToHost), "d2h");
+    std::vector<std::pair<std::pair<int, long long>, long long>> cand;   // ((table level, node), table entry)
+    for (const longlong2 &h : hl) {
+      uint32_t lv = 0;
+      ck(cudaMemcpy(&lv, D->Slvl.as<uint32_t>() + h.y, 4, cudaMemcpyDeviceToHost), "d2h");
+      cand.push_back({{(int)lv, h.x}, h.y});
+    }
     std::sort(cand.begin(), cand.end());
     const void *const *tp = upload_tree(D->par, D->gat, D->nl);
     DBuf outb;
-    outb.ensure(64 * sizeof(int2) + 16);
+    outb.ensure(64 * sizeof(int2) + 16 + E * sizeof(Z4<int32_t>) + 16);
+    Z4<int32_t> *cres = (Z4<int32_t> *)((char *)outb.p + 64 * sizeof(int2) + 16);
     for (const auto &cd : cand) {
-      const long long j = cd.second;
-      NodeMeta mj;
-      ck(cudaMemcpy(&mj, fMeta.as<NodeMeta>() + j, sizeof mj, cudaMemcpyDeviceToHost), "d2h");
-      k_table_confirm<NQ, int32_t><<<1, 32, 0, s>>>(sp, fR.as<Z4<int32_t>>() + j * E, mj.k, D->S1.as<uint64_t>(),
+      const long long j = cd.first.second, hitj = cd.second;
+      int kj = 0;
+      const Z4<int32_t> *Sj = fR.as<Z4<int32_t>>() + j * E;
+      if (lean) {                       // rebuild the node from its parent
+        uint32_t pp = 0;
+        uint8_t gg = 0;
+        ck(cudaMemcpy(&pp, par[t].as<uint32_t>() + j, 4, cudaMemcpyDeviceToHost), "d2h");
+        ck(cudaMemcpy(&gg, gat[t].as<uint8_t>() + j, 1, cudaMemcpyDeviceToHost), "d2h");
+        k_child_residual<NQ, int32_t><<<1, 32, 0, s>>>(sp, fR.as<Z4<int32_t>>(), fMeta.as<NodeMeta>(),
+                                                       (unsigned long long)pp * hs.G + gg, hs.G, cres,
+                                                       (int *)(outb.as<int2>() + 64) + 1);
+        launches++;
+        ck(cudaMemcpyAsync(&kj, (int *)(outb.as<int2>() + 64) + 1, 4, cudaMemcpyDeviceToHost, s), "d2h");
+        ck(cudaStreamSynchronize(s), "candidate");
+        Sj = cres;
+      } else {
+        NodeMeta mj;
+        ck(cudaMemcpy(&mj, fMeta.as<NodeMeta>() + j, sizeof mj, cudaMemcpyDeviceToHost), "d2h");
+        kj = mj.k;
+      }
+      k_table_confirm<NQ, int32_t><<<1, 32, 0, s>>>(sp, Sj, kj, D->S1.as<uint64_t>(),
                                                     D->S2.as<uint64_t>(), D->Sidx.as<uint32_t>(), D->Slvl.as<uint32_t>(),
-                                                    D->ns, hit[j], maxc, (const uint32_t *const *)tp,
+                                                    D->ns, hitj, maxc, (const uint32_t *const *)tp,
                                                     (const uint8_t *const *)(tp + D->nl + 1), outb.as<int2>(), 64,
                                                     (int *)(outb.as<int2>() + 64));
       launches++;
