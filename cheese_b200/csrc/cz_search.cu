@@ -1742,8 +1742,9 @@ uint64_t powmod_h(uint64_t a, uint64_t e) {
 
 // survivor records to provision for `children` children at an expected survivor rate: 1.5x the expectation
 // plus 4096, at least 1 Mi (never more than every child), at most 8 GiB of records
-inline unsigned long long survivor_room(unsigned long long children, double rate, size_t rec) {
-  const unsigned long long lim = ((unsigned long long)8 << 30) / rec;
+inline unsigned long long survivor_room(unsigned long long children, double rate, size_t rec,
+                                        size_t lim_bytes = (size_t)8 << 30) {
+  const unsigned long long lim = lim_bytes / rec;
   double want = 1.5 * rate * (double)children + 4096.0;
   if (want < (double)(1 << 20)) want = (double)(1 << 20);
   unsigned long long cap = want >= (double)children ? children : (unsigned long long)want;
@@ -1886,7 +1887,12 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
     // survivors capacity: the previous level's survivor rate with room to spare (at least 1 Mi records, at most
     // every child); when more survive, the level is redone once with the exact count (the kernel counts every
     // survivor, stored or not)
-    unsigned long long cap = keep ? survivor_room((unsigned long long)m * G, surv_rate, 40) : 0;
+    size_t lim_bytes = (size_t)8 << 30;         // above 8 GiB of records, up to 40 % of the free device memory
+    if (keep && 1.5 * surv_rate * (double)m * G * 40.0 > (double)lim_bytes) {
+      size_t fr = 0, tot = 0;
+      if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) lim_bytes = std::max(lim_bytes, (size_t)(0.4 * (double)fr));
+    }
+    unsigned long long cap = keep ? survivor_room((unsigned long long)m * G, surv_rate, 40, lim_bytes) : 0;
     DevStats *dst = stats.as<DevStats>();
     // deferred T evaluations: at most one entry per child of a gate whose T bound is not inherited
     int ncl = 0;
