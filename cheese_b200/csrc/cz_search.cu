@@ -100,7 +100,18 @@ template <typename ST> struct ExpandArgs {
   NodeMeta *smeta;
   TQEntry *tq;                     // deferred T evaluations (nullptr: in place)
   unsigned long long tqcap;
+  const struct GoalShort *gshort = nullptr;   // the level's goal pass (nullptr: none); a complete hit skips it
 };
+
+// The goal pass of a level: the parents whose stored lower bound is <= 1 (no other parent has a child equal to the
+// goal: its bounds are sound), listed with their children tested for the goal before the level runs. When it finds
+// the goal, the level is the found level: it prints no statistics line, so the bounds of its other children are
+// never needed.
+struct GoalShort {
+  unsigned long long count, found, first;   // candidates (all, even past the list's room), goal children, first one
+  unsigned int ovf, pad;
+};
+constexpr unsigned GOAL_LIST = 1u << 16;
 
 // ---------------- arithmetic helpers ----------------
 template <typename ST> __device__ __forceinline__ bool zz(const Z4<ST> &x) { return !(x.a | x.b | x.c | x.d); }
@@ -845,9 +856,70 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
   }
 }
 
+// goal pass, step 1: parents whose stored bounds allow a goal child (combine of H, T, CX and support <= 1)
+__global__ void k_goal_candidates(const NodeMeta *meta, long long m, uint32_t *list, GoalShort *gs) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < m; p += (long long)gridDim.x * blockDim.x) {
+    const NodeMeta pm = meta[p];
+    const int hs = (pm.hsn & 1) ? 2 : 0, h = pm.k > hs ? pm.k : hs;
+    if (combine(h, pm.T, pm.c2, __popc((pm.hsn >> 1) & 7)) > 1) continue;
+    const unsigned long long i = atomicAdd(&gs->count, 1ULL);
+    if (i < GOAL_LIST) list[i] = (uint32_t)p;
+  }
+}
+// goal pass, step 2 (one warp per candidate parent): its children past the window rules, tested for the goal
+template <int NQ, typename ST>
+__global__ void __launch_bounds__(EXP_WARPS * 32) k_goal_level(const DevSpec sp, const Z4<ST> *R, const NodeMeta *meta,
+                                                              const uint32_t *list, int GS, GoalShort *gs) {
+  constexpr int E = (1 << NQ) * (1 << NQ), EPL = E >= 32 ? E / 32 : 1;
+  __shared__ Z4<ST> sP[EXP_WARPS][E], sC[EXP_WARPS][E];
+  __shared__ DevSpec s_sp;
+  for (int i = threadIdx.x; i < (int)(sizeof(DevSpec) / 4); i += blockDim.x) ((int *)&s_sp)[i] = ((const int *)&sp)[i];
+  __syncthreads();
+  const unsigned long long n = gs->count;
+  if (n > GOAL_LIST) return;                   // the list is not complete: no shortcut for this level
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int G = s_sp.G;
+  unsigned long long found = 0, first = ~0ULL;
+  bool ovf = false;
+  for (unsigned long long i = blockIdx.x * (unsigned long long)EXP_WARPS + w; i < n;
+       i += (unsigned long long)gridDim.x * EXP_WARPS) {
+    const uint32_t p = list[i];
+    const NodeMeta pm = meta[p];
+    const int g1 = pm.g1 == 0xff ? -1 : pm.g1, g2 = pm.g2 == 0xff ? -1 : pm.g2;
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < EPL; q++) {
+      const int e = lane + 32 * q;
+      if (e < E) sP[w][e] = R[(size_t)p * E + e];
+    }
+    __syncwarp();
+    for (int g = 0; g < G; g++) {
+      if (g1 >= 0 && __ldg(&s_sp.bad2[g1 * G + g])) continue;
+      if (g2 >= 0) {
+        const uint32_t tri = ((uint32_t)g2 * G + (uint32_t)g1) * G + (uint32_t)g;
+        if ((__ldg(&s_sp.bad3[tri >> 5]) >> (tri & 31)) & 1) continue;
+      }
+      bool o;
+      const int k = warp_child<NQ, ST>(sP[w], sC[w], g, pm.k, s_sp, &s_sp, lane, o);
+      if (o) { ovf = true; continue; }
+      const Cheap ch = warp_cheap<NQ, ST>(sC[w], k, s_sp, lane, true, false, 0, 0);
+      if (ch.goal) {
+        found++;
+        const unsigned long long oi = (unsigned long long)p * GS + g;
+        if (oi < first) first = oi;
+      }
+    }
+  }
+  if (lane == 0) {
+    if (found) { atomicAdd(&gs->found, found); atomicMin(&gs->first, first); }
+    if (ovf) atomicExch(&gs->ovf, 1u);
+  }
+}
+
 template <int NQ, typename ST>
 __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, const ExpandArgs<ST> a) {
   constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
+  if (a.gshort && a.gshort->found && !a.gshort->ovf && a.gshort->count <= GOAL_LIST) return;   // the found level
   __shared__ ExpandSmem<NQ, ST> sm;
   __shared__ DevSpec s_sp;                     // the spec for out-of-line helpers (a shared address, no local copy)
   for (int i = threadIdx.x; i < (int)(sizeof(DevSpec) / 4); i += blockDim.x) ((int *)&s_sp)[i] = ((const int *)&sp)[i];
@@ -1761,6 +1833,7 @@ struct Engine::Impl {
   DBuf tq;                                 // deferred T evaluations of the current level
   DBuf k0, k1, v0, v1, hist, part;         // sort
   DBuf work, tmp, kidx, kslot;             // dedupe
+  DBuf gshort;                             // the goal pass: its counters and candidate list
   DBuf stats;
   struct SpecDev {                         // device copies of one parsed spec's tables
     uint64_t uid = 0;
@@ -1824,7 +1897,7 @@ struct Engine::Impl {
   size_t trim() {
     size_t n = 0;
     for (DBuf *b : {&fR, &fMeta, &fR2, &fMeta2, &sH1, &sH2, &sIdx, &sMeta, &tq, &k0, &k1, &v0, &v1, &hist, &part,
-                    &work, &tmp, &kidx, &kslot, &fK1, &fK2, &keys2, &old}) {
+                    &work, &tmp, &kidx, &kslot, &fK1, &fK2, &keys2, &old, &gshort}) {
       n += b->cap;
       b->release();
     }
@@ -1841,7 +1914,7 @@ struct Engine::Impl {
       b->release();
     for (auto &sd : specs) sd.release();
     for (auto &kv : dtabs) { kv.second->release(); delete kv.second; }
-    for (DBuf *b : {&fK1, &fK2, &tptrs, &keys2, &old}) b->release();
+    for (DBuf *b : {&fK1, &fK2, &tptrs, &keys2, &old, &gshort}) b->release();
     for (auto &b : par) b.release();
     for (auto &b : gat) b.release();
     side.release();
@@ -1898,6 +1971,22 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
     int ncl = 0;
     for (int g = 0; g < G; g++) ncl += !(hs.gflags[g] & GF_CLIFFORD);
     unsigned long long tqcap = (unsigned long long)m * (unsigned long long)std::max(1, ncl) + 1024;
+    // goal pass: the parents that may have a goal child, their children tested first (a hit makes this the found
+    // level and the level kernels return at once)
+    GoalShort *gsd = nullptr;
+    GoalShort hgs{0, 0, ~0ULL, 0, 0};
+    if (hs.standard && !sp.nogoal && m > 0) {
+      gshort.ensure(sizeof(GoalShort) + (size_t)GOAL_LIST * 4 + 64);
+      gsd = gshort.as<GoalShort>();
+      uint32_t *glist = (uint32_t *)(gsd + 1);
+      ck(cudaMemcpyAsync(gsd, &hgs, sizeof hgs, cudaMemcpyHostToDevice, s), "h2d");
+      const unsigned gm_ = (unsigned)std::max<long long>(1, std::min<long long>((m + 255) / 256, (long long)nsm * 8));
+      k_goal_candidates<<<gm_, 256, 0, s>>>(fMeta.as<NodeMeta>(), m, glist, gsd);
+      k_goal_level<NQ, ST><<<(unsigned)nsm * 2, EXP_WARPS * 32, 0, s>>>(sp, fR.as<Z4<ST>>(), fMeta.as<NodeMeta>(), glist,
+                                                                       G, gsd);
+      launches += 2;
+      ck(cudaGetLastError(), "goal pass");
+    }
     for (int attempt = 0; attempt < 2; attempt++) {
       if (keep) {
         sH1.ensure(cap * 8); sH2.ensure(cap * 8); sIdx.ensure(cap * 8);
@@ -1912,7 +2001,7 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
       a.R = fR.as<Z4<ST>>(); a.meta = fMeta.as<NodeMeta>(); a.st = dst; a.cap = cap;
       a.sh1 = sH1.as<uint64_t>(); a.sh2 = sH2.as<uint64_t>(); a.sidx = sIdx.as<uint64_t>();
       a.smeta = sMeta.as<NodeMeta>();
-      a.tq = tq.as<TQEntry>(); a.tqcap = tqcap;
+      a.tq = tq.as<TQEntry>(); a.tqcap = tqcap; a.gshort = gsd;
       const long long want = (m + EXP_WARPS - 1) / EXP_WARPS;
       const long long grid = std::max<long long>(1, std::min<long long>(want, (long long)nsm * 2 * 8));
       if (opt.profile) ck(cudaEventRecord(ev[0], s), "event");
@@ -1930,12 +2019,31 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
       ck(cudaMemcpyAsync(hstats, dst, sizeof(DevStats), cudaMemcpyDeviceToHost, s), "d2h");
       d2h += sizeof(DevStats);
       h2d += 8;
+      if (gsd) { ck(cudaMemcpyAsync(&hgs, gsd, sizeof hgs, cudaMemcpyDeviceToHost, s), "d2h"); d2h += sizeof hgs; }
       ck(cudaStreamSynchronize(s), "expand");
+      if (gsd && hgs.found && !hgs.ovf && hgs.count <= GOAL_LIST) break;   // the found level (kernels skipped)
       if (opt.profile) { float ms = 0; cudaEventElapsedTime(&ms, ev[0], ev[1]); res.expand_ms += ms; }
       if (hstats->ovf) return -2;                       // promote to int64 limbs and redo this level
       if (!hstats->surv_overflow && hstats->n_tq <= tqcap) break;
       cap = std::max<unsigned long long>(cap, hstats->n_surv);   // exact counts: grow and redo once
       tqcap = std::max<unsigned long long>(tqcap, hstats->n_tq);
+    }
+    if (gsd && hgs.found && !hgs.ovf && hgs.count <= GOAL_LIST) {   // found by the goal pass
+      const unsigned long long o = hgs.first;
+      std::vector<int> c(t);
+      c[t - 1] = (int)(o % G);
+      uint32_t i = (uint32_t)(o / G);
+      for (int l = t - 1; l >= 1; l--) {
+        uint8_t gg; uint32_t pp;
+        ck(cudaMemcpy(&gg, gat[l].as<uint8_t>() + i, 1, cudaMemcpyDeviceToHost), "d2h");
+        ck(cudaMemcpy(&pp, par[l].as<uint32_t>() + i, 4, cudaMemcpyDeviceToHost), "d2h");
+        c[l - 1] = gg; i = pp;
+        d2h += 5;
+      }
+      res.circuit = c;
+      res.n_found = (long long)hgs.found;
+      res.levels = t;
+      return RC_CIRCUIT;
     }
     if (hstats->n_tq > tqcap) { res.error = "T queue overflow"; return RC_CUDA; }
     if (hstats->surv_overflow) { res.error = "survivor buffer overflow"; return RC_CUDA; }
