@@ -186,7 +186,9 @@ def systems(eng, args):
                       "speedup": tp / tb, "mismatches": bad,
                       "launches": sum(b.info()["kernel_launches"] for b in sess.values()),
                       "steps": sum(b.info()["steps"] for b in sess.values())}
-    del sess, plain
+    for b in sess.values():
+        b.close()
+    del sess, plain, b
     # table-driven T count: Clifford BFS table + K = 4 coset table (3 qubits), then seeded queries, each verified
     t0 = time.perf_counter()
     ct = eng.clifford_table(3)

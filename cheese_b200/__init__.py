@@ -494,10 +494,14 @@ class Batch:
             raise RuntimeError(f"cz_batch_result failed: {rc}")
         return SearchOutcome(self.specs[jid], res.rc, levels, res)
 
-    def __del__(self):
+    def close(self):
+        """free the session's device buffers now"""
         if getattr(self, "_h", None) and _lib is not None:
             _lib.cz_batch_destroy(self._h)
             self._h = None
+
+    def __del__(self):
+        self.close()
 
 
 REQ_GATES, REQ_TCOUNT, REQ_CLIFFORD, REQ_GATES_QASM, REQ_TCOUNT_QASM = 0, 1, 2, 3, 4

@@ -971,7 +971,76 @@ template <typename ST> struct BatchArgs {
   NodeMeta *smeta;
   TQEntry *tq;
   unsigned long long tqcap;
+  const GoalShort *gshort = nullptr;  // the chunk's goal pass (nullptr: none) and its per-job results
+  const ulonglong2 *jgoal = nullptr;  // per job: goal children found by the pass, first of them
 };
+
+// the batch's goal pass: candidate parents (stored lower bound <= 1) of jobs whose spec has the bounds, in nodes
+// [p0, p1); then their children tested for the goal, per job
+__global__ void k_goal_candidates_batch(const NodeMeta *meta, const uint32_t *fjob, const DevSpec *specs, long long p0,
+                                        long long p1, uint32_t *list, GoalShort *gs) {
+  for (long long p = p0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; p < p1;
+       p += (long long)gridDim.x * blockDim.x) {
+    const DevSpec &sp = specs[fjob[p]];
+    if (!sp.standard || sp.nogoal) continue;
+    const NodeMeta pm = meta[p];
+    const int hs = (pm.hsn & 1) ? 2 : 0, h = pm.k > hs ? pm.k : hs;
+    if (combine(h, pm.T, pm.c2, __popc((pm.hsn >> 1) & 7)) > 1) continue;
+    const unsigned long long i = atomicAdd(&gs->count, 1ULL);
+    if (i < GOAL_LIST) list[i] = (uint32_t)p;
+  }
+}
+template <int NQ, typename ST>
+__global__ void __launch_bounds__(EXP_WARPS * 32) k_goal_level_batch(const DevSpec *specs, const uint32_t *fjob,
+                                                                    const Z4<ST> *R, const NodeMeta *meta,
+                                                                    const uint32_t *list, GoalShort *gs,
+                                                                    ulonglong2 *jgoal) {
+  constexpr int E = (1 << NQ) * (1 << NQ), EPL = E >= 32 ? E / 32 : 1;
+  __shared__ Z4<ST> sP[EXP_WARPS][E], sC[EXP_WARPS][E];
+  __shared__ DevSpec sps[EXP_WARPS];
+  const unsigned long long n = gs->count;
+  if (n > GOAL_LIST) return;                   // incomplete list: no shortcut in this chunk
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  DevSpec &sp = sps[w];
+  for (unsigned long long i = blockIdx.x * (unsigned long long)EXP_WARPS + w; i < n;
+       i += (unsigned long long)gridDim.x * EXP_WARPS) {
+    const uint32_t p = list[i];
+    const int job = (int)fjob[p];
+    __syncwarp();
+    for (int x = lane; x < (int)(sizeof(DevSpec) / 4); x += 32) ((int *)&sp)[x] = ((const int *)(specs + job))[x];
+    const NodeMeta pm = meta[p];
+    const int g1 = pm.g1 == 0xff ? -1 : pm.g1, g2 = pm.g2 == 0xff ? -1 : pm.g2;
+#pragma unroll
+    for (int q = 0; q < EPL; q++) {
+      const int e = lane + 32 * q;
+      if (e < E) sP[w][e] = R[(size_t)p * E + e];
+    }
+    __syncwarp();
+    const int G = sp.G;
+    unsigned long long found = 0, first = ~0ULL;
+    bool ovf = false;
+    for (int g = 0; g < G; g++) {
+      if (g1 >= 0 && __ldg(&sp.bad2[g1 * G + g])) continue;
+      if (g2 >= 0) {
+        const uint32_t tri = ((uint32_t)g2 * G + (uint32_t)g1) * G + (uint32_t)g;
+        if ((__ldg(&sp.bad3[tri >> 5]) >> (tri & 31)) & 1) continue;
+      }
+      bool o;
+      const int k = warp_child<NQ, ST>(sP[w], sC[w], g, pm.k, sp, &sp, lane, o);
+      if (o) { ovf = true; continue; }
+      const Cheap ch = warp_cheap<NQ, ST>(sC[w], k, sp, lane, true, false, 0, 0);
+      if (ch.goal) {
+        found++;
+        const unsigned long long oi = (unsigned long long)p * BATCH_GS + g;
+        if (oi < first) first = oi;
+      }
+    }
+    if (lane == 0) {
+      if (found) { atomicAdd(&jgoal[job].x, found); atomicMin(&jgoal[job].y, first); }
+      if (ovf) atomicExch(&gs->ovf, 1u);
+    }
+  }
+}
 
 template <int NQ, typename ST>
 __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand_batch(const BatchArgs<ST> a) {
@@ -987,8 +1056,9 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand_batch(const BatchA
   const ExpandOut<ST> o{a.st, a.cap, a.sh1, a.sh2, a.sidx, a.smeta, a.tq, a.tqcap};
   WarpTally c;
   int job = -1, rem = 0;
-  bool keep = false;
+  bool keep = false, skip = false;
   unsigned conjmask = 0;
+  const bool pass_ok = a.gshort && !a.gshort->ovf && a.gshort->count <= GOAL_LIST;
   for (;;) {
     unsigned long long p = 0;
     if (lane == 0) p = a.p0 + atomicAdd(&a.st->work, 1ULL);
@@ -998,6 +1068,8 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand_batch(const BatchA
     if (pj != job) {                             // another job: flush the tallies, load its spec
       if (job >= 0) c.flush(a.jst + job, lane);
       job = pj;
+      skip = pass_ok && a.jgoal[job].x > 0;      // the goal pass found this job's goal: its found level
+      if (skip) continue;
       __syncwarp();
       for (int i = lane; i < (int)(sizeof(DevSpec) / 4); i += 32) ((int *)&sp)[i] = ((const int *)(a.specs + job))[i];
       __syncwarp();
@@ -1007,6 +1079,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand_batch(const BatchA
       conjmask = 0;
       for (int i = 0; i < sp.nsym; i++) conjmask |= (unsigned)(sp.symconj[i] != 0) << i;
     }
+    if (skip) continue;
 #pragma unroll
     for (int j = 0; j < EPL; j++) {
       const int e = lane + 32 * j;
@@ -3381,6 +3454,7 @@ struct BatchImpl : BatchSession::Impl {
   DBuf dspecs, jt, jst, jact, jdist;
   DBuf fR, fMeta, fJob, fR2, fMeta2, fJob2;
   DBuf sH1, sH2, sIdx, sMeta, stats;       // survivors: 32-byte records
+  DBuf bgoal, jgoal;                       // the goal pass: counters + candidate list, per-job results
   DBuf tq;                                 // deferred T evaluations
   DBuf k0, k1, v0, v1, hist, part, work, tmp, kidx, kslot, cnt;
   DBuf rJob, rTk, tptr, wbuf;
@@ -3405,7 +3479,7 @@ struct BatchImpl : BatchSession::Impl {
     cudaSetDevice(eng.device());
     for (DBuf *b : {&dspecs, &jt, &jst, &jact, &jdist, &fR, &fMeta, &fJob, &fR2, &fMeta2, &fJob2, &sH1, &sH2, &sIdx,
                     &sMeta, &tq, &stats, &k0, &k1, &v0, &v1, &hist, &part, &work, &tmp, &kidx, &kslot, &cnt, &rJob,
-                    &rTk, &tptr, &wbuf})
+                    &rTk, &tptr, &wbuf, &bgoal, &jgoal})
       b->release();
     for (auto &b : tpar) b.release();
     for (auto &b : tgat) b.release();
@@ -3691,6 +3765,25 @@ struct BatchImpl : BatchSession::Impl {
         tqcap += (unsigned long long)J[i].seg * (unsigned long long)std::max(1, ncl);
       }
       DevStats h{};
+      // goal pass over the chunk: jobs whose goal it finds skip their found level in the level kernels
+      bgoal.ensure(sizeof(GoalShort) + (size_t)GOAL_LIST * 4 + 64);
+      jgoal.ensure((size_t)nj * sizeof(ulonglong2) + 16);
+      GoalShort *gsd = bgoal.as<GoalShort>();
+      ulonglong2 *jg = jgoal.as<ulonglong2>();
+      {
+        const GoalShort g0{0, 0, ~0ULL, 0, 0};
+        const std::vector<ulonglong2> z(jn, make_ulonglong2(0ULL, ~0ULL));
+        ck(cudaMemcpyAsync(gsd, &g0, sizeof g0, cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(jg + jlo, z.data(), jn * sizeof(ulonglong2), cudaMemcpyHostToDevice, s), "h2d");
+        const unsigned gc = (unsigned)std::max<long long>(1, std::min<long long>((cm + 255) / 256, (long long)nsm * 8));
+        k_goal_candidates_batch<<<gc, 256, 0, s>>>(fMeta.as<NodeMeta>(), fJob.as<uint32_t>(), dspecs.as<DevSpec>(),
+                                                   ch.p0, ch.p1, (uint32_t *)(gsd + 1), gsd);
+        k_goal_level_batch<NQ, ST><<<(unsigned)nsm * 2, EXP_WARPS * 32, 0, s>>>(
+            dspecs.as<DevSpec>(), fJob.as<uint32_t>(), fR.as<Z4<ST>>(), fMeta.as<NodeMeta>(), (uint32_t *)(gsd + 1), gsd,
+            jg);
+        nlaunch += 2;
+        ck(cudaGetLastError(), "goal pass");
+      }
       for (int attempt = 0; attempt < 2; attempt++) {
         tq.ensure(tqcap * sizeof(TQEntry));
         if (cap) {
@@ -3709,6 +3802,7 @@ struct BatchImpl : BatchSession::Impl {
         a.sh1 = sH1.as<uint64_t>(); a.sh2 = sH2.as<uint64_t>(); a.sidx = sIdx.as<uint64_t>();
         a.smeta = sMeta.as<NodeMeta>();
         a.tq = tq.as<TQEntry>(); a.tqcap = tqcap;
+        a.gshort = gsd; a.jgoal = jg;
         const long long want = (cm + EXP_WARPS - 1) / EXP_WARPS;
         const long long grid = std::max<long long>(1, std::min<long long>(want, (long long)nsm * 2 * 8));
         k_expand_batch<NQ, ST><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(a);
@@ -3729,7 +3823,14 @@ struct BatchImpl : BatchSession::Impl {
       if (h.surv_overflow || h.n_tq > tqcap) throw std::runtime_error("survivor or T queue overflow");
       ck(cudaMemcpyAsync(hj.data() + jlo, jst.as<DevStats>() + jlo, jn * sizeof(DevStats), cudaMemcpyDeviceToHost, s),
          "d2h");
+      GoalShort hgs{};
+      std::vector<ulonglong2> hjg(jn);
+      ck(cudaMemcpyAsync(&hgs, gsd, sizeof hgs, cudaMemcpyDeviceToHost, s), "d2h");
+      ck(cudaMemcpyAsync(hjg.data(), jg + jlo, jn * sizeof(ulonglong2), cudaMemcpyDeviceToHost, s), "d2h");
       ck(cudaStreamSynchronize(s), "job stats");
+      if (!hgs.ovf && hgs.count <= GOAL_LIST)            // jobs found by the goal pass (their level kernels skipped)
+        for (int i : ch.jobs)
+          if (hjg[i - jlo].x) { hj[i].found = hjg[i - jlo].x; hj[i].first_found = hjg[i - jlo].y; }
       std::vector<int> found_ids;
       size_t nsort = 0;
       for (int i : ch.jobs) {
