@@ -1861,10 +1861,11 @@ struct DBuf {
     if (p) ck(cudaFree(p), "free");
     p = nullptr;
     cap = 0;
-    // grow by half again for small buffers; exactly (2 MiB granules) once a buffer passes 1 GiB
+    // grow by half again below 1 GiB (small buffers in 256-byte steps, at least 64 KiB), exactly (2 MiB granules)
+    // once a buffer passes 1 GiB: a stream of growing requests reallocates a buffer only a few times
     size_t c = bytes >= ((size_t)1 << 30) ? bytes : std::max(bytes, old + old / 2);
-    c = (c + ((size_t)2 << 20) - 1) & ~(((size_t)2 << 20) - 1);
-    if (bytes < ((size_t)2 << 20)) c = (bytes + 255) & ~(size_t)255;
+    if (c < ((size_t)2 << 20)) c = std::max<size_t>((c + 255) & ~(size_t)255, (size_t)64 << 10);
+    else c = (c + ((size_t)2 << 20) - 1) & ~(((size_t)2 << 20) - 1);
     if (c >= ((size_t)64 << 20) && std::getenv("CZ_TRACE_ALLOC")) {   // large device allocations, for diagnosis
       size_t fr = 0, tot = 0;
       cudaMemGetInfo(&fr, &tot);
