@@ -159,6 +159,52 @@ def reference_arm(args, ws, rank):
         "e2e": {"value": v, "unit": "prefixes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
+def reference_gpu_tcount(eng):
+    """the reference's own sm_100a builds of tcount and cliffopt (oracle/_ref, compiled from its sources) on this
+    GPU, one process per query as its scripts run them, beside this library on the same inputs: the 3-qubit K = 4
+    coset table build, eight seeded T-count queries (table loaded from the cache file by each process), and six
+    zero-T Clifford-segment jobs (each reference process builds the 92,897,280-element table first)"""
+    import subprocess
+    import tempfile
+    tc, co = ROOT / "oracle" / "_ref" / "tcount-ref", ROOT / "oracle" / "_ref" / "cliffopt-ref"
+    if not tc.exists() or not co.exists():
+        return {"unavailable": "oracle/_ref/tcount-ref or cliffopt-ref not built (make -C oracle)"}
+    gold = ROOT / "tests" / "golden"
+    tmp = Path(tempfile.mkdtemp())
+    (tmp / "build").mkdir()
+    qs = [gold / "tcount" / f"q3-{i}.tspec" for i in range(8)]
+    out = {}
+    try:
+        t0 = time.perf_counter()
+        p = subprocess.run([str(tc), str(qs[0]), "--table", "4"], cwd=tmp, capture_output=True, text=True, timeout=900)
+        out["tcount_table_and_first_query_s"] = time.perf_counter() - t0
+        ok = p.returncode == 0
+        t0 = time.perf_counter()
+        for q in qs:
+            p = subprocess.run([str(tc), str(q), "--table", "4"], cwd=tmp, capture_output=True, text=True, timeout=900)
+            ok = ok and p.returncode == 0
+        out["tcount_per_query_s"] = (time.perf_counter() - t0) / len(qs)
+        out["tcount_ok"] = ok
+        t0 = time.perf_counter()
+        for q in qs:
+            eng.tcount(q.read_text(), table_k=4, cache_dir=None)
+        out["ours_tcount_per_query_s"] = (time.perf_counter() - t0) / len(qs)
+        jobs = [gold / "cliffopt" / f"c3-{i}.job" for i in range(6)]
+        t0 = time.perf_counter()
+        for j in jobs:
+            p = subprocess.run([str(co), str(j)], cwd=tmp, capture_output=True, text=True, timeout=900)
+            ok = ok and p.returncode == 0
+        out["cliffopt_per_job_s"] = (time.perf_counter() - t0) / len(jobs)
+        t0 = time.perf_counter()
+        for j in jobs:
+            eng.cliffopt(j.read_text())
+        out["ours_cliffopt_per_job_s"] = (time.perf_counter() - t0) / len(jobs)
+        out["ok"] = ok
+    except subprocess.TimeoutExpired as e:
+        out["unavailable"] = f"timed out: {e.cmd[0]}"
+    return out
+
+
 def systems(eng, args):
     """the batched, served and table-driven workloads beside the headline metric (one GPU)"""
     import statistics
@@ -210,6 +256,7 @@ def systems(eng, args):
                            "clifford_elements": ct["elements"], "coset_table_s": r0["table_seconds"],
                            "coset_table_cosets": r0["table_cosets"], "queries": nq, "queries_s": nq / t_q,
                            "ms_per_query": 1e3 * t_q / nq, "verified": ver}
+    out["table_tcount"]["reference_gpu"] = reference_gpu_tcount(eng)
     # distance table (--table 8, 17.9M classes): the optimum of Toffoli (15 gates, budgets 1..14 proved) and the
     # Fredkin proofs of budgets 15 and 16, through the library (table built once, resident) and as the reference's
     # run.sh does it (one drop-in process per budget, the table cached on disk by the first)
