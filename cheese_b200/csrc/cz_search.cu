@@ -647,22 +647,51 @@ __device__ __noinline__ void warp_class_key(const Z4<ST> *S, int k, int nsym, un
     h = fmix64(h ^ ((uint64_t)(int64_t)y.c * 0xc2b2ae3d27d4eb4fULL + (uint64_t)(int64_t)y.d));
     c1[j] = h; c2[j] = fmix64(h + 0x632be59bd9b4e019ULL);
   }
+  // the symmetries four at a time: per lane, the partial sums of the four images; then a reduce-scatter across the
+  // warp (lane bit 4 halves the four symmetries, bit 3 halves again, bits 2..0 finish the sums), so each lane ends
+  // with the full sums of one symmetry and finalises only that one; the minimum over lanes and groups is the key.
+  // The sums are the same sums mod 2^64 as one symmetry at a time, so the keys are the same.
   uint64_t b1 = ~0ULL, b2 = ~0ULL;
-  for (int s = 0; s < nsym; s++) {
-    const bool cj = (conjmask >> s) & 1;
-    uint64_t a = 0, b = 0;
+  const int hb = (lane >> 4) & 1, hc = (lane >> 3) & 1;
+  for (int g0 = 0; g0 < nsym; g0 += 4) {
+    uint64_t A[4], B[4];
 #pragma unroll
-    for (int j = 0; j < EPL; j++) {
-      const int e = lane + 32 * j;
-      if (e >= E) continue;
-      const int pos = perm[s][e >> NQ] * N + perm[s][e & (N - 1)];
-      a += (cj ? c1[j] : f1[j]) * W1[pos];
-      b += (cj ? c2[j] : f2[j]) * W2[pos];
+    for (int i = 0; i < 4; i++) {
+      A[i] = 0; B[i] = 0;
+      const int s = g0 + i;
+      if (s >= nsym) continue;
+      const bool cj = (conjmask >> s) & 1;
+#pragma unroll
+      for (int j = 0; j < EPL; j++) {
+        const int e = lane + 32 * j;
+        if (e >= E) continue;
+        const int pos = perm[s][e >> NQ] * N + perm[s][e & (N - 1)];
+        A[i] += (cj ? c1[j] : f1[j]) * W1[pos];
+        B[i] += (cj ? c2[j] : f2[j]) * W2[pos];
+      }
+    }
+    uint64_t A2[2], B2[2];
+#pragma unroll
+    for (int i = 0; i < 2; i++) {              // lanes with bit 4 clear keep symmetries 0, 1; the others 2, 3
+      const uint64_t sa = hb ? A[i] : A[i + 2], sb = hb ? B[i] : B[i + 2];
+      A2[i] = (hb ? A[i + 2] : A[i]) + __shfl_xor_sync(FULL, sa, 16);
+      B2[i] = (hb ? B[i + 2] : B[i]) + __shfl_xor_sync(FULL, sb, 16);
+    }
+    uint64_t a = (hc ? A2[1] : A2[0]) + __shfl_xor_sync(FULL, hc ? A2[0] : A2[1], 8);
+    uint64_t b = (hc ? B2[1] : B2[0]) + __shfl_xor_sync(FULL, hc ? B2[0] : B2[1], 8);
+#pragma unroll
+    for (int m = 4; m; m >>= 1) { a += __shfl_xor_sync(FULL, a, m); b += __shfl_xor_sync(FULL, b, m); }
+    const int s = g0 + 2 * hb + hc;             // the symmetry this lane now holds
+    uint64_t x1 = ~0ULL, x2 = ~0ULL;
+    if (s < nsym) {
+      x1 = fmix64(a + (uint64_t)k * 0xa0761d6478bd642fULL);
+      x2 = fmix64(b ^ ((uint64_t)k * 0xe7037ed1a0b428dbULL + 0x8ebc6af09c88c6e3ULL));
     }
 #pragma unroll
-    for (int m = 16; m; m >>= 1) { a += __shfl_xor_sync(FULL, a, m); b += __shfl_xor_sync(FULL, b, m); }
-    const uint64_t x1 = fmix64(a + (uint64_t)k * 0xa0761d6478bd642fULL);
-    const uint64_t x2 = fmix64(b ^ ((uint64_t)k * 0xe7037ed1a0b428dbULL + 0x8ebc6af09c88c6e3ULL));
+    for (int m = 16; m >= 8; m >>= 1) {
+      const uint64_t o1 = __shfl_xor_sync(FULL, x1, m), o2 = __shfl_xor_sync(FULL, x2, m);
+      if (o1 < x1 || (o1 == x1 && o2 < x2)) { x1 = o1; x2 = o2; }
+    }
     if (x1 < b1 || (x1 == b1 && x2 < b2)) { b1 = x1; b2 = x2; }
   }
   k1 = b1; k2 = b2;
