@@ -232,14 +232,20 @@ __global__ void __launch_bounds__(TC_T) k_tc_keys(const TDev sp, const THist H, 
   }
 }
 
-// child o = parent i * G + (p - 1): parent i of level tp, peeled by rotation p
+// child o = parent i * G + (p - 1): parent i of level tp, peeled by rotation p. With pmx, each parent's matrix and
+// exponent are kept (2 P^2 ints at pmx + 2 P^2 i, pe[i]) so the exact dedupe rebuilds a child with one peel.
 __global__ void __launch_bounds__(TC_T) k_tc_children(const TDev sp, const THist H, int tp, long long m, uint64_t *k1o,
-                                                      uint64_t *k2o, int *ovf) {
+                                                      uint64_t *k2o, int *ovf, int *pmx, int *pe) {
   const TSm s = tsm_carve(sp.P);
-  const int G = sp.G;
+  const int G = sp.G, PP = sp.P * sp.P;
   for (long long i = blockIdx.x; i < m; i += gridDim.x) {
     blk_path(H, tp, (uint32_t)i, s.seq);
     const int e = blk_build(s.ax, s.ay, sp, s.seq, tp, ovf);
+    if (pmx) {
+      int *dst = pmx + (size_t)i * 2 * PP;
+      for (int x = threadIdx.x; x < PP; x += blockDim.x) { dst[x] = s.ax[x]; dst[PP + x] = s.ay[x]; }
+      if (threadIdx.x == 0) pe[i] = e;
+    }
     for (int p = 1; p <= G; p++) {
       const int ec = blk_peel(s.ax, s.ay, e, s.bx, s.by, p, sp, ovf);
       uint64_t k1, k2;
@@ -266,9 +272,23 @@ __global__ void k_tc_runs(const uint64_t *keys, const uint32_t *vals, size_t n, 
 // one CTA per run of equal key prefixes: order by (h1, h2, index), keep the first member of every exact coset
 __global__ void __launch_bounds__(TC_T) k_tc_resolve(const TDev sp, const THist H, int tp, const uint2 *work,
                                                      const uint32_t *vals, const uint64_t *h1, const uint64_t *h2,
-                                                     uint32_t *tmp, uint64_t *kept, TcStats *st, int *ovf) {
+                                                     uint32_t *tmp, uint64_t *kept, TcStats *st, int *ovf,
+                                                     const int *pmx, const int *pe) {
   const TSm s = tsm_carve(sp.P);
-  const int G = sp.G;
+  const int G = sp.G, PP = sp.P * sp.P;
+  // child v of level tp + 1 into (mx, my): its parent's kept matrix peeled once, or rebuilt from the base
+  auto child = [&](uint32_t v, int *mx, int *my) {
+    if (pmx) {
+      const int *src = pmx + (size_t)(v / G) * 2 * PP;
+      for (int x = threadIdx.x; x < PP; x += blockDim.x) { mx[x] = src[x]; my[x] = src[PP + x]; }
+      __syncthreads();
+      return blk_peel(mx, my, pe[v / G], mx, my, (int)(v % G) + 1, sp, ovf);
+    }
+    blk_path(H, tp, v / G, s.seq);
+    if (threadIdx.x == 0) s.seq[tp] = (uint8_t)(v % G + 1);
+    __syncthreads();
+    return blk_build(mx, my, sp, s.seq, tp + 1, ovf);
+  };
   const unsigned long long nw = st->n_work;
   for (unsigned long long w = blockIdx.x; w < nw; w += gridDim.x) {
     const uint2 wk = work[w];
@@ -299,20 +319,14 @@ __global__ void __launch_bounds__(TC_T) k_tc_resolve(const TDev sp, const THist 
         const uint32_t t2 = tmp[start + i2];
         if (!(t2 & 0x80000000u)) continue;
         if (!built) {                                                 // the candidate into B
-          blk_path(H, tp, (vi & 0x7fffffffu) / G, s.seq);
-          if (threadIdx.x == 0) s.seq[tp] = (uint8_t)(vi % G + 1);
-          __syncthreads();
-          eb = blk_build(s.bx, s.by, sp, s.seq, tp + 1, ovf);
+          eb = child(vi & 0x7fffffffu, s.bx, s.by);
           uint64_t k1, k2;
           blk_colkey(s.bx, s.by, eb, sp.P, s.fb, s.sb, s.b1, s.b2, s, k1, k2);
           built = true;
         }
         if (loaded != (int)i2) {                                      // the kept member into A
           const uint32_t v2 = t2 & 0x7fffffffu;
-          blk_path(H, tp, v2 / G, s.seq);
-          if (threadIdx.x == 0) s.seq[tp] = (uint8_t)(v2 % G + 1);
-          __syncthreads();
-          ea = blk_build(s.ax, s.ay, sp, s.seq, tp + 1, ovf);
+          ea = child(v2, s.ax, s.ay);
           uint64_t k1, k2;
           blk_colkey(s.ax, s.ay, ea, sp.P, s.fa, s.sa, s.a1, s.a2, s, k1, k2);
           loaded = (int)i2;
@@ -446,6 +460,7 @@ class TcountContext {
   std::map<std::pair<int, int>, Table *> tables;   // resident: (n, K)
   Buf bx, by, ix, iy, tr, ts, ovf, stats;
   Buf h1, h2, k0, k1, v0, v1, hist, part, work, tmp, kept, hits;
+  Buf pmat, pexp;                                  // parents' matrices and exponents of the level being grown
   long long launches = 0;
   TcountContext(int d, void *stream) : dev(d), s((cudaStream_t)stream) {
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -455,12 +470,13 @@ class TcountContext {
     for (auto &kv : tables) { kv.second->D.release(); kv.second->S1.release(); kv.second->S2.release();
                               kv.second->Sidx.release(); kv.second->Slvl.release(); delete kv.second; }
     for (Buf *b : {&bx, &by, &ix, &iy, &tr, &ts, &ovf, &stats, &h1, &h2, &k0, &k1, &v0, &v1, &hist, &part, &work, &tmp,
-                   &kept, &hits})
+                   &kept, &hits, &pmat, &pexp})
       b->release();
   }
   size_t trim() {                              // work buffers back to the device; resident tables stay
     size_t n = 0;
-    for (Buf *b : {&bx, &by, &ix, &iy, &tr, &ts, &h1, &h2, &k0, &k1, &v0, &v1, &hist, &part, &work, &tmp, &kept, &hits}) {
+    for (Buf *b : {&bx, &by, &ix, &iy, &tr, &ts, &h1, &h2, &k0, &k1, &v0, &v1, &hist, &part, &work, &tmp, &kept, &hits,
+                   &pmat, &pexp}) {
       n += b->cap;
       b->release();
     }
@@ -492,7 +508,15 @@ class TcountContext {
     const long long m = T.n[tp], nc = m * G;
     if (nc >= (1LL << 32)) throw std::runtime_error("level too large for 32-bit child indices");
     h1.ensure(nc * 8); h2.ensure(nc * 8);
-    k_tc_children<<<grid(m), TC_T, smem(sp.P), s>>>(sp, T.hist(), tp, m, h1.as<uint64_t>(), h2.as<uint64_t>(), ovf.as<int>());
+    // the parents' matrices, kept for the exact dedupe (up to 16 GB; beyond, children are rebuilt from the base)
+    const size_t pm_bytes = (size_t)m * 2 * sp.P * sp.P * 4;
+    int *pmx = nullptr, *pe = nullptr;
+    if (pm_bytes <= ((size_t)16 << 30)) {
+      pmat.ensure(pm_bytes + 16); pexp.ensure((size_t)m * 4 + 16);
+      pmx = pmat.as<int>(); pe = pexp.as<int>();
+    }
+    k_tc_children<<<grid(m), TC_T, smem(sp.P), s>>>(sp, T.hist(), tp, m, h1.as<uint64_t>(), h2.as<uint64_t>(), ovf.as<int>(),
+                                                    pmx, pe);
     launches++;
     tck(cudaGetLastError(), "children kernel");
     check_ovf();
@@ -513,7 +537,7 @@ class TcountContext {
     k_tc_runs<<<gb, 256, 0, s>>>(sk, sv, n, kept.as<uint64_t>(), work.as<uint2>(), stats.as<TcStats>());
     k_tc_resolve<<<(unsigned)nsm * 4, TC_T, smem(sp.P), s>>>(sp, T.hist(), tp, work.as<uint2>(), sv, h1.as<uint64_t>(),
                                                              h2.as<uint64_t>(), tmp.as<uint32_t>(), kept.as<uint64_t>(),
-                                                             stats.as<TcStats>(), ovf.as<int>());
+                                                             stats.as<TcStats>(), ovf.as<int>(), pmx, pe);
     launches += 2;
     tck(cudaGetLastError(), "dedupe");
     TcStats hs{};
