@@ -269,6 +269,51 @@ __global__ void k_tc_runs(const uint64_t *keys, const uint32_t *vals, size_t n, 
   }
 }
 
+// keys sorted by all 64 bits of h1 (stable: index order within a run): the first member of every run is kept, every
+// other member is listed for a check against its run's first member
+__global__ void k_tc_split(const uint64_t *keys, const uint32_t *vals, size_t n, uint64_t *kept, uint32_t *check,
+                           TcStats *st) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    if (i == 0 || keys[i - 1] != keys[i]) kept[atomicAdd(&st->n_kept, 1ULL)] = vals[i];
+    else check[atomicAdd(&st->n_work, 1ULL)] = (uint32_t)i;
+  }
+}
+// one CTA per listed member: is it exactly the coset of its run's first member (equal h2 and the same multiset of
+// columns)? Children are rebuilt from their kept parents with one peel. A member that is not counts as unresolved:
+// the level is then deduped by the sequential resolver instead, which handles any mix of cosets in a run.
+__global__ void __launch_bounds__(TC_T) k_tc_dupcheck(const TDev sp, const uint64_t *keys, const uint32_t *vals,
+                                                      size_t n, const uint32_t *check, const uint64_t *h2,
+                                                      const int *pmx, const int *pe, TcStats *st,
+                                                      unsigned long long *unresolved, int *ovf) {
+  const TSm s = tsm_carve(sp.P);
+  const int G = sp.G, PP = sp.P * sp.P;
+  const unsigned long long nw = st->n_work;
+  auto child = [&](uint32_t v, int *mx, int *my) {
+    const int *src = pmx + (size_t)(v / G) * 2 * PP;
+    for (int x = threadIdx.x; x < PP; x += blockDim.x) { mx[x] = src[x]; my[x] = src[PP + x]; }
+    __syncthreads();
+    return blk_peel(mx, my, pe[v / G], mx, my, (int)(v % G) + 1, sp, ovf);
+  };
+  for (unsigned long long w = blockIdx.x; w < nw; w += gridDim.x) {
+    const uint32_t i = check[w];
+    const uint64_t key = keys[i];
+    size_t lo = 0, hi = i;                       // the run's first position: lower bound of the key
+    while (lo < hi) { const size_t mid = (lo + hi) / 2; if (keys[mid] < key) lo = mid + 1; else hi = mid; }
+    const uint32_t v0 = vals[lo], vi = vals[i];
+    bool same = h2[v0] == h2[vi];
+    if (same) {
+      const int ea = child(v0, s.ax, s.ay);
+      uint64_t k1, k2;
+      blk_colkey(s.ax, s.ay, ea, sp.P, s.fa, s.sa, s.a1, s.a2, s, k1, k2);
+      const int eb = child(vi, s.bx, s.by);
+      blk_colkey(s.bx, s.by, eb, sp.P, s.fb, s.sb, s.b1, s.b2, s, k1, k2);
+      same = blk_same(s, ea, eb, sp.P);
+    }
+    if (!same && threadIdx.x == 0) atomicAdd(unresolved, 1ULL);
+    __syncthreads();
+  }
+}
+
 // one CTA per run of equal key prefixes: order by (h1, h2, index), keep the first member of every exact coset
 __global__ void __launch_bounds__(TC_T) k_tc_resolve(const TDev sp, const THist H, int tp, const uint2 *work,
                                                      const uint32_t *vals, const uint64_t *h1, const uint64_t *h2,
@@ -520,30 +565,57 @@ class TcountContext {
     launches++;
     tck(cudaGetLastError(), "children kernel");
     check_ovf();
-    // dedupe: sort by the top 32 key bits, singletons kept, runs resolved exactly
+    // dedupe. With the parents' matrices kept: sort by all 64 bits of h1, keep each run's first member, and check
+    // every other member against it in parallel; only if some member is not an exact copy of its run's first (a
+    // hash collision) is the level deduped by the sequential resolver below, which is also the path without kept
+    // matrices: sort by the top 32 key bits, singletons kept, runs resolved exactly
     const size_t n = (size_t)nc;
     k0.ensure(n * 8); k1.ensure(n * 8); v0.ensure(n * 4); v1.ensure(n * 4);
     hist.ensure(sort_hist_words(n) * 4); part.ensure(scan_partials_words(sort_hist_words(n)) * 4);
-    work.ensure(n * sizeof(uint2)); tmp.ensure(n * 4); kept.ensure(n * 8); stats.ensure(sizeof(TcStats));
+    work.ensure(n * sizeof(uint2)); tmp.ensure(n * 4); kept.ensure(n * 8); stats.ensure(sizeof(TcStats) + 16);
     SortScratch sc{hist.as<uint32_t>(), part.as<uint32_t>(), hist.cap / 4, part.cap / 4};
     const unsigned gb = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)nsm * 16);
-    k_tc_seen_init<<<gb, 256, 0, s>>>(h1.as<uint64_t>(), n, k0.as<uint64_t>(), v0.as<uint32_t>());
-    const bool f = radix_sort(k0.as<uint64_t>(), v0.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(), n, 32, 64, sc,
-                              s, nullptr);
-    launches += 1 + 20;
-    const uint64_t *sk = f ? k1.as<uint64_t>() : k0.as<uint64_t>();
-    const uint32_t *sv = f ? v1.as<uint32_t>() : v0.as<uint32_t>();
-    tck(cudaMemsetAsync(stats.p, 0, sizeof(TcStats), s), "memset");
-    k_tc_runs<<<gb, 256, 0, s>>>(sk, sv, n, kept.as<uint64_t>(), work.as<uint2>(), stats.as<TcStats>());
-    k_tc_resolve<<<(unsigned)nsm * 4, TC_T, smem(sp.P), s>>>(sp, T.hist(), tp, work.as<uint2>(), sv, h1.as<uint64_t>(),
-                                                             h2.as<uint64_t>(), tmp.as<uint32_t>(), kept.as<uint64_t>(),
-                                                             stats.as<TcStats>(), ovf.as<int>(), pmx, pe);
-    launches += 2;
-    tck(cudaGetLastError(), "dedupe");
     TcStats hs{};
-    tck(cudaMemcpyAsync(&hs, stats.p, sizeof hs, cudaMemcpyDeviceToHost, s), "d2h");
-    tck(cudaStreamSynchronize(s), "dedupe");
-    check_ovf();
+    bool resolved = false;
+    if (pmx) {
+      unsigned long long *unres = (unsigned long long *)(stats.as<TcStats>() + 1);
+      k_tc_seen_init<<<gb, 256, 0, s>>>(h1.as<uint64_t>(), n, k0.as<uint64_t>(), v0.as<uint32_t>());
+      const bool f = radix_sort(k0.as<uint64_t>(), v0.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(), n, 0, 64,
+                                sc, s, nullptr);
+      launches += 1 + 40;
+      const uint64_t *sk = f ? k1.as<uint64_t>() : k0.as<uint64_t>();
+      const uint32_t *sv = f ? v1.as<uint32_t>() : v0.as<uint32_t>();
+      tck(cudaMemsetAsync(stats.p, 0, sizeof(TcStats) + 8, s), "memset");
+      k_tc_split<<<gb, 256, 0, s>>>(sk, sv, n, kept.as<uint64_t>(), tmp.as<uint32_t>(), stats.as<TcStats>());
+      k_tc_dupcheck<<<(unsigned)nsm * 8, TC_T, smem(sp.P), s>>>(sp, sk, sv, n, tmp.as<uint32_t>(), h2.as<uint64_t>(),
+                                                                pmx, pe, stats.as<TcStats>(), unres, ovf.as<int>());
+      launches += 2;
+      tck(cudaGetLastError(), "dedupe");
+      unsigned long long hu = 0;
+      tck(cudaMemcpyAsync(&hs, stats.p, sizeof hs, cudaMemcpyDeviceToHost, s), "d2h");
+      tck(cudaMemcpyAsync(&hu, unres, 8, cudaMemcpyDeviceToHost, s), "d2h");
+      tck(cudaStreamSynchronize(s), "dedupe");
+      check_ovf();
+      resolved = hu == 0;
+    }
+    if (!resolved) {
+      k_tc_seen_init<<<gb, 256, 0, s>>>(h1.as<uint64_t>(), n, k0.as<uint64_t>(), v0.as<uint32_t>());
+      const bool f = radix_sort(k0.as<uint64_t>(), v0.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(), n, 32, 64,
+                                sc, s, nullptr);
+      launches += 1 + 20;
+      const uint64_t *sk = f ? k1.as<uint64_t>() : k0.as<uint64_t>();
+      const uint32_t *sv = f ? v1.as<uint32_t>() : v0.as<uint32_t>();
+      tck(cudaMemsetAsync(stats.p, 0, sizeof(TcStats), s), "memset");
+      k_tc_runs<<<gb, 256, 0, s>>>(sk, sv, n, kept.as<uint64_t>(), work.as<uint2>(), stats.as<TcStats>());
+      k_tc_resolve<<<(unsigned)nsm * 4, TC_T, smem(sp.P), s>>>(sp, T.hist(), tp, work.as<uint2>(), sv, h1.as<uint64_t>(),
+                                                               h2.as<uint64_t>(), tmp.as<uint32_t>(), kept.as<uint64_t>(),
+                                                               stats.as<TcStats>(), ovf.as<int>(), pmx, pe);
+      launches += 2;
+      tck(cudaGetLastError(), "dedupe");
+      tck(cudaMemcpyAsync(&hs, stats.p, sizeof hs, cudaMemcpyDeviceToHost, s), "d2h");
+      tck(cudaStreamSynchronize(s), "dedupe");
+      check_ovf();
+    }
     const size_t nk = (size_t)hs.n_kept;
     // index order: radix sort of the kept child indices (< 2^32)
     const bool fk = radix_sort(kept.as<uint64_t>(), v0.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(), nk, 0, 32,
@@ -866,7 +938,7 @@ int tcount_run(TcountContext *ctx, const TSpec &sp, const TcOptions &opt,
     const int P = sp.P, lp = 2 * sp.n;
     const size_t sm = ctx->smem(P);
     for (const void *k : {(const void *)k_tc_keys, (const void *)k_tc_children, (const void *)k_tc_resolve,
-                          (const void *)k_tc_lookup})
+                          (const void *)k_tc_dupcheck, (const void *)k_tc_lookup})
       tck(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm), "smem attribute");
     ctx->bx.ensure(P * P * 4); ctx->by.ensure(P * P * 4); ctx->ix.ensure(P * P * 4); ctx->iy.ensure(P * P * 4);
     ctx->tr.ensure(P * P); ctx->ts.ensure(P * P); ctx->ovf.ensure(4);
