@@ -52,10 +52,6 @@ int main(int argc, char **argv) {
   }
   if (depth > CZ_MAX_DEPTH) { std::fprintf(stderr, "depth > %d\n", CZ_MAX_DEPTH); return 3; }
   std::fprintf(stderr, "cheese: n %d, %d candidates, depth %d, dedupe %d\n", n, G, depth, opt.dedupe);
-  if (spec && cz_spec_is_states(spec)) {
-    std::fprintf(stderr, "state targets: GPU path not ready yet, use build/cheese-cpu\n");
-    return 3;
-  }
   if (prc == CZ_ERR_USAGE || !spec) { std::fprintf(stderr, "n = %d not built (NQ_MIN..NQ_MAX)\n", n); return 3; }
   opt.depth = depth;
   opt.mitm = mitm;

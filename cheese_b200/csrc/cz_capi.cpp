@@ -153,11 +153,6 @@ int cz_search(cz_engine *engine, const cz_spec *spec, const cz_options *opt, cz_
   cz_options_default(&o);
   if (opt) o = *opt;
   const cz::HostSpec &hs = spec->hs;
-  if (hs.states) {
-    put_err(out->error, sizeof out->error, "state targets: GPU path not ready yet, use build/cheese-cpu");
-    out->rc = CZ_ERR_USAGE;
-    return CZ_ERR_USAGE;
-  }
   const int depth = o.depth >= 0 ? o.depth : hs.depth;
   if (depth > CZ_MAX_DEPTH) {
     put_err(out->error, sizeof out->error, "depth > " + std::to_string(CZ_MAX_DEPTH));

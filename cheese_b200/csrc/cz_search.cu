@@ -65,6 +65,8 @@ struct DevSpec {
   const int *cxtable;
   const int4 *ginv;                    // GMAX x 64 local inverse matrices (a, b, c, d as int32)
   const longlong2 *goal;               // N*N entries as (a, b), (c, d) pairs
+  int states, m;                       // state targets: m rows (images of the inputs) are searched for the goal rows
+  const int *ginfo;                    // state targets: per row the goal's sde, nullity and Schmidt rank per cut
 };
 
 // per frontier node: exponent, bounds carried to the children, last two gates (0xff: none), H structure (bit 0:
@@ -626,6 +628,181 @@ template <int NQ, typename ST> __device__ bool warp_goal(const Z4<ST> *S, int k,
   return __all_sync(FULL, ok);
 }
 
+// ---------------- state targets (rows j < m: the images of the inputs; cheese.cu:451-583) ----------------
+// H: the sde of a row changes by at most 1 per H. T: the stabilizer nullity of a row changes by at most 1 per T and
+// not at all under Cliffords. CX: the Schmidt rank of a row across a cut changes by at most a factor 2 per crossing
+// two-qubit gate. Ranks are exact (minors in int64 under a coefficient bound), as in the reference.
+template <typename ST> __device__ __forceinline__ Zw zw_of(const Z4<ST> &x) { return Zw{x.a, x.b, x.c, x.d}; }
+__device__ __forceinline__ int zval_dev(Zw x) {          // sqrt2-adic valuation, x != 0
+  int v = 0;
+  while (zdiv2ok(x)) { x = zdown(x); v++; if (v > 200) break; }
+  return v;
+}
+__device__ __forceinline__ int64_t zbig_dev(const Zw &x) {
+  int64_t m = 0, v;
+  v = x.a < 0 ? -x.a : x.a; if (v > m) m = v;
+  v = x.b < 0 ? -x.b : x.b; if (v > m) m = v;
+  v = x.c < 0 ? -x.c : x.c; if (v > m) m = v;
+  v = x.d < 0 ? -x.d : x.d; if (v > m) m = v;
+  return m;
+}
+template <typename ST> __device__ int state_row_sde(const Z4<ST> *row, int N, int k) {
+  int v = 1 << 30;
+  for (int x = 0; x < N; x++)
+    if (!zz(row[x])) { const int z = zval_dev(zw_of(row[x])); if (z < v) v = z; }
+  return v == (1 << 30) || k - v < 0 ? 0 : k - v;
+}
+__device__ __forceinline__ Zw zneg_dev(Zw x) { return Zw{-x.a, -x.b, -x.c, -x.d}; }
+// P_b |v> = +-|v>  <=>  <v|P_b|v> = +-<v|v>; P_b per qubit digit: 1 X, 2 Y, 3 Z
+template <typename ST> __device__ bool state_pauli_stab(const Z4<ST> *row, int nq, int b, Zw nrm) {
+  int f = 0, y = 0, z = 0;
+  for (int q = 0; q < nq; q++) {
+    const int d = (b >> (2 * q)) & 3;
+    if (d == 1 || d == 2) f |= 1 << q;
+    if (d == 2) y |= 1 << q;
+    if (d == 3) z |= 1 << q;
+  }
+  Zw acc{0, 0, 0, 0};
+  for (int x = 0; x < (1 << nq); x++) {
+    const Z4<ST> u = row[x ^ f], v = row[x];
+    if (zz(u) || zz(v)) continue;
+    const int ph = (2 * __popc(y) + 4 * __popc(x & (y | z))) & 7;
+    acc = zadd(acc, zmul(zconj(zw_of(u)), zmul(zw_of(v), zwpow(ph))));
+  }
+  return zeq(acc, nrm) || zeq(acc, zneg_dev(nrm));
+}
+__device__ Zw state_det(const Zw *M, int r, int stride) {        // r <= 4: Laplace along the first row
+  if (r == 1) return M[0];
+  if (r == 2) return zsub(zmul(M[0], M[stride + 1]), zmul(M[1], M[stride]));
+  Zw acc{0, 0, 0, 0};
+  Zw sub[9];
+  for (int j = 0; j < r; j++) {
+    if (zzero(M[j])) continue;
+    int t = 0;
+    for (int i = 1; i < r; i++)
+      for (int c = 0; c < r; c++)
+        if (c != j) sub[t++] = M[i * stride + c];
+    Zw d3;
+    if (r - 1 == 2) d3 = zsub(zmul(sub[0], sub[3]), zmul(sub[1], sub[2]));
+    else {                                                         // r - 1 == 3
+      d3 = Zw{0, 0, 0, 0};
+      for (int jj = 0; jj < 3; jj++) {
+        if (zzero(sub[jj])) continue;
+        Zw m2[4];
+        int u = 0;
+        for (int i = 1; i < 3; i++)
+          for (int c = 0; c < 3; c++)
+            if (c != jj) m2[u++] = sub[i * 3 + c];
+        const Zw d2 = zmul(sub[jj], zsub(zmul(m2[0], m2[3]), zmul(m2[1], m2[2])));
+        d3 = (jj & 1) ? zsub(d3, d2) : zadd(d3, d2);
+      }
+    }
+    const Zw d = zmul(M[j], d3);
+    acc = (j & 1) ? zsub(acc, d) : zadd(acc, d);
+  }
+  return acc;
+}
+// exact Schmidt rank of the row reshaped (qubits A, |A| = sa) x (the rest); -1 if the coefficients are too large
+template <typename ST> __device__ int state_row_rank(const Z4<ST> *row, int nq, int A, int sa) {
+  const int R = 1 << sa, C = 1 << (nq - sa), N = 1 << nq;
+  Zw M[4 * 16];
+  int64_t B = 0;
+  for (int x = 0; x < N; x++) {
+    int ia = 0, ib = 0, na = 0, nb = 0;
+    for (int q = 0; q < nq; q++) {
+      if ((A >> q) & 1) ia |= ((x >> q) & 1) << na++;
+      else ib |= ((x >> q) & 1) << nb++;
+    }
+    M[ia * C + ib] = zw_of(row[x]);
+    const int64_t v = zbig_dev(zw_of(row[x]));
+    if (v > B) B = v;
+  }
+  const int64_t lim[5] = {0, 1LL << 40, 1LL << 29, 1LL << 18, 1LL << 12};
+  for (int r = R < C ? R : C; r >= 2; r--) {
+    if (B >= lim[r]) return -1;
+    int rs[4], cs[4];
+    for (int rm = 0; rm < (1 << R); rm++) {
+      if (__popc(rm) != r) continue;
+      int t = 0;
+      for (int i = 0; i < R; i++) if ((rm >> i) & 1) rs[t++] = i;
+      for (int cm = 0; cm < (1 << C); cm++) {
+        if (__popc(cm) != r) continue;
+        int u = 0;
+        for (int i = 0; i < C; i++) if ((cm >> i) & 1) cs[u++] = i;
+        Zw sub[16];
+        for (int i = 0; i < r; i++)
+          for (int j = 0; j < r; j++) sub[i * r + j] = M[rs[i] * C + cs[j]];
+        if (!zzero(state_det(sub, r, r))) return r;
+      }
+    }
+  }
+  for (int x = 0; x < N; x++) if (!zz(row[x])) return 1;
+  return 0;
+}
+__device__ __forceinline__ int state_rank_need(int rv, int rt) {  // fewest crossing two-qubit gates between ranks
+  if (rv < 0 || rt <= 0 || rv == 0) return 0;
+  const int lo = rv < rt ? rv : rt, hi = rv < rt ? rt : rv;
+  int c = 0;
+  while ((lo << c) < hi) c++;
+  return c;
+}
+__device__ __forceinline__ int warp_imax(int v) {
+  for (int m = 16; m; m >>= 1) { const int o = __shfl_xor_sync(FULL, v, m); if (o > v) v = o; }
+  return v;
+}
+// H and CX bounds of a state residual: h = max over rows of |sde - goal sde|, c2 from the per-cut rank needs
+template <int NQ, typename ST> __device__ __noinline__ void warp_state_cheap(const Z4<ST> *S, int k, const DevSpec &sp, int lane,
+                                                                int &h, int &c2) {
+  constexpr int N = 1 << NQ;
+  const int W = 2 + sp.ncuts;
+  int d = 0;
+  if (lane < sp.m) { d = state_row_sde(S + lane * N, N, k) - sp.ginfo[lane * W]; if (d < 0) d = -d; }
+  h = warp_imax(d);
+  int mine[CUTMAX];
+  for (int c = 0; c < CUTMAX; c++) mine[c] = 0;
+  for (int it = lane; it < sp.m * sp.ncuts; it += 32) {
+    const int j = it / sp.ncuts, c = it % sp.ncuts;
+    const int nd = state_rank_need(state_row_rank(S + j * N, NQ, sp.cutmask[c], sp.cutsize[c]), sp.ginfo[j * W + 2 + c]);
+    if (nd > mine[c]) mine[c] = nd;
+  }
+  int idx = 0, mult = 1, mx = 0;
+  for (int c = 0; c < sp.ncuts; c++) {
+    int nd = warp_imax(mine[c]);
+    if (nd > sp.rad[c] - 1) nd = sp.rad[c] - 1;
+    idx += nd * mult;
+    mult *= sp.rad[c];
+    if (nd > mx) mx = nd;
+  }
+  c2 = sp.have_table ? sp.cxtable[idx] : mx;
+}
+// T bound of a state residual: max over rows of |stabilizer nullity - the goal's|
+template <int NQ, typename ST> __device__ __noinline__ int warp_state_t(const Z4<ST> *S, const DevSpec &sp, int lane) {
+  constexpr int N = 1 << NQ, PP = 1 << (2 * NQ);
+  int best = 0;
+  for (int j = 0; j < sp.m; j++) {
+    const Z4<ST> *row = S + j * N;
+    int64_t B = 0;
+    Zw nrm{0, 0, 0, 0};
+    for (int x = 0; x < N; x++) {
+      const int64_t v = zbig_dev(zw_of(row[x]));
+      if (v > B) B = v;
+      if (!zz(row[x])) nrm = zadd(nrm, zmul(zconj(zw_of(row[x])), zw_of(row[x])));
+    }
+    if (B >= (1LL << 27)) continue;                                   // int64-safe products only
+    int cnt = 0;
+    for (int b0 = 0; b0 < PP; b0 += 32) {
+      const int b = b0 + lane;
+      cnt += __popc(__ballot_sync(FULL, b < PP && state_pauli_stab(row, NQ, b, nrm)));
+    }
+    int r = 0;
+    while ((2 << r) <= cnt) r++;
+    int d = (NQ - r) - sp.ginfo[j * (2 + sp.ncuts) + 1];
+    if (d < 0) d = -d;
+    if (d > best) best = d;
+  }
+  return best;
+}
+
 // class key: the smallest (h1, h2) over the symmetry orbit of S; per orbit element a position-weighted sum of
 // per-entry hashes (the key only has to be class-invariant: classes are always compared exactly)
 template <int NQ, typename ST>
@@ -747,7 +924,7 @@ template <typename ST> struct ExpandOut {
 // every child of parent p (residual already in P): window rules, exact prechecks, child residual, bounds, class key,
 // survivor append. sp is the parent's spec (kernel parameter or a shared copy), sps its shared-memory address for
 // the out-of-line helpers; child index = p * GS + g.
-template <int NQ, typename ST>
+template <int NQ, typename ST, bool STATES = false>
 __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *sps, const uint8_t (*perm)[8],
                                               unsigned conjmask, const uint64_t *W1, const uint64_t *W2,
                                               const Z4<ST> *P, Z4<ST> *C, unsigned long long p, const NodeMeta pm,
@@ -758,7 +935,7 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
   const int g1 = pm.g1 == 0xff ? -1 : pm.g1, g2 = pm.g2 == 0xff ? -1 : pm.g2;
   const int kP = pm.k, TP = pm.T, c2P = pm.c2, hsP = (pm.hsn & 1) ? 2 : 0, ntP = (pm.hsn >> 1) & 7;
   const int suppP = __popc(ntP);
-  const bool pre_ok = sp.standard && kP < INHERIT_KMAX;
+  const bool pre_ok = sp.standard && !sp.states && kP < INHERIT_KMAX;
   unsigned tcache = 0;                       // per qubit: 1 + T bound of its odd-diagonal child (0: unknown)
   unsigned long long pend[3] = {0, 0, 0};    // per qubit: 1 + queue entry of its deferred odd-diagonal child
   // queue a deferred T evaluation: a second odd diagonal on the same qubit joins its sibling's entry
@@ -813,9 +990,9 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
     c.full++;
     const int k = warp_child<NQ, ST>(P, C, g, kP, sp, sps, lane, ovf);
     if (ovf) { c.ovf = true; continue; }
-    const bool need_b = sp.standard != 0;
+    const bool need_b = sp.standard != 0 && !sp.states;
     const bool need_hs = need_b && !(fl & GF_MONAFF);
-    // the child is the goal only if the parent equals the gate, i.e. acts on no other qubit
+    // the child is the goal only if the parent equals the gate, i.e. acts on no other qubit (unitary targets)
     const Cheap ch = warp_cheap<NQ, ST>(C, k, sp, lane, (ntP & ~gm) == 0 || !need_b, need_hs, need_b ? gm : 0, ntP);
     if (ch.goal) {
       if (sp.nogoal) c.dead++;
@@ -826,7 +1003,17 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
     const bool cacheT = (fl & GF_TDIAG) && k <= INHERIT_KMAX;
     bool alive = true;
     int T = 0, c2 = 0, hs = 0, needs = 0;
-    if (sp.lite) {
+    if constexpr (STATES) {                    // state targets (cheese.cu:683-716): no inherited bounds
+      if (sp.standard || sp.lite) {
+        int h = k;
+        if (!sp.lite) warp_state_cheap<NQ, ST>(C, k, *sps, lane, h, c2);
+        if (combine(h, 0, c2, 0) > rem) alive = false;
+        else {
+          T = warp_state_t<NQ, ST>(C, *sps, lane); c.teval++;
+          alive = combine(h, T, c2, 0) <= rem;
+        }
+      }
+    } else if (sp.lite) {
       if (k > rem) alive = false;
       else {
         if (inheritT) T = TP;
@@ -945,7 +1132,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32) k_goal_level(const DevSpec sp,
   }
 }
 
-template <int NQ, typename ST>
+template <int NQ, typename ST, bool STATES = false>
 __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, const ExpandArgs<ST> a) {
   constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
   if (a.gshort && a.gshort->found && !a.gshort->ovf && a.gshort->count <= GOAL_LIST) return;   // the found level
@@ -973,7 +1160,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, 
     }
     const NodeMeta pm = a.meta[p];
     __syncwarp();
-    expand_parent<NQ, ST>(sp, &s_sp, sm.perm, conjmask, sm.W1, sm.W2, P, C, p, pm, a.rem, a.keep != 0, sp.G, o, c,
+    expand_parent<NQ, ST, STATES>(sp, &s_sp, sm.perm, conjmask, sm.W1, sm.W2, P, C, p, pm, a.rem, a.keep != 0, sp.G, o, c,
                           lane);
     __syncwarp();
   }
@@ -1011,7 +1198,7 @@ __global__ void k_goal_candidates_batch(const NodeMeta *meta, const uint32_t *fj
   for (long long p = p0 + blockIdx.x * (long long)blockDim.x + threadIdx.x; p < p1;
        p += (long long)gridDim.x * blockDim.x) {
     const DevSpec &sp = specs[fjob[p]];
-    if (!sp.standard || sp.nogoal) continue;
+    if (!sp.standard || sp.states || sp.nogoal) continue;
     const NodeMeta pm = meta[p];
     const int hs = (pm.hsn & 1) ? 2 : 0, h = pm.k > hs ? pm.k : hs;
     if (combine(h, pm.T, pm.c2, __popc((pm.hsn >> 1) & 7)) > 1) continue;
@@ -1941,8 +2128,10 @@ struct Engine::Impl {
   struct SpecDev {                         // device copies of one parsed spec's tables
     uint64_t uid = 0;
     long long used = 0;
-    DBuf ginv, bad2, bad3, cxt, goal;
-    void release() { ginv.release(); bad2.release(); bad3.release(); cxt.release(); goal.release(); uid = 0; }
+    DBuf ginv, bad2, bad3, cxt, goal, ginfo;
+    void release() {
+      ginv.release(); bad2.release(); bad3.release(); cxt.release(); goal.release(); ginfo.release(); uid = 0;
+    }
   };
   SpecDev specs[8];
   long long use_clock = 0;
@@ -2078,7 +2267,7 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
     // level and the level kernels return at once)
     GoalShort *gsd = nullptr;
     GoalShort hgs{0, 0, ~0ULL, 0, 0};
-    if (hs.standard && !sp.nogoal && m > 0) {
+    if (hs.standard && !hs.states && !sp.nogoal && m > 0) {
       gshort.ensure(sizeof(GoalShort) + (size_t)GOAL_LIST * 4 + 64);
       gsd = gshort.as<GoalShort>();
       uint32_t *glist = (uint32_t *)(gsd + 1);
@@ -2108,7 +2297,8 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
       const long long want = (m + EXP_WARPS - 1) / EXP_WARPS;
       const long long grid = std::max<long long>(1, std::min<long long>(want, (long long)nsm * 2 * 8));
       if (opt.profile) ck(cudaEventRecord(ev[0], s), "event");
-      k_expand<NQ, ST><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(sp, a);
+      if (hs.states) k_expand<NQ, ST, true><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(sp, a);
+      else k_expand<NQ, ST, false><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(sp, a);
       TBoundArgs<ST> tb;
       tb.R = fR.as<Z4<ST>>(); tb.meta = fMeta.as<NodeMeta>(); tb.tq = tq.as<TQEntry>(); tb.tqcap = tqcap;
       tb.GS = G; tb.rem = depth - t; tb.keep = keep; tb.fjob = nullptr; tb.specs = nullptr; tb.jt = nullptr;
@@ -3028,6 +3218,17 @@ DevSpec devspec_host(const HostSpec &hs, const SymGroup &grp, int depth, bool no
       gl[2 * (r * N + c)] = make_longlong2(r == c ? 1 : 0, 0);
       gl[2 * (r * N + c) + 1] = make_longlong2(0, 0);
     }
+  sp.states = hs.states;
+  sp.m = hs.states ? hs.m : N;
+  if (hs.states) {                     // the goal: the reference's rows over sqrt2^gk, compared exactly
+    sp.goal_id = 0;
+    sp.gk = hs.gk;
+    for (int e = 0; e < E; e++) {
+      const Zw z = hs.goal[e];
+      gl[2 * e] = make_longlong2(z.a, z.b);
+      gl[2 * e + 1] = make_longlong2(z.c, z.d);
+    }
+  }
   return sp;
 }
 
@@ -3050,6 +3251,9 @@ DevSpec Engine::Impl::prepare(const HostSpec &hs, const SymGroup &grp, int depth
     if (!hs.cxtable.empty())
       ck(cudaMemcpyAsync(sd->cxt.p, hs.cxtable.data(), hs.cxtable.size() * 4, cudaMemcpyHostToDevice, s), "h2d");
     ck(cudaMemcpyAsync(sd->goal.p, gl.data(), gl.size() * sizeof(longlong2), cudaMemcpyHostToDevice, s), "h2d");
+    sd->ginfo.ensure(std::max<size_t>(1, hs.ginfo.size()) * 4);
+    if (!hs.ginfo.empty())
+      ck(cudaMemcpyAsync(sd->ginfo.p, hs.ginfo.data(), hs.ginfo.size() * 4, cudaMemcpyHostToDevice, s), "h2d");
     ck(cudaStreamSynchronize(s), "spec upload");   // the host vectors above go out of scope
     h2d += (long long)(gi.size() * sizeof(int4) + hs.bad2.size() + hs.bad3.size() * 4 + hs.cxtable.size() * 4 +
                        gl.size() * sizeof(longlong2));
@@ -3057,7 +3261,7 @@ DevSpec Engine::Impl::prepare(const HostSpec &hs, const SymGroup &grp, int depth
   }
   sd->used = ++use_clock;
   sp.ginv = sd->ginv.as<int4>(); sp.bad2 = sd->bad2.as<uint8_t>(); sp.bad3 = sd->bad3.as<uint32_t>();
-  sp.cxtable = sd->cxt.as<int>(); sp.goal = sd->goal.as<longlong2>();
+  sp.cxtable = sd->cxt.as<int>(); sp.goal = sd->goal.as<longlong2>(); sp.ginfo = sd->ginfo.as<int>();
 
   return sp;
 }
@@ -3067,15 +3271,15 @@ int Engine::Impl::run(const HostSpec &hs, const Options &opt, const std::functio
                       SearchResult &res) {
   constexpr int N = 1 << NQ, E = N * N;
   const int depth = opt.depth >= 0 ? opt.depth : hs.depth;
-  const SymGroup grp = sym_group(hs, opt.sym);
+  const SymGroup grp = sym_group(hs, opt.sym && !hs.states);   // no symmetry classes for state targets
   res.nsym = grp.nsym;
-  // depth 0: the target is the identity (cheese.cu:1794-1801)
+  // depth 0: the target is the goal (the identity; for state targets the goal rows) (cheese.cu:1794-1801)
   {
-    bool done = hs.tk == 0;
+    bool done = hs.tk == (hs.states ? hs.gk : 0);
     for (int r = 0; r < N && done; r++)
       for (int c = 0; c < N && done; c++) {
         const Zw x = hs.target[r * N + c];
-        done = r == c ? (x.a == 1 && !x.b && !x.c && !x.d) : zzero(x);
+        done = hs.states ? zeq(x, hs.goal[r * N + c]) : r == c ? (x.a == 1 && !x.b && !x.c && !x.d) : zzero(x);
       }
     if (done && !opt.nogoal) { res.depth0 = true; return RC_CIRCUIT; }
   }
@@ -3295,7 +3499,11 @@ int Engine::search(const HostSpec &hs, const Options &opt, const std::function<v
   int rc;
   try {
     ck(cudaSetDevice(dev_), "cudaSetDevice");
-    if (opt.mitm && !hs.states) {
+    if (opt.mitm && hs.states) {
+      res.nsym = 1;
+      res.error = "--mitm: unitary targets only";
+      rc = RC_USAGE;
+    } else if (opt.mitm) {
       switch (hs.n) {
         case 1: rc = impl_->run_mitm<1>(hs, opt, cb, res); break;
         case 2: rc = impl_->run_mitm<2>(hs, opt, cb, res); break;

@@ -162,16 +162,19 @@ int parse_spec(const char *text, size_t len, HostSpec &s, std::string &err) {
       if (v == "states") s.states = 1;
       else if (v != "unitary" && v != "exact") { err = "unsupported " + tok + " " + v; return RC_SPEC; }
     } else if (tok == "pairs") s.m = (int)in.num();
-    else if (tok == "start") {                 // state targets: parsed for the grammar, refused at run time
-      (void)in.num();
+    else if (tok == "start") {                 // state targets: the rows e_in_j (the residual's start)
+      const int k = (int)in.num();
       if (s.n < 1 || s.n > NQMAX) { in.fail = true; break; }
       const int N = 1 << s.n;
-      for (int i = 0; i < N * N; i++) (void)in.zw();
+      s.target.assign((size_t)N * N, Zw{0, 0, 0, 0});
+      for (int i = 0; i < N * N; i++) s.target[i] = in.zw();
+      s.tk = k;
       have_start = true;
-    } else if (tok == "goal") {
+    } else if (tok == "goal") {                // state targets: per pair sde, nullity, Schmidt rank per cut
       const int m = (int)in.num();
       const int w = 2 + (int)s.cutmask.size();
-      for (int i = 0; i < m * w; i++) (void)in.num();
+      s.ginfo.assign((size_t)std::max(0, m * w), 0);
+      for (int i = 0; i < m * w; i++) s.ginfo[i] = (int)in.num();
       have_ginfo = m * w > 0;
     } else if (tok == "depth") s.depth = (int)in.num();
     else if (tok == "standard") s.standard = (int)in.num();
@@ -189,11 +192,17 @@ int parse_spec(const char *text, size_t len, HostSpec &s, std::string &err) {
         std::array<int, 3> q{0, 0, 0};
         for (int j = 0; j < nq; j++) q[j] = (int)in.num();
         const int L = 1 << nq;
-        (void)in.num();                                  // forward exponent (state targets only)
-        for (int i = 0; i < L * L; i++) (void)in.zw();   // forward matrix
-        const int ik = (int)in.num();
+        const int fk = (int)in.num();                   // forward exponent and matrix
+        std::array<Zw, LMAX * LMAX> fwd{};
+        for (int i = 0; i < L * L; i++) fwd[i] = in.zw();
+        int ik = (int)in.num();
         std::array<Zw, LMAX * LMAX> inv{};
         for (int i = 0; i < L * L; i++) inv[i] = in.zw();
+        if (s.states) {          // rows are images of the inputs (transposed): a gate multiplies them by its transpose
+          ik = fk;
+          for (int a = 0; a < L; a++)
+            for (int b = 0; b < L; b++) inv[a * L + b] = fwd[b * L + a];
+        }
         s.names.push_back(name); s.gnq.push_back(nq); s.gq.push_back(q); s.gik.push_back(ik); s.ginv.push_back(inv);
       }
     } else if (tok == "bad2") {
@@ -219,7 +228,7 @@ int parse_spec(const char *text, size_t len, HostSpec &s, std::string &err) {
       std::vector<Zw> M(N * N);
       for (auto &x : M) x = in.zw();
       if (!s.states) { s.target = M; s.tk = k; s.gk = 0; }
-      else have_goal_rows = true;
+      else { s.goal = M; s.gk = k; have_goal_rows = true; }
     } else if (tok == "cuts") {
       const int m = (int)in.num();
       for (int i = 0; i < m && !in.fail; i++) {
@@ -236,12 +245,11 @@ int parse_spec(const char *text, size_t len, HostSpec &s, std::string &err) {
     } else if (tok == "end") break;
     else { err = "unknown spec field " + tok; return RC_SPEC; }
   }
-  if (s.states) {                              // parsed for the grammar; the search refuses it (exit 3)
+  if (s.states) {                              // the reference's reader: every part of a state spec present
     if (!have_start || !have_goal_rows || !have_ginfo || s.m < 1 || s.m > (1 << std::max(0, std::min(s.n, 6)))) {
       err = "states spec incomplete";
       return RC_SPEC;
     }
-    return 0;
   }
   if (s.n < 1 || s.n > NQMAX) { err = "n = " + std::to_string(s.n) + " not built"; return RC_USAGE; }
   const int N = 1 << s.n;

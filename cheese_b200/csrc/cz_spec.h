@@ -20,7 +20,9 @@ struct HostSpec {
   std::vector<std::array<Zw, LMAX * LMAX>> ginv;   // inverse gate local matrix / sqrt2^ik (row m, column lc)
   std::vector<uint8_t> bad2;                        // G x G
   std::vector<uint32_t> bad3;                       // bitset G^3
-  std::vector<Zw> target;                           // N x N, exponent tk
+  std::vector<Zw> target;                           // N x N, exponent tk (state targets: the start rows)
+  std::vector<Zw> goal;                             // state targets: the goal rows (N x N, exponent gk)
+  std::vector<int> ginfo;                           // state targets: per pair sde, nullity, Schmidt rank per cut
   std::vector<int> cutmask, cutsize, rad, cxtable;
   std::vector<uint8_t> gflags;                      // GateFlag bits per candidate
 };

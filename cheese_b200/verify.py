@@ -28,3 +28,23 @@ def equivalent(spec_text, names):
     n, T = spec_target(spec_text)
     k, M = circuit_unitary(n, names)
     return (k, [list(r) for r in M]) == (T[0], [list(r) for r in T[1]])
+
+
+def state_equivalent(spec_text, names):
+    """for a state-target spec: the circuit maps every listed input basis state to the target's image exactly
+    (global phase included), i.e. its columns at the inputs, as rows, equal the spec's goal rows"""
+    toks = spec_text.split()
+    n = int(toks[toks.index("n") + 1])
+    m = int(toks[toks.index("pairs") + 1])
+    N = 1 << n
+    i = toks.index("start")
+    vals = list(map(int, toks[i + 2:i + 2 + 4 * N * N]))
+    inputs = []
+    for r in range(m):
+        row = [tuple(vals[4 * (r * N + c):4 * (r * N + c) + 4]) for c in range(N)]
+        inputs.append(next(c for c in range(N) if row[c] != (0, 0, 0, 0)))
+    _, G = spec_target(spec_text)
+    k, M = circuit_unitary(n, names)
+    rows = [[M[r][x] for r in range(N)] for x in inputs] + [[(0, 0, 0, 0)] * N for _ in range(N - m)]
+    kk, R = normalise(k, rows)
+    return (kk, [list(r) for r in R]) == (G[0], [list(r) for r in G[1]])

@@ -28,6 +28,10 @@ _GATES = {
     "h": (1, {(0, 0): 0, (0, 1): 0, (1, 0): 0, (1, 1): 4}),
     # cx with control = local bit 0, target = local bit 1
     "cx": (0, {(0, 0): 0, (1, 3): 0, (2, 2): 0, (3, 1): 0}),
+    "y": (0, {(0, 1): 6, (1, 0): 2}),
+    "cz": (0, {(0, 0): 0, (1, 1): 0, (2, 2): 0, (3, 3): 4}),
+    # ccx: controls local bits 0 and 1, target bit 2 (local states 3 and 7 swap)
+    "ccx": (0, {(l, {3: 7, 7: 3}.get(l, l)): 0 for l in range(8)}),
 }
 ONE_QUBIT = ["x", "z", "h", "s", "sdg"]
 

@@ -37,8 +37,9 @@ void cz_spec_free(cz_spec *spec);
 int cz_spec_info(const cz_spec *spec, int *n, int *gates, int *depth);
 /* candidate name, e.g. "L_cx_0_1" (NULL when out of range) */
 const char *cz_spec_gate_name(const cz_spec *spec, int g);
-/* 1 when the spec is a state-target spec ("mode states"), which the GPU search refuses like the reference's
- * GPU binary (src/cheese.cu:1871-1876) */
+/* 1 when the spec is a state-target spec ("mode states": the circuit must map every listed input basis state to
+ * the target's image, cheese.cu:451-583). The reference's GPU binary refuses these (src/cheese.cu:1871-1876) and
+ * only its CPU build searches them; cz_search searches them on the GPU with the CPU build's bounds and results. */
 int cz_spec_is_states(const cz_spec *spec);
 
 /* Search engine on CUDA device `device` (replaces the device setup of run<NQ>, src/cheese.cu:1762-1792). */

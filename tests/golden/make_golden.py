@@ -11,6 +11,7 @@ Writes
   tests/golden/cases.json               per case: spec, flags, exit code and the reference's stdout with every
                                         "seconds" value replaced by 0.00 (machine dependent, never compared)
   tests/golden/mitm_cases.json          the same for --mitm runs
+  tests/golden/state_cases.json         the same for state targets (RUS without measurement), reference CPU build
   tests/golden/spec_circuits.json       the reference's qasm targets (circuit, budget) and extra reference-written
                                         specs (W3 off, ccx, cz / y gate sets) for the C++ spec generator
   tests/golden/table_cases.json         the same for --table K runs, each in a fresh working directory (so the
@@ -105,6 +106,57 @@ def specgen_cases(ref, write_spec):
     print(f"{len(out)} spec-generation cases written", file=sys.stderr)
 
 
+# state targets (RUS without measurement, reference cheese.cu:451-583, run by its CPU build): the reference's own RUS
+# targets with their ancilla qubits starting in |0>, and seeded random circuits with random input sets
+# (case stem, rus id or None, ancillas, budgets)
+STATE_CASES = [("rus28-states", 28, [1], [2, 3, 4]), ("rus2-states", 2, [1], [5, 6, 7]),
+               ("rus12-states", 12, [1], [5, 6, 7, 8]), ("rus20-states", 20, [2], [5, 6, 7, 8, 9]),
+               ("rus1-states", 1, [1], [7, 8, 9, 10, 11]), ("rus3-states", 3, [1], [7, 8, 9, 10, 11]),
+               ("rus7-states", 7, [1, 2], [3, 4, 5, 6, 7]), ("rus8-states", 8, [1, 2], [6, 7, 8, 9, 10])]
+
+
+def state_cases(ref, binp):
+    from cheese import spec as refspec
+    sys.path.insert(0, str(ROOT))
+    from cheese_b200 import workloads
+    out = []
+
+    def run(name, stem, d):
+        t0 = time.time()
+        try:
+            p = subprocess.run([str(binp), str(GOLD / "specs" / f"{stem}.spec"), "--depth", str(d)],
+                               capture_output=True, text=True, timeout=300)
+        except subprocess.TimeoutExpired:
+            print(f"{name}: timed out, left out", file=sys.stderr)
+            return
+        lines = [SECONDS.sub('"seconds": 0.00', l) for l in p.stdout.splitlines()]
+        print(f"{name}: rc {p.returncode}, {len(lines)} lines, {time.time() - t0:.1f} s", file=sys.stderr)
+        out.append({"name": name, "spec": stem, "flags": ["--depth", str(d)], "rc": p.returncode, "stdout": lines})
+
+    for stem, rid, anc, budgets in STATE_CASES:
+        n, circ = refspec.parse_qasm(Path(ref) / "benchmarks" / "rus" / str(rid) / "spec.qasm")
+        mask = sum(1 << q for q in anc)
+        inputs = [x for x in range(1 << n) if not x & mask]
+        buf = io.StringIO()
+        refspec.write_spec(buf, n, circ, budgets[0], inputs=inputs)
+        (GOLD / "specs" / f"{stem}.spec").write_text(buf.getvalue())
+        for d in budgets:
+            run(f"{stem}-{d}", stem, d)
+    rng = random.Random(4242)
+    for i in range(6):
+        n, circ = workloads.random_circuit(rng, n=2 if i < 3 else 3, L=rng.randint(4, 7))
+        inputs = sorted(rng.sample(range(1 << n), rng.randint(1, (1 << n) - 1)))
+        stem = f"states-rand-{i}"
+        buf = io.StringIO()
+        refspec.write_spec(buf, n, circ, len(circ), inputs=inputs)
+        (GOLD / "specs" / f"{stem}.spec").write_text(buf.getvalue())
+        run(f"{stem}-{len(circ)}", stem, len(circ))
+        out[-1]["circuit"] = [[g, list(qs)] for g, qs in circ]
+        out[-1]["inputs"] = inputs
+    (GOLD / "state_cases.json").write_text(json.dumps(out, indent=1) + "\n")
+    print(f"{len(out)} state cases written", file=sys.stderr)
+
+
 def mitm_cases(binp):
     out = []
     for name, stem, flags in MITM_CASES:
@@ -161,6 +213,7 @@ def main():
     ap.add_argument("--table-only", action="store_true", help="write only the --table K cases")
     ap.add_argument("--mitm-only", action="store_true", help="write only the --mitm cases")
     ap.add_argument("--specgen-only", action="store_true", help="write only the spec-generation cases")
+    ap.add_argument("--states-only", action="store_true", help="write only the state-target cases")
     o = ap.parse_args()
     sys.dont_write_bytecode = True
     sys.path.insert(0, str(Path(o.ref) / "python"))
@@ -194,6 +247,9 @@ def main():
         return
     if o.specgen_only:
         specgen_cases(o.ref, write_spec)
+        return
+    if o.states_only:
+        state_cases(o.ref, binp)
         return
     # target specs written by the reference generator (budget line = the first budget used)
     qdir = Path(o.ref) / "tests" / "qasm"
@@ -240,6 +296,7 @@ def main():
     table_cases(binp, write_spec)
     mitm_cases(binp)
     specgen_cases(o.ref, write_spec)
+    state_cases(o.ref, binp)
 
 
 if __name__ == "__main__":

@@ -60,8 +60,8 @@ def test_too_many_gates_is_a_spec_error():
     assert e.value.rc == 2 and "too many gates" in str(e.value)
 
 
-def test_state_specs_are_parsed_then_refused():
-    # a state-target spec: parsed (grammar) and flagged; the search refuses it like the reference GPU binary
+def test_state_specs_are_parsed():
+    # a state-target spec: parsed (grammar, start rows, goal rows and goal bounds) and flagged
     s = cz.Spec(spec_text("cs-states"))
     assert s.states
     with pytest.raises(cz.SpecError) as e:      # a states header without its start / goal blocks

@@ -52,9 +52,10 @@ def test_forced_int64_limbs_identical(engine):
         assert (a.rc, a.lines()) == (b.rc, b.lines()) == (c["rc"], c["stdout"])
 
 
-def test_state_targets_refused_like_reference_gpu_binary(engine):
+def test_state_target_met_by_the_empty_circuit(engine):
+    """the CS target on inputs |00>, |01> (control 0) is already met: the reference CPU build's depth-0 answer"""
     out = engine.search(spec_text("cs-states"))
-    assert out.rc == 3 and "state targets" in out.error
+    assert out.rc == 0 and out.depth0 and out.lines() == ['{"found": 0, "circuit": []}']
 
 
 def test_depth_above_limit_is_usage_error(engine):
@@ -112,7 +113,8 @@ def test_drop_in_binary(tmp_path):
     p = subprocess.run([str(exe), str(spec_path("toffoli")), "--depth", "60"], capture_output=True, text=True)
     assert p.returncode == 3 and "depth > 48" in p.stderr
     p = subprocess.run([str(exe), str(spec_path("cs-states"))], capture_output=True, text=True)
-    assert p.returncode == 3 and "state targets" in p.stderr
+    assert p.returncode == 0 and p.stdout == '{"found": 0, "circuit": []}\n'
+    assert "symmetry classes: 1 group elements" in p.stderr
 
 
 def test_trim_releases_and_search_repeats(engine):
