@@ -313,17 +313,39 @@ def systems(eng, args):
         "reference_published": "RTX 3060 Ti: K=8 table 17.9M classes in 30 s; Toffoli optimum 27 s (budget 14 1.5 s, "
                                "15 11.1 s); Fredkin budget 15 11.3 s, 16 91 s, 17 out of memory at level 8 "
                                "(docs/PLAN.md:87-95)"}
+    # state targets (RUS without measurement): the reference's GPU binary refuses them, its CPU build searches them;
+    # both on the same three specs (budgets where the optimum is found or proved), the CPU build on all host cores
+    st = {}
+    cases = [("rus1-states", 11), ("rus3-states", 11), ("rus8-states", 9)]
+    t0 = time.perf_counter()
+    for stem, d in cases:
+        r = eng.search((SPECS / f"{stem}.spec").read_text(), depth=d)
+        st[f"{stem}-{d}"] = r.rc
+    st["ours_s"] = time.perf_counter() - t0
+    if REF_CPU.exists():
+        env = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count() or 1))
+        t0 = time.perf_counter()
+        for stem, d in cases:
+            subprocess.run([str(REF_CPU), str(SPECS / f"{stem}.spec"), "--depth", str(d)], capture_output=True,
+                           env=env, timeout=900)
+        st["reference_cpu_s"] = time.perf_counter() - t0
+        st["reference_cpu_threads"] = os.cpu_count()
+    out["state_targets"] = {"workload": "RUS 1 budget 11, RUS 3 budget 11, RUS 8 budget 9 (ancillas in |0>)", **st}
     # serving: seeded Poisson streams of the mixed workload, against the same requests run one by one
     N = args.serve_requests
     reqs = tcwork.serve_requests(eng, 5, N)
+
+    def sequential():
+        for kind, text, depth, _ in reqs:
+            if kind == 0:
+                eng.search(text, depth=depth)
+            elif kind == 1:
+                eng.tcount(text, table_k=4, cache_dir=None)
+            else:
+                eng.cliffopt(text)
+    sequential()                               # warm, as the server's engines are: buffers grown, tables resident
     t0 = time.perf_counter()
-    for kind, text, depth, _ in reqs:
-        if kind == 0:
-            eng.search(text, depth=depth)
-        elif kind == 1:
-            eng.tcount(text, table_k=4, cache_dir=None)
-        else:
-            eng.cliffopt(text)
+    sequential()
     t_seq = time.perf_counter() - t0
     # the same requests through the drop-in binaries, one process per request (how the reference's scripts run
     # them), on a subset: the T-count table cache is written once beforehand and loaded by every process
