@@ -57,6 +57,7 @@ __device__ __forceinline__ uint64_t fmix(uint64_t h) {
 struct TSm {
   int *ax, *ay, *bx, *by;
   int *fa, *fb, *sa, *sb;                     // per column: first nonzero row, sign
+  int *gm;                                    // per column: scratch of the exact comparison
   unsigned long long *a1, *a2, *b1, *b2;      // per column: hash partial sums, then column hashes
   unsigned long long *w1, *w2;                // per row weights
   unsigned long long *red;                    // 4 words
@@ -64,7 +65,7 @@ struct TSm {
   uint8_t *seq;                               // MAXT + 1
 };
 __host__ __device__ inline size_t tsm_bytes(int P) {
-  return (size_t)4 * P * P * 4 + (size_t)4 * MAXP * 4 + (size_t)6 * MAXP * 8 + 4 * 8 + 8 * 4 + MAXT + 8;
+  return (size_t)4 * P * P * 4 + (size_t)5 * MAXP * 4 + (size_t)6 * MAXP * 8 + 4 * 8 + 8 * 4 + MAXT + 8;
 }
 __device__ TSm tsm_carve(int P) {
   extern __shared__ unsigned long long smraw[];
@@ -74,7 +75,7 @@ __device__ TSm tsm_carve(int P) {
   s.w1 = q; q += MAXP; s.w2 = q; q += MAXP; s.red = q; q += 4;
   int *p = (int *)q;
   s.ax = p; p += P * P; s.ay = p; p += P * P; s.bx = p; p += P * P; s.by = p; p += P * P;
-  s.fa = p; p += MAXP; s.fb = p; p += MAXP; s.sa = p; p += MAXP; s.sb = p; p += MAXP;
+  s.fa = p; p += MAXP; s.fb = p; p += MAXP; s.sa = p; p += MAXP; s.sb = p; p += MAXP; s.gm = p; p += MAXP;
   s.misc = p; p += 8;
   s.seq = (uint8_t *)p;
   for (int i = threadIdx.x; i < MAXP; i += blockDim.x) {
@@ -193,10 +194,8 @@ __device__ void blk_colkey(const int *mx, const int *my, int e, int P, int *firs
   __syncthreads();
 }
 
-// exact coset equality of A and B (both keyed by blk_colkey): same exponent and the same multiset of
-// sign-normalised columns
-__device__ bool blk_same(const TSm &s, int ea, int eb, int P) {
-  if (ea != eb) return false;
+// exact multiset comparison by counting, for the rare case of two different columns with equal hashes
+__device__ bool blk_same_counted(const TSm &s, int P) {
   const int tid = threadIdx.x;
   bool eq = true;
   if (tid < P) {
@@ -216,6 +215,47 @@ __device__ bool blk_same(const TSm &s, int ea, int eb, int P) {
     eq = na == nb;
   }
   return __syncthreads_and(eq);
+}
+
+// exact coset equality of A and B (both keyed by blk_colkey): same exponent and the same multiset of
+// sign-normalised columns. Per column: the number of A and of B columns with its hash (equal counts for every
+// hash), its group's first A column, first B column and, for B's own columns, first B column; then, in lockstep
+// over the rows, every A column equals its group's first A column and first B column, and every B column equals its
+// group's first B column. The per-column searches keep no data-dependent inner loop, so a warp never serialises.
+// Only when the hash counts agree but a group holds different columns is the counting comparison run.
+// (fa and fb, the first nonzero rows, are not needed after the keys: they hold the group indices here.)
+__device__ bool blk_same(const TSm &s, int ea, int eb, int P) {
+  if (ea != eb) return false;
+  const int tid = threadIdx.x;
+  bool ok = true;
+  if (tid < P) {
+    const int c = tid;
+    const unsigned long long ha1 = s.a1[c], ha2 = s.a2[c], hb1 = s.b1[c], hb2 = s.b2[c];
+    int ka = 0, kb = 0, ra = P, rb = P, rbb = P;
+    for (int d = 0; d < P; d++) {
+      const bool ia = s.a1[d] == ha1 && s.a2[d] == ha2;
+      const bool ib = s.b1[d] == ha1 && s.b2[d] == ha2;
+      const bool bb = s.b1[d] == hb1 && s.b2[d] == hb2;
+      ka += ia; kb += ib;
+      if (ia && d < ra) ra = d;
+      if (ib && d < rb) rb = d;
+      if (bb && d < rbb) rbb = d;
+    }
+    ok = ka == kb && rb < P;
+    s.fa[c] = ra; s.fb[c] = rbb; s.gm[c] = rb < P ? rb : 0;
+  }
+  if (!__syncthreads_and(ok)) return false;       // the hash multisets differ, so the column multisets do
+  const int c = tid & (P - 1), q = tid / P, stride = TC_T / P;
+  const int ra = s.fa[c], rbb = s.fb[c], rb = s.gm[c];
+  const int sc = s.sa[c], sra = s.sa[ra], srb = s.sb[rb], sbc = s.sb[c], srbb = s.sb[rbb];
+  for (int a = q; a < P && ok; a += stride) {
+    const int x = sc * s.ax[a * P + c], y = sc * s.ay[a * P + c];
+    if (x != sra * s.ax[a * P + ra] || y != sra * s.ay[a * P + ra]) ok = false;
+    if (x != srb * s.bx[a * P + rb] || y != srb * s.by[a * P + rb]) ok = false;
+    if (sbc * s.bx[a * P + c] != srbb * s.bx[a * P + rbb] || sbc * s.by[a * P + c] != srbb * s.by[a * P + rbb]) ok = false;
+  }
+  if (__syncthreads_and(ok)) return true;
+  return blk_same_counted(s, P);                  // a hash group holds different columns: count exact matches
 }
 
 // ---------------- kernels ----------------
