@@ -212,24 +212,28 @@ def systems(eng, args):
     import cheese_b200 as cz
     from cheese_b200 import tcwork, workloads
     out = {}
-    # batched search: 512 seeded targets, plain job by job vs one batch session per qubit count
+    # batched search: 512 seeded targets, plain job by job vs one batch session per qubit count. Both arms run once
+    # untimed first, so both are timed warm: the engine's buffers and the sessions' device memory already grown.
     jobs = workloads.batch(1, 512)
     specs = [cz.Spec(workloads.make_spec(n, c, d)) for n, c, d in jobs]
-    eng.search(specs[0])
-    t0 = time.perf_counter()
-    plain = [eng.search(s) for s in specs]
-    tp = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    sess = {n: cz.Batch(eng, n) for n in (2, 3)}
-    ids = [sess[s.n].submit(s) for s in specs]
-    for b in sess.values():
-        b.run()
-    tb = time.perf_counter() - t0
+    for rep in range(2):
+        t0 = time.perf_counter()
+        plain = [eng.search(s) for s in specs]
+        tp = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        sess = {n: cz.Batch(eng, n) for n in (2, 3)}
+        ids = [sess[s.n].submit(s) for s in specs]
+        for b in sess.values():
+            b.run()
+        tb = time.perf_counter() - t0
+        if not rep:
+            for b in sess.values():
+                b.close()
     bad = sum(1 for s, i, p in zip(specs, ids, plain)
               if (lambda r: r.rc != p.rc or r.lines() != p.lines() or r.circuit != p.circuit)(sess[s.n].result(i)))
     out["batched"] = {"workload": "512 seeded targets: random circuits of L in [6,12] gates over 2-3 qubits "
                                   "(T/Tdg with prob 0.3), budget L", "plain_jobs_s": 512 / tp, "batched_jobs_s": 512 / tb,
-                      "speedup": tp / tb, "mismatches": bad,
+                      "speedup": tp / tb, "mismatches": bad, "timing": "warm (second pass of both arms)",
                       "launches": sum(b.info()["kernel_launches"] for b in sess.values()),
                       "steps": sum(b.info()["steps"] for b in sess.values())}
     for b in sess.values():

@@ -26,7 +26,7 @@ def strip(lines):
 
 def table_line(stderr):
     tab = [l for l in stderr.splitlines() if l.startswith("table")]
-    return re.sub(r"\(([0-9.]+) s\)", "(0.0 s)", tab[0]) if tab else ""
+    return re.sub(r"(\(|, )([0-9.]+) s\)", r"\g<1>0.0 s)", tab[0]) if tab else ""
 
 
 def run_cli(case, cwd):
