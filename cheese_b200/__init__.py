@@ -132,6 +132,10 @@ SIGNATURES = {
     "cz_spec_generate": (C.c_int, [C.c_char_p, C.c_size_t, C.c_int, C.c_int, C.POINTER(C.c_char_p),
                                    C.POINTER(C.c_int), C.c_int, C.c_int, C.c_char_p, C.c_size_t,
                                    C.POINTER(C.c_size_t), C.POINTER(SpecGenInfo), C.c_char_p, C.c_size_t]),
+    "cz_spec_generate_states": (C.c_int, [C.c_char_p, C.c_size_t, C.c_int, C.c_int, C.POINTER(C.c_char_p),
+                                          C.POINTER(C.c_int), C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int,
+                                          C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(SpecGenInfo),
+                                          C.c_char_p, C.c_size_t]),
     "cz_tspec_generate": (C.c_int, [C.c_char_p, C.c_size_t, C.c_int, C.c_int, C.POINTER(C.c_char_p),
                                     C.POINTER(C.c_int), C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t), C.c_char_p,
                                     C.c_size_t]),
@@ -239,17 +243,26 @@ def _gen_call(fn, *args):
         return out.value.decode()
 
 
-def spec_generate(n=None, circ=None, depth=1, w3=True, qasm=None):
+def spec_generate(n=None, circ=None, depth=1, w3=True, qasm=None, inputs=None):
     """the gate-count spec text of a target circuit (gate list [(name, qubits)] on n qubits, or QASM text), as the
-    reference's spec generator writes it; returns (text, info dict)"""
+    reference's spec generator writes it; with `inputs` (basis states, bit q = qubit q) the state-target spec of
+    those inputs (`--inputs`; `state_inputs(n, ancilla)` gives the `--ancilla` list). Returns (text, info dict)."""
     q, ql, ng, names, qs = _gen_args(circ, qasm)
     info = SpecGenInfo()
+    inputs = list(inputs or [])
+    arr = (C.c_int * max(1, len(inputs)))(*inputs)
 
     def fn(*a):
         *head, out, cap, need, err, errlen = a
-        return lib().cz_spec_generate(*head, out, cap, need, C.byref(info), err, errlen)
+        return lib().cz_spec_generate_states(*head, arr, len(inputs), out, cap, need, C.byref(info), err, errlen)
     text = _gen_call(fn, q, ql, n or 0, ng, names, qs, depth, 0 if w3 else 1)
     return text, {k: getattr(info, k) for k, _ in SpecGenInfo._fields_}
+
+
+def state_inputs(n, ancilla):
+    """the input basis states of a state target whose `ancilla` qubits start in |0> (spec.py state_inputs)"""
+    mask = sum(1 << a for a in ancilla)
+    return [x for x in range(1 << n) if not x & mask]
 
 
 def tspec_generate(n=None, circ=None, qasm=None):

@@ -533,12 +533,24 @@ int specgen_out(const std::string &text, char *out, size_t cap, size_t *out_len)
 int cz_spec_generate(const char *qasm, size_t qasm_len, int n, int ngates, const char *const *names,
                      const int *qubits, int depth, int no_w3, char *out, size_t cap, size_t *out_len,
                      cz_specgen_info *info, char *err, size_t errlen) {
+  return cz_spec_generate_states(qasm, qasm_len, n, ngates, names, qubits, depth, no_w3, nullptr, 0, out, cap,
+                                 out_len, info, err, errlen);
+}
+
+int cz_spec_generate_states(const char *qasm, size_t qasm_len, int n, int ngates, const char *const *names,
+                            const int *qubits, int depth, int no_w3, const int *inputs, int ninputs, char *out,
+                            size_t cap, size_t *out_len, cz_specgen_info *info, char *err, size_t errlen) {
   std::string e, text;
   std::vector<cz::CircGate> circ;
   int nq = 0;
+  if (ninputs < 0 || (ninputs > 0 && !inputs)) {
+    put_err(err, errlen, "bad input list");
+    return 2;
+  }
   int rc = specgen_input(qasm, qasm_len, n, ngates, names, qubits, nq, circ, e);
   cz::SpecGenInfo gi;
-  if (!rc) rc = cz::spec_generate(nq, circ, depth, no_w3 == 0, text, gi, e);
+  const std::vector<int> in(inputs, inputs + ninputs);
+  if (!rc) rc = cz::spec_generate(nq, circ, depth, no_w3 == 0, in, text, gi, e);
   if (rc) {
     put_err(err, errlen, e);
     return rc;

@@ -104,7 +104,7 @@ struct cz_server {
           std::string ge, text;
           cz::SpecGenInfo gi;
           int grc = cz::parse_qasm(r->text.data(), r->text.size(), nq, circ, ge);
-          if (!grc) grc = cz::spec_generate(nq, circ, r->depth >= 0 ? r->depth : (int)circ.size(), true, text, gi, ge);
+          if (!grc) grc = cz::spec_generate(nq, circ, r->depth >= 0 ? r->depth : (int)circ.size(), true, {}, text, gi, ge);
           if (grc) {
             r->rc = grc;
             r->error = ge;

@@ -443,11 +443,94 @@ int ptm_sde(const std::string &g) {
   return best;
 }
 
+// State targets (spec.py:229-325): the goal side of the state bounds, per goal row (the image of one input basis
+// state, over sqrt2^k): its sde, its stabilizer nullity and its Schmidt rank across every cut.
+
+// least s >= 0 with sqrt2^s * (row / sqrt2^k) integral (spec.py row_sde)
+int row_sde(int k, const std::vector<Z> &row) {
+  int v = -1;
+  for (const Z &x : row)
+    if (!x.zero()) v = v < 0 ? val(x) : std::min(v, val(x));
+  return std::max(0, k - std::max(v, 0));
+}
+// n - log2 of the number of Paulis P with P|v> = +-|v> (spec.py nullity; the identity always counts)
+int nullity(int n, const std::vector<Z> &row) {
+  const Z nrm = inner(row, row), neg{-nrm.a, -nrm.b, -nrm.c, -nrm.d};
+  long long cnt = 0;
+  for (int b = 0; b < (1 << (2 * n)); b++) {
+    const Z v = inner(row, pauli_apply(n, b, row));
+    cnt += v == nrm || v == neg;
+  }
+  int bits = 0;
+  for (long long c = cnt; c; c >>= 1) bits++;
+  return n - (bits - 1);
+}
+// exact determinant by cofactor expansion along the first row (zero entries skipped); only its zero test is used
+Z det(const std::vector<std::vector<Z>> &M) {
+  const size_t r = M.size();
+  if (r == 1) return M[0][0];
+  Z acc;
+  for (size_t j = 0; j < r; j++) {
+    if (M[0][j].zero()) continue;
+    std::vector<std::vector<Z>> sub(r - 1);
+    for (size_t i = 1; i < r; i++) {
+      sub[i - 1].reserve(r - 1);
+      for (size_t c = 0; c < r; c++)
+        if (c != j) sub[i - 1].push_back(M[i][c]);
+    }
+    Z t = zmul(M[0][j], det(sub));
+    if (j % 2) t = Z{-t.a, -t.b, -t.c, -t.d};
+    acc = zadd(acc, t);
+  }
+  return acc;
+}
+// next r-subset of {0 .. m-1} in lexicographic order; false after the last
+bool next_subset(std::vector<int> &s, int m) {
+  const int r = (int)s.size();
+  int i = r - 1;
+  while (i >= 0 && s[i] == m - r + i) i--;
+  if (i < 0) return false;
+  s[i]++;
+  for (int j = i + 1; j < r; j++) s[j] = s[j - 1] + 1;
+  return true;
+}
+// rank of the state reshaped as (qubits A) x (the rest): the size of its largest nonzero minor (spec.py schmidt_rank)
+int schmidt_rank(int n, const std::vector<int> &A, const std::vector<Z> &row) {
+  std::vector<int> B;
+  for (int q = 0; q < n; q++)
+    if (std::find(A.begin(), A.end(), q) == A.end()) B.push_back(q);
+  const int R = 1 << A.size(), C = 1 << B.size();
+  std::vector<std::vector<Z>> M(R, std::vector<Z>(C));
+  for (size_t x = 0; x < row.size(); x++) {
+    int ia = 0, ib = 0;
+    for (size_t i = 0; i < A.size(); i++) ia |= (int)((x >> A[i]) & 1) << i;
+    for (size_t i = 0; i < B.size(); i++) ib |= (int)((x >> B[i]) & 1) << i;
+    M[ia][ib] = row[x];
+  }
+  for (int r = std::min(R, C); r > 0; r--) {
+    std::vector<int> rows(r);
+    for (int i = 0; i < r; i++) rows[i] = i;
+    do {
+      std::vector<int> cols(r);
+      for (int i = 0; i < r; i++) cols[i] = i;
+      do {
+        std::vector<std::vector<Z>> sub(r, std::vector<Z>(r));
+        for (int i = 0; i < r; i++)
+          for (int j = 0; j < r; j++) sub[i][j] = M[rows[i]][cols[j]];
+        if (!det(sub).zero()) return r;
+      } while (next_subset(cols, C));
+    } while (next_subset(rows, R));
+  }
+  return 0;
+}
+
 // the parts of a spec that depend only on (n, gate set, W3 on/off), cached
 struct GateSetPart {
   std::vector<Cand> cs;
+  std::vector<std::vector<int>> cuts;
   std::string text;          // "standard" .. through the bad3 block
-  std::string tail;          // "cuts" .. "end"
+  std::string cuts_text;     // the "cuts" block
+  std::string cx_text;       // "cxtable" .. "end"
   int nbad2 = 0, nbad3 = 0;
 };
 std::mutex cache_mu;
@@ -505,14 +588,16 @@ std::shared_ptr<const GateSetPart> gate_set_part(int n, const std::vector<std::s
   for (const auto &p : bad2) w += std::to_string(p[0]) + " " + std::to_string(p[1]) + "\n";
   w += "bad3 " + std::to_string(bad3.size()) + "\n";
   for (const auto &t : bad3) w += std::to_string(t[0]) + " " + std::to_string(t[1]) + " " + std::to_string(t[2]) + "\n";
-  const auto cs = cuts(n);
-  std::string &tl = P->tail;
-  tl += "cuts " + std::to_string(cs.size()) + "\n";
+  P->cuts = cuts(n);
+  const auto &cs = P->cuts;
+  std::string &ct = P->cuts_text;
+  ct += "cuts " + std::to_string(cs.size()) + "\n";
   for (const auto &A : cs) {
-    tl += std::to_string(A.size());
-    for (int q : A) tl += " " + std::to_string(q);
-    tl += "\n";
+    ct += std::to_string(A.size());
+    for (int q : A) ct += " " + std::to_string(q);
+    ct += "\n";
   }
+  std::string &tl = P->cx_text;
   std::vector<int> rad, best;
   if (!cx_table(n, cs, rad, best)) {
     tl += "cxtable 0\n";
@@ -604,23 +689,59 @@ int parse_qasm(const char *text, size_t len, int &n, std::vector<CircGate> &circ
   return check_circuit(n, circ, err);
 }
 
-int spec_generate(int n, const std::vector<CircGate> &circ, int depth, bool use_w3, std::string &out,
-                  SpecGenInfo &info, std::string &err) {
+int spec_generate(int n, const std::vector<CircGate> &circ, int depth, bool use_w3, const std::vector<int> &inputs,
+                  std::string &out, SpecGenInfo &info, std::string &err) {
   try {
     if (int rc = check_circuit(n, circ, err)) return rc;
+    const int N = 1 << n, m = (int)inputs.size();
+    if (m > N) { err = std::to_string(m) + " inputs for " + std::to_string(N) + " basis states"; return 2; }
+    for (int x : inputs)
+      if (x < 0 || x >= N) { err = "input " + std::to_string(x) + " out of range"; return 2; }
     std::set<std::string> gs = {"x", "z", "h", "s", "sdg", "t", "tdg", "cx"};
     for (const CircGate &g : circ) gs.insert(g.g);
     const std::vector<std::string> gl(gs.begin(), gs.end());   // byte order, as Python's sorted()
     const auto P = gate_set_part(n, gl, use_w3);
     const Mat U = unitary(n, circ);
-    out = "cheese-spec 1\nn " + std::to_string(n) + "\nmode unitary\nphase exact\ndepth " + std::to_string(depth) + "\n";
+    auto block = [&](const Mat &M) {
+      std::string t = std::to_string(M.k) + "\n";
+      for (int r = 0; r < M.N; r++) {
+        for (int c = 0; c < M.N; c++) t += (c ? " " : "") + zs(M.at(r, c));
+        t += "\n";
+      }
+      return t;
+    };
+    out = "cheese-spec 1\nn " + std::to_string(n) + "\nmode " + (m ? "states" : "unitary") + "\nphase exact\ndepth " +
+          std::to_string(depth) + "\n";
     out += P->text;
-    out += "target " + std::to_string(U.k) + "\n";
-    for (int r = 0; r < U.N; r++) {
-      for (int c = 0; c < U.N; c++) out += (c ? " " : "") + zs(U.at(r, c));
-      out += "\n";
+    if (!m) {
+      out += "target " + block(U);
+      out += P->cuts_text;
+    } else {
+      // start rows e_x and goal rows U e_x (the transposed images, spec.py state_pairs), zero rows up to N; the goal
+      // rows share one exponent, normalised together
+      Mat S, G;
+      S.N = G.N = N;
+      S.e.assign((size_t)N * N, Z{});
+      G.e.assign((size_t)N * N, Z{});
+      G.k = U.k;
+      for (int j = 0; j < m; j++) {
+        S.at(j, inputs[j]) = Z{1, 0, 0, 0};
+        for (int r = 0; r < N; r++) G.at(j, r) = U.at(r, inputs[j]);
+      }
+      normalise(G);
+      out += "pairs " + std::to_string(m) + "\n";
+      out += "start " + block(S);
+      out += "target " + block(G);
+      out += P->cuts_text;
+      out += "goal " + std::to_string(m) + "\n";
+      for (int j = 0; j < m; j++) {
+        const std::vector<Z> row(G.e.begin() + (size_t)j * N, G.e.begin() + (size_t)(j + 1) * N);
+        out += std::to_string(row_sde(G.k, row)) + " " + std::to_string(nullity(n, row));
+        for (const auto &A : P->cuts) out += " " + std::to_string(schmidt_rank(n, A, row));
+        out += "\n";
+      }
     }
-    out += P->tail;
+    out += P->cx_text;
     info.candidates = (int)P->cs.size();
     info.bad2 = P->nbad2;
     info.bad3 = P->nbad3;

@@ -20,9 +20,11 @@ int parse_qasm(const char *text, size_t len, int &n, std::vector<CircGate> &circ
 
 struct SpecGenInfo { int candidates = 0, bad2 = 0, bad3 = 0; };
 // the gate-count spec of the circuit's unitary with budget `depth` (gate set: Clifford+T plus the circuit's own
-// gates); returns 0, or 2 with err (unknown gate, bad qubit, n out of range, coefficient overflow)
-int spec_generate(int n, const std::vector<CircGate> &circ, int depth, bool use_w3, std::string &out,
-                  SpecGenInfo &info, std::string &err);
+// gates). With `inputs` (basis states, bit q = qubit q) it is the state-target spec of spec.py:356-415 instead: the
+// start rows e_x, the goal rows U e_x and, per goal row, its sde, stabilizer nullity and Schmidt ranks across the
+// cuts. Returns 0, or 2 with err (unknown gate, bad qubit, n out of range, bad input, coefficient overflow).
+int spec_generate(int n, const std::vector<CircGate> &circ, int depth, bool use_w3, const std::vector<int> &inputs,
+                  std::string &out, SpecGenInfo &info, std::string &err);
 // the T-count spec (channel representation and Pauli rotation tables) of the circuit's unitary
 int tspec_generate(int n, const std::vector<CircGate> &circ, std::string &out, std::string &err);
 

@@ -338,6 +338,14 @@ typedef struct {
 int cz_spec_generate(const char *qasm, size_t qasm_len, int n, int ngates, const char *const *names,
                      const int *qubits, int depth, int no_w3, char *out, size_t cap, size_t *out_len,
                      cz_specgen_info *info, char *err, size_t errlen);
+/* The state-target spec of a target circuit, as `python -m cheese.spec TARGET.qasm DEPTH --inputs a,b,..` (or
+ * `--ancilla q ..`: every basis state with those qubits 0) writes it (spec.py:229-325, 356-424): "mode states", the
+ * start rows e_x and the goal rows U e_x of the ninputs input basis states (bit q of x = qubit q), and per goal row
+ * its sde, stabilizer nullity and Schmidt ranks across the cuts. Other arguments and returns as cz_spec_generate;
+ * 2 also for an input out of range or more inputs than basis states. */
+int cz_spec_generate_states(const char *qasm, size_t qasm_len, int n, int ngates, const char *const *names,
+                            const int *qubits, int depth, int no_w3, const int *inputs, int ninputs, char *out,
+                            size_t cap, size_t *out_len, cz_specgen_info *info, char *err, size_t errlen);
 /* The T-count spec of a target circuit, as `python -m cheese.tcount spec TARGET.qasm` writes it (tcount.py:79-168):
  * the channel representation and the Pauli rotation tables. Arguments and returns as cz_spec_generate. */
 int cz_tspec_generate(const char *qasm, size_t qasm_len, int n, int ngates, const char *const *names,

@@ -12,6 +12,8 @@ Writes
                                         "seconds" value replaced by 0.00 (machine dependent, never compared)
   tests/golden/mitm_cases.json          the same for --mitm runs
   tests/golden/state_cases.json         the same for state targets (RUS without measurement), reference CPU build
+  tests/golden/state_spec_cases.json    state-target specs written by the reference's generator (circuit, inputs,
+                                        spec text) for the C++ generator
   tests/golden/spec_circuits.json       the reference's qasm targets (circuit, budget) and extra reference-written
                                         specs (W3 off, ccx, cz / y gate sets) for the C++ spec generator
   tests/golden/table_cases.json         the same for --table K runs, each in a fresh working directory (so the
@@ -157,6 +159,40 @@ def state_cases(ref, binp):
     print(f"{len(out)} state cases written", file=sys.stderr)
 
 
+def state_specgen_cases():
+    """state-target specs written by the reference's generator (spec.py:229-325, 356-424) for the C++ generator: the
+    qasm targets of the spec-generation cases with ancillas in |0>, and seeded random circuits of 2-4 qubits (some
+    with y / cz / ccx) on random input sets. W3 is off so that the fixture stays small: the W3 rules do not depend on
+    the target and are checked on the unitary specs."""
+    from cheese import spec as refspec
+    from cheese_b200 import workloads
+    named = json.loads((GOLD / "spec_circuits.json").read_text())
+    out = []
+
+    def add(name, n, circ, depth, inputs, ancilla=None):
+        buf = io.StringIO()
+        refspec.write_spec(buf, n, [(g, tuple(q)) for g, q in circ], depth, use3=False, inputs=inputs)
+        out.append({"name": name, "n": n, "circuit": [[g, list(q)] for g, q in circ], "depth": depth,
+                    "inputs": inputs, "ancilla": ancilla, "spec": buf.getvalue()})
+
+    for stem, anc in [("toffoli", [2]), ("ccz", [2]), ("fredkin", [0]), ("peres", [1, 2]), ("cs", [1]),
+                      ("qft_2", [0]), ("relative-phase-toffoli", [2]), ("half_adder_3", [2]), ("grover_3", [0])]:
+        c = named[stem]
+        mask = sum(1 << a for a in anc)
+        add(f"{stem}-anc{''.join(map(str, anc))}", c["n"], c["circuit"], c["depth"],
+            [x for x in range(1 << c["n"]) if not x & mask], anc)
+    rng = random.Random(5150)
+    for i in range(12):
+        n = 2 + i % 3
+        _, circ = workloads.random_circuit(rng, n=n, L=rng.randint(3, 8))
+        if i % 4 == 3:                                  # other gate sets: y, cz and (3+ qubits) ccx
+            circ += [("y", (rng.randrange(n),)), ("cz", (0, 1))] + ([("ccx", (0, 1, 2))] if n >= 3 else [])
+        inputs = sorted(rng.sample(range(1 << n), rng.randint(1, 1 << n)))
+        add(f"rand-{i}", n, circ, len(circ), inputs)
+    (GOLD / "state_spec_cases.json").write_text(json.dumps(out, indent=1) + "\n")
+    print(f"{len(out)} state spec-generation cases written", file=sys.stderr)
+
+
 def mitm_cases(binp):
     out = []
     for name, stem, flags in MITM_CASES:
@@ -214,6 +250,8 @@ def main():
     ap.add_argument("--mitm-only", action="store_true", help="write only the --mitm cases")
     ap.add_argument("--specgen-only", action="store_true", help="write only the spec-generation cases")
     ap.add_argument("--states-only", action="store_true", help="write only the state-target cases")
+    ap.add_argument("--state-specgen-only", action="store_true",
+                    help="write only the state-target spec-generation cases (no reference binary needed)")
     o = ap.parse_args()
     sys.dont_write_bytecode = True
     sys.path.insert(0, str(Path(o.ref) / "python"))
@@ -221,6 +259,9 @@ def main():
     sys.path.insert(0, str(ROOT))
     from cheese_b200 import workloads
 
+    if o.state_specgen_only:
+        state_specgen_cases()
+        return
     binp = ROOT / "oracle" / "_ref" / "cheese-cpu"
     b64 = ROOT / "oracle" / "_ref" / "cheese-cpu-store64"
     assert binp.exists(), "build the reference CPU binary first: make -C oracle"

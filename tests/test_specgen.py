@@ -1,7 +1,7 @@
 """The C++ spec generators (host code, no GPU) against the reference's own writers: every spec file the reference's
 python/cheese/spec.py wrote for a fixture circuit is reproduced line for line, except that the W3 triples of one
 (first, second) pair may come in another order (the reference lists them in Python set order; the set is the same),
-and every T-count spec its tcount.py wrote is reproduced byte for byte."""
+every T-count spec its tcount.py wrote is reproduced byte for byte, and so is every state-target spec (mode states)."""
 import json
 import random
 import subprocess
@@ -109,6 +109,57 @@ def test_cli(tmp_path):
     assert p.stderr.strip() == f"toffoli: 3 qubits, 27 candidates, W2 pairs {nb2}, W3 triples {nb3}"
     p = subprocess.run([str(cz.BIN_DIR / "cheese-spec"), "--tcount", str(q)], capture_output=True, text=True)
     assert p.returncode == 0 and p.stdout == (GOLD / "tcount" / "toffoli.tspec").read_text()
-    p = subprocess.run([str(cz.BIN_DIR / "cheese-spec"), str(q), "5", "--ancilla", "2"], capture_output=True,
+    # state targets: --ancilla (every basis state with qubit 2 in |0>) and the same inputs listed with --inputs
+    st = next(c for c in STATE_CASES if c["name"] == "toffoli-anc2")
+    for flags in (["--ancilla", "2"], ["--inputs", ",".join(map(str, st["inputs"]))]):
+        p = subprocess.run([str(cz.BIN_DIR / "cheese-spec"), str(q), str(st["depth"]), "--no-w3"] + flags,
+                           capture_output=True, text=True)
+        assert p.returncode == 0, p.stderr
+        assert p.stdout == st["spec"]
+    p = subprocess.run([str(cz.BIN_DIR / "cheese-spec"), str(q), "5", "--inputs", "0,8"], capture_output=True,
                        text=True)
-    assert p.returncode == 3
+    assert p.returncode == 2 and "input 8 out of range" in p.stderr
+    p = subprocess.run([str(cz.BIN_DIR / "cheese-spec"), str(q), "5", "--ancilla"], capture_output=True, text=True)
+    assert p.returncode == 2 and p.stderr.startswith("usage")
+
+
+STATE_CASES = json.loads((GOLD / "state_spec_cases.json").read_text())
+
+
+@pytest.mark.parametrize("case", STATE_CASES, ids=[c["name"] for c in STATE_CASES])
+def test_state_spec_matches_reference_writer(case):
+    """state-target specs (start and goal rows, per goal row its sde, stabilizer nullity and Schmidt ranks) byte for
+    byte as the reference's generator wrote them"""
+    import cheese_b200 as cz
+    circ = [(g, tuple(q)) for g, q in case["circuit"]]
+    text, info = cz.spec_generate(case["n"], circ, depth=case["depth"], w3=False, inputs=case["inputs"])
+    assert text == case["spec"]
+    if case["ancilla"]:
+        assert cz.state_inputs(case["n"], case["ancilla"]) == case["inputs"]
+
+
+def test_state_specs_of_search_fixtures():
+    """the state-target specs that the GPU search fixtures use (reference-written, W3 on): the seeded random
+    circuits on random input sets, and CS with its ancilla in |0>"""
+    import cheese_b200 as cz
+    cases = [c for c in json.loads((GOLD / "state_cases.json").read_text()) if "inputs" in c]
+    assert len(cases) == 6
+    for c in cases:
+        want = spec_path(c["spec"]).read_text()
+        n = int(want.split("\nn ")[1].split()[0])
+        depth = int(want.split("\ndepth ")[1].split()[0])
+        text, _ = cz.spec_generate(n, circ_of(c), depth=depth, inputs=c["inputs"])
+        assert parts(text) == parts(want), c["name"]
+    cs = CASES["cs"]
+    text, _ = cz.spec_generate(cs["n"], circ_of(cs), depth=5, inputs=[0, 1])
+    assert parts(text) == parts(spec_path("cs-states").read_text())
+
+
+def test_state_spec_errors():
+    import cheese_b200 as cz
+    with pytest.raises(cz.SpecError) as e:
+        cz.spec_generate(2, [("h", (0,))], depth=3, inputs=[0, 4])
+    assert e.value.rc == 2 and "input 4 out of range" in str(e.value)
+    with pytest.raises(cz.SpecError) as e:
+        cz.spec_generate(1, [("h", (0,))], depth=3, inputs=[0, 1, 0])
+    assert e.value.rc == 2 and "3 inputs for 2 basis states" in str(e.value)
