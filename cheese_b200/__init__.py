@@ -72,6 +72,15 @@ class TcResult(C.Structure):
 TC_LEVEL_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(TcLevel))
 
 
+class RusResult(C.Structure):
+    _fields_ = [("rc", C.c_int), ("tcount", C.c_int), ("split_j", C.c_int), ("split_c", C.c_int), ("maxt", C.c_int),
+                ("root", C.c_uint32), ("cliff", C.c_int), ("fw", C.c_int * 32), ("tb", C.c_int * 32),
+                ("table_cosets", C.c_int64), ("table_levels", C.c_int), ("table_loaded", C.c_int),
+                ("table_built", C.c_int), ("table_resident", C.c_int), ("table_seconds", C.c_double),
+                ("total_seconds", C.c_double), ("kernel_launches", C.c_int64), ("table_path", C.c_char * 256),
+                ("error", C.c_char * 256)]
+
+
 class CliffTableInfo(C.Structure):
     _fields_ = [("n", C.c_int), ("order", C.c_int64), ("elements", C.c_int64), ("max_distance", C.c_int),
                 ("per_distance", C.c_int64 * 32), ("built", C.c_int), ("seconds", C.c_double)]
@@ -141,6 +150,10 @@ SIGNATURES = {
                                     C.c_size_t]),
     "cz_tcount": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(TcOptions), TC_LEVEL_FN, C.c_void_p,
                             C.POINTER(TcResult)]),
+    "cz_rus_options_default": (None, [C.POINTER(TcOptions)]),
+    "cz_rspec_check": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(C.c_int), C.c_char_p, C.c_size_t]),
+    "cz_rus": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(TcOptions), TC_LEVEL_FN, C.c_void_p,
+                         C.POINTER(RusResult)]),
     "cz_clifford_table": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(CliffTableInfo), C.c_char_p, C.c_size_t]),
     "cz_clifford_dist": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.c_size_t, C.POINTER(C.c_int)]),
     "cz_clifford_element": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_uint64), C.c_size_t,
@@ -353,6 +366,44 @@ class Engine:
         out["error"] = res.error.decode()
         out["table_path"] = res.table_path.decode()
         return rc, levels, out
+
+    def rus(self, rspec, table_k=8, maxt=16, cache_dir="build", on_level=None):
+        """`rus SPEC --table K --max T`: (rc, level dicts, result dict); `lines()` of the result are the drop-in's
+        stdout lines with "seconds" 0.00"""
+        if isinstance(rspec, str):
+            rspec = rspec.encode()
+        opt = TcOptions(table_k, maxt, cache_dir.encode() if cache_dir else None)
+        levels = []
+
+        def cb(_u, p):
+            l = p.contents
+            d = {k: getattr(l, k) for k, _ in TcLevel._fields_}
+            levels.append(d)
+            if on_level:
+                on_level(d)
+
+        res = RusResult()
+        rc = lib().cz_rus(self._h, rspec, len(rspec), C.byref(opt), TC_LEVEL_FN(cb), None, C.byref(res))
+        out = {k: getattr(res, k) for k, _ in RusResult._fields_ if k not in ("fw", "tb")}
+        out["fw"] = [res.fw[i] for i in range(res.split_j)] if rc == 0 else []
+        out["tb"] = [res.tb[i] for i in range(res.split_c)] if rc == 0 else []
+        out["error"] = res.error.decode()
+        out["table_path"] = res.table_path.decode()
+        return rc, levels, out
+
+    @staticmethod
+    def rus_lines(rc, levels, out):
+        """the drop-in's stdout lines of a `rus` call, "seconds" printed as 0.00"""
+        lines = [f'{{"dir": "{"table" if l["table"] else "search"}", "t": {l["t"]}, "parents": {l["parents"]}, '
+                 f'"children": {l["children"]}, "cosets": {l["cosets"]}, "new": {l["fresh"]}, "seconds": 0.00}}'
+                 for l in levels]
+        if rc == 0:
+            lines.append(f'{{"tcount": {out["tcount"]}, "root": {out["root"]}, "fw": [{", ".join(map(str, out["fw"]))}], '
+                         f'"cliff": {out["cliff"]}, "tb": [{", ".join(map(str, out["tb"]))}], '
+                         f'"split": [{out["split_j"]}, {out["split_c"]}], "seconds": 0.00}}')
+        elif rc == 1:
+            lines.append(f'{{"tcount_above": {out["maxt"]}, "seconds": 0.00}}')
+        return lines
 
     def clifford_table(self, n):
         """the resident BFS table of the n-qubit Clifford group: info dict (per_distance as a list)"""

@@ -7,6 +7,8 @@ Outputs (git-ignored, carried to the GPU host with the working tree):
     cheese_b200/bin/cheese                drop-in for the reference's build/cheese
     cheese_b200/bin/tcount                drop-in for the reference's build/tcount
     cheese_b200/bin/cliffopt              drop-in for the reference's build/cliffopt
+    cheese_b200/bin/rus                   drop-in for the reference's build/rus
+    cheese_b200/bin/cheese-spec           the reference's spec writers (spec.py, tcount.py spec) as one binary
 """
 import os
 import subprocess
@@ -23,12 +25,12 @@ HOSTCXX = os.environ.get("CZ_HOSTCXX", "/usr/bin/g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-ccbin", HOSTCXX, "-Xcompiler", "-fPIC"]
 
-LIB_SOURCES = ["cz_search.cu", "cz_tcount.cu", "cz_clifford.cu", "cz_spec.cpp", "cz_specgen.cpp", "cz_capi.cpp",
-               "cz_serve.cpp"]
+LIB_SOURCES = ["cz_search.cu", "cz_tcount.cu", "cz_clifford.cu", "cz_rus.cu", "cz_spec.cpp", "cz_specgen.cpp",
+               "cz_capi.cpp", "cz_serve.cpp"]
 HEADERS = ["cz_common.h", "cz_spec.h", "cz_engine.h", "cz_sort.cuh", "cz_tcount.h", "cz_clifford.h", "cz_tableau.h",
-           "cz_capi_internal.h", "cz_specgen.h"]
+           "cz_capi_internal.h", "cz_specgen.h", "cz_rus.h", "cz_rus_node.h"]
 BINARIES = {"cheese": "cli_cheese.cpp", "tcount": "cli_tcount.cpp", "cliffopt": "cli_cliffopt.cpp",
-            "cheese-spec": "cli_spec.cpp"}
+            "cheese-spec": "cli_spec.cpp", "rus": "cli_rus.cpp"}
 
 
 def _stale(out, deps):

@@ -62,7 +62,7 @@ int cz_engine_create(int device, cz_engine **out, char *err, size_t errlen) {
     return CZ_ERR_CUDA;
   }
   try {
-    cz_engine *e = new cz_engine{new cz::Engine(device), nullptr, nullptr};
+    cz_engine *e = new cz_engine{new cz::Engine(device), nullptr, nullptr, nullptr};
     *out = e;
     return 0;
   } catch (const std::exception &ex) {
@@ -76,6 +76,7 @@ int64_t cz_engine_trim(cz_engine *engine) {
   size_t n = engine->e->trim();
   if (engine->tc) n += cz::tcount_context_trim(engine->tc);
   if (engine->cl) n += cz::clifford_context_trim(engine->cl);
+  if (engine->ru) n += cz::rus_context_trim(engine->ru);
   return (int64_t)n;
 }
 
@@ -83,6 +84,7 @@ void cz_engine_destroy(cz_engine *engine) {
   if (!engine) return;
   if (engine->tc) cz::tcount_context_destroy(engine->tc);
   if (engine->cl) cz::clifford_context_destroy(engine->cl);
+  if (engine->ru) cz::rus_context_destroy(engine->ru);
   delete engine->e;
   delete engine;
 }
@@ -388,6 +390,67 @@ int cz_tcount(cz_engine *engine, const char *tspec, size_t len, const cz_tcount_
   out->tcount = r.tcount; out->split_j = r.split_j; out->split_c = r.split_c; out->maxt = r.maxt;
   out->nrot = (int)std::min<size_t>(r.rotations.size(), CZ_TCOUNT_MAXROT);
   for (int i = 0; i < out->nrot; i++) { out->rot_p[i] = r.rotations[i].first; out->rot_inv[i] = r.rotations[i].second; }
+  out->table_cosets = r.table_cosets; out->table_levels = r.table_levels;
+  out->table_loaded = r.table_loaded; out->table_built = r.table_built; out->table_resident = r.table_resident;
+  out->table_seconds = r.table_seconds; out->total_seconds = r.total_seconds; out->kernel_launches = r.launches;
+  put_err(out->table_path, sizeof out->table_path, r.table_path);
+  put_err(out->error, sizeof out->error, r.error);
+  return rc;
+}
+
+void cz_rus_options_default(cz_rus_options *opt) {
+  if (!opt) return;
+  opt->table_k = 8; opt->maxt = 16; opt->cache_dir = "build";
+}
+
+int cz_rspec_check(const char *rspec, size_t len, int *nroot, char *err, size_t errlen) {
+  cz::RSpec sp;
+  std::string msg;
+  const int rc = cz::parse_rspec(rspec ? rspec : "", rspec ? len : 0, sp, msg);
+  if (nroot) *nroot = rc ? 0 : sp.nroot;
+  if (err && errlen) put_err(err, errlen, msg);
+  return rc;
+}
+
+int cz_rus(cz_engine *engine, const char *rspec, size_t len, const cz_rus_options *opt, cz_tcount_level_fn on_level,
+           void *user, cz_rus_result *out) {
+  if (!engine || !out) return CZ_ERR_USAGE;
+  std::memset(out, 0, sizeof *out);
+  cz_rus_options o;
+  cz_rus_options_default(&o);
+  if (opt) o = *opt;
+  cz::RSpec sp;
+  std::string err;
+  int rc = cz::parse_rspec(rspec ? rspec : "", rspec ? len : 0, sp, err);
+  if (rc) { out->rc = rc; put_err(out->error, sizeof out->error, err); return rc; }
+  if (o.table_k < 0 || o.table_k > CZ_RUS_MAXPEEL || o.maxt > 63) {
+    out->rc = CZ_ERR_USAGE;
+    put_err(out->error, sizeof out->error, "table depth or max T-count out of range");
+    return CZ_ERR_USAGE;
+  }
+  cz::RusOptions ro;
+  ro.table_k = o.table_k; ro.maxt = o.maxt;
+  ro.use_cache = o.cache_dir != nullptr;
+  if (o.cache_dir) ro.cache_dir = o.cache_dir;
+  cz::RusResult r;
+  try {
+    if (!engine->ru) engine->ru = cz::rus_context_create(engine->e->device(), engine->e->stream());
+    rc = cz::rus_run(engine->ru, sp, ro, [&](const cz::RusLevel &L) {
+      if (!on_level) return;
+      cz_tcount_level l;
+      l.table = L.table; l.t = L.t; l.parents = L.parents; l.children = L.children; l.cosets = L.cosets;
+      l.fresh = L.fresh; l.seconds = L.seconds;
+      on_level(user, &l);
+    }, r);
+  } catch (const std::exception &ex) {
+    r.error = ex.what();
+    rc = CZ_ERR_CUDA;
+  }
+  out->rc = rc;
+  out->tcount = r.tcount; out->split_j = r.split_j; out->split_c = r.split_c; out->maxt = r.maxt;
+  out->root = r.root; out->cliff = r.cliff;
+  for (size_t i = 0; i < r.fw.size() && i < CZ_RUS_MAXPEEL; i++) out->fw[i] = r.fw[i];
+  for (size_t i = 0; i < r.tb.size() && i < CZ_RUS_MAXPEEL; i++) out->tb[i] = r.tb[i];
   out->table_cosets = r.table_cosets; out->table_levels = r.table_levels;
   out->table_loaded = r.table_loaded; out->table_built = r.table_built; out->table_resident = r.table_resident;
   out->table_seconds = r.table_seconds; out->total_seconds = r.total_seconds; out->kernel_launches = r.launches;

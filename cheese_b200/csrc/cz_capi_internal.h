@@ -3,6 +3,7 @@
 #include "../../include/cheese_b200.h"
 #include "cz_clifford.h"
 #include "cz_engine.h"
+#include "cz_rus.h"
 #include "cz_spec.h"
 #include "cz_tcount.h"
 
@@ -10,4 +11,4 @@
 
 struct cz_spec { cz::HostSpec hs; };
 struct cz_batch { cz::BatchSession *b; std::string err; };
-struct cz_engine { cz::Engine *e; cz::TcountContext *tc; cz::CliffordContext *cl; };
+struct cz_engine { cz::Engine *e; cz::TcountContext *tc; cz::CliffordContext *cl; cz::RusContext *ru; };

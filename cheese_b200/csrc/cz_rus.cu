@@ -1,0 +1,765 @@
+// sm_100a kernels and host loop of the RUS T-count search (the reference's src/rus.cu).
+//
+// Reference semantics: a level peels every rotation p = 1..15 off every node (children in parent-major order,
+// rus.cu:226-234), labels each child by its left-coset key, keeps per key group the child with the smallest index
+// plus every member that is not the same coset as it (exact, with an explicit Clifford, rus.cu:262-282, 372-380) and,
+// while building the table, drops cosets already present at a lower level (rus.cu:395-428). The search peels
+// rotations off the roots level by level and looks every node up in the table; the first level with a hit gives the
+// optimum, the node with the smallest table level wins (rus.cu:549-586).
+//
+// B200 design: the matrices are tiny (16 x 4 entries, 528 bytes with the exponent), so one thread owns one node and
+// works on it in registers / local memory; a level's node matrices are stored in HBM once (the reference replays
+// every node's whole peel path for every child and every comparison), so a child costs one peel of its stored
+// parent. The coset key is this build's own hash of the same invariant as the reference's (exponent, sign-normalised
+// row 0 and the multiset of sign-normalised rows 1..15); groups are therefore the same. Dedupe reuses the radix sort
+// of the gate-count search; the table stays resident in HBM for the engine's lifetime, sorted by key with
+// (level, index) order inside equal keys.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <sstream>
+#include <stdexcept>
+
+#include "cz_rus.h"
+#include "cz_rus_node.h"
+#include "cz_sort.cuh"
+
+namespace cz {
+
+namespace {
+
+using namespace rus;
+constexpr uint32_t RUS_CACHE_MAGIC = 0x54525a43u;   // "CZRT": the table file's keys use this build's coset hash
+constexpr uint32_t RUS_KEY_VERSION = 1;
+
+#define GRID_STRIDE(j, n) \
+  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < (long long)(n); j += (long long)gridDim.x * blockDim.x)
+
+__global__ void __launch_bounds__(RT) k_rus_keys(const int *FM, long long n, uint64_t *k1, uint64_t *k2) {
+  GRID_STRIDE(j, n) {
+    RM M;
+    rm_load(M, FM + (size_t)j * MS);
+    rm_key(M, k1[j], k2[j]);
+  }
+}
+
+// child o = stored parent o / 15 peeled by rotation o % 15 + 1: its key
+__global__ void __launch_bounds__(RT) k_rus_children(const int *FM, long long m, RDev sp, uint64_t *k1, uint64_t *k2,
+                                                     int *ovf) {
+  GRID_STRIDE(o, m * NG) {
+    RM P, C;
+    rm_load(P, FM + (size_t)(o / NG) * MS);
+    if (rm_peel(P, C, (int)(o % NG) + 1, sp)) atomicOr(ovf, 1);
+    rm_key(C, k1[o], k2[o]);
+  }
+}
+
+__global__ void k_rus_sortinit(const uint64_t *k1, long long n, uint64_t *keys, uint32_t *vals) {
+  GRID_STRIDE(i, n) { keys[i] = k1[i]; vals[i] = (uint32_t)i; }
+}
+
+// sorted position j (sorted by the first key, stable, so child index ascending inside a run): its group head is the
+// first position of the run with the same second key; j is kept if it is the head or not the head's coset
+__global__ void __launch_bounds__(RT) k_rus_dupcheck(const uint64_t *sk, const uint32_t *sv, long long n,
+                                                     const uint64_t *k2, const int *FM, RDev sp, uint32_t *keep,
+                                                     int *ovf) {
+  GRID_STRIDE(j, n) {
+    long long i = j;
+    while (i > 0 && sk[i - 1] == sk[j]) i--;
+    const uint64_t mine = k2[sv[j]];
+    long long h = j;
+    for (long long q = i; q < j; q++)
+      if (k2[sv[q]] == mine) { h = q; break; }
+    if (h == j) { keep[j] = 1; continue; }
+    RM P, A, B;
+    bool bad = false;
+    rm_load(P, FM + (size_t)(sv[h] / NG) * MS);
+    bad |= rm_peel(P, A, (int)(sv[h] % NG) + 1, sp);
+    rm_load(P, FM + (size_t)(sv[j] / NG) * MS);
+    bad |= rm_peel(P, B, (int)(sv[j] % NG) + 1, sp);
+    if (bad) atomicOr(ovf, 1);
+    keep[j] = rm_equiv(A, B, sp) < 0 ? 1u : 0u;
+  }
+}
+
+__global__ void k_rus_scatter(const uint32_t *sv, const uint32_t *keep, const uint32_t *pos, long long n,
+                              uint64_t *out) {
+  GRID_STRIDE(j, n) if (keep[j]) out[pos[j]] = sv[j];
+}
+
+// kept child idx (ascending) -> the new level: parent, rotation, stored matrix and key
+__global__ void __launch_bounds__(RT) k_rus_materialise(const uint64_t *kidx, long long nk, const int *FMp, RDev sp,
+                                                        int *FMn, uint64_t *F1, uint64_t *F2, uint32_t *par,
+                                                        uint8_t *gat, int *ovf) {
+  GRID_STRIDE(j, nk) {
+    const uint32_t idx = (uint32_t)kidx[j];
+    RM P, C;
+    rm_load(P, FMp + (size_t)(idx / NG) * MS);
+    if (rm_peel(P, C, (int)(idx % NG) + 1, sp)) atomicOr(ovf, 1);
+    rm_store(C, FMn + (size_t)j * MS);
+    rm_key(C, F1[j], F2[j]);
+    par[j] = idx / NG;
+    gat[j] = (uint8_t)(idx % NG + 1);
+  }
+}
+
+// node j (stored matrix) against the table: the entry of the smallest level <= maxc that is the same left coset
+// (node = C x entry), first in (level, index) order among equal keys; hit = its position or -1, cl = the Clifford
+__global__ void __launch_bounds__(RT) k_rus_lookup(const int *FMq, const uint64_t *F1, const uint64_t *F2, long long n,
+                                                   RDev sp, const int *troot, RHist Ht, const uint64_t *S1,
+                                                   const uint64_t *S2, const uint32_t *Sidx, const uint32_t *Slvl,
+                                                   long long ns, int maxc, long long *hit, int *cl, int *ovf) {
+  GRID_STRIDE(j, n) {
+    const uint64_t a = F1[j], b = F2[j];
+    long long lo = 0, hi = ns;
+    while (lo < hi) {
+      const long long mid = (lo + hi) / 2;
+      if (S1[mid] != a ? S1[mid] < a : S2[mid] < b) lo = mid + 1; else hi = mid;
+    }
+    long long res = -1;
+    int rl = 1 << 30, rc = -1;
+    bool built = false;
+    RM A, M, W;
+    for (long long x = lo; x < ns && S1[x] == a && S2[x] == b; x++) {
+      const int lv = (int)Slvl[x];
+      if (lv > maxc || lv >= rl) continue;
+      if (!built) { rm_load(A, FMq + (size_t)j * MS); built = true; }
+      if (rm_replay(M, W, troot, Ht, lv, Sidx[x], sp)) atomicOr(ovf, 1);
+      const int c = rm_equiv(M, A, sp);
+      if (c >= 0) { res = x; rl = lv; rc = c; }
+    }
+    hit[j] = res;
+    if (cl) cl[j] = rc;
+  }
+}
+
+__global__ void k_rus_fresh_flags(const long long *hit, long long n, uint32_t *flag) {
+  GRID_STRIDE(j, n) flag[j] = hit[j] < 0 ? 1u : 0u;
+}
+// the fresh nodes of the level, compacted: parent, rotation, matrix, key; and their table records (level t, index)
+__global__ void k_rus_compact(const uint32_t *flag, const uint32_t *pos, long long n, const uint32_t *par,
+                              const uint8_t *gat, const int *FM, const uint64_t *F1, const uint64_t *F2, uint32_t *par2,
+                              uint8_t *gat2, int *FM2, uint64_t *G1, uint64_t *G2) {
+  GRID_STRIDE(j, n) {
+    if (!flag[j]) continue;
+    const uint32_t q = pos[j];
+    par2[q] = par[j];
+    gat2[q] = gat[j];
+    G1[q] = F1[j];
+    G2[q] = F2[j];
+    for (int i = 0; i < MS; i++) FM2[(size_t)q * MS + i] = FM[(size_t)j * MS + i];
+  }
+}
+
+__global__ void k_rus_iota(long long n, uint32_t *v) { GRID_STRIDE(i, n) v[i] = (uint32_t)i; }
+__global__ void k_rus_gather64(const uint64_t *src, const uint32_t *order, long long n, uint64_t *dst) {
+  GRID_STRIDE(i, n) dst[i] = src[order[i]];
+}
+__global__ void k_rus_gather32(const uint32_t *src, const uint32_t *order, long long n, uint32_t *dst) {
+  GRID_STRIDE(i, n) dst[i] = src[order[i]];
+}
+__global__ void k_rus_fill32(uint32_t *dst, long long n, uint32_t v) { GRID_STRIDE(i, n) dst[i] = v; }
+
+double now_s() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
+struct RusCudaError : std::runtime_error { using std::runtime_error::runtime_error; };
+void rck(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw RusCudaError(std::string("CUDA error after ") + what + ": " + cudaGetErrorString(e));
+  }
+}
+struct Buf {
+  void *p = nullptr;
+  size_t cap = 0;
+  void ensure(size_t b) {
+    if (b <= cap) return;
+    if (p) rck(cudaFree(p), "free");
+    size_t c = std::max(b, cap + cap / 2);
+    c = (c + 255) & ~(size_t)255;
+    rck(cudaMalloc(&p, c), "cudaMalloc");
+    cap = c;
+  }
+  template <typename T> T *as() const { return (T *)p; }
+  void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+};
+
+// a tree of peel sequences over its roots: level l holds (parent, rotation) per node; the top level's matrices and
+// keys (the matrices only while the tree grows)
+struct Tree {
+  std::vector<Buf> par = std::vector<Buf>(1), gat = std::vector<Buf>(1);
+  std::vector<long long> n{0};
+  Buf FM, F1, F2;
+  int top() const { return (int)n.size() - 1; }
+  RHist hist() const {
+    RHist H{};
+    for (int l = 1; l <= top() && l <= MAXT; l++) { H.par[l] = par[l].as<uint32_t>(); H.gat[l] = gat[l].as<uint8_t>(); }
+    return H;
+  }
+  void release() { for (auto &b : par) b.release(); for (auto &b : gat) b.release(); FM.release(); F1.release(); F2.release(); }
+};
+struct Table {                    // cosets reachable from J00: its tree + every coset's key record, sorted
+  Tree D;
+  Buf troot;                      // J00 (MS ints)
+  Buf S1, S2, Sidx, Slvl;
+  long long ns = 0;
+  void release() { D.release(); troot.release(); S1.release(); S2.release(); Sidx.release(); Slvl.release(); }
+};
+
+uint64_t fnv(uint64_t h, const void *p, size_t n) {
+  const unsigned char *b = (const unsigned char *)p;
+  for (size_t i = 0; i < n; i++) { h ^= b[i]; h *= 0x100000001b3ULL; }
+  return h;
+}
+// the parts of a spec the table depends on: J00, the rotation tables, the Clifford list
+uint64_t table_fingerprint(const RSpec &sp) {
+  uint64_t h = 0xcbf29ce484222325ULL;
+  h = fnv(h, &sp.te, sizeof sp.te);
+  h = fnv(h, sp.tx.data(), sp.tx.size() * 4);
+  h = fnv(h, sp.ty.data(), sp.ty.size() * 4);
+  h = fnv(h, sp.tr.data(), sp.tr.size() * 4);
+  h = fnv(h, sp.ts.data(), sp.ts.size() * 4);
+  h = fnv(h, sp.perm.data(), sp.perm.size());
+  h = fnv(h, sp.sign.data(), sp.sign.size());
+  return h;
+}
+
+std::vector<int> packed(int e, const int *x, const int *y) {
+  std::vector<int> v(MS, 0);
+  for (int i = 0; i < NE; i++) { v[i] = x[i]; v[NE + i] = y[i]; }
+  v[2 * NE] = e;
+  return v;
+}
+
+}  // namespace
+
+class RusContext {
+ public:
+  int dev;
+  cudaStream_t s;
+  int nsm = 148;
+  std::map<std::pair<int, uint64_t>, Table *> tables;   // resident: (K, fingerprint)
+  uint64_t spec_fp = 0;                                 // the fixed tables currently on the device
+  Buf tr, ts, perm, sign, bygen, ovf, roots;
+  Buf h1, h2, k0, k1, v0, v1, hist, part, keep, pos, kept, hits, cls, flag, total, fm2, g1, g2, p2, q2;
+  long long launches = 0;
+  RusContext(int d, void *stream) : dev(d), s((cudaStream_t)stream) {
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  }
+  ~RusContext() {
+    cudaSetDevice(dev);
+    for (auto &kv : tables) { kv.second->release(); delete kv.second; }
+    for (Buf *b : all()) b->release();
+  }
+  std::vector<Buf *> work() {
+    return {&roots, &h1, &h2, &k0, &k1, &v0, &v1, &hist, &part, &keep, &pos, &kept, &hits, &cls, &flag, &total, &fm2,
+            &g1, &g2, &p2, &q2};
+  }
+  std::vector<Buf *> all() {
+    std::vector<Buf *> v = work();
+    for (Buf *b : {&tr, &ts, &perm, &sign, &bygen, &ovf}) v.push_back(b);
+    return v;
+  }
+  size_t trim() {
+    size_t n = 0;
+    for (Buf *b : work()) { n += b->cap; b->release(); }
+    return n;
+  }
+  unsigned grid(long long n) const {
+    return (unsigned)std::max<long long>(1, std::min<long long>((n + RT - 1) / RT, (long long)nsm * 16));
+  }
+  void check_ovf() {
+    int v = 0;
+    rck(cudaMemcpyAsync(&v, ovf.p, 4, cudaMemcpyDeviceToHost, s), "d2h");
+    rck(cudaStreamSynchronize(s), "sync");
+    if (v) throw std::overflow_error("coefficient overflow (int32)");
+  }
+  RDev upload(const RSpec &sp) {
+    const uint64_t fp = table_fingerprint(sp);
+    if (fp != spec_fp || !bygen.p) {
+      std::vector<int8_t> t8(sp.tr.begin(), sp.tr.end()), s8(sp.ts.begin(), sp.ts.end());
+      std::vector<int> bg(1 << 20, -1);
+      const int G[4] = {1, 3, 4, 12};
+      for (int c = 0; c < NCL; c++) {
+        int key = 0;
+        for (int g = 0; g < 4; g++) key |= ((sp.perm[c * NR + G[g]] << 1) | (sp.sign[c * NR + G[g]] < 0)) << (5 * g);
+        bg[key] = c;
+      }
+      tr.ensure(t8.size()); ts.ensure(s8.size()); perm.ensure(sp.perm.size()); sign.ensure(sp.sign.size());
+      bygen.ensure(bg.size() * 4);
+      rck(cudaMemcpyAsync(tr.p, t8.data(), t8.size(), cudaMemcpyHostToDevice, s), "h2d");
+      rck(cudaMemcpyAsync(ts.p, s8.data(), s8.size(), cudaMemcpyHostToDevice, s), "h2d");
+      rck(cudaMemcpyAsync(perm.p, sp.perm.data(), sp.perm.size(), cudaMemcpyHostToDevice, s), "h2d");
+      rck(cudaMemcpyAsync(sign.p, sp.sign.data(), sp.sign.size(), cudaMemcpyHostToDevice, s), "h2d");
+      rck(cudaMemcpyAsync(bygen.p, bg.data(), bg.size() * 4, cudaMemcpyHostToDevice, s), "h2d");
+      rck(cudaStreamSynchronize(s), "h2d");
+      spec_fp = fp;
+    }
+    ovf.ensure(16);
+    rck(cudaMemsetAsync(ovf.p, 0, 4, s), "memset");
+    return RDev{tr.as<int8_t>(), ts.as<int8_t>(), perm.as<uint8_t>(), sign.as<int8_t>(), bygen.as<int>()};
+  }
+
+  // level 0 of T: the given root matrices, stored with their keys
+  void set_roots(Tree &T, const std::vector<int> &mats, long long n) {
+    T.n[0] = n;
+    T.FM.ensure((size_t)n * MS * 4);
+    T.F1.ensure(n * 8); T.F2.ensure(n * 8);
+    rck(cudaMemcpyAsync(T.FM.p, mats.data(), (size_t)n * MS * 4, cudaMemcpyHostToDevice, s), "h2d");
+    k_rus_keys<<<grid(n), RT, 0, s>>>(T.FM.as<int>(), n, T.F1.as<uint64_t>(), T.F2.as<uint64_t>());
+    launches++;
+    rck(cudaGetLastError(), "keys kernel");
+  }
+
+  // node j of level t of T against the table (hit position or -1, Clifford)
+  void lookup(const RDev &sp, const Tree &T, long long n, Table &tab, int maxc, bool want_cliff) {
+    hits.ensure(n * 8 + 8);
+    if (want_cliff) cls.ensure(n * 4 + 4);
+    k_rus_lookup<<<grid(n), RT, 0, s>>>(T.FM.as<int>(), T.F1.as<uint64_t>(), T.F2.as<uint64_t>(), n, sp,
+                                        tab.troot.as<int>(), tab.D.hist(), tab.S1.as<uint64_t>(), tab.S2.as<uint64_t>(),
+                                        tab.Sidx.as<uint32_t>(), tab.Slvl.as<uint32_t>(), tab.ns, maxc,
+                                        hits.as<long long>(), want_cliff ? cls.as<int>() : nullptr, ovf.as<int>());
+    launches++;
+    rck(cudaGetLastError(), "lookup kernel");
+  }
+
+  // (S1, S2) sorted, (level, index) order inside equal keys: the old records followed by the new ones, re-sorted by
+  // the second and then the first key with a stable sort
+  void merge_table(Table &tab, const uint64_t *n1, const uint64_t *n2, long long nf, uint32_t lvl) {
+    const long long N = tab.ns + nf;
+    Buf A1, A2, Ai, Al;
+    A1.ensure(N * 8 + 8); A2.ensure(N * 8 + 8); Ai.ensure(N * 4 + 4); Al.ensure(N * 4 + 4);
+    if (tab.ns) {
+      rck(cudaMemcpyAsync(A1.p, tab.S1.p, tab.ns * 8, cudaMemcpyDeviceToDevice, s), "d2d");
+      rck(cudaMemcpyAsync(A2.p, tab.S2.p, tab.ns * 8, cudaMemcpyDeviceToDevice, s), "d2d");
+      rck(cudaMemcpyAsync(Ai.p, tab.Sidx.p, tab.ns * 4, cudaMemcpyDeviceToDevice, s), "d2d");
+      rck(cudaMemcpyAsync(Al.p, tab.Slvl.p, tab.ns * 4, cudaMemcpyDeviceToDevice, s), "d2d");
+    }
+    if (nf) {
+      rck(cudaMemcpyAsync(A1.as<uint64_t>() + tab.ns, n1, nf * 8, cudaMemcpyDeviceToDevice, s), "d2d");
+      rck(cudaMemcpyAsync(A2.as<uint64_t>() + tab.ns, n2, nf * 8, cudaMemcpyDeviceToDevice, s), "d2d");
+      k_rus_iota<<<grid(nf), RT, 0, s>>>(nf, Ai.as<uint32_t>() + tab.ns);
+      k_rus_fill32<<<grid(nf), RT, 0, s>>>(Al.as<uint32_t>() + tab.ns, nf, lvl);
+      launches += 2;
+    }
+    k0.ensure(N * 8 + 8); k1.ensure(N * 8 + 8); v0.ensure(N * 4 + 4); v1.ensure(N * 4 + 4);
+    hist.ensure(sort_hist_words(N) * 4 + 4); part.ensure(scan_partials_words(sort_hist_words(N)) * 4 + 4);
+    SortScratch sc{hist.as<uint32_t>(), part.as<uint32_t>(), hist.cap / 4, part.cap / 4};
+    rck(cudaMemcpyAsync(k0.p, A2.p, N * 8, cudaMemcpyDeviceToDevice, s), "d2d");
+    k_rus_iota<<<grid(N), RT, 0, s>>>(N, v0.as<uint32_t>());
+    launches++;
+    int nl = 0;
+    bool f = radix_sort(k0.as<uint64_t>(), v0.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(), N, 0, 64, sc, s, &nl);
+    uint32_t *ord = f ? v1.as<uint32_t>() : v0.as<uint32_t>();
+    // second pass: the first key in that order, the order as values
+    Buf o2, kk;
+    o2.ensure(N * 4 + 4); kk.ensure(N * 8 + 8);
+    rck(cudaMemcpyAsync(o2.p, ord, N * 4, cudaMemcpyDeviceToDevice, s), "d2d");
+    k_rus_gather64<<<grid(N), RT, 0, s>>>(A1.as<uint64_t>(), o2.as<uint32_t>(), N, kk.as<uint64_t>());
+    launches++;
+    f = radix_sort(kk.as<uint64_t>(), o2.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(), N, 0, 64, sc, s, &nl);
+    launches += nl;
+    const uint32_t *fin = f ? v1.as<uint32_t>() : o2.as<uint32_t>();
+    tab.S1.ensure(N * 8 + 8); tab.S2.ensure(N * 8 + 8); tab.Sidx.ensure(N * 4 + 4); tab.Slvl.ensure(N * 4 + 4);
+    k_rus_gather64<<<grid(N), RT, 0, s>>>(A1.as<uint64_t>(), fin, N, tab.S1.as<uint64_t>());
+    k_rus_gather64<<<grid(N), RT, 0, s>>>(A2.as<uint64_t>(), fin, N, tab.S2.as<uint64_t>());
+    k_rus_gather32<<<grid(N), RT, 0, s>>>(Ai.as<uint32_t>(), fin, N, tab.Sidx.as<uint32_t>());
+    k_rus_gather32<<<grid(N), RT, 0, s>>>(Al.as<uint32_t>(), fin, N, tab.Slvl.as<uint32_t>());
+    launches += 4;
+    rck(cudaGetLastError(), "table merge");
+    rck(cudaStreamSynchronize(s), "table merge");
+    tab.ns = N;
+    A1.release(); A2.release(); Ai.release(); Al.release(); o2.release(); kk.release();
+  }
+
+  // one more level of T (its top level's matrices stored); tab: drop cosets present in the table at a lower level
+  // and add the rest to it. Returns the new nodes.
+  long long grow(const RDev &sp, Tree &T, Table *tab, const std::function<void(const RusLevel &)> &cb) {
+    const double t0 = now_s();
+    const int t = T.top() + 1, tp = t - 1;
+    if (t > MAXT) throw std::runtime_error("peel sequence longer than 32");
+    const long long m = T.n[tp], nc = m * NG;
+    if (nc >= (1LL << 32)) throw std::runtime_error("level too large for 32-bit child indices");
+    const size_t n = (size_t)nc;
+    h1.ensure(n * 8 + 8); h2.ensure(n * 8 + 8);
+    if (nc) {
+      k_rus_children<<<grid(nc), RT, 0, s>>>(T.FM.as<int>(), m, sp, h1.as<uint64_t>(), h2.as<uint64_t>(), ovf.as<int>());
+      launches++;
+      rck(cudaGetLastError(), "children kernel");
+    }
+    check_ovf();
+    // dedupe: stable sort by the first key, then every member checked against its group's head
+    k0.ensure(n * 8 + 8); k1.ensure(n * 8 + 8); v0.ensure(n * 4 + 4); v1.ensure(n * 4 + 4);
+    hist.ensure(sort_hist_words(n) * 4 + 4); part.ensure(scan_partials_words(std::max(sort_hist_words(n), n)) * 4 + 4);
+    keep.ensure(n * 4 + 4); pos.ensure(n * 4 + 4); kept.ensure(n * 8 + 8); total.ensure(16);
+    SortScratch sc{hist.as<uint32_t>(), part.as<uint32_t>(), hist.cap / 4, part.cap / 4};
+    long long nk = 0;
+    if (nc) {
+      k_rus_sortinit<<<grid(nc), RT, 0, s>>>(h1.as<uint64_t>(), nc, k0.as<uint64_t>(), v0.as<uint32_t>());
+      int nl = 0;
+      const bool f = radix_sort(k0.as<uint64_t>(), v0.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(), n, 0, 64, sc,
+                                s, &nl);
+      launches += 1 + nl;
+      const uint64_t *sk = f ? k1.as<uint64_t>() : k0.as<uint64_t>();
+      const uint32_t *sv = f ? v1.as<uint32_t>() : v0.as<uint32_t>();
+      k_rus_dupcheck<<<grid(nc), RT, 0, s>>>(sk, sv, nc, h2.as<uint64_t>(), T.FM.as<int>(), sp, keep.as<uint32_t>(),
+                                             ovf.as<int>());
+      exclusive_scan(keep.as<uint32_t>(), pos.as<uint32_t>(), n, part.as<uint32_t>(), total.as<uint32_t>(), s);
+      k_rus_scatter<<<grid(nc), RT, 0, s>>>(sv, keep.as<uint32_t>(), pos.as<uint32_t>(), nc, kept.as<uint64_t>());
+      launches += 5;
+      rck(cudaGetLastError(), "dedupe");
+      uint32_t hk = 0;
+      rck(cudaMemcpyAsync(&hk, total.p, 4, cudaMemcpyDeviceToHost, s), "d2h");
+      rck(cudaStreamSynchronize(s), "dedupe");
+      check_ovf();
+      nk = hk;
+    }
+    // index order, then the new level
+    const bool fk = radix_sort(kept.as<uint64_t>(), v0.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(), (size_t)nk, 0,
+                               32, sc, s, nullptr);
+    if (nk > 1) launches += 20;
+    const uint64_t *kidx = fk ? k1.as<uint64_t>() : kept.as<uint64_t>();
+    T.par.emplace_back(); T.gat.emplace_back(); T.n.push_back(nk);
+    T.par.back().ensure(nk * 4 + 4); T.gat.back().ensure(nk + 4);
+    fm2.ensure((size_t)nk * MS * 4 + 16); g1.ensure(nk * 8 + 8); g2.ensure(nk * 8 + 8);
+    if (nk) {
+      k_rus_materialise<<<grid(nk), RT, 0, s>>>(kidx, nk, T.FM.as<int>(), sp, fm2.as<int>(), g1.as<uint64_t>(),
+                                                g2.as<uint64_t>(), T.par.back().as<uint32_t>(),
+                                                T.gat.back().as<uint8_t>(), ovf.as<int>());
+      launches++;
+      rck(cudaGetLastError(), "materialise");
+    }
+    std::swap(T.FM, fm2);
+    std::swap(T.F1, g1);
+    std::swap(T.F2, g2);
+    check_ovf();
+    long long fresh = nk;
+    if (tab && nk) {
+      lookup(sp, T, nk, *tab, t - 1, false);
+      check_ovf();
+      flag.ensure(nk * 4 + 4); pos.ensure(nk * 4 + 4);
+      part.ensure(scan_partials_words(nk) * 4 + 4);
+      k_rus_fresh_flags<<<grid(nk), RT, 0, s>>>(hits.as<long long>(), nk, flag.as<uint32_t>());
+      exclusive_scan(flag.as<uint32_t>(), pos.as<uint32_t>(), (size_t)nk, part.as<uint32_t>(), total.as<uint32_t>(), s);
+      launches += 4;
+      uint32_t hf = 0;
+      rck(cudaMemcpyAsync(&hf, total.p, 4, cudaMemcpyDeviceToHost, s), "d2h");
+      rck(cudaStreamSynchronize(s), "table filter");
+      fresh = hf;
+      p2.ensure(fresh * 4 + 4); q2.ensure(fresh + 4); fm2.ensure((size_t)fresh * MS * 4 + 16);
+      g1.ensure(fresh * 8 + 8); g2.ensure(fresh * 8 + 8);
+      k_rus_compact<<<grid(nk), RT, 0, s>>>(flag.as<uint32_t>(), pos.as<uint32_t>(), nk, T.par.back().as<uint32_t>(),
+                                            T.gat.back().as<uint8_t>(), T.FM.as<int>(), T.F1.as<uint64_t>(),
+                                            T.F2.as<uint64_t>(), p2.as<uint32_t>(), q2.as<uint8_t>(), fm2.as<int>(),
+                                            g1.as<uint64_t>(), g2.as<uint64_t>());
+      launches++;
+      rck(cudaGetLastError(), "compact");
+      std::swap(T.par.back(), p2);
+      std::swap(T.gat.back(), q2);
+      std::swap(T.FM, fm2);
+      std::swap(T.F1, g1);
+      std::swap(T.F2, g2);
+      T.n.back() = fresh;
+      merge_table(*tab, T.F1.as<uint64_t>(), T.F2.as<uint64_t>(), fresh, (uint32_t)t);
+    }
+    rck(cudaStreamSynchronize(s), "level");
+    if (cb) {
+      RusLevel L;
+      L.table = tab != nullptr; L.t = t; L.parents = m; L.children = nc; L.cosets = nk; L.fresh = fresh;
+      L.seconds = now_s() - t0;
+      cb(L);
+    }
+    return fresh;
+  }
+
+  void save(const std::string &path, const Table &tab, uint64_t fp) {
+    FILE *f = std::fopen(path.c_str(), "wb");
+    if (!f) { std::fprintf(stderr, "cannot write %s (table not cached)\n", path.c_str()); return; }
+    const Tree &D = tab.D;
+    const int nl = D.top();
+    std::fwrite(&nl, sizeof nl, 1, f);
+    for (int l = 1; l <= nl; l++) {
+      const long n = (long)D.n[l];
+      std::vector<uint32_t> P(n);
+      std::vector<uint8_t> G(n);
+      cudaMemcpy(P.data(), D.par[l].p, n * 4, cudaMemcpyDeviceToHost);
+      cudaMemcpy(G.data(), D.gat[l].p, n, cudaMemcpyDeviceToHost);
+      std::fwrite(&n, sizeof n, 1, f); std::fwrite(P.data(), 4, n, f); std::fwrite(G.data(), 1, n, f);
+    }
+    const long ns = (long)tab.ns;   // records {h1, h2, idx, lvl} as the reference lays them out (keys: this build's)
+    std::vector<uint64_t> a1(ns), a2(ns);
+    std::vector<uint32_t> ai(ns), al(ns);
+    cudaMemcpy(a1.data(), tab.S1.p, ns * 8, cudaMemcpyDeviceToHost);
+    cudaMemcpy(a2.data(), tab.S2.p, ns * 8, cudaMemcpyDeviceToHost);
+    cudaMemcpy(ai.data(), tab.Sidx.p, ns * 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(al.data(), tab.Slvl.p, ns * 4, cudaMemcpyDeviceToHost);
+    std::fwrite(&ns, sizeof ns, 1, f);
+    for (long i = 0; i < ns; i++) {
+      std::fwrite(&a1[i], 8, 1, f); std::fwrite(&a2[i], 8, 1, f); std::fwrite(&ai[i], 4, 1, f); std::fwrite(&al[i], 4, 1, f);
+    }
+    const uint32_t trailer[2] = {RUS_CACHE_MAGIC, RUS_KEY_VERSION};
+    std::fwrite(trailer, 4, 2, f);
+    std::fwrite(&fp, 8, 1, f);
+    std::fclose(f);
+  }
+  bool load(const std::string &path, Table &tab, int K, uint64_t fp) {
+    FILE *f = std::fopen(path.c_str(), "rb");
+    if (!f) return false;
+    std::fseek(f, 0, SEEK_END);
+    const long size = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    int nl = 0;
+    bool ok = std::fread(&nl, sizeof nl, 1, f) == 1 && nl >= 0 && nl <= K;
+    std::vector<std::vector<uint32_t>> P;
+    std::vector<std::vector<uint8_t>> G;
+    long total_n = 0;
+    for (int l = 1; ok && l <= nl; l++) {
+      long n = 0;
+      ok = std::fread(&n, sizeof n, 1, f) == 1 && n >= 0 && n <= size;
+      if (!ok) break;
+      P.emplace_back(n); G.emplace_back(n);
+      ok = std::fread(P.back().data(), 4, n, f) == (size_t)n && std::fread(G.back().data(), 1, n, f) == (size_t)n;
+      total_n += n;
+    }
+    long ns = 0;
+    ok = ok && std::fread(&ns, sizeof ns, 1, f) == 1 && ns == total_n + 1;
+    std::vector<uint64_t> a1, a2;
+    std::vector<uint32_t> ai, al;
+    if (ok) {
+      a1.resize(ns); a2.resize(ns); ai.resize(ns); al.resize(ns);
+      for (long i = 0; ok && i < ns; i++)
+        ok = std::fread(&a1[i], 8, 1, f) == 1 && std::fread(&a2[i], 8, 1, f) == 1 && std::fread(&ai[i], 4, 1, f) == 1 &&
+             std::fread(&al[i], 4, 1, f) == 1 && (int)al[i] <= nl;
+    }
+    uint32_t trailer[2] = {0, 0};
+    uint64_t ffp = 0;
+    ok = ok && std::fread(trailer, 4, 2, f) == 2 && trailer[0] == RUS_CACHE_MAGIC && trailer[1] == RUS_KEY_VERSION &&
+         std::fread(&ffp, 8, 1, f) == 1 && ffp == fp;
+    std::fclose(f);
+    if (!ok) return false;
+    // every record names a node of the tree: its level and index in range, and every parent index in range
+    for (long i = 0; i < ns && ok; i++) ok = (al[i] == 0 && ai[i] == 0) || (al[i] >= 1 && ai[i] < P[al[i] - 1].size());
+    for (int l = 1; l <= nl && ok; l++) {
+      const size_t below = l == 1 ? 1 : P[l - 2].size();
+      for (size_t j = 0; j < P[l - 1].size() && ok; j++) ok = P[l - 1][j] < below && G[l - 1][j] >= 1 && G[l - 1][j] <= NG;
+    }
+    if (!ok) return false;
+    tab.D.n[0] = 1;
+    for (int l = 1; l <= nl; l++) {
+      const long n = (long)P[l - 1].size();
+      tab.D.par.emplace_back(); tab.D.gat.emplace_back(); tab.D.n.push_back(n);
+      tab.D.par.back().ensure(n * 4 + 4); tab.D.gat.back().ensure(n + 4);
+      rck(cudaMemcpyAsync(tab.D.par.back().p, P[l - 1].data(), n * 4, cudaMemcpyHostToDevice, s), "h2d");
+      rck(cudaMemcpyAsync(tab.D.gat.back().p, G[l - 1].data(), n, cudaMemcpyHostToDevice, s), "h2d");
+    }
+    tab.S1.ensure(ns * 8); tab.S2.ensure(ns * 8); tab.Sidx.ensure(ns * 4); tab.Slvl.ensure(ns * 4);
+    rck(cudaMemcpyAsync(tab.S1.p, a1.data(), ns * 8, cudaMemcpyHostToDevice, s), "h2d");
+    rck(cudaMemcpyAsync(tab.S2.p, a2.data(), ns * 8, cudaMemcpyHostToDevice, s), "h2d");
+    rck(cudaMemcpyAsync(tab.Sidx.p, ai.data(), ns * 4, cudaMemcpyHostToDevice, s), "h2d");
+    rck(cudaMemcpyAsync(tab.Slvl.p, al.data(), ns * 4, cudaMemcpyHostToDevice, s), "h2d");
+    rck(cudaStreamSynchronize(s), "h2d");
+    tab.ns = ns;
+    return true;
+  }
+
+  Table *table(const RDev &sp, const RSpec &spec, const RusOptions &opt,
+               const std::function<void(const RusLevel &)> &cb, RusResult &res) {
+    const uint64_t fp = table_fingerprint(spec);
+    const auto key = std::make_pair(opt.table_k, fp);
+    char path[512];
+    std::snprintf(path, sizeof path, "%s/rus-table-k%d.cz.bin", opt.cache_dir.c_str(), opt.table_k);
+    res.table_path = path;
+    auto it = tables.find(key);
+    if (it != tables.end()) { res.table_resident = true; return it->second; }
+    const double t0 = now_s();
+    Table *tab = new Table;
+    try {
+      const std::vector<int> j00 = packed(spec.te, spec.tx.data(), spec.ty.data());
+      tab->troot.ensure(MS * 4);
+      rck(cudaMemcpyAsync(tab->troot.p, j00.data(), MS * 4, cudaMemcpyHostToDevice, s), "h2d");
+      if (opt.use_cache && load(path, *tab, opt.table_k, fp)) {
+        res.table_loaded = true;
+      } else {
+        tab->D.release();
+        tab->D = Tree{};
+        set_roots(tab->D, j00, 1);                      // level 0: the coset of J00
+        merge_table(*tab, tab->D.F1.as<uint64_t>(), tab->D.F2.as<uint64_t>(), 1, 0);
+        for (int l = 1; l <= opt.table_k; l++) if (!grow(sp, tab->D, tab, cb)) break;
+        tab->D.FM.release(); tab->D.F1.release(); tab->D.F2.release();
+        res.table_built = true;
+        if (opt.use_cache) save(path, *tab, fp);
+      }
+    } catch (...) {
+      tab->release();
+      delete tab;
+      throw;
+    }
+    res.table_seconds = now_s() - t0;
+    tables[key] = tab;
+    return tab;
+  }
+
+  int run(const RSpec &spec, const RusOptions &opt, const std::function<void(const RusLevel &)> &cb, RusResult &res) {
+    const double t0 = now_s();
+    rck(cudaSetDevice(dev), "cudaSetDevice");
+    const long long l0 = launches;
+    res.maxt = opt.maxt;
+    const RDev sp = upload(spec);
+    Table *tab = table(sp, spec, opt, cb, res);
+    res.table_cosets = tab->ns;
+    res.table_levels = tab->D.top();
+    const int Dtop = tab->D.top();
+    Tree T;
+    try {
+      std::vector<int> mats;
+      for (int r = 0; r < spec.nroot; r++) {
+        const std::vector<int> m = packed(spec.re[r], spec.rx.data() + (size_t)r * NE, spec.ry.data() + (size_t)r * NE);
+        mats.insert(mats.end(), m.begin(), m.end());
+      }
+      set_roots(T, mats, spec.nroot);
+      int rc = 1;
+      for (int j = 0; j <= opt.maxt; j++) {
+        if (j > 0 && !grow(sp, T, nullptr, cb)) break;
+        const long long n = T.n[j];
+        const int maxc = std::min(Dtop, opt.maxt - j);
+        lookup(sp, T, n, *tab, maxc, true);
+        check_ovf();
+        std::vector<long long> hh(n);
+        std::vector<int> hc(n);
+        rck(cudaMemcpyAsync(hh.data(), hits.p, n * 8, cudaMemcpyDeviceToHost, s), "d2h");
+        rck(cudaMemcpyAsync(hc.data(), cls.p, n * 4, cudaMemcpyDeviceToHost, s), "d2h");
+        rck(cudaStreamSynchronize(s), "d2h");
+        long long best = -1, bestx = -1;
+        int bestc = 1 << 30;
+        for (long long i = 0; i < n; i++) {
+          if (hh[i] < 0) continue;
+          uint32_t lv = 0;
+          rck(cudaMemcpy(&lv, tab->Slvl.as<uint32_t>() + hh[i], 4, cudaMemcpyDeviceToHost), "d2h");
+          if ((int)lv < bestc) { bestc = (int)lv; best = i; bestx = hh[i]; }
+        }
+        if (best >= 0) {
+          uint32_t i = (uint32_t)best;
+          res.fw.assign(j, 0);
+          for (int l = j; l >= 1; l--) {
+            uint8_t g = 0;
+            rck(cudaMemcpy(&g, T.gat[l].as<uint8_t>() + i, 1, cudaMemcpyDeviceToHost), "d2h");
+            rck(cudaMemcpy(&i, T.par[l].as<uint32_t>() + i, 4, cudaMemcpyDeviceToHost), "d2h");
+            res.fw[l - 1] = g;
+          }
+          res.root = i;
+          uint32_t ti = 0;
+          rck(cudaMemcpy(&ti, tab->Sidx.as<uint32_t>() + bestx, 4, cudaMemcpyDeviceToHost), "d2h");
+          res.tb.assign(bestc, 0);
+          for (int l = bestc; l >= 1; l--) {
+            uint8_t g = 0;
+            rck(cudaMemcpy(&g, tab->D.gat[l].as<uint8_t>() + ti, 1, cudaMemcpyDeviceToHost), "d2h");
+            rck(cudaMemcpy(&ti, tab->D.par[l].as<uint32_t>() + ti, 4, cudaMemcpyDeviceToHost), "d2h");
+            res.tb[l - 1] = g;
+          }
+          res.cliff = hc[best];
+          res.tcount = j + bestc;
+          res.split_j = j;
+          res.split_c = bestc;
+          rc = 0;
+          break;
+        }
+        if (j + Dtop >= opt.maxt) break;
+      }
+      T.release();
+      res.rc = rc;
+    } catch (...) {
+      T.release();
+      throw;
+    }
+    res.launches = launches - l0;
+    res.total_seconds = now_s() - t0;
+    return res.rc;
+  }
+};
+
+int parse_rspec(const char *text, size_t len, RSpec &s, std::string &err) {
+  std::istringstream in(std::string(text, len));
+  std::string tok;
+  int ver = 0;
+  if (!(in >> tok) || tok != "rus-spec" || !(in >> ver)) { err = "not a rus spec"; return 2; }
+  bool have_t = false, have_c = false;
+  auto read_mat = [&](std::vector<int> &x, std::vector<int> &y, int &e) {
+    if (!(in >> e)) return false;
+    for (int i = 0; i < NE; i++) {
+      int a, b;
+      if (!(in >> a >> b)) return false;
+      x.push_back(a); y.push_back(b);
+    }
+    return true;
+  };
+  while (in >> tok) {
+    if (tok == "table-root") {
+      s.tx.clear(); s.ty.clear();
+      if (!read_mat(s.tx, s.ty, s.te)) { err = "bad table-root"; return 2; }
+      have_t = true;
+    } else if (tok == "roots") {
+      int m = 0;
+      if (!(in >> m) || m < 0 || m > (1 << 20)) { err = "bad roots"; return 2; }
+      s.nroot = m; s.rx.clear(); s.ry.clear(); s.re.assign(m, 0);
+      for (int r = 0; r < m; r++)
+        if (!read_mat(s.rx, s.ry, s.re[r])) { err = "bad roots"; return 2; }
+    } else if (tok == "rotations") {
+      int m = 0;
+      if (!(in >> m) || m < 0 || m > 64) { err = "bad rotations"; return 2; }
+      s.tr.assign((size_t)m * NR, 0); s.ts.assign((size_t)m * NR, 0);
+      for (int i = 0; i < m * NR; i++)
+        if (!(in >> s.tr[i] >> s.ts[i]) || s.tr[i] < -1 || s.tr[i] >= NR || s.ts[i] < -1 || s.ts[i] > 1) {
+          err = "bad rotations"; return 2;
+        }
+    } else if (tok == "cliffords") {
+      int m = 0;
+      if (!(in >> m)) { err = "bad cliffords"; return 2; }
+      if (m != NCL) { err = "expected 11520 Cliffords"; return 2; }
+      s.perm.assign((size_t)m * NR, 0); s.sign.assign((size_t)m * NR, 0);
+      for (int i = 0; i < m * NR; i++) {
+        int p, g;
+        if (!(in >> p >> g) || p < 0 || p >= NR || (g != 1 && g != -1)) { err = "bad cliffords"; return 2; }
+        s.perm[i] = (uint8_t)p; s.sign[i] = (int8_t)g;
+      }
+      have_c = true;
+    } else if (tok == "end") {
+      break;
+    } else {
+      err = "unknown field " + tok;
+      return 2;
+    }
+  }
+  if (!s.nroot || !have_t || s.tr.size() != (size_t)NG * NR || !have_c) { err = "incomplete spec"; return 2; }
+  std::vector<int> bygen(1 << 20, -1);
+  const int G[4] = {1, 3, 4, 12};
+  for (int c = 0; c < NCL; c++) {
+    int key = 0;
+    for (int g = 0; g < 4; g++) key |= ((s.perm[c * NR + G[g]] << 1) | (s.sign[c * NR + G[g]] < 0)) << (5 * g);
+    if (bygen[key] >= 0) { err = "Clifford table: generator images not unique"; return 2; }
+    bygen[key] = c;
+  }
+  return 0;
+}
+
+RusContext *rus_context_create(int device, void *stream) { return new RusContext(device, stream); }
+void rus_context_destroy(RusContext *c) { delete c; }
+size_t rus_context_trim(RusContext *c) { return c ? c->trim() : 0; }
+
+int rus_run(RusContext *ctx, const RSpec &sp, const RusOptions &opt,
+            const std::function<void(const RusLevel &)> &on_level, RusResult &res) {
+  try {
+    return ctx->run(sp, opt, on_level, res);
+  } catch (const std::overflow_error &e) {
+    res.rc = 4;
+    res.error = e.what();
+  } catch (const std::exception &e) {
+    res.rc = 5;
+    res.error = e.what();
+  }
+  return res.rc;
+}
+
+}  // namespace cz

@@ -274,6 +274,45 @@ int cz_tspec_check(const char *tspec, size_t len, int *n, char *err, size_t errl
 int cz_tcount(cz_engine *engine, const char *tspec, size_t len, const cz_tcount_options *opt,
               cz_tcount_level_fn on_level, void *user, cz_tcount_result *out);
 
+/* ---------------- RUS T-count (the reference's build/rus, src/rus.cu) ---------------- */
+/* flags of `rus SPEC [--table K] [--max T]` (rus.cu:512-523) and the table cache directory: the table of K is cached
+ * in <cache_dir>/rus-table-k<K>.cz.bin (this build's coset keys; the reference's rus-table-k<K>.bin is not read). */
+typedef struct {
+  int table_k;            /* --table K (default 8) */
+  int maxt;               /* --max T (default 16) */
+  const char *cache_dir;  /* default "build"; NULL: no cache */
+} cz_rus_options;
+void cz_rus_options_default(cz_rus_options *opt);
+
+#define CZ_RUS_MAXPEEL 32
+typedef struct {
+  int rc;                 /* 0 found, 1 none with T-count <= maxt, 2 spec, 3 usage, 4 overflow, 5 CUDA */
+  int tcount;             /* rc 0: the optimal RUS T-count */
+  int split_j, split_c;   /* peels of the search node and of the table entry */
+  int maxt;
+  uint32_t root;          /* the root the search node descends from */
+  int cliff;              /* the Clifford C (node = C x table entry): index into the spec's Clifford list */
+  int fw[CZ_RUS_MAXPEEL], tb[CZ_RUS_MAXPEEL];   /* rotation indices 1..15 of the two peel sequences */
+  int64_t table_cosets;   /* cosets in the table (all levels) */
+  int table_levels;
+  int table_loaded, table_built, table_resident;
+  double table_seconds, total_seconds;
+  int64_t kernel_launches;
+  char table_path[256];
+  char error[256];
+} cz_rus_result;
+
+/* Parse a rus-spec without touching the device: 0 and the number of roots in *nroot, or 2 (not a rus spec, unknown
+ * field, incomplete spec, Clifford list not 11520 long or its generator images not unique: the exits of rus.cu's
+ * read_spec and main, :486-510, 528-533) with the message. */
+int cz_rspec_check(const char *rspec, size_t len, int *nroot, char *err, size_t errlen);
+
+/* Optimal T-count of a two-qubit repeat-until-success circuit with measurement, from its rus-spec (written by
+ * python/cheese/rus.py; replaces rus.cu's main, :512-587). Level lines go to on_level as cz_tcount_level (the same
+ * fields). The engine keeps each table resident in device memory after its first use. */
+int cz_rus(cz_engine *engine, const char *rspec, size_t len, const cz_rus_options *opt, cz_tcount_level_fn on_level,
+           void *user, cz_rus_result *out);
+
 /* ---------------- Clifford table (the reference's build/cliffopt, src/clifford.cu) ---------------- */
 /* Tableau of an n <= 3 qubit Clifford up to phase, as the reference packs it (clifford.cu:16-19, 46-58): row
  * i < n is the image of X_i, row n + i the image of Z_i, each row (x bits | z bits << n | sign << 2n) of 2n + 1

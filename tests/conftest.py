@@ -56,3 +56,17 @@ def strip_seconds(lines):
     import re
     pat = re.compile(r'"seconds": [0-9.]+')
     return [pat.sub('"seconds": 0.00', l) for l in lines]
+
+
+def rus_cases():
+    return json.loads((GOLD / "rus_cases.json").read_text())
+
+
+def rus_spec_text(target):
+    """a rus-spec as the reference's writer prints it: the shared blocks (table root, rotations, Cliffords, stored
+    once) joined with the target's roots"""
+    import gzip
+    with gzip.open(GOLD / "rus" / "common.rspec.gz", "rt") as f:
+        common = f.read()
+    root, rest = common.split("\n@@\n")
+    return "rus-spec 1\n" + root + (GOLD / "rus" / f"{target}.roots").read_text() + rest + "end\n"
