@@ -497,9 +497,12 @@ class RusContext {
     cudaMemcpy(ai.data(), tab.Sidx.p, ns * 4, cudaMemcpyDeviceToHost);
     cudaMemcpy(al.data(), tab.Slvl.p, ns * 4, cudaMemcpyDeviceToHost);
     std::fwrite(&ns, sizeof ns, 1, f);
+    std::vector<unsigned char> rec((size_t)ns * 24);
     for (long i = 0; i < ns; i++) {
-      std::fwrite(&a1[i], 8, 1, f); std::fwrite(&a2[i], 8, 1, f); std::fwrite(&ai[i], 4, 1, f); std::fwrite(&al[i], 4, 1, f);
+      unsigned char *r = rec.data() + (size_t)i * 24;
+      std::memcpy(r, &a1[i], 8); std::memcpy(r + 8, &a2[i], 8); std::memcpy(r + 16, &ai[i], 4); std::memcpy(r + 20, &al[i], 4);
     }
+    std::fwrite(rec.data(), 1, rec.size(), f);
     const uint32_t trailer[2] = {RUS_CACHE_MAGIC, RUS_KEY_VERSION};
     std::fwrite(trailer, 4, 2, f);
     std::fwrite(&fp, 8, 1, f);
@@ -530,9 +533,13 @@ class RusContext {
     std::vector<uint32_t> ai, al;
     if (ok) {
       a1.resize(ns); a2.resize(ns); ai.resize(ns); al.resize(ns);
-      for (long i = 0; ok && i < ns; i++)
-        ok = std::fread(&a1[i], 8, 1, f) == 1 && std::fread(&a2[i], 8, 1, f) == 1 && std::fread(&ai[i], 4, 1, f) == 1 &&
-             std::fread(&al[i], 4, 1, f) == 1 && (int)al[i] <= nl;
+      std::vector<unsigned char> rec((size_t)ns * 24);
+      ok = std::fread(rec.data(), 1, rec.size(), f) == rec.size();
+      for (long i = 0; ok && i < ns; i++) {
+        const unsigned char *r = rec.data() + (size_t)i * 24;
+        std::memcpy(&a1[i], r, 8); std::memcpy(&a2[i], r + 8, 8); std::memcpy(&ai[i], r + 16, 4); std::memcpy(&al[i], r + 20, 4);
+        ok = (int)al[i] <= nl;
+      }
     }
     uint32_t trailer[2] = {0, 0};
     uint64_t ffp = 0;
@@ -590,6 +597,7 @@ class RusContext {
         for (int l = 1; l <= opt.table_k; l++) if (!grow(sp, tab->D, tab, cb)) break;
         tab->D.FM.release(); tab->D.F1.release(); tab->D.F2.release();
         res.table_built = true;
+        res.table_seconds = now_s() - t0;           // as the reference reports it: before the cache file is written
         if (opt.use_cache) save(path, *tab, fp);
       }
     } catch (...) {
@@ -597,7 +605,7 @@ class RusContext {
       delete tab;
       throw;
     }
-    res.table_seconds = now_s() - t0;
+    if (!res.table_built) res.table_seconds = now_s() - t0;
     tables[key] = tab;
     return tab;
   }
