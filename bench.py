@@ -205,6 +205,53 @@ def reference_gpu_tcount(eng):
     return out
 
 
+def rus_spec(target):
+    """a committed rus-spec fixture (written by the reference's rus.py): shared blocks joined with the target's roots"""
+    import gzip
+    gold = ROOT / "tests" / "golden" / "rus"
+    with gzip.open(gold / "common.rspec.gz", "rt") as f:
+        root_blk, rest = f.read().split("\n@@\n")
+    return "rus-spec 1\n" + root_blk + (gold / f"{target}.roots").read_text() + rest + "end\n"
+
+
+def rus_leg(eng):
+    """RUS T-count with measurement (the reference's build/rus) on its 0229 regression target: the K = 8 table
+    (5.7M cosets) built in the library, then queries with it resident; beside it the reference's own sm_100a build,
+    one process per query as rus.sh runs it (cold: builds and writes its table; cached: loads it)"""
+    import tempfile
+    try:
+        rspec = rus_spec("ricotta-rus-0229")
+        t0 = time.perf_counter()
+        rc, _, r = eng.rus(rspec, table_k=8, maxt=11, cache_dir=None)
+        first = time.perf_counter() - t0
+        q = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            rc, _, r2 = eng.rus(rspec, table_k=8, maxt=11, cache_dir=None)
+            q.append(time.perf_counter() - t0)
+        out = {"workload": "ricotta-rus-0229 (the reference's RUS regression target), --table 8 --max 11",
+               "rc": rc, "tcount": r2["tcount"], "split": [r2["split_j"], r2["split_c"]],
+               "table_cosets": r["table_cosets"], "table_build_s": r["table_seconds"], "first_call_s": first,
+               "query_ms_median": 1e3 * statistics.median(q)}
+        ref = ROOT / "oracle" / "_ref" / "rus-ref"
+        if ref.exists():
+            d = Path(tempfile.mkdtemp())
+            (d / "build").mkdir()
+            (d / "t.rspec").write_text(rspec)
+            for rep in ("cold", "cached"):
+                t0 = time.perf_counter()
+                p = subprocess.run([str(ref), "t.rspec", "--table", "8", "--max", "11"], cwd=d, capture_output=True,
+                                   text=True, timeout=600)
+                last = json.loads(p.stdout.splitlines()[-1]) if p.stdout.strip() else {}
+                out[f"reference_gpu_{rep}"] = {"rc": p.returncode, "process_s": time.perf_counter() - t0,
+                                               "seconds": last.get("seconds"), "tcount": last.get("tcount"),
+                                               "split": last.get("split")}
+        eng.trim()
+        return out
+    except Exception as e:                     # a failed side leg must not lose the headline line
+        return {"error": str(e)[:300]}
+
+
 def systems(eng, args):
     """the batched, served and table-driven workloads beside the headline metric (one GPU)"""
     import statistics
@@ -335,6 +382,7 @@ def systems(eng, args):
         st["reference_cpu_s"] = time.perf_counter() - t0
         st["reference_cpu_threads"] = os.cpu_count()
     out["state_targets"] = {"workload": "RUS 1 budget 11, RUS 3 budget 11, RUS 8 budget 9 (ancillas in |0>)", **st}
+    out["rus"] = rus_leg(eng)
     # serving: seeded Poisson streams of the mixed workload, against the same requests run one by one
     N = args.serve_requests
     reqs = tcwork.serve_requests(eng, 5, N)

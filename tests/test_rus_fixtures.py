@@ -76,3 +76,9 @@ def test_spec_check():
     for t, msg in bad:
         assert L.cz_rspec_check(t, len(t), C.byref(n), err, 256) == 2, msg
         assert err.value.decode() == msg
+
+
+def test_bench_reads_the_same_specs():
+    import bench
+    for t in {c["target"] for c in CASES}:
+        assert bench.rus_spec(t) == rus_spec_text(t)
