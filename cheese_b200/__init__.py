@@ -72,6 +72,11 @@ class TcResult(C.Structure):
 TC_LEVEL_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(TcLevel))
 
 
+class RspecInfo(C.Structure):
+    _fields_ = [("outcome", C.c_int), ("roots", C.c_int), ("rescalings", C.c_int), ("failure_amplitudes", C.c_int),
+                ("p", C.c_int64 * 3)]
+
+
 class RusResult(C.Structure):
     _fields_ = [("rc", C.c_int), ("tcount", C.c_int), ("split_j", C.c_int), ("split_c", C.c_int), ("maxt", C.c_int),
                 ("root", C.c_uint32), ("cliff", C.c_int), ("fw", C.c_int * 32), ("tb", C.c_int * 32),
@@ -145,6 +150,9 @@ SIGNATURES = {
                                           C.POINTER(C.c_int), C.c_int, C.c_int, C.POINTER(C.c_int), C.c_int,
                                           C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(SpecGenInfo),
                                           C.c_char_p, C.c_size_t]),
+    "cz_rspec_generate": (C.c_int, [C.c_char_p, C.c_size_t, C.c_int, C.c_int, C.POINTER(C.c_char_p),
+                                    C.POINTER(C.c_int), C.c_int, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t),
+                                    C.POINTER(RspecInfo), C.c_char_p, C.c_size_t]),
     "cz_tspec_generate": (C.c_int, [C.c_char_p, C.c_size_t, C.c_int, C.c_int, C.POINTER(C.c_char_p),
                                     C.POINTER(C.c_int), C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t), C.c_char_p,
                                     C.c_size_t]),
@@ -276,6 +284,20 @@ def state_inputs(n, ancilla):
     """the input basis states of a state target whose `ancilla` qubits start in |0> (spec.py state_inputs)"""
     mask = sum(1 << a for a in ancilla)
     return [x for x in range(1 << n) if not x & mask]
+
+
+def rspec_generate(n=None, circ=None, qasm=None, outcome=-1):
+    """the rus-spec of a two-qubit RUS circuit, as the reference's rus.py writes it; returns (text, info dict)"""
+    q, ql, ng, names, qs = _gen_args(circ, qasm)
+    info = RspecInfo()
+
+    def fn(*a):
+        *head, out, cap, need, err, errlen = a
+        return lib().cz_rspec_generate(*head, out, cap, need, C.byref(info), err, errlen)
+    text = _gen_call(fn, q, ql, n or 0, ng, names, qs, outcome)
+    d = {k: getattr(info, k) for k, _ in RspecInfo._fields_ if k != "p"}
+    d["p"] = list(info.p)
+    return text, d
 
 
 def tspec_generate(n=None, circ=None, qasm=None):

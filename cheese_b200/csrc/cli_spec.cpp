@@ -4,6 +4,8 @@
 //                                             --inputs (or --ancilla: every basis state with those qubits 0) the
 //                                             state-target spec (spec.py:418-424)
 //   cheese-spec --tcount TARGET.qasm          the T-count spec (python -m cheese.tcount spec, tcount.py:171-174)
+//   cheese-spec --rus TARGET.qasm [--outcome K]
+//                                             the RUS spec (python -m cheese.rus spec, rus.py:334-342)
 #include <climits>
 #include <cstdio>
 #include <cstdlib>
@@ -17,12 +19,14 @@
 
 static int usage() {
   std::fprintf(stderr, "usage: cheese-spec TARGET.qasm DEPTH [--no-w3] [--ancilla Q ..] [--inputs A,B,..]\n"
-                       "       cheese-spec --tcount TARGET.qasm\n");
+                       "       cheese-spec --tcount TARGET.qasm\n"
+                       "       cheese-spec --rus TARGET.qasm [--outcome K]\n");
   return 2;
 }
 
 int main(int argc, char **argv) {
-  bool tcount = false, no_w3 = false, have_inputs = false;
+  bool tcount = false, rus = false, no_w3 = false, have_inputs = false;
+  int outcome = -1;
   std::vector<const char *> pos;
   std::vector<int> ancilla, inputs;
   auto integer = [](const char *a, int &v) {
@@ -35,6 +39,10 @@ int main(int argc, char **argv) {
   for (int i = 1; i < argc; i++) {
     int v;
     if (!std::strcmp(argv[i], "--tcount")) tcount = true;
+    else if (!std::strcmp(argv[i], "--rus")) rus = true;
+    else if (!std::strcmp(argv[i], "--outcome")) {
+      if (++i >= argc || !integer(argv[i], outcome)) return usage();
+    }
     else if (!std::strcmp(argv[i], "--no-w3")) no_w3 = true;
     else if (!std::strcmp(argv[i], "--ancilla")) {      // one or more qubit indices
       const size_t before = ancilla.size();
@@ -55,7 +63,8 @@ int main(int argc, char **argv) {
     } else if (argv[i][0] == '-' && argv[i][1] == '-') return usage();
     else pos.push_back(argv[i]);
   }
-  if (pos.size() != (tcount ? 1u : 2u)) return usage();
+  if (tcount && rus) return usage();
+  if (pos.size() != (tcount || rus ? 1u : 2u)) return usage();
   std::ifstream f(pos[0], std::ios::binary);
   if (!f) { std::fprintf(stderr, "cannot read %s\n", pos[0]); return 2; }
   std::stringstream ss;
@@ -78,6 +87,21 @@ int main(int argc, char **argv) {
     if (rc == 2) { std::fprintf(stderr, "%s\n", err); return 2; }
     for (long long x = 0; x < (1LL << info.n); x++)
       if (!(x & mask)) inputs.push_back((int)x);
+  }
+  if (rus) {
+    cz_rspec_info ri;
+    for (int attempt = 0; attempt < 2; attempt++) {
+      rc = cz_rspec_generate(q.data(), q.size(), 0, 0, nullptr, nullptr, outcome, out.data(), out.size(), &need, &ri, err,
+                             sizeof err);
+      if (rc != 3) break;
+      out.assign(need + 1, 0);
+    }
+    if (rc) { std::fprintf(stderr, "%s\n", err); return 2; }
+    std::fprintf(stderr, "{\"outcome\": %d, \"roots\": %d, \"p\": [%lld, %lld, %lld], \"rescalings\": %d, "
+                         "\"failure_amplitudes\": %d}\n", ri.outcome, ri.roots, (long long)ri.p[0], (long long)ri.p[1],
+                 (long long)ri.p[2], ri.rescalings, ri.failure_amplitudes);
+    std::fwrite(out.data(), 1, need, stdout);
+    return 0;
   }
   for (int attempt = 0; attempt < 2; attempt++) {
     rc = tcount ? cz_tspec_generate(q.data(), q.size(), 0, 0, nullptr, nullptr, out.data(), out.size(), &need, err,

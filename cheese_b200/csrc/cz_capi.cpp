@@ -625,6 +625,27 @@ int cz_spec_generate_states(const char *qasm, size_t qasm_len, int n, int ngates
   return specgen_out(text, out, cap, out_len);
 }
 
+int cz_rspec_generate(const char *qasm, size_t qasm_len, int n, int ngates, const char *const *names,
+                      const int *qubits, int outcome, char *out, size_t cap, size_t *out_len, cz_rspec_info *info,
+                      char *err, size_t errlen) {
+  std::string e, text;
+  std::vector<cz::CircGate> circ;
+  int nq = 0;
+  int rc = specgen_input(qasm, qasm_len, n, ngates, names, qubits, nq, circ, e);
+  cz::RusSpecInfo ri;
+  if (!rc) rc = cz::rspec_generate(nq, circ, qasm ? std::string(qasm, qasm_len) : std::string(), outcome, text, ri, e);
+  if (rc) {
+    put_err(err, errlen, e);
+    return rc;
+  }
+  if (info) {
+    info->outcome = ri.outcome; info->roots = ri.roots; info->rescalings = ri.rescalings;
+    info->failure_amplitudes = ri.failure_amplitudes;
+    for (int i = 0; i < 3; i++) info->p[i] = ri.p[i];
+  }
+  return specgen_out(text, out, cap, out_len);
+}
+
 int cz_tspec_generate(const char *qasm, size_t qasm_len, int n, int ngates, const char *const *names,
                       const int *qubits, char *out, size_t cap, size_t *out_len, char *err, size_t errlen) {
   std::string e, text;

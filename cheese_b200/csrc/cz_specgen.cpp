@@ -612,6 +612,303 @@ std::shared_ptr<const GateSetPart> gate_set_part(int n, const std::vector<std::s
   return it->second;
 }
 
+// P_p on n qubits, digits per qubit (0 I, 1 X, 2 Y, 3 Z) at bits 2q (tcount.py pauli_matrix)
+std::vector<Mat> pauli_mats(int n) {
+  const int P = 1 << (2 * n), N = 1 << n;
+  std::vector<Mat> paulis(P);
+  for (int p = 0; p < P; p++) {
+    Mat M;
+    M.N = N;
+    M.e.assign((size_t)N * N, Z{});
+    for (int x = 0; x < N; x++) {
+      int flip = 0, ph = 0;
+      for (int q = 0; q < n; q++) {
+        const int dg = (p >> (2 * q)) & 3, bit = (x >> q) & 1;
+        if (dg == 1) flip |= 1 << q;
+        else if (dg == 2) { flip |= 1 << q; ph += 2 + 4 * bit; }
+        else if (dg == 3) ph += 4 * bit;
+      }
+      M.at(x ^ flip, x) = wpow(ph);
+    }
+    paulis[p] = M;
+  }
+  return paulis;
+}
+// the rotation tables (tcount.py pauli_tables): for each P_p (p >= 1) and Pauli c, (-1, 0) when they commute, else
+// (r, sign) with i P_p P_c = sign P_r; false if some product is not a signed Pauli
+bool rotation_block(int n, const std::vector<Mat> &paulis, std::string &out) {
+  const int P = 1 << (2 * n);
+  out += "rotations " + std::to_string(P - 1) + "\n";
+  const Z iw{0, 0, 1, 0};
+  for (int p = 1; p < P; p++) {
+    for (int c = 0; c < P; c++) {
+      const Mat M1 = matmul(paulis[p], paulis[c]), M2 = matmul(paulis[c], paulis[p]);
+      int hr = -1, hs = 0;
+      if (M1.e != M2.e) {
+        std::vector<Z> M(M1.e.size());
+        for (size_t i = 0; i < M.size(); i++) M[i] = zmul(iw, M1.e[i]);
+        for (int r = 0; r < P && hr < 0; r++)
+          for (int sign : {1, -1}) {
+            bool eq = true;
+            for (size_t i = 0; i < M.size() && eq; i++) {
+              const Z &q = paulis[r].e[i];
+              eq = M[i] == Z{sign * q.a, sign * q.b, sign * q.c, sign * q.d};
+            }
+            if (eq) { hr = r; hs = sign; }
+          }
+        if (hr < 0) return false;
+      }
+      out += (c ? " " : "") + std::to_string(hr) + " " + std::to_string(hs);
+    }
+    out += "\n";
+  }
+  return true;
+}
+
+// ---------- RUS specs (python/cheese/rus.py): roots of a two-qubit RUS circuit, table root, Clifford list ----------
+
+// exact rationals (reduced, denominator > 0); numerators and denominators stay below 2^62 so products fit __int128
+struct Rat { __int128 n = 0, d = 1; };
+__int128 gcd128(__int128 a, __int128 b) {
+  if (a < 0) a = -a;
+  if (b < 0) b = -b;
+  while (b) { const __int128 t = a % b; a = b; b = t; }
+  return a;
+}
+Rat rat(__int128 n, __int128 d) {
+  if (d == 0) throw std::overflow_error("division by zero");
+  if (d < 0) { n = -n; d = -d; }
+  const __int128 g = gcd128(n, d);
+  if (g > 1) { n /= g; d /= g; }
+  const __int128 lim = (__int128)1 << 62;
+  if (n >= lim || n <= -lim || d >= lim) throw std::overflow_error("coefficient exceeds 62 bits");
+  return {n, d};
+}
+Rat radd(const Rat &a, const Rat &b) { return rat(a.n * b.d + b.n * a.d, a.d * b.d); }
+Rat rsub(const Rat &a, const Rat &b) { return rat(a.n * b.d - b.n * a.d, a.d * b.d); }
+Rat rmul(const Rat &a, const Rat &b) { return rat(a.n * b.n, a.d * b.d); }
+Rat rint(int64_t v) { return Rat{v, 1}; }
+using QW = std::array<Rat, 4>;                     // an element of Q(w), coefficients of 1, w, w^2, w^3
+QW qw(const Z &z) { return {rint(z.a), rint(z.b), rint(z.c), rint(z.d)}; }
+QW qmul(const QW &x, const QW &y) {                // w^4 = -1
+  QW o = {rint(0), rint(0), rint(0), rint(0)};
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) {
+      const Rat p = rmul(x[i], y[j]);
+      o[(i + j) % 4] = i + j < 4 ? radd(o[(i + j) % 4], p) : rsub(o[(i + j) % 4], p);
+    }
+  return o;
+}
+QW qup(const QW &z) { return {rsub(z[1], z[3]), radd(z[0], z[2]), radd(z[1], z[3]), rsub(z[2], z[0])}; }   // times sqrt2
+
+// |z|^2 = A + B sqrt2 for z in Z[w]
+std::pair<int64_t, int64_t> norm2(const Z &z) {
+  return {chk((__int128)z.a * z.a + (__int128)z.b * z.b + (__int128)z.c * z.c + (__int128)z.d * z.d),
+          chk((__int128)z.a * z.b + (__int128)z.b * z.c + (__int128)z.c * z.d - (__int128)z.a * z.d)};
+}
+// iteration order of the Python set {s, -s} (CPython: 8 slots, hash(v) = v except hash(-1) = -2, probe
+// i = 5 i + 1 + perturb with perturb shifted right by 5), which orders the reference's norm solutions
+std::vector<int64_t> py_pair_order(int64_t s) {
+  if (s == 0) return {0};
+  int64_t slot[8] = {0};
+  bool used[8] = {false};
+  for (int64_t v : {s, -s}) {
+    const uint64_t h = (uint64_t)(v == -1 ? -2 : v);
+    uint64_t i = h & 7, perturb = h;
+    while (used[i]) { perturb >>= 5; i = (i * 5 + 1 + perturb) & 7; }
+    used[i] = true;
+    slot[i] = v;
+  }
+  std::vector<int64_t> out;
+  for (int i = 0; i < 8; i++) if (used[i]) out.push_back(slot[i]);
+  return out;
+}
+// every z in Z[w] with |z|^2 = A + B sqrt2, in the reference's enumeration order (rus.py norm_solutions)
+std::vector<Z> norm_solutions(int64_t A, int64_t B) {
+  if (A < 0) throw std::overflow_error("negative norm: not a RUS circuit");
+  int64_t r = 0;
+  while ((r + 1) * (r + 1) <= A) r++;
+  r += 1;
+  std::map<int64_t, int64_t> sq;
+  for (int64_t i = 0; i <= r; i++) sq[i * i] = i;
+  std::vector<Z> out;
+  for (int64_t x0 = -r; x0 <= r; x0++)
+    for (int64_t x1 = -r; x1 <= r; x1++)
+      for (int64_t x2 = -r; x2 <= r; x2++) {
+        auto it = sq.find(A - x0 * x0 - x1 * x1 - x2 * x2);
+        if (it == sq.end()) continue;
+        for (int64_t x3 : py_pair_order(it->second))
+          if (x0 * x1 + x1 * x2 + x2 * x3 - x0 * x3 == B) out.push_back(Z{x0, x1, x2, x3});
+      }
+  return out;
+}
+
+// a Pauli transfer matrix of a 4 x 2 isometry: 16 x 4 entries (x + y sqrt2) / sqrt2^e
+struct Ptm {
+  int e = 0;
+  std::vector<std::array<int64_t, 2>> v;           // row-major 16 x 4
+};
+// Jc[a][b] = Tr(P_a J P_b J^dag) / 2, normalised (rus.py ptm); J is 4 x 2 over sqrt2^k, row 2 i + ancilla
+Ptm ptm(const std::vector<Z> &J, int k) {
+  const std::vector<Mat> P16 = pauli_mats(2), P1 = pauli_mats(1);
+  Ptm X;
+  X.v.resize(64);
+  for (int b = 0; b < 4; b++) {
+    Z A[4][4];                                      // J P_b J^dag, over sqrt2^(2k)
+    for (int r = 0; r < 4; r++)
+      for (int c = 0; c < 4; c++) {
+        Z acc;
+        for (int i = 0; i < 2; i++)
+          for (int j = 0; j < 2; j++) {
+            const Z &p = P1[b].at(i, j);
+            if (p.zero() || J[r * 2 + i].zero() || J[c * 2 + j].zero()) continue;
+            acc = zadd(acc, zmul(zmul(J[r * 2 + i], p), conj(J[c * 2 + j])));
+          }
+        A[r][c] = acc;
+      }
+    for (int a = 0; a < 16; a++) {
+      Z tr;
+      for (int r = 0; r < 4; r++)
+        for (int c = 0; c < 4; c++)
+          if (!P16[a].at(r, c).zero() && !A[c][r].zero()) tr = zadd(tr, zmul(P16[a].at(r, c), A[c][r]));
+      if (tr.c != 0 || tr.d != -tr.b) throw std::overflow_error("transfer-matrix entry not real");
+      X.v[a * 4 + b] = {tr.a, tr.b};
+    }
+  }
+  X.e = 2 * k + 2;                                  // the trace's sqrt2^(2k) and the 1/2
+  while (X.e > 0) {
+    bool even = true;
+    for (const auto &t : X.v) even = even && (t[0] % 2 == 0);
+    if (!even) break;
+    for (auto &t : X.v) t = {t[1], t[0] / 2};       // (x + y s) / s = y + (x / 2) s
+    X.e--;
+  }
+  return X;
+}
+
+// the 11520 two-qubit Cliffords mod phase as row actions C^dag P_a C = s P_pi(a), in breadth-first order over the
+// generators h q0, h q1, s q0, s q1, cz (rus.py cliffords)
+struct CliffordList {
+  std::vector<std::array<int8_t, 16>> perm, sign;
+  std::map<std::array<int, 4>, int> bygen;          // images (row, sign) of X_q0, Z_q0, X_q1, Z_q1 -> index
+};
+const CliffordList &clifford_list() {
+  static const CliffordList L = [] {
+    CliffordList out;
+    const std::vector<Mat> P16 = pauli_mats(2);
+    const std::pair<const char *, std::array<int, 2>> gens[5] = {
+        {"h", {0, -1}}, {"h", {1, -1}}, {"s", {0, -1}}, {"s", {1, -1}}, {"cz", {0, 1}}};
+    std::vector<std::array<int8_t, 16>> gp(5), gs(5);
+    for (int g = 0; g < 5; g++) {
+      const Mat C = gate_matrix(gates().at(gens[g].first), gens[g].second.data(), 2), Cd = dagger(C);
+      for (int a = 0; a < 16; a++) {
+        const Mat A = matmul(matmul(Cd, P16[a]), C);
+        int hb = -1, hs = 0;
+        for (int b = 0; b < 16 && hb < 0; b++)
+          for (int sg : {1, -1}) {
+            bool eq = true;
+            for (size_t i = 0; i < A.e.size() && eq; i++) {
+              const Z &q = P16[b].e[i];
+              eq = A.e[i] == Z{sg * q.a, sg * q.b, sg * q.c, sg * q.d};
+            }
+            if (eq && hb < 0) { hb = b; hs = sg; }
+          }
+        if (hb < 0) throw std::logic_error("Clifford generator does not map Paulis to Paulis");
+        gp[g][a] = (int8_t)hb;
+        gs[g][a] = (int8_t)hs;
+      }
+    }
+    std::array<int8_t, 16> ip, is;
+    for (int a = 0; a < 16; a++) { ip[a] = (int8_t)a; is[a] = 1; }
+    std::set<std::pair<std::array<int8_t, 16>, std::array<int8_t, 16>>> seen{{ip, is}};
+    out.perm.push_back(ip); out.sign.push_back(is);
+    std::vector<size_t> frontier{0};
+    while (!frontier.empty()) {
+      std::vector<size_t> nxt;
+      for (size_t f : frontier)
+        for (int g = 0; g < 5; g++) {               // G C: (G C)^dag P (G C) = C^dag (G^dag P G) C
+          std::array<int8_t, 16> bp, bs;
+          for (int x = 0; x < 16; x++) {
+            bp[x] = out.perm[f][gp[g][x]];
+            bs[x] = (int8_t)(gs[g][x] * out.sign[f][gp[g][x]]);
+          }
+          if (seen.insert({bp, bs}).second) {
+            out.perm.push_back(bp); out.sign.push_back(bs);
+            nxt.push_back(out.perm.size() - 1);
+          }
+        }
+      frontier = nxt;
+    }
+    if (out.perm.size() != 11520) throw std::logic_error("two-qubit Clifford group order");
+    const int G4[4] = {1, 3, 4, 12};
+    for (size_t c = 0; c < out.perm.size(); c++) {
+      std::array<int, 4> key;
+      for (int g = 0; g < 4; g++) key[g] = out.perm[c][G4[g]] * 2 + (out.sign[c][G4[g]] < 0);
+      out.bygen.emplace(key, (int)c);
+    }
+    return out;
+  }();
+  return L;
+}
+// some Clifford c with B = C_c A (B[x] = s_c(x) A[pi_c(x)] for every row)
+bool ptm_equivalent(const Ptm &A, const Ptm &B) {
+  if (A.e != B.e) return false;
+  const CliffordList &L = clifford_list();
+  auto row_eq = [&](int ra, int s, int rb) {
+    for (int c = 0; c < 4; c++)
+      if (s * A.v[ra * 4 + c][0] != B.v[rb * 4 + c][0] || s * A.v[ra * 4 + c][1] != B.v[rb * 4 + c][1]) return false;
+    return true;
+  };
+  const int G4[4] = {1, 3, 4, 12};
+  std::vector<int> cand[4];
+  for (int g = 0; g < 4; g++) {
+    for (int r = 1; r < 16; r++)
+      for (int s : {1, -1})
+        if (row_eq(r, s, G4[g])) cand[g].push_back(r * 2 + (s < 0));
+    if (cand[g].empty()) return false;
+  }
+  for (int i0 : cand[0]) for (int i1 : cand[1]) for (int i2 : cand[2]) for (int i3 : cand[3]) {
+    auto it = L.bygen.find({i0, i1, i2, i3});
+    if (it == L.bygen.end()) continue;
+    const int c = it->second;
+    bool ok = true;
+    for (int x = 0; x < 16 && ok; x++) ok = row_eq(L.perm[c][x], L.sign[c][x], x);
+    if (ok) return true;
+  }
+  return false;
+}
+
+// 1 x 1 normal form of A when A is a multiple of the identity (rus.py scalar)
+bool scalar(const Mat &A, int &k, Z &z) {
+  for (int r = 0; r < A.N; r++)
+    for (int c = 0; c < A.N; c++)
+      if (r != c ? !A.at(r, c).zero() : A.at(r, c) != A.at(0, 0)) return false;
+  Mat S;
+  S.N = 1; S.k = A.k; S.e = {A.at(0, 0)};
+  normalise(S);
+  k = S.k;
+  z = S.e[0];
+  return true;
+}
+// B / sqrt2^k proportional to a one-qubit Clifford: B B^dag = q I and B P B^dag Q = +-q I (rus.py clifford_block)
+bool clifford_block(const Mat &B) {
+  int kg;
+  Z zg;
+  if (!scalar(matmul(B, dagger(B)), kg, zg) || zg.zero()) return false;
+  const std::vector<Mat> P1 = pauli_mats(1);
+  for (int p : {1, 3}) {
+    const Mat A = matmul(matmul(B, P1[p]), dagger(B));
+    bool any = false;
+    for (int q : {1, 2, 3}) {
+      int k;
+      Z z;
+      if (scalar(matmul(A, P1[q]), k, z) && k == kg && (z == zg || z == Z{-zg.a, -zg.b, -zg.c, -zg.d})) any = true;
+    }
+    if (!any) return false;
+  }
+  return true;
+}
+
 int check_circuit(int n, const std::vector<CircGate> &circ, std::string &err) {
   if (n < 1 || n > 6) { err = "n = " + std::to_string(n) + " out of range (1..6)"; return 2; }
   for (const CircGate &g : circ) {
@@ -758,23 +1055,7 @@ int tspec_generate(int n, const std::vector<CircGate> &circ, std::string &out, s
     if (n > 4) { err = "T-count specs for n <= 4"; return 2; }
     const Mat U = unitary(n, circ);
     const int P = 1 << (2 * n), N = 1 << n;
-    std::vector<Mat> paulis(P);
-    for (int p = 0; p < P; p++) {
-      Mat M;
-      M.N = N;
-      M.e.assign((size_t)N * N, Z{});
-      for (int x = 0; x < N; x++) {
-        int flip = 0, ph = 0;
-        for (int q = 0; q < n; q++) {
-          const int dg = (p >> (2 * q)) & 3, bit = (x >> q) & 1;
-          if (dg == 1) flip |= 1 << q;
-          else if (dg == 2) { flip |= 1 << q; ph += 2 + 4 * bit; }
-          else if (dg == 3) ph += 4 * bit;
-        }
-        M.at(x ^ flip, x) = wpow(ph);
-      }
-      paulis[p] = M;
-    }
+    const std::vector<Mat> paulis = pauli_mats(n);
     // channel: Uc[a][b] = Tr(P_a U P_b U^dag) / 2^n = (x + y sqrt2) / sqrt2^e, one exponent for the matrix
     const Mat Ud = dagger(U);
     std::vector<int> ks((size_t)P * P);
@@ -810,31 +1091,171 @@ int tspec_generate(int n, const std::vector<CircGate> &circ, std::string &out, s
     }
     // rotation tables: for each P_p (p >= 1) and Pauli c, (-1, 0) when they commute, else (r, sign) with
     // i P_p P_c = sign P_r
-    out += "rotations " + std::to_string(P - 1) + "\n";
-    const Z iw{0, 0, 1, 0};
-    for (int p = 1; p < P; p++) {
-      for (int c = 0; c < P; c++) {
-        const Mat M1 = matmul(paulis[p], paulis[c]), M2 = matmul(paulis[c], paulis[p]);
-        int hr = -1, hs = 0;
-        if (M1.e != M2.e) {
-          std::vector<Z> M(M1.e.size());
-          for (size_t i = 0; i < M.size(); i++) M[i] = zmul(iw, M1.e[i]);
-          for (int r = 0; r < P && hr < 0; r++)
-            for (int sign : {1, -1}) {
-              bool eq = true;
-              for (size_t i = 0; i < M.size() && eq; i++) {
-                const Z &q = paulis[r].e[i];
-                eq = M[i] == Z{sign * q.a, sign * q.b, sign * q.c, sign * q.d};
-              }
-              if (eq) { hr = r; hs = sign; }
-            }
-          if (hr < 0) { err = "i P Q is not a signed Pauli"; return 2; }
-        }
-        out += (c ? " " : "") + std::to_string(hr) + " " + std::to_string(hs);
+    if (!rotation_block(n, paulis, out)) { err = "i P Q is not a signed Pauli"; return 2; }
+    out += "end\n";
+    return 0;
+  } catch (const std::overflow_error &e) {
+    err = e.what();
+    return 2;
+  }
+}
+
+int rspec_generate(int n, const std::vector<CircGate> &circ, const std::string &qasm_text, int outcome,
+                   std::string &out, RusSpecInfo &info, std::string &err) {
+  try {
+    if (int rc = check_circuit(n, circ, err)) return rc;
+    if (n != 2) { err = "RUS mode: two qubits (q0 ancilla, measured; q1 data)"; return 2; }
+    const Mat W = unitary(n, circ);
+    // blocks B_o[i][j] = <o, i| W |0, j> (ancilla q0 = bit 0 of an index)
+    Mat Bk[2];
+    for (int o = 0; o < 2; o++) {
+      Bk[o].N = 2; Bk[o].k = W.k; Bk[o].e.assign(4, Z{});
+      for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) Bk[o].at(i, j) = W.at(o + 2 * i, 2 * j);
+    }
+    int ks = outcome;
+    if (ks < 0) {                                   // a "success outcome K" comment, else the non-Clifford branch
+      const size_t at = qasm_text.find("success outcome ");
+      if (at != std::string::npos && at + 16 < qasm_text.size() && isdigit((unsigned char)qasm_text[at + 16])) {
+        ks = qasm_text[at + 16] - '0';
+      } else {
+        const bool c0 = clifford_block(Bk[0]), c1 = clifford_block(Bk[1]);
+        if (c0 == c1) { err = "not a RUS circuit: need exactly one branch proportional to a Clifford"; return 2; }
+        ks = c0 ? 1 : 0;
       }
+    }
+    if (ks != 0 && ks != 1) { err = "success outcome must be 0 or 1"; return 2; }
+    const Mat &M = Bk[ks];
+    const int kW = W.k, m = kW + 1;                 // Pr[success] = (A + B sqrt2) / 2^m
+    int64_t A = 0, Bs = 0;
+    for (const Z &z : M.e) { const auto nz = norm2(z); A = chk((__int128)A + nz.first); Bs = chk((__int128)Bs + nz.second); }
+    if (m > 60) { err = "coefficient overflow"; return 2; }
+    std::vector<Z> gam = norm_solutions(((int64_t)1 << m) - A, -Bs);   // gamma = g / sqrt2^m, |gamma|^2 = 1 - p
+    // one gamma per orbit {w^k gamma}: keyed by the smallest w^k gamma, first position, last value (a Python dict)
+    std::vector<std::pair<std::array<int64_t, 4>, Z>> orbit;
+    for (const Z &g : gam) {
+      std::array<int64_t, 4> key{};
+      for (int k = 0; k < 8; k++) {
+        const Z r = zmul(wpow(k), g);
+        const std::array<int64_t, 4> t{r.a, r.b, r.c, r.d};
+        if (k == 0 || t < key) key = t;
+      }
+      auto it = std::find_if(orbit.begin(), orbit.end(), [&](const auto &e) { return e.first == key; });
+      if (it == orbit.end()) orbit.push_back({key, g}); else it->second = g;
+    }
+    // rescalings u = h / m0 (|u| = 1) that keep u M exact
+    Z m0;
+    for (const Z &z : M.e) if (!z.zero()) { m0 = z; break; }
+    if (m0.zero()) { err = "zero success block"; return 2; }
+    const auto nm = norm2(m0);
+    const Rat d = rat((__int128)nm.first * nm.first - (__int128)2 * nm.second * nm.second, 1);
+    const Rat invd = rat(d.d, d.n);                 // 1 / |m0|^2 = (a0 - b0 sqrt2) / (a0^2 - 2 b0^2)
+    const QW inv = {rmul(rint(nm.first), invd), rmul(rint(-nm.second), invd), rint(0), rmul(rint(nm.second), invd)};
+    std::vector<QW> us;
+    for (const Z &h : norm_solutions(nm.first, nm.second)) {
+      const QW u = qmul(qmul(qw(h), qw(conj(m0))), inv);
+      bool exact = true;
+      for (const Z &z : M.e) {
+        const QW v = qmul(u, qw(z));
+        for (const Rat &c : v) exact = exact && ((c.d & (c.d - 1)) == 0);
+      }
+      if (exact) us.push_back(u);
+    }
+    // one-qubit Cliffords mod phase, one per coset of the left Paulis (6 of 24), in breadth-first order over h, s
+    const std::vector<Mat> P1 = pauli_mats(1);
+    auto phase_key = [](const Mat &U) {             // min over global phases of the entries, then the exponent
+      std::vector<int64_t> best;
+      for (int ph = 0; ph < 8; ph++) {
+        std::vector<int64_t> t;
+        for (const Z &x : U.e) { const Z r = zmul(wpow(ph), x); t.insert(t.end(), {r.a, r.b, r.c, r.d}); }
+        if (ph == 0 || t < best) best = t;
+      }
+      best.push_back(U.k);
+      return best;
+    };
+    const int q0[1] = {0};
+    const Mat Hg = gate_matrix(gates().at("h"), q0, 1), Sg = gate_matrix(gates().at("s"), q0, 1);
+    std::vector<Mat> D1, fr{identity(2)};
+    std::set<std::vector<int64_t>> allD, seenD;
+    while (!fr.empty()) {
+      std::vector<Mat> nx;
+      for (const Mat &U : fr) {
+        if (!allD.insert(phase_key(U)).second) continue;
+        nx.push_back(matmul(Hg, U));
+        nx.push_back(matmul(Sg, U));
+        std::vector<int64_t> coset;
+        for (int q = 0; q < 4; q++) {
+          const std::vector<int64_t> k = phase_key(matmul(P1[q], U));
+          if (q == 0 || k < coset) coset = k;
+        }
+        if (seenD.insert(coset).second) D1.push_back(U);
+      }
+      fr = nx;
+    }
+    if (allD.size() != 24 || D1.size() != 6) { err = "one-qubit Clifford enumeration"; return 2; }
+    // roots: success block u M (outcome moved to 0), failure block gamma D, distinct up to left Cliffords
+    std::vector<Ptm> roots;
+    for (const QW &u : us)
+      for (const auto &og : orbit)
+        for (const Mat &D : D1) {
+          QW vals[8];
+          for (int i = 0; i < 2; i++)
+            for (int anc = 0; anc < 2; anc++)
+              for (int j = 0; j < 2; j++) {
+                QW v;
+                int k;
+                if (anc == 0) { v = qmul(u, qw(M.at(i, j))); k = kW; }
+                else { v = qw(zmul(og.second, D.at(i, j))); k = m + D.k; }
+                for (int t = 0; t < k; t++) {
+                  v = qup(v);
+                  for (Rat &c : v) c = rat(c.n, c.d * 2);
+                }
+                vals[4 * i + 2 * anc + j] = v;
+              }
+          int E = 0;
+          for (;;) {
+            bool integral = true;
+            for (const QW &v : vals) for (const Rat &c : v) integral = integral && c.d == 1;
+            if (integral) break;
+            for (QW &v : vals) v = qup(v);
+            if (++E > 200) { err = "coefficient overflow"; return 2; }
+          }
+          std::vector<Z> J(8);
+          for (int r = 0; r < 8; r++) J[r] = Z{(int64_t)vals[r][0].n, (int64_t)vals[r][1].n, (int64_t)vals[r][2].n,
+                                               (int64_t)vals[r][3].n};
+          const Ptm X = ptm(J, E);
+          bool fresh = true;
+          for (const Ptm &Y : roots) fresh = fresh && !ptm_equivalent(Y, X);
+          if (fresh) roots.push_back(X);
+        }
+    auto mat = [](const Ptm &X) {
+      std::string t = std::to_string(X.e) + "\n";
+      for (int a = 0; a < 16; a++) {
+        for (int b = 0; b < 4; b++)
+          t += (b ? " " : "") + std::to_string(X.v[a * 4 + b][0]) + " " + std::to_string(X.v[a * 4 + b][1]);
+        t += "\n";
+      }
+      return t;
+    };
+    std::vector<Z> j00(8);
+    j00[0] = Z{1, 0, 0, 0};                         // J00 = |0> x I: row 2 i + 0, column i
+    j00[5] = Z{1, 0, 0, 0};
+    out = "rus-spec 1\ntable-root\n" + mat(ptm(j00, 0));
+    out += "roots " + std::to_string(roots.size()) + "\n";
+    for (const Ptm &X : roots) out += mat(X);
+    if (!rotation_block(2, pauli_mats(2), out)) { err = "i P Q is not a signed Pauli"; return 2; }
+    const CliffordList &L = clifford_list();
+    out += "cliffords " + std::to_string(L.perm.size()) + "\n";
+    for (size_t c = 0; c < L.perm.size(); c++) {
+      for (int x = 0; x < 16; x++) out += (x ? " " : "") + std::to_string(L.perm[c][x]) + " " + std::to_string(L.sign[c][x]);
       out += "\n";
     }
     out += "end\n";
+    info.outcome = ks;
+    info.roots = (int)roots.size();
+    info.p[0] = A; info.p[1] = Bs; info.p[2] = m;
+    info.rescalings = (int)us.size();
+    info.failure_amplitudes = (int)orbit.size();
     return 0;
   } catch (const std::overflow_error &e) {
     err = e.what();

@@ -3,6 +3,7 @@
 // Z[w] arithmetic. The per-gate-set parts (candidates, window rules, CX table) are cached, so a served request pays
 // only for its target.
 #pragma once
+#include <cstdint>
 #include <string>
 #include <vector>
 
@@ -27,5 +28,13 @@ int spec_generate(int n, const std::vector<CircGate> &circ, int depth, bool use_
                   std::string &out, SpecGenInfo &info, std::string &err);
 // the T-count spec (channel representation and Pauli rotation tables) of the circuit's unitary
 int tspec_generate(int n, const std::vector<CircGate> &circ, std::string &out, std::string &err);
+
+struct RusSpecInfo { int outcome = 0, roots = 0, rescalings = 0, failure_amplitudes = 0; int64_t p[3] = {0, 0, 0}; };
+// the rus-spec of a two-qubit RUS circuit (q0 ancilla, measured; q1 data), as python/cheese/rus.py spec writes it:
+// the table root J00, the roots (every valid isometry for this success branch up to left Cliffords), the rotation
+// tables and the 11520 Cliffords. outcome: the success outcome, or -1 for the "success outcome K" comment in
+// qasm_text, else the branch that is not proportional to a Clifford. Returns 0, or 2 with err.
+int rspec_generate(int n, const std::vector<CircGate> &circ, const std::string &qasm_text, int outcome,
+                   std::string &out, RusSpecInfo &info, std::string &err);
 
 }  // namespace cz

@@ -390,6 +390,20 @@ int cz_spec_generate_states(const char *qasm, size_t qasm_len, int n, int ngates
 int cz_tspec_generate(const char *qasm, size_t qasm_len, int n, int ngates, const char *const *names,
                       const int *qubits, char *out, size_t cap, size_t *out_len, char *err, size_t errlen);
 
+/* The rus-spec of a two-qubit repeat-until-success circuit (q0 ancilla, measured; q1 data), as `python -m cheese.rus
+ * spec TARGET.qasm [--outcome K]` writes it (rus.py:214-303): the table root, the roots (every valid isometry for
+ * the success branch up to left Cliffords), the rotation tables and the 11520 Cliffords. outcome: the success
+ * outcome, or -1 for the QASM text's "success outcome K" comment, else the branch not proportional to a Clifford.
+ * info (may be NULL): outcome, roots, p = (A, B, m) with Pr[success] = (A + B sqrt2) / 2^m, rescalings, failure
+ * amplitudes. Circuit input, out, out_len and returns as cz_spec_generate. */
+typedef struct {
+  int outcome, roots, rescalings, failure_amplitudes;
+  int64_t p[3];
+} cz_rspec_info;
+int cz_rspec_generate(const char *qasm, size_t qasm_len, int n, int ngates, const char *const *names,
+                      const int *qubits, int outcome, char *out, size_t cap, size_t *out_len, cz_rspec_info *info,
+                      char *err, size_t errlen);
+
 /* The library version string and the CUDA architecture it was compiled for ("sm_100a"). */
 const char *cz_version(void);
 

@@ -17,6 +17,8 @@ Writes
   tests/golden/rus/common.rspec.gz     table-root, rotations and cliffords blocks
   tests/golden/rus/<target>.roots      the roots block of each target
   tests/golden/rus_cases.json          per case: target, flags, exit code, stdout ("seconds" 0.00), verified
+  tests/golden/rus_spec_cases.json     (--specgen-only) variant RUS circuits with the reference writer's roots
+                                       block and its info line, for the C++ writer
 """
 import argparse
 import gzip
@@ -48,10 +50,58 @@ def join_spec(common, roots):
     return "rus-spec 1\n" + root + roots + rest + "end\n"
 
 
+def variants(ref):
+    """The regression targets themselves, and RUS circuits derived from them: seeded Clifford gates on the data qubit before and after
+    (and a CZ after: a Pauli correction per outcome), some with the outcomes swapped by an X on the ancilla; comments
+    dropped, so the writer detects the success outcome. Their optimal RUS T-counts equal the targets' (Cliffords
+    are free on either side)."""
+    import random
+    rng = random.Random(7301)
+    out = []
+    for stem in ("ricotta-rus-0003", "ricotta-rus-0229"):
+        text = (Path(ref) / "tests" / "qasm" / f"{stem}.qasm").read_text()
+        out.append((stem, stem, text))              # as is: its "success outcome" comment names the outcome
+        lines = text.splitlines()
+        head = [l for l in lines if l.startswith(("OPENQASM", "include", "qreg", "creg"))]
+        body = [l for l in lines if l and not l.startswith(("OPENQASM", "include", "qreg", "creg", "//", "measure"))]
+        for i in range(4):
+            pre = [f"{rng.choice(['h', 's', 'sdg', 'x', 'y', 'z'])} q[1];" for _ in range(rng.randint(1, 3))]
+            post = [f"{rng.choice(['h', 's', 'sdg', 'x', 'y', 'z'])} q[1];" for _ in range(rng.randint(1, 3))]
+            if i % 2:
+                post.append("cz q[0],q[1];")
+            if i >= 2:
+                post.append("x q[0];")
+            text = "\n".join(head + pre + body + post + ["measure q[0] -> c[0];"]) + "\n"
+            out.append((f"{stem}-v{i}", stem, text))
+    return out
+
+
+def specgen_cases(ref, common):
+    """the reference writer's rus-specs of the variant circuits, for the C++ writer"""
+    cases = []
+    with tempfile.TemporaryDirectory() as td:
+        for name, stem, text in variants(ref):
+            q = Path(td) / f"{name}.qasm"
+            q.write_text(text)
+            p = subprocess.run([sys.executable, "-m", "cheese.rus", "spec", str(q)], capture_output=True, text=True,
+                               cwd=Path(ref) / "python", check=True)
+            root, roots, rest = split_spec(p.stdout)
+            assert root + "\n@@\n" + rest == common, "the shared spec blocks differ"
+            cases.append({"name": name, "base": stem, "qasm": text, "roots": roots,
+                          "info": json.loads(p.stderr.strip().splitlines()[-1])})
+            print(f"{name}: {cases[-1]['info']}", file=sys.stderr)
+    (GOLD / "rus_spec_cases.json").write_text(json.dumps(cases, indent=1) + "\n")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--specgen-only", action="store_true", help="write only the spec-writer cases (variants)")
     o = ap.parse_args()
+    if o.specgen_only:
+        with gzip.open(GOLD / "rus" / "common.rspec.gz", "rt") as f:
+            specgen_cases(o.ref, f.read())
+        return
     assert ORACLE.exists(), "build the C restatement first: make -C oracle"
     (GOLD / "rus").mkdir(parents=True, exist_ok=True)
     common = None

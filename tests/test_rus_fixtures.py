@@ -82,3 +82,49 @@ def test_bench_reads_the_same_specs():
     import bench
     for t in {c["target"] for c in CASES}:
         assert bench.rus_spec(t) == rus_spec_text(t)
+
+
+SPEC_CASES = json.loads((GOLD / "rus_spec_cases.json").read_text())
+
+
+@pytest.mark.parametrize("case", SPEC_CASES, ids=[c["name"] for c in SPEC_CASES])
+def test_rspec_writer_matches_reference(case):
+    """the C++ writer of rus-specs (roots, table root, rotation tables, Clifford list) byte for byte as the
+    reference's rus.py writes them, with the same summary (success outcome, roots, Pr[success], rescalings)"""
+    import gzip
+    import cheese_b200 as cz
+    with gzip.open(GOLD / "rus" / "common.rspec.gz", "rt") as f:
+        root, rest = f.read().split("\n@@\n")
+    text, info = cz.rspec_generate(qasm=case["qasm"])
+    assert text == "rus-spec 1\n" + root + case["roots"] + rest + "end\n"
+    assert info == case["info"]
+
+
+def test_rspec_writer_cli_and_errors(tmp_path):
+    import cheese_b200 as cz
+    case = next(c for c in SPEC_CASES if c["name"] == "ricotta-rus-0229-v2")
+    q = tmp_path / "v.qasm"
+    q.write_text(case["qasm"])
+    p = subprocess.run([str(cz.BIN_DIR / "cheese-spec"), "--rus", str(q)], capture_output=True, text=True)
+    assert p.returncode == 0 and p.stdout == cz.rspec_generate(qasm=case["qasm"])[0]
+    assert json.loads(p.stderr) == case["info"]
+    with pytest.raises(cz.SpecError) as e:
+        cz.rspec_generate(3, [("h", (0,))])
+    assert e.value.rc == 2 and "two qubits" in str(e.value)
+    with pytest.raises(cz.SpecError) as e:
+        cz.rspec_generate(2, [("h", (0,)), ("t", (1,))])
+    assert e.value.rc == 2 and "not a RUS circuit" in str(e.value)
+
+
+def test_variants_keep_the_optimum(tmp_path, rus_oracle):
+    """Cliffords on either side are free: the C restatement finds the targets' optima for the derived circuits"""
+    import cheese_b200 as cz
+    for name, flags, last in (("ricotta-rus-0003-v1", ["--table", "4", "--max", "3"], {"tcount_above": 3}),
+                              ("ricotta-rus-0003-v2", ["--table", "3", "--max", "4"], {"tcount": 4}),
+                              ("ricotta-rus-0229-v3", ["--table", "7", "--max", "11"], {"tcount": 10})):
+        case = next(c for c in SPEC_CASES if c["name"] == name)
+        spec = tmp_path / f"{name}.rspec"
+        spec.write_text(cz.rspec_generate(qasm=case["qasm"])[0])
+        p = subprocess.run([str(rus_oracle), str(spec)] + flags, capture_output=True, text=True, timeout=600)
+        got = json.loads(p.stdout.splitlines()[-1])
+        assert {k: got[k] for k in last} == last, name
