@@ -128,3 +128,17 @@ def test_variants_keep_the_optimum(tmp_path, rus_oracle):
         p = subprocess.run([str(rus_oracle), str(spec)] + flags, capture_output=True, text=True, timeout=600)
         got = json.loads(p.stdout.splitlines()[-1])
         assert {k: got[k] for k in last} == last, name
+
+
+def test_drop_in_rejects_before_the_device(tmp_path):
+    """usage and spec errors are reported before any device work (the reference reads its spec before CUDA setup),
+    so they behave the same on a host without a GPU"""
+    import cheese_b200 as cz
+    p = subprocess.run([str(cz.BIN_DIR / "rus")], capture_output=True, text=True)
+    assert p.returncode == 3 and p.stderr.startswith("usage: rus SPEC")
+    for text, msg in (("rus-spec 1\nroots 0\nend\n", "incomplete spec"), ("cheese-spec 1\n", "not a rus spec"),
+                      ("rus-spec 1\nmystery 1\nend\n", "unknown field mystery")):
+        f = tmp_path / "bad.rspec"
+        f.write_text(text)
+        p = subprocess.run([str(cz.BIN_DIR / "rus"), str(f)], capture_output=True, text=True)
+        assert p.returncode == 2 and p.stderr.strip() == msg
