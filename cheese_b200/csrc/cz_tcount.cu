@@ -766,13 +766,16 @@ class TcountContext {
 bool TcountContext::load(const std::string &path, const TDev &si, Table &tab, int K) {
   FILE *f = std::fopen(path.c_str(), "rb");
   if (!f) return false;
+  std::fseek(f, 0, SEEK_END);
+  const long size = std::ftell(f);
+  std::fseek(f, 0, SEEK_SET);
   int nl = 0;
   bool ok = std::fread(&nl, sizeof nl, 1, f) == 1 && nl >= 0 && nl <= MAXT && nl <= K;
   std::vector<std::vector<uint32_t>> P;
   std::vector<std::vector<uint8_t>> G;
   for (int l = 1; ok && l <= nl; l++) {
     long n = 0;
-    ok = std::fread(&n, sizeof n, 1, f) == 1 && n >= 0;
+    ok = std::fread(&n, sizeof n, 1, f) == 1 && n >= 0 && n <= size;
     if (!ok) break;
     P.emplace_back(n); G.emplace_back(n);
     ok = std::fread(P.back().data(), 4, n, f) == (size_t)n && std::fread(G.back().data(), 1, n, f) == (size_t)n;
@@ -782,7 +785,7 @@ bool TcountContext::load(const std::string &path, const TDev &si, Table &tab, in
   std::vector<uint64_t> k1, k2;
   std::vector<uint32_t> ki, kl;
   bool trusted = false;
-  if (ok && std::fread(&ns, sizeof ns, 1, f) == 1 && ns > 0) {
+  if (ok && std::fread(&ns, sizeof ns, 1, f) == 1 && ns > 0 && ns <= size) {
     k1.resize(ns); k2.resize(ns); ki.resize(ns); kl.resize(ns);
     bool kok = true;
     for (long i = 0; kok && i < ns; i++)
@@ -792,7 +795,16 @@ bool TcountContext::load(const std::string &path, const TDev &si, Table &tab, in
     trusted = kok && std::fread(trailer, 4, 2, f) == 2 && trailer[0] == TC_CACHE_MAGIC && trailer[1] == TC_KEY_VERSION;
   }
   std::fclose(f);
+  // every parent index and rotation in range (a damaged file is rebuilt, never replayed out of bounds), and every
+  // trusted key record names a node of the tree
+  for (int l = 1; ok && l <= nl; l++) {
+    const size_t below = l == 1 ? 1 : P[l - 2].size();
+    for (size_t j = 0; ok && j < P[l - 1].size(); j++)
+      ok = P[l - 1][j] < below && G[l - 1][j] >= 1 && (int)G[l - 1][j] < si.P;
+  }
   if (!ok) return false;
+  for (long i = 0; trusted && i < ns; i++)
+    trusted = kl[i] == 0 ? ki[i] == 0 : (kl[i] <= (uint32_t)nl && ki[i] < P[kl[i] - 1].size());
   Tree &D = tab.D;
   if (trusted) {
     for (int l = 1; l <= nl; l++) {
