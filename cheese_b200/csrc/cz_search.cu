@@ -2234,7 +2234,7 @@ struct Engine::Impl {
                                  SearchResult &res);
   void seen_add(DistTable &D, long long n, int lvl);                         // append fK1/fK2 level to D's keys
   const void *const *upload_tree(const std::vector<DBuf> &p, const std::vector<DBuf> &g, int upto);
-  bool table_load(const std::string &path, DistTable &D, int K);
+  bool table_load(const std::string &path, DistTable &D, int K, int G);
   void table_save(const std::string &path, const DistTable &D);
 };
 
@@ -2609,24 +2609,27 @@ bool host_circuit_ok(const HostSpec &hs, const std::vector<int> &c) {
 }
 }  // namespace
 
-bool Engine::Impl::table_load(const std::string &path, DistTable &D, int K) {
+bool Engine::Impl::table_load(const std::string &path, DistTable &D, int K, int G) {
   FILE *f = path.empty() ? nullptr : std::fopen(path.c_str(), "rb");
   if (!f) return false;
+  std::fseek(f, 0, SEEK_END);
+  const long size = std::ftell(f);
+  std::fseek(f, 0, SEEK_SET);
   int nl = 0;
   bool ok = std::fread(&nl, sizeof nl, 1, f) == 1 && nl >= 0 && nl <= K;
   std::vector<std::vector<uint32_t>> P;
-  std::vector<std::vector<uint8_t>> G;
+  std::vector<std::vector<uint8_t>> Gt;
   for (int l = 1; ok && l <= nl; l++) {
     long n = 0;
-    ok = std::fread(&n, sizeof n, 1, f) == 1 && n > 0;
+    ok = std::fread(&n, sizeof n, 1, f) == 1 && n > 0 && n <= size;
     if (!ok) break;
-    P.emplace_back(n); G.emplace_back(n);
-    ok = std::fread(P.back().data(), 4, n, f) == (size_t)n && std::fread(G.back().data(), 1, n, f) == (size_t)n;
+    P.emplace_back(n); Gt.emplace_back(n);
+    ok = std::fread(P.back().data(), 4, n, f) == (size_t)n && std::fread(Gt.back().data(), 1, n, f) == (size_t)n;
   }
   long ns = 0;
   std::vector<KeyRec> keys;
   bool trusted = false;
-  if (ok && std::fread(&ns, sizeof ns, 1, f) == 1 && ns > 0) {
+  if (ok && std::fread(&ns, sizeof ns, 1, f) == 1 && ns > 0 && ns <= size) {
     // the keys are read only when the file ends with this library's trailer (the same class hash)
     uint32_t trailer[2] = {0, 0};
     const long pos = std::ftell(f);
@@ -2640,7 +2643,15 @@ bool Engine::Impl::table_load(const std::string &path, DistTable &D, int K) {
     ok = false;
   }
   std::fclose(f);
+  // every parent index and candidate in range (a damaged file is rebuilt, never replayed out of bounds), and every
+  // trusted key record names a node of the tree
+  for (int l = 1; ok && l <= nl; l++) {
+    const size_t below = l == 1 ? 1 : P[l - 2].size();
+    for (size_t j = 0; ok && j < P[l - 1].size(); j++) ok = P[l - 1][j] < below && (int)Gt[l - 1][j] < G;
+  }
   if (!ok) return false;
+  for (size_t i = 0; trusted && i < keys.size(); i++)
+    trusted = keys[i].lvl == 0 ? keys[i].idx == 0 : (keys[i].lvl <= (uint32_t)nl && keys[i].idx < P[keys[i].lvl - 1].size());
   D.K = K; D.nl = nl;
   D.par.assign(nl + 1, DBuf{}); D.gat.assign(nl + 1, DBuf{}); D.n.assign(nl + 1, 0);
   D.n[0] = 1;
@@ -2649,7 +2660,7 @@ bool Engine::Impl::table_load(const std::string &path, DistTable &D, int K) {
     D.n[l] = n;
     D.par[l].ensure(n * 4 + 4); D.gat[l].ensure(n + 4);
     ck(cudaMemcpyAsync(D.par[l].p, P[l - 1].data(), n * 4, cudaMemcpyHostToDevice, s), "h2d");
-    ck(cudaMemcpyAsync(D.gat[l].p, G[l - 1].data(), n, cudaMemcpyHostToDevice, s), "h2d");
+    ck(cudaMemcpyAsync(D.gat[l].p, Gt[l - 1].data(), n, cudaMemcpyHostToDevice, s), "h2d");
   }
   if (trusted) {
     D.S1.ensure(ns * 8); D.S2.ensure(ns * 8); D.Sidx.ensure(ns * 4); D.Slvl.ensure(ns * 4);
@@ -2717,7 +2728,7 @@ Engine::Impl::DistTable *Engine::Impl::get_table(const HostSpec &hs, const SymGr
   hI.tk = 0; hI.standard = 0; hI.lite = 0; hI.uid = hs.uid ^ 0x7461626c65ULL;
   const DevSpec sp = prepare<NQ>(hI, grp, K + 1, true);
   DistTable *D = new DistTable;
-  if (table_load(path, *D, K)) {
+  if (table_load(path, *D, K, hs.G)) {
     res.table_loaded = true;
     if (!D->ns) {                                     // another program's keys: recompute them with this build's hash
       fK1.ensure(16); fK2.ensure(16);
