@@ -773,7 +773,7 @@ template <int NQ, typename ST> __device__ __noinline__ void warp_state_cheap(con
     mult *= sp.rad[c];
     if (nd > mx) mx = nd;
   }
-  c2 = sp.have_table ? sp.cxtable[idx] : mx;
+  c2 = sp.have_table && idx < sp.ncx ? sp.cxtable[idx] : mx;
 }
 // T bound of a state residual: max over rows of |stabilizer nullity - the goal's|
 template <int NQ, typename ST> __device__ __noinline__ int warp_state_t(const Z4<ST> *S, const DevSpec &sp, int lane) {

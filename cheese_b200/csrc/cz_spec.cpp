@@ -233,8 +233,13 @@ int parse_spec(const char *text, size_t len, HostSpec &s, std::string &err) {
       const int m = (int)in.num();
       for (int i = 0; i < m && !in.fail; i++) {
         const int sz = (int)in.num();
+        if (sz < 1 || sz > 30) { err = "bad cut"; return RC_SPEC; }
         int mask = 0;
-        for (int j = 0; j < sz; j++) mask |= 1 << (int)in.num();
+        for (int j = 0; j < sz; j++) {
+          const int q = (int)in.num();
+          if (q < 0 || q > 30 || (mask >> q & 1)) { err = "bad cut"; return RC_SPEC; }
+          mask |= 1 << q;
+        }
         if ((int)s.cutmask.size() < CUTMAX) { s.cutmask.push_back(mask); s.cutsize.push_back(sz); s.rad.push_back(2 * sz + 1); }
       }
     } else if (tok == "cxtable") {
@@ -271,8 +276,10 @@ int parse_spec(const char *text, size_t len, HostSpec &s, std::string &err) {
     if (s.gnq[g] == 2 && schmidt_rank_p(s.ginv[g]) <= 2) f |= GF_RANK2;
     s.gflags.push_back(f);
   }
-  for (size_t i = 0; i < s.cutmask.size(); i++)
+  for (size_t i = 0; i < s.cutmask.size(); i++) {
     if (s.cutsize[i] > s.n / 2 || s.cutsize[i] < 1) { err = "cut larger than half the register"; return RC_SPEC; }
+    if (s.cutmask[i] >> s.n) { err = "cut acts outside the register"; return RC_SPEC; }
+  }
   return 0;
 }
 

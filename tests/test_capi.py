@@ -67,3 +67,15 @@ def test_state_specs_are_parsed():
     with pytest.raises(cz.SpecError) as e:      # a states header without its start / goal blocks
         cz.Spec(spec_text("cs").replace("mode unitary", "mode states"))
     assert e.value.rc == 2 and "states spec incomplete" in str(e.value)
+
+
+def test_cuts_outside_the_register_are_refused():
+    """a cut naming a qubit outside the register (or twice) is refused on the host: the device never indexes with it"""
+    t = spec_text("toffoli")
+    head, tail = t[:t.index("cuts ")], t[t.index("cxtable"):]
+    for cuts, msg in (("cuts 3\n1 0\n1 1\n1 3\n", "cut acts outside the register"), ("cuts 1\n2 0 0\n", "bad cut"),
+                      ("cuts 1\n1 -1\n", "bad cut")):
+        with pytest.raises(cz.SpecError) as e:
+            cz.Spec(head + cuts + tail)
+        assert e.value.rc == 2 and msg in str(e.value)
+    cz.Spec(head + "cuts 3\n1 0\n1 1\n1 2\n" + tail)
