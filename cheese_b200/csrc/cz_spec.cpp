@@ -251,7 +251,8 @@ int parse_spec(const char *text, size_t len, HostSpec &s, std::string &err) {
     else { err = "unknown spec field " + tok; return RC_SPEC; }
   }
   if (s.states) {                              // the reference's reader: every part of a state spec present
-    if (!have_start || !have_goal_rows || !have_ginfo || s.m < 1 || s.m > (1 << std::max(0, std::min(s.n, 6)))) {
+    if (!have_start || !have_goal_rows || !have_ginfo || s.m < 1 || s.m > (1 << std::max(0, std::min(s.n, 6))) ||
+        s.ginfo.size() != (size_t)s.m * (2 + s.cutmask.size())) {
       err = "states spec incomplete";
       return RC_SPEC;
     }

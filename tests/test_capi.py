@@ -79,3 +79,13 @@ def test_cuts_outside_the_register_are_refused():
             cz.Spec(head + cuts + tail)
         assert e.value.rc == 2 and msg in str(e.value)
     cz.Spec(head + "cuts 3\n1 0\n1 1\n1 2\n" + tail)
+
+
+def test_state_goal_info_must_cover_every_pair():
+    """the goal lines (sde, nullity, one Schmidt rank per cut) must cover every pair and cut the device reads"""
+    t = spec_text("cs-states")
+    short = t.replace("goal 2\n0 0 1\n0 0 1\n", "goal 1\n0 0 1\n")
+    assert short != t
+    with pytest.raises(cz.SpecError) as e:
+        cz.Spec(short)
+    assert e.value.rc == 2 and "states spec incomplete" in str(e.value)
