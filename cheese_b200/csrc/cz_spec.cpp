@@ -262,6 +262,12 @@ int parse_spec(const char *text, size_t len, HostSpec &s, std::string &err) {
   if ((int)s.target.size() != N * N) { s.target.assign(N * N, Zw{0, 0, 0, 0}); }
   if (s.bad2.empty()) s.bad2.assign((size_t)s.G * s.G, 0);
   if (s.bad3.empty()) s.bad3.assign(((size_t)s.G * s.G * s.G + 31) / 32, 0);
+  // the window tables are indexed by candidate on the device: their sizes must be those of the final gate list
+  if ((int)s.names.size() != s.G || s.bad2.size() != (size_t)s.G * s.G ||
+      s.bad3.size() != ((size_t)s.G * s.G * s.G + 31) / 32) {
+    err = "window rules do not match the gate list";
+    return RC_SPEC;
+  }
   if (s.tdiv < 1) s.tdiv = 1;
   for (int g = 0; g < s.G; g++) {
     for (int j = 0; j < s.gnq[g]; j++)
