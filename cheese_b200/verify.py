@@ -48,3 +48,185 @@ def state_equivalent(spec_text, names):
     rows = [[M[r][x] for r in range(N)] for x in inputs] + [[(0, 0, 0, 0)] * N for _ in range(N - m)]
     kk, R = normalise(k, rows)
     return (kk, [list(r) for r in R]) == (G[0], [list(r) for r in G[1]])
+
+
+# ---------- RUS circuits (the role of the reference's `python -m cheese.rus verify`, rus.py:306-331) ----------
+ZERO4 = (0, 0, 0, 0)
+_CGEN = [("h", (0,)), ("h", (1,)), ("s", (0,)), ("s", (1,)), ("cz", (0, 1))]
+_CLIFFORDS = None
+
+
+def _pauli(n, p):
+    """P_p, digits per qubit (0 I, 1 X, 2 Y, 3 Z) at bits 2q, as (0, rows)"""
+    N = 1 << n
+    M = [[ZERO4] * N for _ in range(N)]
+    for x in range(N):
+        flip = ph = 0
+        for q in range(n):
+            d, bit = (p >> (2 * q)) & 3, (x >> q) & 1
+            if d in (1, 2):
+                flip |= 1 << q
+            ph += (2 + 4 * bit) if d == 2 else (4 * bit if d == 3 else 0)
+        M[x ^ flip][x] = _wpow(ph)
+    return 0, M
+
+
+def _wpow(p):
+    p &= 7
+    out = [0, 0, 0, 0]
+    out[p & 3] = 1 if p < 4 else -1
+    return tuple(out)
+
+
+def _adj(A):
+    k, a = A
+    return k, [[(a[j][i][0], -a[j][i][3], -a[j][i][2], -a[j][i][1]) for j in range(len(a))] for i in range(len(a[0]))]
+
+
+def _clifford_words():
+    """the 11520 two-qubit Cliffords mod phase as (perm, sign, word), in breadth-first order over h q0, h q1, s q0,
+    s q1, cz: the order (and so the indices) of a rus-spec's Clifford list; word = generator indices in time order"""
+    global _CLIFFORDS
+    if _CLIFFORDS:
+        return _CLIFFORDS
+    P16 = [_pauli(2, p) for p in range(16)]
+    acts = []
+    for g, qs in _CGEN:
+        C = gate_matrix(g, qs, 2)
+        Cd = _adj(C)
+        pi, sg = [0] * 16, [1] * 16
+        for a in range(16):
+            _, A = matmul(matmul(Cd, P16[a]), C)
+            pi[a], sg[a] = next((b, s) for b in range(16) for s in (1, -1)
+                                if all(A[i][j] == tuple(s * v for v in P16[b][1][i][j]) for i in range(4) for j in range(4)))
+        acts.append((pi, sg))
+    ident = (tuple(range(16)), (1,) * 16)
+    seen, order, frontier = {ident: ()}, [ident], [ident]
+    while frontier:
+        nxt = []
+        for a in frontier:
+            for gi, (pg, sgn) in enumerate(acts):
+                b = (tuple(a[0][pg[x]] for x in range(16)), tuple(sgn[x] * a[1][pg[x]] for x in range(16)))
+                if b not in seen:
+                    seen[b] = seen[a] + (gi,)
+                    order.append(b)
+                    nxt.append(b)
+        frontier = nxt
+    _CLIFFORDS = [(p, s, seen[(p, s)]) for p, s in order]
+    return _CLIFFORDS
+
+
+def _rotation(p, inv):
+    """time-ordered gates of R(P_p) on two qubits (R(P)^-1 if inv): basis changes, a CX ladder onto the first
+    support qubit, T or Tdg there, the ladder and the basis changes undone"""
+    sup = [(q, (p >> (2 * q)) & 3) for q in range(2) if (p >> (2 * q)) & 3]
+    q0 = sup[0][0]
+    ladder = [("cx", (q, q0)) for q, _ in sup[1:]]
+    pre, post = [], []
+    for q, d in sup:
+        if d == 1:
+            pre.append(("h", (q,)))
+            post.append(("h", (q,)))
+        elif d == 2:
+            pre += [("sdg", (q,)), ("h", (q,))]
+            post += [("h", (q,)), ("s", (q,))]
+    return pre + ladder + [("tdg" if inv else "t", (q0,))] + ladder + post
+
+
+def rus_circuit(res):
+    """the gates (time order) of a `rus` result: W = R(P_1)..R(P_j) C R(Q_c)^-1..R(Q_1)^-1 with fw = (P_1..P_j), the
+    Clifford C = the spec's Clifford `cliff` and tb = (Q_1..Q_c)"""
+    gates = []
+    for q in res["tb"]:
+        gates += _rotation(q, True)
+    for gi in _clifford_words()[res["cliff"]][2]:
+        g, qs = _CGEN[gi]
+        gates += [("h", (1,)), ("cx", (0, 1)), ("h", (1,))] if g == "cz" else [(g, qs)]
+    for p in reversed(res["fw"]):
+        gates += _rotation(p, False)
+    return gates
+
+
+def _blocks(W):
+    k, w = W
+    return k, [[[w[o + 2 * i][2 * j] for j in range(2)] for i in range(2)] for o in range(2)]
+
+
+def _scalar(A):
+    k, a = A
+    if any(a[i][j] != ZERO4 for i in range(len(a)) for j in range(len(a)) if i != j) or \
+            len({a[i][i] for i in range(len(a))}) != 1:
+        return None
+    kk, m = normalise(k, [[a[0][0]]])
+    return kk, m[0][0]
+
+
+def _clifford_block(k, B):
+    """B / sqrt2^k proportional to a one-qubit Clifford: B B^dag = q I and B P B^dag Q = +-q I"""
+    Bm = (k, [list(r) for r in B])
+    G = _scalar(matmul(Bm, _adj(Bm)))
+    if G is None or G[1] == ZERO4:
+        return False
+    negG = (G[0], tuple(-v for v in G[1]))
+    for p in (1, 3):
+        A = matmul(matmul(Bm, _pauli(1, p)), _adj(Bm))
+        if not any(_scalar(matmul(A, _pauli(1, q))) in (G, negG) for q in (1, 2, 3)):
+            return False
+    return True
+
+
+def rus_success_outcome(qasm_text, W):
+    """the "success outcome K" comment of the file, else the branch that is not proportional to a Clifford"""
+    import re
+    m = re.search(r"success outcome (\d)", qasm_text)
+    if m:
+        return int(m.group(1))
+    k, B = _blocks(W)
+    cl = [_clifford_block(k, B[o]) for o in range(2)]
+    if cl.count(True) != 1:
+        raise ValueError("not a RUS circuit: need exactly one branch proportional to a Clifford")
+    return cl.index(False)
+
+
+def parse_qasm(text):
+    """(n, [(gate, qubits)]) of the OpenQASM subset the spec writers read (qreg / qubit declaration, one gate per
+    statement; measure, creg, comments skipped)"""
+    import re
+    n, circ = 0, []
+    for line in text.splitlines():
+        line = line.split("//")[0].strip()
+        m = re.match(r"(?:qreg\s+\w+|qubit)\[(\d+)\]", line)
+        if m:
+            n = int(m.group(1))
+            continue
+        m = re.match(r"([a-z]+)\s+(.*);", line)
+        if m and m.group(1) in ("x", "y", "z", "h", "s", "sdg", "t", "tdg", "cx", "cz", "ccx"):
+            circ.append((m.group(1), tuple(int(q) for q in re.findall(r"\[(\d+)\]", m.group(2)))))
+    return n, circ
+
+
+def rus_check(qasm_text, res, outcome=None):
+    """exact check of a `rus` result against its target circuit: the result's circuit V has the target's success
+    branch (outcome 0 of V = a unit times the target's outcome-ks branch, so the same success unitary and
+    probability), its failure branch is proportional to a Clifford, and its T-count is the reported one"""
+    from .workloads import unitary
+    n, circ = parse_qasm(qasm_text)
+    if n != 2:
+        return False
+    W = unitary(2, circ)
+    ks = outcome if outcome is not None else rus_success_outcome(qasm_text, W)
+    gates = rus_circuit(res)
+    V = unitary(2, gates)
+    kW, BW = _blocks(W)
+    kV, BV = _blocks(V)
+    M = (kW, [list(r) for r in BW[ks]])
+    S = (kV, [list(r) for r in BV[0]])
+    pM = _scalar(matmul(M, _adj(M)))                      # M M^dag = p I
+    mu = _scalar(matmul(S, _adj(M)))                      # S M^dag = mu I, so S = (mu / p) M
+    if pM is None or mu is None:
+        return False
+    from .workloads import zmul
+    conj = lambda z: (z[0], -z[3], -z[2], -z[1])
+    sq = lambda s, z: normalise(2 * s[0], [[zmul(s[1], z)]])
+    tcount = sum(g in ("t", "tdg") for g, _ in gates)
+    return sq(mu, conj(mu[1])) == sq(pM, pM[1]) and _clifford_block(kV, BV[1]) and tcount == res["tcount"]

@@ -62,7 +62,11 @@ def test_cache_roundtrip(specs, tmp_path):
 
 
 def test_api_matches(specs):
+    import json
     import cheese_b200 as cz
+    from cheese_b200 import verify
+    from conftest import GOLD
+    qasm = {c["name"]: c["qasm"] for c in json.loads((GOLD / "rus_spec_cases.json").read_text())}
     eng = cz.Engine()
     for case in CASES:
         k, mx = int(case["flags"][1]), int(case["flags"][3])
@@ -71,6 +75,8 @@ def test_api_matches(specs):
         want = case["stdout"] if out["table_built"] else [l for l in case["stdout"] if '"dir": "table"' not in l]
         assert eng.rus_lines(rc, levels, out) == want, case["name"]
         assert out["kernel_launches"] > 0
+        if rc == 0:                                   # the found circuit, checked exactly against its target
+            assert verify.rus_check(qasm[case["target"]], out), case["name"]
     eng.trim()
 
 

@@ -142,3 +142,18 @@ def test_drop_in_rejects_before_the_device(tmp_path):
         f.write_text(text)
         p = subprocess.run([str(cz.BIN_DIR / "rus"), str(f)], capture_output=True, text=True)
         assert p.returncode == 2 and p.stderr.strip() == msg
+
+
+def test_found_circuits_verify_exactly():
+    """every found circuit of the fixtures passes the exact RUS check of cheese_b200.verify (the role of the
+    reference's `rus.py verify`), and damaged results do not"""
+    from cheese_b200 import verify
+    qasm = {c["name"]: c["qasm"] for c in SPEC_CASES}
+    found = [c for c in CASES if c["rc"] == 0]
+    assert len(found) == 7
+    for c in found:
+        assert verify.rus_check(qasm[c["target"]], json.loads(c["stdout"][-1])), c["name"]
+    res = json.loads(found[-1]["stdout"][-1])
+    for damage in ({"cliff": (res["cliff"] + 1) % 11520}, {"tb": res["tb"][:-1]}, {"fw": res["fw"][1:] + [1]},
+                   {"tcount": res["tcount"] - 1}):
+        assert not verify.rus_check(qasm[found[-1]["target"]], {**res, **damage}), damage
