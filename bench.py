@@ -246,6 +246,8 @@ def rus_leg(eng):
                 out[f"reference_gpu_{rep}"] = {"rc": p.returncode, "process_s": time.perf_counter() - t0,
                                                "seconds": last.get("seconds"), "tcount": last.get("tcount"),
                                                "split": last.get("split")}
+            import shutil
+            shutil.rmtree(d, ignore_errors=True)      # its K = 8 table file (about 140 MB)
         eng.trim()
         return out
     except Exception as e:                     # a failed side leg must not lose the headline line
