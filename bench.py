@@ -235,19 +235,21 @@ def rus_leg(eng):
                "query_ms_median": 1e3 * statistics.median(q)}
         ref = ROOT / "oracle" / "_ref" / "rus-ref"
         if ref.exists():
-            d = Path(tempfile.mkdtemp())
-            (d / "build").mkdir()
-            (d / "t.rspec").write_text(rspec)
-            for rep in ("cold", "cached"):
-                t0 = time.perf_counter()
-                p = subprocess.run([str(ref), "t.rspec", "--table", "8", "--max", "11"], cwd=d, capture_output=True,
-                                   text=True, timeout=600)
-                last = json.loads(p.stdout.splitlines()[-1]) if p.stdout.strip() else {}
-                out[f"reference_gpu_{rep}"] = {"rc": p.returncode, "process_s": time.perf_counter() - t0,
-                                               "seconds": last.get("seconds"), "tcount": last.get("tcount"),
-                                               "split": last.get("split")}
             import shutil
-            shutil.rmtree(d, ignore_errors=True)      # its K = 8 table file (about 140 MB)
+            d = Path(tempfile.mkdtemp())
+            try:
+                (d / "build").mkdir()
+                (d / "t.rspec").write_text(rspec)
+                for rep in ("cold", "cached"):
+                    t0 = time.perf_counter()
+                    p = subprocess.run([str(ref), "t.rspec", "--table", "8", "--max", "11"], cwd=d,
+                                       capture_output=True, text=True, timeout=600)
+                    last = json.loads(p.stdout.splitlines()[-1]) if p.stdout.strip() else {}
+                    out[f"reference_gpu_{rep}"] = {"rc": p.returncode, "process_s": time.perf_counter() - t0,
+                                                   "seconds": last.get("seconds"), "tcount": last.get("tcount"),
+                                                   "split": last.get("split")}
+            finally:
+                shutil.rmtree(d, ignore_errors=True)      # its K = 8 table file (about 140 MB), on every path
         eng.trim()
         return out
     except Exception as e:                     # a failed side leg must not lose the headline line

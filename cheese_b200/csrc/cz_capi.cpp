@@ -300,6 +300,7 @@ int cz_search_text(cz_engine *engine, const char *spec_text, size_t len, const c
 int cz_eval_bounds(cz_engine *engine, const cz_spec *spec, int count, const int64_t *entries, const int *k,
                    int *bounds) {
   if (!engine || !spec || count < 0 || (count && (!entries || !k || !bounds))) return CZ_ERR_USAGE;
+  if (spec->hs.states) return CZ_ERR_USAGE;   // the bounds are those of unitary residuals (like --mitm)
   if (!count) return 0;
   std::string err;
   try {
@@ -314,6 +315,10 @@ int cz_eval_bounds_noalloc(const cz_spec *spec, int count, const int64_t *d_entr
   static_assert(CZ_NOALLOC_SCRATCH_BYTES == cz::NOALLOC_SCRATCH_BYTES, "header and library disagree");
   static_assert(CZ_NOALLOC_MAX_CXTABLE == cz::NOALLOC_MAX_CXTABLE, "header and library disagree");
   if (!spec) { put_err(err, errlen, "null spec"); return CZ_ERR_USAGE; }
+  if (spec->hs.states) {
+    put_err(err, errlen, "state-target spec: these bounds are defined for unitary residuals only");
+    return CZ_ERR_USAGE;
+  }
   std::string e;
   int rc;
   try {

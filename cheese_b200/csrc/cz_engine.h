@@ -68,8 +68,10 @@ constexpr size_t NOALLOC_SCRATCH_BYTES = 86016;
 // Bounds of `count` residuals held in the caller's device memory (entries: count x N^2 x 4 int64 limbs, 16-byte
 // aligned; exponents: count ints; bounds: count x 4 ints, 16-byte aligned), on the caller's stream, without any
 // device allocation: the spec's tables are staged in a static device array shared by all calls (calls that overlap
-// on the GPU race on it). The first call on a device looks the array up (cudaGetSymbolAddress); make that first
-// call before any stream capture.
+// on the GPU race on it). Each call copies the tables from host memory and waits for the caller's stream before
+// it queues the kernel. The first call on a device looks the array up (cudaGetSymbolAddress); make that first
+// call before any stream capture. The address is kept per device index: it assumes the primary context and no
+// device reset in between.
 int eval_bounds_noalloc(const HostSpec &hs, int count, const int64_t *d_entries, const int *d_k, int *d_bounds,
                         void *stream, std::string &err);
 

@@ -3421,8 +3421,8 @@ void eval_bounds_noalloc_nq(const HostSpec &hs, unsigned char *base, int count, 
   sp.bad3 = nullptr;
   int nsm = 148;
   int dev = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  ck(cudaGetDevice(&dev), "cudaGetDevice");
+  ck(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "SM count");
   const int grid = std::max(1, std::min((count + EXP_WARPS - 1) / EXP_WARPS, nsm * 8));
   k_eval_bounds<NQ, int64_t><<<grid, EXP_WARPS * 32, 0, st>>>(sp, (const Z4<int64_t> *)d_entries, d_k, count,
                                                               (int4 *)d_bounds);

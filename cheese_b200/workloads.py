@@ -1,5 +1,5 @@
 """Synthetic workloads in the reference's input format: seeded random Clifford+T circuits, their exact unitaries,
-and cheese spec files assembled from a per-qubit-count base spec.
+and their cheese spec files (written by the library's native spec writer).
 
 Exact arithmetic: an entry of Z[w] (w = e^{i pi/4}) is (a, b, c, d) = a + b w + c w^2 + d w^3; a matrix is
 (k, rows) meaning rows / sqrt2^k with k as small as possible (the normal form of the reference's spec writer,
@@ -11,11 +11,9 @@ ordered pair of distinct qubits), budget L.
 """
 import os
 import random
-from pathlib import Path
 
 ZERO = (0, 0, 0, 0)
 ONE = (1, 0, 0, 0)
-DATA = Path(__file__).resolve().parent / "data"
 
 # gate -> (sqrt2 exponent, local matrix as {(row, col): w-power}); bit j of a local index is qubit qs[j]
 _GATES = {
@@ -141,24 +139,11 @@ def batch(seed, count=512):
     return out
 
 
-def target_block(k, M):
-    return f"target {k}\n" + "".join(" ".join(" ".join(map(str, x)) for x in row) + "\n" for row in M)
-
-
-def base_spec(n):
-    """the default Clifford+T spec of n qubits (candidates, window rules, cuts, CX table) minus its target"""
-    return (DATA / f"base-n{n}.spec").read_text()
-
-
-def make_spec(n, circ, depth, base=None):
-    """spec text for the circuit's unitary with budget `depth`: the base spec's fields with this target"""
-    base = base_spec(n) if base is None else base
-    k, M = unitary(n, circ)
-    head, rest = base.split("target ", 1)
-    tail = rest[rest.index("cuts "):]
-    lines = head.splitlines(keepends=True)
-    lines = [f"depth {depth}\n" if ln.startswith("depth ") else ln for ln in lines]
-    return "".join(lines) + target_block(k, M) + tail
+def make_spec(n, circ, depth):
+    """spec text for the circuit's unitary with budget `depth`, written by the library's native spec writer
+    (cz_spec_generate: the default Clifford+T candidates, window rules, cuts and CX table of n qubits)"""
+    from . import spec_generate
+    return spec_generate(n, list(circ), depth=depth)[0]
 
 
 def qasm(n, circ):

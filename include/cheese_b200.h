@@ -199,7 +199,8 @@ int cz_search_text(cz_engine *engine, const char *spec_text, size_t len, const c
  * as the search: entries = count x N^2 x (a, b, c, d) limbs (value (a + b w + c w^2 + d w^3) / sqrt2^k), k = their
  * exponents; bounds = count x 4 ints (T bound = PTM sde, CX bound, H structure 0/2, support; the last two are -1
  * when the residual is the identity, where the search stops before the bounds). These are the
- * reference's ptm_wht, cx_bound, h_struct and support (src/cheese.cu:305-338, 585-597, 429-449). */
+ * reference's ptm_wht, cx_bound, h_struct and support (src/cheese.cu:305-338, 585-597, 429-449). A state-target
+ * spec is refused with CZ_ERR_USAGE (its search uses the row bounds of src/cheese.cu:451-583 instead). */
 int cz_eval_bounds(cz_engine *engine, const cz_spec *spec, int count, const int64_t *entries, const int *k,
                    int *bounds);
 
@@ -207,13 +208,18 @@ int cz_eval_bounds(cz_engine *engine, const cz_spec *spec, int count, const int6
  * memory (code running under a custom or fixed-size allocator, inside a memory-capped service, or in a process
  * whose allocator is owned by another runtime): it calls no cudaMalloc / cudaFree and creates no engine. The
  * caller passes device buffers: d_entries (count x N^2 x 4 int64 limbs, 16-byte aligned), d_k (count ints) and
- * d_bounds (count x 4 ints, 16-byte aligned), and the stream to run on (NULL: the legacy default stream); the call
- * returns once the kernel is queued after the staged tables. The spec's tables (gate matrices, CX table, goal)
+ * d_bounds (count x 4 ints, 16-byte aligned), and the stream to run on (NULL: the legacy default stream). Each
+ * call copies the spec's tables from host memory into the array on that stream and waits for the stream
+ * (cudaStreamSynchronize) before it queues the kernel, so the host blocks until the work queued earlier on the
+ * stream has finished (with NULL: the work of every blocking stream); the results are in d_bounds once the
+ * kernel, queued last, completes. The spec's tables (gate matrices, CX table, goal)
  * are staged in a static device array of CZ_NOALLOC_SCRATCH_BYTES that every GPU loading this library keeps
  * until the process exits; a spec whose CX table has more than CZ_NOALLOC_MAX_CXTABLE entries is refused with
- * CZ_ERR_USAGE. All calls share that array and each rewrites it in full, so calls that overlap on the GPU race.
+ * CZ_ERR_USAGE, and so is a state-target spec (these are bounds of unitary residuals). All calls share that
+ * array and each rewrites it in full, so calls that overlap on the GPU race.
  * The first call on a device looks the array up (cudaGetSymbolAddress) with that device current: make it before
- * any stream capture. */
+ * any stream capture. The address is kept per device index for the life of the process; it assumes the device's
+ * primary context (the runtime's) and no cudaDeviceReset in between. */
 #define CZ_NOALLOC_SCRATCH_BYTES 86016
 #define CZ_NOALLOC_MAX_CXTABLE 4096
 int cz_eval_bounds_noalloc(const cz_spec *spec, int count, const int64_t *d_entries, const int *d_k, int *d_bounds,

@@ -3,7 +3,7 @@
 Run in a container that has the reference source tree (read-only is fine) and the C restatement built
 (`make -C oracle`):
 
-    python tests/golden/make_golden_rus.py [--ref /path/to/reference]
+    python tests/golden/make_golden_rus.py --ref /path/to/reference
 
 The rus-specs are written by the reference's own writer (python -m cheese.rus spec) for its RUS regression targets
 (tests/qasm/ricotta-rus-*.qasm). Every spec shares its table root, rotation tables and Clifford list, so those are
@@ -95,7 +95,7 @@ def specgen_cases(ref, common):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="the reference's source tree (read only)")
     ap.add_argument("--specgen-only", action="store_true", help="write only the spec-writer cases (variants)")
     o = ap.parse_args()
     if o.specgen_only:

@@ -1,7 +1,7 @@
 """Golden fixtures of the T-count and Clifford-table paths.
 
 Step 1 (any machine with the reference tree, which provides the qasm targets):
-    python tests/golden/make_golden_tc.py inputs [--ref /path/to/reference]
+    python tests/golden/make_golden_tc.py inputs --ref /path/to/reference
   writes tests/golden/tcount/*.tspec (the reference's targets and seeded table-driven queries, in the reference's
   tcount-spec format, checked against its tcount.py where it exists) and tests/golden/cliffopt/*.job.
 
@@ -159,7 +159,8 @@ if __name__ == "__main__":
     if sys.argv[1] == "oracle":
         oracle_outputs()
     elif sys.argv[1] == "inputs":
-        ref = sys.argv[sys.argv.index("--ref") + 1] if "--ref" in sys.argv else "/root/reference"
-        inputs(ref)
+        if "--ref" not in sys.argv:
+            sys.exit("inputs: --ref /path/to/reference is required (the reference's source tree)")
+        inputs(sys.argv[sys.argv.index("--ref") + 1])
     else:
         outputs(sys.argv[2])

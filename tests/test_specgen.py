@@ -52,13 +52,18 @@ def test_random_targets_match_reference_writer():
         assert parts(text) == parts(want), c["name"]
 
 
-def test_same_as_base_spec_assembly():
-    """the Python assembly from the reference-written base specs gives the same spec"""
-    import cheese_b200 as cz
+def test_same_as_reference_base_spec_with_python_target():
+    """the native writer against the reference-written base spec of each qubit count with the target block that the
+    Python exact arithmetic (workloads.unitary) gives: the same candidates, rules, cuts, CX table and target"""
     from cheese_b200 import workloads
+    base = {n: spec_path(f"base-n{n}").read_text() for n in (2, 3)}
     for n, circ, d in workloads.batch(3, 40):
-        text, _ = cz.spec_generate(n, circ, depth=d)
-        assert parts(text) == parts(workloads.make_spec(n, circ, d))
+        k, M = workloads.unitary(n, circ)
+        head, rest = base[n].split("target ", 1)
+        head = "".join(f"depth {d}\n" if ln.startswith("depth ") else ln for ln in head.splitlines(keepends=True))
+        target = f"target {k}\n" + "".join(" ".join(" ".join(map(str, x)) for x in row) + "\n" for row in M)
+        want = head + target + rest[rest.index("cuts "):]
+        assert parts(workloads.make_spec(n, circ, d)) == parts(want)
 
 
 @pytest.mark.parametrize("name", ["cs", "qft_2", "toffoli", "ccz", "fredkin", "peres", "relative-phase-toffoli"])

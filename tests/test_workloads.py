@@ -7,13 +7,15 @@ from conftest import golden_cases, spec_text
 
 
 def test_spec_assembly_matches_reference_writer():
-    # the golden random specs were written by the reference's spec generator for these circuits
+    # the golden random specs were written by the reference's spec generator for these circuits; the W3 triples are
+    # the same set (the reference lists them in the iteration order of a Python set)
+    from test_specgen import parts
     for c in golden_cases():
         if "circuit" not in c:
             continue
         circ = [(g, tuple(q)) for g, q in c["circuit"]]
         n = 3 if "L_cx_0_2" in spec_text(c["spec"]) else 2
-        assert workloads.make_spec(n, circ, len(circ)) == spec_text(c["spec"]), c["name"]
+        assert parts(workloads.make_spec(n, circ, len(circ))) == parts(spec_text(c["spec"])), c["name"]
 
 
 def test_found_circuits_in_golden_outputs_verify_exactly():
