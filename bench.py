@@ -31,6 +31,7 @@ sys.path.insert(0, str(ROOT))
 SPECS = ROOT / "tests" / "golden" / "specs"
 REF_CPU = ROOT / "oracle" / "_ref" / "cheese-cpu"
 WORKLOAD = [("toffoli", 11), ("toffoli", 12), ("ccz", 8)]
+SAMPLE = [("ccz", 8), ("toffoli", 11)]   # the reference CPU arm's per-step sample when the host allows it
 METRIC = "prefixes/s"
 # algorithmic int32 operations (a multiply or an add counts 1) per unit of work of the level kernel, 3 qubits, as
 # the kernel computes them:
@@ -117,6 +118,57 @@ def run_ref_cpu(cases, threads):
             raise RuntimeError(f"reference CPU build failed on {stem} {d}: {p.stderr[-300:]}")
         pre += sum(json.loads(l).get("prefixes", 0) for l in p.stdout.splitlines() if '"prefixes"' in l)
     return pre, time.perf_counter() - t0
+
+
+REF_GPU = ROOT / "oracle" / "_ref" / "cheese-gpu-ref"
+
+
+def reference_gpu(eng, specs):
+    """The reference's own GPU build (src/cheese.cu compiled for sm_100a with its build.sh "cuda" flags) on the same
+    B200: each search of the workload as one process (its CLI; the last level line's "seconds" is its search time
+    without CUDA start-up), every JSON line compared with this library's (seconds excluded); then its --table 8 path
+    to the Toffoli optimum, one process per budget as the reference's run.sh does (the first builds the table and
+    writes its cache file, the others load it)."""
+    import shutil
+    import tempfile
+    if not REF_GPU.exists():
+        return {"unavailable": "oracle/_ref/cheese-gpu-ref not built (make -C oracle REF=<reference tree> refgpu)"}
+    out, tot_pre, tot_s = {}, 0, 0.0
+    d = Path(tempfile.mkdtemp())
+    try:
+        (d / "build").mkdir()
+        for stem, dd in WORKLOAD:
+            t0 = time.perf_counter()
+            p = subprocess.run([str(REF_GPU), str(SPECS / f"{stem}.spec"), "--depth", str(dd)], cwd=d,
+                               capture_output=True, text=True, timeout=900)
+            wall = time.perf_counter() - t0
+            lines = p.stdout.splitlines()
+            lv = [json.loads(l) for l in lines if '"prefixes"' in l]
+            search_s = lv[-1]["seconds"] if lv else None
+            mine = eng.search(specs[stem], depth=dd)
+            import re
+            same = [re.sub(r'"seconds": [0-9.]+', '"seconds": 0.00', l) for l in lines] == mine.lines()
+            pre = sum(x["prefixes"] for x in lv)
+            out[f"{stem}-{dd}"] = {"rc": p.returncode, "process_s": wall, "search_s": search_s, "prefixes": pre,
+                                   "same_lines": same}
+            tot_pre += pre
+            tot_s += search_s or 0.0
+        out["prefixes_per_s"] = tot_pre / tot_s if tot_s else None
+        out["toffoli12_proof_s"] = out.get("toffoli-12", {}).get("search_s")
+        t0 = time.perf_counter()
+        budgets = {}
+        for dd in range(1, 16):
+            a = time.perf_counter()
+            p = subprocess.run([str(REF_GPU), str(SPECS / "toffoli.spec"), "--depth", str(dd), "--table", "8"], cwd=d,
+                               capture_output=True, text=True, timeout=900)
+            budgets[str(dd)] = {"rc": p.returncode, "s": time.perf_counter() - a}
+            if p.returncode != 1:
+                break
+        out["table8_toffoli_optimum"] = {"total_s": time.perf_counter() - t0, "budgets": budgets,
+                                         "found_at": next((int(k) for k, v in budgets.items() if v["rc"] == 0), None)}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)   # its distance-table cache file
+    return out
 
 
 def reference_sample(steps, warmup, threads):
@@ -539,13 +591,33 @@ def main():
         m = re.search(r"bytes per parent \(for bench.py scaling\): (\d+)", tf.read_text())
         if m and exp_launches:
             traffic = int(m.group(1)) * parents / exp_launches
+    # this library's rate on the reference arm's per-step sample (ccz 8 + toffoli 11), device-timed like value, so
+    # the two arms can be compared on the same work
+    s_pre, s_ms = 0, 0.0
+    for _ in range(3):
+        for stem, d in SAMPLE:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            flush.fill_(1)
+            e0.record(stream)
+            o = eng.search(specs[stem], depth=d)
+            e1.record(stream)
+            e1.synchronize()
+            s_pre += o.raw.prefixes
+            s_ms += e0.elapsed_time(e1)
     cpu = None
+    ref_gpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and REF_CPU.exists():
         threads = os.cpu_count() or 1
-        cases = [("ccz", 8), ("toffoli", 11)]
-        cp, cs = run_ref_cpu(cases, threads)
+        cp, cs = run_ref_cpu(SAMPLE, threads)
+        tp, ts = run_ref_cpu([("toffoli", 12)], threads)
         cpu = {"value": cp / cs, "unit": "prefixes/s", "cores": threads, "kind": "reference",
-               "sample": "ccz-8 + toffoli-11 once, reference CPU build (OpenMP), %.1f s" % cs}
+               "sample": "ccz-8 + toffoli-11 once, reference CPU build (OpenMP), %.1f s" % cs,
+               "toffoli12_proof_s": ts, "toffoli12_prefixes_per_s": tp / ts}
+    if rank == 0 and ws == 1 and not args.no_systems:
+        try:
+            ref_gpu = reference_gpu(eng, specs)
+        except Exception as e:               # a failed side leg must not lose the headline line
+            ref_gpu = {"error": str(e)[:300]}
     extra = systems(eng, args) if (rank == 0 and ws == 1 and not args.no_systems) else {}
     if rank == 0:
         out = {
@@ -555,7 +627,9 @@ def main():
             "config": {"workload": "deep proofs, 3 qubits, 27 Clifford+T candidates: toffoli budget 11 + toffoli "
                                    "budget 12 + ccz budget 8 per step", "parallelism": f"replicas x{ws}",
                        "l2": "flushed between steps (256 MiB write)", "toffoli12_proof_ms": t12_ms / args.steps,
-                       "prefixes_per_step": prefixes / args.steps / ws},
+                       "prefixes_per_step": prefixes / args.steps / ws,
+                       "sample_rate": s_pre / (s_ms / 1e3) if s_ms else None,
+                       "sample": "ccz-8 + toffoli-11 (the reference arm's per-step sample), device-timed"},
             "e2e": {"value": e2e_pre / e2e_s, "unit": "prefixes/s", "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps},
             "gpu_launches": launches,
@@ -564,6 +638,7 @@ def main():
                          "peak_source": "measured in this run: IMAD loop (multiply-add = 2 ops)",
                          "launch_ms": launch_ms, "ops_per_launch": ops / max(1, exp_launches)},
             "cpu_baseline": cpu,
+            "reference_gpu": ref_gpu,
             "clocks": clk.summary(),
         }
         out.update(extra)

@@ -6,6 +6,10 @@
 #include <cstdlib>
 #include <atomic>
 #include <cstring>
+#include <map>
+#include <string>
+#include <unordered_map>
+#include <vector>
 
 namespace cz {
 
@@ -291,54 +295,95 @@ int parse_spec(const char *text, size_t len, HostSpec &s, std::string &err) {
 }
 
 namespace {
-std::vector<std::string> split_name(const std::string &nm) {
-  std::vector<std::string> parts;
-  size_t a = 0, b;
-  while ((b = nm.find('_', a)) != std::string::npos) { parts.push_back(nm.substr(a, b - a)); a = b + 1; }
-  parts.push_back(nm.substr(a));
-  return parts;
-}
-// image of candidate g under a relabelling (and conjugation): names are L_<gate>_<q>[_<q>...]
-int sym_gate(const HostSpec &hs, const std::vector<int> &perm, bool conj, int g) {
-  const std::vector<std::string> parts = split_name(hs.names[g]);
-  if (parts.size() < 2) return -1;
-  std::string gate = parts[1];
-  if (conj) {
-    if (gate == "t") gate = "tdg"; else if (gate == "tdg") gate = "t";
-    else if (gate == "s") gate = "sdg"; else if (gate == "sdg") gate = "s";
-    else if (gate != "x" && gate != "z" && gate != "h" && gate != "cx" && gate != "cz" && gate != "ccx") return -1;
-  }
+// A candidate name "L_<gate>_<q>[_<q>...]" read once: its gate word and its qubits (std::atoi of each field, as the
+// reference's reader takes them). well = the name has a gate field and every qubit lies in the register.
+struct CandName {
+  std::string word;
   std::vector<int> qs;
-  for (size_t i = 2; i < parts.size(); i++) {
-    const int q = std::atoi(parts[i].c_str());
-    if (q < 0 || q >= (int)perm.size()) return -1;
-    qs.push_back(perm[q]);
+  bool well = false;
+};
+CandName read_cand(const std::string &nm, int n) {
+  CandName c;
+  std::vector<std::string> f(1);
+  for (char ch : nm) {
+    if (ch == '_') f.emplace_back();
+    else f.back() += ch;
   }
-  if (gate == "ccx" && qs.size() == 3 && qs[0] > qs[1]) std::swap(qs[0], qs[1]);
-  std::string want = "L_" + gate;
-  for (int q : qs) want += "_" + std::to_string(q);
-  for (int h = 0; h < hs.G; h++) if (hs.names[h] == want) return h;
-  return -1;
+  if (f.size() < 2) return c;
+  c.word = f[1];
+  c.well = true;
+  for (size_t i = 2; i < f.size(); i++) {
+    c.qs.push_back(std::atoi(f[i].c_str()));
+    if (c.qs.back() < 0 || c.qs.back() >= n) c.well = false;
+  }
+  return c;
+}
+// The gate word of a gate's complex conjugate: the phase gates swap with their inverses, the real gates map to
+// themselves; "" for any other word (y, whose conjugate is -y, and unknown gates): no conjugating symmetry then.
+std::string conjugate_word(const std::string &w) {
+  static const std::map<std::string, std::string> table = {
+      {"t", "tdg"}, {"tdg", "t"}, {"s", "sdg"}, {"sdg", "s"},
+      {"x", "x"}, {"z", "z"}, {"h", "h"}, {"cx", "cx"}, {"cz", "cz"}, {"ccx", "ccx"}};
+  const auto it = table.find(w);
+  return it == table.end() ? std::string() : it->second;
+}
+// The qubit relabellings of n qubits (perm[i] = image of qubit i) in lexicographic order, read off an n-digit
+// base-n counter (only the bijective digit strings are kept).
+std::vector<std::vector<int>> relabellings(int n) {
+  std::vector<std::vector<int>> out;
+  std::vector<int> d(n, 0);
+  for (;;) {
+    int seen = 0;
+    for (int v : d) seen |= 1 << v;
+    if (seen == (1 << n) - 1) out.push_back(d);
+    int i = n - 1;
+    while (i >= 0 && d[i] == n - 1) d[i--] = 0;
+    if (i < 0) break;
+    d[i]++;
+  }
+  return out;
 }
 }  // namespace
 
+// Elements are ordered conjugation-free first, each half by relabelling in lexicographic order (the element order
+// decides which symmetry the class comparisons try first). A relabelling x conjugation is kept when the image of
+// every candidate name (gate word conjugated, qubits relabelled, the two ccx controls written in ascending order)
+// names a candidate; the image is the first candidate of that name.
 SymGroup sym_group(const HostSpec &hs, bool on) {
   const int n = hs.n, N = 1 << n;
+  std::vector<CandName> cand;
+  std::unordered_map<std::string, int> by_name;
+  for (int g = 0; g < hs.G; g++) {
+    cand.push_back(read_cand(hs.names[g], n));
+    by_name.emplace(hs.names[g], g);          // keeps the first index of a repeated name
+  }
+  auto image = [&](const CandName &c, const std::vector<int> &perm, bool conj) {
+    if (!c.well) return -1;
+    const std::string w = conj ? conjugate_word(c.word) : c.word;
+    if (w.empty()) return -1;
+    std::vector<int> q(c.qs.size());
+    for (size_t i = 0; i < q.size(); i++) q[i] = perm[c.qs[i]];
+    if (w == "ccx" && q.size() == 3 && q[0] > q[1]) std::swap(q[0], q[1]);
+    std::string nm = "L_" + w;
+    for (int x : q) nm += "_" + std::to_string(x);
+    const auto it = by_name.find(nm);
+    return it == by_name.end() ? -1 : it->second;
+  };
+  std::vector<std::vector<int>> perms = relabellings(n);
+  if (!on) perms.resize(1);                     // the identity comes first
   SymGroup g;
-  std::vector<int> p(n);
-  for (int i = 0; i < n; i++) p[i] = i;
-  std::vector<std::vector<int>> perms;
-  do perms.push_back(p); while (on && std::next_permutation(p.begin(), p.end()));
-  for (int cj = 0; cj < (on ? 2 : 1); cj++)
-    for (auto &pm : perms) {
+  for (int conj = 0; conj <= (on ? 1 : 0); conj++)
+    for (const auto &perm : perms) {
       std::vector<int> gm(hs.G);
-      bool ok = true;
-      for (int c = 0; c < hs.G && ok; c++) ok = (gm[c] = sym_gate(hs, pm, cj, c)) >= 0;
-      if (!ok) continue;
-      g.perm.push_back(pm); g.conj.push_back((uint8_t)cj); g.gmap.push_back(gm);
+      int c = 0;
+      while (c < hs.G && (gm[c] = image(cand[c], perm, conj != 0)) >= 0) c++;
+      if (c < hs.G) continue;
+      g.perm.push_back(perm);
+      g.conj.push_back((uint8_t)conj);
+      g.gmap.push_back(std::move(gm));
       for (int x = 0; x < N; x++) {
         int y = 0;
-        for (int i = 0; i < n; i++) if ((x >> i) & 1) y |= 1 << pm[i];
+        for (int b = x; b; b &= b - 1) y |= 1 << perm[__builtin_ctz(b)];
         g.bperm.push_back((uint8_t)y);
       }
     }

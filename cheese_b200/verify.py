@@ -52,8 +52,6 @@ def state_equivalent(spec_text, names):
 
 # ---------- RUS circuits (the role of the reference's `python -m cheese.rus verify`, rus.py:306-331) ----------
 ZERO4 = (0, 0, 0, 0)
-_CGEN = [("h", (0,)), ("h", (1,)), ("s", (0,)), ("s", (1,)), ("cz", (0, 1))]
-_CLIFFORDS = None
 
 
 def _pauli(n, p):
@@ -83,39 +81,6 @@ def _adj(A):
     return k, [[(a[j][i][0], -a[j][i][3], -a[j][i][2], -a[j][i][1]) for j in range(len(a))] for i in range(len(a[0]))]
 
 
-def _clifford_words():
-    """the 11520 two-qubit Cliffords mod phase as (perm, sign, word), in breadth-first order over h q0, h q1, s q0,
-    s q1, cz: the order (and so the indices) of a rus-spec's Clifford list; word = generator indices in time order"""
-    global _CLIFFORDS
-    if _CLIFFORDS:
-        return _CLIFFORDS
-    P16 = [_pauli(2, p) for p in range(16)]
-    acts = []
-    for g, qs in _CGEN:
-        C = gate_matrix(g, qs, 2)
-        Cd = _adj(C)
-        pi, sg = [0] * 16, [1] * 16
-        for a in range(16):
-            _, A = matmul(matmul(Cd, P16[a]), C)
-            pi[a], sg[a] = next((b, s) for b in range(16) for s in (1, -1)
-                                if all(A[i][j] == tuple(s * v for v in P16[b][1][i][j]) for i in range(4) for j in range(4)))
-        acts.append((pi, sg))
-    ident = (tuple(range(16)), (1,) * 16)
-    seen, order, frontier = {ident: ()}, [ident], [ident]
-    while frontier:
-        nxt = []
-        for a in frontier:
-            for gi, (pg, sgn) in enumerate(acts):
-                b = (tuple(a[0][pg[x]] for x in range(16)), tuple(sgn[x] * a[1][pg[x]] for x in range(16)))
-                if b not in seen:
-                    seen[b] = seen[a] + (gi,)
-                    order.append(b)
-                    nxt.append(b)
-        frontier = nxt
-    _CLIFFORDS = [(p, s, seen[(p, s)]) for p, s in order]
-    return _CLIFFORDS
-
-
 def _rotation(p, inv):
     """time-ordered gates of R(P_p) on two qubits (R(P)^-1 if inv): basis changes, a CX ladder onto the first
     support qubit, T or Tdg there, the ladder and the basis changes undone"""
@@ -133,14 +98,100 @@ def _rotation(p, inv):
     return pre + ladder + [("tdg" if inv else "t", (q0,))] + ladder + post
 
 
-def rus_circuit(res):
+_GACT = None
+
+
+def rspec_cliffords(rspec_text):
+    """the Clifford list of a rus-spec (its "cliffords" block): per Clifford C, (perm, sign) with
+    C^dag P_a C = sign[a] P_perm[a] for the 16 two-qubit Paulis a (digits per qubit 0 I, 1 X, 2 Y, 3 Z at bits 2q)"""
+    toks = rspec_text.split()
+    i = toks.index("cliffords")
+    m = int(toks[i + 1])
+    vals = list(map(int, toks[i + 2:i + 2 + 32 * m]))
+    return [(tuple(vals[32 * c:32 * c + 32:2]), tuple(vals[32 * c + 1:32 * c + 32:2])) for c in range(m)]
+
+
+def _gate_actions():
+    """conjugation actions (perm, sign) of h q0, h q1, s q0, s q1 and cz on the 16 Paulis, from their matrices"""
+    global _GACT
+    if _GACT is None:
+        P16 = [_pauli(2, p) for p in range(16)]
+        _GACT = {}
+        for g, qs in (("h", (0,)), ("h", (1,)), ("s", (0,)), ("s", (1,)), ("cz", (0, 1))):
+            C = gate_matrix(g, qs, 2)
+            Cd = _adj(C)
+            perm, sign = [0] * 16, [0] * 16
+            for a in range(16):
+                k, A = matmul(matmul(Cd, P16[a]), C)
+                for b in range(16):
+                    for sg in (1, -1):
+                        if (k, A) == (0, [[tuple(sg * v for v in x) for x in row] for row in P16[b][1]]):
+                            perm[a], sign[a] = b, sg
+            _GACT[(g, qs)] = (perm, sign)
+    return _GACT
+
+
+def clifford_word(action):
+    """a gate word (time order; gates h, sdg and cz) of the two-qubit Clifford with the given Pauli action
+    (perm, sign), up to global phase. The images of X_q and Z_q are reduced to +X_q and +Z_q by conjugation with
+    gates g_1 .. g_m, qubit by qubit: Z_q's image made a lone Z on q, then X_q's image a lone X on q with gates that
+    keep Z_q, then the signs. So C g_1 .. g_m is the identity up to phase and C = g_m^-1 .. g_1^-1 (g_1^-1 first)."""
+    act = _gate_actions()
+    X = lambda q: 1 << (2 * q)
+    Z = lambda q: 3 << (2 * q)
+    img = {P: (action[1][P], action[0][P]) for q in range(2) for P in (X(q), Z(q))}
+    word = []
+
+    def apply(*gates):                      # right-multiply the Clifford by each gate: its images conjugated by it
+        for g in gates:
+            perm, sign = act[g]
+            for P, (sg, b) in img.items():
+                img[P] = (sg * sign[b], perm[b])
+            word.append(g)
+
+    H = lambda q: ("h", (q,))
+    S = lambda q: ("s", (q,))
+    CZ = ("cz", (0, 1))
+    cx = lambda c, t: apply(H(t), CZ, H(t))  # CX(c -> t) = H_t CZ H_t
+    digit = lambda b, q: (b >> (2 * q)) & 3
+    for q in range(2):
+        o = 1 - q
+        # Z_q's image: every Y (S: Y -> X) and X (H: X -> Z) digit on qubits >= q turned into Z, then a lone Z on q
+        for j in range(q, 2):
+            if digit(img[Z(q)][1], j) == 2:
+                apply(S(j))
+            if digit(img[Z(q)][1], j) == 1:
+                apply(H(j))
+        if q == 0:
+            if digit(img[Z(q)][1], q) == 0:
+                cx(q, o)                         # Z_o -> Z_q Z_o: a Z on q
+            if digit(img[Z(q)][1], o):
+                cx(o, q)                         # Z_q -> Z_o Z_q: the Z on o cleared
+            # X_q's image anticommutes with Z_q (an X or Y on q); CX(q -> o), CZ and S_q keep Z_q
+            if digit(img[X(q)][1], o) in (1, 2):
+                cx(q, o)                         # X_q -> X_q X_o: no X part left on o
+            if digit(img[X(q)][1], o) == 3:
+                apply(CZ)                        # X_q -> X_q Z_o: the Z on o cleared
+        if digit(img[X(q)][1], q) == 2:
+            apply(S(q))                          # Y_q -> X_q
+    for q in range(2):                           # signs: Z_q = S_q S_q flips X_q's, X_q = H_q Z_q H_q flips Z_q's
+        if img[X(q)][0] < 0:
+            apply(S(q), S(q))
+        if img[Z(q)][0] < 0:
+            apply(H(q), S(q), S(q), H(q))
+    if any(img[P] != (1, P) for P in img):
+        raise ValueError("not a Clifford action")
+    inverse = {"h": "h", "cz": "cz", "s": "sdg"}
+    return [(inverse[g], qs) for g, qs in word]
+
+
+def rus_circuit(res, cliffords):
     """the gates (time order) of a `rus` result: W = R(P_1)..R(P_j) C R(Q_c)^-1..R(Q_1)^-1 with fw = (P_1..P_j), the
-    Clifford C = the spec's Clifford `cliff` and tb = (Q_1..Q_c)"""
+    Clifford C = entry `cliff` of the rus-spec's Clifford list (rspec_cliffords) and tb = (Q_1..Q_c)"""
     gates = []
     for q in res["tb"]:
         gates += _rotation(q, True)
-    for gi in _clifford_words()[res["cliff"]][2]:
-        g, qs = _CGEN[gi]
+    for g, qs in clifford_word(cliffords[res["cliff"]]):
         gates += [("h", (1,)), ("cx", (0, 1)), ("h", (1,))] if g == "cz" else [(g, qs)]
     for p in reversed(res["fw"]):
         gates += _rotation(p, False)
@@ -205,17 +256,18 @@ def parse_qasm(text):
     return n, circ
 
 
-def rus_check(qasm_text, res, outcome=None):
+def rus_check(qasm_text, res, cliffords, outcome=None):
     """exact check of a `rus` result against its target circuit: the result's circuit V has the target's success
     branch (outcome 0 of V = a unit times the target's outcome-ks branch, so the same success unitary and
-    probability), its failure branch is proportional to a Clifford, and its T-count is the reported one"""
+    probability), its failure branch is proportional to a Clifford, and its T-count is the reported one.
+    cliffords: the Clifford list of the rus-spec the result came from (rspec_cliffords)"""
     from .workloads import unitary
     n, circ = parse_qasm(qasm_text)
     if n != 2:
         return False
     W = unitary(2, circ)
     ks = outcome if outcome is not None else rus_success_outcome(qasm_text, W)
-    gates = rus_circuit(res)
+    gates = rus_circuit(res, cliffords)
     V = unitary(2, gates)
     kW, BW = _blocks(W)
     kV, BV = _blocks(V)

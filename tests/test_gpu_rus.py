@@ -76,7 +76,8 @@ def test_api_matches(specs):
         assert eng.rus_lines(rc, levels, out) == want, case["name"]
         assert out["kernel_launches"] > 0
         if rc == 0:                                   # the found circuit, checked exactly against its target
-            assert verify.rus_check(qasm[case["target"]], out), case["name"]
+            cl = verify.rspec_cliffords(specs[case["target"]].read_text())
+            assert verify.rus_check(qasm[case["target"]], out, cl), case["name"]
     eng.trim()
 
 

@@ -148,12 +148,36 @@ def test_found_circuits_verify_exactly():
     """every found circuit of the fixtures passes the exact RUS check of cheese_b200.verify (the role of the
     reference's `rus.py verify`), and damaged results do not"""
     from cheese_b200 import verify
+    from conftest import rus_spec_text
     qasm = {c["name"]: c["qasm"] for c in SPEC_CASES}
     found = [c for c in CASES if c["rc"] == 0]
     assert len(found) == 7
     for c in found:
-        assert verify.rus_check(qasm[c["target"]], json.loads(c["stdout"][-1])), c["name"]
+        cl = verify.rspec_cliffords(rus_spec_text(c["target"]))
+        assert verify.rus_check(qasm[c["target"]], json.loads(c["stdout"][-1]), cl), c["name"]
     res = json.loads(found[-1]["stdout"][-1])
+    cl = verify.rspec_cliffords(rus_spec_text(found[-1]["target"]))
     for damage in ({"cliff": (res["cliff"] + 1) % 11520}, {"tb": res["tb"][:-1]}, {"fw": res["fw"][1:] + [1]},
                    {"tcount": res["tcount"] - 1}):
-        assert not verify.rus_check(qasm[found[-1]["target"]], {**res, **damage}), damage
+        assert not verify.rus_check(qasm[found[-1]["target"]], {**res, **damage}, cl), damage
+
+
+def test_clifford_words_realise_the_spec_list():
+    """the gate word built for an entry of a rus-spec's Clifford list has that entry's Pauli action exactly"""
+    import random
+    from conftest import rus_spec_text
+    from cheese_b200.workloads import matmul, unitary
+    cl = verify_mod().rspec_cliffords(rus_spec_text(CASES[0]["target"]))
+    assert len(cl) == 11520
+    P = [verify_mod()._pauli(2, p) for p in range(16)]
+    for i in list(range(40)) + random.Random(3).sample(range(11520), 200):
+        U = unitary(2, verify_mod().clifford_word(cl[i]))
+        Ud = verify_mod()._adj(U)
+        for a in range(16):
+            b, s = cl[i][0][a], cl[i][1][a]
+            assert matmul(matmul(Ud, P[a]), U) == (0, [[tuple(s * v for v in x) for x in r] for r in P[b][1]]), i
+
+
+def verify_mod():
+    from cheese_b200 import verify
+    return verify
