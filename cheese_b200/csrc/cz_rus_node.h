@@ -105,44 +105,60 @@ CZ_RUS_FN bool row_eq(const RM &A, int ra, int s, const RM &B, int rb) {   // s 
     if (s * A.x[ra * NC + c] != B.x[rb * NC + c] || s * A.y[ra * NC + c] != B.y[rb * NC + c]) return false;
   return true;
 }
-// the Clifford c with B = C_c A (B[a] = s_c(a) A[pi_c(a)] for every row), else -1. Enumeration of rus.cu:152-200: the
-// images of X_q0, Z_q0, X_q1, Z_q1 are rows of A equal up to sign to B's generator rows (rows ascending, + before -),
-// filtered by the generators' commutation pattern, looked up by their images and confirmed on all 16 rows; the first
-// confirmed one is returned, so the reported Clifford is the reference's.
+// sign of a row's first nonzero entry (x before y, column by column); 0 for a zero row. When s A[ra] == B[rb] the
+// rows' first nonzero entries sit at the same place, so s is the product of the two rows' signs.
+CZ_RUS_FN int row_lead_sign(const RM &A, int r) {
+  for (int c = 0; c < NC; c++) {
+    if (A.x[r * NC + c]) return A.x[r * NC + c] > 0 ? 1 : -1;
+    if (A.y[r * NC + c]) return A.y[r * NC + c] > 0 ? 1 : -1;
+  }
+  return 0;
+}
+CZ_RUS_FN int low_bit(uint32_t m) {
+#ifdef __CUDA_ARCH__
+  return __ffs((int)m) - 1;
+#else
+  return __builtin_ctz(m);
+#endif
+}
+// The Clifford c with B = C_c A (B[a] = s_c(a) A[pi_c(a)] for every row a), else -1; exact. A Clifford is named by
+// its images of the generator rows X_q0, Z_q0, X_q1, Z_q1 (rows 1, 3, 4, 12), each an image row and a sign: 5 bits
+// (row << 1 | minus), the key of sp.bygen (-1 for images no Clifford has). The possible images of each generator are
+// read off A once, as a mask over (row, sign) with bit 2 (row - 1) + minus, by one comparison per row with the signs
+// taken from the rows' leading entries. The Cliffords those masks allow are tried in ascending order of (image of
+// X_q0, of Z_q0, of X_q1, of Z_q1), each image ordered by row and then + before -, and the first that maps every
+// row is returned: when A repeats a row up to sign several Cliffords qualify, and this order picks the reference's.
 CZ_RUS_FN int rm_equiv(const RM &A, const RM &B, const RDev &sp) {
   if (A.e != B.e) return -1;
   const int gen[4] = {1, 3, 4, 12};
-  uint8_t cand[4][30];
-  int nc[4];
+  uint32_t mask[4];
   for (int g = 0; g < 4; g++) {
-    nc[g] = 0;
-    for (int r = 1; r < NR; r++)
-      for (int s = 1; s >= -1; s -= 2)
-        if (row_eq(A, r, s, B, gen[g])) cand[g][nc[g]++] = (uint8_t)((r << 1) | (s < 0));
-    if (!nc[g]) return -1;
+    const int sb = row_lead_sign(B, gen[g]);
+    uint32_t m = 0;
+    for (int r = 1; r < NR; r++) {
+      const int sa = row_lead_sign(A, r);
+      if (!sa && !sb) m |= 3u << (2 * (r - 1));                        // zero rows: equal with either sign
+      else if (sa && sb && row_eq(A, r, sa * sb, B, gen[g])) m |= 1u << (2 * (r - 1) + (sa * sb < 0));
+    }
+    if (!m) return -1;
+    mask[g] = m;
   }
-  auto com = [&](int p, int q) { return sp.tr[(p - 1) * NR + q] < 0; };   // P_p and P_q commute
-  for (int i0 = 0; i0 < nc[0]; i0++) {
-    const int b0 = cand[0][i0] >> 1;
-    for (int i1 = 0; i1 < nc[1]; i1++) {
-      const int b1 = cand[1][i1] >> 1;
-      if (com(b0, b1)) continue;
-      for (int i2 = 0; i2 < nc[2]; i2++) {
-        const int b2 = cand[2][i2] >> 1;
-        if (!com(b0, b2) || !com(b1, b2)) continue;
-        for (int i3 = 0; i3 < nc[3]; i3++) {
-          const int b3 = cand[3][i3] >> 1;
-          if (com(b2, b3) || !com(b0, b3) || !com(b1, b3)) continue;
-          const int key = cand[0][i0] | cand[1][i1] << 5 | cand[2][i2] << 10 | cand[3][i3] << 15;
+  for (uint32_t m0 = mask[0]; m0; m0 &= m0 - 1)
+    for (uint32_t m1 = mask[1]; m1; m1 &= m1 - 1)
+      for (uint32_t m2 = mask[2]; m2; m2 &= m2 - 1)
+        for (uint32_t m3 = mask[3]; m3; m3 &= m3 - 1) {
+          int key = 0;
+          const uint32_t ms[4] = {m0, m1, m2, m3};
+          for (int g = 0; g < 4; g++) {
+            const int b = low_bit(ms[g]);
+            key |= ((((b >> 1) + 1) << 1) | (b & 1)) << (5 * g);
+          }
           const int c = sp.bygen[key];
           if (c < 0) continue;
           bool ok = true;
           for (int a = 0; ok && a < NR; a++) ok = row_eq(A, sp.perm[c * NR + a], sp.sign[c * NR + a], B, a);
           if (ok) return c;
         }
-      }
-    }
-  }
   return -1;
 }
 

@@ -159,155 +159,123 @@ template <typename ST> __device__ __forceinline__ uint32_t zmodp(const Z4<ST> &x
 
 // ---------------- per-warp bound evaluations (child residual S in shared memory) ----------------
 
-// T bound: max(0, max over nonzero PTM entries of their sde), Walsh-Hadamard form of cheese.cu:397-449
-template <int NQ, typename U, typename ST> __device__ __noinline__ int warp_ptm(const Z4<ST> *S, int k, int lane) {
-  constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
-  Z4<U> y[EPL];
-#pragma unroll
-  for (int j = 0; j < EPL; j++) {
-    const int e = lane + 32 * j;
-    y[j] = e < E ? toU<U>(zcj(S[e])) : Z4<U>{0, 0, 0, 0};
+// ---- T bound: max(0, max over the nonzero PTM entries of their sde) (cheese.cu:397-449) ----
+// PTM entry (f, z) up to a unit: X_f(z) = sum_e (-1)^{e.z} Q_f[e], Q_f[e] = S[e ^ f] conj(S[e]), e and f running over
+// the E = N^2 (row, column) index pairs. Computed in Z[w] mod 2^b (b = 32 while 2 (n + k) <= 64, else 64): the
+// valuations are read off the low bits, as the reference does.
+//
+// One lane per pair f != 0, its transforms in registers. For f != 0, Q_f[e ^ f] = conj Q_f[e], so over a subgroup H
+// of index 2 that misses f, X_f(z) = sum_{e in H} (-1)^{e.z} (Q + (-1)^{f.z} conj Q)[e]: with Q = a + b w + c w^2 +
+// d w^3, Q + conj Q = 2a + (b - d) sqrt2 and Q - conj Q = i (2c + (b + d) sqrt2), so four real transforms over the
+// E/2 points of H (of a, c, b - d, b + d) give every output, and an output 2A + X sqrt2 has valuation
+// min(2 v2(A) + 2, 2 v2(X) + 1). H is {e < E/2} when f has its top bit, else {e : bit j of e is 0} with j the lowest
+// set bit of f; point i of H is e(i) = i with a 0 bit inserted at j (a linear map, so the transform over i is the
+// transform over H). With 32 lanes a round takes 32 pairs (f = lane + 32 r); f = 0 (Q = |S|^2 = alpha + beta sqrt2,
+// one 64-point transform each) is done by the whole warp, each lane holding points lane + 32 t.
+// Valuations fold into OR words: m = ctz(OR of 2A, X, alpha, beta over all outputs) is the least 2-adic valuation,
+// and v = 2 m + 1 unless bit m is set in the OR of the 2A and alpha outputs (then v = 2 m).
+// PASSES splits the four components into passes (fewer live registers, the products recomputed per pass).
+template <typename U> __device__ __forceinline__ U pair_component(int comp, const Z4<U> &x, const Z4<U> &y) {
+  switch (comp) {   // the coordinates of x conj(y): a, c, b - d, b + d
+    case 0: return y.a * x.a + y.b * x.b + y.c * x.c + y.d * x.d;
+    case 1: return y.a * x.c + y.b * x.d - y.c * x.a - y.d * x.b;
+    case 2: return (y.b - y.d) * x.a + (y.a + y.c) * x.b + (y.b + y.d) * x.c - (y.a - y.c) * x.d;
+    default: return (y.a - y.c) * x.b + (y.b - y.d) * x.c + (y.a + y.c) * x.d - (y.b + y.d) * x.a;
   }
-  U o1 = 0, o2 = 0;
-#pragma unroll 1
-  for (int f = 0; f < E; f++) {         // f = (fa, fb): Q[x][c] = S[x ^ fa][c ^ fb] conj(S[x][c])
-    Z4<U> q[EPL];
-#pragma unroll
-    for (int j = 0; j < EPL; j++) {
-      const int e = lane + 32 * j;
-      q[j] = e < E ? umul(toU<U>(S[e ^ f]), y[j]) : Z4<U>{0, 0, 0, 0};
-    }
-#pragma unroll
-    for (int h = 1; h < E; h <<= 1) {
-      if (h < 32) {
-#pragma unroll
-        for (int j = 0; j < EPL; j++) {
-          const Z4<U> o = ushfl(q[j], h);
-          q[j] = (lane & h) ? usub(o, q[j]) : uadd(q[j], o);
-        }
-      } else {
-        const int hj = h >> 5;
-#pragma unroll
-        for (int j = 0; j < EPL; j++)
-          if (!(j & hj)) { const Z4<U> u = q[j], v = q[j | hj]; q[j] = uadd(u, v); q[j | hj] = usub(u, v); }
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < EPL; j++) { o1 |= q[j].a | q[j].b | q[j].c | q[j].d; o2 |= (q[j].a ^ q[j].c) | (q[j].b ^ q[j].d); }
-  }
-#pragma unroll
-  for (int m = 16; m; m >>= 1) { o1 |= __shfl_xor_sync(FULL, o1, m); o2 |= __shfl_xor_sync(FULL, o2, m); }
-  if (!o1) return 0;
-  const int mv = sizeof(U) == 8 ? __ffsll((long long)o1) - 1 : __ffs((int)o1) - 1;
-  const int v = 2 * mv + (((o2 >> mv) & 1) ? 0 : 1);
-  const int top = 2 * (NQ + k);
-  return top - v > 0 ? top - v : 0;
 }
-// The same bound for 3 qubits with the conjugate pairing of the products: for f = (fa, fb) != 0,
-// Q[e ^ f] = conj(Q[e]), so with j the lowest set bit of f and H = {e : e_j = 0} (32 points),
-//   X(z) = sum_{e in H} (-1)^{e.z} (Q[e] + (-1)^{f.z} conj(Q[e])),
-// i.e. half of the outputs are the 32-point transform of Q + conj Q = (2a, b - d, 0, d - b) and the other half that
-// of Q - conj Q = (0, b + d, 2c, b + d): four real 32-point transforms of (a, c, b - d, b + d) instead of a 64-point
-// transform over Z[w]. For f = 0, Q = |S[e]|^2 = (alpha, beta, 0, -beta). Valuations need only two OR words per
-// class: with m = ctz(OR of all coefficients), the sqrt2-parity bit is bit m of OR(a ^ c | b ^ d), which is bit m
-// of 2A | 2C | A0 (b - d and its negative agree at bit m).
-// Layout: 8 pairs per warp iteration, 4 lanes per pair, 8 products per lane (3 butterfly stages in registers, 2
-// across the 4 lanes as shuffle + multiply-add); pairs are ordered by j so the f-independent operand S[e] is a
-// 4-address broadcast in 7 of the 8 iterations.
-__device__ __forceinline__ int pair_of(int idx) {   // the 63 nonzero f ordered by lowest set bit; 64th: none
-  if (idx < 32) return 2 * idx + 1;
-  if (idx < 48) return 4 * (idx - 32) + 2;
-  if (idx < 56) return 8 * (idx - 48) + 4;
-  if (idx < 60) return 16 * (idx - 56) + 8;
-  if (idx < 62) return 32 * (idx - 60) + 16;
-  return idx == 62 ? 32 : 0;
-}
-template <typename ST> __device__ __noinline__ int warp_ptm3(const Z4<ST> *S, int k, int lane) {
-  using U = uint32_t;
-  U R1 = 0, R2 = 0, P = 0, Q = 0;
-  {   // f = 0: entries lane, lane + 32; bit 5 in registers, bits 0..4 across lanes
-    U al[2], be[2];
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const Z4<U> y = toU<U>(S[lane + 32 * h]);
-      al[h] = y.a * y.a + y.b * y.b + y.c * y.c + y.d * y.d;
-      be[h] = y.a * y.b + y.b * y.c + y.c * y.d - y.d * y.a;
-    }
-    U a0 = al[0] + al[1], a1 = al[0] - al[1], b0 = be[0] + be[1], b1 = be[0] - be[1];
-#pragma unroll
-    for (int h = 1; h < 32; h <<= 1) {
-      const U sg = (lane & h) ? 0xffffffffu : 1u;
-      a0 = __shfl_xor_sync(FULL, a0, h) + sg * a0;
-      a1 = __shfl_xor_sync(FULL, a1, h) + sg * a1;
-      b0 = __shfl_xor_sync(FULL, b0, h) + sg * b0;
-      b1 = __shfl_xor_sync(FULL, b1, h) + sg * b1;
-    }
-    R1 = a0 | a1 | b0 | b1;
-    R2 = a0 | a1;
-  }
-  const int pg = lane >> 2, sub = lane & 3;
+template <int NQ, typename U, int PASSES, typename ST>
+__device__ __forceinline__ int tbound_lanes(const Z4<ST> *S, int k, int lane) {
+  constexpr int E = 1 << (2 * NQ), HP = E / 2, CPP = 4 / PASSES;
+  static_assert(4 % PASSES == 0, "passes split the four components evenly");
+  U P = 0, Q = 0;
 #pragma unroll 1
-  for (int it = 0; it < 8; it++) {
-    const int f = pair_of(it * 8 + pg);
-    const int j = f ? __ffs(f) - 1 : 0;
-    const int lo = (1 << j) - 1;
-    U A[8], C[8], X[8], Y[8];     // transforms of a, c, b - d, b + d
+  for (int f = lane; f < E; f += 32) {
+    if (f == 0) continue;
+    const int lomask = (f & HP) ? E - 1 : (f & -f) - 1;   // bits below the inserted 0 (all of them: none inserted)
+#pragma unroll 1
+    for (int pass = 0; pass < PASSES; pass++) {
+      U v[CPP][HP];
 #pragma unroll
-    for (int kk = 0; kk < 8; kk++) {
-      const int i = sub * 8 + kk;
-      const int e = ((i & ~lo) << 1) | (i & lo);
-      if (f) {
-        const Z4<U> x = toU<U>(S[e ^ f]), y = toU<U>(S[e]);
-        const U m1 = y.b - y.d, m2 = y.a + y.c, m3 = y.b + y.d, m4 = y.a - y.c;
-        A[kk] = y.a * x.a + y.b * x.b + y.c * x.c + y.d * x.d;
-        C[kk] = y.a * x.c + y.b * x.d - y.c * x.a - y.d * x.b;
-        X[kk] = m1 * x.a + m2 * x.b + m3 * x.c - m4 * x.d;
-        Y[kk] = m4 * x.b + m1 * x.c + m2 * x.d - m3 * x.a;
-      } else {
-        A[kk] = C[kk] = X[kk] = Y[kk] = 0;
+      for (int i = 0; i < HP; i++) {
+        const int e = (i & lomask) | ((i & ~lomask) << 1);
+        const Z4<U> y = toU<U>(S[e]), x = toU<U>(S[e ^ f]);
+#pragma unroll
+        for (int c = 0; c < CPP; c++) v[c][i] = pair_component<U>(pass * CPP + c, x, y);
+      }
+#pragma unroll
+      for (int h = 1; h < HP; h <<= 1)
+#pragma unroll
+        for (int i = 0; i < HP; i++)
+          if (!(i & h)) {
+#pragma unroll
+            for (int c = 0; c < CPP; c++) {
+              const U u = v[c][i], w = v[c][i | h];
+              v[c][i] = u + w;
+              v[c][i | h] = u - w;
+            }
+          }
+#pragma unroll
+      for (int c = 0; c < CPP; c++) {
+        U o = 0;
+#pragma unroll
+        for (int i = 0; i < HP; i++) o |= v[c][i];
+        if (pass * CPP + c < 2) P |= o;
+        else Q |= o;
       }
     }
+  }
+  // f = 0: alpha = |y|^2 real part, beta its sqrt2 part, transformed over all E points across the warp
+  constexpr int PL = E > 32 ? E / 32 : 1;   // points per lane
+  U al[PL], be[PL];
 #pragma unroll
-    for (int h = 1; h < 8; h <<= 1)
+  for (int t = 0; t < PL; t++) {
+    const int e = lane + 32 * t;
+    const Z4<U> y = e < E ? toU<U>(S[e]) : Z4<U>{0, 0, 0, 0};
+    al[t] = y.a * y.a + y.b * y.b + y.c * y.c + y.d * y.d;
+    be[t] = y.a * y.b + y.b * y.c + y.c * y.d - y.d * y.a;
+  }
 #pragma unroll
-      for (int kk = 0; kk < 8; kk++)
-        if (!(kk & h)) {
-          U u, v;
-          u = A[kk]; v = A[kk | h]; A[kk] = u + v; A[kk | h] = u - v;
-          u = C[kk]; v = C[kk | h]; C[kk] = u + v; C[kk | h] = u - v;
-          u = X[kk]; v = X[kk | h]; X[kk] = u + v; X[kk | h] = u - v;
-          u = Y[kk]; v = Y[kk | h]; Y[kk] = u + v; Y[kk | h] = u - v;
-        }
+  for (int h = 1; h < PL; h <<= 1)
 #pragma unroll
-    for (int h = 1; h < 4; h <<= 1) {
-      const U sg = (sub & h) ? 0xffffffffu : 1u;
-#pragma unroll
-      for (int kk = 0; kk < 8; kk++) {
-        A[kk] = __shfl_xor_sync(FULL, A[kk], h) + sg * A[kk];
-        C[kk] = __shfl_xor_sync(FULL, C[kk], h) + sg * C[kk];
-        X[kk] = __shfl_xor_sync(FULL, X[kk], h) + sg * X[kk];
-        Y[kk] = __shfl_xor_sync(FULL, Y[kk], h) + sg * Y[kk];
+    for (int t = 0; t < PL; t++)
+      if (!(t & h)) {
+        U u = al[t], w = al[t | h]; al[t] = u + w; al[t | h] = u - w;
+        u = be[t]; w = be[t | h]; be[t] = u + w; be[t | h] = u - w;
       }
-    }
+  U R1 = 0, R2 = 0;
 #pragma unroll
-    for (int kk = 0; kk < 8; kk++) { P |= A[kk] | C[kk]; Q |= X[kk] | Y[kk]; }
+  for (int t = 0; t < PL; t++) {
+#pragma unroll
+    for (int h = 1; h < 32 && h < E; h <<= 1) {
+      const U oa = __shfl_xor_sync(FULL, al[t], h), ob = __shfl_xor_sync(FULL, be[t], h);
+      al[t] = (lane & h) ? oa - al[t] : al[t] + oa;
+      be[t] = (lane & h) ? ob - be[t] : be[t] + ob;
+    }
+    R1 |= al[t] | be[t];
+    R2 |= al[t];
   }
 #pragma unroll
   for (int m = 16; m; m >>= 1) {
     P |= __shfl_xor_sync(FULL, P, m); Q |= __shfl_xor_sync(FULL, Q, m);
     R1 |= __shfl_xor_sync(FULL, R1, m); R2 |= __shfl_xor_sync(FULL, R2, m);
   }
-  const U O1 = (P << 1) | Q | R1, O2 = (P << 1) | R2;
+  const U O1 = (U)(P << 1) | Q | R1, O2 = (U)(P << 1) | R2;
   if (!O1) return 0;
-  const int mv = __ffs((int)O1) - 1;
+  const int mv = sizeof(U) == 8 ? __ffsll((long long)O1) - 1 : __ffs((int)O1) - 1;
   const int v = 2 * mv + (((O2 >> mv) & 1) ? 0 : 1);
-  const int top = 2 * (3 + k);
+  const int top = 2 * (NQ + k);
   return top - v > 0 ? top - v : 0;
 }
+// 32-bit residues in one pass (3 qubits: 128 transform values per lane); 64-bit residues (k > 29, rare) one
+// component per pass
+template <int NQ, typename ST> __device__ __noinline__ int warp_tbound32(const Z4<ST> *S, int k, int lane) {
+  return tbound_lanes<NQ, uint32_t, 1>(S, k, lane);
+}
+template <int NQ, typename ST> __device__ __noinline__ int warp_tbound64(const Z4<ST> *S, int k, int lane) {
+  return tbound_lanes<NQ, uint64_t, 4>(S, k, lane);
+}
 template <int NQ, typename ST> __device__ __forceinline__ int ptm_bound(const Z4<ST> *S, int k, int lane) {
-  if (2 * (NQ + k) > 64) return warp_ptm<NQ, uint64_t, ST>(S, k, lane);
-  if constexpr (NQ == 3) return warp_ptm3<ST>(S, k, lane);
-  else return warp_ptm<NQ, uint32_t, ST>(S, k, lane);
+  return 2 * (NQ + k) > 64 ? warp_tbound64<NQ, ST>(S, k, lane) : warp_tbound32<NQ, ST>(S, k, lane);
 }
 
 // rank over F_p of the operator-Schmidt matrix across cut A (cheese.cu:271-303): lane j owns column j, fraction-free
@@ -633,174 +601,142 @@ template <int NQ, typename ST> __device__ bool warp_goal(const Z4<ST> *S, int k,
 // not at all under Cliffords. CX: the Schmidt rank of a row across a cut changes by at most a factor 2 per crossing
 // two-qubit gate. Ranks are exact (minors in int64 under a coefficient bound), as in the reference.
 template <typename ST> __device__ __forceinline__ Zw zw_of(const Z4<ST> &x) { return Zw{x.a, x.b, x.c, x.d}; }
-__device__ __forceinline__ int zval_dev(Zw x) {          // sqrt2-adic valuation, x != 0
-  int v = 0;
-  while (zdiv2ok(x)) { x = zdown(x); v++; if (v > 200) break; }
-  return v;
+// sqrt2-adic valuation of a nonzero x = a + b w + c w^2 + d w^3 in closed form: 2 = sqrt2^2, and x / 2^m (m the
+// least 2-adic valuation of the coefficients) is divisible by sqrt2 exactly when a = c and b = d mod 2.
+__device__ __forceinline__ int zval_closed(const Zw &x) {
+  const uint64_t o = (uint64_t)(x.a | x.b | x.c | x.d);
+  const int m = __ffsll((long long)o) - 1;
+  return 2 * m + ((((uint64_t)((x.a ^ x.c) | (x.b ^ x.d)) >> m) & 1) ? 0 : 1);
 }
-__device__ __forceinline__ int64_t zbig_dev(const Zw &x) {
-  int64_t m = 0, v;
-  v = x.a < 0 ? -x.a : x.a; if (v > m) m = v;
-  v = x.b < 0 ? -x.b : x.b; if (v > m) m = v;
-  v = x.c < 0 ? -x.c : x.c; if (v > m) m = v;
-  v = x.d < 0 ? -x.d : x.d; if (v > m) m = v;
-  return m;
-}
-template <typename ST> __device__ int state_row_sde(const Z4<ST> *row, int N, int k) {
-  int v = 1 << 30;
-  for (int x = 0; x < N; x++)
-    if (!zz(row[x])) { const int z = zval_dev(zw_of(row[x])); if (z < v) v = z; }
-  return v == (1 << 30) || k - v < 0 ? 0 : k - v;
-}
-__device__ __forceinline__ Zw zneg_dev(Zw x) { return Zw{-x.a, -x.b, -x.c, -x.d}; }
-// P_b |v> = +-|v>  <=>  <v|P_b|v> = +-<v|v>; P_b per qubit digit: 1 X, 2 Y, 3 Z
-template <typename ST> __device__ bool state_pauli_stab(const Z4<ST> *row, int nq, int b, Zw nrm) {
-  int f = 0, y = 0, z = 0;
-  for (int q = 0; q < nq; q++) {
-    const int d = (b >> (2 * q)) & 3;
-    if (d == 1 || d == 2) f |= 1 << q;
-    if (d == 2) y |= 1 << q;
-    if (d == 3) z |= 1 << q;
-  }
-  Zw acc{0, 0, 0, 0};
-  for (int x = 0; x < (1 << nq); x++) {
-    const Z4<ST> u = row[x ^ f], v = row[x];
-    if (zz(u) || zz(v)) continue;
-    const int ph = (2 * __popc(y) + 4 * __popc(x & (y | z))) & 7;
-    acc = zadd(acc, zmul(zconj(zw_of(u)), zmul(zw_of(v), zwpow(ph))));
-  }
-  return zeq(acc, nrm) || zeq(acc, zneg_dev(nrm));
-}
-__device__ Zw state_det(const Zw *M, int r, int stride) {        // r <= 4: Laplace along the first row
-  if (r == 1) return M[0];
-  if (r == 2) return zsub(zmul(M[0], M[stride + 1]), zmul(M[1], M[stride]));
-  Zw acc{0, 0, 0, 0};
-  Zw sub[9];
-  for (int j = 0; j < r; j++) {
-    if (zzero(M[j])) continue;
-    int t = 0;
-    for (int i = 1; i < r; i++)
-      for (int c = 0; c < r; c++)
-        if (c != j) sub[t++] = M[i * stride + c];
-    Zw d3;
-    if (r - 1 == 2) d3 = zsub(zmul(sub[0], sub[3]), zmul(sub[1], sub[2]));
-    else {                                                         // r - 1 == 3
-      d3 = Zw{0, 0, 0, 0};
-      for (int jj = 0; jj < 3; jj++) {
-        if (zzero(sub[jj])) continue;
-        Zw m2[4];
-        int u = 0;
-        for (int i = 1; i < 3; i++)
-          for (int c = 0; c < 3; c++)
-            if (c != jj) m2[u++] = sub[i * 3 + c];
-        const Zw d2 = zmul(sub[jj], zsub(zmul(m2[0], m2[3]), zmul(m2[1], m2[2])));
-        d3 = (jj & 1) ? zsub(d3, d2) : zadd(d3, d2);
-      }
-    }
-    const Zw d = zmul(M[j], d3);
-    acc = (j & 1) ? zsub(acc, d) : zadd(acc, d);
-  }
-  return acc;
-}
-// exact Schmidt rank of the row reshaped (qubits A, |A| = sa) x (the rest); -1 if the coefficients are too large
-template <typename ST> __device__ int state_row_rank(const Z4<ST> *row, int nq, int A, int sa) {
-  const int R = 1 << sa, C = 1 << (nq - sa), N = 1 << nq;
-  Zw M[4 * 16];
-  int64_t B = 0;
-  for (int x = 0; x < N; x++) {
-    int ia = 0, ib = 0, na = 0, nb = 0;
-    for (int q = 0; q < nq; q++) {
-      if ((A >> q) & 1) ia |= ((x >> q) & 1) << na++;
-      else ib |= ((x >> q) & 1) << nb++;
-    }
-    M[ia * C + ib] = zw_of(row[x]);
-    const int64_t v = zbig_dev(zw_of(row[x]));
-    if (v > B) B = v;
-  }
-  const int64_t lim[5] = {0, 1LL << 40, 1LL << 29, 1LL << 18, 1LL << 12};
-  for (int r = R < C ? R : C; r >= 2; r--) {
-    if (B >= lim[r]) return -1;
-    int rs[4], cs[4];
-    for (int rm = 0; rm < (1 << R); rm++) {
-      if (__popc(rm) != r) continue;
-      int t = 0;
-      for (int i = 0; i < R; i++) if ((rm >> i) & 1) rs[t++] = i;
-      for (int cm = 0; cm < (1 << C); cm++) {
-        if (__popc(cm) != r) continue;
-        int u = 0;
-        for (int i = 0; i < C; i++) if ((cm >> i) & 1) cs[u++] = i;
-        Zw sub[16];
-        for (int i = 0; i < r; i++)
-          for (int j = 0; j < r; j++) sub[i * r + j] = M[rs[i] * C + cs[j]];
-        if (!zzero(state_det(sub, r, r))) return r;
-      }
-    }
-  }
-  for (int x = 0; x < N; x++) if (!zz(row[x])) return 1;
-  return 0;
-}
-__device__ __forceinline__ int state_rank_need(int rv, int rt) {  // fewest crossing two-qubit gates between ranks
-  if (rv < 0 || rt <= 0 || rv == 0) return 0;
-  const int lo = rv < rt ? rv : rt, hi = rv < rt ? rt : rv;
-  int c = 0;
-  while ((lo << c) < hi) c++;
-  return c;
+__device__ __forceinline__ int64_t zmax_abs(const Zw &x) {
+  const int64_t a = x.a < 0 ? -x.a : x.a, b = x.b < 0 ? -x.b : x.b, c = x.c < 0 ? -x.c : x.c, d = x.d < 0 ? -x.d : x.d;
+  return max(max(a, b), max(c, d));
 }
 __device__ __forceinline__ int warp_imax(int v) {
-  for (int m = 16; m; m >>= 1) { const int o = __shfl_xor_sync(FULL, v, m); if (o > v) v = o; }
+  for (int m = 16; m; m >>= 1) v = max(v, __shfl_xor_sync(FULL, v, m));
   return v;
 }
-// H and CX bounds of a state residual: h = max over rows of |sde - goal sde|, c2 from the per-cut rank needs
-template <int NQ, typename ST> __device__ __noinline__ void warp_state_cheap(const Z4<ST> *S, int k, const DevSpec &sp, int lane,
-                                                                int &h, int &c2) {
-  constexpr int N = 1 << NQ;
+// fewest crossing two-qubit gates between Schmidt ranks rv (the row's) and rt (the goal's): the rank changes by at
+// most a factor 2 per crossing gate, so c = ceil(log2(ceil(hi / lo))); 0 when either rank is unknown (-1) or 0
+__device__ __forceinline__ int rank_gates(int rv, int rt) {
+  if (rv <= 0 || rt <= 0) return 0;
+  const int lo = min(rv, rt), q = (max(rv, rt) + lo - 1) / lo;
+  return q > 1 ? 32 - __clz(q - 1) : 0;
+}
+
+// ---------------- state targets (rows j < m: the images of the inputs; cheese.cu:451-583) ----------------
+// H: the sde of a row changes by at most 1 per H. CX: the Schmidt rank of a row across a cut changes by at most a
+// factor 2 per crossing two-qubit gate. T: the stabilizer nullity of a row changes by at most 1 per T and not at all
+// under Cliffords. All three are computed exactly, as the reference does (ranks over Q(w), not mod p).
+//
+// H and CX bounds: h = max over rows of |sde - goal sde|; c2 from the per-cut needs through the CX table. The sde
+// part has each lane on entries lane + 32 t (a row = N consecutive lanes, reduced by shuffles). The rank part has
+// one lane per (row, cut): the row reshaped to R x C across the cut, with R = 2 at up to 3 qubits (cuts of one
+// qubit), has rank 2 when one of its 2 x 2 minors is nonzero, else rank 1 when it is nonzero; a row with a
+// coefficient of 2^29 or more has an unknown rank (-1: no bound), like the reference's int64 guard.
+template <int NQ, typename ST> __device__ __noinline__ void warp_state_cheap(const Z4<ST> *S, int k, const DevSpec &sp,
+                                                                           int lane, int &h, int &c2) {
+  static_assert(NQ <= 3, "state bounds: cuts of one qubit (two-row reshapes)");
+  constexpr int N = 1 << NQ, E = N * N, PL = E > 32 ? E / 32 : 1;
   const int W = 2 + sp.ncuts;
-  int d = 0;
-  if (lane < sp.m) { d = state_row_sde(S + lane * N, N, k) - sp.ginfo[lane * W]; if (d < 0) d = -d; }
-  h = warp_imax(d);
-  int mine[CUTMAX];
-  for (int c = 0; c < CUTMAX; c++) mine[c] = 0;
+  int hmax = 0;
+#pragma unroll
+  for (int t = 0; t < PL; t++) {
+    const int e = lane + 32 * t, j = e / N;
+    const Zw x = e < E ? zw_of(S[e]) : Zw{0, 0, 0, 0};
+    int v = zzero(x) ? 1 << 30 : zval_closed(x);
+#pragma unroll
+    for (int o = 1; o < N; o <<= 1) v = min(v, __shfl_xor_sync(FULL, v, o));
+    if (j < sp.m && e < E && (e & (N - 1)) == 0) {
+      const int sde = v == (1 << 30) || k < v ? 0 : k - v;
+      hmax = max(hmax, abs(sde - sp.ginfo[j * W]));
+    }
+  }
+  h = warp_imax(hmax);
+  int need[CUTMAX];
+  for (int c = 0; c < CUTMAX; c++) need[c] = 0;
   for (int it = lane; it < sp.m * sp.ncuts; it += 32) {
-    const int j = it / sp.ncuts, c = it % sp.ncuts;
-    const int nd = state_rank_need(state_row_rank(S + j * N, NQ, sp.cutmask[c], sp.cutsize[c]), sp.ginfo[j * W + 2 + c]);
-    if (nd > mine[c]) mine[c] = nd;
+    const int j = it / sp.ncuts, c = it % sp.ncuts, A = sp.cutmask[c];
+    Zw M[2][N / 2];
+    int64_t big = 0;
+    bool nonzero = false;
+    for (int x = 0; x < N; x++) {
+      int ia = 0, ib = 0, nb = 0;
+      for (int q = 0; q < NQ; q++) {
+        if ((A >> q) & 1) ia = (x >> q) & 1;
+        else ib |= ((x >> q) & 1) << nb++;
+      }
+      M[ia][ib] = zw_of(S[j * N + x]);
+      big = max(big, zmax_abs(M[ia][ib]));
+      nonzero |= !zzero(M[ia][ib]);
+    }
+    int rank = nonzero ? 1 : 0;
+    if (big >= (1LL << 29)) rank = -1;
+    else
+      for (int p = 0; p < N / 2 && rank == 1; p++)
+        for (int q = p + 1; q < N / 2; q++)
+          if (!zeq(zmul(M[0][p], M[1][q]), zmul(M[0][q], M[1][p]))) { rank = 2; break; }
+    need[c] = max(need[c], rank_gates(rank, sp.ginfo[j * W + 2 + c]));
   }
   int idx = 0, mult = 1, mx = 0;
   for (int c = 0; c < sp.ncuts; c++) {
-    int nd = warp_imax(mine[c]);
-    if (nd > sp.rad[c] - 1) nd = sp.rad[c] - 1;
+    const int nd = min(warp_imax(need[c]), sp.rad[c] - 1);
     idx += nd * mult;
     mult *= sp.rad[c];
-    if (nd > mx) mx = nd;
+    mx = max(mx, nd);
   }
-  c2 = sp.have_table && idx < sp.ncx ? sp.cxtable[idx] : mx;
+  c2 = sp.have_table && idx < sp.ncx ? __ldg(&sp.cxtable[idx]) : mx;
 }
-// T bound of a state residual: max over rows of |stabilizer nullity - the goal's|
+// T bound: max over rows of |stabilizer nullity - the goal's|, nullity = n - log2 of the number of Paulis P with
+// <v|P|v> = +-<v|v>. One lane per (row, X part f) (a row = N consecutive lanes): with the Pauli's Z part z,
+// <v|P|v> = i^{|f & z|} W(z), W = the N-point Walsh-Hadamard transform over x of conj(v[x ^ f]) v[x], so one small
+// transform gives the row's N Paulis of X part f; <v|v> is W(0) of the row's f = 0 lane. Rows with a coefficient of
+// 2^27 or more are skipped (the reference's int64 guard; the transform stays below 2^62).
 template <int NQ, typename ST> __device__ __noinline__ int warp_state_t(const Z4<ST> *S, const DevSpec &sp, int lane) {
-  constexpr int N = 1 << NQ, PP = 1 << (2 * NQ);
+  static_assert(NQ <= 3, "state bounds: one row per N lanes");
+  constexpr int N = 1 << NQ, E = N * N, PL = E > 32 ? E / 32 : 1;
+  const int W = 2 + sp.ncuts;
   int best = 0;
-  for (int j = 0; j < sp.m; j++) {
-    const Z4<ST> *row = S + j * N;
-    int64_t B = 0;
-    Zw nrm{0, 0, 0, 0};
+#pragma unroll
+  for (int t = 0; t < PL; t++) {
+    const int task = lane + 32 * t, j = task / N, f = task & (N - 1);
+    const bool live = task < E && j < sp.m;
+    Zw w[N];
+    int64_t big = 0;
+#pragma unroll
     for (int x = 0; x < N; x++) {
-      const int64_t v = zbig_dev(zw_of(row[x]));
-      if (v > B) B = v;
-      if (!zz(row[x])) nrm = zadd(nrm, zmul(zconj(zw_of(row[x])), zw_of(row[x])));
+      const Zw v = live ? zw_of(S[j * N + x]) : Zw{0, 0, 0, 0}, u = live ? zw_of(S[j * N + (x ^ f)]) : Zw{0, 0, 0, 0};
+      big = max(big, zmax_abs(v));
+      w[x] = zmul(zconj(u), v);
     }
-    if (B >= (1LL << 27)) continue;                                   // int64-safe products only
+#pragma unroll
+    for (int hb = 1; hb < N; hb <<= 1)
+#pragma unroll
+      for (int x = 0; x < N; x++)
+        if (!(x & hb)) { const Zw a = w[x], b = w[x | hb]; w[x] = zadd(a, b); w[x | hb] = zsub(a, b); }
+    // <v|v>, from the row's f = 0 lane
+    const int src = (lane & ~(N - 1)) & 31;
+    const Zw nrm{__shfl_sync(FULL, w[0].a, src), __shfl_sync(FULL, w[0].b, src), __shfl_sync(FULL, w[0].c, src),
+                 __shfl_sync(FULL, w[0].d, src)};
     int cnt = 0;
-    for (int b0 = 0; b0 < PP; b0 += 32) {
-      const int b = b0 + lane;
-      cnt += __popc(__ballot_sync(FULL, b < PP && state_pauli_stab(row, NQ, b, nrm)));
+#pragma unroll
+    for (int z = 0; z < N; z++) {
+      // i^{|f & z|} W(z) = +-nrm  <=>  W(z) = +-i^{-|f & z|} nrm; i = w^2 turns (a, b, c, d) into (-c, -d, a, b)
+      Zw tg = nrm;
+      if (__popc(f & z) & 1) tg = Zw{tg.c, tg.d, -tg.a, -tg.b};                 // times -i (up to the sign)
+      cnt += zeq(w[z], tg) || zeq(w[z], Zw{-tg.a, -tg.b, -tg.c, -tg.d});
     }
-    int r = 0;
-    while ((2 << r) <= cnt) r++;
-    int d = (NQ - r) - sp.ginfo[j * (2 + sp.ncuts) + 1];
-    if (d < 0) d = -d;
-    if (d > best) best = d;
+#pragma unroll
+    for (int o = 1; o < N; o <<= 1) {
+      cnt += __shfl_xor_sync(FULL, cnt, o);
+      big = max(big, (int64_t)__shfl_xor_sync(FULL, (long long)big, o));
+    }
+    if (live && f == 0 && big < (1LL << 27)) {
+      const int r = 31 - __clz(cnt);                                                // cnt >= 1: the identity
+      best = max(best, abs((NQ - r) - sp.ginfo[j * W + 1]));
+    }
   }
-  return best;
+  return warp_imax(best);
 }
 
 // class key: the smallest (h1, h2) over the symmetry orbit of S; per orbit element a position-weighted sum of
@@ -936,7 +872,6 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
   const int kP = pm.k, TP = pm.T, c2P = pm.c2, hsP = (pm.hsn & 1) ? 2 : 0, ntP = (pm.hsn >> 1) & 7;
   const int suppP = __popc(ntP);
   const bool pre_ok = sp.standard && !sp.states && kP < INHERIT_KMAX;
-  unsigned tcache = 0;                       // per qubit: 1 + T bound of its odd-diagonal child (0: unknown)
   unsigned long long pend[3] = {0, 0, 0};    // per qubit: 1 + queue entry of its deferred odd-diagonal child
   // queue a deferred T evaluation: a second odd diagonal on the same qubit joins its sibling's entry
   auto defer = [&](int g, int k, int c2, int needs, int hs, int ntriv, int q0, bool tdiag) {
@@ -968,7 +903,6 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
     c.child++;
     const uint8_t fl = sp.gflags[g];
     const int gm = sp.gmask[g], nq = sp.gnq[g], q0 = sp.gq[g][0];
-    const int tc = (int)((tcache >> (8 * q0)) & 0xff) - 1;
     if (pre_ok) {
       // lower bounds on the child's bounds from the parent's: k drops by at most the gate's sqrt2 exponent;
       // H structure, T and CX bounds are unchanged by monomial-affine / Clifford / one-qubit gates; an odd
@@ -978,7 +912,7 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
       const int ik = sp.gik[g] > 0 ? sp.gik[g] : 0;
       int hlo = kP - ik;
       if ((fl & GF_MONAFF) && hsP > hlo) hlo = hsP;
-      const int tlo = (fl & GF_CLIFFORD) ? TP : ((fl & GF_TDIAG) ? (tc >= 0 ? tc : TP - 1) : 0);
+      const int tlo = (fl & GF_CLIFFORD) ? TP : ((fl & GF_TDIAG) ? TP - 1 : 0);
       const int clo = (fl & GF_ONEQ) ? c2P : ((fl & GF_RANK2) ? c2P - 1 : 0);
       const int slo = suppP - nq;
       if (combine(hlo > 0 ? hlo : 0, tlo > 0 ? tlo : 0, clo > 0 ? clo : 0, slo > 0 ? slo : 0) > rem) {
@@ -1017,12 +951,7 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
       if (k > rem) alive = false;
       else {
         if (inheritT) T = TP;
-        else if (cacheT && tc >= 0) T = tc;
-        else if (o.tq) { defer(g, k, 0, 0, 0, 0, q0, cacheT && (fl & GF_ONEQ) && k == kP); continue; }
-        else {
-          T = ptm_bound<NQ, ST>(C, k, lane); c.teval++;
-          if (cacheT) tcache |= (unsigned)(T + 1) << (8 * q0);
-        }
+        else { defer(g, k, 0, 0, 0, 0, q0, cacheT && (fl & GF_ONEQ) && k == kP); continue; }
         alive = k + (T + sp.tdiv - 1) / sp.tdiv <= rem;
       }
     } else if (need_b) {
@@ -1034,16 +963,11 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
       if (combine(h, 0, c2, supp) > rem) alive = false;
       else {
         if (inheritT) T = TP;
-        else if (cacheT && tc >= 0) T = tc;
-        else if (o.tq) {
+        else {
           // siblings share an entry only when every bound but support is the parent's (one-qubit monomial gates)
           const bool share = cacheT && (fl & GF_ONEQ) && (fl & GF_MONAFF) && k == kP;
           defer(g, k, c2, needs, hs, ch.ntriv, q0, share);
           continue;
-        }
-        else {
-          T = ptm_bound<NQ, ST>(C, k, lane); c.teval++;
-          if (cacheT) tcache |= (unsigned)(T + 1) << (8 * q0);
         }
         alive = combine(h, T, c2, supp) <= rem;
       }
