@@ -141,6 +141,8 @@ SIGNATURES = {
                                          C.c_char_p, C.c_size_t]),
     "cz_engine_stream": (C.c_void_p, [C.c_void_p]),
     "cz_int32_peak": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "cz_sort_pairs": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.c_int,
+                                C.POINTER(C.c_float)]),
     "cz_tcount_options_default": (None, [C.POINTER(TcOptions)]),
     "cz_tspec_check": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(C.c_int), C.c_char_p, C.c_size_t]),
     "cz_spec_generate": (C.c_int, [C.c_char_p, C.c_size_t, C.c_int, C.c_int, C.POINTER(C.c_char_p),
@@ -346,6 +348,14 @@ class Engine:
     def stream(self):
         """the cudaStream_t the engine launches on (an integer handle)"""
         return lib().cz_engine_stream(self._h)
+
+    def sort_pairs(self, keys_ptr, vals_ptr, n, lo=0, hi=64):
+        """the dedupe's radix sort on device buffers (u64 keys, u32 values), in place; returns device ms"""
+        ms = C.c_float()
+        rc = lib().cz_sort_pairs(self._h, C.c_void_p(keys_ptr), C.c_void_p(vals_ptr), n, lo, hi, C.byref(ms))
+        if rc:
+            raise RuntimeError(f"cz_sort_pairs failed: {rc}")
+        return ms.value
 
     def int32_peak(self):
         v = C.c_double()

@@ -333,6 +333,17 @@ int cz_eval_bounds_noalloc(const cz_spec *spec, int count, const int64_t *d_entr
 
 void *cz_engine_stream(cz_engine *engine) { return engine ? engine->e->stream() : nullptr; }
 
+int cz_sort_pairs(cz_engine *engine, uint64_t *d_keys, uint32_t *d_vals, size_t n, int lo, int hi, float *ms) {
+  if (!engine || (n && (!d_keys || !d_vals))) return CZ_ERR_USAGE;
+  if (n < 2) { if (ms) *ms = 0; return 0; }
+  std::string err;
+  try {
+    return engine->e->sort_pairs(d_keys, d_vals, n, lo, hi, ms, err);
+  } catch (const std::exception &) {
+    return CZ_ERR_CUDA;
+  }
+}
+
 int cz_int32_peak(cz_engine *engine, double *ops_per_s) {
   if (!engine || !ops_per_s) return CZ_ERR_USAGE;
   try {

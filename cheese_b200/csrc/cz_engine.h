@@ -91,6 +91,10 @@ class Engine {
   // sustained int32 multiply-add throughput of this device (ops/s, a multiply-add counted as 2), measured by a
   // register-resident IMAD loop timed with CUDA events
   double int32_peak();
+  // sorts n (key, value) pairs held in device memory by bits [lo, hi) of the key (stable radix sort of the dedupe,
+  // in place, on the engine's stream; synchronises); the sort's device time in ms into *ms; returns 0, RC_USAGE (a
+  // bit range that is not whole bytes) or RC_CUDA
+  int sort_pairs(uint64_t *keys, uint32_t *vals, size_t n, int lo, int hi, float *ms, std::string &err);
   int device() const { return dev_; }
   // release the cached work buffers (frontiers, survivor records, sort scratch, tree); resident distance tables and
   // spec tables stay; returns the bytes released

@@ -50,6 +50,7 @@ struct DevSpec {
   int n, G, depth, standard, lite, tdiv, ncuts, have_table, nsym, nogoal, gk, ncx;
   int cutmask[CUTMAX], cutsize[CUTMAX], rad[CUTMAX];
   uint64_t w1, w2, w3;                 // w, w^2, w^3 mod p with w = 3^((p-1)/8)
+  uint32_t wm[3];                      // w, w^2, w^3 times 2^32 mod p (the CX bound's Montgomery form)
   uint8_t symperm[SYMMAX][8];
   uint8_t symconj[SYMMAX];
   uint8_t gflags[GMAX];
@@ -78,6 +79,7 @@ struct DevStats {
   unsigned int ovf, surv_overflow;
   unsigned long long n_work, n_kept;
   unsigned long long n_tq, tq_work;   // deferred T evaluations: queued, taken
+  unsigned int sort_err, pad;         // a dedupe sort's look-back gave up (its result is not used)
 };
 
 // A T-bound evaluation deferred from the level kernel to k_tbound: the parent, up to two children that share one
@@ -142,21 +144,6 @@ __device__ __forceinline__ uint64_t fmix64(uint64_t h) {
   h ^= h >> 33; h *= 0xff51afd7ed558ccdULL; h ^= h >> 33; h *= 0xc4ceb9fe1a85ec53ULL; h ^= h >> 33;
   return h;
 }
-__device__ __forceinline__ uint64_t tomodp(int64_t v) {
-  int64_t m = v % (int64_t)PRIME;
-  return (uint64_t)(m < 0 ? m + (int64_t)PRIME : m);
-}
-template <typename ST> __device__ __forceinline__ uint32_t zmodp(const Z4<ST> &x, const DevSpec &sp) {
-  if (sizeof(ST) == 4) {   // |limb| <= 2^31, w^i < 2^30: the whole sum fits in int64, one reduction
-    const int64_t t = (int64_t)x.a + (int64_t)x.b * (int64_t)sp.w1 + (int64_t)x.c * (int64_t)sp.w2 +
-                      (int64_t)x.d * (int64_t)sp.w3;
-    int64_t m = t % (int64_t)PRIME;
-    return (uint32_t)(m < 0 ? m + (int64_t)PRIME : m);
-  }
-  const uint64_t r = tomodp(x.a) + tomodp(x.b) * sp.w1 % PRIME + tomodp(x.c) * sp.w2 % PRIME + tomodp(x.d) * sp.w3 % PRIME;
-  return (uint32_t)(r % PRIME);
-}
-
 // ---------------- per-warp bound evaluations (child residual S in shared memory) ----------------
 
 // ---- T bound: max(0, max over the nonzero PTM entries of their sde) (cheese.cu:397-449) ----
@@ -183,46 +170,56 @@ template <typename U> __device__ __forceinline__ U pair_component(int comp, cons
     default: return (y.a - y.c) * x.b + (y.b - y.d) * x.c + (y.a + y.c) * x.d - (y.b + y.d) * x.a;
   }
 }
-template <int NQ, typename U, int PASSES, typename ST>
-__device__ __forceinline__ int tbound_lanes(const Z4<ST> *S, int k, int lane) {
+// the pairs of one round: f (f = 0 skipped) with point map e(i) = insert a 0 at bit j of i, or (IDENT: every f of
+// the round has the top bit) e(i) = i, known at compile time
+template <int NQ, typename U, int PASSES, bool IDENT, typename ST>
+__device__ __forceinline__ void tbound_round(const Z4<ST> *S, int f, U &P, U &Q) {
   constexpr int E = 1 << (2 * NQ), HP = E / 2, CPP = 4 / PASSES;
   static_assert(4 % PASSES == 0, "passes split the four components evenly");
-  U P = 0, Q = 0;
+  if (f == 0) return;
+  const int lomask = IDENT ? E - 1 : ((f & HP) ? E - 1 : (f & -f) - 1);   // bits below the inserted 0
 #pragma unroll 1
-  for (int f = lane; f < E; f += 32) {
-    if (f == 0) continue;
-    const int lomask = (f & HP) ? E - 1 : (f & -f) - 1;   // bits below the inserted 0 (all of them: none inserted)
-#pragma unroll 1
-    for (int pass = 0; pass < PASSES; pass++) {
-      U v[CPP][HP];
+  for (int pass = 0; pass < PASSES; pass++) {
+    U v[CPP][HP];
 #pragma unroll
-      for (int i = 0; i < HP; i++) {
-        const int e = (i & lomask) | ((i & ~lomask) << 1);
-        const Z4<U> y = toU<U>(S[e]), x = toU<U>(S[e ^ f]);
+    for (int i = 0; i < HP; i++) {
+      const int e = IDENT ? i : (i & lomask) | ((i & ~lomask) << 1);
+      const Z4<U> y = toU<U>(S[e]), x = toU<U>(S[e ^ f]);
 #pragma unroll
-        for (int c = 0; c < CPP; c++) v[c][i] = pair_component<U>(pass * CPP + c, x, y);
-      }
-#pragma unroll
-      for (int h = 1; h < HP; h <<= 1)
-#pragma unroll
-        for (int i = 0; i < HP; i++)
-          if (!(i & h)) {
-#pragma unroll
-            for (int c = 0; c < CPP; c++) {
-              const U u = v[c][i], w = v[c][i | h];
-              v[c][i] = u + w;
-              v[c][i | h] = u - w;
-            }
-          }
-#pragma unroll
-      for (int c = 0; c < CPP; c++) {
-        U o = 0;
-#pragma unroll
-        for (int i = 0; i < HP; i++) o |= v[c][i];
-        if (pass * CPP + c < 2) P |= o;
-        else Q |= o;
-      }
+      for (int c = 0; c < CPP; c++) v[c][i] = pair_component<U>(pass * CPP + c, x, y);
     }
+#pragma unroll
+    for (int h = 1; h < HP; h <<= 1)
+#pragma unroll
+      for (int i = 0; i < HP; i++)
+        if (!(i & h)) {
+#pragma unroll
+          for (int c = 0; c < CPP; c++) {
+            const U u = v[c][i], w = v[c][i | h];
+            v[c][i] = u + w;
+            v[c][i | h] = u - w;
+          }
+        }
+#pragma unroll
+    for (int c = 0; c < CPP; c++) {
+      U o = 0;
+#pragma unroll
+      for (int i = 0; i < HP; i++) o |= v[c][i];
+      if (pass * CPP + c < 2) P |= o;
+      else Q |= o;
+    }
+  }
+}
+template <int NQ, typename U, int PASSES, typename ST, bool SPLIT = true>
+__device__ __forceinline__ int tbound_lanes(const Z4<ST> *S, int k, int lane) {
+  constexpr int E = 1 << (2 * NQ);
+  U P = 0, Q = 0;
+  if constexpr (E == 64 && SPLIT) {        // round 0: f = lane (insert map), round 1: f = 32 + lane (top bit)
+    tbound_round<NQ, U, PASSES, false>(S, lane, P, Q);
+    tbound_round<NQ, U, PASSES, true>(S, 32 + lane, P, Q);
+  } else {
+#pragma unroll 1
+    for (int f = lane; f < E; f += 32) tbound_round<NQ, U, PASSES, false>(S, f, P, Q);
   }
   // f = 0: alpha = |y|^2 real part, beta its sqrt2 part, transformed over all E points across the warp
   constexpr int PL = E > 32 ? E / 32 : 1;   // points per lane
@@ -278,70 +275,103 @@ template <int NQ, typename ST> __device__ __forceinline__ int ptm_bound(const Z4
   return 2 * (NQ + k) > 64 ? warp_tbound64<NQ, ST>(S, k, lane) : warp_tbound32<NQ, ST>(S, k, lane);
 }
 
-// rank over F_p of the operator-Schmidt matrix across cut A (cheese.cu:271-303): lane j owns column j, fraction-free
-// elimination row by row (the rank does not depend on the order of elimination)
-template <int NQ, typename ST> __device__ int warp_cut_rank(const Z4<ST> *S, int A, int sa, const DevSpec &sp, int lane) {
-  constexpr int N = 1 << NQ, E = N * N;
-  const int na = sa, nb = NQ - sa, R = 1 << (2 * sa), Cc = E / R;
-  const bool act = lane < Cc;
-  const int ob = lane >> nb, ib = lane & ((1 << nb) - 1);
-  uint32_t v[4];
-#pragma unroll
-  for (int rr = 0; rr < 4; rr++) {
-    v[rr] = 0;
-    if (rr < R && act) {
-      const int oa = rr >> na, ia = rr & ((1 << na) - 1);
-      int o = 0, i = 0, xa = 0, xb = 0;
-#pragma unroll
-      for (int q = 0; q < NQ; q++) {
-        if ((A >> q) & 1) { o |= ((oa >> xa) & 1) << q; i |= ((ia >> xa) & 1) << q; xa++; }
-        else { o |= ((ob >> xb) & 1) << q; i |= ((ib >> xb) & 1) << q; xb++; }
-      }
-      v[rr] = zmodp(S[o * N + i], sp);
-    }
-  }
-  int rank = 0;
-#pragma unroll
-  for (int rr = 0; rr < 4; rr++) {
-    if (rr >= R) break;
-    const unsigned bal = __ballot_sync(FULL, act && v[rr] != 0);
-    if (!bal) continue;
-    const int piv = __ffs((int)bal) - 1;
-    const uint64_t a = __shfl_sync(FULL, v[rr], piv);
-#pragma unroll
-    for (int r2 = rr + 1; r2 < 4; r2++) {
-      if (r2 >= R) break;
-      const uint64_t b = __shfl_sync(FULL, v[r2], piv);
-      v[r2] = (uint32_t)((a * v[r2] + (PRIME - b) * (uint64_t)v[rr]) % PRIME);
-    }
-    rank++;
-  }
-  return rank;
+// ---- CX bound (cheese.cu:257-303, 585-597): F_p ranks of the operator-Schmidt matrices across the cuts ----
+// F_p arithmetic in Montgomery form with R = 2^32: mont(x, y) = x y / R mod p. A rank only depends on which
+// elimination results are zero, and every Montgomery product carries the same factor 1 / R, so the elimination
+// v2 <- mont(a, v2) - mont(b, v1) = (a v2 - b v1) / R keeps every rank of the reference's a v2 - b v1.
+constexpr uint32_t inv_mod_2_32(uint32_t p) {      // p^-1 mod 2^32 by Newton's iteration (p odd)
+  uint32_t x = p;
+  for (int i = 0; i < 5; i++) x *= 2u - p * x;
+  return x;
 }
-
-// CX bound from the per-cut needs ceil(log2 rank) (cheese.cu:585-597). Cuts a gate does not cross keep their
+constexpr uint32_t PRIME_NINV = 0u - inv_mod_2_32(PRIME);
+static_assert(PRIME * inv_mod_2_32(PRIME) == 1u, "Montgomery inverse");
+__device__ __forceinline__ uint32_t mont(uint32_t x, uint32_t y) {   // x, y < p
+  const uint64_t t = (uint64_t)x * y;
+  const uint32_t m = (uint32_t)t * PRIME_NINV;
+  const uint32_t u = (uint32_t)((t + (uint64_t)m * PRIME) >> 32);
+  return u >= PRIME ? u - PRIME : u;
+}
+__device__ __forceinline__ uint32_t addp(uint32_t x, uint32_t y) { const uint32_t s = x + y; return s >= PRIME ? s - PRIME : s; }
+__device__ __forceinline__ uint32_t subp(uint32_t x, uint32_t y) { return x >= y ? x - y : x + PRIME - y; }
+template <typename ST> __device__ __forceinline__ uint32_t limb_modp(ST a) {
+  const ST r = a % (ST)PRIME;
+  return (uint32_t)(r < 0 ? r + (ST)PRIME : r);
+}
+// x = a + b w + c w^2 + d w^3 mapped to F_p (w -> a primitive 8th root of unity mod p), in normal form:
+// mont(b mod p, w R mod p) = b w mod p
+template <typename ST> __device__ __forceinline__ uint32_t to_fp(const Z4<ST> &x, const DevSpec &sp) {
+  return addp(addp(limb_modp(x.a), mont(limb_modp(x.b), sp.wm[0])),
+              addp(mont(limb_modp(x.c), sp.wm[1]), mont(limb_modp(x.d), sp.wm[2])));
+}
+// The bound from the per-cut needs ceil(log2 rank) through the CX table. Cuts a gate does not cross keep their
 // parent's need (a gate inside one side is a local map); needs_in = the parent's packed needs, gmask = the gate's
-// qubits (0: recompute every cut). Returns the bound, packs the child's needs into needs_out.
+// qubits (0: every cut recomputed). Every cut has one qubit (at most 3 qubits), so its matrix is 4 x E/4: rows
+// (output bit, input bit) of the cut qubit, columns those of the other qubits. The matrices of 32 / (E/4) cuts are
+// eliminated side by side, one column per lane: per row a ballot finds the group's pivot column, and the rows
+// below are reduced by it. Returns the bound and packs the child's needs (2 bits per cut) into needs_out.
 template <int NQ, typename ST>
 __device__ __noinline__ int warp_cx_bound(const Z4<ST> *S, const DevSpec &sp, int lane, int gmask, int needs_in,
                                           int &needs_out) {
-  constexpr int ALLQ = (1 << NQ) - 1;
-  int idx = 0, mult = 1, mx = 0, packed = 0;
+  constexpr int N = 1 << NQ, CC = N * N / 4 > 0 ? N * N / 4 : 1, SLOTS = 32 / CC, ALLQ = N - 1;
+  static_assert(NQ <= 3, "cuts of one qubit: 4 x E/4 matrices within a warp");
   const bool inherit = sp.ncuts <= 4 && gmask;
+  unsigned todo = 0;
+  for (int i = 0; i < sp.ncuts; i++) {
+    const int A = sp.cutmask[i];
+    if (!(inherit && (!(gmask & A) || !(gmask & ~A & ALLQ)))) todo |= 1u << i;
+  }
+  uint64_t fresh = 0;                        // 3 bits per recomputed cut: its need
+  const int slot = lane / CC, col = lane % CC;
+  while (todo) {
+    int mycut = -1;
+    for (int s2 = 0; s2 < SLOTS; s2++) {      // the group's cuts: the lowest SLOTS cuts still to do
+      const int c = todo ? __ffs(todo) - 1 : -1;
+      if (s2 == slot) mycut = c;
+      todo &= todo - 1;
+    }
+    const int A = mycut >= 0 ? sp.cutmask[mycut] : 0;
+    uint32_t v[4];
+#pragma unroll
+    for (int rr = 0; rr < 4; rr++) {
+      int o = 0, i = 0, nb = 0;
+#pragma unroll
+      for (int q = 0; q < NQ; q++) {
+        if ((A >> q) & 1) { o |= ((rr >> 1) & 1) << q; i |= (rr & 1) << q; }
+        else { o |= ((col >> (NQ - 1 + nb)) & 1) << q; i |= ((col >> nb) & 1) << q; nb++; }
+      }
+      v[rr] = mycut >= 0 ? to_fp(S[o * N + i], sp) : 0u;
+    }
+    const unsigned group = (CC >= 32 ? FULL : ((1u << CC) - 1u)) << (slot * CC);
+    int rank = 0;
+#pragma unroll
+    for (int rr = 0; rr < 4; rr++) {
+      const unsigned bal = __ballot_sync(FULL, v[rr] != 0) & group;
+      const int piv = bal ? __ffs(bal) - 1 : lane;
+      const uint32_t a = __shfl_sync(FULL, v[rr], piv);
+#pragma unroll
+      for (int r2 = rr + 1; r2 < 4; r2++) {
+        const uint32_t b = __shfl_sync(FULL, v[r2], piv);
+        if (bal) v[r2] = subp(mont(a, v[r2]), mont(b, v[rr]));
+      }
+      rank += bal != 0;
+    }
+    const int need = rank <= 1 ? 0 : (rank == 2 ? 1 : 2);
+    for (int s2 = 0; s2 < SLOTS; s2++) {
+      const int c = __shfl_sync(FULL, mycut, s2 * CC), nd = __shfl_sync(FULL, need, s2 * CC);
+      if (c >= 0) fresh |= (uint64_t)nd << (3 * c);
+    }
+  }
+  int idx = 0, mult = 1, mx = 0, packed = 0;
   for (int i = 0; i < sp.ncuts; i++) {
     const int A = sp.cutmask[i];
     int need;
     if (inherit && (!(gmask & A) || !(gmask & ~A & ALLQ))) need = (needs_in >> (2 * i)) & 3;
-    else {
-      const int rk = warp_cut_rank<NQ, ST>(S, A, sp.cutsize[i], sp, lane);
-      need = 0;
-      while ((1 << need) < rk) need++;
-      if (need > sp.rad[i] - 1) need = sp.rad[i] - 1;
-    }
+    else need = min((int)((fresh >> (3 * i)) & 7), sp.rad[i] - 1);
     if (i < 4) packed |= (need & 3) << (2 * i);
     idx += need * mult;
     mult *= sp.rad[i];
-    if (need > mx) mx = need;
+    mx = max(mx, need);
   }
   needs_out = packed;
   return sp.have_table && idx < sp.ncx ? __ldg(&sp.cxtable[idx]) : mx;
@@ -739,90 +769,101 @@ template <int NQ, typename ST> __device__ __noinline__ int warp_state_t(const Z4
   return warp_imax(best);
 }
 
-// class key: the smallest (h1, h2) over the symmetry orbit of S; per orbit element a position-weighted sum of
-// per-entry hashes (the key only has to be class-invariant: classes are always compared exactly)
+// class key: the smallest key over the symmetry orbit of S (qubit relabellings, with conjugation for some), so
+// every member of a class gets the same key; classes are always compared exactly, so the key only has to be
+// class-invariant, and a collision costs an exact comparison, never a wrong answer.
+// Per orbit element two 32-bit position-weighted sums of per-entry 32-bit hashes, sum_e h(S[e]) W[pi(e)] mod 2^32
+// (A and B: independent hashes and weights), form a 64-bit value, finalised with the exponent k. Each lane adds its
+// entries' terms for every element (hash of the entry or of its conjugate, by the element's conjugation); a
+// reduce-scatter over the 32 (element, A/B) sums then leaves lane s with A_s and lane 16 + s with B_s, and the
+// minimum over the elements is taken across lanes. W[pos] packs (weight A, weight B); perm[s][x] is the image of
+// basis index x under element s.
+__device__ __forceinline__ uint32_t fmix32(uint32_t h) {
+  h ^= h >> 16; h *= 0x85ebca6bu; h ^= h >> 13; h *= 0xc2b2ae35u; h ^= h >> 16;
+  return h;
+}
+template <typename ST> __device__ __forceinline__ void entry_hash(const Z4<ST> &x, uint32_t &ha, uint32_t &hb) {
+  // the limbs as 64-bit values (so int32 and int64 storage of one residual hash alike): low and high words
+  const uint64_t a = (uint64_t)(int64_t)x.a, b = (uint64_t)(int64_t)x.b, c = (uint64_t)(int64_t)x.c,
+                 d = (uint64_t)(int64_t)x.d;
+  const uint32_t lo0 = (uint32_t)a * 0x9e3779b1u + (uint32_t)b * 0x85ebca77u + (uint32_t)c * 0xc2b2ae3du +
+                       (uint32_t)d * 0x27d4eb2fu;
+  const uint32_t lo1 = (uint32_t)a * 0x165667b1u + (uint32_t)b * 0xd3a2646cu + (uint32_t)c * 0xfd7046c5u +
+                       (uint32_t)d * 0xb55a4f09u;
+  const uint32_t hi = (uint32_t)(a >> 32) * 0x61c88647u + (uint32_t)(b >> 32) * 0x7a646e4du +
+                      (uint32_t)(c >> 32) * 0x3c6ef372u + (uint32_t)(d >> 32) * 0x5bd1e995u;
+  ha = fmix32(lo0 ^ hi);
+  hb = fmix32(lo1 + (hi ^ 0x1b873593u));
+}
 template <int NQ, typename ST>
 __device__ __noinline__ void warp_class_key(const Z4<ST> *S, int k, int nsym, unsigned conjmask, const uint8_t (*perm)[8],
-                               const uint64_t *W1, const uint64_t *W2, int lane, uint64_t &k1, uint64_t &k2) {
+                                            const uint64_t *W, int lane, uint64_t &k1, uint64_t &k2) {
   constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
-  uint64_t f1[EPL], f2[EPL], c1[EPL], c2[EPL];
+  static_assert(SYMMAX <= 16, "the reduce-scatter holds 16 elements x (A, B)");
+  uint32_t fa[EPL], fb[EPL], ca[EPL], cb[EPL];
+  int row[EPL], col[EPL];
 #pragma unroll
   for (int j = 0; j < EPL; j++) {
     const int e = lane + 32 * j;
-    f1[j] = f2[j] = c1[j] = c2[j] = 0;
+    fa[j] = fb[j] = ca[j] = cb[j] = 0;
+    row[j] = (e >> NQ) & (N - 1);
+    col[j] = e & (N - 1);
     if (e >= E) continue;
     const Z4<ST> x = S[e];
-    uint64_t h = fmix64((uint64_t)(int64_t)x.a * 0x9e3779b97f4a7c15ULL + (uint64_t)(int64_t)x.b);
-    h = fmix64(h ^ ((uint64_t)(int64_t)x.c * 0xc2b2ae3d27d4eb4fULL + (uint64_t)(int64_t)x.d));
-    f1[j] = h; f2[j] = fmix64(h + 0x632be59bd9b4e019ULL);
-    const Z4<ST> y = zcj(x);
-    h = fmix64((uint64_t)(int64_t)y.a * 0x9e3779b97f4a7c15ULL + (uint64_t)(int64_t)y.b);
-    h = fmix64(h ^ ((uint64_t)(int64_t)y.c * 0xc2b2ae3d27d4eb4fULL + (uint64_t)(int64_t)y.d));
-    c1[j] = h; c2[j] = fmix64(h + 0x632be59bd9b4e019ULL);
+    entry_hash(x, fa[j], fb[j]);
+    entry_hash(zcj(x), ca[j], cb[j]);
   }
-  // the symmetries four at a time: per lane, the partial sums of the four images; then a reduce-scatter across the
-  // warp (lane bit 4 halves the four symmetries, bit 3 halves again, bits 2..0 finish the sums), so each lane ends
-  // with the full sums of one symmetry and finalises only that one; the minimum over lanes and groups is the key.
-  // The sums are the same sums mod 2^64 as one symmetry at a time, so the keys are the same.
-  uint64_t b1 = ~0ULL, b2 = ~0ULL;
-  const int hb = (lane >> 4) & 1, hc = (lane >> 3) & 1;
-  for (int g0 = 0; g0 < nsym; g0 += 4) {
-    uint64_t A[4], B[4];
+  uint32_t v[32];
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-      A[i] = 0; B[i] = 0;
-      const int s = g0 + i;
-      if (s >= nsym) continue;
-      const bool cj = (conjmask >> s) & 1;
+  for (int s = 0; s < 16; s++) {
+    v[s] = v[16 + s] = 0;
+    if (s >= nsym) continue;
+    const bool cj = (conjmask >> s) & 1;
 #pragma unroll
-      for (int j = 0; j < EPL; j++) {
-        const int e = lane + 32 * j;
-        if (e >= E) continue;
-        const int pos = perm[s][e >> NQ] * N + perm[s][e & (N - 1)];
-        A[i] += (cj ? c1[j] : f1[j]) * W1[pos];
-        B[i] += (cj ? c2[j] : f2[j]) * W2[pos];
-      }
+    for (int j = 0; j < EPL; j++) {
+      if (lane + 32 * j >= E) continue;
+      const uint64_t w = W[perm[s][row[j]] * N + perm[s][col[j]]];
+      v[s] += (cj ? ca[j] : fa[j]) * (uint32_t)w;
+      v[16 + s] += (cj ? cb[j] : fb[j]) * (uint32_t)(w >> 32);
     }
-    uint64_t A2[2], B2[2];
-#pragma unroll
-    for (int i = 0; i < 2; i++) {              // lanes with bit 4 clear keep symmetries 0, 1; the others 2, 3
-      const uint64_t sa = hb ? A[i] : A[i + 2], sb = hb ? B[i] : B[i + 2];
-      A2[i] = (hb ? A[i + 2] : A[i]) + __shfl_xor_sync(FULL, sa, 16);
-      B2[i] = (hb ? B[i + 2] : B[i]) + __shfl_xor_sync(FULL, sb, 16);
-    }
-    uint64_t a = (hc ? A2[1] : A2[0]) + __shfl_xor_sync(FULL, hc ? A2[0] : A2[1], 8);
-    uint64_t b = (hc ? B2[1] : B2[0]) + __shfl_xor_sync(FULL, hc ? B2[0] : B2[1], 8);
-#pragma unroll
-    for (int m = 4; m; m >>= 1) { a += __shfl_xor_sync(FULL, a, m); b += __shfl_xor_sync(FULL, b, m); }
-    const int s = g0 + 2 * hb + hc;             // the symmetry this lane now holds
-    uint64_t x1 = ~0ULL, x2 = ~0ULL;
-    if (s < nsym) {
-      x1 = fmix64(a + (uint64_t)k * 0xa0761d6478bd642fULL);
-      x2 = fmix64(b ^ ((uint64_t)k * 0xe7037ed1a0b428dbULL + 0x8ebc6af09c88c6e3ULL));
-    }
-#pragma unroll
-    for (int m = 16; m >= 8; m >>= 1) {
-      const uint64_t o1 = __shfl_xor_sync(FULL, x1, m), o2 = __shfl_xor_sync(FULL, x2, m);
-      if (o1 < x1 || (o1 == x1 && o2 < x2)) { x1 = o1; x2 = o2; }
-    }
-    if (x1 < b1 || (x1 == b1 && x2 < b2)) { b1 = x1; b2 = x2; }
   }
-  k1 = b1; k2 = b2;
+  // reduce-scatter: at offset o a lane keeps the half of its values on its side of lane bit o and adds the
+  // partner's copy of that half
+#pragma unroll
+  for (int o = 16, n = 16; o; o >>= 1, n >>= 1) {
+    const bool up = lane & o;
+#pragma unroll
+    for (int i = 0; i < n; i++) {
+      const uint32_t keep = up ? v[n + i] : v[i], give = up ? v[i] : v[n + i];
+      v[i] = keep + __shfl_xor_sync(FULL, give, o);
+    }
+  }
+  const uint32_t other = __shfl_xor_sync(FULL, v[0], 16);   // lane s < 16: A_s here, B_s from lane 16 + s
+  uint64_t x1 = ~0ULL, x2 = ~0ULL;
+  if (lane < nsym) {
+    x1 = fmix64((((uint64_t)v[0] << 32) | other) + (uint64_t)k * 0xa0761d6478bd642fULL);
+    x2 = fmix64(x1 ^ 0xe7037ed1a0b428dbULL);
+  }
+#pragma unroll
+  for (int m = 16; m; m >>= 1) {
+    const uint64_t o1 = __shfl_xor_sync(FULL, x1, m), o2 = __shfl_xor_sync(FULL, x2, m);
+    if (o1 < x1 || (o1 == x1 && o2 < x2)) { x1 = o1; x2 = o2; }
+  }
+  k1 = x1; k2 = x2;
 }
 
 template <int NQ, typename ST> struct ExpandSmem {
   static constexpr int E = (1 << NQ) * (1 << NQ);
   Z4<ST> P[EXP_WARPS][E];
   Z4<ST> C[EXP_WARPS][E];
-  uint64_t W1[E], W2[E];
+  uint64_t W[E];
   uint8_t perm[SYMMAX][8];
 };
 
-__device__ __forceinline__ void init_weights(uint64_t *W1, uint64_t *W2, int E) {
-  for (int i = threadIdx.x; i < E; i += blockDim.x) {
-    W1[i] = fmix64(0x243f6a8885a308d3ULL + (uint64_t)i * 0x13198a2e03707345ULL) | 1;
-    W2[i] = fmix64(0xa4093822299f31d0ULL + (uint64_t)i * 0x082efa98ec4e6c89ULL) | 1;
-  }
+// the class key's position weights: (weight A, weight B), both odd
+__device__ __forceinline__ void init_weights(uint64_t *W, int E) {
+  for (int i = threadIdx.x; i < E; i += blockDim.x)
+    W[i] = fmix64(0x243f6a8885a308d3ULL + (uint64_t)i * 0x13198a2e03707345ULL) | 0x0000000100000001ULL;
 }
 
 // ---------------- the level kernel ----------------
@@ -862,7 +903,7 @@ template <typename ST> struct ExpandOut {
 // the out-of-line helpers; child index = p * GS + g.
 template <int NQ, typename ST, bool STATES = false>
 __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *sps, const uint8_t (*perm)[8],
-                                              unsigned conjmask, const uint64_t *W1, const uint64_t *W2,
+                                              unsigned conjmask, const uint64_t *W,
                                               const Z4<ST> *P, Z4<ST> *C, unsigned long long p, const NodeMeta pm,
                                               int rem, bool keep, int GS, const ExpandOut<ST> &o, WarpTally &c,
                                               int lane) {
@@ -894,32 +935,44 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
     }
     if (tdiag) pend[q0] = e + 1;
   };
-  for (int g = 0; g < G; g++) {
-    if (g1 >= 0 && __ldg(&sp.bad2[g1 * G + g])) { c.w2++; continue; }
-    if (g2 >= 0) {
-      const uint32_t tri = ((uint32_t)g2 * G + (uint32_t)g1) * G + (uint32_t)g;
-      if ((__ldg(&sp.bad3[tri >> 5]) >> (tri & 31)) & 1) { c.w3++; continue; }
-    }
-    c.child++;
-    const uint8_t fl = sp.gflags[g];
-    const int gm = sp.gmask[g], nq = sp.gnq[g], q0 = sp.gq[g][0];
-    if (pre_ok) {
-      // lower bounds on the child's bounds from the parent's: k drops by at most the gate's sqrt2 exponent;
-      // H structure, T and CX bounds are unchanged by monomial-affine / Clifford / one-qubit gates; an odd
-      // diagonal changes T by at most 1; a gate of Schmidt rank 2 changes the CX bound by at most 1; support
-      // changes only on the gate's qubits. combine is monotone in every argument, so exceeding the budget with
-      // these proves the child dead (the goal has all bounds 0 and is never removed here).
-      const int ik = sp.gik[g] > 0 ? sp.gik[g] : 0;
-      int hlo = kP - ik;
-      if ((fl & GF_MONAFF) && hsP > hlo) hlo = hsP;
-      const int tlo = (fl & GF_CLIFFORD) ? TP : ((fl & GF_TDIAG) ? TP - 1 : 0);
-      const int clo = (fl & GF_ONEQ) ? c2P : ((fl & GF_RANK2) ? c2P - 1 : 0);
-      const int slo = suppP - nq;
-      if (combine(hlo > 0 ? hlo : 0, tlo > 0 ? tlo : 0, clo > 0 ? clo : 0, slo > 0 ? slo : 0) > rem) {
-        c.dead++;
-        continue;
+  // the fates decided without the child's residual, one candidate per lane: window cuts (W2, W3) and the exact
+  // prechecks. Lower bounds on the child's bounds from the parent's: k drops by at most the gate's sqrt2 exponent;
+  // H structure, T and CX bounds are unchanged by monomial-affine / Clifford / one-qubit gates; an odd diagonal
+  // changes T by at most 1; a gate of Schmidt rank 2 changes the CX bound by at most 1; support changes only on
+  // the gate's qubits. combine is monotone in every argument, so exceeding the budget with these proves the child
+  // dead (the goal has all bounds 0 and is never removed here). The other children are evaluated in order.
+  unsigned long long full = 0;
+  for (int g0 = 0; g0 < G; g0 += 32) {
+    const int g = g0 + lane;
+    int fate = 0;                            // 0: no candidate, 1: W2 cut, 2: W3 cut, 3: dead by precheck, 4: full
+    if (g < G) {
+      fate = 4;
+      if (g1 >= 0 && __ldg(&sp.bad2[g1 * G + g])) fate = 1;
+      else if (g2 >= 0) {
+        const uint32_t tri = ((uint32_t)g2 * G + (uint32_t)g1) * G + (uint32_t)g;
+        if ((__ldg(&sp.bad3[tri >> 5]) >> (tri & 31)) & 1) fate = 2;
+      }
+      if (fate == 4 && pre_ok) {
+        const uint8_t fl = sps->gflags[g];
+        const int ik = sps->gik[g] > 0 ? sps->gik[g] : 0;
+        int hlo = kP - ik;
+        if ((fl & GF_MONAFF) && hsP > hlo) hlo = hsP;
+        const int tlo = (fl & GF_CLIFFORD) ? TP : ((fl & GF_TDIAG) ? TP - 1 : 0);
+        const int clo = (fl & GF_ONEQ) ? c2P : ((fl & GF_RANK2) ? c2P - 1 : 0);
+        const int slo = suppP - sps->gnq[g];
+        if (combine(max(hlo, 0), max(tlo, 0), max(clo, 0), max(slo, 0)) > rem) fate = 3;
       }
     }
+    c.w2 += __popc(__ballot_sync(FULL, fate == 1));
+    c.w3 += __popc(__ballot_sync(FULL, fate == 2));
+    c.child += __popc(__ballot_sync(FULL, fate >= 3));
+    c.dead += __popc(__ballot_sync(FULL, fate == 3));
+    full |= (unsigned long long)__ballot_sync(FULL, fate == 4) << g0;
+  }
+  for (; full; full &= full - 1) {
+    const int g = __ffsll((long long)full) - 1;
+    const uint8_t fl = sp.gflags[g];
+    const int gm = sp.gmask[g], q0 = sp.gq[g][0];
     bool ovf;
     c.full++;
     const int k = warp_child<NQ, ST>(P, C, g, kP, sp, sps, lane, ovf);
@@ -976,7 +1029,7 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
     c.alive++;
     if (!keep) continue;
     uint64_t k1, k2;
-    warp_class_key<NQ, ST>(C, k, sp.nsym, conjmask, perm, W1, W2, lane, k1, k2);
+    warp_class_key<NQ, ST>(C, k, sp.nsym, conjmask, perm, W, lane, k1, k2);
     unsigned long long slot = 0;
     if (lane == 0) slot = atomicAdd(&o.st->n_surv, 1ULL);
     slot = __shfl_sync(FULL, slot, 0);
@@ -1063,7 +1116,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, 
   __shared__ ExpandSmem<NQ, ST> sm;
   __shared__ DevSpec s_sp;                     // the spec for out-of-line helpers (a shared address, no local copy)
   for (int i = threadIdx.x; i < (int)(sizeof(DevSpec) / 4); i += blockDim.x) ((int *)&s_sp)[i] = ((const int *)&sp)[i];
-  init_weights(sm.W1, sm.W2, E);
+  init_weights(sm.W, E);
   for (int i = threadIdx.x; i < SYMMAX * 8; i += blockDim.x) sm.perm[i / 8][i % 8] = sp.symperm[i / 8][i % 8];
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1084,7 +1137,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, 
     }
     const NodeMeta pm = a.meta[p];
     __syncwarp();
-    expand_parent<NQ, ST, STATES>(sp, &s_sp, sm.perm, conjmask, sm.W1, sm.W2, P, C, p, pm, a.rem, a.keep != 0, sp.G, o, c,
+    expand_parent<NQ, ST, STATES>(sp, &s_sp, sm.perm, conjmask, sm.W, P, C, p, pm, a.rem, a.keep != 0, sp.G, o, c,
                           lane);
     __syncwarp();
   }
@@ -1186,9 +1239,9 @@ template <int NQ, typename ST>
 __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand_batch(const BatchArgs<ST> a) {
   constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
   __shared__ Z4<ST> sP[EXP_WARPS][E], sC[EXP_WARPS][E];
-  __shared__ uint64_t W1[E], W2[E];
+  __shared__ uint64_t W[E];
   __shared__ DevSpec sps[EXP_WARPS];           // each warp's current job spec
-  init_weights(W1, W2, E);
+  init_weights(W, E);
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   Z4<ST> *P = sP[w], *C = sC[w];
@@ -1227,7 +1280,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand_batch(const BatchA
     }
     const NodeMeta pm = a.meta[p];
     __syncwarp();
-    expand_parent<NQ, ST>(sp, &sp, sp.symperm, conjmask, W1, W2, P, C, p, pm, rem, keep, BATCH_GS, o, c, lane);
+    expand_parent<NQ, ST>(sp, &sp, sp.symperm, conjmask, W, P, C, p, pm, rem, keep, BATCH_GS, o, c, lane);
     __syncwarp();
   }
   if (job >= 0) c.flush(a.jst + job, lane);
@@ -1277,9 +1330,9 @@ template <int NQ, typename ST>
 __global__ void __launch_bounds__(TB_WARPS * 32) k_tbound(const __grid_constant__ DevSpec sp0, const TBoundArgs<ST> a) {
   constexpr int N = 1 << NQ, E = N * N;
   __shared__ Z4<ST> sP[TB_WARPS][E], sC[TB_WARPS][E];
-  __shared__ uint64_t W1[E], W2[E];
+  __shared__ uint64_t W[E];
   __shared__ DevSpec sps[TB_WARPS];
-  init_weights(W1, W2, E);
+  init_weights(W, E);
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   Z4<ST> *P = sP[w], *C = sC[w];
@@ -1319,7 +1372,7 @@ __global__ void __launch_bounds__(TB_WARPS * 32) k_tbound(const __grid_constant_
       c.alive++;
       if (!keep) continue;
       uint64_t k1, k2;
-      warp_class_key<NQ, ST>(C, q.k, sp.nsym, conjmask, sp.symperm, W1, W2, lane, k1, k2);
+      warp_class_key<NQ, ST>(C, q.k, sp.nsym, conjmask, sp.symperm, W, lane, k1, k2);
       unsigned long long slot = 0;
       if (lane == 0) slot = atomicAdd(&a.st->n_surv, 1ULL);
       slot = __shfl_sync(FULL, slot, 0);
@@ -1593,8 +1646,8 @@ __global__ void __launch_bounds__(RES_WARPS * 32) k_node_keys(const __grid_const
                                                             uint64_t *F2) {
   constexpr int E = (1 << NQ) * (1 << NQ), EPL = E >= 32 ? E / 32 : 1;
   __shared__ Z4<ST> sC[RES_WARPS][E];
-  __shared__ uint64_t W1[E], W2[E];
-  init_weights(W1, W2, E);
+  __shared__ uint64_t W[E];
+  init_weights(W, E);
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   unsigned conjmask = 0;
@@ -1607,7 +1660,7 @@ __global__ void __launch_bounds__(RES_WARPS * 32) k_node_keys(const __grid_const
     }
     __syncwarp();
     uint64_t k1, k2;
-    warp_class_key<NQ, ST>(sC[w], meta[j].k, sp.nsym, conjmask, sp.symperm, W1, W2, lane, k1, k2);
+    warp_class_key<NQ, ST>(sC[w], meta[j].k, sp.nsym, conjmask, sp.symperm, W, lane, k1, k2);
     if (lane == 0) { F1[j] = k1; F2[j] = k2; }
     __syncwarp();
   }
@@ -1777,9 +1830,9 @@ __global__ void __launch_bounds__(RES_WARPS * 32) k_replay_keys(const __grid_con
                                                               const uint8_t *const *tgat, uint64_t *F1, uint64_t *F2) {
   constexpr int E = (1 << NQ) * (1 << NQ);
   __shared__ Z4<ST> sP[RES_WARPS][E], sC[RES_WARPS][E];
-  __shared__ uint64_t W1[E], W2[E];
+  __shared__ uint64_t W[E];
   __shared__ uint8_t spath[RES_WARPS][64];
-  init_weights(W1, W2, E);
+  init_weights(W, E);
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   unsigned conjmask = 0;
@@ -1787,7 +1840,7 @@ __global__ void __launch_bounds__(RES_WARPS * 32) k_replay_keys(const __grid_con
   for (long long j = blockIdx.x * (long long)RES_WARPS + w; j < n; j += (long long)gridDim.x * RES_WARPS) {
     const int k = warp_replay<NQ, ST>(sp, tpar, tgat, lvl, (uint32_t)j, sP[w], sC[w], spath[w], lane);
     uint64_t k1, k2;
-    warp_class_key<NQ, ST>(sC[w], k, sp.nsym, conjmask, sp.symperm, W1, W2, lane, k1, k2);
+    warp_class_key<NQ, ST>(sC[w], k, sp.nsym, conjmask, sp.symperm, W, lane, k1, k2);
     if (lane == 0) { F1[j] = k1; F2[j] = k2; }
     __syncwarp();
   }
@@ -1858,14 +1911,14 @@ template <int NQ> struct MitmSmem {
   static constexpr int E = (1 << NQ) * (1 << NQ);
   Z4<int32_t> U[E], Ud[E];
   Z4<int32_t> P[RES_WARPS][E], C[RES_WARPS][E], K[RES_WARPS][E];
-  uint64_t W1[E], W2[E];
+  uint64_t W[E];
   uint8_t path[RES_WARPS][64];
 };
 template <int NQ>
 __device__ void mitm_smem_init(MitmSmem<NQ> &sm, const Z4<int32_t> *U, const Z4<int32_t> *Ud) {
   constexpr int E = MitmSmem<NQ>::E;
   for (int e = threadIdx.x; e < E; e += blockDim.x) { sm.U[e] = U[e]; sm.Ud[e] = Ud[e]; }
-  init_weights(sm.W1, sm.W2, E);
+  init_weights(sm.W, E);
   __syncthreads();
 }
 // K of backward node j: U times its residual (rebuilt from U^dag), in sm.K[w]; returns K's exponent
@@ -1896,7 +1949,7 @@ __global__ void __launch_bounds__(RES_WARPS * 32) k_mitm_bwd_keys(const __grid_c
     bool o;
     const int k = mitm_bwd_residual<NQ>(sp, sm, lv, tpar, tgat, j, ku, w, lane, o);
     uint64_t k1, k2;
-    warp_class_key<NQ, int32_t>(sm.K[w], k, 1, 0u, sp.symperm, sm.W1, sm.W2, lane, k1, k2);
+    warp_class_key<NQ, int32_t>(sm.K[w], k, 1, 0u, sp.symperm, sm.W, lane, k1, k2);
     if (lane == 0) {
       B1[j] = k1; B2[j] = k2;
       if (o) atomicExch(ovf, 1);
@@ -2306,7 +2359,7 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
         launches++;
         const bool f = radix_sort(k0.as<uint64_t>(), v0.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(), ns, 32,
                                   64, sc, s, nullptr);
-        launches += 4 * 5;
+        launches += 1 + 4;   // the sort: upsweep + one launch per 8-bit pass
         const uint64_t *sk = f ? k1.as<uint64_t>() : k0.as<uint64_t>();
         const uint32_t *sv = f ? v1.as<uint32_t>() : v0.as<uint32_t>();
         k_runs<<<gb, 256, 0, s>>>(sk, sv, ns, sIdx.as<uint64_t>(), kidx.as<uint64_t>(), kslot.as<uint32_t>(),
@@ -2355,7 +2408,7 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
       const int hi = ((bits + 7) / 8) * 8;
       const bool f2 = radix_sort(kidx.as<uint64_t>(), kslot.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(),
                                  (size_t)distinct, 0, hi, sc, s, nullptr);
-      if (distinct > 1) launches += (hi / 8) * 5;
+      if (distinct > 1) launches += 1 + hi / 8;
       const uint64_t *ki = f2 ? k1.as<uint64_t>() : kidx.as<uint64_t>();
       const uint32_t *vi = f2 ? v1.as<uint32_t>() : kslot.as<uint32_t>();
       if ((int)par.size() <= t) { par.resize(t + 1); gat.resize(t + 1); }
@@ -2454,7 +2507,7 @@ void Engine::Impl::seen_add(DistTable &D, long long n, int lvl) {
   k_sort_init<<<gb, 256, 0, s>>>(a1.as<uint64_t>(), tot, k0.as<uint64_t>(), v0.as<uint32_t>());
   const bool f = radix_sort(k0.as<uint64_t>(), v0.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(), tot, 0, 64, sc,
                             s, nullptr);
-  launches += 1 + 8 * 5;
+  launches += 1 + 1 + 8;
   const uint32_t *order = f ? v1.as<uint32_t>() : v0.as<uint32_t>();
   D.S1.ensure(tot * 8); D.S2.ensure(tot * 8); D.Sidx.ensure(tot * 4); D.Slvl.ensure(tot * 4);
   k_keys_gather<<<gb, 256, 0, s>>>(order, tot, a1.as<uint64_t>(), a2.as<uint64_t>(), ai.as<uint32_t>(),
@@ -2488,7 +2541,7 @@ std::string dist_table_path(const HostSpec &hs, const SymGroup &grp, int K, cons
   return dir.empty() ? std::string() : dir + "/" + buf;
 }
 constexpr uint32_t DT_MAGIC = 0x54445a43u;   // "CZDT": the file's keys use this build's class hash
-constexpr uint32_t DT_KEY_VERSION = 1;
+constexpr uint32_t DT_KEY_VERSION = 2;   // 2: 32-bit weighted sums per orbit element
 
 // exact check on the host: the circuit's gates, applied to the target (residual times each gate's inverse), give
 // the goal (the identity, exponent 0)
@@ -2994,7 +3047,7 @@ int Engine::Impl::run_mitm(const HostSpec &hs, const Options &opt, const std::fu
   k_sort_init<<<gf, 256, 0, s>>>(fK1.as<uint64_t>(), nf, k0.as<uint64_t>(), v0.as<uint32_t>());
   const bool fl = radix_sort(k0.as<uint64_t>(), v0.as<uint32_t>(), k1.as<uint64_t>(), v1.as<uint32_t>(), nf, 0, 64, sc,
                              s, nullptr);
-  launches += 1 + 8 * 5;
+  launches += 1 + 1 + 8;
   S1.ensure(nf * 8); S2.ensure(nf * 8); Si.ensure(nf * 4);
   k_mitm_sorted<<<gf, 256, 0, s>>>(fl ? v1.as<uint32_t>() : v0.as<uint32_t>(), nf, fK1.as<uint64_t>(),
                                    fK2.as<uint64_t>(), S1.as<uint64_t>(), S2.as<uint64_t>(), Si.as<uint32_t>());
@@ -3097,6 +3150,8 @@ DevSpec devspec_host(const HostSpec &hs, const SymGroup &grp, int depth, bool no
   sp.nsym = grp.nsym; sp.nogoal = nogoal; sp.gk = 0;
   for (int i = 0; i < sp.ncuts; i++) { sp.cutmask[i] = hs.cutmask[i]; sp.cutsize[i] = hs.cutsize[i]; sp.rad[i] = hs.rad[i]; }
   sp.w1 = powmod_h(3, (PRIME - 1) / 8); sp.w2 = sp.w1 * sp.w1 % PRIME; sp.w3 = sp.w2 * sp.w1 % PRIME;
+  sp.wm[0] = (uint32_t)((sp.w1 << 32) % PRIME); sp.wm[1] = (uint32_t)((sp.w2 << 32) % PRIME);
+  sp.wm[2] = (uint32_t)((sp.w3 << 32) % PRIME);
   for (int s2 = 0; s2 < grp.nsym; s2++) {
     for (int x = 0; x < N; x++) sp.symperm[s2][x] = grp.bperm[s2 * N + x];
     sp.symconj[s2] = grp.conj[s2];
@@ -3424,6 +3479,36 @@ double Engine::int32_peak() {
   o.release();
   const double imads = (double)blocks * threads * iters * 8;
   return 2.0 * imads / (best * 1e-3);
+}
+
+int Engine::sort_pairs(uint64_t *keys, uint32_t *vals, size_t n, int lo, int hi, float *ms, std::string &err) {
+  if (lo < 0 || hi > 64 || lo > hi || (hi - lo) % 8) { err = "bit range [lo, hi) must be whole bytes within 64"; return RC_USAGE; }
+  try {
+    ck(cudaSetDevice(dev_), "cudaSetDevice");
+    Impl &I = *impl_;
+    I.k1.ensure(n * 8 + 8); I.v1.ensure(n * 4 + 4);
+    I.hist.ensure(sort_hist_words(n) * 4);
+    SortScratch sc{I.hist.as<uint32_t>(), nullptr, I.hist.cap / 4, 0};
+    ck(cudaEventRecord(I.ev[0], I.s), "event");
+    int nl = 0;
+    const bool f = radix_sort(keys, vals, I.k1.as<uint64_t>(), I.v1.as<uint32_t>(), n, lo, hi, sc, I.s, &nl);
+    I.launches += nl;
+    ck(cudaEventRecord(I.ev[1], I.s), "event");
+    if (f) {
+      ck(cudaMemcpyAsync(keys, I.k1.p, n * 8, cudaMemcpyDeviceToDevice, I.s), "d2d");
+      ck(cudaMemcpyAsync(vals, I.v1.p, n * 4, cudaMemcpyDeviceToDevice, I.s), "d2d");
+    }
+    ck(cudaGetLastError(), "sort");
+    const bool failed = sort_failed(sc, I.s);
+    float t = 0;
+    ck(cudaEventElapsedTime(&t, I.ev[0], I.ev[1]), "event");
+    if (ms) *ms = t;
+    if (failed) { err = "a look-back wait gave up (the result is exact; the predecessors were counted directly)"; }
+  } catch (const CudaError &e) {
+    err = e.what();
+    return RC_CUDA;
+  }
+  return 0;
 }
 
 int Engine::search(const HostSpec &hs, const Options &opt, const std::function<void(const LevelStats &)> &cb,

@@ -1,10 +1,10 @@
 // Device primitives of the frontier dedupe: exclusive scan and a stable LSD radix sort of (u64 key, u32 value)
-// pairs over a chosen bit range, 8-bit digits. Reduce-then-scan per pass: per-tile digit histograms (digit-major,
-// so one exclusive scan gives every tile's output base per digit), then a stable scatter that ranks keys inside
-// the tile with warp match + per-warp digit counts in shared memory. All launches go to the caller's stream.
+// pairs over a chosen bit range, 8-bit digits, one launch per digit pass (see radix_sort). All launches go to the
+// caller's stream.
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 namespace cz {
@@ -103,82 +103,216 @@ inline void exclusive_scan(const uint32_t *in, uint32_t *out, size_t n, uint32_t
 inline size_t scan_partials_words(size_t n) { return (n + SCAN_CHUNK - 1) / SCAN_CHUNK + 1; }
 
 // ---------------- radix sort ----------------
-__global__ void k_digit_hist(const uint64_t *keys, size_t n, int shift, uint32_t *hist, uint32_t ntiles) {
-  __shared__ uint32_t h[256];
-  h[threadIdx.x] = 0;
+// Stable LSD radix sort of (u64 key, u32 value) pairs by bits [lo, hi) of the key, 8-bit digits, one launch per
+// digit pass:
+//  * k_sort_upsweep reads the keys once and counts every pass's digits (global histograms);
+//  * k_sort_onesweep, per pass, takes tiles of OS_TILE keys in the order of an atomic ticket. A tile counts its
+//    digits, publishes them, and finds the keys of earlier tiles per digit by looking back over their published
+//    words (decoupled look-back: an earlier tile's word is either its own count or, once its look-back is done, the
+//    inclusive prefix; walking back stops at the first prefix). It then ranks its keys stably in shared memory
+//    (warp match + per-warp digit counts, round by round in input order), places them there in digit order, and
+//    writes them out so that neighbouring threads write neighbouring addresses.
+// A tile waits only for tiles with smaller tickets, whose blocks are already running, so the waits end; every wait
+// is still bounded (OS_SPIN_MAX polls). Should one give up, the tile counts the earlier tiles' digits itself from
+// the input (slow, still exact) and the sort records it (sort_failed), so a result is never wrong and nothing hangs.
+// Status words: tag (pass + 1, 4 bits) | state (2 bits: 1 count, 2 prefix) | value (58 bits); the scratch is
+// cleared once per sort, and the tag tells one pass's words from the previous pass's.
+constexpr int OS_THREADS = 256;
+constexpr int OS_ITEMS = 8;
+constexpr int OS_TILE = OS_THREADS * OS_ITEMS;     // keys per tile
+constexpr int OS_MAXPASS = 8;
+constexpr long long OS_SPIN_MAX = 1LL << 26;
+constexpr size_t OS_HEAD_WORDS = 256 * OS_MAXPASS + 16;   // digit counts per pass, tickets per pass, error flag
+constexpr unsigned long long OS_VALUE = (1ULL << 58) - 1;
+
+inline size_t sort_tiles(size_t n) { return (n + OS_TILE - 1) / OS_TILE; }
+// 32-bit words of sort scratch for n keys (header + one 64-bit status word per tile and digit)
+inline size_t sort_hist_words(size_t n) { return OS_HEAD_WORDS + 2 * 256 * (sort_tiles(n) + 1); }
+
+__global__ void __launch_bounds__(256) k_sort_upsweep(const uint64_t *keys, size_t n, int lo, int npass,
+                                                       uint32_t *counts) {
+  __shared__ uint32_t h[OS_MAXPASS][256];
+  for (int p = 0; p < npass; p++) h[p][threadIdx.x] = 0;
   __syncthreads();
-  const size_t base = (size_t)blockIdx.x * SORT_TILE;
-  for (int i = 0; i < SORT_ITEMS; i++) {
-    const size_t j = base + (size_t)i * SORT_THREADS + threadIdx.x;
-    if (j < n) atomicAdd(&h[(keys[j] >> shift) & 255], 1u);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    for (int p = 0; p < npass; p++) atomicAdd(&h[p][(k >> (lo + 8 * p)) & 255], 1u);
   }
   __syncthreads();
-  hist[(size_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+  for (int p = 0; p < npass; p++)
+    if (h[p][threadIdx.x]) atomicAdd(&counts[p * 256 + threadIdx.x], h[p][threadIdx.x]);
 }
 
-__global__ void __launch_bounds__(SORT_THREADS) k_digit_scatter(const uint64_t *kin, const uint32_t *vin, uint64_t *kout,
-                                                                uint32_t *vout, size_t n, int shift,
-                                                                const uint32_t *offs, uint32_t ntiles) {
-  constexpr int NW = SORT_THREADS / 32;
-  __shared__ uint32_t base[256];
-  __shared__ uint32_t wcnt[NW][256];
+__device__ __forceinline__ unsigned long long os_load(const unsigned long long *p) {
+  return *(const volatile unsigned long long *)p;
+}
+__device__ __forceinline__ void os_store(unsigned long long *p, unsigned long long v) {
+  *(volatile unsigned long long *)p = v;
+}
+// exclusive scan of one u32 per thread over the 256 threads of the block
+__device__ __forceinline__ uint32_t os_block_scan(uint32_t v, uint32_t *ws) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t inc = warp_incl_scan(v, lane);
+  if (lane == 31) ws[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    const uint32_t x = lane < OS_THREADS / 32 ? ws[lane] : 0;
+    const uint32_t xi = warp_incl_scan(x, lane);
+    if (lane < OS_THREADS / 32) ws[lane] = xi - x;
+  }
+  __syncthreads();
+  const uint32_t r = ws[w] + inc - v;
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(OS_THREADS) k_sort_onesweep(const uint64_t *kin, const uint32_t *vin, uint64_t *kout,
+                                                               uint32_t *vout, size_t n, int shift, int pass,
+                                                               uint32_t *head, unsigned long long *status,
+                                                               unsigned *err) {
+  constexpr int NW = OS_THREADS / 32;
+  __shared__ uint64_t sk[OS_TILE];
+  __shared__ uint32_t sv[OS_TILE];
+  __shared__ uint32_t cnt[256], lex[256], run[256], wcnt[NW][256], ws[NW];
+  __shared__ unsigned long long gbase[256];
+  __shared__ unsigned ticket;
+  __shared__ int fallback;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  base[tid] = offs[(size_t)tid * ntiles + blockIdx.x];
+  const uint32_t *counts = head + pass * 256;
+  unsigned *tickets = head + 256 * OS_MAXPASS;
+  if (tid == 0) { ticket = atomicAdd(&tickets[pass], 1u); fallback = 0; }
+  cnt[tid] = 0;
   for (int x = 0; x < NW; x++) wcnt[x][tid] = 0;
   __syncthreads();
-  const size_t start = (size_t)blockIdx.x * SORT_TILE;
-  const unsigned lt = (1u << lane) - 1;
-  for (int r = 0; r < SORT_ITEMS; r++) {
-    const size_t i = start + (size_t)r * SORT_THREADS + tid;
-    const bool valid = i < n;
-    uint64_t key = 0;
-    uint32_t val = 0;
-    int d = 256;
-    if (valid) { key = kin[i]; val = vin[i]; d = (int)((key >> shift) & 255); }
-    const unsigned peers = __match_any_sync(0xffffffffu, d);
-    const int lrank = __popc(peers & lt);
-    const bool leader = lane == __ffs(peers) - 1;
-    if (valid && leader) wcnt[w][d] = __popc(peers);
+  const size_t tile = ticket, start = tile * OS_TILE;
+  const unsigned long long tag = (unsigned long long)(pass + 1) << 60;
+  uint64_t key[OS_ITEMS];
+  uint32_t val[OS_ITEMS];
+  int dig[OS_ITEMS];
+#pragma unroll
+  for (int r = 0; r < OS_ITEMS; r++) {            // striped: round r holds positions start + r * 256 + tid
+    const size_t i = start + (size_t)r * OS_THREADS + tid;
+    dig[r] = 256;
+    if (i < n) {
+      key[r] = kin[i];
+      val[r] = vin[i];
+      dig[r] = (int)((key[r] >> shift) & 255);
+      atomicAdd(&cnt[dig[r]], 1u);
+    }
+  }
+  __syncthreads();
+  // this tile's count of digit tid: publish it, then add up the earlier tiles' counts by looking back
+  const uint32_t mine = cnt[tid];
+  unsigned long long *st = status + tile * 256 + tid;
+  unsigned long long before = 0;
+  bool ok = true;
+  if (tile == 0) {
+    os_store(st, tag | (2ULL << 58) | mine);
+  } else {
+    os_store(st, tag | (1ULL << 58) | mine);
+    for (long long j = (long long)tile - 1; j >= 0 && ok; j--) {
+      const unsigned long long *q = status + (size_t)j * 256 + tid;
+      unsigned long long v = os_load(q);
+      long long spins = 0;
+      while ((v >> 60) != (tag >> 60) && ++spins < OS_SPIN_MAX) {
+        __nanosleep(64);
+        v = os_load(q);
+      }
+      if ((v >> 60) != (tag >> 60)) { ok = false; break; }
+      before += v & OS_VALUE;
+      if (((v >> 58) & 3) == 2) break;
+    }
+  }
+  if (!ok) { atomicOr(err, 1u); fallback = 1; }
+  __syncthreads();
+  if (fallback) {                                 // a wait gave up: count the earlier tiles' digits directly
+    run[tid] = 0;
     __syncthreads();
-    if (valid) {
+    for (size_t i = tid; i < start; i += OS_THREADS) atomicAdd(&run[(kin[i] >> shift) & 255], 1u);
+    __syncthreads();
+    before = run[tid];
+    __syncthreads();
+  }
+  if (tile != 0) os_store(st, tag | (2ULL << 58) | ((before + mine) & OS_VALUE));
+  // output base of digit tid for this tile: keys of smaller digits (all tiles) + this digit's keys in earlier tiles
+  const uint32_t dtotal = counts[tid];
+  const uint32_t dex = os_block_scan(dtotal, ws);
+  gbase[tid] = (unsigned long long)dex + before;
+  const uint32_t lx = os_block_scan(mine, ws);
+  lex[tid] = lx;
+  run[tid] = lx;
+  __syncthreads();
+  // stable local ranks, round by round in input order; keys placed in shared memory in digit order
+  const unsigned lt = (1u << lane) - 1;
+#pragma unroll
+  for (int r = 0; r < OS_ITEMS; r++) {
+    const int d = dig[r];
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const bool leader = lane == __ffs(peers) - 1;
+    if (d < 256 && leader) wcnt[w][d] = __popc(peers);
+    __syncthreads();
+    if (d < 256) {
       uint32_t pre = 0;
       for (int x = 0; x < w; x++) pre += wcnt[x][d];
-      const uint32_t pos = base[d] + pre + lrank;
-      kout[pos] = key;
-      vout[pos] = val;
+      const uint32_t pos = run[d] + pre + __popc(peers & lt);
+      sk[pos] = key[r];
+      sv[pos] = val[r];
     }
     __syncthreads();
-    if (valid && leader) { atomicAdd(&base[d], (uint32_t)__popc(peers)); wcnt[w][d] = 0; }
+    if (d < 256 && leader) { atomicAdd(&run[d], (uint32_t)__popc(peers)); wcnt[w][d] = 0; }
     __syncthreads();
+  }
+  const int tn = (int)(n - start < (size_t)OS_TILE ? n - start : (size_t)OS_TILE);
+  for (int i = tid; i < tn; i += OS_THREADS) {
+    const uint64_t k = sk[i];
+    const int d = (int)((k >> shift) & 255);
+    const unsigned long long pos = gbase[d] + (unsigned long long)(i - (int)lex[d]);
+    kout[pos] = k;
+    vout[pos] = sv[i];
   }
 }
 
 struct SortScratch {
-  uint32_t *hist = nullptr;       // 256 * ntiles
-  uint32_t *partials = nullptr;   // scan partials
+  uint32_t *hist = nullptr;       // sort scratch: sort_hist_words(n) words
+  uint32_t *partials = nullptr;   // unused by the sort (kept for the callers' scan buffers)
   size_t cap_hist = 0, cap_part = 0;
+  uint32_t *err = nullptr;        // where a failed look-back is flagged (nullptr: the scratch's own word)
 };
-inline size_t sort_hist_words(size_t n) { return 256 * ((n + SORT_TILE - 1) / SORT_TILE); }
 
-// sorts (k0, v0) by bits [lo, hi) of the key, stable; uses (k1, v1) as the other buffer. Returns true when the
-// result ended in (k1, v1). Counts launches into *launches.
+// sorts (k0, v0) by bits [lo, hi) of the key (hi - lo a multiple of 8, at most 64), stable; uses (k1, v1) as the
+// other buffer. Returns true when the result ended in (k1, v1). Counts launches into *launches.
 inline bool radix_sort(uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1, size_t n, int lo, int hi,
                        const SortScratch &sc, cudaStream_t s, int *launches) {
   if (n <= 1 || hi <= lo) return false;
-  const uint32_t ntiles = (uint32_t)((n + SORT_TILE - 1) / SORT_TILE);
+  const int npass = (hi - lo + 7) / 8;
+  const size_t ntiles = sort_tiles(n);
+  cudaMemsetAsync(sc.hist, 0, (OS_HEAD_WORDS + 2 * 256 * ntiles) * 4, s);
+  unsigned long long *status = (unsigned long long *)(sc.hist + OS_HEAD_WORDS);
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const unsigned ub = (unsigned)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, (size_t)nsm * 8));
+  k_sort_upsweep<<<ub, 256, 0, s>>>(k0, n, lo, npass, sc.hist);
   bool flip = false;
-  for (int shift = lo; shift < hi; shift += 8) {
+  for (int p = 0; p < npass; p++) {
     const uint64_t *ki = flip ? k1 : k0;
     const uint32_t *vi = flip ? v1 : v0;
     uint64_t *ko = flip ? k0 : k1;
     uint32_t *vo = flip ? v0 : v1;
-    k_digit_hist<<<ntiles, SORT_THREADS, 0, s>>>(ki, n, shift, sc.hist, ntiles);
-    exclusive_scan(sc.hist, sc.hist, (size_t)256 * ntiles, sc.partials, nullptr, s);
-    k_digit_scatter<<<ntiles, SORT_THREADS, 0, s>>>(ki, vi, ko, vo, n, shift, sc.hist, ntiles);
-    if (launches) *launches += 5;
+    k_sort_onesweep<<<(unsigned)ntiles, OS_THREADS, 0, s>>>(ki, vi, ko, vo, n, lo + 8 * p, p, sc.hist, status,
+                                                             sc.err ? sc.err : sc.hist + 256 * OS_MAXPASS + OS_MAXPASS);
     flip = !flip;
   }
+  if (launches) *launches += 1 + npass;
   return flip;
+}
+// true when a look-back wait of the last sort on this scratch gave up (the result is exact all the same: the tile
+// counted its predecessors' digits itself); synchronises the stream
+inline bool sort_failed(const SortScratch &sc, cudaStream_t s) {
+  uint32_t e = 0;
+  cudaMemcpyAsync(&e, sc.hist + 256 * OS_MAXPASS + OS_MAXPASS, 4, cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  return e != 0;
 }
 
 }  // namespace

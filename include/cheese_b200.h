@@ -233,6 +233,13 @@ void *cz_engine_stream(cz_engine *engine);
  * register-resident IMAD loop timed with CUDA events. The denominator of the level kernel's roofline. */
 int cz_int32_peak(cz_engine *engine, double *ops_per_s);
 
+/* No counterpart in the reference (its dedupe sorts with Thrust, src/cheese.cu:1335-1343). The frontier dedupe's
+ * stable LSD radix sort on caller-held device buffers: n (key, value) pairs sorted in place by bits [lo, hi) of the
+ * key (hi - lo a multiple of 8, hi <= 64), equal keys in their input order, on the engine's stream; returns once
+ * sorted, with the sort's device time in *ms (may be NULL). The engine holds the ping-pong buffers (12 n bytes) and
+ * the scratch. For tests and measurement of the dedupe at scale. */
+int cz_sort_pairs(cz_engine *engine, uint64_t *d_keys, uint32_t *d_vals, size_t n, int lo, int hi, float *ms);
+
 /* ---------------- T-count (the reference's build/tcount, src/tcount.cu) ---------------- */
 /* flags of `tcount TSPEC [--table K] [--max T]` (tcount.cu:452-465) and the table cache directory: the table of
  * (n, K) is cached in <cache_dir>/tcount-table-n<n>-k<K>.cz.bin; a reference-written
