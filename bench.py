@@ -121,6 +121,9 @@ def run_ref_cpu(cases, threads):
 
 
 REF_GPU = ROOT / "oracle" / "_ref" / "cheese-gpu-ref"
+# large-frontier instances pinned to the reference (tests/golden/heavy_cases.json): (name, spec, budget, classes on)
+LARGE = [("toffoli-12-nosym", "toffoli", 12, False), ("heavy-28", "heavy-28", 12, True),
+         ("heavy-17", "heavy-17", 12, True), ("heavy-6", "heavy-6", 12, True), ("heavy-24", "heavy-24", 12, True)]
 
 
 def reference_gpu(eng, specs):
@@ -155,6 +158,37 @@ def reference_gpu(eng, specs):
             tot_s += search_s or 0.0
         out["prefixes_per_s"] = tot_pre / tot_s if tot_s else None
         out["toffoli12_proof_s"] = out.get("toffoli-12", {}).get("search_s")
+        # the large-frontier regime (levels of 1e7-4.4e7 prefixes, millions of survivors): long enough for the
+        # reference's 10 ms "seconds" resolution; this library device-timed on the same specs
+        import torch
+        stream = torch.cuda.ExternalStream(eng.stream, device=f"cuda:{eng.device}")
+        large, r_s, o_s, r_pre = {}, 0.0, 0.0, 0
+        for name, stem, dd, sym in LARGE:
+            t0 = time.perf_counter()
+            p = subprocess.run([str(REF_GPU), str(SPECS / f"{stem}.spec"), "--depth", str(dd)] +
+                               ([] if sym else ["--no-sym"]), cwd=d, capture_output=True, text=True, timeout=900)
+            wall = time.perf_counter() - t0
+            lines = p.stdout.splitlines()
+            lv = [json.loads(l) for l in lines if '"prefixes"' in l]
+            text = (SPECS / f"{stem}.spec").read_text()
+            eng.search(text, depth=dd, sym=sym)                      # warm (buffers grown)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            mine = eng.search(text, depth=dd, sym=sym)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            import re
+            same = [re.sub(r'"seconds": [0-9.]+', '"seconds": 0.00', l) for l in lines] == mine.lines()
+            ref_search = max((x["seconds"] for x in lv), default=None)
+            large[name] = {"rc": p.returncode, "same_lines": same, "prefixes": sum(x["prefixes"] for x in lv),
+                           "reference_search_s": ref_search, "reference_process_s": wall, "ours_ms": ms}
+            r_s += ref_search or 0.0
+            o_s += ms / 1e3
+            r_pre += large[name]["prefixes"]
+        out["large_frontier"] = {"cases": large, "reference_prefixes_per_s": r_pre / r_s if r_s else None,
+                                 "ours_prefixes_per_s": r_pre / o_s if o_s else None,
+                                 "ours_vs_reference": (r_s / o_s) if o_s else None}
         t0 = time.perf_counter()
         budgets = {}
         for dd in range(1, 16):
@@ -319,12 +353,24 @@ def systems(eng, args):
     # untimed first, so both are timed warm: the engine's buffers and the sessions' device memory already grown.
     jobs = workloads.batch(1, 512)
     specs = [cz.Spec(workloads.make_spec(n, c, d)) for n, c, d in jobs]
+    # the autotuner: per qubit count, probe jobs from another seed of the same generator
+    probe = [(n, cz.Spec(workloads.make_spec(n, c, d))) for n, c, d in workloads.batch(2, 96)]
+    t0 = time.perf_counter()
+    tuning = {n: cz.autotune(eng, n, [s for m, s in probe if m == n][:48]) for n in (2, 3)}
+    t_tune = time.perf_counter() - t0
     for rep in range(2):
         t0 = time.perf_counter()
-        plain = [eng.search(s) for s in specs]
+        per_job = []
+        plain = []
+        for s in specs:
+            a = time.perf_counter()
+            plain.append(eng.search(s))
+            per_job.append(time.perf_counter() - a)
         tp = time.perf_counter() - t0
         t0 = time.perf_counter()
         sess = {n: cz.Batch(eng, n) for n in (2, 3)}
+        for n, b in sess.items():
+            b.set_tuning(tuning[n])
         ids = [sess[s.n].submit(s) for s in specs]
         for b in sess.values():
             b.run()
@@ -334,20 +380,52 @@ def systems(eng, args):
                 b.close()
     bad = sum(1 for s, i, p in zip(specs, ids, plain)
               if (lambda r: r.rc != p.rc or r.lines() != p.lines() or r.circuit != p.circuit)(sess[s.n].result(i)))
+    launches = sum(b.info()["kernel_launches"] for b in sess.values())
+    steps = sum(b.info()["steps"] for b in sess.values())
+    for b in sess.values():
+        b.close()
+    # the light jobs alone (plain time under 5 ms each): the part of the mix that is launch and sync bound
+    light = [s for s, t in zip(specs, per_job) if t < 5e-3]
+    t0 = time.perf_counter()
+    for s in light:
+        eng.search(s)
+    tpl = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    sess = {n: cz.Batch(eng, n) for n in (2, 3)}
+    for n, b in sess.items():
+        b.set_tuning(tuning[n])
+    for s in light:
+        sess[s.n].submit(s)
+    for b in sess.values():
+        b.run()
+    tbl = time.perf_counter() - t0
+    for b in sess.values():
+        b.close()
     out["batched"] = {"workload": "512 seeded targets: random circuits of L in [6,12] gates over 2-3 qubits "
                                   "(T/Tdg with prob 0.3), budget L", "plain_jobs_s": 512 / tp, "batched_jobs_s": 512 / tb,
                       "speedup": tp / tb, "mismatches": bad, "timing": "warm (second pass of both arms)",
-                      "launches": sum(b.info()["kernel_launches"] for b in sess.values()),
-                      "steps": sum(b.info()["steps"] for b in sess.values())}
-    for b in sess.values():
-        b.close()
-    del sess, plain, b
+                      "launches": launches, "steps": steps,
+                      "light_subset": {"jobs": len(light), "rule": "plain time under 5 ms",
+                                       "plain_jobs_s": len(light) / tpl if tpl else None,
+                                       "batched_jobs_s": len(light) / tbl if tbl else None,
+                                       "speedup": tpl / tbl if tbl else None},
+                      "autotune": {"probe": "48 jobs per qubit count from seed 2 of the same generator",
+                                   "search_space": {"chunk_gib": [8, 1, 2, 4], "expand_blocks_per_sm": [16, 4, 8, 32],
+                                                    "tbound_blocks_per_sm": [4, 1, 2, 8]},
+                                   "seconds": t_tune,
+                                   "chosen": {str(n): {"chunk_gib": t.chunk_bytes / 2 ** 30,
+                                                       "expand_blocks_per_sm": t.expand_blocks_per_sm,
+                                                       "tbound_blocks_per_sm": t.tbound_blocks_per_sm,
+                                                       "probe_s": t.best_seconds,
+                                                       "trial_s": list(t.trial_seconds[:t.trials])}
+                                              for n, t in tuning.items()}}}
+    del sess, plain
     # table-driven T count: Clifford BFS table + K = 4 coset table (3 qubits), then seeded queries, each verified
     t0 = time.perf_counter()
     ct = eng.clifford_table(3)
     t_cl = time.perf_counter() - t0
     qs = tcwork.table_queries(eng, 4, 1024)
-    nq = min(len(qs), 256)
+    nq = len(qs)
     specs_t = [tcwork.tspec_of_circuit(3, c) for c, _ in qs[:nq]]
     t0 = time.perf_counter()
     rc, lv, r0 = eng.tcount(specs_t[0], table_k=4, cache_dir=None)
@@ -471,7 +549,7 @@ def systems(eng, args):
         f.write_text(text)
         subprocess.run([str(exes[kind]), str(f)], cwd=tmp, capture_output=True, timeout=600)
     t_cli = time.perf_counter() - t0
-    srv = cz.Server(memory_gb=100.0)
+    srv = cz.Server(memory_gb=180.0)               # the admission limit of the serving configuration
     warm = [srv.submit(k, t) for k, t, _, _ in [next(r for r in reqs if r[0] == 1), next(r for r in reqs if r[0] == 2)]]
     srv.wait(2, 900)
     rates = {}

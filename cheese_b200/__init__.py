@@ -121,6 +121,11 @@ class BatchInfo(C.Structure):
                 ("steps", C.c_int64), ("kernel_launches", C.c_int64), ("device_bytes", C.c_int64),
                 ("waits", C.c_int64)]
 
+class BatchTuning(C.Structure):
+    _fields_ = [("chunk_bytes", C.c_int64), ("expand_blocks_per_sm", C.c_int), ("tbound_blocks_per_sm", C.c_int),
+                ("trials", C.c_int), ("trial_seconds", C.c_double * 16), ("best_seconds", C.c_double)]
+
+
 # every C entry point of include/cheese_b200.h with its ctypes signature
 SIGNATURES = {
     "cz_spec_parse": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t]),
@@ -141,6 +146,9 @@ SIGNATURES = {
                                          C.c_char_p, C.c_size_t]),
     "cz_engine_stream": (C.c_void_p, [C.c_void_p]),
     "cz_int32_peak": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "cz_batch_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(BatchTuning)]),
+    "cz_batch_autotune": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p), C.c_int, C.POINTER(Options),
+                                    C.POINTER(BatchTuning)]),
     "cz_sort_pairs": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.c_int,
                                 C.POINTER(C.c_float)]),
     "cz_tcount_options_default": (None, [C.POINTER(TcOptions)]),
@@ -325,6 +333,7 @@ class Engine:
 
     def __init__(self, device=0):
         self._h = C.c_void_p()
+        self.device = device
         err = C.create_string_buffer(256)
         rc = lib().cz_engine_create(device, C.byref(self._h), err, 256)
         if rc:
@@ -533,6 +542,18 @@ class Engine:
         return SearchOutcome(spec, rc, levels, res)
 
 
+def autotune(engine, nq, probe_specs):
+    """the batch autotuner (cz_batch_autotune) on probe specs of nq qubits: a BatchTuning with the probe times"""
+    specs = [s if isinstance(s, Spec) else Spec(s) for s in probe_specs]
+    arr = (C.c_void_p * len(specs))(*[s._h.value for s in specs])
+    out = BatchTuning()
+    opt = Options(-1, 1, 1, 0, 0, 0, None, 0)
+    rc = lib().cz_batch_autotune(engine._h, nq, arr, len(specs), C.byref(opt), C.byref(out))
+    if rc:
+        raise RuntimeError(f"cz_batch_autotune failed: {rc}")
+    return out
+
+
 class Batch:
     """a batch session of one qubit count on an engine: submit specs, step, collect SearchOutcomes"""
 
@@ -545,6 +566,12 @@ class Batch:
         if memory_gb is not None:
             lib().cz_batch_set_memory(self._h, memory_gb)
         self.specs = {}
+
+    def set_tuning(self, tuning):
+        """apply a BatchTuning (e.g. from autotune)"""
+        rc = lib().cz_batch_set_tuning(self._h, C.byref(tuning))
+        if rc:
+            raise RuntimeError(f"cz_batch_set_tuning failed: {rc}")
 
     def submit(self, spec, depth=-1, dedupe=True, sym=True, store64=False):
         if not isinstance(spec, Spec):

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "cz_capi_internal.h"
 #include "cz_specgen.h"
@@ -246,6 +247,53 @@ int cz_batch_step(cz_batch *batch, int *running) {
 }
 
 const char *cz_batch_error(const cz_batch *batch) { return batch ? batch->err.c_str() : "";
+}
+
+int cz_batch_set_tuning(cz_batch *batch, const cz_batch_tuning *t) {
+  if (!batch || !t || t->chunk_bytes <= 0 || t->expand_blocks_per_sm < 1 || t->tbound_blocks_per_sm < 1 ||
+      t->expand_blocks_per_sm > 64 || t->tbound_blocks_per_sm > 64)
+    return CZ_ERR_USAGE;
+  cz::BatchTuning bt;
+  bt.chunk_bytes = (size_t)t->chunk_bytes;
+  bt.expand_blocks_per_sm = t->expand_blocks_per_sm;
+  bt.tbound_blocks_per_sm = t->tbound_blocks_per_sm;
+  batch->b->set_tuning(bt);
+  return 0;
+}
+
+int cz_batch_autotune(cz_engine *engine, int nq, const cz_spec *const *probe, int nprobe, const cz_options *opt,
+                      cz_batch_tuning *out) {
+  if (!engine || !out || nq < 1 || nq > 3 || nprobe < 1 || !probe) return CZ_ERR_USAGE;
+  std::memset(out, 0, sizeof *out);
+  cz_options o;
+  cz_options_default(&o);
+  if (opt) o = *opt;
+  cz::Options eo;
+  eo.depth = o.depth; eo.dedupe = o.dedupe != 0; eo.sym = o.sym != 0; eo.store64 = o.store64; eo.profile = false;
+  std::vector<const cz::HostSpec *> hs;
+  for (int i = 0; i < nprobe; i++) {
+    if (!probe[i] || probe[i]->hs.n != nq || probe[i]->hs.states) return CZ_ERR_USAGE;
+    hs.push_back(&probe[i]->hs);
+  }
+  try {
+    std::vector<cz::TuneTrial> trials;
+    const cz::BatchTuning best = cz::autotune_batch(*engine->e, nq, hs, eo, &trials);
+    out->chunk_bytes = (int64_t)best.chunk_bytes;
+    out->expand_blocks_per_sm = best.expand_blocks_per_sm;
+    out->tbound_blocks_per_sm = best.tbound_blocks_per_sm;
+    out->trials = (int)std::min<size_t>(trials.size(), 16);
+    out->best_seconds = 1e30;
+    for (size_t i = 0; i < trials.size(); i++) {
+      if (i < 16) out->trial_seconds[i] = trials[i].seconds;
+      const cz::BatchTuning &t = trials[i].t;
+      if (t.chunk_bytes == best.chunk_bytes && t.expand_blocks_per_sm == best.expand_blocks_per_sm &&
+          t.tbound_blocks_per_sm == best.tbound_blocks_per_sm)
+        out->best_seconds = std::min(out->best_seconds, trials[i].seconds);
+    }
+    return 0;
+  } catch (const std::exception &) {
+    return CZ_ERR_CUDA;
+  }
 }
 
 int cz_batch_info_get(const cz_batch *batch, cz_batch_info *out) {

@@ -8,8 +8,9 @@
 //
 // B200 design:
 //  * the table is direct-addressed by a perfect rank of the group element (cz_tableau.h): a 92.9 MB byte array of
-//    distances at n = 3 that stays in L2 while it is probed, a visited bitmap for the BFS claims (11.6 MB), and
-//    the element of every rank (u64) for candidate enumeration and uniform draws. No keys, no probing chains;
+//    distances at n = 3 that stays in L2 while it is probed, and a visited bitmap for the BFS claims (11.6 MB). No
+//    keys, no probing chains, and no element array: the element of a rank is computed back from the rank (unrank)
+//    for candidate enumeration and uniform draws, so the BFS writes one byte per new element at a random place;
 //  * BFS: one thread per frontier element, all generators applied bit-parallel to the packed tableau, claims by
 //    atomicOr on the bitmap after a plain read, warp-aggregated appends to the next frontier;
 //  * beam step: dist(X) = dist(X^-1) (the generator set is closed under inverses), and X^-1 is the candidate
@@ -100,7 +101,7 @@ struct CBuf {
 template <int N>
 __global__ void __launch_bounds__(CL_T) k_cl_bfs(const uint64_t *front, unsigned long long nf, uint64_t *next,
                                                  unsigned long long cap, unsigned long long *nn, uint32_t *seen,
-                                                 uint8_t *dist, uint64_t *elem, uint8_t d, int *ovf) {
+                                                 uint8_t *dist, uint8_t d, int *ovf) {
   using T = Tb<N>;
   const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
   const int lane = threadIdx.x & 31;
@@ -119,7 +120,7 @@ __global__ void __launch_bounds__(CL_T) k_cl_bfs(const uint64_t *front, unsigned
       } else {
         atomicOr(ovf, 2);
       }
-      if (fresh) { dist[r] = d; elem[r] = C; }
+      if (fresh) dist[r] = d;
       const unsigned am = __activemask();
       const unsigned bal = __ballot_sync(am, fresh);
       if (bal) {
@@ -139,7 +140,7 @@ __global__ void __launch_bounds__(CL_T) k_cl_bfs(const uint64_t *front, unsigned
 
 // placements of a T on qubit q: every K with K Z_q' K^-1 = +-Z_q for some q' (clifford.cu:170-183)
 template <int N>
-__global__ void k_cl_cands(const uint64_t *elem, unsigned long long order, uint64_t *lists, unsigned long long capq,
+__global__ void k_cl_cands(unsigned long long order, uint64_t *lists, unsigned long long capq,
                            unsigned long long *cnt, int *ovf) {
   using T = Tb<N>;
   const int lane = threadIdx.x & 31;
@@ -148,7 +149,7 @@ __global__ void k_cl_cands(const uint64_t *elem, unsigned long long order, uint6
   for (unsigned long long it = 0; it < nit; it++) {
     const unsigned long long r = it * stride + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = r < order;
-    const uint64_t K = valid ? elem[r] : 0;
+    const uint64_t K = valid ? T::unrank((uint32_t)r) : 0;   // every rank is an element (the BFS covers the group)
 #pragma unroll
     for (int q = 0; q < N; q++) {
       bool hit = false;
@@ -308,9 +309,9 @@ __global__ void k_cl_dist(const uint64_t *tab, size_t n, const uint8_t *dist, in
   }
 }
 template <int N>
-__global__ void k_cl_elem(const uint64_t *idx, size_t n, unsigned long long order, const uint64_t *elem, uint64_t *out) {
+__global__ void k_cl_elem(const uint64_t *idx, size_t n, unsigned long long order, uint64_t *out) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    out[i] = idx[i] < order ? elem[idx[i]] : 0;
+    out[i] = idx[i] < order ? Tb<N>::unrank((uint32_t)idx[i]) : 0;
 }
 // one warp per segment: the optimal word of X, generators indexed into gs (clifford.cu:352-371)
 template <int N>
@@ -359,11 +360,11 @@ void h_image_table(int n, uint64_t B, uint8_t *tab) {
 struct CTable {
   int n = 0;
   long long order = 0;
-  CBuf dist, elem;
+  CBuf dist;
   CBuf candK[3], candM[3];
   unsigned long long ncand[3] = {0, 0, 0};
   CliffTableInfo info;
-  void release() { dist.release(); elem.release(); for (int q = 0; q < 3; q++) { candK[q].release(); candM[q].release(); } }
+  void release() { dist.release(); for (int q = 0; q < 3; q++) { candK[q].release(); candM[q].release(); } }
 };
 
 class CliffordContext {
@@ -416,7 +417,6 @@ void CliffordContext::build(CTable &t) {
   t.n = N;
   t.order = (long long)order;
   t.dist.ensure(order);
-  t.elem.ensure(order * 8);
   CBuf seen, fa, fb;
   const unsigned long long words = (order + 31) / 32;
   seen.ensure(words * 4);
@@ -431,7 +431,6 @@ void CliffordContext::build(CTable &t) {
   const uint32_t bit = 1u << (r0 & 31);
   clk(cudaMemcpyAsync(t.dist.as<uint8_t>() + r0, &zero, 1, cudaMemcpyHostToDevice, s), "h2d");
   clk(cudaMemcpyAsync(seen.as<uint32_t>() + (r0 >> 5), &bit, 4, cudaMemcpyHostToDevice, s), "h2d");
-  clk(cudaMemcpyAsync(t.elem.as<uint64_t>() + r0, &id, 8, cudaMemcpyHostToDevice, s), "h2d");
   clk(cudaMemcpyAsync(fa.p, &id, 8, cudaMemcpyHostToDevice, s), "h2d");
   CliffTableInfo &inf = t.info;
   inf = CliffTableInfo{};
@@ -441,7 +440,7 @@ void CliffordContext::build(CTable &t) {
   for (int d = 1; nf; d++) {
     clk(cudaMemsetAsync(cnt.p, 0, 8, s), "memset");
     k_cl_bfs<N><<<grid(nf), CL_T, 0, s>>>(fa.as<uint64_t>(), nf, fb.as<uint64_t>(), order, cnt.as<unsigned long long>(),
-                                          seen.as<uint32_t>(), t.dist.as<uint8_t>(), t.elem.as<uint64_t>(), (uint8_t)d,
+                                          seen.as<uint32_t>(), t.dist.as<uint8_t>(), (uint8_t)d,
                                           ovf.as<int>());
     launches++;
     clk(cudaGetLastError(), "bfs");
@@ -465,7 +464,7 @@ void CliffordContext::build(CTable &t) {
   CBuf lists;
   lists.ensure(capq * N * 8);
   clk(cudaMemsetAsync(cnt.p, 0, 64, s), "memset");
-  k_cl_cands<N><<<grid(order), CL_T, 0, s>>>(t.elem.as<uint64_t>(), order, lists.as<uint64_t>(), capq,
+  k_cl_cands<N><<<grid(order), CL_T, 0, s>>>(order, lists.as<uint64_t>(), capq,
                                              cnt.as<unsigned long long>(), ovf.as<int>());
   launches++;
   clk(cudaGetLastError(), "candidates");
@@ -873,9 +872,9 @@ int clifford_element(CliffordContext *c, int n, const uint64_t *index, size_t co
     c->tmp.ensure(count * 8); c->pk.ensure(count * 8);
     clk(cudaMemcpyAsync(c->tmp.p, index, count * 8, cudaMemcpyHostToDevice, c->s), "h2d");
     const unsigned g = c->grid(count);
-    if (n == 1) k_cl_elem<1><<<g, CL_T, 0, c->s>>>(c->tmp.as<uint64_t>(), count, t.order, t.elem.as<uint64_t>(), c->pk.as<uint64_t>());
-    else if (n == 2) k_cl_elem<2><<<g, CL_T, 0, c->s>>>(c->tmp.as<uint64_t>(), count, t.order, t.elem.as<uint64_t>(), c->pk.as<uint64_t>());
-    else k_cl_elem<3><<<g, CL_T, 0, c->s>>>(c->tmp.as<uint64_t>(), count, t.order, t.elem.as<uint64_t>(), c->pk.as<uint64_t>());
+    if (n == 1) k_cl_elem<1><<<g, CL_T, 0, c->s>>>(c->tmp.as<uint64_t>(), count, t.order, c->pk.as<uint64_t>());
+    else if (n == 2) k_cl_elem<2><<<g, CL_T, 0, c->s>>>(c->tmp.as<uint64_t>(), count, t.order, c->pk.as<uint64_t>());
+    else k_cl_elem<3><<<g, CL_T, 0, c->s>>>(c->tmp.as<uint64_t>(), count, t.order, c->pk.as<uint64_t>());
     c->launches++;
     clk(cudaGetLastError(), "element");
     clk(cudaMemcpyAsync(tabp, c->pk.p, count * 8, cudaMemcpyDeviceToHost, c->s), "d2h");

@@ -118,6 +118,14 @@ struct BatchJob {
   bool plain = false;                  // ran through Engine::search
 };
 
+// Launch and chunking parameters of a batch step (the batched search's tunables): survivor records a chunk of jobs
+// may plan for, expand blocks per SM (a persistent grid over a work counter) and deferred-T blocks per SM.
+struct BatchTuning {
+  size_t chunk_bytes = (size_t)8 << 30;
+  int expand_blocks_per_sm = 16;
+  int tbound_blocks_per_sm = 4;
+};
+
 class BatchSession {
  public:
   BatchSession(Engine &engine, int nq);
@@ -142,9 +150,19 @@ class BatchSession {
   // wait a step, their nodes carried over
   void set_memory_budget(size_t bytes);
   long long waits() const;             // job-steps spent waiting for memory
+  void set_tuning(const BatchTuning &t);
+  BatchTuning tuning() const;
   struct Impl;
  private:
   Impl *impl_;
 };
+
+// A project-written autotuner for batch sessions: every candidate tuning of a fixed search space is timed on the
+// same probe jobs (fresh sessions on `engine`, host wall time from the first submit to the last job's end), one
+// parameter at a time from the defaults (coordinate descent: chunk budget, then expand blocks, then deferred-T
+// blocks). Returns the fastest; times[i] (may be null) receives each probe run's seconds in the order tried.
+struct TuneTrial { BatchTuning t; double seconds; };
+BatchTuning autotune_batch(Engine &engine, int nq, const std::vector<const HostSpec *> &probe, const Options &opt,
+                           std::vector<TuneTrial> *trials);
 
 }  // namespace cz

@@ -42,6 +42,8 @@ namespace {
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int RC_STOP = -3;        // levels(): stopped after the requested level
 constexpr int EXP_WARPS = 8;       // warps per expand block
+constexpr int EXP_MINB = 4;        // expand blocks per SM: 32 warps (64 registers; latency-bound code, measured
+                                   // 6 % faster than 2 blocks of 128 registers despite small spills)
 constexpr int INHERIT_KMAX = 60;
 enum GateKind : uint8_t { GK_GENERAL = 0, GK_ONEQ = 1, GK_PERM = 2 };   // the T bound is computed exactly (mod 2^32 / 2^64) only while 2(n + k) <= 128
 
@@ -116,6 +118,16 @@ struct GoalShort {
   unsigned int ovf, pad;
 };
 constexpr unsigned GOAL_LIST = 1u << 16;
+
+// ---------------- asynchronous copies (cp.async: global -> shared, 16 bytes, bypassing registers) ----------------
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int K> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(K) : "memory");
+}
 
 // ---------------- arithmetic helpers ----------------
 template <typename ST> __device__ __forceinline__ bool zz(const Z4<ST> &x) { return !(x.a | x.b | x.c | x.d); }
@@ -210,7 +222,7 @@ __device__ __forceinline__ void tbound_round(const Z4<ST> *S, int f, U &P, U &Q)
     }
   }
 }
-template <int NQ, typename U, int PASSES, typename ST, bool SPLIT = true>
+template <int NQ, typename U, int PASSES, typename ST, bool SPLIT = false>
 __device__ __forceinline__ int tbound_lanes(const Z4<ST> *S, int k, int lane) {
   constexpr int E = 1 << (2 * NQ);
   U P = 0, Q = 0;
@@ -969,6 +981,7 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
     c.dead += __popc(__ballot_sync(FULL, fate == 3));
     full |= (unsigned long long)__ballot_sync(FULL, fate == 4) << g0;
   }
+  const bool need_b = sp.standard != 0 && !sp.states;
   for (; full; full &= full - 1) {
     const int g = __ffsll((long long)full) - 1;
     const uint8_t fl = sp.gflags[g];
@@ -977,7 +990,6 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
     c.full++;
     const int k = warp_child<NQ, ST>(P, C, g, kP, sp, sps, lane, ovf);
     if (ovf) { c.ovf = true; continue; }
-    const bool need_b = sp.standard != 0 && !sp.states;
     const bool need_hs = need_b && !(fl & GF_MONAFF);
     // the child is the goal only if the parent equals the gate, i.e. acts on no other qubit (unitary targets)
     const Cheap ch = warp_cheap<NQ, ST>(C, k, sp, lane, (ntP & ~gm) == 0 || !need_b, need_hs, need_b ? gm : 0, ntP);
@@ -1110,7 +1122,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32) k_goal_level(const DevSpec sp,
 }
 
 template <int NQ, typename ST, bool STATES = false>
-__global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand(const DevSpec sp, const ExpandArgs<ST> a) {
+__global__ void __launch_bounds__(EXP_WARPS * 32, EXP_MINB) k_expand(const DevSpec sp, const ExpandArgs<ST> a) {
   constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
   if (a.gshort && a.gshort->found && !a.gshort->ovf && a.gshort->count <= GOAL_LIST) return;   // the found level
   __shared__ ExpandSmem<NQ, ST> sm;
@@ -1236,7 +1248,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32) k_goal_level_batch(const DevSp
 }
 
 template <int NQ, typename ST>
-__global__ void __launch_bounds__(EXP_WARPS * 32, 2) k_expand_batch(const BatchArgs<ST> a) {
+__global__ void __launch_bounds__(EXP_WARPS * 32, EXP_MINB) k_expand_batch(const BatchArgs<ST> a) {
   constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
   __shared__ Z4<ST> sP[EXP_WARPS][E], sC[EXP_WARPS][E];
   __shared__ uint64_t W[E];
@@ -1328,26 +1340,51 @@ template <typename ST> struct TBoundArgs {
 };
 template <int NQ, typename ST>
 __global__ void __launch_bounds__(TB_WARPS * 32) k_tbound(const __grid_constant__ DevSpec sp0, const TBoundArgs<ST> a) {
-  constexpr int N = 1 << NQ, E = N * N;
-  __shared__ Z4<ST> sP[TB_WARPS][E], sC[TB_WARPS][E];
+  constexpr int N = 1 << NQ, E = N * N, CHUNKS = E * (int)sizeof(Z4<ST>) / 16;
+  constexpr int NB = sizeof(ST) == 4 ? 2 : 1;            // int64 limbs: one buffer (shared memory), no overlap
+  __shared__ __align__(16) Z4<ST> sP[TB_WARPS][NB][E];  // the entry's parent, and the next entry's arriving
+  __shared__ Z4<ST> sC[TB_WARPS][E];
   __shared__ uint64_t W[E];
   __shared__ DevSpec sps[TB_WARPS];
   init_weights(W, E);
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  Z4<ST> *P = sP[w], *C = sC[w];
+  Z4<ST> *C = sC[w];
   DevSpec &sp = sps[w];
   const unsigned long long n = a.st->n_tq < a.tqcap ? a.st->n_tq : a.tqcap;
   WarpTally c;
   int job = -2, rem = a.rem;
   bool keep = a.keep != 0;
   unsigned conjmask = 0;
-  for (;;) {
+  // entries are taken one ahead: the next entry's parent residual is copied into shared memory asynchronously
+  // (cp.async) while the current entry's T bound runs
+  auto take = [&](TQEntry &q, int b) {
     unsigned long long e = 0;
     if (lane == 0) e = atomicAdd(&a.st->tq_work, 1ULL);
     e = __shfl_sync(FULL, e, 0);
-    if (e >= n) break;
-    const TQEntry q = a.tq[e];
+    if (e >= n) return false;
+    q = a.tq[e];
+    const char *src = (const char *)(a.R + q.p * (unsigned long long)E);
+    char *dst = (char *)sP[w][b];
+    for (int i = lane; i < CHUNKS; i += 32) cp_async16(dst + 16 * i, src + 16 * i);
+    return true;
+  };
+  TQEntry q;
+  int b = 0;
+  bool have = take(q, 0);
+  cp_async_commit();
+  while (have) {
+    TQEntry q2;
+    bool more = false;
+    if constexpr (NB == 2) {
+      more = take(q2, b ^ 1);
+      cp_async_commit();
+      cp_async_wait<1>();                            // this entry's parent has arrived (the next may be in flight)
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncwarp();
+    const Z4<ST> *P = sP[w][b];
     const int pj = a.fjob ? (int)a.fjob[q.p] : -1;
     if (pj != job) {                                 // the spec of this entry's job (or the search's)
       if (job >= 0) c.flush(a.jst + job, lane);
@@ -1363,7 +1400,10 @@ __global__ void __launch_bounds__(TB_WARPS * 32) k_tbound(const __grid_constant_
     const NodeMeta pm = a.meta[q.p];
     int T = 0;
     for (int s2 = 0; s2 < q.n; s2++) {
-      warp_materialize<NQ, ST>(a.R, a.meta, q.p * (unsigned long long)a.GS + q.g[s2], a.GS, sp, &sp, P, C, lane);
+      bool ovf;
+      __syncwarp();
+      (void)warp_child<NQ, ST>(P, C, q.g[s2], pm.k, sp, &sp, lane, ovf);   // the level kernel's child residual
+      __syncwarp();
       if (s2 == 0) { T = ptm_bound<NQ, ST>(C, q.k, lane); c.teval++; }
       bool alive;
       if (sp.lite) alive = q.k + (T + sp.tdiv - 1) / sp.tdiv <= rem;
@@ -1390,7 +1430,16 @@ __global__ void __launch_bounds__(TB_WARPS * 32) k_tbound(const __grid_constant_
       }
       __syncwarp();
     }
+    __syncwarp();                                    // every lane is done with this buffer before it is refilled
+    if constexpr (NB == 1) {
+      more = take(q2, 0);
+      cp_async_commit();
+    }
+    have = more;
+    q = q2;
+    b ^= NB - 1;
   }
+  cp_async_wait<0>();
   if (a.fjob) { if (job >= 0) c.flush(a.jst + job, lane); }
   else c.flush(a.st, lane);
 }
@@ -3683,6 +3732,7 @@ struct BatchSession::Impl {
   virtual size_t projected_bytes() const = 0;
   virtual void set_budget(size_t bytes) = 0;
   virtual long long waits() const = 0;
+  BatchTuning tune;
 };
 
 namespace {
@@ -3933,7 +3983,7 @@ struct BatchImpl : BatchSession::Impl {
     nlaunch++;
     const size_t rec = 40 + 36;                                          // survivor record + its sort entries
     const size_t node = E * sizeof(Z4<ST>) + sizeof(NodeMeta) + 4 + 5;     // frontier node + its tree entry
-    const unsigned long long cap_limit = ((unsigned long long)8 << 30) / rec;
+    const unsigned long long cap_limit = std::max<unsigned long long>(1 << 16, tune.chunk_bytes / rec);
     // the plan, in frontier (= id) order: chunks of advancing jobs whose expected survivors fit the survivor
     // budget, and runs of waiting jobs carried over unchanged. A job advances while the step's planned memory (this
     // frontier, the next one, survivor room) stays under the session budget; the first job always advances.
@@ -4062,14 +4112,14 @@ struct BatchImpl : BatchSession::Impl {
         a.tq = tq.as<TQEntry>(); a.tqcap = tqcap;
         a.gshort = gsd; a.jgoal = jg;
         const long long want = (cm + EXP_WARPS - 1) / EXP_WARPS;
-        const long long grid = std::max<long long>(1, std::min<long long>(want, (long long)nsm * 2 * 8));
+        const long long grid = std::max<long long>(1, std::min<long long>(want, (long long)nsm * tune.expand_blocks_per_sm));
         k_expand_batch<NQ, ST><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(a);
         TBoundArgs<ST> tb;
         tb.R = fR.as<Z4<ST>>(); tb.meta = fMeta.as<NodeMeta>(); tb.tq = tq.as<TQEntry>(); tb.tqcap = tqcap;
         tb.GS = BATCH_GS; tb.rem = 0; tb.keep = 0; tb.fjob = fJob.as<uint32_t>(); tb.specs = dspecs.as<DevSpec>();
         tb.jt = jt.as<int>(); tb.jst = jst.as<DevStats>(); tb.st = dst; tb.cap = cap; tb.sh1 = sH1.as<uint64_t>();
         tb.sh2 = sH2.as<uint64_t>(); tb.sidx = sIdx.as<uint64_t>(); tb.smeta = sMeta.as<NodeMeta>();
-        k_tbound<NQ, ST><<<(unsigned)nsm * 4, TB_WARPS * 32, 0, s>>>(DevSpec{}, tb);
+        k_tbound<NQ, ST><<<(unsigned)(nsm * tune.tbound_blocks_per_sm), TB_WARPS * 32, 0, s>>>(DevSpec{}, tb);
         nlaunch += 2;
         ck(cudaGetLastError(), "batched expand");
         ck(cudaMemcpyAsync(&h, dst, sizeof(DevStats), cudaMemcpyDeviceToHost, s), "d2h");
@@ -4282,6 +4332,42 @@ long long BatchSession::steps() const { return impl_->steps(); }
 size_t BatchSession::device_bytes() const { return impl_->device_bytes(); }
 size_t BatchSession::projected_bytes() const { return impl_->projected_bytes(); }
 void BatchSession::set_memory_budget(size_t bytes) { impl_->set_budget(bytes); }
+void BatchSession::set_tuning(const BatchTuning &t) { impl_->tune = t; }
+BatchTuning BatchSession::tuning() const { return impl_->tune; }
+
+BatchTuning autotune_batch(Engine &engine, int nq, const std::vector<const HostSpec *> &probe, const Options &opt,
+                           std::vector<TuneTrial> *trials) {
+  // the search space, committed here: chunk budget (bytes of survivor records per chunk of jobs), expand blocks per
+  // SM, deferred-T blocks per SM; the defaults first in each list
+  static const size_t chunk_space[] = {(size_t)8 << 30, (size_t)1 << 30, (size_t)2 << 30, (size_t)4 << 30};
+  static const int expand_space[] = {16, 4, 8, 32};
+  static const int tbound_space[] = {4, 1, 2, 8};
+  auto run = [&](const BatchTuning &t) {
+    BatchSession b(engine, nq);
+    b.set_tuning(t);
+    const double t0 = now_s();
+    for (const HostSpec *hs : probe) b.submit(*hs, opt);
+    while (b.step() > 0) {}
+    const double sec = now_s() - t0;
+    if (trials) trials->push_back({t, sec});
+    return sec;
+  };
+  BatchTuning best;
+  run(best);                                      // warm-up: device buffers grown, spec tables uploaded
+  if (trials) trials->clear();
+  double best_s = run(best);
+  for (int dim = 0; dim < 3; dim++) {
+    for (int i = 1; i < 4; i++) {
+      BatchTuning t = best;
+      if (dim == 0) t.chunk_bytes = chunk_space[i];
+      else if (dim == 1) t.expand_blocks_per_sm = expand_space[i];
+      else t.tbound_blocks_per_sm = tbound_space[i];
+      const double sec = run(t);
+      if (sec < best_s) { best_s = sec; best = t; }
+    }
+  }
+  return best;
+}
 long long BatchSession::waits() const { return impl_->waits(); }
 
 }  // namespace cz

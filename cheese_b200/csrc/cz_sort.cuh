@@ -166,7 +166,7 @@ __device__ __forceinline__ uint32_t os_block_scan(uint32_t v, uint32_t *ws) {
   return r;
 }
 
-__global__ void __launch_bounds__(OS_THREADS) k_sort_onesweep(const uint64_t *kin, const uint32_t *vin, uint64_t *kout,
+__global__ void __launch_bounds__(OS_THREADS, 4) k_sort_onesweep(const uint64_t *kin, const uint32_t *vin, uint64_t *kout,
                                                                uint32_t *vout, size_t n, int shift, int pass,
                                                                uint32_t *head, unsigned long long *status,
                                                                unsigned *err) {

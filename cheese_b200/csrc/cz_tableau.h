@@ -211,6 +211,67 @@ struct Tb {
     }
     return r * (1u << (2 * N)) + signs;
   }
+  // the element of rank r (the inverse of rank): the digits give, qubit by qubit from the last, the images A of X_i
+  // and B of Z_i in the remaining space; the rows found for the later qubits are put back into that space (a zero
+  // inserted for the qubit) and the rank's transvections for (A, B), which are involutions, are undone in reverse.
+  CZ_HD static uint64_t unrank(uint32_t r) {
+    const uint32_t signs = r & ((1u << (2 * N)) - 1);
+    r >>= 2 * N;
+    uint32_t d[N];
+    for (int i = N - 1; i >= 0; i--) {
+      const int m = N - i;
+      const uint32_t R = ((1u << (2 * m)) - 1) * (1u << (2 * m - 1));
+      d[i] = r % R;
+      r /= R;
+    }
+    uint32_t v[ROWS];
+    for (int i = N - 1; i >= 0; i--) {
+      const int m = N - i;
+      const uint32_t full = (1u << (2 * m)) - 1, nb = 1u << (2 * m - 1), e = 1u, f = 1u << m;
+      const uint32_t A = d[i] / nb + 1, ib = d[i] % nb;
+      const uint32_t u = ((A >> m) | (A << m)) & full;
+      const int p = tb_ctz(u);
+      uint32_t B = ((ib >> p) << (p + 1)) | (ib & ((1u << p) - 1));
+      if (symp(A, B, m) != 1) B |= 1u << p;            // bit p of B flips <A, B>
+      // the transvections the rank applies for (A, B), replayed on (A, B) to find them
+      uint32_t h[4];
+      int nh = 0;
+      uint32_t b = B;
+      auto tv = [&](uint32_t x) { b ^= symp(b, x, m) ? x : 0u; h[nh++] = x; };
+      if (A != e) {
+        if ((A >> m) & 1u) {
+          tv(A ^ e);
+        } else {
+          uint32_t w = f;
+          if (!(A & 1u)) {
+            const uint32_t supp = ((A | (A >> m)) & ((1u << m) - 1)) & ~1u;
+            const int j = tb_ctz(supp);
+            w ^= ((A >> j) & 1u) ? (1u << (m + j)) : (1u << j);
+          }
+          tv(A ^ w);
+          tv(w ^ e);
+        }
+      }
+      if (b != f) {
+        if (!(b & 1u)) tv(e);
+        tv(b ^ f);
+      }
+      const uint32_t km = (1u << (m - 1)) - 1;
+      for (int j = 2 * i + 2; j < ROWS; j++) {
+        const uint32_t x = v[j];
+        v[j] = ((x & km) << 1) | (((x >> (m - 1)) & km) << (m + 1));
+        for (int t = nh - 1; t >= 0; t--) v[j] ^= symp(v[j], h[t], m) ? h[t] : 0u;
+      }
+      v[2 * i] = A;
+      v[2 * i + 1] = B;
+    }
+    uint64_t T = 0;
+    for (int i = 0; i < N; i++) {
+      T |= (uint64_t)(v[2 * i] | (((signs >> i) & 1u) << SB)) << (i * RB);
+      T |= (uint64_t)(v[2 * i + 1] | (((signs >> (N + i)) & 1u) << SB)) << ((N + i) * RB);
+    }
+    return T;
+  }
 };
 
 }  // namespace cz

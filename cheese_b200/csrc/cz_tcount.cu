@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(TC_T) k_tc_keys(const TDev sp, const THist H, 
 
 // child o = parent i * G + (p - 1): parent i of level tp, peeled by rotation p. With pmx, each parent's matrix and
 // exponent are kept (2 P^2 ints at pmx + 2 P^2 i, pe[i]) so the exact dedupe rebuilds a child with one peel.
-__global__ void __launch_bounds__(TC_T) k_tc_children(const TDev sp, const THist H, int tp, long long m, uint64_t *k1o,
+__global__ void __launch_bounds__(TC_T, 2) k_tc_children(const TDev sp, const THist H, int tp, long long m, uint64_t *k1o,
                                                       uint64_t *k2o, int *ovf, int *pmx, int *pe) {
   const TSm s = tsm_carve(sp.P);
   const int G = sp.G, PP = sp.P * sp.P;

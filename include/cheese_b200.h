@@ -139,6 +139,22 @@ int cz_batch_step(cz_batch *batch, int *running);
 /* the message of the last failed cz_batch_step ("" if none) */
 const char *cz_batch_error(const cz_batch *batch);
 int cz_batch_info_get(const cz_batch *batch, cz_batch_info *out);
+/* The batch step's tunables: survivor-record bytes a chunk of jobs may plan for, expand blocks per SM, deferred
+ * T-bound blocks per SM (defaults 8 GiB, 16, 4). Results do not depend on them, only the time. */
+typedef struct {
+  int64_t chunk_bytes;
+  int expand_blocks_per_sm, tbound_blocks_per_sm;
+  int trials;                       /* cz_batch_autotune: probe runs timed */
+  double trial_seconds[16];         /* their host wall times, in the order tried */
+  double best_seconds;              /* the chosen tuning's probe time */
+} cz_batch_tuning;
+int cz_batch_set_tuning(cz_batch *batch, const cz_batch_tuning *t);
+/* The autotuner (no counterpart in the reference): times every candidate of a fixed search space on the probe jobs
+ * (nprobe specs of qubit count nq, each run to its end in a fresh session on the engine; chunk budget {8, 1, 2, 4}
+ * GiB, expand blocks per SM {16, 4, 8, 32}, deferred-T blocks per SM {4, 1, 2, 8}, one parameter at a time from the
+ * defaults) and writes the fastest to *out, with the probe times. Apply it with cz_batch_set_tuning. */
+int cz_batch_autotune(cz_engine *engine, int nq, const cz_spec *const *probe, int nprobe, const cz_options *opt,
+                      cz_batch_tuning *out);
 /* 1 when the job has finished. */
 int cz_batch_done(const cz_batch *batch, int job);
 /* A finished job: its level lines through on_level (in order) and its result, as cz_search gives them. */

@@ -122,3 +122,23 @@ def test_session_info(eng):
     b.run()
     info = b.info()
     assert info["running"] == 0 and info["steps"] >= 1 and info["kernel_launches"] > 0
+
+
+def test_tuning_changes_time_not_results(eng):
+    """the autotuner returns a tuning from its search space, and sessions run under extreme tunings (small chunks,
+    few or many blocks) give the plain path's results"""
+    import cheese_b200 as cz
+    jobs = [(n, s) for n, s in _jobs(23, 40) if n == 3]
+    t = cz.autotune(eng, 3, [s for _, s in jobs[:8]])
+    assert t.chunk_bytes in (8 << 30, 1 << 30, 2 << 30, 4 << 30)
+    assert t.expand_blocks_per_sm in (16, 4, 8, 32) and t.tbound_blocks_per_sm in (4, 1, 2, 8)
+    assert t.trials == 10 and t.best_seconds > 0
+    plain = [_plain(eng, s) for _, s in jobs]
+    for chunk, eb, tb in ((1 << 20, 1, 1), (1 << 30, 32, 8)):
+        b = cz.Batch(eng, 3)
+        b.set_tuning(cz.BatchTuning(chunk, eb, tb, 0, (0.0,) * 16, 0.0))
+        ids = [b.submit(s) for _, s in jobs]
+        b.run()
+        for i, p in zip(ids, plain):
+            _same(b.result(i), p)
+        b.close()
