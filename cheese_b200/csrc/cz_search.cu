@@ -323,7 +323,7 @@ template <typename ST> __device__ __forceinline__ uint32_t to_fp(const Z4<ST> &x
 // eliminated side by side, one column per lane: per row a ballot finds the group's pivot column, and the rows
 // below are reduced by it. Returns the bound and packs the child's needs (2 bits per cut) into needs_out.
 template <int NQ, typename ST>
-__device__ __noinline__ int warp_cx_bound(const Z4<ST> *S, const DevSpec &sp, int lane, int gmask, int needs_in,
+__device__ __forceinline__ int warp_cx_bound(const Z4<ST> *S, const DevSpec &sp, int lane, int gmask, int needs_in,
                                           int &needs_out) {
   constexpr int N = 1 << NQ, CC = N * N / 4 > 0 ? N * N / 4 : 1, SLOTS = 32 / CC, ALLQ = N - 1;
   static_assert(NQ <= 3, "cuts of one qubit: 4 x E/4 matrices within a warp");
@@ -808,7 +808,7 @@ template <typename ST> __device__ __forceinline__ void entry_hash(const Z4<ST> &
   hb = fmix32(lo1 + (hi ^ 0x1b873593u));
 }
 template <int NQ, typename ST>
-__device__ __noinline__ void warp_class_key(const Z4<ST> *S, int k, int nsym, unsigned conjmask, const uint8_t (*perm)[8],
+__device__ __forceinline__ void warp_class_key(const Z4<ST> *S, int k, int nsym, unsigned conjmask, const uint8_t (*perm)[8],
                                             const uint64_t *W, int lane, uint64_t &k1, uint64_t &k2) {
   constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
   static_assert(SYMMAX <= 16, "the reduce-scatter holds 16 elements x (A, B)");
@@ -3537,7 +3537,8 @@ int Engine::sort_pairs(uint64_t *keys, uint32_t *vals, size_t n, int lo, int hi,
     Impl &I = *impl_;
     I.k1.ensure(n * 8 + 8); I.v1.ensure(n * 4 + 4);
     I.hist.ensure(sort_hist_words(n) * 4);
-    SortScratch sc{I.hist.as<uint32_t>(), nullptr, I.hist.cap / 4, 0};
+    I.part.ensure(scan_partials_words(sort_hist_words(n)) * 4);
+    SortScratch sc{I.hist.as<uint32_t>(), I.part.as<uint32_t>(), I.hist.cap / 4, I.part.cap / 4};
     ck(cudaEventRecord(I.ev[0], I.s), "event");
     int nl = 0;
     const bool f = radix_sort(keys, vals, I.k1.as<uint64_t>(), I.v1.as<uint32_t>(), n, lo, hi, sc, I.s, &nl);
@@ -3548,11 +3549,12 @@ int Engine::sort_pairs(uint64_t *keys, uint32_t *vals, size_t n, int lo, int hi,
       ck(cudaMemcpyAsync(vals, I.v1.p, n * 4, cudaMemcpyDeviceToDevice, I.s), "d2d");
     }
     ck(cudaGetLastError(), "sort");
-    const bool failed = sort_failed(sc, I.s);
+    const uint32_t flags = sort_failed(sc, I.s);
     float t = 0;
     ck(cudaEventElapsedTime(&t, I.ev[0], I.ev[1]), "event");
     if (ms) *ms = t;
-    if (failed) { err = "a look-back wait gave up (the result is exact; the predecessors were counted directly)"; }
+    if (flags & 2u) { err = "the keys changed while they were sorted (order the buffers before the call)"; return RC_CUDA; }
+    if (flags & 1u) err = "a look-back wait gave up (the result is exact; the predecessors were counted directly)";
   } catch (const CudaError &e) {
     err = e.what();
     return RC_CUDA;

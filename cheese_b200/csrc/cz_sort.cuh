@@ -124,6 +124,7 @@ constexpr int OS_MAXPASS = 8;
 constexpr long long OS_SPIN_MAX = 1LL << 26;
 constexpr size_t OS_HEAD_WORDS = 256 * OS_MAXPASS + 16;   // digit counts per pass, tickets per pass, error flag
 constexpr unsigned long long OS_VALUE = (1ULL << 58) - 1;
+constexpr size_t OS_SCAN_MIN = (size_t)1 << 22;     // sorts of at least this many keys take the scan path
 
 inline size_t sort_tiles(size_t n) { return (n + OS_TILE - 1) / OS_TILE; }
 // 32-bit words of sort scratch for n keys (header + one 64-bit status word per tile and digit)
@@ -141,6 +142,21 @@ __global__ void __launch_bounds__(256) k_sort_upsweep(const uint64_t *keys, size
   __syncthreads();
   for (int p = 0; p < npass; p++)
     if (h[p][threadIdx.x]) atomicAdd(&counts[p * 256 + threadIdx.x], h[p][threadIdx.x]);
+}
+
+// per-tile digit counts of one pass, digit-major (hist[d * ntiles + tile]), tiles of OS_TILE keys
+__global__ void __launch_bounds__(256) k_sort_tilehist(const uint64_t *keys, size_t n, int shift, uint32_t *hist,
+                                                       uint32_t ntiles) {
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const size_t base = (size_t)blockIdx.x * OS_TILE;
+  for (int i = threadIdx.x; i < OS_TILE; i += 256) {
+    const size_t j = base + i;
+    if (j < n) atomicAdd(&h[(keys[j] >> shift) & 255], 1u);
+  }
+  __syncthreads();
+  hist[(size_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
 }
 
 __device__ __forceinline__ unsigned long long os_load(const unsigned long long *p) {
@@ -166,10 +182,11 @@ __device__ __forceinline__ uint32_t os_block_scan(uint32_t v, uint32_t *ws) {
   return r;
 }
 
-__global__ void __launch_bounds__(OS_THREADS, 4) k_sort_onesweep(const uint64_t *kin, const uint32_t *vin, uint64_t *kout,
+template <bool LOOKBACK>
+__global__ void __launch_bounds__(OS_THREADS, 5) k_sort_onesweep(const uint64_t *kin, const uint32_t *vin, uint64_t *kout,
                                                                uint32_t *vout, size_t n, int shift, int pass,
                                                                uint32_t *head, unsigned long long *status,
-                                                               unsigned *err) {
+                                                               unsigned *err, const uint32_t *offs, uint32_t ntiles) {
   constexpr int NW = OS_THREADS / 32;
   __shared__ uint64_t sk[OS_TILE];
   __shared__ uint32_t sv[OS_TILE];
@@ -180,7 +197,7 @@ __global__ void __launch_bounds__(OS_THREADS, 4) k_sort_onesweep(const uint64_t 
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const uint32_t *counts = head + pass * 256;
   unsigned *tickets = head + 256 * OS_MAXPASS;
-  if (tid == 0) { ticket = atomicAdd(&tickets[pass], 1u); fallback = 0; }
+  if (tid == 0) { ticket = LOOKBACK ? atomicAdd(&tickets[pass], 1u) : blockIdx.x; fallback = 0; }
   cnt[tid] = 0;
   for (int x = 0; x < NW; x++) wcnt[x][tid] = 0;
   __syncthreads();
@@ -201,43 +218,46 @@ __global__ void __launch_bounds__(OS_THREADS, 4) k_sort_onesweep(const uint64_t 
     }
   }
   __syncthreads();
-  // this tile's count of digit tid: publish it, then add up the earlier tiles' counts by looking back
   const uint32_t mine = cnt[tid];
-  unsigned long long *st = status + tile * 256 + tid;
-  unsigned long long before = 0;
-  bool ok = true;
-  if (tile == 0) {
-    os_store(st, tag | (2ULL << 58) | mine);
-  } else {
-    os_store(st, tag | (1ULL << 58) | mine);
-    for (long long j = (long long)tile - 1; j >= 0 && ok; j--) {
-      const unsigned long long *q = status + (size_t)j * 256 + tid;
-      unsigned long long v = os_load(q);
-      long long spins = 0;
-      while ((v >> 60) != (tag >> 60) && ++spins < OS_SPIN_MAX) {
-        __nanosleep(64);
-        v = os_load(q);
+  if constexpr (LOOKBACK) {
+    // this tile's count of digit tid: publish it, then add up the earlier tiles' counts by looking back
+    unsigned long long *st = status + tile * 256 + tid;
+    unsigned long long before = 0;
+    bool ok = true;
+    if (tile == 0) {
+      os_store(st, tag | (2ULL << 58) | mine);
+    } else {
+      os_store(st, tag | (1ULL << 58) | mine);
+      for (long long j = (long long)tile - 1; j >= 0 && ok; j--) {
+        const unsigned long long *q = status + (size_t)j * 256 + tid;
+        unsigned long long v = os_load(q);
+        long long spins = 0;
+        while ((v >> 60) != (tag >> 60) && ++spins < OS_SPIN_MAX) {
+          __nanosleep(64);
+          v = os_load(q);
+        }
+        if ((v >> 60) != (tag >> 60)) { ok = false; break; }
+        before += v & OS_VALUE;
+        if (((v >> 58) & 3) == 2) break;
       }
-      if ((v >> 60) != (tag >> 60)) { ok = false; break; }
-      before += v & OS_VALUE;
-      if (((v >> 58) & 3) == 2) break;
     }
+    if (!ok) { atomicOr(err, 1u); fallback = 1; }
+    __syncthreads();
+    if (fallback) {                               // a wait gave up: count the earlier tiles' digits directly
+      run[tid] = 0;
+      __syncthreads();
+      for (size_t i = tid; i < start; i += OS_THREADS) atomicAdd(&run[(kin[i] >> shift) & 255], 1u);
+      __syncthreads();
+      before = run[tid];
+      __syncthreads();
+    }
+    if (tile != 0) os_store(st, tag | (2ULL << 58) | ((before + mine) & OS_VALUE));
+    // output base of digit tid for this tile: keys of smaller digits (all tiles) + this digit's in earlier tiles
+    const uint32_t dex = os_block_scan(counts[tid], ws);
+    gbase[tid] = (unsigned long long)dex + before;
+  } else {
+    gbase[tid] = offs[(size_t)tid * ntiles + tile];   // the scanned digit-major tile histograms
   }
-  if (!ok) { atomicOr(err, 1u); fallback = 1; }
-  __syncthreads();
-  if (fallback) {                                 // a wait gave up: count the earlier tiles' digits directly
-    run[tid] = 0;
-    __syncthreads();
-    for (size_t i = tid; i < start; i += OS_THREADS) atomicAdd(&run[(kin[i] >> shift) & 255], 1u);
-    __syncthreads();
-    before = run[tid];
-    __syncthreads();
-  }
-  if (tile != 0) os_store(st, tag | (2ULL << 58) | ((before + mine) & OS_VALUE));
-  // output base of digit tid for this tile: keys of smaller digits (all tiles) + this digit's keys in earlier tiles
-  const uint32_t dtotal = counts[tid];
-  const uint32_t dex = os_block_scan(dtotal, ws);
-  gbase[tid] = (unsigned long long)dex + before;
   const uint32_t lx = os_block_scan(mine, ws);
   lex[tid] = lx;
   run[tid] = lx;
@@ -267,14 +287,18 @@ __global__ void __launch_bounds__(OS_THREADS, 4) k_sort_onesweep(const uint64_t 
     const uint64_t k = sk[i];
     const int d = (int)((k >> shift) & 255);
     const unsigned long long pos = gbase[d] + (unsigned long long)(i - (int)lex[d]);
-    kout[pos] = k;
-    vout[pos] = sv[i];
+    if (pos < n) {                                // always, for a consistent input (nothing else writes the keys)
+      kout[pos] = k;
+      vout[pos] = sv[i];
+    } else {
+      atomicOr(err, 2u);
+    }
   }
 }
 
 struct SortScratch {
   uint32_t *hist = nullptr;       // sort scratch: sort_hist_words(n) words
-  uint32_t *partials = nullptr;   // unused by the sort (kept for the callers' scan buffers)
+  uint32_t *partials = nullptr;   // scan partials: scan_partials_words(sort_hist_words(n)) words (large sorts)
   size_t cap_hist = 0, cap_part = 0;
   uint32_t *err = nullptr;        // where a failed look-back is flagged (nullptr: the scratch's own word)
 };
@@ -286,33 +310,46 @@ inline bool radix_sort(uint64_t *k0, uint32_t *v0, uint64_t *k1, uint32_t *v1, s
   if (n <= 1 || hi <= lo) return false;
   const int npass = (hi - lo + 7) / 8;
   const size_t ntiles = sort_tiles(n);
-  cudaMemsetAsync(sc.hist, 0, (OS_HEAD_WORDS + 2 * 256 * ntiles) * 4, s);
+  const bool scan = n >= OS_SCAN_MIN && sc.partials && sc.cap_part >= scan_partials_words(256 * ntiles);
+  cudaMemsetAsync(sc.hist, 0, (OS_HEAD_WORDS + (scan ? 0 : 2 * 256 * ntiles)) * 4, s);
   unsigned long long *status = (unsigned long long *)(sc.hist + OS_HEAD_WORDS);
-  int dev = 0, nsm = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  const unsigned ub = (unsigned)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, (size_t)nsm * 8));
-  k_sort_upsweep<<<ub, 256, 0, s>>>(k0, n, lo, npass, sc.hist);
+  uint32_t *offs = sc.hist + OS_HEAD_WORDS;                  // scan path: the digit-major tile histograms
+  unsigned *err = sc.err ? sc.err : sc.hist + 256 * OS_MAXPASS + OS_MAXPASS;
+  if (!scan) {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned ub = (unsigned)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, (size_t)nsm * 8));
+    k_sort_upsweep<<<ub, 256, 0, s>>>(k0, n, lo, npass, sc.hist);
+  }
   bool flip = false;
   for (int p = 0; p < npass; p++) {
     const uint64_t *ki = flip ? k1 : k0;
     const uint32_t *vi = flip ? v1 : v0;
     uint64_t *ko = flip ? k0 : k1;
     uint32_t *vo = flip ? v0 : v1;
-    k_sort_onesweep<<<(unsigned)ntiles, OS_THREADS, 0, s>>>(ki, vi, ko, vo, n, lo + 8 * p, p, sc.hist, status,
-                                                             sc.err ? sc.err : sc.hist + 256 * OS_MAXPASS + OS_MAXPASS);
+    if (scan) {
+      k_sort_tilehist<<<(unsigned)ntiles, 256, 0, s>>>(ki, n, lo + 8 * p, offs, (uint32_t)ntiles);
+      exclusive_scan(offs, offs, 256 * ntiles, sc.partials, nullptr, s);
+      k_sort_onesweep<false><<<(unsigned)ntiles, OS_THREADS, 0, s>>>(ki, vi, ko, vo, n, lo + 8 * p, p, sc.hist, status,
+                                                                   err, offs, (uint32_t)ntiles);
+    } else {
+      k_sort_onesweep<true><<<(unsigned)ntiles, OS_THREADS, 0, s>>>(ki, vi, ko, vo, n, lo + 8 * p, p, sc.hist, status,
+                                                                  err, nullptr, 0);
+    }
     flip = !flip;
   }
-  if (launches) *launches += 1 + npass;
+  if (launches) *launches += scan ? 5 * npass : 1 + npass;
   return flip;
 }
-// true when a look-back wait of the last sort on this scratch gave up (the result is exact all the same: the tile
-// counted its predecessors' digits itself); synchronises the stream
-inline bool sort_failed(const SortScratch &sc, cudaStream_t s) {
+// the last sort's flags on this scratch (synchronises the stream): bit 0, a look-back wait gave up (the result is
+// exact all the same: the tile counted its predecessors' digits itself); bit 1, a scatter position fell outside the
+// array (the keys changed while the sort ran; those writes were skipped and the result is not to be used)
+inline uint32_t sort_failed(const SortScratch &sc, cudaStream_t s) {
   uint32_t e = 0;
-  cudaMemcpyAsync(&e, sc.hist + 256 * OS_MAXPASS + OS_MAXPASS, 4, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(&e, sc.err ? sc.err : sc.hist + 256 * OS_MAXPASS + OS_MAXPASS, 4, cudaMemcpyDeviceToHost, s);
   cudaStreamSynchronize(s);
-  return e != 0;
+  return e;
 }
 
 }  // namespace

@@ -251,9 +251,10 @@ int cz_int32_peak(cz_engine *engine, double *ops_per_s);
 
 /* No counterpart in the reference (its dedupe sorts with Thrust, src/cheese.cu:1335-1343). The frontier dedupe's
  * stable LSD radix sort on caller-held device buffers: n (key, value) pairs sorted in place by bits [lo, hi) of the
- * key (hi - lo a multiple of 8, hi <= 64), equal keys in their input order, on the engine's stream; returns once
- * sorted, with the sort's device time in *ms (may be NULL). The engine holds the ping-pong buffers (12 n bytes) and
- * the scratch. For tests and measurement of the dedupe at scale. */
+ * key (hi - lo a multiple of 8, hi <= 64), equal keys in their input order, on the engine's stream (cz_engine_stream:
+ * work that fills the buffers on another stream must be finished or ordered before the call); returns once sorted,
+ * with the sort's device time in *ms (may be NULL). The engine holds the ping-pong buffers (12 n bytes) and the
+ * scratch. For tests and measurement of the dedupe at scale. */
 int cz_sort_pairs(cz_engine *engine, uint64_t *d_keys, uint32_t *d_vals, size_t n, int lo, int hi, float *ms);
 
 /* ---------------- T-count (the reference's build/tcount, src/tcount.cu) ---------------- */

@@ -1,5 +1,6 @@
-"""The frontier dedupe's radix sort (cz_sort_pairs: one upsweep launch, then one launch per 8-bit digit pass with
-decoupled look-back) against a stable reference sort. The dedupe relies on stability (equal class keys keep the
+"""The frontier dedupe's radix sort (cz_sort_pairs) against a stable reference sort: below 2^22 keys one launch
+per 8-bit digit pass with decoupled look-back, from 2^22 keys per-tile histograms, a scan and the same staged
+scatter per pass. The dedupe relies on stability (equal class keys keep the
 order of their child indices) and on the bit ranges it sorts by: the top 32 bits of the class key, and the low
 bytes of the child index when the kept classes are put back in order."""
 import pytest
@@ -28,7 +29,8 @@ def stable_reference(keys, vals, lo, hi):
 
 @pytest.mark.parametrize("n,lo,hi,spread", [
     (2, 0, 64, 64), (2047, 32, 64, 64), (2048, 32, 64, 64), (2049, 32, 64, 64), (100000, 32, 64, 64),
-    (100000, 32, 64, 3), (300001, 0, 64, 64), (1 << 20, 0, 24, 24), (3 << 20, 32, 64, 9), (5000000, 32, 64, 64)])
+    (100000, 32, 64, 3), (300001, 0, 64, 64), (1 << 20, 0, 24, 24), (3 << 20, 32, 64, 9), (1 << 22, 32, 64, 12),
+    (5000000, 32, 64, 64), (9000001, 0, 40, 64)])
 def test_sort_matches_stable_reference(engine, n, lo, hi, spread):
     """few distinct keys (spread = random bits in the key) exercise long equal runs across many tiles"""
     import torch
@@ -39,6 +41,7 @@ def test_sort_matches_stable_reference(engine, n, lo, hi, spread):
     vals = torch.arange(n, dtype=torch.int32, device=dev)
     want_k, want_v = stable_reference(keys, vals, lo, hi)
     k, v = keys.clone(), vals.clone()
+    torch.cuda.synchronize()                  # the sort runs on the engine's stream, not torch's
     engine.sort_pairs(k.data_ptr(), v.data_ptr(), n, lo, hi)
     torch.cuda.synchronize()
     assert torch.equal(v, want_v)
