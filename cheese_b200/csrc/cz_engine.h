@@ -158,9 +158,10 @@ class BatchSession {
 };
 
 // A project-written autotuner for batch sessions: every candidate tuning of a fixed search space is timed on the
-// same probe jobs (fresh sessions on `engine`, host wall time from the first submit to the last job's end), one
-// parameter at a time from the defaults (coordinate descent: chunk budget, then expand blocks, then deferred-T
-// blocks). Returns the fastest; times[i] (may be null) receives each probe run's seconds in the order tried.
+// same probe jobs (one session on `engine`, warmed up by a first untimed run, the probe jobs submitted again for each
+// trial; host wall time from the first submit to the last job's end), one parameter at a time from the defaults
+// (coordinate descent: chunk budget, then expand blocks, then deferred-T blocks). Returns the fastest; trials (may
+// be null) receives each timed run's tuning and seconds in the order tried.
 struct TuneTrial { BatchTuning t; double seconds; };
 BatchTuning autotune_batch(Engine &engine, int nq, const std::vector<const HostSpec *> &probe, const Options &opt,
                            std::vector<TuneTrial> *trials);

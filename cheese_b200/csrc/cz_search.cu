@@ -21,9 +21,11 @@
 //   reference reads off entry by entry (cheese.cu:419-449);
 // * dedupe = stable LSD radix sort of survivor keys, run detection, exact class comparison inside runs (warp per
 //   run), then a radix sort of the kept indices restores lexicographic order and a gather builds the next level.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -1298,6 +1300,46 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, EXP_MINB) k_expand_batch(const
   if (job >= 0) c.flush(a.jst + job, lane);
 }
 
+// A chunk that holds one job: its spec is a kernel parameter, as in the plain level kernel (k_expand), so the level
+// code keeps that kernel's register allocation (the many-job kernel above reads the spec from shared memory and
+// spills at the same register limit); outputs, child indices and the job's tallies are the many-job kernel's.
+template <int NQ, typename ST>
+__global__ void __launch_bounds__(EXP_WARPS * 32, EXP_MINB) k_expand_solo(const DevSpec sp, const BatchArgs<ST> a,
+                                                                         int job) {
+  constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
+  if (a.gshort && !a.gshort->ovf && a.gshort->count <= GOAL_LIST && a.jgoal[job].x > 0) return;   // its found level
+  __shared__ ExpandSmem<NQ, ST> sm;
+  __shared__ DevSpec s_sp;
+  for (int i = threadIdx.x; i < (int)(sizeof(DevSpec) / 4); i += blockDim.x) ((int *)&s_sp)[i] = ((const int *)&sp)[i];
+  init_weights(sm.W, E);
+  for (int i = threadIdx.x; i < SYMMAX * 8; i += blockDim.x) sm.perm[i / 8][i % 8] = sp.symperm[i / 8][i % 8];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  Z4<ST> *P = sm.P[w], *C = sm.C[w];
+  unsigned conjmask = 0;
+  for (int i = 0; i < sp.nsym; i++) conjmask |= (unsigned)(sp.symconj[i] != 0) << i;
+  const int t = a.jt[job];
+  const ExpandOut<ST> o{a.st, a.cap, a.sh1, a.sh2, a.sidx, a.smeta, a.tq, a.tqcap};
+  WarpTally c;
+  for (;;) {
+    unsigned long long p = 0;
+    if (lane == 0) p = a.p0 + atomicAdd(&a.st->work, 1ULL);
+    p = __shfl_sync(FULL, p, 0);
+    if ((long long)p >= a.m) break;
+#pragma unroll
+    for (int j = 0; j < EPL; j++) {
+      const int e = lane + 32 * j;
+      if (e < E) P[e] = a.R[p * E + e];
+    }
+    const NodeMeta pm = a.meta[p];
+    __syncwarp();
+    expand_parent<NQ, ST>(sp, &s_sp, sm.perm, conjmask, sm.W, P, C, p, pm, sp.depth - t, t < sp.depth, BATCH_GS, o, c,
+                          lane);
+    __syncwarp();
+  }
+  c.flush(a.jst + job, lane);
+}
+
 // a survivor's residual: its parent (index sidx / GS in frontier R) times its gate g = sidx % GS, into C; P is the
 // warp's staging buffer. The same warp_child as the level kernel, so the result is the residual it evaluated.
 template <int NQ, typename ST>
@@ -1338,7 +1380,7 @@ template <typename ST> struct TBoundArgs {
   uint64_t *sh1, *sh2, *sidx;
   NodeMeta *smeta;
 };
-template <int NQ, typename ST>
+template <int NQ, typename ST, bool BATCHED = false>
 __global__ void __launch_bounds__(TB_WARPS * 32) k_tbound(const __grid_constant__ DevSpec sp0, const TBoundArgs<ST> a) {
   constexpr int N = 1 << NQ, E = N * N, CHUNKS = E * (int)sizeof(Z4<ST>) / 16;
   constexpr int NB = sizeof(ST) == 4 ? 2 : 1;            // int64 limbs: one buffer (shared memory), no overlap
@@ -1350,7 +1392,13 @@ __global__ void __launch_bounds__(TB_WARPS * 32) k_tbound(const __grid_constant_
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   Z4<ST> *C = sC[w];
-  DevSpec &sp = sps[w];
+  // the search's spec is copied to shared memory once; a batch's entries read their job's spec where it lies (the
+  // entries of a many-job chunk change job often, and the specs stay in cache)
+  if constexpr (!BATCHED) {
+    for (int i = lane; i < (int)(sizeof(DevSpec) / 4); i += 32) ((int *)&sps[w])[i] = ((const int *)&sp0)[i];
+    __syncwarp();
+  }
+  const DevSpec *spp = &sps[w];
   const unsigned long long n = a.st->n_tq < a.tqcap ? a.st->n_tq : a.tqcap;
   WarpTally c;
   int job = -2, rem = a.rem;
@@ -1385,18 +1433,19 @@ __global__ void __launch_bounds__(TB_WARPS * 32) k_tbound(const __grid_constant_
     }
     __syncwarp();
     const Z4<ST> *P = sP[w][b];
-    const int pj = a.fjob ? (int)a.fjob[q.p] : -1;
+    const int pj = BATCHED ? (int)a.fjob[q.p] : -1;
     if (pj != job) {                                 // the spec of this entry's job (or the search's)
       if (job >= 0) c.flush(a.jst + job, lane);
       job = pj;
-      __syncwarp();
-      const int *src = (const int *)(a.fjob ? a.specs + job : &sp0);
-      for (int i = lane; i < (int)(sizeof(DevSpec) / 4); i += 32) ((int *)&sp)[i] = src[i];
-      __syncwarp();
-      if (a.fjob) { const int t = a.jt[job]; rem = sp.depth - t; keep = t < sp.depth; }
+      if constexpr (BATCHED) {
+        spp = a.specs + job;
+        const int t = a.jt[job];
+        rem = spp->depth - t; keep = t < spp->depth;
+      }
       conjmask = 0;
-      for (int i = 0; i < sp.nsym; i++) conjmask |= (unsigned)(sp.symconj[i] != 0) << i;
+      for (int i = 0; i < spp->nsym; i++) conjmask |= (unsigned)(spp->symconj[i] != 0) << i;
     }
+    const DevSpec &sp = BATCHED ? *spp : sps[w];
     const NodeMeta pm = a.meta[q.p];
     int T = 0;
     for (int s2 = 0; s2 < q.n; s2++) {
@@ -1440,7 +1489,7 @@ __global__ void __launch_bounds__(TB_WARPS * 32) k_tbound(const __grid_constant_
     b ^= NB - 1;
   }
   cp_async_wait<0>();
-  if (a.fjob) { if (job >= 0) c.flush(a.jst + job, lane); }
+  if constexpr (BATCHED) { if (job >= 0) c.flush(a.jst + job, lane); }
   else c.flush(a.st, lane);
 }
 
@@ -2118,6 +2167,105 @@ struct DBuf {
   }
   template <typename T> T *as() const { return (T *)p; }
   void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+};
+
+// A device buffer that grows in place. One large virtual address range is reserved for it; physical memory is
+// created and mapped into the range as the buffer grows (the driver's virtual memory management), so growing keeps
+// the contents without a copy and frees nothing, and the address never changes. Memory goes back to the device only
+// at release(). The driver entry points are looked up through the runtime (no link-time dependency on libcuda).
+struct Vmm {
+  decltype(&::cuMemAddressReserve) reserve = nullptr;
+  decltype(&::cuMemAddressFree) addr_free = nullptr;
+  decltype(&::cuMemCreate) create = nullptr;
+  decltype(&::cuMemRelease) mem_release = nullptr;
+  decltype(&::cuMemMap) map = nullptr;
+  decltype(&::cuMemUnmap) unmap = nullptr;
+  decltype(&::cuMemSetAccess) set_access = nullptr;
+  decltype(&::cuMemGetAllocationGranularity) granularity = nullptr;
+  bool ok = false;
+  static const Vmm &get() {
+    static const Vmm v = [] {
+      Vmm x;
+      auto look = [](const char *name, void **f) {
+        cudaDriverEntryPointQueryResult q;
+        return cudaGetDriverEntryPoint(name, f, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess;
+      };
+      x.ok = look("cuMemAddressReserve", (void **)&x.reserve) && look("cuMemAddressFree", (void **)&x.addr_free) &&
+             look("cuMemCreate", (void **)&x.create) && look("cuMemRelease", (void **)&x.mem_release) &&
+             look("cuMemMap", (void **)&x.map) && look("cuMemUnmap", (void **)&x.unmap) &&
+             look("cuMemSetAccess", (void **)&x.set_access) &&
+             look("cuMemGetAllocationGranularity", (void **)&x.granularity);
+      return x;
+    }();
+    return v;
+  }
+};
+
+struct VBuf {
+  static constexpr size_t RESERVE = (size_t)256 << 30;    // address range per buffer (more than the device holds)
+  static constexpr size_t STEP = (size_t)256 << 20;       // smallest growth step
+  void *p = nullptr;                                      // start of the range (nullptr until the first growth)
+  size_t cap = 0;                                         // bytes mapped
+  std::vector<std::pair<CUmemGenericAllocationHandle, size_t>> maps;   // physical blocks in address order
+  static void drv(CUresult r, const char *what) {
+    if (r != CUDA_SUCCESS) throw CudaError(std::string("CUDA driver error ") + std::to_string((int)r) + " in " + what);
+  }
+  void ensure(size_t bytes) {
+    if (bytes <= cap) return;
+    const Vmm &v = Vmm::get();
+    if (!v.ok) throw CudaError("the driver's virtual memory management entry points are missing");
+    int dev = 0;
+    ck(cudaGetDevice(&dev), "cudaGetDevice");
+    CUmemAllocationProp prop{};
+    prop.type = CU_MEM_ALLOCATION_TYPE_PINNED;
+    prop.location.type = CU_MEM_LOCATION_TYPE_DEVICE;
+    prop.location.id = dev;
+    size_t gran = 0;
+    drv(v.granularity(&gran, &prop, CU_MEM_ALLOC_GRANULARITY_RECOMMENDED), "cuMemGetAllocationGranularity");
+    if (!p) {
+      CUdeviceptr base = 0;
+      drv(v.reserve(&base, RESERVE, 0, 0, 0), "cuMemAddressReserve");
+      p = (void *)base;
+    }
+    const size_t need = bytes - cap;
+    size_t step = std::max(need, std::max(STEP, cap / 8));
+    step = (step + gran - 1) / gran * gran;
+    if (cap + step > RESERVE) step = (need + gran - 1) / gran * gran;
+    if (cap + step > RESERVE) throw CudaError("device buffer larger than its address range");
+    CUmemGenericAllocationHandle h;
+    if (v.create(&h, step, &prop, 0) != CUDA_SUCCESS) {   // no room for the step: the exact need
+      step = (need + gran - 1) / gran * gran;
+      drv(v.create(&h, step, &prop, 0), "cuMemCreate (device memory exhausted)");
+    }
+    const CUdeviceptr at = (CUdeviceptr)p + cap;
+    CUresult r = v.map(at, step, 0, h, 0);
+    if (r == CUDA_SUCCESS) {
+      CUmemAccessDesc acc{};
+      acc.location = prop.location;
+      acc.flags = CU_MEM_ACCESS_FLAGS_PROT_READWRITE;
+      r = v.set_access(at, step, &acc, 1);
+      if (r != CUDA_SUCCESS) v.unmap(at, step);
+    }
+    if (r != CUDA_SUCCESS) { v.mem_release(h); drv(r, "cuMemMap"); }
+    maps.push_back({h, step});
+    cap += step;
+  }
+  template <typename T> T *as() const { return (T *)p; }
+  // the caller has waited for every use of the buffer on the device
+  void release() {
+    if (!p) return;
+    const Vmm &v = Vmm::get();
+    size_t off = 0;
+    for (auto &m : maps) {
+      v.unmap((CUdeviceptr)p + off, m.second);
+      v.mem_release(m.first);
+      off += m.second;
+    }
+    v.addr_free((CUdeviceptr)p, RESERVE);
+    maps.clear();
+    p = nullptr;
+    cap = 0;
+  }
 };
 
 uint64_t powmod_h(uint64_t a, uint64_t e) {
@@ -3709,7 +3857,8 @@ __global__ void k_carry(long long p0, long long n, int E, const Z4<ST> *R, const
   }
 }
 
-struct SpecTables { DBuf ginv, bad2, bad3, cxt, goal; };   // one spec's device tables, shared by equal specs
+// device addresses of one spec's tables (inverse gates, window rules, CX table, goal), shared by equal specs
+struct SpecTables { const int4 *ginv; const uint8_t *bad2; const uint32_t *bad3; const int *cxt; const longlong2 *goal; };
 
 uint64_t bytes_hash(uint64_t h, const void *p, size_t n) {
   const unsigned char *b = (const unsigned char *)p;
@@ -3760,16 +3909,22 @@ struct BatchImpl : BatchSession::Impl {
   int nsm = 148;
   std::vector<Job> J;
   std::vector<int> queue;            // submitted, not yet admitted
-  std::map<uint64_t, SpecTables *> tables;
+  std::map<uint64_t, SpecTables> tables;
+  std::vector<DBuf> arenas;          // the spec tables of each admission, one device block each, kept for the session
   DBuf dspecs, jt, jst, jact, jdist;
-  DBuf fR, fMeta, fJob, fR2, fMeta2, fJob2;
-  DBuf sH1, sH2, sIdx, sMeta, stats;       // survivors: 32-byte records
+  // the large buffers grow in place (frontiers, survivors, T queue, dedupe scratch): no copies, no frees
+  VBuf fR, fMeta, fJob, fR2, fMeta2, fJob2;
+  VBuf sH1, sH2, sIdx, sMeta;              // survivors: 40-byte records
+  DBuf stats;
   DBuf bgoal, jgoal;                       // the goal pass: counters + candidate list, per-job results
-  DBuf tq;                                 // deferred T evaluations
-  DBuf k0, k1, v0, v1, hist, part, work, tmp, kidx, kslot, cnt;
+  VBuf tq;                                 // deferred T evaluations
+  VBuf k0, k1, v0, v1, work, tmp, kidx, kslot;
+  DBuf hist, part, cnt;
   DBuf rJob, rTk, tptr, wbuf;
   std::vector<DBuf> tpar, tgat;      // tree of every step
+  std::vector<DBuf> spare_par, spare_gat;   // tree buffers of released steps, for later steps
   long long m = 0;                   // frontier nodes
+  long long tree_lo = 0;             // tree levels below this step are released
   long long nlaunch = 0, nstep = 0;
   int nrun = 0;
   size_t spec_cap = 0;
@@ -3787,17 +3942,18 @@ struct BatchImpl : BatchSession::Impl {
   long long waits() const override { return nwait; }
   ~BatchImpl() override {
     cudaSetDevice(eng.device());
-    for (DBuf *b : {&dspecs, &jt, &jst, &jact, &jdist, &fR, &fMeta, &fJob, &fR2, &fMeta2, &fJob2, &sH1, &sH2, &sIdx,
-                    &sMeta, &tq, &stats, &k0, &k1, &v0, &v1, &hist, &part, &work, &tmp, &kidx, &kslot, &cnt, &rJob,
-                    &rTk, &tptr, &wbuf, &bgoal, &jgoal})
+    cudaStreamSynchronize(s);          // unmapping does not wait for the device
+    for (DBuf *b : {&dspecs, &jt, &jst, &jact, &jdist, &stats, &hist, &part, &cnt, &rJob, &rTk, &tptr, &wbuf, &bgoal,
+                    &jgoal})
+      b->release();
+    for (VBuf *b : {&fR, &fMeta, &fJob, &fR2, &fMeta2, &fJob2, &sH1, &sH2, &sIdx, &sMeta, &tq, &k0, &k1, &v0, &v1,
+                    &work, &tmp, &kidx, &kslot})
       b->release();
     for (auto &b : tpar) b.release();
+    for (auto &b : spare_par) b.release();
+    for (auto &b : spare_gat) b.release();
     for (auto &b : tgat) b.release();
-    for (auto &kv : tables) {
-      kv.second->ginv.release(); kv.second->bad2.release(); kv.second->bad3.release(); kv.second->cxt.release();
-      kv.second->goal.release();
-      delete kv.second;
-    }
+    for (auto &b : arenas) b.release();
   }
   int nq() const override { return NQ; }
   int running() const override { return nrun + (int)queue.size(); }
@@ -3808,23 +3964,38 @@ struct BatchImpl : BatchSession::Impl {
   long long steps() const override { return nstep; }
   size_t device_bytes() const override {
     size_t b = 0;
-    for (const DBuf *x : {&dspecs, &jt, &jst, &jact, &jdist, &fR, &fMeta, &fJob, &fR2, &fMeta2, &fJob2, &sH1, &sH2,
-                          &sIdx, &sMeta, &k0, &k1, &v0, &v1, &hist, &part, &work, &tmp, &kidx, &kslot})
+    for (const DBuf *x : {&dspecs, &jt, &jst, &jact, &jdist, &hist, &part})
+      b += x->cap;
+    for (const VBuf *x : {&fR, &fMeta, &fJob, &fR2, &fMeta2, &fJob2, &sH1, &sH2, &sIdx, &sMeta, &tq, &k0, &k1, &v0, &v1,
+                          &work, &tmp, &kidx, &kslot})
       b += x->cap;
     for (auto &x : tpar) b += x.cap;
     for (auto &x : tgat) b += x.cap;
+    for (auto &x : spare_par) b += x.cap;
+    for (auto &x : spare_gat) b += x.cap;
+    for (auto &x : arenas) b += x.cap;
     return b;
   }
 
-  size_t projected_bytes() const override {   // this frontier + every running job's expected survivors and nodes
-    const size_t node = E * sizeof(Z4<ST>) + sizeof(NodeMeta) + 4 + 5, surv = 40 + 36;
-    size_t b = (size_t)m * node;
+  // device bytes of a frontier node with its tree entry, and of a survivor record with its dedupe sort entries
+  static constexpr size_t NODE_BYTES = E * sizeof(Z4<ST>) + sizeof(NodeMeta) + 4 + 5;
+  static constexpr size_t SURV_BYTES = 40 + 48;
+  static constexpr unsigned long long SOLO_CHILDREN = 1ull << 22;
+  // expected nodes of the job's next frontier: its children at the previous level's survivor and distinct rates,
+  // with a quarter more survivors and 1024 nodes to spare (every child at the first level)
+  double next_nodes(const Job &j) const {
+    const double all = j.t < j.depth ? (double)j.seg * j.hs.G : 0.0;
+    return std::min(all, (1.25 * j.rate * all + 1024.0) * j.drate);
+  }
+  size_t projected_bytes() const override {   // this frontier, the next one, and one chunk's survivor room
+    double b = (double)m * NODE_BYTES, want = 0;
     for (const Job &j : J)
       if (j.running && j.t < j.depth) {
         const double all = (double)j.seg * j.hs.G;
-        b += (size_t)(std::min(all, 1.5 * j.rate * all + 4096.0) * (double)(surv + node));
+        b += next_nodes(j) * NODE_BYTES;
+        want += std::min(all, 1.5 * j.rate * all + 4096.0);
       }
-    return b;
+    return (size_t)(b + std::min(want, (double)(tune.chunk_bytes / SURV_BYTES)) * SURV_BYTES);
   }
 
   int submit(const HostSpec &hs, const Options &opt) override {
@@ -3854,8 +4025,23 @@ struct BatchImpl : BatchSession::Impl {
     j.out.finished_step = (int)nstep;
   }
 
-  // device tables of a spec, shared by every job whose tables have the same content
-  void upload_spec(Job &j) {
+  // Host staging of one admission: every new spec's tables, then the admitted jobs' device specs, root residuals and
+  // (job, T exponent) pairs, each section 256-byte aligned, moved to the device by one copy. Pageable copies wait for
+  // the stream, so one copy per admission instead of several per job.
+  struct Stage {
+    std::vector<unsigned char> b;
+    size_t put(const void *p, size_t n) {
+      const size_t o = (b.size() + 255) & ~(size_t)255;
+      b.resize(o + std::max<size_t>(n, 4), 0);
+      if (n) std::memcpy(b.data() + o, p, n);
+      return o;
+    }
+  };
+
+  // the spec's device specialisation; its tables come from an earlier admission when an equal spec had them, else
+  // they are staged (offsets into the staging block, made device addresses once the block is on the device)
+  void stage_spec(Job &j, Stage &st, std::map<uint64_t, std::array<size_t, 5>> &fresh, std::vector<std::pair<int, uint64_t>> &fix,
+                  int id) {
     const SymGroup grp = sym_group(j.hs, j.opt.sym);
     j.out.res.nsym = grp.nsym;
     std::vector<int4> gi;
@@ -3867,30 +4053,25 @@ struct BatchImpl : BatchSession::Impl {
     h = bytes_hash(h, j.hs.bad3.data(), j.hs.bad3.size() * 4);
     h = bytes_hash(h, j.hs.cxtable.data(), j.hs.cxtable.size() * 4);
     h = bytes_hash(h, gl.data(), gl.size() * sizeof(longlong2));
-    SpecTables *tb;
     auto it = tables.find(h);
-    if (it != tables.end()) tb = it->second;
-    else {
-      tb = new SpecTables;
-      tb->ginv.ensure(gi.size() * sizeof(int4)); tb->bad2.ensure(j.hs.bad2.size() + 1);
-      tb->bad3.ensure(j.hs.bad3.size() * 4 + 4); tb->cxt.ensure(std::max<size_t>(1, j.hs.cxtable.size()) * 4);
-      tb->goal.ensure(gl.size() * sizeof(longlong2));
-      ck(cudaMemcpyAsync(tb->ginv.p, gi.data(), gi.size() * sizeof(int4), cudaMemcpyHostToDevice, s), "h2d");
-      ck(cudaMemcpyAsync(tb->bad2.p, j.hs.bad2.data(), j.hs.bad2.size(), cudaMemcpyHostToDevice, s), "h2d");
-      ck(cudaMemcpyAsync(tb->bad3.p, j.hs.bad3.data(), j.hs.bad3.size() * 4, cudaMemcpyHostToDevice, s), "h2d");
-      if (!j.hs.cxtable.empty())
-        ck(cudaMemcpyAsync(tb->cxt.p, j.hs.cxtable.data(), j.hs.cxtable.size() * 4, cudaMemcpyHostToDevice, s), "h2d");
-      ck(cudaMemcpyAsync(tb->goal.p, gl.data(), gl.size() * sizeof(longlong2), cudaMemcpyHostToDevice, s), "h2d");
-      ck(cudaStreamSynchronize(s), "spec upload");
-      tables[h] = tb;
+    if (it != tables.end()) {
+      const SpecTables &t = it->second;
+      j.sp.ginv = t.ginv; j.sp.bad2 = t.bad2; j.sp.bad3 = t.bad3; j.sp.cxtable = t.cxt; j.sp.goal = t.goal;
+      return;
     }
-    j.sp.ginv = tb->ginv.as<int4>(); j.sp.bad2 = tb->bad2.as<uint8_t>(); j.sp.bad3 = tb->bad3.as<uint32_t>();
-    j.sp.cxtable = tb->cxt.as<int>(); j.sp.goal = tb->goal.as<longlong2>();
+    if (!fresh.count(h))
+      fresh[h] = {st.put(gi.data(), gi.size() * sizeof(int4)), st.put(j.hs.bad2.data(), j.hs.bad2.size()),
+                  st.put(j.hs.bad3.data(), j.hs.bad3.size() * 4), st.put(j.hs.cxtable.data(), j.hs.cxtable.size() * 4),
+                  st.put(gl.data(), gl.size() * sizeof(longlong2))};
+    fix.push_back({id, h});
   }
 
   // admit the queued jobs: depth-0 and unsupported ones finish here, the others append their root to the frontier
   void admit() {
     std::vector<int> roots;
+    Stage st;
+    std::map<uint64_t, std::array<size_t, 5>> fresh;
+    std::vector<std::pair<int, uint64_t>> fix;
     for (int id : queue) {
       Job &j = J[id];
       j.queued = false;
@@ -3906,9 +4087,10 @@ struct BatchImpl : BatchSession::Impl {
       auto f32 = [](int64_t v) { return v >= INT32_MIN && v <= INT32_MAX; };
       for (const Zw &z : j.hs.target) if (!f32(z.a) || !f32(z.b) || !f32(z.c) || !f32(z.d)) wide = true;
       if (wide || !j.opt.dedupe || j.opt.nogoal || j.depth < 1 || j.depth > MAXDEPTH_WALK) { run_plain(j); continue; }
-      upload_spec(j);
+      stage_spec(j, st, fresh, fix, id);
       roots.push_back(id);
     }
+    const int qlo = queue.empty() ? 0 : queue.front(), qhi = queue.empty() ? -1 : queue.back();
     queue.clear();
     // device specs: one per job id
     if (J.size() > spec_cap) {
@@ -3922,33 +4104,66 @@ struct BatchImpl : BatchSession::Impl {
       nd.p = nullptr;
     }
     if (roots.empty()) return;
+    // the staged tables get their device block first: the job specs staged after them hold its addresses
+    st.b.resize((st.b.size() + 255) & ~(size_t)255, 0);
+    const size_t tables_end = st.b.size();
+    DBuf arena;
+    if (tables_end) {
+      arena.ensure(tables_end);
+      const char *base = arena.as<char>();
+      for (auto &kv : fresh)
+        tables[kv.first] = SpecTables{(const int4 *)(base + kv.second[0]), (const uint8_t *)(base + kv.second[1]),
+                                      (const uint32_t *)(base + kv.second[2]), (const int *)(base + kv.second[3]),
+                                      (const longlong2 *)(base + kv.second[4])};
+      for (auto &f : fix) {
+        const SpecTables &t = tables[f.second];
+        DevSpec &sp = J[f.first].sp;
+        sp.ginv = t.ginv; sp.bad2 = t.bad2; sp.bad3 = t.bad3; sp.cxtable = t.cxt; sp.goal = t.goal;
+      }
+    }
+    // queued ids are consecutive and newer than every admitted job: their specs are one range of the spec array
+    // (jobs that finished above get a zeroed entry they never read)
+    std::vector<DevSpec> sps((size_t)(qhi - qlo + 1));
+    std::memset((void *)sps.data(), 0, sps.size() * sizeof(DevSpec));
+    const long long nr = (long long)roots.size();
     std::vector<Z4<int32_t>> rr(roots.size() * E);
-    std::vector<uint32_t> rj(roots.size());
-    std::vector<int> rk(roots.size());
+    std::vector<uint32_t> rjk(2 * roots.size());
     for (size_t i = 0; i < roots.size(); i++) {
       Job &j = J[roots[i]];
       for (int e = 0; e < E; e++)
         rr[i * E + e] = {(int32_t)j.hs.target[e].a, (int32_t)j.hs.target[e].b, (int32_t)j.hs.target[e].c,
                          (int32_t)j.hs.target[e].d};
-      rj[i] = (uint32_t)roots[i];
-      rk[i] = j.hs.tk;
-      ck(cudaMemcpyAsync(dspecs.as<DevSpec>() + roots[i], &j.sp, sizeof(DevSpec), cudaMemcpyHostToDevice, s), "h2d");
+      rjk[i] = (uint32_t)roots[i];
+      rjk[roots.size() + i] = (uint32_t)j.hs.tk;
+      sps[roots[i] - qlo] = j.sp;
       j.t = 1;
       j.seg = 1;
       j.running = true;
       nrun++;
     }
-    const long long nr = (long long)roots.size();
-    // grow the frontier (contents kept) and append the roots
+    const size_t o_sp = st.put(sps.data(), sps.size() * sizeof(DevSpec));
+    const size_t o_rr = st.put(rr.data(), rr.size() * sizeof(Z4<int32_t>));
+    const size_t o_rj = st.put(rjk.data(), rjk.size() * 4);
+    // grow the frontier (contents kept); new tables go to a device block kept for the session, the rest of the staged
+    // bytes to a work buffer, from which the specs and the roots' residuals are copied into place
     grow_keep(fR, (size_t)(m + nr) * E * sizeof(Z4<ST>), (size_t)m * E * sizeof(Z4<ST>));
     grow_keep(fMeta, (size_t)(m + nr) * sizeof(NodeMeta), (size_t)m * sizeof(NodeMeta));
     grow_keep(fJob, (size_t)(m + nr) * 4, (size_t)m * 4);
-    rJob.ensure(nr * 4); rTk.ensure(nr * 4);
-    ck(cudaMemcpyAsync(fR.as<Z4<ST>>() + m * E, rr.data(), rr.size() * sizeof(Z4<ST>), cudaMemcpyHostToDevice, s), "h2d");
-    ck(cudaMemcpyAsync(fJob.as<uint32_t>() + m, rj.data(), nr * 4, cudaMemcpyHostToDevice, s), "h2d");
-    ck(cudaMemcpyAsync(rJob.p, rj.data(), nr * 4, cudaMemcpyHostToDevice, s), "h2d");
-    ck(cudaMemcpyAsync(rTk.p, rk.data(), nr * 4, cudaMemcpyHostToDevice, s), "h2d");
-    k_root_batch<NQ><<<(unsigned)nr, 32, 0, s>>>(dspecs.as<DevSpec>(), rJob.as<uint32_t>(), rTk.as<int>(), (int)nr,
+    if (tables_end) {
+      ck(cudaMemcpyAsync(arena.p, st.b.data(), tables_end, cudaMemcpyHostToDevice, s), "h2d");
+      arenas.push_back(arena);
+      arena.p = nullptr;
+    }
+    wbuf.ensure(st.b.size() - tables_end);
+    ck(cudaMemcpyAsync(wbuf.p, st.b.data() + tables_end, st.b.size() - tables_end, cudaMemcpyHostToDevice, s), "h2d");
+    const char *w = wbuf.as<char>() - tables_end;     // staging offsets past the tables, as device addresses
+    ck(cudaMemcpyAsync(dspecs.as<DevSpec>() + qlo, w + o_sp, sps.size() * sizeof(DevSpec), cudaMemcpyDeviceToDevice, s),
+       "d2d");
+    ck(cudaMemcpyAsync(fR.as<Z4<ST>>() + m * E, w + o_rr, rr.size() * sizeof(Z4<int32_t>), cudaMemcpyDeviceToDevice, s),
+       "d2d");
+    const uint32_t *rj = (const uint32_t *)(w + o_rj);
+    ck(cudaMemcpyAsync(fJob.as<uint32_t>() + m, rj, nr * 4, cudaMemcpyDeviceToDevice, s), "d2d");
+    k_root_batch<NQ><<<(unsigned)nr, 32, 0, s>>>(dspecs.as<DevSpec>(), rj, (const int *)(rj + nr), (int)nr,
                                                  fR.as<Z4<ST>>() + m * E, fMeta.as<NodeMeta>() + m);
     nlaunch++;
     ck(cudaGetLastError(), "root kernel");
@@ -3956,6 +4171,7 @@ struct BatchImpl : BatchSession::Impl {
     m += nr;
   }
 
+  void grow_keep(VBuf &b, size_t bytes, size_t) { b.ensure(bytes); }   // grows in place: contents stay
   // grow b to `bytes`, keeping its first `keep` bytes (half again as much room below 1 GB, a tenth above)
   void grow_keep(DBuf &b, size_t bytes, size_t keep) {
     if (bytes <= b.cap) return;
@@ -3983,13 +4199,13 @@ struct BatchImpl : BatchSession::Impl {
     ck(cudaMemcpyAsync(jt.p, ht.data(), nj * 4, cudaMemcpyHostToDevice, s), "h2d");
     k_jst_init<<<(nj + 255) / 256, 256, 0, s>>>(jst.as<DevStats>(), nj);
     nlaunch++;
-    const size_t rec = 40 + 36;                                          // survivor record + its sort entries
-    const size_t node = E * sizeof(Z4<ST>) + sizeof(NodeMeta) + 4 + 5;     // frontier node + its tree entry
+    const size_t rec = SURV_BYTES, node = NODE_BYTES;
     const unsigned long long cap_limit = std::max<unsigned long long>(1 << 16, tune.chunk_bytes / rec);
     // the plan, in frontier (= id) order: chunks of advancing jobs whose expected survivors fit the survivor
     // budget, and runs of waiting jobs carried over unchanged. A job advances while the step's planned memory (this
-    // frontier, the next one, survivor room) stays under the session budget; the first job always advances.
-    struct Op { bool carry; long long p0, p1; unsigned long long cap, all; std::vector<int> jobs; };
+    // frontier, the next one at each job's last survivor and distinct rates, the survivor room of one chunk, which
+    // every chunk reuses) stays under the session budget; the first job always advances.
+    struct Op { bool carry; long long p0, p1; unsigned long long cap, all; std::vector<int> jobs; bool solo = false; };
     std::vector<Op> ops;
     size_t step_budget = budget;
     if ((size_t)m * node * 8 > budget / 4) {              // a large step: never plan past what the device has left
@@ -4002,6 +4218,7 @@ struct BatchImpl : BatchSession::Impl {
     }
     {
       size_t planned = (size_t)m * node;
+      unsigned long long want_all = 0;
       bool any_adv = false;
       Op c{false, 0, 0, 0, 0, {}};
       long long off = 0;
@@ -4010,12 +4227,21 @@ struct BatchImpl : BatchSession::Impl {
         if (!j.running || j.seg == 0) continue;
         const unsigned long long all = j.t < j.depth ? (unsigned long long)j.seg * j.hs.G : 0;
         const unsigned long long want = all ? std::min<unsigned long long>(all, (unsigned long long)(1.5 * j.rate * (double)all) + 4096) : 0;
-        const size_t cost = (size_t)want * (node + rec);
-        const bool adv = !any_adv || planned + cost <= step_budget;
+        const size_t cost = (size_t)next_nodes(j) * node;
+        const size_t room = (size_t)std::min(cap_limit, want_all + want) * rec;
+        const bool adv = !any_adv || planned + cost + room <= step_budget;
         planned += adv ? cost : (size_t)j.seg * node;
+        if (adv) want_all += want;
         any_adv |= adv;
-        if (!c.jobs.empty() && (c.carry == adv || (adv && c.cap + want > cap_limit))) { ops.push_back(c); c = Op{!adv, off, off, 0, 0, {}}; }
+        // a job of at least SOLO_CHILDREN children fills the GPU by itself: it gets a chunk of its own (the one-job
+        // level kernel); smaller jobs share chunks
+        const bool solo = adv && all >= SOLO_CHILDREN;
+        if (!c.jobs.empty() && (c.carry == adv || (adv && (c.cap + want > cap_limit || solo || c.solo)))) {
+          ops.push_back(c);
+          c = Op{!adv, off, off, 0, 0, {}};
+        }
         c.carry = !adv;
+        c.solo = solo;
         c.jobs.push_back(i);
         if (adv) { c.cap += want; c.all += all; }
         off += j.seg;
@@ -4030,13 +4256,13 @@ struct BatchImpl : BatchSession::Impl {
       size_t est = 0;                                     // next frontier: carried nodes + expected distinct children
       for (const Op &o : ops) {
         if (o.carry) { est += (size_t)(o.p1 - o.p0); continue; }
-        for (int i : o.jobs) {
-          const Job &j = J[i];
-          const double all = j.t < j.depth ? (double)j.seg * j.hs.G : 0.0;
-          est += (size_t)std::min(all, (1.25 * j.rate * all + 1024.0) * j.drate);
-        }
+        for (int i : o.jobs) est += (size_t)next_nodes(J[i]);
       }
-      fR2.ensure(est * E * sizeof(Z4<ST>) + 16); fMeta2.ensure(est * sizeof(NodeMeta) + 16); fJob2.ensure(est * 4 + 4);
+      // (the next frontier itself grows in place chunk by chunk; the tree is sized ahead, its growth copies)
+      if (!tpar[nstep].p && !spare_par.empty()) {        // tree buffers of released levels are reused
+        tpar[nstep] = spare_par.back(); spare_par.pop_back();
+        tgat[nstep] = spare_gat.back(); spare_gat.pop_back();
+      }
       tpar[nstep].ensure(est * 4 + 4); tgat[nstep].ensure(est + 4);
     }
     std::vector<DevStats> hj(nj);
@@ -4094,6 +4320,8 @@ struct BatchImpl : BatchSession::Impl {
         nlaunch += 2;
         ck(cudaGetLastError(), "goal pass");
       }
+      GoalShort hgs{};
+      std::vector<ulonglong2> hjg(jn);
       for (int attempt = 0; attempt < 2; attempt++) {
         tq.ensure(tqcap * sizeof(TQEntry));
         if (cap) {
@@ -4115,29 +4343,28 @@ struct BatchImpl : BatchSession::Impl {
         a.gshort = gsd; a.jgoal = jg;
         const long long want = (cm + EXP_WARPS - 1) / EXP_WARPS;
         const long long grid = std::max<long long>(1, std::min<long long>(want, (long long)nsm * tune.expand_blocks_per_sm));
-        k_expand_batch<NQ, ST><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(a);
+        if (ch.jobs.size() == 1) k_expand_solo<NQ, ST><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(J[jlo].sp, a, jlo);
+        else k_expand_batch<NQ, ST><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(a);
         TBoundArgs<ST> tb;
         tb.R = fR.as<Z4<ST>>(); tb.meta = fMeta.as<NodeMeta>(); tb.tq = tq.as<TQEntry>(); tb.tqcap = tqcap;
         tb.GS = BATCH_GS; tb.rem = 0; tb.keep = 0; tb.fjob = fJob.as<uint32_t>(); tb.specs = dspecs.as<DevSpec>();
         tb.jt = jt.as<int>(); tb.jst = jst.as<DevStats>(); tb.st = dst; tb.cap = cap; tb.sh1 = sH1.as<uint64_t>();
         tb.sh2 = sH2.as<uint64_t>(); tb.sidx = sIdx.as<uint64_t>(); tb.smeta = sMeta.as<NodeMeta>();
-        k_tbound<NQ, ST><<<(unsigned)(nsm * tune.tbound_blocks_per_sm), TB_WARPS * 32, 0, s>>>(DevSpec{}, tb);
+        k_tbound<NQ, ST, true><<<(unsigned)(nsm * tune.tbound_blocks_per_sm), TB_WARPS * 32, 0, s>>>(DevSpec{}, tb);
         nlaunch += 2;
         ck(cudaGetLastError(), "batched expand");
+        // the chunk's counters, the jobs' statistics and the goal pass's results, read back with one wait
         ck(cudaMemcpyAsync(&h, dst, sizeof(DevStats), cudaMemcpyDeviceToHost, s), "d2h");
+        ck(cudaMemcpyAsync(hj.data() + jlo, jst.as<DevStats>() + jlo, jn * sizeof(DevStats), cudaMemcpyDeviceToHost, s),
+           "d2h");
+        ck(cudaMemcpyAsync(&hgs, gsd, sizeof hgs, cudaMemcpyDeviceToHost, s), "d2h");
+        ck(cudaMemcpyAsync(hjg.data(), jg + jlo, jn * sizeof(ulonglong2), cudaMemcpyDeviceToHost, s), "d2h");
         ck(cudaStreamSynchronize(s), "batched expand");
         if (!h.surv_overflow && h.n_tq <= tqcap) break;
         cap = std::max<unsigned long long>(cap, h.n_surv);  // every survivor and entry was counted: exact room
         tqcap = std::max<unsigned long long>(tqcap, h.n_tq);
       }
       if (h.surv_overflow || h.n_tq > tqcap) throw std::runtime_error("survivor or T queue overflow");
-      ck(cudaMemcpyAsync(hj.data() + jlo, jst.as<DevStats>() + jlo, jn * sizeof(DevStats), cudaMemcpyDeviceToHost, s),
-         "d2h");
-      GoalShort hgs{};
-      std::vector<ulonglong2> hjg(jn);
-      ck(cudaMemcpyAsync(&hgs, gsd, sizeof hgs, cudaMemcpyDeviceToHost, s), "d2h");
-      ck(cudaMemcpyAsync(hjg.data(), jg + jlo, jn * sizeof(ulonglong2), cudaMemcpyDeviceToHost, s), "d2h");
-      ck(cudaStreamSynchronize(s), "job stats");
       if (!hgs.ovf && hgs.count <= GOAL_LIST)            // jobs found by the goal pass (their level kernels skipped)
         for (int i : ch.jobs)
           if (hjg[i - jlo].x) { hj[i].found = hjg[i - jlo].x; hj[i].first_found = hjg[i - jlo].y; }
@@ -4216,11 +4443,11 @@ struct BatchImpl : BatchSession::Impl {
           distinct, sMeta.as<NodeMeta>(), fR2.as<Z4<ST>>() + o0 * E, fMeta2.as<NodeMeta>() + o0,
           tpar[nstep].as<uint32_t>() + o0, tgat[nstep].as<uint8_t>() + o0, fJob2.as<uint32_t>() + o0);
       nlaunch++;
-      ck(cudaGetLastError(), "batched gather");
-      ck(cudaStreamSynchronize(s), "batched gather");
+      ck(cudaGetLastError(), "batched gather");   // the next chunk's work queues behind the gather (no wait here)
       for (int i : ch.jobs) dist[i] = cd[i];
       total_distinct = o1;
     }
+    ck(cudaStreamSynchronize(s), "batched gather");
     std::swap(fR, fR2); std::swap(fMeta, fMeta2); std::swap(fJob, fJob2);
     // level lines of the running jobs
     const double secs = now_s() - t0;
@@ -4253,6 +4480,15 @@ struct BatchImpl : BatchSession::Impl {
       j.running = false;
       j.seg = 0;
       run_plain(j);
+    }
+    // tree levels older than every running job's first step: no walk reads them again; their buffers go to the
+  // spare lists (freeing device memory synchronises the device and can take milliseconds)
+    long long oldest = nstep;
+    for (const Job &j : J) if (j.running) oldest = std::min<long long>(oldest, j.out.joined_step);
+    for (; tree_lo < oldest && tree_lo < (long long)tpar.size(); tree_lo++) {
+      if (!tpar[tree_lo].p) continue;
+      spare_par.push_back(tpar[tree_lo]); spare_gat.push_back(tgat[tree_lo]);
+      tpar[tree_lo] = DBuf(); tgat[tree_lo] = DBuf();
     }
     return running();
   }
@@ -4344,8 +4580,10 @@ BatchTuning autotune_batch(Engine &engine, int nq, const std::vector<const HostS
   static const size_t chunk_space[] = {(size_t)8 << 30, (size_t)1 << 30, (size_t)2 << 30, (size_t)4 << 30};
   static const int expand_space[] = {16, 4, 8, 32};
   static const int tbound_space[] = {4, 1, 2, 8};
+  // every trial on one session, so that all of them run with its buffers already grown and its spec tables on the
+  // device (the probe jobs are submitted again for each trial)
+  BatchSession b(engine, nq);
   auto run = [&](const BatchTuning &t) {
-    BatchSession b(engine, nq);
     b.set_tuning(t);
     const double t0 = now_s();
     for (const HostSpec *hs : probe) b.submit(*hs, opt);
@@ -4355,7 +4593,7 @@ BatchTuning autotune_batch(Engine &engine, int nq, const std::vector<const HostS
     return sec;
   };
   BatchTuning best;
-  run(best);                                      // warm-up: device buffers grown, spec tables uploaded
+  run(best);                                      // warm-up
   if (trials) trials->clear();
   double best_s = run(best);
   for (int dim = 0; dim < 3; dim++) {

@@ -150,7 +150,8 @@ typedef struct {
 } cz_batch_tuning;
 int cz_batch_set_tuning(cz_batch *batch, const cz_batch_tuning *t);
 /* The autotuner (no counterpart in the reference): times every candidate of a fixed search space on the probe jobs
- * (nprobe specs of qubit count nq, each run to its end in a fresh session on the engine; chunk budget {8, 1, 2, 4}
+ * (nprobe specs of qubit count nq, run to their end on one session of the engine, once untimed and then once per
+ * candidate; chunk budget {8, 1, 2, 4}
  * GiB, expand blocks per SM {16, 4, 8, 32}, deferred-T blocks per SM {4, 1, 2, 8}, one parameter at a time from the
  * defaults) and writes the fastest to *out, with the probe times. Apply it with cz_batch_set_tuning. */
 int cz_batch_autotune(cz_engine *engine, int nq, const cz_spec *const *probe, int nprobe, const cz_options *opt,
