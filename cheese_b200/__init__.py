@@ -340,8 +340,9 @@ class Engine:
             raise RuntimeError(f"engine on device {device}: {err.value.decode()}")
 
     def close(self):
-        if self._h:
-            lib().cz_engine_destroy(self._h)
+        lib_ = _lib                           # (at interpreter exit the module's globals may already be gone)
+        if self._h and lib_ is not None:
+            lib_.cz_engine_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):

@@ -1394,16 +1394,17 @@ __global__ void __launch_bounds__(TB_WARPS * 32) k_tbound(const __grid_constant_
   Z4<ST> *C = sC[w];
   // the search's spec is copied to shared memory once; a batch's entries read their job's spec where it lies (the
   // entries of a many-job chunk change job often, and the specs stay in cache)
+  unsigned conjmask = 0;
   if constexpr (!BATCHED) {
     for (int i = lane; i < (int)(sizeof(DevSpec) / 4); i += 32) ((int *)&sps[w])[i] = ((const int *)&sp0)[i];
     __syncwarp();
+    for (int i = 0; i < sps[w].nsym; i++) conjmask |= (unsigned)(sps[w].symconj[i] != 0) << i;
   }
   const DevSpec *spp = &sps[w];
   const unsigned long long n = a.st->n_tq < a.tqcap ? a.st->n_tq : a.tqcap;
   WarpTally c;
   int job = -2, rem = a.rem;
   bool keep = a.keep != 0;
-  unsigned conjmask = 0;
   // entries are taken one ahead: the next entry's parent residual is copied into shared memory asynchronously
   // (cp.async) while the current entry's T bound runs
   auto take = [&](TQEntry &q, int b) {
@@ -1433,17 +1434,17 @@ __global__ void __launch_bounds__(TB_WARPS * 32) k_tbound(const __grid_constant_
     }
     __syncwarp();
     const Z4<ST> *P = sP[w][b];
-    const int pj = BATCHED ? (int)a.fjob[q.p] : -1;
-    if (pj != job) {                                 // the spec of this entry's job (or the search's)
-      if (job >= 0) c.flush(a.jst + job, lane);
-      job = pj;
-      if constexpr (BATCHED) {
+    if constexpr (BATCHED) {
+      const int pj = (int)a.fjob[q.p];
+      if (pj != job) {                               // the spec of this entry's job
+        if (job >= 0) c.flush(a.jst + job, lane);
+        job = pj;
         spp = a.specs + job;
         const int t = a.jt[job];
         rem = spp->depth - t; keep = t < spp->depth;
+        conjmask = 0;
+        for (int i = 0; i < spp->nsym; i++) conjmask |= (unsigned)(spp->symconj[i] != 0) << i;
       }
-      conjmask = 0;
-      for (int i = 0; i < spp->nsym; i++) conjmask |= (unsigned)(spp->symconj[i] != 0) << i;
     }
     const DevSpec &sp = BATCHED ? *spp : sps[w];
     const NodeMeta pm = a.meta[q.p];
