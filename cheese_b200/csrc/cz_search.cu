@@ -84,6 +84,7 @@ struct DevStats {
   unsigned long long n_work, n_kept;
   unsigned long long n_tq, tq_work;   // deferred T evaluations: queued, taken
   unsigned int sort_err, pad;         // a dedupe sort's look-back gave up (its result is not used)
+  unsigned long long work2;           // parent counter of the level kernel's second part (multi-qubit gates)
 };
 
 // A T-bound evaluation deferred from the level kernel to k_tbound: the parent, up to two children that share one
@@ -500,12 +501,16 @@ __device__ __noinline__ int child_general(const Z4<ST> *P, Z4<ST> *C, int g, int
 // / w-power entries (x z h s sdg t tdg) pair the entries that differ in the gate's column bit, so each lane owns
 // both inputs of its two outputs and every product is a signed rotation; permutation gates (cx, ccx) copy.
 // Anything else goes through child_general.
-template <int NQ, typename ST>
+// PART 1: g acts on one qubit (its kind is GK_ONEQ or GK_GENERAL); PART 2: on more (GK_PERM or GK_GENERAL); any
+// other kind goes the general way, so each part's code holds one specialised update
+template <int NQ, typename ST, int PART = 0>
 __device__ __forceinline__ int warp_child(const Z4<ST> *P, Z4<ST> *C, int g, int kp, const DevSpec &sp,
                                           const DevSpec *sps, int lane, bool &ovf) {
   constexpr int N = 1 << NQ, E = N * N;
   const int kind = sp.gkind[g];
-  if (sizeof(ST) != 4 || kp > 56 || kind == GK_GENERAL) return child_general<NQ, ST>(P, C, g, kp, sps, lane, ovf);
+  if (sizeof(ST) != 4 || kp > 56 || kind == GK_GENERAL || (PART == 1 && kind != GK_ONEQ) ||
+      (PART == 2 && kind != GK_PERM))
+    return child_general<NQ, ST>(P, C, g, kp, sps, lane, ovf);
   I4 v[2] = {I4{0, 0, 0, 0}, I4{0, 0, 0, 0}};
   int ei[2] = {-1, -1};
   const int4 *P4 = (const int4 *)P;
@@ -915,7 +920,11 @@ template <typename ST> struct ExpandOut {
 // every child of parent p (residual already in P): window rules, exact prechecks, child residual, bounds, class key,
 // survivor append. sp is the parent's spec (kernel parameter or a shared copy), sps its shared-memory address for
 // the out-of-line helpers; child index = p * GS + g.
-template <int NQ, typename ST, bool STATES = false>
+// PART: 0 every candidate; 1 the one-qubit gates; 2 the multi-qubit gates. The plain level runs the two parts as
+// two launches: each warp then walks the code of one kind of child (instruction fetch is the level kernel's main
+// stall; measured 3 % faster than one launch), at the price of reading each parent twice. (Three parts, the odd
+// diagonals on their own, measured slower than one.)
+template <int NQ, typename ST, bool STATES = false, int PART = 0>
 __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *sps, const uint8_t (*perm)[8],
                                               unsigned conjmask, const uint64_t *W,
                                               const Z4<ST> *P, Z4<ST> *C, unsigned long long p, const NodeMeta pm,
@@ -959,7 +968,7 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
   for (int g0 = 0; g0 < G; g0 += 32) {
     const int g = g0 + lane;
     int fate = 0;                            // 0: no candidate, 1: W2 cut, 2: W3 cut, 3: dead by precheck, 4: full
-    if (g < G) {
+    if (g < G && (PART == 0 || ((sp.gflags[g] & GF_ONEQ) != 0) == (PART == 1))) {
       fate = 4;
       if (g1 >= 0 && __ldg(&sp.bad2[g1 * G + g])) fate = 1;
       else if (g2 >= 0) {
@@ -990,7 +999,7 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
     const int gm = sp.gmask[g], q0 = sp.gq[g][0];
     bool ovf;
     c.full++;
-    const int k = warp_child<NQ, ST>(P, C, g, kP, sp, sps, lane, ovf);
+    const int k = warp_child<NQ, ST, PART>(P, C, g, kP, sp, sps, lane, ovf);
     if (ovf) { c.ovf = true; continue; }
     const bool need_hs = need_b && !(fl & GF_MONAFF);
     // the child is the goal only if the parent equals the gate, i.e. acts on no other qubit (unitary targets)
@@ -1025,7 +1034,7 @@ __device__ __forceinline__ void expand_parent(const DevSpec &sp, const DevSpec *
       hs = need_hs ? ch.hs : hsP;
       const int h = k > hs ? k : hs;
       const int supp = __popc(ch.ntriv);
-      if (fl & GF_ONEQ) { c2 = c2P; needs = pm.needs; }
+      if (PART == 1 || (PART == 0 && (fl & GF_ONEQ))) { c2 = c2P; needs = pm.needs; }
       else c2 = warp_cx_bound<NQ, ST>(C, *sps, lane, gm, pm.needs, needs);
       if (combine(h, 0, c2, supp) > rem) alive = false;
       else {
@@ -1123,7 +1132,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32) k_goal_level(const DevSpec sp,
   }
 }
 
-template <int NQ, typename ST, bool STATES = false>
+template <int NQ, typename ST, bool STATES = false, int PART = 0>
 __global__ void __launch_bounds__(EXP_WARPS * 32, EXP_MINB) k_expand(const DevSpec sp, const ExpandArgs<ST> a) {
   constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
   if (a.gshort && a.gshort->found && !a.gshort->ovf && a.gshort->count <= GOAL_LIST) return;   // the found level
@@ -1141,7 +1150,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, EXP_MINB) k_expand(const DevSp
   WarpTally c;
   for (;;) {
     unsigned long long p = 0;
-    if (lane == 0) p = atomicAdd(&a.st->work, 1ULL);
+    if (lane == 0) p = atomicAdd(PART == 2 ? &a.st->work2 : &a.st->work, 1ULL);
     p = __shfl_sync(FULL, p, 0);
     if ((long long)p >= a.m) break;
 #pragma unroll
@@ -1151,7 +1160,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, EXP_MINB) k_expand(const DevSp
     }
     const NodeMeta pm = a.meta[p];
     __syncwarp();
-    expand_parent<NQ, ST, STATES>(sp, &s_sp, sm.perm, conjmask, sm.W, P, C, p, pm, a.rem, a.keep != 0, sp.G, o, c,
+    expand_parent<NQ, ST, STATES, PART>(sp, &s_sp, sm.perm, conjmask, sm.W, P, C, p, pm, a.rem, a.keep != 0, sp.G, o, c,
                           lane);
     __syncwarp();
   }
@@ -1303,7 +1312,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, EXP_MINB) k_expand_batch(const
 // A chunk that holds one job: its spec is a kernel parameter, as in the plain level kernel (k_expand), so the level
 // code keeps that kernel's register allocation (the many-job kernel above reads the spec from shared memory and
 // spills at the same register limit); outputs, child indices and the job's tallies are the many-job kernel's.
-template <int NQ, typename ST>
+template <int NQ, typename ST, int PART>
 __global__ void __launch_bounds__(EXP_WARPS * 32, EXP_MINB) k_expand_solo(const DevSpec sp, const BatchArgs<ST> a,
                                                                          int job) {
   constexpr int N = 1 << NQ, E = N * N, EPL = E >= 32 ? E / 32 : 1;
@@ -1323,7 +1332,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, EXP_MINB) k_expand_solo(const 
   WarpTally c;
   for (;;) {
     unsigned long long p = 0;
-    if (lane == 0) p = a.p0 + atomicAdd(&a.st->work, 1ULL);
+    if (lane == 0) p = a.p0 + atomicAdd(PART == 2 ? &a.st->work2 : &a.st->work, 1ULL);
     p = __shfl_sync(FULL, p, 0);
     if ((long long)p >= a.m) break;
 #pragma unroll
@@ -1333,7 +1342,7 @@ __global__ void __launch_bounds__(EXP_WARPS * 32, EXP_MINB) k_expand_solo(const 
     }
     const NodeMeta pm = a.meta[p];
     __syncwarp();
-    expand_parent<NQ, ST>(sp, &s_sp, sm.perm, conjmask, sm.W, P, C, p, pm, sp.depth - t, t < sp.depth, BATCH_GS, o, c,
+    expand_parent<NQ, ST, false, PART>(sp, &s_sp, sm.perm, conjmask, sm.W, P, C, p, pm, sp.depth - t, t < sp.depth, BATCH_GS, o, c,
                           lane);
     __syncwarp();
   }
@@ -2473,7 +2482,11 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
       const long long grid = std::max<long long>(1, std::min<long long>(want, (long long)nsm * 2 * 8));
       if (opt.profile) ck(cudaEventRecord(ev[0], s), "event");
       if (hs.states) k_expand<NQ, ST, true><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(sp, a);
-      else k_expand<NQ, ST, false><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(sp, a);
+      else {                                     // one-qubit gates, then the others: two smaller loop bodies
+        k_expand<NQ, ST, false, 1><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(sp, a);
+        k_expand<NQ, ST, false, 2><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(sp, a);
+        launches++;
+      }
       TBoundArgs<ST> tb;
       tb.R = fR.as<Z4<ST>>(); tb.meta = fMeta.as<NodeMeta>(); tb.tq = tq.as<TQEntry>(); tb.tqcap = tqcap;
       tb.GS = G; tb.rem = depth - t; tb.keep = keep; tb.fjob = nullptr; tb.specs = nullptr; tb.jt = nullptr;
@@ -4344,8 +4357,13 @@ struct BatchImpl : BatchSession::Impl {
         a.gshort = gsd; a.jgoal = jg;
         const long long want = (cm + EXP_WARPS - 1) / EXP_WARPS;
         const long long grid = std::max<long long>(1, std::min<long long>(want, (long long)nsm * tune.expand_blocks_per_sm));
-        if (ch.jobs.size() == 1) k_expand_solo<NQ, ST><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(J[jlo].sp, a, jlo);
-        else k_expand_batch<NQ, ST><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(a);
+        if (ch.jobs.size() == 1) {               // the plain level's two parts
+          k_expand_solo<NQ, ST, 1><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(J[jlo].sp, a, jlo);
+          k_expand_solo<NQ, ST, 2><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(J[jlo].sp, a, jlo);
+          nlaunch++;
+        } else {
+          k_expand_batch<NQ, ST><<<(unsigned)grid, EXP_WARPS * 32, 0, s>>>(a);
+        }
         TBoundArgs<ST> tb;
         tb.R = fR.as<Z4<ST>>(); tb.meta = fMeta.as<NodeMeta>(); tb.tq = tq.as<TQEntry>(); tb.tqcap = tqcap;
         tb.GS = BATCH_GS; tb.rem = 0; tb.keep = 0; tb.fjob = fJob.as<uint32_t>(); tb.specs = dspecs.as<DevSpec>();
