@@ -1191,6 +1191,22 @@ template <typename ST> struct BatchArgs {
   const ulonglong2 *jgoal = nullptr;  // per job: goal children found by the pass, first of them
 };
 
+// a level's statistics block cleared (first found: none), the goal pass's header, and a batch chunk's per-job goal
+// results (none found) — each when given
+__global__ void k_level_init(GoalShort *gs, DevStats *st, ulonglong2 *jg = nullptr, int jn = 0) {
+  const int i = threadIdx.x;
+  constexpr int W = (int)(sizeof(DevStats) / 8);
+  static_assert(sizeof(DevStats) % 8 == 0, "statistics block of 8-byte words");
+  if (st)
+    for (int j = i; j < W; j += blockDim.x) ((unsigned long long *)st)[j] = 0;
+  for (int j = i; j < jn; j += blockDim.x) jg[j] = make_ulonglong2(0ULL, ~0ULL);
+  __syncthreads();
+  if (i == 0) {
+    if (st) st->first_found = ~0ULL;
+    if (gs) { gs->count = 0; gs->found = 0; gs->first = ~0ULL; gs->ovf = 0; gs->pad = 0; }
+  }
+}
+
 // the batch's goal pass: candidate parents (stored lower bound <= 1) of jobs whose spec has the bounds, in nodes
 // [p0, p1); then their children tested for the goal, per job
 __global__ void k_goal_candidates_batch(const NodeMeta *meta, const uint32_t *fjob, const DevSpec *specs, long long p0,
@@ -2451,11 +2467,17 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
     // level and the level kernels return at once)
     GoalShort *gsd = nullptr;
     GoalShort hgs{0, 0, ~0ULL, 0, 0};
-    if (hs.standard && !hs.states && !sp.nogoal && m > 0) {
+    const bool goal_pass = hs.standard && !hs.states && !sp.nogoal && m > 0;
+    if (goal_pass) {
       gshort.ensure(sizeof(GoalShort) + (size_t)GOAL_LIST * 4 + 64);
       gsd = gshort.as<GoalShort>();
+    }
+    // the level's counters and the goal pass's header set on the device (a copy from pageable host memory would
+    // wait for the stream)
+    k_level_init<<<1, 32, 0, s>>>(gsd, stats.as<DevStats>());
+    launches++;
+    if (goal_pass) {
       uint32_t *glist = (uint32_t *)(gsd + 1);
-      ck(cudaMemcpyAsync(gsd, &hgs, sizeof hgs, cudaMemcpyHostToDevice, s), "h2d");
       const unsigned gm_ = (unsigned)std::max<long long>(1, std::min<long long>((m + 255) / 256, (long long)nsm * 8));
       k_goal_candidates<<<gm_, 256, 0, s>>>(fMeta.as<NodeMeta>(), m, glist, gsd);
       k_goal_level<NQ, ST><<<(unsigned)nsm * 2, EXP_WARPS * 32, 0, s>>>(sp, fR.as<Z4<ST>>(), fMeta.as<NodeMeta>(), glist,
@@ -2469,9 +2491,7 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
         sMeta.ensure(cap * sizeof(NodeMeta));
       }
       tq.ensure(tqcap * sizeof(TQEntry));
-      ck(cudaMemsetAsync(dst, 0, sizeof(DevStats), s), "memset");
-      const unsigned long long ffinit = ~0ULL;
-      ck(cudaMemcpyAsync(&dst->first_found, &ffinit, 8, cudaMemcpyHostToDevice, s), "h2d");
+      if (attempt) { k_level_init<<<1, 32, 0, s>>>(nullptr, dst); launches++; }
       ExpandArgs<ST> a;
       a.m = m; a.t = t; a.rem = depth - t; a.keep = keep;
       a.R = fR.as<Z4<ST>>(); a.meta = fMeta.as<NodeMeta>(); a.st = dst; a.cap = cap;
@@ -2499,7 +2519,6 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
       if (opt.profile) ck(cudaEventRecord(ev[1], s), "event");
       ck(cudaMemcpyAsync(hstats, dst, sizeof(DevStats), cudaMemcpyDeviceToHost, s), "d2h");
       d2h += sizeof(DevStats);
-      h2d += 8;
       if (gsd) { ck(cudaMemcpyAsync(&hgs, gsd, sizeof hgs, cudaMemcpyDeviceToHost, s), "d2h"); d2h += sizeof hgs; }
       ck(cudaStreamSynchronize(s), "expand");
       if (gsd && hgs.found && !hgs.ovf && hgs.count <= GOAL_LIST) break;   // the found level (kernels skipped)
@@ -4321,10 +4340,8 @@ struct BatchImpl : BatchSession::Impl {
       GoalShort *gsd = bgoal.as<GoalShort>();
       ulonglong2 *jg = jgoal.as<ulonglong2>();
       {
-        const GoalShort g0{0, 0, ~0ULL, 0, 0};
-        const std::vector<ulonglong2> z(jn, make_ulonglong2(0ULL, ~0ULL));
-        ck(cudaMemcpyAsync(gsd, &g0, sizeof g0, cudaMemcpyHostToDevice, s), "h2d");
-        ck(cudaMemcpyAsync(jg + jlo, z.data(), jn * sizeof(ulonglong2), cudaMemcpyHostToDevice, s), "h2d");
+        k_level_init<<<1, 256, 0, s>>>(gsd, nullptr, jg + jlo, jn);   // (no copies from pageable memory)
+        nlaunch++;
         const unsigned gc = (unsigned)std::max<long long>(1, std::min<long long>((cm + 255) / 256, (long long)nsm * 8));
         k_goal_candidates_batch<<<gc, 256, 0, s>>>(fMeta.as<NodeMeta>(), fJob.as<uint32_t>(), dspecs.as<DevSpec>(),
                                                    ch.p0, ch.p1, (uint32_t *)(gsd + 1), gsd);
