@@ -109,9 +109,11 @@ inline size_t scan_partials_words(size_t n) { return (n + SCAN_CHUNK - 1) / SCAN
 //  * k_sort_onesweep, per pass, takes tiles of OS_TILE keys in the order of an atomic ticket. A tile counts its
 //    digits, publishes them, and finds the keys of earlier tiles per digit by looking back over their published
 //    words (decoupled look-back: an earlier tile's word is either its own count or, once its look-back is done, the
-//    inclusive prefix; walking back stops at the first prefix). It then ranks its keys stably in shared memory
-//    (warp match + per-warp digit counts, round by round in input order), places them there in digit order, and
-//    writes them out so that neighbouring threads write neighbouring addresses.
+//    inclusive prefix; walking back stops at the first prefix). Its keys are ranked stably without block barriers
+//    between rounds: each warp holds a contiguous eighth of the tile and ranks its keys among its own (warp match,
+//    one counter update per digit group), a scan over the warps' counts per digit joins the eighths, and the keys are
+//    placed in shared memory in digit order and written out so that neighbouring threads write neighbouring
+//    addresses.
 // A tile waits only for tiles with smaller tickets, whose blocks are already running, so the waits end; every wait
 // is still bounded (OS_SPIN_MAX polls). Should one give up, the tile counts the earlier tiles' digits itself from
 // the input (slow, still exact) and the sort records it (sort_failed), so a result is never wrong and nothing hangs.
@@ -183,14 +185,14 @@ __device__ __forceinline__ uint32_t os_block_scan(uint32_t v, uint32_t *ws) {
 }
 
 template <bool LOOKBACK>
-__global__ void __launch_bounds__(OS_THREADS, 5) k_sort_onesweep(const uint64_t *kin, const uint32_t *vin, uint64_t *kout,
+__global__ void __launch_bounds__(OS_THREADS, 4) k_sort_onesweep(const uint64_t *kin, const uint32_t *vin, uint64_t *kout,
                                                                uint32_t *vout, size_t n, int shift, int pass,
                                                                uint32_t *head, unsigned long long *status,
                                                                unsigned *err, const uint32_t *offs, uint32_t ntiles) {
   constexpr int NW = OS_THREADS / 32;
   __shared__ uint64_t sk[OS_TILE];
   __shared__ uint32_t sv[OS_TILE];
-  __shared__ uint32_t cnt[256], lex[256], run[256], wcnt[NW][256], ws[NW];
+  __shared__ uint32_t lex[256], run[256], wcnt[NW][256], ws[NW];
   __shared__ unsigned long long gbase[256];
   __shared__ unsigned ticket;
   __shared__ int fallback;
@@ -198,27 +200,48 @@ __global__ void __launch_bounds__(OS_THREADS, 5) k_sort_onesweep(const uint64_t 
   const uint32_t *counts = head + pass * 256;
   unsigned *tickets = head + 256 * OS_MAXPASS;
   if (tid == 0) { ticket = LOOKBACK ? atomicAdd(&tickets[pass], 1u) : blockIdx.x; fallback = 0; }
-  cnt[tid] = 0;
   for (int x = 0; x < NW; x++) wcnt[x][tid] = 0;
   __syncthreads();
   const size_t tile = ticket, start = tile * OS_TILE;
   const unsigned long long tag = (unsigned long long)(pass + 1) << 60;
+  // warp w holds tile positions [w * 32 * OS_ITEMS, (w + 1) * 32 * OS_ITEMS), round r lane l the position
+  // w * 32 * OS_ITEMS + 32 r + l: input order is (warp, round, lane)
   uint64_t key[OS_ITEMS];
-  uint32_t val[OS_ITEMS];
+  uint32_t val[OS_ITEMS], wr[OS_ITEMS];
   int dig[OS_ITEMS];
 #pragma unroll
-  for (int r = 0; r < OS_ITEMS; r++) {            // striped: round r holds positions start + r * 256 + tid
-    const size_t i = start + (size_t)r * OS_THREADS + tid;
+  for (int r = 0; r < OS_ITEMS; r++) {
+    const size_t i = start + (size_t)w * 32 * OS_ITEMS + 32 * r + lane;
     dig[r] = 256;
     if (i < n) {
       key[r] = kin[i];
       val[r] = vin[i];
       dig[r] = (int)((key[r] >> shift) & 255);
-      atomicAdd(&cnt[dig[r]], 1u);
     }
   }
+  // each warp's digit counts and every key's rank among its warp's keys of the same digit (earlier rounds, then
+  // lower lanes): one leader per digit group updates the warp's counter, so no atomics and no block barrier
+  const unsigned lt = (1u << lane) - 1;
+#pragma unroll
+  for (int r = 0; r < OS_ITEMS; r++) {
+    const int d = dig[r];
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const int leader = __ffs(peers) - 1;
+    uint32_t old = 0;
+    if (d < 256 && lane == leader) { old = wcnt[w][d]; wcnt[w][d] = old + (uint32_t)__popc(peers); }
+    old = __shfl_sync(0xffffffffu, old, leader);
+    wr[r] = old + (uint32_t)__popc(peers & lt);
+    __syncwarp();
+  }
   __syncthreads();
-  const uint32_t mine = cnt[tid];
+  // per digit tid: the warps' counts become exclusive prefixes (earlier warps' keys of the digit); the tile's count
+  uint32_t mine = 0;
+#pragma unroll
+  for (int x = 0; x < NW; x++) {
+    const uint32_t t = wcnt[x][tid];
+    wcnt[x][tid] = mine;
+    mine += t;
+  }
   if constexpr (LOOKBACK) {
     // this tile's count of digit tid: publish it, then add up the earlier tiles' counts by looking back
     unsigned long long *st = status + tile * 256 + tid;
@@ -258,30 +281,19 @@ __global__ void __launch_bounds__(OS_THREADS, 5) k_sort_onesweep(const uint64_t 
   } else {
     gbase[tid] = offs[(size_t)tid * ntiles + tile];   // the scanned digit-major tile histograms
   }
-  const uint32_t lx = os_block_scan(mine, ws);
-  lex[tid] = lx;
-  run[tid] = lx;
+  lex[tid] = os_block_scan(mine, ws);             // keys of smaller digits in this tile
   __syncthreads();
-  // stable local ranks, round by round in input order; keys placed in shared memory in digit order
-  const unsigned lt = (1u << lane) - 1;
+  // each key to its place in the tile's digit order: smaller digits, earlier warps' keys of its digit, its rank
 #pragma unroll
   for (int r = 0; r < OS_ITEMS; r++) {
     const int d = dig[r];
-    const unsigned peers = __match_any_sync(0xffffffffu, d);
-    const bool leader = lane == __ffs(peers) - 1;
-    if (d < 256 && leader) wcnt[w][d] = __popc(peers);
-    __syncthreads();
     if (d < 256) {
-      uint32_t pre = 0;
-      for (int x = 0; x < w; x++) pre += wcnt[x][d];
-      const uint32_t pos = run[d] + pre + __popc(peers & lt);
+      const uint32_t pos = lex[d] + wcnt[w][d] + wr[r];
       sk[pos] = key[r];
       sv[pos] = val[r];
     }
-    __syncthreads();
-    if (d < 256 && leader) { atomicAdd(&run[d], (uint32_t)__popc(peers)); wcnt[w][d] = 0; }
-    __syncthreads();
   }
+  __syncthreads();
   const int tn = (int)(n - start < (size_t)OS_TILE ? n - start : (size_t)OS_TILE);
   for (int i = tid; i < tn; i += OS_THREADS) {
     const uint64_t k = sk[i];
