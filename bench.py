@@ -591,6 +591,7 @@ def systems(eng, args):
         f.write_text(text)
         subprocess.run([str(exes[kind]), str(f)], cwd=tmp, capture_output=True, timeout=600)
     t_cli = time.perf_counter() - t0
+    eng.trim()                                     # the server runs its own engines: give them this one's buffers
     srv = cz.Server(memory_gb=180.0)               # the admission limit of the serving configuration
     warm = [srv.submit(k, t) for k, t, _, _ in [next(r for r in reqs if r[0] == 1), next(r for r in reqs if r[0] == 2)]]
     srv.wait(2, 900)
