@@ -2445,6 +2445,13 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
   const int G = hs.G;
   long long m = front_m;
   double surv_rate = 1.0;                              // survivors per child of the previous level
+  bool ded_pending = false;                            // a level's dedupe events recorded, not yet read
+  auto read_dedupe = [&]() {                           // (after a wait on the stream)
+    if (!ded_pending) return;
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, ev[2], ev[3]) == cudaSuccess) res.dedupe_ms += ms;
+    ded_pending = false;
+  };
   if ((int)level_n.size() < t_start) level_n.resize(t_start, 0);
   for (int t = t_start; t <= depth && t <= stop; t++) {
     const double t0 = now_s();
@@ -2521,6 +2528,7 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
       d2h += sizeof(DevStats);
       if (gsd) { ck(cudaMemcpyAsync(&hgs, gsd, sizeof hgs, cudaMemcpyDeviceToHost, s), "d2h"); d2h += sizeof hgs; }
       ck(cudaStreamSynchronize(s), "expand");
+      read_dedupe();
       if (gsd && hgs.found && !hgs.ovf && hgs.count <= GOAL_LIST) break;   // the found level (kernels skipped)
       if (opt.profile) { float ms = 0; cudaEventElapsedTime(&ms, ev[0], ev[1]); res.expand_ms += ms; }
       if (hstats->ovf) return -2;                       // promote to int64 limbs and redo this level
@@ -2670,9 +2678,10 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
         launches++;
       }
       if (building && distinct) seen_add(*building, distinct, t);
-      if (opt.profile) ck(cudaEventRecord(ev[3], s), "event");
-      ck(cudaStreamSynchronize(s), "gather");
-      if (opt.profile) { float ms = 0; cudaEventElapsedTime(&ms, ev[2], ev[3]); res.dedupe_ms += ms; }
+      // no wait here: the next level's work queues behind the gather on the stream (the host only needs the
+      // counts it already has); the dedupe's device time is read at the next wait
+      if (opt.profile) { ck(cudaEventRecord(ev[3], s), "event"); ded_pending = true; }
+      ck(cudaGetLastError(), "gather");
     }
     L.distinct = distinct;
     L.proved_unsat = distinct == 0;
@@ -2680,14 +2689,16 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
     L.dir = building ? 1 : level_dir;
     res.levels = t;
     cb(L);
-    if (!distinct) return RC_PROOF;
+    if (!distinct) { ck(cudaStreamSynchronize(s), "gather"); read_dedupe(); return RC_PROOF; }
     m = distinct;
     front_m = m;
     if ((int)level_n.size() <= t) level_n.resize(t + 1, 0);
     level_n[t] = distinct;
     t_start = t + 1;
-    if (t == stop) return RC_STOP;
+    if (t == stop) { ck(cudaStreamSynchronize(s), "gather"); read_dedupe(); return RC_STOP; }
   }
+  ck(cudaStreamSynchronize(s), "gather");
+  read_dedupe();
   return RC_PROOF;   // stopped at the last level (not reachable: the last level keeps nothing)
 }
 
