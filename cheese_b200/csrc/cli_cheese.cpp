@@ -45,7 +45,7 @@ int main(int argc, char **argv) {
     if (!std::strcmp(argv[i], "--depth") && i + 1 < argc) depth = std::atoi(argv[++i]);
     else if (!std::strcmp(argv[i], "--no-dedupe")) opt.dedupe = 0;
     else if (!std::strcmp(argv[i], "--chunk") && i + 1 < argc) ++i;      // the whole level runs in one launch
-    else if (!std::strcmp(argv[i], "--profile")) profile = 1;
+    else if (!std::strcmp(argv[i], "--profile")) profile = 2;   // both phases timed
     else if (!std::strcmp(argv[i], "--mitm")) mitm = 1;
     else if (!std::strcmp(argv[i], "--no-sym")) opt.sym = 0;
     else if (!std::strcmp(argv[i], "--table") && i + 1 < argc) tablek = std::atoi(argv[++i]);

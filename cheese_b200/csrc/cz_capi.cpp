@@ -163,7 +163,7 @@ int cz_search(cz_engine *engine, const cz_spec *spec, const cz_options *opt, cz_
     return CZ_ERR_USAGE;
   }
   cz::Options eo;
-  eo.depth = depth; eo.dedupe = o.dedupe != 0; eo.sym = o.sym != 0; eo.store64 = o.store64; eo.profile = o.profile != 0;
+  eo.depth = depth; eo.dedupe = o.dedupe != 0; eo.sym = o.sym != 0; eo.store64 = o.store64; eo.profile = o.profile < 0 ? 0 : o.profile;
   if (o.table_k < 0 || o.table_k > CZ_MAX_DEPTH) {
     put_err(out->error, sizeof out->error, "table depth out of range");
     out->rc = CZ_ERR_USAGE;

@@ -14,7 +14,7 @@ struct Options {
   bool dedupe = true;        // --no-dedupe
   bool sym = true;           // --no-sym
   int store64 = 0;           // 0: int32 residual limbs, promoted to int64 when a value leaves int32; 1: int64 from the start
-  bool profile = false;      // per-phase device times (CUDA events on the engine's stream)
+  int profile = 0;           // device times (CUDA events on the engine's stream): 1 level kernels, 2 also the dedupe
   bool nogoal = false;       // never report the goal (distance-table build)
   int table_k = 0;           // --table K
   std::string cache_dir = "build";   // distance-table cache directory ("" : no cache)

@@ -2584,7 +2584,7 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
     long long distinct = 0;
     const size_t ns = keep ? (size_t)h.n_surv : 0;
     if (ns) {
-      if (opt.profile) ck(cudaEventRecord(ev[2], s), "event");
+      if (opt.profile > 1) ck(cudaEventRecord(ev[2], s), "event");
       k0.ensure(ns * 8); k1.ensure(ns * 8); v0.ensure(ns * 4); v1.ensure(ns * 4);
       kidx.ensure(ns * 8); kslot.ensure(ns * 4);
       hist.ensure(sort_hist_words(ns) * 4);
@@ -2680,7 +2680,7 @@ int Engine::Impl::levels(const HostSpec &hs, const DevSpec &sp, const Options &o
       if (building && distinct) seen_add(*building, distinct, t);
       // no wait here: the next level's work queues behind the gather on the stream (the host only needs the
       // counts it already has); the dedupe's device time is read at the next wait
-      if (opt.profile) { ck(cudaEventRecord(ev[3], s), "event"); ded_pending = true; }
+      if (opt.profile > 1) { ck(cudaEventRecord(ev[3], s), "event"); ded_pending = true; }
       ck(cudaGetLastError(), "gather");
     }
     L.distinct = distinct;

@@ -56,7 +56,8 @@ typedef struct {
   int dedupe;       /* 1; 0: --no-dedupe */
   int sym;          /* 1; 0: --no-sym */
   int store64;      /* 0: int32 limbs promoted to int64 on demand; 1: int64 limbs throughout */
-  int profile;      /* 1: record device times per phase (cz_result.expand_ms / dedupe_ms) */
+  int profile;      /* 1: device time of the level kernels (cz_result.expand_ms); 2: also of the dedupe (dedupe_ms).
+                     * Each timed phase adds two events per level to the stream. */
   int table_k;      /* --table K: 0 none; K > 0 the distance table of the last K gates (cheese.cu:1431-1593) */
   const char *cache_dir;   /* distance-table cache directory ("build" by default; NULL: no cache) */
   int mitm;         /* --mitm: meet in the middle (cheese.cu:1595-1760); symmetry classes off, like the reference */
@@ -86,7 +87,7 @@ typedef struct {
   int64_t kernel_launches;     /* device kernels launched by this call */
   int64_t t_evals;             /* Walsh-Hadamard T-bound evaluations */
   int64_t children;            /* children evaluated past the window rules */
-  double expand_ms, dedupe_ms; /* device time per phase (profile = 1) */
+  double expand_ms, dedupe_ms; /* device time per phase (profile >= 1, profile = 2) */
   double total_ms;             /* host wall time of the call */
   int64_t expand_launches;     /* launches of the level kernel */
   int64_t h2d_bytes, d2h_bytes;/* host<->device bytes moved by the call */
