@@ -131,12 +131,14 @@ CZ_RUS_FN int low_bit(uint32_t m) {
 CZ_RUS_FN int rm_equiv(const RM &A, const RM &B, const RDev &sp) {
   if (A.e != B.e) return -1;
   const int gen[4] = {1, 3, 4, 12};
+  int la[NR];                                   // A's row signs, read once for the four generators
+  for (int r = 1; r < NR; r++) la[r] = row_lead_sign(A, r);
   uint32_t mask[4];
   for (int g = 0; g < 4; g++) {
     const int sb = row_lead_sign(B, gen[g]);
     uint32_t m = 0;
     for (int r = 1; r < NR; r++) {
-      const int sa = row_lead_sign(A, r);
+      const int sa = la[r];
       if (!sa && !sb) m |= 3u << (2 * (r - 1));                        // zero rows: equal with either sign
       else if (sa && sb && row_eq(A, r, sa * sb, B, gen[g])) m |= 1u << (2 * (r - 1) + (sa * sb < 0));
     }
