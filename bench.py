@@ -593,8 +593,9 @@ def systems(eng, args):
     t_cli = time.perf_counter() - t0
     eng.trim()                                     # the server runs its own engines: give them this one's buffers
     srv = cz.Server(memory_gb=180.0)               # the admission limit of the serving configuration
-    warm = [srv.submit(k, t) for k, t, _, _ in [next(r for r in reqs if r[0] == 1), next(r for r in reqs if r[0] == 2)]]
-    srv.wait(2, 900)
+    for k, t, d, _ in [next(r for r in reqs if r[0] == kind) for kind in (0, 1, 2)]:   # one request of each kind
+        srv.submit(k, t, d)                        # first: its engines, tables and batch session set up
+    srv.wait(3, 900)
     rates = {}
     for rate in (10, 30, 100, 300, 1000):
         arr = tcwork.poisson_arrivals(rate, N, rate)
