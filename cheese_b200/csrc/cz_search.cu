@@ -4397,7 +4397,14 @@ struct BatchImpl : BatchSession::Impl {
         tb.GS = BATCH_GS; tb.rem = 0; tb.keep = 0; tb.fjob = fJob.as<uint32_t>(); tb.specs = dspecs.as<DevSpec>();
         tb.jt = jt.as<int>(); tb.jst = jst.as<DevStats>(); tb.st = dst; tb.cap = cap; tb.sh1 = sH1.as<uint64_t>();
         tb.sh2 = sH2.as<uint64_t>(); tb.sidx = sIdx.as<uint64_t>(); tb.smeta = sMeta.as<NodeMeta>();
-        k_tbound<NQ, ST, true><<<(unsigned)(nsm * tune.tbound_blocks_per_sm), TB_WARPS * 32, 0, s>>>(DevSpec{}, tb);
+        if (ch.jobs.size() == 1) {               // one job: the plain kernel, its spec a parameter (its tallies go
+          const Job &jj = J[jlo];                 // to the chunk's block and are added to the job's below)
+          tb.fjob = nullptr; tb.specs = nullptr; tb.jt = nullptr; tb.jst = nullptr;
+          tb.rem = jj.sp.depth - jj.t; tb.keep = jj.t < jj.sp.depth;
+          k_tbound<NQ, ST, false><<<(unsigned)(nsm * tune.tbound_blocks_per_sm), TB_WARPS * 32, 0, s>>>(jj.sp, tb);
+        } else {
+          k_tbound<NQ, ST, true><<<(unsigned)(nsm * tune.tbound_blocks_per_sm), TB_WARPS * 32, 0, s>>>(DevSpec{}, tb);
+        }
         nlaunch += 2;
         ck(cudaGetLastError(), "batched expand");
         // the chunk's counters, the jobs' statistics and the goal pass's results, read back with one wait
@@ -4412,6 +4419,11 @@ struct BatchImpl : BatchSession::Impl {
         tqcap = std::max<unsigned long long>(tqcap, h.n_tq);
       }
       if (h.surv_overflow || h.n_tq > tqcap) throw std::runtime_error("survivor or T queue overflow");
+      if (ch.jobs.size() == 1) {                 // the one-job T kernel's tallies, kept in the chunk's block
+        DevStats &d = hj[jlo];
+        d.dead += h.dead; d.alive += h.alive; d.t_evals += h.t_evals;
+        if (h.ovf) d.ovf = 1;
+      }
       if (!hgs.ovf && hgs.count <= GOAL_LIST)            // jobs found by the goal pass (their level kernels skipped)
         for (int i : ch.jobs)
           if (hjg[i - jlo].x) { hj[i].found = hjg[i - jlo].x; hj[i].first_found = hjg[i - jlo].y; }
