@@ -1234,12 +1234,16 @@ __global__ void __launch_bounds__(EXP_WARPS * 32) k_goal_level_batch(const DevSp
   if (n > GOAL_LIST) return;                   // incomplete list: no shortcut in this chunk
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   DevSpec &sp = sps[w];
+  int cur = -1;                                // the job whose spec the warp holds
   for (unsigned long long i = blockIdx.x * (unsigned long long)EXP_WARPS + w; i < n;
        i += (unsigned long long)gridDim.x * EXP_WARPS) {
     const uint32_t p = list[i];
     const int job = (int)fjob[p];
     __syncwarp();
-    for (int x = lane; x < (int)(sizeof(DevSpec) / 4); x += 32) ((int *)&sp)[x] = ((const int *)(specs + job))[x];
+    if (job != cur) {
+      for (int x = lane; x < (int)(sizeof(DevSpec) / 4); x += 32) ((int *)&sp)[x] = ((const int *)(specs + job))[x];
+      cur = job;
+    }
     const NodeMeta pm = meta[p];
     const int g1 = pm.g1 == 0xff ? -1 : pm.g1, g2 = pm.g2 == 0xff ? -1 : pm.g2;
 #pragma unroll
