@@ -4468,8 +4468,12 @@ struct BatchImpl : BatchSession::Impl {
       const unsigned gs = (unsigned)std::max<size_t>(1, std::min<size_t>((nsort + 255) / 256, (size_t)nsm * 16));
       k_runs<<<gs, 256, 0, s>>>(sk, sv, nsort, sIdx.as<uint64_t>(), kidx.as<uint64_t>(), kslot.as<uint32_t>(),
                                 work.as<uint2>(), dst);
+      // a one-job chunk passes its job's spec as the kernels' parameter (a shared copy, as in the plain level)
+      const bool one = ch.jobs.size() == 1;
+      const DevSpec one_sp = one ? J[jlo].sp : DevSpec{};
       k_resolve<NQ, ST><<<(unsigned)nsm * 8, RES_WARPS * 32, 0, s>>>(
-          DevSpec{}, dspecs.as<DevSpec>(), fJob.as<uint32_t>(), BATCH_GS, fR.as<Z4<ST>>(), fMeta.as<NodeMeta>(),
+          one_sp, one ? nullptr : dspecs.as<DevSpec>(), one ? nullptr : fJob.as<uint32_t>(), BATCH_GS, fR.as<Z4<ST>>(),
+          fMeta.as<NodeMeta>(),
           work.as<uint2>(), sv, sH1.as<uint64_t>(), sH2.as<uint64_t>(), sIdx.as<uint64_t>(), sMeta.as<NodeMeta>(),
           tmp.as<uint32_t>(), kidx.as<uint64_t>(), kslot.as<uint32_t>(), dst);
       nlaunch += 2;
@@ -4502,7 +4506,7 @@ struct BatchImpl : BatchSession::Impl {
       const unsigned gg = (unsigned)std::max<size_t>(1, std::min<size_t>((distinct + RES_WARPS - 1) / RES_WARPS,
                                                                          (size_t)nsm * 16));
       k_materialize<NQ, ST><<<gg, RES_WARPS * 32, 0, s>>>(
-          DevSpec{}, dspecs.as<DevSpec>(), fJob.as<uint32_t>(), BATCH_GS, fR.as<Z4<ST>>(), fMeta.as<NodeMeta>(), ki, vi,
+          one_sp, one ? nullptr : dspecs.as<DevSpec>(), fJob.as<uint32_t>(), BATCH_GS, fR.as<Z4<ST>>(), fMeta.as<NodeMeta>(), ki, vi,
           distinct, sMeta.as<NodeMeta>(), fR2.as<Z4<ST>>() + o0 * E, fMeta2.as<NodeMeta>() + o0,
           tpar[nstep].as<uint32_t>() + o0, tgat[nstep].as<uint8_t>() + o0, fJob2.as<uint32_t>() + o0);
       nlaunch++;
